@@ -1,0 +1,316 @@
+"""ctypes binding of the C oracle (``oracle/loki_oracle.c``). Test infrastructure only."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+
+MAX_LEVELS = 40
+MAX_PARAMS = 5
+MAX_WIDTHS = 64
+
+u64 = ctypes.c_uint64
+u32 = ctypes.c_uint32
+f64 = ctypes.c_double
+f32 = ctypes.c_float
+vp = ctypes.c_void_p
+
+
+class Cfg(ctypes.Structure):
+    _fields_ = [
+        ("nsamps", u64),
+        ("tsamp", f64),
+        ("nbins", u64),
+        ("eta", f64),
+        ("nparams", u32),
+        ("limits", f64 * (2 * MAX_PARAMS)),
+        ("bseg_brute", u64),
+        ("bseg_ffa", u64),
+        ("ducy_max", f64),
+        ("wtsp", f64),
+    ]
+
+
+class Plan(ctypes.Structure):
+    _fields_ = [
+        ("nparams", u32),
+        ("n_levels", u32),
+        ("nsamps", u64),
+        ("nbins", u64),
+        ("tsamp", f64),
+        ("eta", f64),
+        ("tseg_brute", f64),
+        ("bseg_brute", u64),
+        ("bseg_ffa", u64),
+        ("limits", f64 * (2 * MAX_PARAMS)),
+        ("segment_lens", u64 * MAX_LEVELS),
+        ("nsegments", u64 * MAX_LEVELS),
+        ("tsegments", f64 * MAX_LEVELS),
+        ("ncoords", u64 * MAX_LEVELS),
+        ("ncoords_offsets", u32 * (MAX_LEVELS + 1)),
+        ("param_counts", (u64 * MAX_PARAMS) * MAX_LEVELS),
+        ("dparams", (f64 * MAX_PARAMS) * MAX_LEVELS),
+        ("buffer_size", u64),
+        ("coord_size", u64),
+        ("n_widths", u32),
+        ("widths", u64 * MAX_WIDTHS),
+    ]
+
+
+COORD_FREQ_DTYPE = np.dtype([("idx", np.uint32), ("shift", np.float32)])
+COORD_DTYPE = np.dtype(
+    [("i_tail", np.uint32), ("shift_tail", np.float32), ("i_head", np.uint32), ("shift_head", np.float32)]
+)
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError(f"oracle library missing: {_LIB_PATH} (run `make -C oracle oracle`)")
+        L = ctypes.CDLL(_LIB_PATH)
+        L.lko_last_error.restype = ctypes.c_char_p
+        L.lko_phase_idx.restype = f32
+        L.lko_phase_idx.argtypes = [f64, f64, u64, f64]
+        L.lko_phase_idx_uint.restype = u32
+        L.lko_phase_idx_uint.argtypes = [f64, f64, u64, f64]
+        L.lko_param_val_at_idx.restype = f64
+        L.lko_param_val_at_idx.argtypes = [f64, f64, u64, u64]
+        L.lko_nearest_idx.restype = u64
+        L.lko_nearest_idx.argtypes = [f64, f64, f64, u64]
+        L.lko_range_param.restype = u64
+        L.lko_range_param.argtypes = [f64, f64, f64, vp, u64]
+        L.lko_box_widths.restype = u64
+        L.lko_box_widths.argtypes = [u64, f64, f64, vp, u64]
+        L.lko_brute_fold.argtypes = [vp, vp, u64, vp, u64, u64, u64, f64, f64, vp]
+        L.lko_phase_map.argtypes = [vp, u64, u64, u64, f64, f64, vp]
+        L.lko_merge_freq.argtypes = [vp, vp, vp, u64, u64, u64, u64]
+        L.lko_merge_taylor.argtypes = [vp, vp, vp, u64, u64, u64, u64]
+        L.lko_ffa.argtypes = [vp, vp, vp, u32, vp]
+        L.lko_snr_boxcar_3d.argtypes = [vp, u64, u64, vp, u64, vp]
+        L.lko_snr_boxcar_3d_max.argtypes = [vp, u64, u64, vp, u64, vp]
+        L.lko_snr_boxcar_2d_max.argtypes = [vp, u64, u64, vp, u64, f32, vp]
+        L.lko_circular_prefix_sum.argtypes = [vp, vp, u64, u64]
+        L.lko_compact.restype = u64
+        L.lko_compact.argtypes = [vp, u64, f32, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(lib().lko_last_error().decode())
+
+
+def make_cfg(
+    nsamps: int,
+    tsamp: float,
+    nbins: int,
+    eta: float,
+    param_limits,
+    bseg_brute: int | None = None,
+    bseg_ffa: int | None = None,
+    ducy_max: float = 0.2,
+    wtsp: float = 1.5,
+) -> Cfg:
+    lim = np.asarray(param_limits, dtype=np.float64).reshape(-1, 2)
+    c = Cfg()
+    c.nsamps = nsamps
+    c.tsamp = tsamp
+    c.nbins = nbins
+    c.eta = eta
+    c.nparams = lim.shape[0]
+    for i, (a, b) in enumerate(lim):
+        c.limits[2 * i] = a
+        c.limits[2 * i + 1] = b
+    c.bseg_brute = bseg_brute or 0
+    c.bseg_ffa = bseg_ffa or 0
+    c.ducy_max = ducy_max
+    c.wtsp = wtsp
+    return c
+
+
+@dataclass
+class OraclePlan:
+    raw: Plan
+
+    @property
+    def n_levels(self) -> int:
+        return self.raw.n_levels
+
+    @property
+    def nparams(self) -> int:
+        return self.raw.nparams
+
+    @property
+    def nbins(self) -> int:
+        return self.raw.nbins
+
+    @property
+    def ncoords(self) -> np.ndarray:
+        return np.array(self.raw.ncoords[: self.n_levels], dtype=np.uint64)
+
+    @property
+    def nsegments(self) -> np.ndarray:
+        return np.array(self.raw.nsegments[: self.n_levels], dtype=np.uint64)
+
+    @property
+    def segment_lens(self) -> np.ndarray:
+        return np.array(self.raw.segment_lens[: self.n_levels], dtype=np.uint64)
+
+    @property
+    def ncoords_offsets(self) -> np.ndarray:
+        return np.array(self.raw.ncoords_offsets[: self.n_levels + 1], dtype=np.uint32)
+
+    @property
+    def param_counts(self) -> np.ndarray:
+        return np.array([list(self.raw.param_counts[l][: self.nparams]) for l in range(self.n_levels)], dtype=np.uint64)
+
+    @property
+    def dparams(self) -> np.ndarray:
+        return np.array([list(self.raw.dparams[l][: self.nparams]) for l in range(self.n_levels)])
+
+    @property
+    def widths(self) -> np.ndarray:
+        return np.array(self.raw.widths[: self.raw.n_widths], dtype=np.uint64)
+
+    @property
+    def buffer_size(self) -> int:
+        return self.raw.buffer_size
+
+    @property
+    def coord_size(self) -> int:
+        return self.raw.coord_size
+
+    def fold_size(self, level: int | None = None) -> int:
+        l = self.n_levels - 1 if level is None else level
+        return int(self.nsegments[l] * self.ncoords[l] * 2 * self.nbins)
+
+    def freqs0(self) -> np.ndarray:
+        r = self.raw
+        np_ = self.nparams
+        n = int(r.param_counts[0][np_ - 1])
+        out = np.zeros(n, dtype=np.float64)
+        lib().lko_range_param(r.limits[2 * (np_ - 1)], r.limits[2 * (np_ - 1) + 1], r.dparams[0][np_ - 1], _p(out), n)
+        return out
+
+    def t_ref0(self) -> float:
+        return 0.0 if self.nparams == 1 else self.raw.tsegments[0] / 2.0
+
+
+def plan_create(cfg: Cfg) -> OraclePlan:
+    p = Plan()
+    _check(lib().lko_plan_create(ctypes.byref(cfg), ctypes.byref(p)))
+    return OraclePlan(p)
+
+
+def resolve(plan: OraclePlan) -> np.ndarray:
+    if plan.nparams == 1:
+        out = np.zeros(plan.coord_size, dtype=COORD_FREQ_DTYPE)
+        _check(lib().lko_resolve_freq(ctypes.byref(plan.raw), _p(out)))
+    else:
+        out = np.zeros(plan.coord_size, dtype=COORD_DTYPE)
+        _check(lib().lko_resolve_taylor(ctypes.byref(plan.raw), _p(out)))
+    return out
+
+
+def brute_fold(ts_e, ts_v, freqs, segment_len, nbins, tsamp, t_ref=0.0) -> np.ndarray:
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+    nseg = ts_e.size // segment_len
+    out = np.zeros(nseg * freqs.size * 2 * nbins, dtype=np.float32)
+    _check(lib().lko_brute_fold(_p(ts_e), _p(ts_v), ts_e.size, _p(freqs), freqs.size, segment_len, nbins, tsamp, t_ref, _p(out)))
+    return out
+
+
+def phase_map(freqs, segment_len, nbins, tsamp, t_ref=0.0) -> np.ndarray:
+    freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+    out = np.zeros((freqs.size, segment_len), dtype=np.uint32)
+    lib().lko_phase_map(_p(freqs), freqs.size, segment_len, nbins, tsamp, t_ref, _p(out))
+    return out
+
+
+def ffa(plan: OraclePlan, ts_e, ts_v, level: int | None = None) -> np.ndarray:
+    l = plan.n_levels - 1 if level is None else level
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    out = np.zeros(plan.fold_size(l), dtype=np.float32)
+    _check(lib().lko_ffa(ctypes.byref(plan.raw), _p(ts_e), _p(ts_v), l, _p(out)))
+    return out
+
+
+def snr_boxcar_3d(folds, widths, nbins) -> np.ndarray:
+    folds = np.ascontiguousarray(folds, dtype=np.float32)
+    w = np.ascontiguousarray(widths, dtype=np.uint64)
+    nprof = folds.size // (2 * nbins)
+    out = np.zeros((nprof, w.size), dtype=np.float32)
+    lib().lko_snr_boxcar_3d(_p(folds), nprof, nbins, _p(w), w.size, _p(out))
+    return out
+
+
+def snr_boxcar_3d_max(folds, widths, nbins) -> np.ndarray:
+    folds = np.ascontiguousarray(folds, dtype=np.float32)
+    w = np.ascontiguousarray(widths, dtype=np.uint64)
+    nprof = folds.size // (2 * nbins)
+    out = np.zeros(nprof, dtype=np.float32)
+    lib().lko_snr_boxcar_3d_max(_p(folds), nprof, nbins, _p(w), w.size, _p(out))
+    return out
+
+
+def snr_boxcar_2d_max(folds, widths, nbins, stdnoise=1.0) -> np.ndarray:
+    folds = np.ascontiguousarray(folds, dtype=np.float32)
+    w = np.ascontiguousarray(widths, dtype=np.uint64)
+    nprof = folds.size // nbins
+    out = np.zeros(nprof, dtype=np.float32)
+    lib().lko_snr_boxcar_2d_max(_p(folds), nprof, nbins, _p(w), w.size, stdnoise, _p(out))
+    return out
+
+
+def circular_prefix_sum(x, nsum) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.zeros(nsum, dtype=np.float32)
+    lib().lko_circular_prefix_sum(_p(x), _p(out), x.size, nsum)
+    return out
+
+
+def compact(scores, snr_min) -> tuple[np.ndarray, np.ndarray]:
+    s = np.ascontiguousarray(scores, dtype=np.float32).ravel()
+    idx = np.zeros(s.size, dtype=np.uint32)
+    val = np.zeros(s.size, dtype=np.float32)
+    n = lib().lko_compact(_p(s), s.size, snr_min, _p(idx), _p(val))
+    return idx[:n].copy(), val[:n].copy()
+
+
+def box_widths(nbins, ducy_max=0.2, wtsp=1.5) -> np.ndarray:
+    out = np.zeros(MAX_WIDTHS, dtype=np.uint64)
+    n = lib().lko_box_widths(nbins, ducy_max, wtsp, _p(out), MAX_WIDTHS)
+    return out[:n].copy()
+
+
+def phase_idx(t, f, nbins, delay=0.0) -> float:
+    return lib().lko_phase_idx(t, f, nbins, delay)
+
+
+def phase_idx_uint(t, f, nbins, delay=0.0) -> int:
+    return lib().lko_phase_idx_uint(t, f, nbins, delay)
+
+
+def nearest_idx(val, vmin, vmax, count) -> int:
+    return lib().lko_nearest_idx(val, vmin, vmax, count)
+
+
+def param_val_at_idx(vmin, vmax, count, i) -> float:
+    return lib().lko_param_val_at_idx(vmin, vmax, count, i)

@@ -1,0 +1,142 @@
+/* Test infrastructure only: the CPU oracle for the loki time-domain FFA path.
+ *
+ * A plain-C restatement of the reference's algorithm, used by tests/, by
+ * __graft_entry__.smoke() and by bench.py's cpu_baseline leg as the checker.
+ * The product (loki_b200) never links or calls it. Every function names the
+ * reference file:line it restates. Arithmetic is written operation by
+ * operation in the reference's order so that, built with
+ * -O2 -fno-fast-math -ffp-contract=off, the results are bit-identical to the
+ * reference's own code built with the same flags (checked against
+ * oracle/_ref in tests/test_oracle_vs_ref.py and the committed fixtures).
+ */
+#ifndef LOKI_ORACLE_H
+#define LOKI_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LKO_MAX_LEVELS 40
+#define LKO_MAX_PARAMS 5
+#define LKO_MAX_WIDTHS 64
+
+/* Search configuration (subset of PulsarSearchConfig, include/loki/search/
+ * configs.hpp:25-47). limits holds (min, max) pairs ordered (..., accel, freq).
+ * bseg_brute / bseg_ffa == 0 select the reference defaults. */
+typedef struct lko_cfg {
+    uint64_t nsamps;
+    double tsamp;
+    uint64_t nbins;
+    double eta;
+    uint32_t nparams;
+    double limits[2 * LKO_MAX_PARAMS];
+    uint64_t bseg_brute;
+    uint64_t bseg_ffa;
+    double ducy_max;
+    double wtsp;
+} lko_cfg;
+
+/* FFAPlanBase geometry (lib/plans.cpp:264-320). */
+typedef struct lko_plan {
+    uint32_t nparams;
+    uint32_t n_levels;
+    uint64_t nsamps;
+    uint64_t nbins;
+    double tsamp;
+    double eta;
+    double tseg_brute;
+    uint64_t bseg_brute;
+    uint64_t bseg_ffa;
+    double limits[2 * LKO_MAX_PARAMS];
+    uint64_t segment_lens[LKO_MAX_LEVELS];
+    uint64_t nsegments[LKO_MAX_LEVELS];
+    double tsegments[LKO_MAX_LEVELS];
+    uint64_t ncoords[LKO_MAX_LEVELS];
+    uint32_t ncoords_offsets[LKO_MAX_LEVELS + 1];
+    uint64_t param_counts[LKO_MAX_LEVELS][LKO_MAX_PARAMS];
+    double dparams[LKO_MAX_LEVELS][LKO_MAX_PARAMS];
+    uint64_t buffer_size;     /* max over levels of nseg*ncoords*2*nbins */
+    uint64_t coord_size;      /* sum over levels of ncoords */
+    uint32_t n_widths;        /* generate_box_width_trials(nbins, ...) */
+    uint64_t widths[LKO_MAX_WIDTHS];
+} lko_plan;
+
+/* FFACoordFreq / FFACoord (include/loki/common/coord.hpp:15-25). */
+typedef struct lko_coord_freq {
+    uint32_t idx;
+    float shift;
+} lko_coord_freq;
+
+typedef struct lko_coord {
+    uint32_t i_tail;
+    float shift_tail;
+    uint32_t i_head;
+    float shift_head;
+} lko_coord;
+
+const char* lko_last_error(void);
+
+/* Plan construction: 0 on success, non-zero with lko_last_error() set. */
+int lko_plan_create(const lko_cfg* cfg, lko_plan* out);
+
+/* Scalar phase / grid helpers (lib/loki/psr_utils.hpp:32-63, 235-320). */
+float lko_phase_idx(double proper_time, double freq, uint64_t nbins, double delay);
+uint32_t lko_phase_idx_uint(double proper_time, double freq, uint64_t nbins, double delay);
+double lko_param_val_at_idx(double vmin, double vmax, uint64_t count, uint64_t i);
+uint64_t lko_nearest_idx(double val, double vmin, double vmax, uint64_t count);
+uint64_t lko_range_param_count(double vmin, double vmax, double dv);
+/* psr_utils::range_param (lib/loki/psr_utils.hpp:254-270); returns npoints. */
+uint64_t lko_range_param(double vmin, double vmax, double dv, double* out, uint64_t max_out);
+uint64_t lko_box_widths(uint64_t nbins, double ducy_max, double wtsp, uint64_t* out,
+                        uint64_t max_out);
+
+/* Coordinate tables of every level, flat, coord_size entries (level 0 left
+ * zero as in the reference). */
+int lko_resolve_freq(const lko_plan* plan, lko_coord_freq* out);
+int lko_resolve_taylor(const lko_plan* plan, lko_coord* out);
+
+/* Brute fold (lib/fold.cpp:113-142, lib/kernels.cpp:550-580,1132-1154).
+ * out: [nsamps/segment_len, nfreqs, 2, nbins]. */
+int lko_brute_fold(const float* ts_e, const float* ts_v, uint64_t nsamps,
+                   const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                   uint64_t nbins, double tsamp, double t_ref, float* out);
+
+/* Phase map of the brute fold, uint32 [nfreqs, segment_len]. */
+void lko_phase_map(const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                   uint64_t nbins, double tsamp, double t_ref, uint32_t* out);
+
+/* One merge level (lib/kernels.cpp:118-146,722-827 and 71-112,829-940). */
+void lko_merge_freq(const float* fold_in, float* fold_out, const lko_coord_freq* coords,
+                    uint64_t ncoords_cur, uint64_t ncoords_prev, uint64_t nsegments,
+                    uint64_t nbins);
+void lko_merge_taylor(const float* fold_in, float* fold_out, const lko_coord* coords,
+                      uint64_t ncoords_cur, uint64_t ncoords_prev, uint64_t nsegments,
+                      uint64_t nbins);
+
+/* Whole FFA (lib/ffa.cpp:242-310). level_out selects the level whose fold is
+ * written to fold_out (n_levels-1 for the final fold). */
+int lko_ffa(const lko_plan* plan, const float* ts_e, const float* ts_v,
+            uint32_t level_out, float* fold_out);
+
+/* Boxcar S/N (lib/score.cpp:95-172, lib/utils.cpp:22-67). */
+void lko_snr_boxcar_3d(const float* folds, uint64_t nprofiles, uint64_t nbins,
+                       const uint64_t* widths, uint64_t nwidths, float* scores);
+void lko_snr_boxcar_3d_max(const float* folds, uint64_t nprofiles, uint64_t nbins,
+                           const uint64_t* widths, uint64_t nwidths, float* scores);
+void lko_snr_boxcar_2d_max(const float* folds, uint64_t nprofiles, uint64_t nbins,
+                           const uint64_t* widths, uint64_t nwidths, float stdnoise,
+                           float* scores);
+void lko_circular_prefix_sum(const float* x, float* out, uint64_t nbins, uint64_t nsum);
+
+/* Threshold compaction `score >= snr_min` in flat order
+ * (lib/ffa_freq_sweep.cpp:182-195). Returns the number kept. */
+uint64_t lko_compact(const float* scores, uint64_t n, float snr_min, uint32_t* idx_out,
+                     float* score_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOKI_ORACLE_H */

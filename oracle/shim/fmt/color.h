@@ -1,0 +1,3 @@
+#pragma once
+// Oracle build shim: forwards to the fmt copy bundled with spdlog (header-only).
+#include <spdlog/fmt/bundled/color.h>
