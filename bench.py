@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark: Taylor-FFA acceleration search (f, fdot) + boxcar S/N + candidate
+compaction on one B200 per rank.
+
+Workload (one "step" = one pass of the hot path over one time series):
+  2^22 float32 samples at 64 us (268 s), seed 7, N(0,1) noise plus 4 injected
+  accelerated pulsars; search f in [5, 50] Hz, accel in [-200, 200] m/s^2,
+  nbins 64, eta 2, boxcar widths {1,2,3,4,6,8,12,16}; scores of all
+  1,932,740 final (accel, freq) cells x 8 widths, compacted at S/N >= 7.
+Metric: param-trials/s = final coordinates x widths per second (whole job).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs an independent replica (the FFA of one series
+does not shard: "replicas only"); value = trials of all ranks / max step time.
+The reference arm times the reference's own CPU code (oracle/_ref, built from
+the reference sources with its Release flags) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "param-trials/s (FFA+S/N)"
+UNIT = "param-trials/s"
+SNR_MIN = 7.0
+FLUSH_BYTES = 256 << 20  # > 126 MB L2: written between timed steps
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--storage", default="fp32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from loki_b200.synthetic import taylor_accel_workload
+
+    return taylor_accel_workload(seed=7)
+
+
+def config_dict(params, extra=None):
+    d = {
+        "workload": "taylor_ffa_accel_2^22x64us_nbins64_eta2",
+        "nsamps": params["nsamps"],
+        "tsamp": params["tsamp"],
+        "nbins": params["nbins"],
+        "eta": params["eta"],
+        "param_limits": params["param_limits"],
+        "score_widths": params["score_widths"],
+        "snr_min": SNR_MIN,
+        "l2": f"flushed: {FLUSH_BYTES >> 20} MiB written between timed steps",
+        "parallelism": "replicas",
+    }
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---- clocks -----------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- peaks / ncu data ---------------------------------------------------------
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(stage: str):
+    """Per-launch DRAM bytes of a stage from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as fh:
+            return json.load(fh).get(stage)
+    except (OSError, ValueError):
+        return None
+
+
+# ---- reference CPU path -------------------------------------------------------
+
+def reference_runner(params, kind="timing"):
+    from oracle import ref
+
+    nthreads = os.cpu_count() or 1
+    cfg = ref.make_cfg(params["nsamps"], params["tsamp"], params["nbins"], params["eta"], params["param_limits"],
+                       nthreads=nthreads)
+    ffa = ref.RefFFA(cfg, kind=kind)
+    widths = np.array(params["score_widths"], dtype=np.uint64)
+    ntrials = int(ffa.ncoords[-1]) * widths.size
+
+    def step(ts_e, ts_v):
+        fold = ffa.execute(ts_e, ts_v)
+        scores = ref.snr_boxcar_3d(fold, widths, params["nbins"], nthreads=nthreads, kind=kind).ravel()
+        idx = np.flatnonzero(scores >= SNR_MIN)  # FFAFreqSweep compaction (>=, flat order)
+        return idx, scores[idx]
+
+    return step, ntrials, nthreads
+
+
+def cpu_baseline(params, ts_e, ts_v, budget_s=20.0):
+    from oracle import ref
+
+    if not ref.available("timing"):
+        return None
+    step, ntrials, nthreads = reference_runner(params)
+    step(ts_e, ts_v)  # warm-up
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < 5 and (not times or time.perf_counter() + times[-1] < t_end):
+        t0 = time.perf_counter()
+        step(ts_e, ts_v)
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": ntrials / med, "unit": UNIT, "cores": nthreads, "kind": "reference",
+            "sample": f"full workload, median of {len(times)} runs of FFA::execute + snr_boxcar_3d + "
+                      f"compaction ({med:.3f} s each), reference CPU code built with its Release flags"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    from oracle import ref
+
+    ts_e, ts_v, params, _ = workload()
+    if not ref.available("timing"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
+        return 0
+    step, ntrials, nthreads = reference_runner(params)
+    for _ in range(max(args.warmup, 1)):
+        step(ts_e, ts_v)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step(ts_e, ts_v)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = ntrials * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": config_dict(params, {"cpu_threads": nthreads}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                         "sample": f"full workload per step, {args.steps} steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---- our path -------------------------------------------------------------------
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from loki_b200 import _capi as C
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local_rank}"))
+
+    ts_e, ts_v, params, _ = workload()
+    cfg = PulsarSearchConfig(params["nsamps"], params["tsamp"], params["nbins"], params["eta"],
+                             np.array(params["param_limits"]), use_fourier=False,
+                             score_widths=params["score_widths"], snr_min=SNR_MIN)
+    ffa = FFACUDA(cfg, device_id=local_rank, fold_storage=args.storage)
+    nc = int(ffa.plan.ncoords[-1])
+    nw = cfg.n_scoring_widths
+    ntrials = nc * nw
+    cap = 1 << 20
+    dev = f"cuda:{local_rank}"
+    e = torch.from_numpy(ts_e).to(dev)
+    v = torch.from_numpy(ts_v).to(dev)
+    idx = torch.empty(cap, dtype=torch.int32, device=dev)
+    snr = torch.empty(cap, dtype=torch.float32, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    L = C.lib()
+
+    def step():
+        C.check(L.lk_ffa_search(ffa._h, e.data_ptr(), v.data_ptr(), SNR_MIN, idx.data_ptr(), snr.data_ptr(),
+                                cap, cnt.data_ptr(), sp))
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if ffa.status() != 0:
+        raise RuntimeError("device status word set during warm-up")
+
+    ffa.set_profiling(True)
+    stage_ms: dict[str, float] = {}
+    stage_bytes: dict[str, int] = {}
+    stage_launches: dict[str, int] = {}
+    launches = 0
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        step()
+        stops[k].record(stream)
+        for st in ffa.profile():  # synchronises the stream
+            key = st["stage"] if st["level"] < 0 else f'{st["stage"]}_l{st["level"]}'
+            stage_ms[key] = stage_ms.get(key, 0.0) + st["ms"]
+            stage_bytes[key] = st["bytes"]
+            stage_launches[key] = st["launches"]
+            launches += st["launches"]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    ffa.set_profiling(False)
+    step_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / args.steps
+    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms_max = float(t.item())
+    value = ntrials * world / (step_ms_max / 1e3)
+    ncand = int(cnt.item())
+
+    # roofline of the dominant stage
+    dom = max(stage_ms, key=stage_ms.get)
+    dom_ms = stage_ms[dom] / args.steps
+    achieved = stage_bytes[dom] / (dom_ms / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic(dom),
+                "algorithmic_bytes": stage_bytes[dom], "avg_ms": dom_ms}
+    stages = {k: {"avg_ms": stage_ms[k] / args.steps, "bytes": stage_bytes[k],
+                  "gbs": stage_bytes[k] / (stage_ms[k] / args.steps / 1e3) / 1e9}
+              for k in sorted(stage_ms, key=stage_ms.get, reverse=True)}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        he = torch.from_numpy(ts_e).pin_memory()
+        hv = torch.from_numpy(ts_v).pin_memory()
+        hcnt = torch.zeros(1, dtype=torch.int64).pin_memory()
+        hidx = torch.empty(cap, dtype=torch.int32).pin_memory()
+        hsnr = torch.empty(cap, dtype=torch.float32).pin_memory()
+        d2h = 0
+        for k in range(args.warmup + args.steps):
+            if k == args.warmup:
+                if dist is not None:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                d2h = 0
+            e.copy_(he, non_blocking=True)
+            v.copy_(hv, non_blocking=True)
+            step()
+            hcnt.copy_(cnt, non_blocking=True)
+            torch.cuda.synchronize()
+            n = min(int(hcnt.item()), cap)
+            hidx[:n].copy_(idx[:n], non_blocking=True)
+            hsnr[:n].copy_(snr[:n], non_blocking=True)
+            torch.cuda.synchronize()
+            d2h += 8 + 8 * n
+        e2e_s = time.perf_counter() - t0
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = {"value": ntrials * world * args.steps / float(t.item()), "unit": UNIT,
+               "h2d_bytes_per_step": 2 * 4 * params["nsamps"], "d2h_bytes_per_step": d2h // args.steps,
+               "api": "loki_b200 FFACUDA executor (lk_ffa_search) with pinned host input and result read-back"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(params, ts_e, ts_v)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(params, {"fold_storage": args.storage, "final_coords": nc, "n_widths": nw,
+                                           "candidates": ncand}),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "stages": stages, "wall_s": wall,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,225 @@
+/* loki_b200: B200-native (sm_100a) FFA folding, boxcar scoring and pruning
+ * leaf step for pulsar searches, behind a plain C ABI.
+ *
+ * Conventions
+ *   - Every entry point returns int: LK_OK (0) or an lk_status code; the
+ *     message of the last failure on the calling thread is lk_last_error().
+ *   - Device buffers (d_*) are owned by the caller. Objects (lk_plan, lk_ffa,
+ *     lk_brute_fold) own their device tables and scratch.
+ *   - Work is enqueued on the given stream (cudaStream_t passed as
+ *     lk_stream_t; NULL is the legacy default stream). Entry points named
+ *     *_execute / *_scores / *_search do not synchronise the stream.
+ *   - A plan is immutable after creation; an executor is used by one stream
+ *     at a time.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   lk_plan_*         plans::FFAPlan<float>, search::PulsarSearchConfig
+ *                     (include/loki/common/plans.hpp:21-140,
+ *                      include/loki/search/configs.hpp:22-164)
+ *   lk_ffa_*          algorithms::FFACUDA<float> (include/loki/algorithms/ffa.hpp:100-153),
+ *                     compute_ffa_cuda / compute_ffa_scores_cuda (lib/ffa_cuda.cu:609-650)
+ *   lk_brute_fold_*   algorithms::BruteFoldCUDA<float> (include/loki/algorithms/fold.hpp:78-134)
+ *   lk_snr_boxcar_*   detection::snr_boxcar_{3d,3d_max,2d_max}_cuda (lib/score_cuda.cu:253-513)
+ *   lk_compact_ge     score compaction of FFAFreqSweep (lib/ffa_freq_sweep.cpp:182-195)
+ */
+#ifndef LOKI_B200_H
+#define LOKI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* lk_stream_t;
+
+enum lk_status {
+    LK_OK = 0,
+    LK_ERR_INVALID_ARG = 1,   /* argument/config rejected (reference throws invalid_argument/runtime_error) */
+    LK_ERR_OOM = 2,           /* device or host allocation failed */
+    LK_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+    LK_ERR_DEVICE_TIMEOUT = 4,/* a bounded device-side wait gave up (status word set) */
+    LK_ERR_UNSUPPORTED = 5,   /* valid request outside what this build implements */
+    LK_ERR_INTERNAL = 6
+};
+
+/* Storage type of intermediate fold levels. Accumulation is always FP32. */
+enum lk_dtype { LK_FP32 = 0, LK_BF16 = 1, LK_FP16 = 2 };
+
+enum lk_score_mode { LK_SCORE_PER_WIDTH = 0, LK_SCORE_MAX = 1 };
+
+#define LK_MAX_PARAMS 5
+#define LK_MAX_WIDTHS 32
+#define LK_MAX_LEVELS 40
+
+/* Search configuration: the PulsarSearchConfig fields the FFA path reads
+ * (include/loki/search/configs.hpp:25-47). param_limits holds nparams
+ * (min, max) pairs ordered (..., jerk, accel, freq). bseg_brute / bseg_ffa of
+ * 0 select the reference defaults (lib/configs.cpp:295-302).
+ * n_score_widths == 0 selects generate_box_width_trials(nbins, ducy_max, wtsp)
+ * (lib/score.cpp:390-405); otherwise score_widths[0..n) are used as given. */
+typedef struct lk_config {
+    uint64_t nsamps;
+    double tsamp;
+    uint64_t nbins;
+    double eta;
+    uint32_t nparams;
+    double param_limits[2 * LK_MAX_PARAMS];
+    double ducy_max;
+    double wtsp;
+    uint64_t bseg_brute;
+    uint64_t bseg_ffa;
+    double snr_min;
+    uint32_t n_score_widths;
+    uint32_t score_widths[LK_MAX_WIDTHS];
+} lk_config;
+
+/* Plan geometry (FFAPlanBase getters, include/loki/common/plans.hpp:38-78). */
+typedef struct lk_plan_info {
+    uint32_t nparams;
+    uint32_t n_levels;
+    uint64_t nsamps;
+    uint64_t nbins;
+    double tsamp;
+    uint64_t bseg_brute;
+    uint64_t bseg_ffa;
+    double tseg_brute;
+    double tseg_ffa;
+    uint64_t segment_lens[LK_MAX_LEVELS];
+    uint64_t nsegments[LK_MAX_LEVELS];
+    double tsegments[LK_MAX_LEVELS];
+    uint64_t ncoords[LK_MAX_LEVELS];
+    uint32_t ncoords_offsets[LK_MAX_LEVELS + 1];
+    uint64_t param_counts[LK_MAX_LEVELS][LK_MAX_PARAMS];
+    double dparams[LK_MAX_LEVELS][LK_MAX_PARAMS];
+    double dparams_actual[LK_MAX_LEVELS][LK_MAX_PARAMS];
+    uint64_t buffer_size;     /* FFAPlan::get_buffer_size (lib/plans.cpp:463-470) */
+    uint64_t fold_size;       /* final level [nseg, counts..., 2, nbins] */
+    uint64_t brute_fold_size; /* level 0 */
+    uint64_t coord_size;      /* sum of ncoords over levels */
+    uint32_t n_widths;
+    uint32_t widths[LK_MAX_WIDTHS];
+    double snr_min;
+} lk_plan_info;
+
+typedef struct lk_plan lk_plan;
+typedef struct lk_ffa lk_ffa;
+typedef struct lk_brute_fold lk_brute_fold;
+
+/* ---- library ---------------------------------------------------------- */
+const char* lk_last_error(void);
+int lk_version(void);
+
+/* ---- plan (host only; no device work) ---------------------------------- */
+/* Replaces FFAPlan<float>(PulsarSearchConfig(...)) (lib/plans.cpp:33-36,264-333,
+ * lib/configs.cpp:16-95). */
+int lk_plan_create(const lk_config* cfg, lk_plan** out);
+void lk_plan_destroy(lk_plan* plan);
+int lk_plan_get_info(const lk_plan* plan, lk_plan_info* out);
+/* Cell centres of one parameter at one level: psr_utils::range_param
+ * (lib/loki/psr_utils.hpp:254-270), as FFAPlanBase::compute_param_grid
+ * (lib/plans.cpp:152-162). Writes min(n, count) values. */
+int lk_plan_param_grid(const lk_plan* plan, uint32_t level, uint32_t iparam, double* out,
+                       uint64_t n);
+/* Grid steps for a segment of length tseg_cur seconds, nparams values:
+ * kind 0 = PulsarSearchConfig::get_dparams, 1 = get_dparams_f,
+ * 2 = get_dparams_actual (lib/configs.cpp:152-174). */
+int lk_plan_dparams(const lk_plan* plan, double tseg_cur, int kind, double* out);
+
+/* Resolve the coordinate tables of every level on the device, in the
+ * reference layout (FFACoordFreq {u32 idx; f32 shift} when nparams == 1,
+ * FFACoord {u32 i_tail; f32 shift_tail; u32 i_head; f32 shift_head}
+ * otherwise), coord_size entries, level 0 zeroed. Replaces
+ * FFAPlanBase::resolve_coordinates[_freq] (lib/plans.cpp:64-132). */
+int lk_plan_resolve_coords(const lk_plan* plan, void* d_coords, uint64_t n_coords,
+                           lk_stream_t stream);
+
+/* ---- FFA executor (replaces FFACUDA<float>) ---------------------------- */
+/* Builds the device tables (coordinates, brute-fold run tables) and scratch
+ * for `plan` on `device`. storage: lk_dtype of intermediate levels. */
+int lk_ffa_create(const lk_plan* plan, int device, int storage, lk_ffa** out);
+void lk_ffa_destroy(lk_ffa* ffa);
+/* Device bytes owned by the executor. */
+int lk_ffa_workspace_bytes(const lk_ffa* ffa, uint64_t* bytes);
+/* Final-level fold, FP32, fold_size floats. Replaces FFACUDA::execute
+ * (lib/ffa_cuda.cu:171-196). */
+int lk_ffa_execute(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float* d_fold,
+                   uint64_t fold_len, lk_stream_t stream);
+/* Boxcar S/N of every final coordinate and width, [ncoords, n_widths] FP32;
+ * the final merge level and the score are one kernel (the final fold is not
+ * written). Replaces compute_ffa_scores_cuda (lib/ffa_cuda.cu:630-650). */
+int lk_ffa_scores(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float* d_scores,
+                  uint64_t scores_len, lk_stream_t stream);
+/* Scores plus threshold compaction `score >= snr_min` in flat index order
+ * (coord * n_widths + width), as FFAFreqSweep::execute_ffa_region
+ * (lib/ffa_freq_sweep.cpp:182-195). Writes up to max_cands (index, S/N)
+ * pairs and the total number passing to *d_count (which may exceed
+ * max_cands; the kept entries are then the first max_cands in order). */
+int lk_ffa_search(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float snr_min,
+                  uint32_t* d_idx, float* d_snr, uint64_t max_cands, uint64_t* d_count,
+                  lk_stream_t stream);
+/* Synchronises the stream and reports the executor's device status word
+ * (0 = no bounded wait gave up). */
+int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status);
+
+/* Per-stage timing with CUDA events recorded on the launching stream
+ * (no reference counterpart; used by benchmarks). When enabled, every
+ * execute/scores/search call records one event pair per kernel stage. */
+enum lk_stage_kind {
+    LK_STAGE_TRANSPOSE = 0,
+    LK_STAGE_BRUTE_FOLD = 1,
+    LK_STAGE_MERGE = 2,
+    LK_STAGE_MERGE_SCORE = 3,
+    LK_STAGE_COMPACT = 4
+};
+typedef struct lk_stage_time {
+    int32_t kind;       /* lk_stage_kind */
+    int32_t level;      /* FFA level the stage produces (-1 if none) */
+    uint32_t launches;  /* kernels launched by the stage */
+    float ms;           /* elapsed GPU time of the last call */
+    uint64_t bytes;     /* algorithmic bytes moved (reads + writes) */
+} lk_stage_time;
+int lk_ffa_set_profiling(lk_ffa* ffa, int enable);
+/* Synchronises the stream, then reports the stages of the last call. */
+int lk_ffa_get_profile(lk_ffa* ffa, lk_stream_t stream, lk_stage_time* out, uint32_t max_out,
+                       uint32_t* n_out);
+
+/* ---- brute fold (replaces BruteFoldCUDA<float>) ------------------------ */
+int lk_brute_fold_create(const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                         uint64_t nbins, uint64_t nsamps, double tsamp, double t_ref,
+                         int device, lk_brute_fold** out);
+void lk_brute_fold_destroy(lk_brute_fold* bf);
+/* d_fold: [nsamps/segment_len, nfreqs, 2, nbins] FP32. */
+int lk_brute_fold_execute(lk_brute_fold* bf, const float* d_ts_e, const float* d_ts_v,
+                          float* d_fold, lk_stream_t stream);
+
+/* ---- boxcar S/N -------------------------------------------------------- */
+/* detection::generate_box_width_trials (lib/score.cpp:390-405): writes up to
+ * max_out widths and their number to *n_out. */
+int lk_box_width_trials(uint64_t nbins, double ducy_max, double wtsp, uint32_t* out,
+                        uint32_t max_out, uint32_t* n_out);
+/* d_folds [nprofiles, 2, nbins] (E row, V row). mode LK_SCORE_PER_WIDTH
+ * writes [nprofiles, nwidths]; LK_SCORE_MAX writes [nprofiles]. */
+int lk_snr_boxcar_3d(const float* d_folds, uint64_t nprofiles, uint32_t nbins,
+                     const uint32_t* widths, uint32_t nwidths, int mode, float* d_scores,
+                     lk_stream_t stream);
+/* d_folds [nprofiles, nbins], S/N divided by stdnoise; [nprofiles] max. */
+int lk_snr_boxcar_2d_max(const float* d_folds, uint64_t nprofiles, uint32_t nbins,
+                         const uint32_t* widths, uint32_t nwidths, float stdnoise,
+                         float* d_scores, lk_stream_t stream);
+
+/* ---- compaction -------------------------------------------------------- */
+/* Device scratch bytes lk_compact_ge needs for n inputs. */
+uint64_t lk_compact_scratch_bytes(uint64_t n);
+/* Keep d_scores[i] >= thr in increasing i: up to max_out (i, score) pairs;
+ * *d_count = number passing. d_scratch: lk_compact_scratch_bytes(n) bytes. */
+int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
+                  float* d_vals, uint64_t max_out, uint64_t* d_count, void* d_scratch,
+                  lk_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOKI_B200_H */

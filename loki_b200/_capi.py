@@ -1,0 +1,160 @@
+"""ctypes binding of ``libloki_b200.so`` (the C ABI in ``include/loki_b200.h``).
+
+The shared library is built in-tree (``make -C loki_b200/csrc``); importing this
+module without it raises ``ImportError`` -- there is no fallback path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libloki_b200.so")
+
+LK_OK = 0
+LK_ERR_INVALID_ARG = 1
+LK_ERR_OOM = 2
+LK_ERR_CUDA = 3
+LK_ERR_DEVICE_TIMEOUT = 4
+LK_ERR_UNSUPPORTED = 5
+LK_ERR_INTERNAL = 6
+
+LK_FP32, LK_BF16, LK_FP16 = 0, 1, 2
+LK_SCORE_PER_WIDTH, LK_SCORE_MAX = 0, 1
+
+LK_MAX_PARAMS = 5
+LK_MAX_WIDTHS = 32
+LK_MAX_LEVELS = 40
+
+u64 = ctypes.c_uint64
+u32 = ctypes.c_uint32
+i32 = ctypes.c_int
+f64 = ctypes.c_double
+f32 = ctypes.c_float
+vp = ctypes.c_void_p
+
+
+class LokiError(RuntimeError):
+    """Raised for a failed library call; ``status`` is the lk_status code.
+
+    The reference raises ``RuntimeError`` (its DetailedException derives from
+    std::runtime_error), so this subclasses it.
+    """
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class LkConfig(ctypes.Structure):
+    _fields_ = [
+        ("nsamps", u64),
+        ("tsamp", f64),
+        ("nbins", u64),
+        ("eta", f64),
+        ("nparams", u32),
+        ("param_limits", f64 * (2 * LK_MAX_PARAMS)),
+        ("ducy_max", f64),
+        ("wtsp", f64),
+        ("bseg_brute", u64),
+        ("bseg_ffa", u64),
+        ("snr_min", f64),
+        ("n_score_widths", u32),
+        ("score_widths", u32 * LK_MAX_WIDTHS),
+    ]
+
+
+class LkPlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("nparams", u32),
+        ("n_levels", u32),
+        ("nsamps", u64),
+        ("nbins", u64),
+        ("tsamp", f64),
+        ("bseg_brute", u64),
+        ("bseg_ffa", u64),
+        ("tseg_brute", f64),
+        ("tseg_ffa", f64),
+        ("segment_lens", u64 * LK_MAX_LEVELS),
+        ("nsegments", u64 * LK_MAX_LEVELS),
+        ("tsegments", f64 * LK_MAX_LEVELS),
+        ("ncoords", u64 * LK_MAX_LEVELS),
+        ("ncoords_offsets", u32 * (LK_MAX_LEVELS + 1)),
+        ("param_counts", (u64 * LK_MAX_PARAMS) * LK_MAX_LEVELS),
+        ("dparams", (f64 * LK_MAX_PARAMS) * LK_MAX_LEVELS),
+        ("dparams_actual", (f64 * LK_MAX_PARAMS) * LK_MAX_LEVELS),
+        ("buffer_size", u64),
+        ("fold_size", u64),
+        ("brute_fold_size", u64),
+        ("coord_size", u64),
+        ("n_widths", u32),
+        ("widths", u32 * LK_MAX_WIDTHS),
+        ("snr_min", f64),
+    ]
+
+
+STAGE_NAMES = {0: "transpose", 1: "brute_fold", 2: "merge", 3: "merge_score", 4: "compact"}
+
+
+class LkStageTime(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("level", ctypes.c_int32), ("launches", u32), ("ms", f32),
+                ("bytes", u64)]
+
+
+# (name, restype, argtypes) of every exported entry point, in header order.
+SIGNATURES = [
+    ("lk_last_error", ctypes.c_char_p, []),
+    ("lk_version", i32, []),
+    ("lk_plan_create", i32, [vp, vp]),
+    ("lk_plan_destroy", None, [vp]),
+    ("lk_plan_get_info", i32, [vp, vp]),
+    ("lk_plan_param_grid", i32, [vp, u32, u32, vp, u64]),
+    ("lk_plan_dparams", i32, [vp, f64, i32, vp]),
+    ("lk_plan_resolve_coords", i32, [vp, vp, u64, vp]),
+    ("lk_ffa_create", i32, [vp, i32, i32, vp]),
+    ("lk_ffa_destroy", None, [vp]),
+    ("lk_ffa_workspace_bytes", i32, [vp, vp]),
+    ("lk_ffa_execute", i32, [vp, vp, vp, vp, u64, vp]),
+    ("lk_ffa_scores", i32, [vp, vp, vp, vp, u64, vp]),
+    ("lk_ffa_search", i32, [vp, vp, vp, f32, vp, vp, u64, vp, vp]),
+    ("lk_ffa_status", i32, [vp, vp, vp]),
+    ("lk_ffa_set_profiling", i32, [vp, i32]),
+    ("lk_ffa_get_profile", i32, [vp, vp, vp, u32, vp]),
+    ("lk_brute_fold_create", i32, [vp, u64, u64, u64, u64, f64, f64, i32, vp]),
+    ("lk_brute_fold_destroy", None, [vp]),
+    ("lk_brute_fold_execute", i32, [vp, vp, vp, vp, vp]),
+    ("lk_box_width_trials", i32, [u64, f64, f64, vp, u32, vp]),
+    ("lk_snr_boxcar_3d", i32, [vp, u64, u32, vp, u32, i32, vp, vp]),
+    ("lk_snr_boxcar_2d_max", i32, [vp, u64, u32, vp, u32, f32, vp, vp]),
+    ("lk_compact_scratch_bytes", u64, [u64]),
+    ("lk_compact_ge", i32, [vp, u64, f32, vp, vp, u64, vp, vp, vp]),
+]
+
+_lib: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded native library (loaded once)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"loki_b200 native library not found at {LIB_PATH}; build it with "
+                "`make -C loki_b200/csrc` (or __graft_entry__.build())"
+            )
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != LK_OK:
+        msg = lib().lk_last_error().decode(errors="replace")
+        if rc == LK_ERR_OOM:
+            raise MemoryError(msg)
+        raise LokiError(rc, msg)

@@ -1,0 +1,354 @@
+// The C ABI (include/loki_b200.h): argument checks, exception-to-status
+// translation and the thread-local error message. No CUDA kernels here.
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "lk_ffa.hpp"
+#include "lk_kernels.hpp"
+
+struct lk_plan {
+    lk::Plan plan;
+};
+struct lk_ffa {
+    std::unique_ptr<lk::FFAExec> exec;
+};
+struct lk_brute_fold {
+    int device = 0;
+    lk::DeviceBuffer status;
+    std::unique_ptr<lk::BruteFoldDevice> bf;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        g_error.clear();
+        return LK_OK;
+    } catch (const lk::Error& e) {
+        g_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_error = "host allocation failed";
+        return LK_ERR_OOM;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return LK_ERR_INTERNAL;
+    } catch (...) {
+        g_error = "unknown error";
+        return LK_ERR_INTERNAL;
+    }
+}
+
+void need(const void* p, const char* name) {
+    if (p == nullptr) {
+        lk::fail(LK_ERR_INVALID_ARG, std::string(name) + " must not be NULL");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lk_last_error(void) { return g_error.c_str(); }
+
+int lk_version(void) { return 100; }
+
+int lk_plan_create(const lk_config* cfg, lk_plan** out) {
+    return guarded([&] {
+        need(cfg, "cfg");
+        need(out, "out");
+        auto p = std::make_unique<lk_plan>();
+        p->plan = lk::make_plan(*cfg);
+        *out = p.release();
+    });
+}
+
+void lk_plan_destroy(lk_plan* plan) { delete plan; }
+
+int lk_plan_get_info(const lk_plan* plan, lk_plan_info* out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        const lk::Plan& p = plan->plan;
+        std::memset(out, 0, sizeof(*out));
+        out->nparams = p.nparams;
+        out->n_levels = p.n_levels;
+        out->nsamps = p.cfg.nsamps;
+        out->nbins = p.cfg.nbins;
+        out->tsamp = p.cfg.tsamp;
+        out->bseg_brute = p.bseg_brute;
+        out->bseg_ffa = p.bseg_ffa;
+        out->tseg_brute = p.tseg_brute;
+        out->tseg_ffa = p.tseg_ffa;
+        for (uint32_t l = 0; l < p.n_levels; ++l) {
+            out->segment_lens[l] = p.segment_lens[l];
+            out->nsegments[l] = p.nsegments[l];
+            out->tsegments[l] = p.tsegments[l];
+            out->ncoords[l] = p.ncoords[l];
+            out->ncoords_offsets[l] = p.ncoords_offsets[l];
+            for (uint32_t i = 0; i < p.nparams; ++i) {
+                out->param_counts[l][i] = p.param_counts[l][i];
+                out->dparams[l][i] = p.dparams[l][i];
+                out->dparams_actual[l][i] = p.dparams_actual[l][i];
+            }
+        }
+        out->ncoords_offsets[p.n_levels] = p.ncoords_offsets[p.n_levels];
+        out->buffer_size = p.buffer_size;
+        out->fold_size = p.fold_size(p.n_levels - 1);
+        out->brute_fold_size = p.fold_size(0);
+        out->coord_size = p.coord_size;
+        out->n_widths = static_cast<uint32_t>(p.widths.size());
+        for (size_t i = 0; i < p.widths.size(); ++i) {
+            out->widths[i] = p.widths[i];
+        }
+        out->snr_min = p.cfg.snr_min;
+    });
+}
+
+int lk_plan_param_grid(const lk_plan* plan, uint32_t level, uint32_t iparam, double* out,
+                       uint64_t n) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        const lk::Plan& p = plan->plan;
+        lk::require(level < p.n_levels && iparam < p.nparams, "level/iparam out of range");
+        const auto g = p.param_grid(level, iparam);
+        std::memcpy(out, g.data(), sizeof(double) * std::min<uint64_t>(n, g.size()));
+    });
+}
+
+int lk_plan_dparams(const lk_plan* plan, double tseg_cur, int kind, double* out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        lk::require(kind >= 0 && kind <= 2, "kind must be 0, 1 or 2");
+        const auto d = plan->plan.dparams_at(tseg_cur, kind);
+        std::memcpy(out, d.data(), sizeof(double) * d.size());
+    });
+}
+
+int lk_plan_resolve_coords(const lk_plan* plan, void* d_coords, uint64_t n_coords,
+                           lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(d_coords, "d_coords");
+        lk::require(n_coords >= plan->plan.coord_size, "coords must hold coord_size entries");
+        lk::resolve_coords_device(plan->plan, d_coords, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_ffa_create(const lk_plan* plan, int device, int storage, lk_ffa** out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        auto f = std::make_unique<lk_ffa>();
+        f->exec = std::make_unique<lk::FFAExec>(plan->plan, device, storage);
+        *out = f.release();
+    });
+}
+
+void lk_ffa_destroy(lk_ffa* ffa) {
+    if (ffa != nullptr) {
+        try {
+            lk::DeviceGuard g(ffa->exec->device);
+            delete ffa;
+        } catch (...) {
+            delete ffa;
+        }
+    }
+}
+
+int lk_ffa_workspace_bytes(const lk_ffa* ffa, uint64_t* bytes) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(bytes, "bytes");
+        *bytes = ffa->exec->device_bytes();
+    });
+}
+
+int lk_ffa_execute(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float* d_fold,
+                   uint64_t fold_len, lk_stream_t stream) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_fold, "d_fold");
+        ffa->exec->execute(d_ts_e, d_ts_v, d_fold, fold_len, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_ffa_scores(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float* d_scores,
+                  uint64_t scores_len, lk_stream_t stream) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_scores, "d_scores");
+        ffa->exec->scores(d_ts_e, d_ts_v, d_scores, scores_len,
+                          reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_ffa_search(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float snr_min,
+                  uint32_t* d_idx, float* d_snr, uint64_t max_cands, uint64_t* d_count,
+                  lk_stream_t stream) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_count, "d_count");
+        if (max_cands > 0) {
+            need(d_idx, "d_idx");
+            need(d_snr, "d_snr");
+        }
+        ffa->exec->search(d_ts_e, d_ts_v, snr_min, d_idx, d_snr, max_cands, d_count,
+                          reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(status, "status");
+        *status = ffa->exec->read_status(reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_ffa_set_profiling(lk_ffa* ffa, int enable) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        ffa->exec->prof.enabled = enable != 0;
+        ffa->exec->prof.reset();
+    });
+}
+
+int lk_ffa_get_profile(lk_ffa* ffa, lk_stream_t stream, lk_stage_time* out, uint32_t max_out,
+                       uint32_t* n_out) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(n_out, "n_out");
+        const auto st = ffa->exec->profile(reinterpret_cast<cudaStream_t>(stream));
+        const auto n = static_cast<uint32_t>(std::min<size_t>(st.size(), max_out));
+        if (n > 0) {
+            need(out, "out");
+            std::copy(st.begin(), st.begin() + n, out);
+        }
+        *n_out = static_cast<uint32_t>(st.size());
+    });
+}
+
+int lk_brute_fold_create(const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                         uint64_t nbins, uint64_t nsamps, double tsamp, double t_ref, int device,
+                         lk_brute_fold** out) {
+    return guarded([&] {
+        need(freqs, "freqs");
+        need(out, "out");
+        lk::DeviceGuard g(device);
+        auto b = std::make_unique<lk_brute_fold>();
+        b->device = device;
+        b->status.alloc(sizeof(uint32_t));
+        LK_CUDA(cudaMemset(b->status.ptr, 0, sizeof(uint32_t)));
+        b->bf = std::make_unique<lk::BruteFoldDevice>(std::vector<double>(freqs, freqs + nfreqs),
+                                                      segment_len, nbins, nsamps, tsamp, t_ref,
+                                                      b->status.as<uint32_t>());
+        *out = b.release();
+    });
+}
+
+void lk_brute_fold_destroy(lk_brute_fold* bf) {
+    if (bf != nullptr) {
+        try {
+            lk::DeviceGuard g(bf->device);
+            delete bf;
+        } catch (...) {
+            delete bf;
+        }
+    }
+}
+
+int lk_brute_fold_execute(lk_brute_fold* bf, const float* d_ts_e, const float* d_ts_v,
+                          float* d_fold, lk_stream_t stream) {
+    return guarded([&] {
+        need(bf, "bf");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_fold, "d_fold");
+        lk::DeviceGuard g(bf->device);
+        bf->bf->execute(d_ts_e, d_ts_v, d_fold, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_box_width_trials(uint64_t nbins, double ducy_max, double wtsp, uint32_t* out,
+                        uint32_t max_out, uint32_t* n_out) {
+    return guarded([&] {
+        need(out, "out");
+        need(n_out, "n_out");
+        const auto w = lk::box_width_trials(nbins, ducy_max, wtsp);
+        lk::require(w.size() <= max_out, "output too small for the width trials");
+        std::copy(w.begin(), w.end(), out);
+        *n_out = static_cast<uint32_t>(w.size());
+    });
+}
+
+int lk_snr_boxcar_3d(const float* d_folds, uint64_t nprofiles, uint32_t nbins,
+                     const uint32_t* widths, uint32_t nwidths, int mode, float* d_scores,
+                     lk_stream_t stream) {
+    return guarded([&] {
+        need(widths, "widths");
+        lk::require(mode == LK_SCORE_PER_WIDTH || mode == LK_SCORE_MAX, "bad score mode");
+        if (nprofiles == 0) {
+            return;
+        }
+        need(d_folds, "d_folds");
+        need(d_scores, "d_scores");
+        const auto sp = lk::make_score_params(widths, nwidths, nbins);
+        lk::score_folds(d_folds, nprofiles, nbins, true, 1.0f, sp, mode, d_scores,
+                        reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_snr_boxcar_2d_max(const float* d_folds, uint64_t nprofiles, uint32_t nbins,
+                         const uint32_t* widths, uint32_t nwidths, float stdnoise,
+                         float* d_scores, lk_stream_t stream) {
+    return guarded([&] {
+        need(widths, "widths");
+        if (nprofiles == 0) {
+            return;
+        }
+        need(d_folds, "d_folds");
+        need(d_scores, "d_scores");
+        const auto sp = lk::make_score_params(widths, nwidths, nbins);
+        // snr_boxcar_impl<false, ...>: inv_stdnoise = 1.0F / stdnoise (lib/score.cpp:117).
+        const float inv = 1.0f / stdnoise;
+        lk::score_folds(d_folds, nprofiles, nbins, false, inv, sp, LK_SCORE_MAX, d_scores,
+                        reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+uint64_t lk_compact_scratch_bytes(uint64_t n) { return lk::compact_scratch_bytes(n); }
+
+int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx, float* d_vals,
+                  uint64_t max_out, uint64_t* d_count, void* d_scratch, lk_stream_t stream) {
+    return guarded([&] {
+        need(d_count, "d_count");
+        if (n > 0) {
+            need(d_scores, "d_scores");
+            need(d_scratch, "d_scratch");
+        }
+        if (max_out > 0) {
+            need(d_idx, "d_idx");
+            need(d_vals, "d_vals");
+        }
+        lk::compact_ge(d_scores, n, thr, d_idx, d_vals, max_out, d_count, d_scratch,
+                       reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// Host-side interfaces of the device building blocks (implemented in .cu files).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "lk_internal.hpp"
+
+namespace lk {
+
+// RAII device allocation.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t n) { alloc(n); }
+    void alloc(size_t n) {
+        release();
+        if (n > 0) {
+            LK_CUDA(cudaMalloc(&ptr, n));
+        }
+        bytes = n;
+    }
+    void release() {
+        if (ptr != nullptr) {
+            cudaFree(ptr);
+        }
+        ptr = nullptr;
+        bytes = 0;
+    }
+    ~DeviceBuffer() { release(); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Brute fold of a time series into [nseg, nfreq, 2, nbins] FP32.
+//
+// Plan-time tables: for every trial frequency the sample -> phase-bin map of
+// one segment (identical for all segments) is encoded as a sequence of run
+// lengths over "virtual bins" v = 0, 1, 2, ... with bin(v) = v mod nbins, in
+// sample order. Replaying the runs in order adds every sample to its bin in
+// increasing sample order, which is the reference's summation order
+// (lib/kernels.cpp:550-580), so the fold is bit-identical.
+class BruteFoldDevice {
+public:
+    BruteFoldDevice(const std::vector<double>& freqs, uint64_t segment_len, uint64_t nbins,
+                    uint64_t nsamps, double tsamp, double t_ref, uint32_t* d_status);
+    // Enqueue: transpose the input into the segment-interleaved scratch, then
+    // fold. d_fold must hold nseg * nfreq * 2 * nbins floats.
+    void execute(const float* d_ts_e, const float* d_ts_v, float* d_fold, cudaStream_t s) {
+        transpose(d_ts_e, d_ts_v, s);
+        fold(d_fold, s);
+    }
+    void transpose(const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
+    void fold(float* d_fold, cudaStream_t s);
+    uint64_t nseg() const { return m_nseg; }
+    uint64_t nfreq() const { return m_nfreq; }
+    uint64_t fold_size() const { return m_nseg * m_nfreq * 2 * m_nbins; }
+    uint64_t device_bytes() const;
+
+private:
+    uint64_t m_nfreq, m_seglen, m_nbins, m_nsamps, m_nseg, m_nseg_pad;
+    uint32_t* m_status;
+    DeviceBuffer m_lens;      // uint16 run lengths, all frequencies
+    DeviceBuffer m_lens_off;  // uint64 offset (entries) per frequency
+    DeviceBuffer m_nper;      // uint32 virtual periods per frequency
+    DeviceBuffer m_xT;        // float [2][seglen][nseg_pad]
+    CUtensorMap m_tmap{};
+    bool m_use_tma = false;
+};
+
+// One merge level: out[s, c] = rot(in[2s, tail(c)], st(c)) + rot(in[2s+1, head(c)], sh(c)).
+void merge_level(const float* d_in, float* d_out, const void* d_coords, bool taylor,
+                 uint64_t ncoords_cur, uint64_t ncoords_prev, uint64_t nsegments,
+                 uint32_t nbins, cudaStream_t s);
+
+// Boxcar scoring parameters shared by the score kernels.
+struct ScoreParams {
+    uint32_t nwidths;
+    uint32_t wmax;
+    uint32_t widths[LK_MAX_WIDTHS];
+    float hb[LK_MAX_WIDTHS];  // h + b
+    float b[LK_MAX_WIDTHS];
+};
+ScoreParams make_score_params(const uint32_t* widths, uint32_t nwidths, uint32_t nbins);
+
+// Final merge level fused with scoring (nsegments == 1).
+void merge_score_level(const float* d_in, const void* d_coords, bool taylor,
+                       uint64_t ncoords_cur, uint64_t ncoords_prev, uint32_t nbins,
+                       const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s);
+
+// Standalone scoring of [nprof, 2, nbins] (is3d) or [nprof, nbins] folds.
+void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d,
+                 float inv_stdnoise, const ScoreParams& sp, int mode, float* d_scores,
+                 cudaStream_t s);
+
+// Ordered compaction of scores >= thr.
+uint64_t compact_scratch_bytes(uint64_t n);
+void compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx, float* d_vals,
+                uint64_t max_out, uint64_t* d_count, void* d_scratch, cudaStream_t s);
+
+}  // namespace lk

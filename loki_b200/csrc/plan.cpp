@@ -1,0 +1,214 @@
+// Host-side search plan: the configuration checks and per-level grid
+// geometry of the reference's PulsarSearchConfig and FFAPlan. The formulas
+// must produce the same integers and doubles as the reference (they fix the
+// coordinate grids every kernel indexes), so each one keeps the reference's
+// operation order; the citations name the lines restated.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <string>
+
+#include "lk_internal.hpp"
+
+namespace lk {
+
+namespace {
+
+bool is_pow2(uint64_t x) { return x != 0 && (x & (x - 1)) == 0; }
+
+// math::factorial<double>(n) = std::tgamma(n + 1) (lib/loki/math.hpp:35-44).
+double factorial_d(double n) { return std::tgamma(n + 1.0); }
+
+// psr_utils::poly_taylor_step_f (lib/psr_utils.cpp:14-29).
+std::vector<double> poly_taylor_step_f(uint32_t nparams, double tobs, uint64_t fold_bins,
+                                       double tol_bins, double t_ref) {
+    const double dphi = tol_bins / static_cast<double>(fold_bins);
+    const double dt = tobs - t_ref;
+    std::vector<double> out(nparams);
+    for (uint32_t i = 0; i < nparams; ++i) {
+        const double orth_factor = std::pow(2.0, static_cast<double>(i));
+        out[nparams - 1 - i] = dphi * orth_factor * factorial_d(static_cast<double>(i + 1)) /
+                               std::pow(dt, static_cast<double>(i + 1));
+    }
+    return out;
+}
+
+// psr_utils::poly_taylor_step_d_f (lib/psr_utils.cpp:31-45): the derivative
+// steps are converted to velocity-like units with c / f_max.
+std::vector<double> poly_taylor_step_d_f(uint32_t nparams, double tobs, uint64_t fold_bins,
+                                         double tol_bins, double f_max, double t_ref) {
+    auto f = poly_taylor_step_f(nparams, tobs, fold_bins, tol_bins, t_ref);
+    for (uint32_t i = 0; i + 1 < nparams; ++i) {
+        f[i] = f[i] * kCval / f_max;
+    }
+    return f;
+}
+
+// psr_utils::range_param_count (lib/loki/psr_utils.hpp:235-242).
+uint64_t range_param_count(double vmin, double vmax, double dv) {
+    require(vmax > vmin, "vmax must be greater than vmin");
+    require(dv > 0, "dv must be positive");
+    if (dv >= (vmax - vmin)) {
+        return 1;
+    }
+    return static_cast<uint64_t>(std::ceil((vmax - vmin) / dv));
+}
+
+}  // namespace
+
+std::vector<double> range_param(double vmin, double vmax, double dv) {
+    require(vmax > vmin, "vmax must be greater than vmin");
+    require(dv > 0, "dv must be positive");
+    if (dv >= (vmax - vmin)) {
+        return {(vmax + vmin) / 2.0};
+    }
+    const auto npoints = static_cast<uint64_t>(std::ceil((vmax - vmin) / dv));
+    const double dv_actual = (vmax - vmin) / static_cast<double>(npoints);
+    const double start = vmin + (0.5 * dv_actual);
+    std::vector<double> out(npoints);
+    for (uint64_t i = 0; i < npoints; ++i) {
+        out[i] = start + (dv_actual * static_cast<double>(i));
+    }
+    return out;
+}
+
+// detection::generate_box_width_trials (lib/score.cpp:390-405).
+std::vector<uint32_t> box_width_trials(uint64_t nbins, double ducy_max, double wtsp) {
+    const auto wmax =
+        static_cast<uint64_t>(std::max(1.0, ducy_max * static_cast<double>(nbins)));
+    std::vector<uint32_t> w = {1};
+    while (w.back() < wmax) {
+        const auto next = std::max(static_cast<uint64_t>(w.back() + 1),
+                                   static_cast<uint64_t>(wtsp * static_cast<double>(w.back())));
+        if (next > wmax) {
+            break;
+        }
+        w.push_back(static_cast<uint32_t>(next));
+    }
+    return w;
+}
+
+std::vector<double> Plan::param_grid(uint32_t level, uint32_t iparam) const {
+    return range_param(lim_min(iparam), lim_max(iparam), dparams[level][iparam]);
+}
+
+// PulsarSearchConfig::get_dparams / get_dparams_f / get_dparams_actual
+// (lib/configs.cpp:152-174).
+std::vector<double> Plan::dparams_at(double tseg_cur, int kind) const {
+    const double t_ref = (nparams == 1) ? 0.0 : tseg_cur / 2.0;
+    if (kind == 1) {
+        return poly_taylor_step_f(nparams, tseg_cur, cfg.nbins, cfg.eta, t_ref);
+    }
+    auto d = poly_taylor_step_d_f(nparams, tseg_cur, cfg.nbins, cfg.eta,
+                                  lim_max(nparams - 1), t_ref);
+    if (kind == 2) {
+        for (uint32_t i = 0; i < nparams; ++i) {
+            const uint64_t c = range_param_count(lim_min(i), lim_max(i), d[i]);
+            d[i] = (lim_max(i) - lim_min(i)) / static_cast<double>(c);
+        }
+    }
+    return d;
+}
+
+Plan make_plan(const lk_config& cfg) {
+    Plan p;
+    p.cfg = cfg;
+    const uint32_t np = cfg.nparams;
+    require(np >= 1 && np <= LK_MAX_PARAMS, "nparams must be in [1, 5]");
+    p.nparams = np;
+    const double f_min = p.lim_min(np - 1);
+    const double f_max = p.lim_max(np - 1);
+
+    // PulsarSearchConfig::Impl ctor + validate (lib/configs.cpp:64-95,262-302).
+    require(cfg.nsamps > 0, "nsamps must be positive");
+    require(is_pow2(cfg.nsamps), "nsamps must be a power of 2");
+    require(cfg.tsamp > 0, "tsamp must be positive");
+    require(cfg.eta > 0, "eta (tolerance bins) must be positive");
+    require(cfg.nbins >= 1, "nbins must be positive");
+    if (cfg.bseg_brute != 0) {
+        p.bseg_brute = cfg.bseg_brute;
+    } else {
+        // get_bseg_brute_default (lib/configs.cpp:295-300).
+        const uint64_t init_levels = (np == 1) ? 1 : 2;
+        const auto levels = static_cast<uint64_t>(
+            std::log2(static_cast<double>(cfg.nsamps) * cfg.tsamp * f_min));
+        require(levels >= init_levels,
+                "observation too short for f_min: cannot derive the default bseg_brute");
+        p.bseg_brute = cfg.nsamps / (uint64_t{1} << (levels - init_levels));
+    }
+    p.bseg_ffa = cfg.bseg_ffa != 0 ? cfg.bseg_ffa : cfg.nsamps;
+    require(is_pow2(p.bseg_brute), "bseg_brute must be a power of 2");
+    require(is_pow2(p.bseg_ffa), "bseg_ffa must be a power of 2");
+    require(p.bseg_brute < cfg.nsamps, "bseg_brute must be less than nsamps");
+    require(p.bseg_ffa <= cfg.nsamps, "bseg_ffa must be less than or equal to nsamps");
+    require(p.bseg_ffa >= p.bseg_brute, "bseg_ffa must be greater than or equal to bseg_brute");
+    for (uint32_t i = 0; i < np; ++i) {
+        require(p.lim_max(i) >= p.lim_min(i),
+                "param_limits[" + std::to_string(i) + "] must be increasing");
+    }
+    p.tseg_brute = static_cast<double>(p.bseg_brute) * cfg.tsamp;
+    p.tseg_ffa = static_cast<double>(p.bseg_ffa) * cfg.tsamp;
+    const auto niters = static_cast<uint64_t>(
+        std::log2(static_cast<double>(p.bseg_ffa) / static_cast<double>(p.bseg_brute)));
+    require(niters + 1 <= LK_MAX_LEVELS, "too many FFA levels");
+    p.n_levels = static_cast<uint32_t>(niters + 1);
+
+    if (cfg.n_score_widths == 0) {
+        p.widths = box_width_trials(cfg.nbins, cfg.ducy_max, cfg.wtsp);
+    } else {
+        require(cfg.n_score_widths <= LK_MAX_WIDTHS, "too many score widths");
+        p.widths.assign(cfg.score_widths, cfg.score_widths + cfg.n_score_widths);
+    }
+    require(!p.widths.empty() && p.widths.size() <= LK_MAX_WIDTHS, "bad score widths");
+    for (auto w : p.widths) {
+        require(w >= 1 && w < cfg.nbins, "score widths must lie in [1, nbins)");
+    }
+
+    // FFAPlanBase::Impl::configure_plan (lib/plans.cpp:264-320).
+    const uint32_t L = p.n_levels;
+    p.segment_lens.resize(L);
+    p.nsegments.resize(L);
+    p.tsegments.resize(L);
+    p.ncoords.resize(L);
+    p.ncoords_offsets.resize(L + 1);
+    p.param_counts.assign(L, std::vector<uint64_t>(np));
+    p.dparams.assign(L, std::vector<double>(np));
+    p.dparams_actual.assign(L, std::vector<double>(np));
+    uint64_t offset = 0;
+    for (uint32_t l = 0; l < L; ++l) {
+        const uint64_t segment_len = p.bseg_brute * (uint64_t{1} << l);
+        const double tsegment = static_cast<double>(segment_len) * cfg.tsamp;
+        p.segment_lens[l] = segment_len;
+        p.nsegments[l] = cfg.nsamps / segment_len;
+        p.tsegments[l] = tsegment;
+        // PulsarSearchConfig::get_dparams (lib/configs.cpp:158-162).
+        const double t_ref = (np == 1) ? 0.0 : tsegment / 2.0;
+        p.dparams[l] = poly_taylor_step_d_f(np, tsegment, cfg.nbins, cfg.eta, f_max, t_ref);
+        uint64_t nc = 1;
+        for (uint32_t i = 0; i < np; ++i) {
+            const uint64_t c = range_param_count(p.lim_min(i), p.lim_max(i), p.dparams[l][i]);
+            p.param_counts[l][i] = c;
+            // get_dparams_actual (lib/configs.cpp:164-174).
+            p.dparams_actual[l][i] = (p.lim_max(i) - p.lim_min(i)) / static_cast<double>(c);
+            nc *= c;
+        }
+        p.ncoords[l] = nc;
+        require(offset + nc <= 0xffffffffULL, "coordinate offsets exceed 32 bits");
+        p.ncoords_offsets[l] = static_cast<uint32_t>(offset);
+        offset += nc;
+        p.buffer_size = std::max(p.buffer_size, p.fold_size(l));
+    }
+    p.ncoords_offsets[L] = static_cast<uint32_t>(offset);
+    p.coord_size = offset;
+    // FFAPlanBase::Impl::validate_plan (lib/plans.cpp:322-333).
+    for (uint32_t i = 0; i + 1 < np; ++i) {
+        require(p.param_counts[0][i] == 1,
+                "FFAPlan::validate_plan: Only one parameter for higher order derivatives is "
+                "supported for the initialization for the first level");
+    }
+    // Final coordinates index the fold with 32-bit values.
+    require(p.ncoords[L - 1] <= 0xffffffffULL, "too many final coordinates");
+    return p;
+}
+
+}  // namespace lk

@@ -1,0 +1,164 @@
+"""FFA on the GPU: ``FFACUDA``, ``compute_ffa_time_cuda``, ``compute_ffa_scores_cuda``,
+mirroring ``libculoki.ffa`` of the reference (src/loki_python_cuda.cpp:148-204,
+lib/ffa_cuda.cu:609-692).
+
+Inputs may be host arrays (copied in, results copied back, as the
+reference's host-span overloads do) or CUDA tensors (work is enqueued on the
+current torch stream and device tensors are returned, as the reference's
+device-span overloads do).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+from . import _device as D
+from .configs import PulsarSearchConfig
+from .plans import FFAPlanTime
+
+_STORAGE = {"fp32": C.LK_FP32, "float32": C.LK_FP32, "bf16": C.LK_BF16, "fp16": C.LK_FP16}
+
+
+def _check_time_domain(cfg: PulsarSearchConfig) -> None:
+    if cfg.use_fourier:
+        raise NotImplementedError(
+            "the Fourier-domain FFA is not implemented; construct the config with use_fourier=False"
+        )
+
+
+class FFACUDA:
+    """Time-domain FFA executor on one device (reference ``FFACUDA<float>``).
+
+    The executor owns the coordinate tables, brute-fold run tables and the
+    intermediate fold buffers; it can be executed many times.
+    """
+
+    def __init__(self, cfg: PulsarSearchConfig, device_id: int = 0, fold_storage: str = "fp32"):
+        D.require_cuda(device_id)
+        self._cfg = cfg
+        self._plan = FFAPlanTime(cfg)
+        self._device = device_id
+        if fold_storage not in _STORAGE:
+            raise ValueError(f"fold_storage must be one of {sorted(_STORAGE)}")
+        h = ctypes.c_void_p()
+        with D.torch().cuda.device(device_id):
+            C.check(C.lib().lk_ffa_create(cfg._plan_handle, device_id, _STORAGE[fold_storage], ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                C.lib().lk_ffa_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def plan(self) -> FFAPlanTime:
+        return self._plan
+
+    @property
+    def device_id(self) -> int:
+        return self._device
+
+    @property
+    def workspace_bytes(self) -> int:
+        n = ctypes.c_uint64()
+        C.check(C.lib().lk_ffa_workspace_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def _inputs(self, ts_e, ts_v):
+        n = self._cfg.nsamps
+        e = D.to_device_f32(ts_e, self._device)
+        v = D.to_device_f32(ts_v, self._device)
+        if e.numel() != n:
+            raise RuntimeError("FFA::execute: ts_e must have size nsamps")
+        if v.numel() != e.numel():
+            raise RuntimeError("FFA::execute: ts_v must have size nsamps")
+        return e, v
+
+    def execute(self, ts_e, ts_v, fold=None):
+        """Final-level fold. With a CUDA tensor `fold` (>= fold_size floats) the
+        result is written there; otherwise a new array/tensor is returned."""
+        host = not (D.is_device_tensor(ts_e) and D.is_device_tensor(ts_v))
+        e, v = self._inputs(ts_e, ts_v)
+        n = self._plan.fold_size
+        out = fold if D.is_device_tensor(fold) else D.empty_f32(n, self._device)
+        if out.numel() < n:
+            raise RuntimeError("FFA::execute: fold must have size >= fold_size")
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_ffa_execute(self._h, D.ptr(e), D.ptr(v), D.ptr(out), out.numel(),
+                                           D.stream_ptr(self._device)))
+        if fold is not None and not D.is_device_tensor(fold):
+            np.copyto(np.asarray(fold).reshape(-1)[:n], out[:n].cpu().numpy())
+            return fold
+        return out[:n].cpu().numpy() if host else out
+
+    def scores(self, ts_e, ts_v, out=None):
+        """Boxcar S/N [ncoords_final, n_widths] (final level fused with scoring)."""
+        host = not (D.is_device_tensor(ts_e) and D.is_device_tensor(ts_v))
+        e, v = self._inputs(ts_e, ts_v)
+        nc = int(self._plan.ncoords[-1])
+        nw = self._cfg.n_scoring_widths
+        res = out if D.is_device_tensor(out) else D.empty_f32(nc * nw, self._device)
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_ffa_scores(self._h, D.ptr(e), D.ptr(v), D.ptr(res), res.numel(),
+                                          D.stream_ptr(self._device)))
+        if host:
+            return res[: nc * nw].cpu().numpy()
+        return res
+
+    def search(self, ts_e, ts_v, snr_min: float | None = None, max_cands: int | None = None):
+        """Scores compacted to ``score >= snr_min`` in flat (coord * n_widths + width)
+        order, as FFAFreqSweep does. Returns (indices, snrs, n_total_passing)."""
+        e, v = self._inputs(ts_e, ts_v)
+        thr = self._cfg.snr_min if snr_min is None else float(snr_min)
+        cap = self._cfg.max_passing_candidates if max_cands is None else int(max_cands)
+        t = D.torch()
+        idx = t.empty(cap, dtype=t.int32, device=f"cuda:{self._device}")
+        snr = D.empty_f32(cap, self._device)
+        cnt = t.zeros(1, dtype=t.int64, device=f"cuda:{self._device}")
+        with t.cuda.device(self._device):
+            C.check(C.lib().lk_ffa_search(self._h, D.ptr(e), D.ptr(v), thr, idx.data_ptr(), D.ptr(snr),
+                                          cap, cnt.data_ptr(), D.stream_ptr(self._device)))
+        total = int(cnt.item())
+        k = min(total, cap)
+        return idx[:k].cpu().numpy().view(np.uint32), snr[:k].cpu().numpy(), total
+
+    def set_profiling(self, enable: bool = True) -> None:
+        """Record CUDA events around every kernel stage of subsequent calls."""
+        C.check(C.lib().lk_ffa_set_profiling(self._h, 1 if enable else 0))
+
+    def profile(self) -> list[dict]:
+        """Stages of the last call: kind, level, launches, GPU ms, algorithmic bytes."""
+        arr = (C.LkStageTime * 128)()
+        n = ctypes.c_uint32()
+        C.check(C.lib().lk_ffa_get_profile(self._h, D.stream_ptr(self._device), arr, 128, ctypes.byref(n)))
+        return [
+            {"stage": C.STAGE_NAMES.get(arr[i].kind, str(arr[i].kind)), "level": arr[i].level,
+             "launches": arr[i].launches, "ms": float(arr[i].ms), "bytes": int(arr[i].bytes)}
+            for i in range(min(n.value, 128))
+        ]
+
+    def status(self) -> int:
+        st = ctypes.c_uint32()
+        C.check(C.lib().lk_ffa_status(self._h, D.stream_ptr(self._device), ctypes.byref(st)))
+        return st.value
+
+
+def compute_ffa_time_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int = 0, quiet: bool = False):
+    """Final-level time-domain fold and its plan (reference lib/ffa_cuda.cu:609-628)."""
+    ffa = FFACUDA(cfg, device_id)
+    return ffa.execute(np.asarray(ts_e, dtype=np.float32), np.asarray(ts_v, dtype=np.float32)), ffa.plan
+
+
+def compute_ffa_scores_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int = 0, quiet: bool = False):
+    """Boxcar S/N of every final coordinate and width, and the plan
+    (reference lib/ffa_cuda.cu:671-692)."""
+    _check_time_domain(cfg)
+    ffa = FFACUDA(cfg, device_id)
+    return ffa.scores(np.asarray(ts_e, dtype=np.float32), np.asarray(ts_v, dtype=np.float32)), ffa.plan

@@ -1,0 +1,96 @@
+"""Seeded synthetic time series for benchmarks and tests.
+
+White N(0, 1) noise (variance series of ones) plus pulse trains with a von
+Mises pulse shape, exp(kappa (cos 2 pi phi - 1)) with
+kappa = ln 2 / (1 - cos(pi duty)) (duty = full width at half maximum as a
+fraction of the period), and a Taylor phase model about the middle of the
+observation: phi(t) = f0 (t - d(t)), d(t) = a t^2 / (2c) + j t^3 / (6c).
+Amplitudes are set so that the noiseless pulse folded at its true parameters
+and scored by the boxcar scorer reaches the requested S/N.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+C_LIGHT = 299792458.0
+
+
+@dataclass
+class Pulsar:
+    f0: float
+    accel: float = 0.0
+    jerk: float = 0.0
+    duty: float = 0.05
+    snr: float = 10.0
+
+
+def von_mises_profile(nbins: int, duty: float, oversample: int = 32) -> np.ndarray:
+    kappa = np.log(2.0) / (1.0 - np.cos(np.pi * duty))
+    phi = (np.arange(nbins * oversample) + 0.5) / (nbins * oversample)
+    p = np.exp(kappa * (np.cos(2 * np.pi * phi) - 1.0))
+    return p.reshape(nbins, oversample).mean(axis=1)
+
+
+def _boxcar_snr(x: np.ndarray, widths) -> float:
+    # Boxcar S/N of a unit-variance profile (same template as the scorer).
+    n = x.size
+    best = -np.inf
+    for w in widths:
+        h = np.sqrt((n - w) / (n * w))
+        b = w * h / (n - w)
+        ext = np.concatenate([x, x[:w]])
+        win = np.convolve(ext, np.ones(w), mode="valid")[:n]
+        best = max(best, (h + b) * win.max() - b * x.sum())
+    return float(best)
+
+
+def amplitude_for_snr(snr: float, nsamps: int, nbins: int, duty: float, widths) -> float:
+    """Per-sample peak amplitude giving the target folded boxcar S/N."""
+    prof = von_mises_profile(nbins, duty)
+    # Folded signal in bin b: A * (nsamps / nbins) * prof_b; noise sd per bin
+    # sqrt(nsamps / nbins): the normalised profile is A * sqrt(nsamps/nbins) * prof.
+    unit = _boxcar_snr(np.sqrt(nsamps / nbins) * prof, widths)
+    return snr / unit
+
+
+def inject(ts: np.ndarray, tsamp: float, psr: Pulsar, nbins: int, widths, chunk: int = 1 << 20) -> None:
+    n = ts.size
+    t_ref = n * tsamp / 2.0
+    kappa = np.log(2.0) / (1.0 - np.cos(np.pi * psr.duty))
+    amp = amplitude_for_snr(psr.snr, n, nbins, psr.duty, widths)
+    for i0 in range(0, n, chunk):
+        t = (np.arange(i0, min(n, i0 + chunk)) * tsamp) - t_ref
+        delay = psr.accel * t * t / (2 * C_LIGHT) + psr.jerk * t**3 / (6 * C_LIGHT)
+        phase = psr.f0 * (t - delay)
+        ts[i0 : i0 + t.size] += (amp * np.exp(kappa * (np.cos(2 * np.pi * phase) - 1.0))).astype(np.float32)
+
+
+def make_series(nsamps: int, tsamp: float, seed: int, pulsars=(), nbins: int = 64, widths=(1, 2, 4, 8)):
+    rng = np.random.default_rng(seed)
+    ts_e = rng.standard_normal(nsamps, dtype=np.float32)
+    for p in pulsars:
+        inject(ts_e, tsamp, p, nbins, widths)
+    ts_v = np.ones(nsamps, dtype=np.float32)
+    return ts_e, ts_v
+
+
+def taylor_accel_workload(seed: int = 7, n_signals: int = 4):
+    """Taylor FFA (f, fdot) workload: 2^22 samples at 64 us, seed 7, four
+    signals with f ~ U(5, 50) Hz, accel ~ U(-150, 150) m/s^2 and fold
+    S/N ~ U(8, 20); searched over f in [5, 50] Hz, |accel| <= 200 m/s^2 at
+    nbins = 64 with boxcar widths {1, 2, 3, 4, 6, 8, 12, 16}."""
+    nsamps, tsamp, nbins = 1 << 22, 64e-6, 64
+    widths = [1, 2, 3, 4, 6, 8, 12, 16]
+    rng = np.random.default_rng(seed + 1000)
+    pulsars = [
+        Pulsar(f0=float(rng.uniform(5, 50)), accel=float(rng.uniform(-150, 150)),
+               duty=0.05, snr=float(rng.uniform(8, 20)))
+        for _ in range(n_signals)
+    ]
+    ts_e, ts_v = make_series(nsamps, tsamp, seed, pulsars, nbins, widths)
+    params = dict(nsamps=nsamps, tsamp=tsamp, nbins=nbins, eta=2.0,
+                  param_limits=[[-200.0, 200.0], [5.0, 50.0]], score_widths=widths)
+    return ts_e, ts_v, params, pulsars

@@ -78,6 +78,9 @@ def lib() -> ctypes.CDLL:
             raise RuntimeError(f"oracle library missing: {_LIB_PATH} (run `make -C oracle oracle`)")
         L = ctypes.CDLL(_LIB_PATH)
         L.lko_last_error.restype = ctypes.c_char_p
+        L.lko_plan_create.argtypes = [vp, vp]
+        L.lko_resolve_freq.argtypes = [vp, vp]
+        L.lko_resolve_taylor.argtypes = [vp, vp]
         L.lko_phase_idx.restype = f32
         L.lko_phase_idx.argtypes = [f64, f64, u64, f64]
         L.lko_phase_idx_uint.restype = u32
@@ -281,8 +284,25 @@ def snr_boxcar_2d_max(folds, widths, nbins, stdnoise=1.0) -> np.ndarray:
 
 def circular_prefix_sum(x, nsum) -> np.ndarray:
     x = np.ascontiguousarray(x, dtype=np.float32)
-    out = np.zeros(nsum, dtype=np.float32)
+    # The reference always writes the first nbins entries, even when nsum < nbins.
+    out = np.zeros(max(nsum, x.size), dtype=np.float32)
     lib().lko_circular_prefix_sum(_p(x), _p(out), x.size, nsum)
+    return out[:nsum].copy()
+
+
+def merge_freq(fold_in, coords, ncur, nprev, nseg, nbins) -> np.ndarray:
+    fold_in = np.ascontiguousarray(fold_in, dtype=np.float32)
+    coords = np.ascontiguousarray(coords, dtype=COORD_FREQ_DTYPE)
+    out = np.zeros(nseg * ncur * 2 * nbins, dtype=np.float32)
+    lib().lko_merge_freq(_p(fold_in), _p(out), _p(coords), ncur, nprev, nseg, nbins)
+    return out
+
+
+def merge_taylor(fold_in, coords, ncur, nprev, nseg, nbins) -> np.ndarray:
+    fold_in = np.ascontiguousarray(fold_in, dtype=np.float32)
+    coords = np.ascontiguousarray(coords, dtype=COORD_DTYPE)
+    out = np.zeros(nseg * ncur * 2 * nbins, dtype=np.float32)
+    lib().lko_merge_taylor(_p(fold_in), _p(out), _p(coords), ncur, nprev, nseg, nbins)
     return out
 
 

@@ -1,0 +1,108 @@
+"""Generates the golden fixtures in this folder from the reference's own code.
+
+Run from the repository root after ``make -C oracle ref``:
+
+    python tests/golden/make_golden.py
+
+Every output comes from ``oracle/_ref/libloki_ref_parity.so`` -- the
+reference's CPU sources compiled unmodified with IEEE flags -- so the fixtures
+pin both the C oracle and the CUDA path to the reference's results on machines
+where the reference cannot be built. Inputs are stored in the fixtures (not
+regenerated from a seed) so they stay valid across numpy versions. Final
+folds are stored in full when small and always as a SHA-256 of their bytes.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import ref  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# name -> (nsamps, tsamp, nbins, eta, param_limits, seed)
+FFA_CASES = {
+    "ffa_freq_nb32": (8192, 64e-6, 32, 1.0, [[50.0, 60.0]], 1),
+    "ffa_freq_nb64": (8192, 64e-6, 64, 1.0, [[70.0, 90.0]], 2),
+    "ffa_accel_nb16": (16384, 8e-3, 16, 1.0, [[-1000.0, 1000.0], [10.0, 10.3]], 3),
+    "ffa_jerk_nb16": (16384, 8e-3, 16, 1.0, [[-100.0, 100.0], [-900.0, 900.0], [10.0, 10.2]], 4),
+}
+WIDTHS = np.array([1, 2, 3, 4, 6, 8, 12], dtype=np.uint64)
+FOLD_KEEP = 1 << 15  # store folds in full up to this many floats
+
+
+def series(n: int, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    rng = np.random.default_rng(seed)
+    ts_e = rng.standard_normal(n).astype(np.float32)
+    ts_v = (1.0 + 0.25 * rng.random(n)).astype(np.float32)
+    return ts_e, ts_v
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main() -> None:
+    if not ref.available():
+        raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` first")
+    for name, (nsamps, tsamp, nbins, eta, lims, seed) in FFA_CASES.items():
+        ts_e, ts_v = series(nsamps, seed)
+        cfg = ref.make_cfg(nsamps, tsamp, nbins, eta, lims)
+        ffa = ref.RefFFA(cfg)
+        fold = ffa.execute(ts_e, ts_v).copy()
+        coords = ref.resolve(cfg, ffa.coord_size)
+        widths = WIDTHS[WIDTHS < nbins]
+        scores = ref.snr_boxcar_3d(fold, widths, nbins)
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"),
+            ts_e=ts_e, ts_v=ts_v, nsamps=nsamps, nbins=nbins, eta=eta, tsamp=tsamp,
+            param_limits=np.array(lims, dtype=np.float64),
+            n_levels=ffa.n_levels, bseg_brute=ffa.bseg_brute, ncoords=ffa.ncoords,
+            param_counts=ffa.param_counts, dparams=ffa.dparams,
+            ncoords_offsets=ffa.ncoords_offsets,
+            coords=coords.view(np.uint32).reshape(coords.size, -1),
+            fold=fold if fold.size <= FOLD_KEEP else fold[:0], fold_sha256=sha(fold),
+            fold_size=fold.size, widths=widths, scores=scores,
+        )
+        print(name, "levels", ffa.n_levels, "final counts", ffa.param_counts[-1].tolist())
+
+    # Brute fold with an explicit frequency list (reference test shape,
+    # tests/python/test_cpu_match.py:20-61, scaled down).
+    ts_e, ts_v = series(1 << 14, 5)
+    freqs = np.linspace(140.0, 145.0, 7)
+    bf = ref.brute_fold(ts_e, ts_v, freqs, 1 << 11, 64, 64e-6, 0.0)
+    np.savez_compressed(os.path.join(OUT, "brute_fold_nb64.npz"), ts_e=ts_e, ts_v=ts_v, freqs=freqs,
+                        segment_len=1 << 11, nbins=64, tsamp=64e-6, t_ref=0.0, fold=bf)
+
+    # Boxcar scores of random (E, V) folds, per width and max; width trials.
+    rng = np.random.default_rng(6)
+    folds = np.empty((96, 2, 48), dtype=np.float32)
+    folds[:, 0] = rng.standard_normal((96, 48)) * 10
+    folds[:, 1] = 50 + rng.random((96, 48)) * 10
+    widths = np.array([1, 2, 3, 5, 8, 13], dtype=np.uint64)
+    np.savez_compressed(os.path.join(OUT, "scores_nb48.npz"), folds=folds, widths=widths,
+                        scores=ref.snr_boxcar_3d(folds, widths, 48),
+                        scores_max=ref.snr_boxcar_3d_max(folds, widths, 48),
+                        trials_64=ref.box_widths(64), trials_128=ref.box_widths(128),
+                        trials_100_03=ref.box_widths(100, 0.3, 1.5))
+
+    # Phase-index known answers straight from psr_utils::get_phase_idx[_uint].
+    pts = []
+    for t, f, nb, d in [(0.0, 10.0, 64, 0.0), (0.1, 10.0, 64, 0.0), (12.3456, 47.3, 128, 0.0),
+                        (-0.25, 21.14, 128, 1e-3), (1.0, 1.0, 32, 0.0), (0.49999, 2.0, 64, 0.0),
+                        (134.2, 50.0, 128, 0.0), (0.0123, 199.9, 32, -0.004),
+                        (0.0078125, 63.99, 64, 0.0), (3.0, 0.333333333333, 16, 0.0)]:
+        pts.append((t, f, nb, d, ref.phase_idx(t, f, nb, d), ref.phase_idx_uint(t, f, nb, d)))
+    np.savez_compressed(os.path.join(OUT, "phase_idx.npz"), cases=np.array(pts, dtype=np.float64))
+    print("done")
+
+
+if __name__ == "__main__":
+    main()
