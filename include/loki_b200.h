@@ -217,6 +217,20 @@ uint64_t lk_compact_scratch_bytes(uint64_t n);
 int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
                   float* d_vals, uint64_t max_out, uint64_t* d_count, void* d_scratch,
                   lk_stream_t stream);
+/* Allocation-free variant of lk_compact_ge; it has no counterpart in the
+ * reference. For callers that may not call cudaMalloc or any allocating
+ * routine where they compact (a host framework that owns all device memory
+ * through its own pool, or a latency-critical loop where an allocation, which
+ * can synchronise the device, is not allowed). The scratch is a static device
+ * array inside the library (768 KiB per GPU that loads the library, held
+ * until exit), so: n must not exceed 2^28 (larger n is rejected with
+ * LK_ERR_INVALID_ARG); calls whose work overlaps on the GPU race on that
+ * array and must be serialised. The first call on a device looks up the
+ * array's device address with that device current; make that first call
+ * before any stream capture. Same results as lk_compact_ge. */
+int lk_compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
+                          float* d_vals, uint64_t max_out, uint64_t* d_count,
+                          lk_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -129,6 +129,7 @@ SIGNATURES = [
     ("lk_snr_boxcar_2d_max", i32, [vp, u64, u32, vp, u32, f32, vp, vp]),
     ("lk_compact_scratch_bytes", u64, [u64]),
     ("lk_compact_ge", i32, [vp, u64, f32, vp, vp, u64, vp, vp, vp]),
+    ("lk_compact_ge_noalloc", i32, [vp, u64, f32, vp, vp, u64, vp, vp]),
 ]
 
 _lib: ctypes.CDLL | None = None

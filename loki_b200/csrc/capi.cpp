@@ -351,4 +351,21 @@ int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
     });
 }
 
+int lk_compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
+                          float* d_vals, uint64_t max_out, uint64_t* d_count,
+                          lk_stream_t stream) {
+    return guarded([&] {
+        need(d_count, "d_count");
+        if (n > 0) {
+            need(d_scores, "d_scores");
+        }
+        if (max_out > 0) {
+            need(d_idx, "d_idx");
+            need(d_vals, "d_vals");
+        }
+        lk::compact_ge_noalloc(d_scores, n, thr, d_idx, d_vals, max_out, d_count,
+                               reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 }  // extern "C"

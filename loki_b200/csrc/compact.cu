@@ -2,6 +2,8 @@
 // i -- the order FFAFreqSweep produces (lib/ffa_freq_sweep.cpp:182-195).
 // Three passes, no atomics, deterministic: per-tile counts, one exclusive scan
 // of the counts, per-tile ordered scatter.
+#include <mutex>
+
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
 
@@ -123,6 +125,65 @@ __global__ void tile_scatter_kernel(const float* __restrict__ x, uint64_t n, flo
 }
 
 }  // namespace
+
+// ---- allocation-free variant -------------------------------------------------
+//
+// For callers that cannot call cudaMalloc (or any allocating routine) at the
+// point where they compact: e.g. a host framework that owns all device memory
+// through its own pool and forbids direct allocations, or a latency-critical
+// loop where an allocation, which may synchronise the device, is not allowed.
+// The tile counts and offsets live in this file-scope device array instead of
+// caller-provided scratch. Limits and sharing rules:
+//   * n <= kNoAllocMaxN (2^28 scores): 65,536 tiles of 4,096, 768 KiB + 16 B
+//     of device memory, held by every GPU that loads the library until exit;
+//   * every call uses the same array, so calls whose work overlaps on the GPU
+//     (e.g. on two streams) race and give wrong results; serialise them;
+//   * the array keeps the previous call's contents; nothing needs clearing,
+//     because each call writes every count and offset it later reads.
+constexpr uint64_t kNoAllocMaxN = 1ull << 28;
+constexpr uint64_t kNoAllocMaxTiles = kNoAllocMaxN / kTile;
+// Same size rule as compact_scratch_bytes(), usable in a static_assert.
+constexpr uint64_t compact_scratch_bytes_c(uint64_t n) {
+    return ((n + kTile - 1) / kTile) * (sizeof(uint32_t) + sizeof(uint64_t)) + 16;
+}
+constexpr size_t kNoAllocScratchBytes =
+    kNoAllocMaxTiles * (sizeof(uint32_t) + sizeof(uint64_t)) + 16;
+
+static __device__ __align__(256) unsigned char g_compact_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+// Device address of g_compact_noalloc_scratch for the current device. In host
+// code the symbol's name is only a host-side stand-in, so the address is
+// looked up once per device (with that device current) and cached.
+void* noalloc_scratch_for_current_device() {
+    static std::mutex mu;
+    static void* addr[64] = {};
+    int dev = -1;
+    LK_CUDA(cudaGetDevice(&dev));
+    require(dev >= 0 && dev < 64, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (addr[dev] == nullptr) {
+        void* p = nullptr;
+        LK_CUDA(cudaGetSymbolAddress(&p, g_compact_noalloc_scratch));
+        addr[dev] = p;
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
+void compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
+                        float* d_vals, uint64_t max_out, uint64_t* d_count, cudaStream_t s) {
+    if (n > kNoAllocMaxN) {
+        fail(LK_ERR_INVALID_ARG,
+             "lk_compact_ge_noalloc: n exceeds the static scratch limit of 2^28 scores");
+    }
+    static_assert(compact_scratch_bytes_c(kNoAllocMaxN) <= kNoAllocScratchBytes,
+                  "static scratch too small");
+    compact_ge(d_scores, n, thr, d_idx, d_vals, max_out, d_count,
+               noalloc_scratch_for_current_device(), s);
+}
 
 uint64_t compact_scratch_bytes(uint64_t n) {
     const uint64_t ntiles = (n + kTile - 1) / kTile;

@@ -103,5 +103,8 @@ void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d
 uint64_t compact_scratch_bytes(uint64_t n);
 void compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx, float* d_vals,
                 uint64_t max_out, uint64_t* d_count, void* d_scratch, cudaStream_t s);
+// Same compaction with its scratch in a static device array (n <= 2^28).
+void compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
+                        float* d_vals, uint64_t max_out, uint64_t* d_count, cudaStream_t s);
 
 }  // namespace lk
