@@ -107,8 +107,9 @@ float* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t last,
         float* out = (l == last && final_out != nullptr) ? final_out : buf[l % 2].as<float>();
         prof.begin(LK_STAGE_MERGE, static_cast<int>(l), 1,
                    4 * (plan.fold_size(l - 1) + plan.fold_size(l)) + coord_bytes(l), s);
-        merge_level(in, out, level_coords(l), taylor, plan.ncoords[l], plan.ncoords[l - 1],
-                    plan.nsegments[l], nbins, s);
+        const uint64_t n_inner = plan.param_counts[l][plan.nparams - 1];
+        merge_level(in, out, level_coords(l), taylor, n_inner, plan.ncoords[l] / n_inner,
+                    plan.ncoords[l - 1], plan.nsegments[l], nbins, s);
         prof.end(s);
         in = out;
     }
@@ -138,9 +139,10 @@ void FFAExec::scores(const float* ts_e, const float* ts_v, float* d_scores, uint
     const uint64_t nscores = plan.ncoords[L - 1] * plan.widths.size();
     prof.begin(LK_STAGE_MERGE_SCORE, static_cast<int>(L - 1), 1,
                4 * plan.fold_size(L - 2) + coord_bytes(L - 1) + 4 * nscores, s);
-    merge_score_level(in, level_coords(L - 1), plan.nparams > 1, plan.ncoords[L - 1],
-                      plan.ncoords[L - 2], static_cast<uint32_t>(plan.cfg.nbins), sp,
-                      LK_SCORE_PER_WIDTH, d_scores, s);
+    const uint64_t n_inner = plan.param_counts[L - 1][plan.nparams - 1];
+    merge_score_level(in, level_coords(L - 1), plan.nparams > 1, n_inner,
+                      plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
+                      static_cast<uint32_t>(plan.cfg.nbins), sp, LK_SCORE_PER_WIDTH, d_scores, s);
     prof.end(s);
 }
 

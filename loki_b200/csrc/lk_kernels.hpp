@@ -41,11 +41,11 @@ struct DeviceBuffer {
 // Brute fold of a time series into [nseg, nfreq, 2, nbins] FP32.
 //
 // Plan-time tables: for every trial frequency the sample -> phase-bin map of
-// one segment (identical for all segments) is encoded as a sequence of run
-// lengths over "virtual bins" v = 0, 1, 2, ... with bin(v) = v mod nbins, in
-// sample order. Replaying the runs in order adds every sample to its bin in
-// increasing sample order, which is the reference's summation order
-// (lib/kernels.cpp:550-580), so the fold is bit-identical.
+// one segment (identical for all segments) is encoded as the runs of equal
+// bin in sample order, split at chunk boundaries. Replaying the runs in order
+// adds every sample to its bin in increasing sample order, which is the
+// reference's summation order (lib/kernels.cpp:550-580), so the fold is
+// bit-identical.
 class BruteFoldDevice {
 public:
     BruteFoldDevice(const std::vector<double>& freqs, uint64_t segment_len, uint64_t nbins,
@@ -64,19 +64,24 @@ public:
     uint64_t device_bytes() const;
 
 private:
-    uint64_t m_nfreq, m_seglen, m_nbins, m_nsamps, m_nseg, m_nseg_pad;
+    uint64_t m_nfreq, m_seglen, m_nbins, m_nsamps, m_nseg = 0, m_nseg_pad = 0;
+    uint64_t m_chunk = 0, m_nchunks = 0;
+    uint32_t m_spl = 1;       // segments per lane (1, 2 or 4)
+    uint32_t m_rows = 2;      // rows (E, V) per consumer warp (1 or 2)
+    uint32_t m_warps = 0;     // consumer warps per block
+    size_t m_smem = 0;        // dynamic shared memory per block
     uint32_t* m_status;
-    DeviceBuffer m_lens;      // uint16 run lengths, all frequencies
-    DeviceBuffer m_lens_off;  // uint64 offset (entries) per frequency
-    DeviceBuffer m_nper;      // uint32 virtual periods per frequency
+    DeviceBuffer m_entries;   // uint32 (bin << 16 | run length), all frequencies
+    DeviceBuffer m_offsets;   // uint64 first entry of each frequency
+    DeviceBuffer m_counts;    // uint8 [nfreq][nchunks] entries per chunk
     DeviceBuffer m_xT;        // float [2][seglen][nseg_pad]
     CUtensorMap m_tmap{};
-    bool m_use_tma = false;
 };
 
 // One merge level: out[s, c] = rot(in[2s, tail(c)], st(c)) + rot(in[2s+1, head(c)], sh(c)).
+// Coordinates are [n_outer][n_inner] (n_inner = frequency cells).
 void merge_level(const float* d_in, float* d_out, const void* d_coords, bool taylor,
-                 uint64_t ncoords_cur, uint64_t ncoords_prev, uint64_t nsegments,
+                 uint64_t n_inner, uint64_t n_outer, uint64_t ncoords_prev, uint64_t nsegments,
                  uint32_t nbins, cudaStream_t s);
 
 // Boxcar scoring parameters shared by the score kernels.
@@ -90,8 +95,8 @@ struct ScoreParams {
 ScoreParams make_score_params(const uint32_t* widths, uint32_t nwidths, uint32_t nbins);
 
 // Final merge level fused with scoring (nsegments == 1).
-void merge_score_level(const float* d_in, const void* d_coords, bool taylor,
-                       uint64_t ncoords_cur, uint64_t ncoords_prev, uint32_t nbins,
+void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
+                       uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                        const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s);
 
 // Standalone scoring of [nprof, 2, nbins] (is3d) or [nprof, nbins] folds.

@@ -9,70 +9,51 @@
 // one FP32 add of the same two operands as the reference, so results are
 // bit-identical.
 //
-// Work split: a warp per (segment, coordinate) row pair; lanes stride over
-// the 2*nbins output elements, so every load and store instruction of a warp
-// touches one contiguous (rotated) 128-byte span of a row.
+// Work split: a block covers up to kCoordsPerBlock consecutive frequency cells
+// of one "outer" row (the higher-derivative cells: accel, or jerk x accel) of
+// one segment; a warp handles one output row pair at a time with lanes
+// striding over the 2*nbins elements (each warp instruction reads one rotated,
+// contiguous 128-byte span). Blocks are numbered frequency-tile-major, so the
+// outer rows that read the same parent rows run at the same time and share
+// them through L2.
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
+#include "lk_merge.cuh"
 
 namespace lk {
 
 namespace {
 
 constexpr int kWarp = 32;
-
-struct CoordFreq {
-    uint32_t idx;
-    float shift;
-};
-struct CoordTaylor {
-    uint32_t i_tail;
-    float shift_tail;
-    uint32_t i_head;
-    float shift_head;
-};
+constexpr int kThreads = 256;
+constexpr uint32_t kCoordsPerBlock = 64;
 
 template <bool TAYLOR>
-__device__ __forceinline__ void load_coord(const void* coords, uint64_t c, uint32_t nbins,
-                                           uint32_t* it, uint32_t* st, uint32_t* ih,
-                                           uint32_t* sh) {
-    if constexpr (TAYLOR) {
-        const CoordTaylor k = reinterpret_cast<const CoordTaylor*>(coords)[c];
-        *it = k.i_tail;
-        *ih = k.i_head;
-        *st = dev::shift_bins(k.shift_tail, nbins);
-        *sh = dev::shift_bins(k.shift_head, nbins);
-    } else {
-        const CoordFreq k = reinterpret_cast<const CoordFreq*>(coords)[c];
-        *it = k.idx;
-        *ih = k.idx;
-        *st = 0;
-        *sh = dev::shift_bins(k.shift, nbins);
-    }
-}
-
-template <bool TAYLOR>
-__global__ void merge_kernel(const float* __restrict__ in, float* __restrict__ out,
-                             const void* __restrict__ coords, uint64_t ncur, uint64_t nprev,
-                             uint64_t nseg, uint32_t nbins) {
-    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / kWarp);
-    const uint64_t w0 = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
-    const uint32_t lane = threadIdx.x % kWarp;
-    const uint64_t total = nseg * ncur;
+__global__ void __launch_bounds__(kThreads)
+    merge_kernel(const float* __restrict__ in, float* __restrict__ out,
+                 const void* __restrict__ coords, uint32_t n_inner, uint32_t n_outer,
+                 uint64_t nprev, uint32_t nbins) {
+    const uint32_t tiles = (n_inner + kCoordsPerBlock - 1) / kCoordsPerBlock;
+    const uint32_t tile = blockIdx.x / n_outer;
+    const uint32_t outer = blockIdx.x - tile * n_outer;
+    const uint64_t s = blockIdx.y;
+    const uint64_t ncur = static_cast<uint64_t>(n_inner) * n_outer;
     const uint32_t row = 2 * nbins;
-    for (uint64_t w = w0; w < total; w += nwarps) {
-        const uint64_t s = w / ncur;
-        const uint64_t c = w - s * ncur;
-        uint32_t it, st, ih, sh;
-        load_coord<TAYLOR>(coords, c, nbins, &it, &st, &ih, &sh);
-        const float* tail = in + ((2 * s) * nprev + it) * row;
-        const float* head = in + ((2 * s + 1) * nprev + ih) * row;
-        float* o = out + w * row;
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    (void)tiles;
+    const uint32_t j0 = tile * kCoordsPerBlock;
+    const uint32_t j1 = min(j0 + kCoordsPerBlock, n_inner);
+    for (uint32_t jf = j0 + warp; jf < j1; jf += kThreads / kWarp) {
+        const uint64_t c = static_cast<uint64_t>(outer) * n_inner + jf;
+        const MergeCoord mc = load_merge_coord<TAYLOR>(coords, c, nbins);
+        const float* tail = in + ((2 * s) * nprev + mc.it) * row;
+        const float* head = in + ((2 * s + 1) * nprev + mc.ih) * row;
+        float* o = out + (s * ncur + c) * row;
         for (uint32_t e = lane; e < row; e += kWarp) {
             const uint32_t r = e >= nbins ? nbins : 0;
             const uint32_t j = e - r;
-            const uint32_t jt = j >= st ? j - st : j + nbins - st;
-            const uint32_t jh = j >= sh ? j - sh : j + nbins - sh;
+            const uint32_t jt = j >= mc.st ? j - mc.st : j + nbins - mc.st;
+            const uint32_t jh = j >= mc.sh ? j - mc.sh : j + nbins - mc.sh;
             o[e] = __fadd_rn(__ldg(tail + r + jt), __ldg(head + r + jh));
         }
     }
@@ -81,18 +62,24 @@ __global__ void merge_kernel(const float* __restrict__ in, float* __restrict__ o
 }  // namespace
 
 void merge_level(const float* d_in, float* d_out, const void* d_coords, bool taylor,
-                 uint64_t ncoords_cur, uint64_t ncoords_prev, uint64_t nsegments,
+                 uint64_t n_inner, uint64_t n_outer, uint64_t ncoords_prev, uint64_t nsegments,
                  uint32_t nbins, cudaStream_t s) {
-    const uint64_t total = ncoords_cur * nsegments;
-    const unsigned threads = 256;
-    const uint64_t want = (total + (threads / kWarp) - 1) / (threads / kWarp);
-    const unsigned blocks = static_cast<unsigned>(want < 148ull * 64 ? want : 148ull * 64);
+    require(n_inner > 0 && n_outer > 0, "empty merge level");
+    const uint64_t tiles = (n_inner + kCoordsPerBlock - 1) / kCoordsPerBlock;
+    require(tiles * n_outer <= 0x7fffffffULL && nsegments <= 65535 && n_inner <= 0xffffffffULL &&
+                n_outer <= 0xffffffffULL,
+            "merge level too large for the launch grid");
+    dim3 grid(static_cast<unsigned>(tiles * n_outer), static_cast<unsigned>(nsegments));
     if (taylor) {
-        merge_kernel<true><<<blocks, threads, 0, s>>>(d_in, d_out, d_coords, ncoords_cur,
-                                                      ncoords_prev, nsegments, nbins);
+        merge_kernel<true><<<grid, kThreads, 0, s>>>(d_in, d_out, d_coords,
+                                                     static_cast<uint32_t>(n_inner),
+                                                     static_cast<uint32_t>(n_outer),
+                                                     ncoords_prev, nbins);
     } else {
-        merge_kernel<false><<<blocks, threads, 0, s>>>(d_in, d_out, d_coords, ncoords_cur,
-                                                       ncoords_prev, nsegments, nbins);
+        merge_kernel<false><<<grid, kThreads, 0, s>>>(d_in, d_out, d_coords,
+                                                      static_cast<uint32_t>(n_inner),
+                                                      static_cast<uint32_t>(n_outer),
+                                                      ncoords_prev, nbins);
     }
     LK_CUDA(cudaGetLastError());
 }

@@ -3,76 +3,65 @@
 //
 // Per profile (reference: snr_boxcar_impl, lib/score.cpp:95-172;
 // circular_prefix_sum / diff_max, lib/utils.cpp:22-67):
-//   x_j   = E_j * (1 / sqrt(V_j))            (3-D folds; 2-D folds use x = fold)
-//   p     = inclusive prefix sum of x, extended circularly by wmax bins
+//   x_j    = E_j * (1 / sqrt(V_j))            (3-D folds; 2-D folds use x = fold)
+//   p      = inclusive prefix sum of x, extended circularly by wmax bins
 //   dmax_w = max_i (p[i + w] - p[i]),  i in [0, nbins)
-//   snr_w = ((h_w + b_w) * dmax_w - b_w * p[nbins-1]) * inv_stdnoise
+//   snr_w  = ((h_w + b_w) * dmax_w - b_w * p[nbins-1]) * inv_stdnoise
 // with h_w = sqrt((n - w) / (n w)), b_w = w h_w / (n - w).
 //
-// One thread scores one profile, sequentially, with IEEE-rounded operations
-// in the reference's order, so scores are bit-identical to the reference's
-// CPU code. Profiles are staged in shared memory with an odd row stride:
-// threads of a warp touch the same column of 32 different rows, which falls
-// in 32 different banks.
+// Two phases per block: (1) warps build the normalised profiles x in shared
+// memory (lanes over bins: coalesced loads, element-parallel sqrt and
+// reciprocal); (2) one thread per profile runs the reference's sequential
+// prefix sum and the width maxima. Every operation is IEEE round-to-nearest
+// in the reference's order, so scores are bit-identical. Profiles are staged
+// with an odd row stride, so the 32 threads of a warp, each at the same column
+// of a different row, hit 32 different banks.
 #include <cfloat>
 #include <cmath>
 
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
+#include "lk_merge.cuh"
 
 namespace lk {
 
 namespace {
 
+constexpr int kWarp = 32;
 
-struct CoordFreq {
-    uint32_t idx;
-    float shift;
-};
-struct CoordTaylor {
-    uint32_t i_tail;
-    float shift_tail;
-    uint32_t i_head;
-    float shift_head;
-};
+// Odd row stride holding a profile and its circular extension.
+inline uint32_t row_stride(uint32_t nbins, uint32_t wmax) { return (nbins + wmax) | 1u; }
 
-// Row stride (floats) of a staged profile: room for E and V (3-D) or the
-// profile (2-D), and for the circular extension of the prefix sum; odd.
-__host__ __device__ inline uint32_t row_stride(uint32_t nbins, bool is3d, uint32_t wmax) {
-    uint32_t need = is3d ? 2 * nbins : nbins;
-    if (nbins + wmax > need) {
-        need = nbins + wmax;
-    }
-    return need | 1u;
+__device__ __forceinline__ float normalise(float e, float v) {
+    // 1.0F / std::sqrt(v) then e * that (lib/score.cpp:134-136): both
+    // correctly rounded, so rcp_rn(sqrt_rn(v)) == 1.0F / sqrt(v) exactly.
+    return __fmul_rn(e, __frcp_rn(__fsqrt_rn(v)));
 }
 
-// Scores the profile staged at r (stride-padded row) in place.
-__device__ __forceinline__ void score_row(float* r, uint32_t nbins, bool is3d,
-                                          float inv_stdnoise, const ScoreParams& sp, int mode,
-                                          float* out) {
-    float acc = 0.0f;
-    for (uint32_t j = 0; j < nbins; ++j) {
-        float x = r[j];
-        if (is3d) {
-            const float inv_sqrt_v = __fdiv_rn(1.0f, __fsqrt_rn(r[nbins + j]));
-            x = __fmul_rn(x, inv_sqrt_v);
-        }
-        acc = (j == 0) ? x : __fadd_rn(acc, x);
+// Scores the normalised profile staged at r (in place). NW >= sp.nwidths is
+// the compile-time width capacity (8, 16 or 32): the width loops are
+// unrolled to NW, so a small NW avoids evaluating unused width slots.
+template <int NW>
+__device__ __forceinline__ void score_row(float* r, uint32_t nbins, float inv_stdnoise,
+                                          const ScoreParams& sp, int mode, float* out) {
+    float acc = r[0];
+    for (uint32_t j = 1; j < nbins; ++j) {
+        acc = __fadd_rn(acc, r[j]);
         r[j] = acc;
     }
     const float sum = acc;
     for (uint32_t k = 0; k < sp.wmax; ++k) {
         r[nbins + k] = __fadd_rn(r[k], sum);
     }
-    float dm[LK_MAX_WIDTHS];
+    float dm[NW];
 #pragma unroll
-    for (int iw = 0; iw < LK_MAX_WIDTHS; ++iw) {
+    for (int iw = 0; iw < NW; ++iw) {
         dm[iw] = -FLT_MAX;
     }
     for (uint32_t i = 0; i < nbins; ++i) {
         const float ri = r[i];
 #pragma unroll
-        for (int iw = 0; iw < LK_MAX_WIDTHS; ++iw) {
+        for (int iw = 0; iw < NW; ++iw) {
             if (iw < static_cast<int>(sp.nwidths)) {
                 const float d = __fsub_rn(r[i + sp.widths[iw]], ri);
                 dm[iw] = (dm[iw] < d) ? d : dm[iw];
@@ -81,7 +70,7 @@ __device__ __forceinline__ void score_row(float* r, uint32_t nbins, bool is3d,
     }
     float best = -FLT_MAX;
 #pragma unroll
-    for (int iw = 0; iw < LK_MAX_WIDTHS; ++iw) {
+    for (int iw = 0; iw < NW; ++iw) {
         if (iw < static_cast<int>(sp.nwidths)) {
             const float base = __fsub_rn(__fmul_rn(sp.hb[iw], dm[iw]), __fmul_rn(sp.b[iw], sum));
             const float snr = __fmul_rn(base, inv_stdnoise);
@@ -97,93 +86,79 @@ __device__ __forceinline__ void score_row(float* r, uint32_t nbins, bool is3d,
     }
 }
 
+template <int NW>
 __global__ void score_kernel(const float* __restrict__ folds, uint64_t nprof, uint32_t nbins,
                              bool is3d, float inv_stdnoise, uint32_t rs, ScoreParams sp, int mode,
                              float* __restrict__ scores) {
     extern __shared__ float rows[];
     const uint32_t T = blockDim.x;
     const uint64_t p0 = static_cast<uint64_t>(blockIdx.x) * T;
+    const uint32_t nhere = static_cast<uint32_t>((nprof - p0) < T ? (nprof - p0) : T);
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
     const uint32_t plen = is3d ? 2 * nbins : nbins;
-    const uint64_t nhere = (nprof - p0) < T ? (nprof - p0) : T;
-    const uint64_t nelem = nhere * plen;
-    const float* src = folds + p0 * plen;
-    for (uint64_t e = threadIdx.x; e < nelem; e += T) {
-        const uint64_t p = e / plen;
-        const uint32_t j = static_cast<uint32_t>(e - p * plen);
-        rows[p * rs + j] = __ldg(src + e);
-    }
-    __syncthreads();
-    if (threadIdx.x < nhere) {
-        const uint64_t p = p0 + threadIdx.x;
-        const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1;
-        score_row(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, is3d, inv_stdnoise, sp,
-                  mode, scores + p * nout);
-    }
-}
-
-// Final FFA level (one segment) merged straight into shared memory and
-// scored; the final fold never reaches global memory.
-template <bool TAYLOR>
-__global__ void merge_score_kernel(const float* __restrict__ in, const void* __restrict__ coords,
-                                   uint64_t ncur, uint64_t nprev, uint32_t nbins, uint32_t rs,
-                                   ScoreParams sp, int mode, float* __restrict__ scores) {
-    extern __shared__ float rows[];
-    const uint32_t T = blockDim.x;
-    uint32_t* c_it = reinterpret_cast<uint32_t*>(rows + static_cast<size_t>(T) * rs);
-    uint32_t* c_ih = c_it + T;
-    uint32_t* c_st = c_ih + T;
-    uint32_t* c_sh = c_st + T;
-    const uint64_t p0 = static_cast<uint64_t>(blockIdx.x) * T;
-    const uint32_t nhere = static_cast<uint32_t>((ncur - p0) < T ? (ncur - p0) : T);
-    if (threadIdx.x < nhere) {
-        const uint64_t c = p0 + threadIdx.x;
-        if constexpr (TAYLOR) {
-            const CoordTaylor k = reinterpret_cast<const CoordTaylor*>(coords)[c];
-            c_it[threadIdx.x] = k.i_tail;
-            c_ih[threadIdx.x] = k.i_head;
-            c_st[threadIdx.x] = dev::shift_bins(k.shift_tail, nbins);
-            c_sh[threadIdx.x] = dev::shift_bins(k.shift_head, nbins);
-        } else {
-            const CoordFreq k = reinterpret_cast<const CoordFreq*>(coords)[c];
-            c_it[threadIdx.x] = k.idx;
-            c_ih[threadIdx.x] = k.idx;
-            c_st[threadIdx.x] = 0;
-            c_sh[threadIdx.x] = dev::shift_bins(k.shift, nbins);
+    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+        const float* src = folds + (p0 + p) * plen;
+        float* dst = rows + static_cast<size_t>(p) * rs;
+        for (uint32_t j = lane; j < nbins; j += kWarp) {
+            dst[j] = is3d ? normalise(__ldg(src + j), __ldg(src + nbins + j)) : __ldg(src + j);
         }
     }
     __syncthreads();
-    const uint32_t plen = 2 * nbins;
-    const float* head_base = in + nprev * plen;  // segment 1 of the previous level
-    // All threads sweep the block's rows; consecutive threads cover
-    // consecutive output bins of one row (coalesced, rotated reads).
-    const uint64_t nelem = static_cast<uint64_t>(nhere) * plen;
-#pragma unroll 4
-    for (uint64_t e = threadIdx.x; e < nelem; e += T) {
-        const uint32_t p = static_cast<uint32_t>(e / plen);
-        const uint32_t el = static_cast<uint32_t>(e - static_cast<uint64_t>(p) * plen);
-        const uint32_t r = el >= nbins ? nbins : 0;
-        const uint32_t j = el - r;
-        const uint32_t st = c_st[p], sh = c_sh[p];
-        const uint32_t jt = j >= st ? j - st : j + nbins - st;
-        const uint32_t jh = j >= sh ? j - sh : j + nbins - sh;
-        const float t = __ldg(in + static_cast<uint64_t>(c_it[p]) * plen + r + jt);
-        const float h = __ldg(head_base + static_cast<uint64_t>(c_ih[p]) * plen + r + jh);
-        rows[static_cast<size_t>(p) * rs + el] = __fadd_rn(t, h);
-    }
-    __syncthreads();
     if (threadIdx.x < nhere) {
         const uint64_t p = p0 + threadIdx.x;
         const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1;
-        score_row(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, true, 1.0f, sp, mode,
-                  scores + p * nout);
+        score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, inv_stdnoise, sp, mode,
+                      scores + p * nout);
+    }
+}
+
+// Final FFA level (one output segment) merged and normalised straight into
+// shared memory, then scored; the final fold never reaches global memory.
+// Block = up to T consecutive frequency cells of one outer row; blocks are
+// numbered frequency-tile-major (see merge.cu).
+template <bool TAYLOR, int NW>
+__global__ void merge_score_kernel(const float* __restrict__ in, const void* __restrict__ coords,
+                                   uint32_t n_inner, uint32_t n_outer, uint64_t nprev,
+                                   uint32_t nbins, uint32_t rs, ScoreParams sp, int mode,
+                                   float* __restrict__ scores) {
+    extern __shared__ float rows[];
+    const uint32_t T = blockDim.x;
+    const uint32_t tile = blockIdx.x / n_outer;
+    const uint32_t outer = blockIdx.x - tile * n_outer;
+    const uint32_t j0 = tile * T;
+    const uint32_t nhere = min(T, n_inner - j0);
+    const uint64_t c0 = static_cast<uint64_t>(outer) * n_inner + j0;
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    const uint32_t plen = 2 * nbins;
+    const float* head_base = in + nprev * plen;  // segment 1 of the previous level
+#pragma unroll 2
+    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+        const MergeCoord mc = load_merge_coord<TAYLOR>(coords, c0 + p, nbins);
+        const float* tail = in + static_cast<uint64_t>(mc.it) * plen;
+        const float* head = head_base + static_cast<uint64_t>(mc.ih) * plen;
+        float* dst = rows + static_cast<size_t>(p) * rs;
+        for (uint32_t j = lane; j < nbins; j += kWarp) {
+            const uint32_t jt = j >= mc.st ? j - mc.st : j + nbins - mc.st;
+            const uint32_t jh = j >= mc.sh ? j - mc.sh : j + nbins - mc.sh;
+            const float e = __fadd_rn(__ldg(tail + jt), __ldg(head + jh));
+            const float v = __fadd_rn(__ldg(tail + nbins + jt), __ldg(head + nbins + jh));
+            dst[j] = normalise(e, v);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nhere) {
+        const uint64_t c = c0 + threadIdx.x;
+        const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1;
+        score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, 1.0f, sp, mode,
+                      scores + c * nout);
     }
 }
 
 // Profiles per block so that the staged rows fit comfortably in shared memory.
-uint32_t profiles_per_block(uint32_t rs, size_t extra_per_profile) {
-    const size_t per = static_cast<size_t>(rs) * sizeof(float) + extra_per_profile;
+uint32_t profiles_per_block(uint32_t rs) {
+    const size_t per = static_cast<size_t>(rs) * sizeof(float);
     uint32_t T = 128;
-    while (T > 32 && T * per > 100 * 1024) {
+    while (T > 32 && T * per > 48 * 1024) {
         T -= 32;
     }
     if (T * per > 200 * 1024) {
@@ -228,36 +203,55 @@ void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d
     if (nprof == 0) {
         return;
     }
-    const uint32_t rs = row_stride(nbins, is3d, sp.wmax);
-    const uint32_t T = profiles_per_block(rs, 0);
+    const uint32_t rs = row_stride(nbins, sp.wmax);
+    const uint32_t T = profiles_per_block(rs);
     const size_t smem = static_cast<size_t>(T) * rs * sizeof(float);
-    set_smem(score_kernel, smem);
-    const auto blocks = static_cast<unsigned>((nprof + T - 1) / T);
-    score_kernel<<<blocks, T, smem, s>>>(d_folds, nprof, nbins, is3d, inv_stdnoise, rs, sp, mode,
-                                         d_scores);
+    const uint64_t blocks = (nprof + T - 1) / T;
+    require(blocks <= 0x7fffffffULL, "too many profiles");
+    auto launch = [&](auto kern) {
+        set_smem(kern, smem);
+        kern<<<static_cast<unsigned>(blocks), T, smem, s>>>(d_folds, nprof, nbins, is3d,
+                                                            inv_stdnoise, rs, sp, mode, d_scores);
+    };
+    if (sp.nwidths <= 8) {
+        launch(score_kernel<8>);
+    } else if (sp.nwidths <= 16) {
+        launch(score_kernel<16>);
+    } else {
+        launch(score_kernel<32>);
+    }
     LK_CUDA(cudaGetLastError());
 }
 
-void merge_score_level(const float* d_in, const void* d_coords, bool taylor,
-                       uint64_t ncoords_cur, uint64_t ncoords_prev, uint32_t nbins,
+void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
+                       uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                        const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s) {
-    if (ncoords_cur == 0) {
+    if (n_inner == 0 || n_outer == 0) {
         return;
     }
-    const uint32_t rs = row_stride(nbins, true, sp.wmax);
-    const uint32_t T = profiles_per_block(rs, 4 * sizeof(uint32_t));
-    const size_t smem = static_cast<size_t>(T) * (rs * sizeof(float) + 4 * sizeof(uint32_t));
-    const auto blocks = static_cast<unsigned>((ncoords_cur + T - 1) / T);
+    const uint32_t rs = row_stride(nbins, sp.wmax);
+    const uint32_t T = profiles_per_block(rs);
+    const size_t smem = static_cast<size_t>(T) * rs * sizeof(float);
+    const uint64_t tiles = (n_inner + T - 1) / T;
+    require(tiles * n_outer <= 0x7fffffffULL && n_inner <= 0xffffffffULL,
+            "final level too large for the launch grid");
+    const auto blocks = static_cast<unsigned>(tiles * n_outer);
+    const auto ni = static_cast<uint32_t>(n_inner);
+    const auto no = static_cast<uint32_t>(n_outer);
+    auto launch = [&](auto kern) {
+        set_smem(kern, smem);
+        kern<<<blocks, T, smem, s>>>(d_in, d_coords, ni, no, ncoords_prev, nbins, rs, sp, mode,
+                                     d_scores);
+    };
+    const int nwb = sp.nwidths <= 8 ? 8 : (sp.nwidths <= 16 ? 16 : 32);
     if (taylor) {
-        set_smem(merge_score_kernel<true>, smem);
-        merge_score_kernel<true><<<blocks, T, smem, s>>>(d_in, d_coords, ncoords_cur,
-                                                         ncoords_prev, nbins, rs, sp, mode,
-                                                         d_scores);
+        if (nwb == 8) launch(merge_score_kernel<true, 8>);
+        else if (nwb == 16) launch(merge_score_kernel<true, 16>);
+        else launch(merge_score_kernel<true, 32>);
     } else {
-        set_smem(merge_score_kernel<false>, smem);
-        merge_score_kernel<false><<<blocks, T, smem, s>>>(d_in, d_coords, ncoords_cur,
-                                                          ncoords_prev, nbins, rs, sp, mode,
-                                                          d_scores);
+        if (nwb == 8) launch(merge_score_kernel<false, 8>);
+        else if (nwb == 16) launch(merge_score_kernel<false, 16>);
+        else launch(merge_score_kernel<false, 32>);
     }
     LK_CUDA(cudaGetLastError());
 }
