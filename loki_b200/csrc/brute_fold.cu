@@ -343,20 +343,17 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// Segments per lane: 4 when the segment count fills 128-segment tiles, else
-// 2 for 64, else 1. LOKI_B200_BF_SPL (1, 2 or 4) overrides it for tuning.
-uint32_t choose_spl(uint64_t nseg) {
+// Segments per lane. One segment per lane measured fastest on B200 for the
+// 2^22-sample, 256-segment, 64-bin accelerated workload (3.96 ms against 4.04
+// for two and 4.85 for four): more segments per lane lengthen each run's
+// shared-memory read-modify-write without saving decode work.
+// LOKI_B200_BF_SPL (1, 2 or 4) overrides it for tuning.
+uint32_t choose_spl(uint64_t /*nseg*/) {
     if (const char* env = std::getenv("LOKI_B200_BF_SPL")) {
         const int v = std::atoi(env);
         if (v == 1 || v == 2 || v == 4) {
             return static_cast<uint32_t>(v);
         }
-    }
-    if (nseg % 128 == 0) {
-        return 4;
-    }
-    if (nseg % 64 == 0) {
-        return 2;
     }
     return 1;
 }
@@ -395,11 +392,12 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
     // Consumer warps per block: as many (frequency, row) accumulators as fit
     // next to the stage ring.
     const size_t stages = kStages * 2 * m_chunk * sw * sizeof(float) + 2 * kStages * sizeof(uint64_t);
-    // Rows per warp: both (E and V share the run decoding) unless the
-    // accumulators of two rows do not fit; LOKI_B200_BF_ROWS=1 forces one.
-    m_rows = 2;
+    // Rows per warp: one (E and V of a frequency on two warps of one block,
+    // 3.96 ms against 4.15 ms for both rows on one warp on the workload
+    // above), or two when LOKI_B200_BF_ROWS=2 asks and the accumulators fit.
+    m_rows = 1;
     if (const char* env = std::getenv("LOKI_B200_BF_ROWS")) {
-        m_rows = std::atoi(env) == 1 ? 1 : 2;
+        m_rows = std::atoi(env) == 2 ? 2 : 1;
     }
     if (stages + 2 * static_cast<size_t>(m_nbins) * sw * sizeof(float) > kSmemLimit) {
         m_rows = 1;
