@@ -93,7 +93,12 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            # Wait (up to 5 s) for the first sample, so that the timed region
+            # that follows is covered by samples.
+            t_end = time.time() + 5.0
+            while time.time() < t_end and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except (OSError, FileNotFoundError):
             self.proc = None
 
@@ -308,6 +313,20 @@ def run_ours(args, rank, world, local_rank):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic(dom),
                 "algorithmic_bytes": stage_bytes[dom], "avg_ms": dom_ms}
+    if dom == "brute_fold_l0":
+        # The brute fold moves little HBM data; its floor is one 4-byte
+        # shared-memory read per (sample, level-0 frequency, row) from the
+        # staged series tile. Peak: 128 B/clock/SM x SMs x max SM clock.
+        nfreq0 = int(ffa.plan.param_counts[0][-1])
+        smem_bytes = 4 * 2 * params["nsamps"] * nfreq0
+        props = torch.cuda.get_device_properties(local_rank)
+        mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+        smem_peak = 128 * props.multi_processor_count * mhz * 1e6 / 1e9
+        smem_ach = smem_bytes / (dom_ms / 1e3) / 1e9
+        roofline["shared_memory"] = {
+            "achieved": smem_ach, "peak": smem_peak, "unit": "GB/s", "frac": smem_ach / smem_peak,
+            "peak_source": "nominal 128 B/clock/SM at the max SM clock",
+            "algorithmic_bytes": smem_bytes, "adds": 2 * params["nsamps"] * nfreq0}
     stages = {k: {"avg_ms": stage_ms[k] / args.steps, "bytes": stage_bytes[k],
                   "gbs": stage_bytes[k] / (stage_ms[k] / args.steps / 1e3) / 1e9}
               for k in sorted(stage_ms, key=stage_ms.get, reverse=True)}
