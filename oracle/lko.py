@@ -104,6 +104,17 @@ def lib() -> ctypes.CDLL:
         L.lko_circular_prefix_sum.argtypes = [vp, vp, u64, u64]
         L.lko_compact.restype = u64
         L.lko_compact.argtypes = [vp, u64, f32, vp, vp]
+        L.lko_middle_out.argtypes = [u64, u64, f64, u64, vp]
+        L.lko_taylor_seed.restype = u64
+        L.lko_taylor_seed.argtypes = [vp, vp]
+        L.lko_taylor_branch.argtypes = [vp, u64, u32, f64, f64, u64, f64, u64, vp, vp, u64, vp]
+        L.lko_taylor_resolve.argtypes = [vp, vp, u64, vp, vp, vp]
+        L.lko_taylor_transform.argtypes = [vp, vp, u64, u32, f64, f64, ctypes.c_int]
+        L.lko_shift_add_batch.argtypes = [vp, vp, vp, vp, vp, vp, u64, u64, u64, u64]
+        L.lko_score_filter.restype = u64
+        L.lko_score_filter.argtypes = [vp, u64, u64, vp, u64, f32, vp, vp]
+        L.lko_prune_run.argtypes = [vp, ctypes.c_int, vp, vp, u64, u64, u64, u64, u64, u64, vp, vp,
+                                    vp, vp, vp, u64, vp]
         _lib = L
     return _lib
 
@@ -334,3 +345,107 @@ def nearest_idx(val, vmin, vmax, count) -> int:
 
 def param_val_at_idx(vmin, vmax, count, i) -> float:
     return lib().lko_param_val_at_idx(vmin, vmax, count, i)
+
+
+# ---- pruning leaf step ----------------------------------------------------------
+
+PRUNE_STATS_DTYPE = np.dtype([
+    ("level", np.uint64), ("seg_idx", np.uint64), ("n_branches", np.uint64), ("n_leaves", np.uint64),
+    ("n_leaves_phy", np.uint64), ("n_leaves_surv", np.uint64), ("threshold", np.float32),
+    ("score_min", np.float32), ("score_max", np.float32), ("pad", np.float32)])
+
+
+def middle_out(nsegments, ref_idx, tsegment, level):
+    """(seg_idx, coord, current_coord, segment_coord) of MiddleOutScheme at a level."""
+    out = np.zeros(7, np.float64)
+    _check(lib().lko_middle_out(nsegments, ref_idx, tsegment, level, _p(out)))
+    return int(out[0]), (out[1], out[2]), (out[3], out[4]), (out[5], out[6])
+
+
+def taylor_seed(plan: OraclePlan) -> np.ndarray:
+    np_ = plan.nparams
+    n = int(plan.ncoords[-1])
+    out = np.zeros((n, np_ + 2, 2), np.float64)
+    k = lib().lko_taylor_seed(ctypes.byref(plan.raw), _p(out))
+    if k != n:
+        raise RuntimeError(lib().lko_last_error().decode())
+    return out
+
+
+def taylor_branch(leaves, nparams, coord_cur, nbins, eta, branch_max, cap=None):
+    leaves = np.ascontiguousarray(leaves, np.float64)
+    stride = (nparams + 2) * 2
+    n = leaves.size // stride
+    cap = n * branch_max if cap is None else cap
+    out = np.zeros(cap * stride, np.float64)
+    org = np.zeros(cap, np.uint64)
+    nout = u64()
+    rc = lib().lko_taylor_branch(_p(leaves), n, nparams, coord_cur[0], coord_cur[1], nbins, eta, branch_max,
+                                 _p(out), _p(org), cap, ctypes.byref(nout))
+    if rc == 2:
+        return taylor_branch(leaves, nparams, coord_cur, nbins, eta, branch_max, cap=nout.value)
+    _check(rc)
+    k = nout.value
+    return out[: k * stride].reshape(k, nparams + 2, 2), org[:k]
+
+
+def taylor_resolve(plan: OraclePlan, leaves, coord_add, coord_cur, coord_init):
+    leaves = np.ascontiguousarray(leaves, np.float64)
+    n = leaves.size // ((plan.nparams + 2) * 2)
+    coords = np.array([*coord_add, *coord_cur, *coord_init], np.float64)
+    idx = np.zeros(n, np.uint64)
+    sh = np.zeros(n, np.float32)
+    lib().lko_taylor_resolve(ctypes.byref(plan.raw), _p(leaves), n, _p(coords), _p(idx), _p(sh))
+    return idx, sh
+
+
+def taylor_transform(leaves, indices, nparams, coord_next, coord_cur, conservative=False):
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    idx = np.ascontiguousarray(indices, np.uint64)
+    lib().lko_taylor_transform(_p(out), _p(idx), idx.size, nparams, coord_next[0], coord_cur[0],
+                               int(conservative))
+    return out
+
+
+def shift_add_batch(folds_tree, indices_tree, folds_ffa, indices_ffa, phase_shift, nbins,
+                    physical_start_idx, capacity):
+    ft = np.ascontiguousarray(folds_tree, np.float32)
+    it = np.ascontiguousarray(indices_tree, np.uint64)
+    ff = np.ascontiguousarray(folds_ffa, np.float32)
+    iff = np.ascontiguousarray(indices_ffa, np.uint64)
+    ps = np.ascontiguousarray(phase_shift, np.float32)
+    out = np.zeros((it.size, 2, nbins), np.float32)
+    lib().lko_shift_add_batch(_p(ft), _p(it), _p(ff), _p(iff), _p(ps), _p(out), nbins, it.size,
+                              physical_start_idx, capacity)
+    return out
+
+
+def score_filter(folds, nbins, widths, threshold):
+    folds = np.ascontiguousarray(folds, np.float32)
+    w = np.ascontiguousarray(widths, np.uint64)
+    n = folds.size // (2 * nbins)
+    scores = np.zeros(n, np.float32)
+    idx = np.zeros(n, np.uint64)
+    k = lib().lko_score_filter(_p(folds), n, nbins, _p(w), w.size, threshold, _p(scores), _p(idx))
+    return scores, idx[:k]
+
+
+def prune_run(plan: OraclePlan, ffa_fold, thresholds, ref_seg, max_sugg, batch_size, branch_max,
+              n_iters, conservative=False):
+    """One pruning run: returns (stats, leaves, folds, scores) of the final tree."""
+    ffa = np.ascontiguousarray(ffa_fold, np.float32).ravel()
+    thr = np.ascontiguousarray(thresholds, np.float32)
+    nbins = plan.nbins
+    stats = np.zeros(n_iters + 1, PRUNE_STATS_DTYPE)
+    nstats = u64()
+    stride = (plan.nparams + 2) * 2
+    leaves = np.zeros(max_sugg * stride, np.float64)
+    folds = np.zeros(max_sugg * 2 * nbins, np.float32)
+    scores = np.zeros(max_sugg, np.float32)
+    n = u64()
+    _check(lib().lko_prune_run(ctypes.byref(plan.raw), int(conservative), _p(ffa), _p(thr), thr.size, ref_seg,
+                               max_sugg, batch_size, branch_max, n_iters, _p(stats), ctypes.byref(nstats),
+                               _p(leaves), _p(folds), _p(scores), max_sugg, ctypes.byref(n)))
+    k = n.value
+    return (stats[: nstats.value], leaves[: k * stride].reshape(k, plan.nparams + 2, 2),
+            folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k])

@@ -661,3 +661,734 @@ uint64_t lko_compact(const float* scores, uint64_t n, float snr_min, uint32_t* i
     }
     return k;
 }
+
+/* ======================================================================== */
+/* Pruning leaf step (Taylor basis).                                         */
+/* ======================================================================== */
+
+/* utils::kZeroEps (lib/loki/utils.hpp:15). */
+static const double kZeroEps = 1e-12;
+
+/* MiddleOutScheme order: np.argsort(|arange(nseg) - ref|, kind="stable")
+ * (lib/loki/psr_utils.hpp:331-347): ref, then ref-1, ref+1, ref-2, ... with
+ * the lower index first on equal distance. */
+static void middle_out_order(uint64_t nseg, uint64_t ref, uint64_t* order) {
+    uint64_t k = 0;
+    order[k++] = ref;
+    for (uint64_t d = 1; k < nseg; ++d) {
+        if (d <= ref) {
+            order[k++] = ref - d;
+        }
+        if (ref + d < nseg && k < nseg) {
+            order[k++] = ref + d;
+        }
+    }
+}
+
+/* get_coord (lib/loki/psr_utils.hpp:378-393). */
+static void mo_coord(const uint64_t* order, uint64_t level, double tseg, double* ref,
+                     double* scale) {
+    uint64_t mn = order[0], mx = order[0];
+    for (uint64_t i = 1; i <= level; ++i) {
+        mn = order[i] < mn ? order[i] : mn;
+        mx = order[i] > mx ? order[i] : mx;
+    }
+    const double min_val = (double)mn;
+    const double max_val = (double)mx;
+    const double ref_val = (min_val + max_val + 1.0) / 2.0;
+    const double scale_val = ref_val - min_val;
+    *ref = ref_val * tseg;
+    *scale = scale_val * tseg;
+}
+
+/* get_current_coord (lib/loki/psr_utils.hpp:440-448). */
+static void mo_current_coord(const uint64_t* order, uint64_t level, double tseg, double* ref,
+                             double* scale) {
+    if (level == 0) {
+        mo_coord(order, 0, tseg, ref, scale);
+        return;
+    }
+    double pr, ps, cr, cs;
+    mo_coord(order, level - 1, tseg, &pr, &ps);
+    mo_coord(order, level, tseg, &cr, &cs);
+    *ref = pr;
+    *scale = cs;
+}
+
+/* get_segment_coord (lib/loki/psr_utils.hpp:402-408). */
+static void mo_segment_coord(const uint64_t* order, uint64_t level, double tseg, double* ref,
+                             double* scale) {
+    const double idx = (double)order[level];
+    *ref = (idx + 0.5) * tseg;
+    *scale = 0.5 * tseg;
+}
+
+int lko_middle_out(uint64_t nseg, uint64_t ref_idx, double tseg, uint64_t level, double* out) {
+    if (nseg == 0 || ref_idx >= nseg || level >= nseg) {
+        return fail("MiddleOutScheme: invalid nsegments / ref_idx / level");
+    }
+    uint64_t* order = (uint64_t*)malloc(sizeof(uint64_t) * nseg);
+    middle_out_order(nseg, ref_idx, order);
+    out[0] = (double)order[level];
+    mo_coord(order, level, tseg, &out[1], &out[2]);
+    mo_current_coord(order, level, tseg, &out[3], &out[4]);
+    mo_segment_coord(order, level, tseg, &out[5], &out[6]);
+    free(order);
+    return 0;
+}
+
+/* FFAPlan::get_dparams_actual of a level (lib/configs.cpp:164-174). */
+static double dparam_actual(const lko_plan* p, uint32_t l, uint32_t i) {
+    return (p->limits[2 * i + 1] - p->limits[2 * i]) / (double)p->param_counts[l][i];
+}
+
+/* core::poly_taylor_seed (lib/taylor.cpp:1197-1257). */
+uint64_t lko_taylor_seed(const lko_plan* p, double* leaves) {
+    const uint32_t np = p->nparams;
+    const uint32_t L = p->n_levels - 1;
+    if (np < 2 || np > 3) {
+        fail("pruning supports nparams 2 or 3");
+        return 0;
+    }
+    const uint64_t stride = (np + 2) * 2;
+    const uint64_t n_accel = p->param_counts[L][np - 2];
+    const uint64_t n_freq = p->param_counts[L][np - 1];
+    if (p->ncoords[L] != n_accel * n_freq) {
+        fail("n_leaves mismatch");
+        return 0;
+    }
+    const double a_min = p->limits[2 * (np - 2)], a_max = p->limits[2 * (np - 2) + 1];
+    const double f_min = p->limits[2 * (np - 1)], f_max = p->limits[2 * (np - 1) + 1];
+    const double d_freq_cur = dparam_actual(p, L, np - 1);
+    uint64_t leaf = 0;
+    for (uint64_t ia = 0; ia < n_accel; ++ia) {
+        const double accel_cur = lko_param_val_at_idx(a_min, a_max, n_accel, ia);
+        for (uint64_t jf = 0; jf < n_freq; ++jf) {
+            const double freq_cur = lko_param_val_at_idx(f_min, f_max, n_freq, jf);
+            double* o = leaves + leaf * stride;
+            for (uint32_t j = 0; j + 1 < np; ++j) {
+                o[j * 2 + 0] = 0;
+                o[j * 2 + 1] = dparam_actual(p, L, j);
+            }
+            o[(np - 2) * 2 + 0] = accel_cur;
+            o[(np - 1) * 2 + 0] = 0;
+            o[(np - 1) * 2 + 1] = d_freq_cur * (kCval / freq_cur);
+            o[np * 2 + 0] = 0;
+            o[np * 2 + 1] = 0;
+            o[(np + 1) * 2 + 0] = freq_cur;
+            o[(np + 1) * 2 + 1] = 0;
+            ++leaf;
+        }
+    }
+    return leaf;
+}
+
+/* Steps and shifts of one parent (lib/taylor.cpp:64-85 accel, 199-227 jerk):
+ * param p holds derivative order k = np - p; K = 1, 4, 24 for k = 1, 2, 3. */
+static void branch_steps(const double* lf, uint32_t np, double dt, double nbins_d, double dphi,
+                         double* sig_new, double* shift) {
+    const double dt2 = dt * dt;
+    const double inv_dt = 1.0 / dt;
+    const double inv_dt2 = inv_dt * inv_dt;
+    const double f0 = lf[(np + 1) * 2];
+    const double dfactor = kCval / f0;
+    if (np == 2) {
+        const double d2_sig_cur = lf[1], d1_sig_cur = lf[3];
+        sig_new[0] = dphi * dfactor * 4.0 * inv_dt2;
+        sig_new[1] = dphi * dfactor * 1.0 * inv_dt;
+        shift[0] = fabs(d2_sig_cur - sig_new[0]) * dt2 * nbins_d / (4.0 * dfactor);
+        shift[1] = fabs(d1_sig_cur - sig_new[1]) * dt * nbins_d / (1.0 * dfactor);
+    } else {
+        const double dt3 = dt2 * dt;
+        const double inv_dt3 = inv_dt2 * inv_dt;
+        const double d3_sig_cur = lf[1], d2_sig_cur = lf[3], d1_sig_cur = lf[5];
+        sig_new[0] = dphi * dfactor * 24.0 * inv_dt3;
+        sig_new[1] = dphi * dfactor * 4.0 * inv_dt2;
+        sig_new[2] = dphi * dfactor * 1.0 * inv_dt;
+        shift[0] = fabs(d3_sig_cur - sig_new[0]) * dt3 * nbins_d / (24.0 * dfactor);
+        shift[1] = fabs(d2_sig_cur - sig_new[1]) * dt2 * nbins_d / (4.0 * dfactor);
+        shift[2] = fabs(d1_sig_cur - sig_new[2]) * dt * nbins_d / (1.0 * dfactor);
+    }
+}
+
+/* psr_utils::branch_one_param_padded + branch_param_padded
+ * (lib/loki/psr_utils.hpp:189-211, lib/psr_utils.cpp:226-259): the count of
+ * child values of one parameter, and (when vals != NULL) the values. */
+static int branch_one(double cur, double sig_cur, double sig_new, double shift, double eta,
+                      uint64_t branch_max, double* vals, double* dparam, uint64_t* count) {
+    if (!(shift >= (eta - kFloatEps))) {
+        if (vals != NULL) {
+            vals[0] = cur;
+        }
+        *dparam = sig_cur;
+        *count = 1;
+        return 0;
+    }
+    if (sig_cur <= kZeroEps || sig_new <= kZeroEps) {
+        return fail("Both dparam_cur and dparam_new must be positive (got %g, %g)", sig_cur,
+                    sig_new);
+    }
+    const double ratio = sig_cur / sig_new;
+    const double c = ceil(ratio - kFloatEps);
+    const uint64_t num = c < 1.0 ? 1 : (uint64_t)c;
+    if (num > branch_max) {
+        return fail("num_points must be less than or equal to branch_max");
+    }
+    const double act = sig_cur / (double)num;
+    const double parent_min = cur - (sig_cur / 2.0);
+    const double first = parent_min + (act / 2.0);
+    if (vals != NULL) {
+        for (uint64_t i = 0; i < num; ++i) {
+            vals[i] = first + ((double)i * act);
+        }
+    }
+    *dparam = act;
+    *count = num;
+    return 0;
+}
+
+int lko_taylor_branch(const double* leaves, uint64_t n, uint32_t np, double t_cur,
+                      double scale_cur, uint64_t nbins, double eta, uint64_t branch_max,
+                      double* out, uint64_t* origins, uint64_t cap_out, uint64_t* n_out) {
+    (void)t_cur;
+    if (np < 2 || np > 3) {
+        return fail("pruning supports nparams 2 or 3");
+    }
+    const uint64_t stride = (np + 2) * 2;
+    const double dt = scale_cur; /* t_obs_minus_t_ref */
+    const double nbins_d = (double)nbins;
+    const double dphi = eta / nbins_d;
+    /* Pass 1: children counts. */
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double* lf = leaves + i * stride;
+        double sig_new[3], shift[3], dp;
+        branch_steps(lf, np, dt, nbins_d, dphi, sig_new, shift);
+        uint64_t prod = 1;
+        for (uint32_t k = 0; k < np; ++k) {
+            uint64_t cnt;
+            if (branch_one(lf[2 * k], lf[2 * k + 1], sig_new[k], shift[k], eta, branch_max, NULL,
+                           &dp, &cnt) != 0) {
+                return 1;
+            }
+            prod *= cnt;
+        }
+        total += prod;
+    }
+    *n_out = total;
+    if (total > cap_out) {
+        return 2;
+    }
+    /* Pass 2: Cartesian product, highest derivative outermost. */
+    double* vals = (double*)malloc(sizeof(double) * 3 * (branch_max > 0 ? branch_max : 1));
+    uint64_t o = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double* lf = leaves + i * stride;
+        double sig_new[3], shift[3], dp[3];
+        uint64_t cnt[3] = {1, 1, 1};
+        branch_steps(lf, np, dt, nbins_d, dphi, sig_new, shift);
+        for (uint32_t k = 0; k < np; ++k) {
+            branch_one(lf[2 * k], lf[2 * k + 1], sig_new[k], shift[k], eta, branch_max,
+                       vals + k * branch_max, &dp[k], &cnt[k]);
+        }
+        for (uint64_t a = 0; a < cnt[0]; ++a) {
+            for (uint64_t b = 0; b < cnt[1]; ++b) {
+                for (uint64_t c = 0; c < (np == 3 ? cnt[2] : 1); ++c) {
+                    double* d = out + o * stride;
+                    d[0] = vals[a];
+                    d[1] = dp[0];
+                    d[2] = vals[branch_max + b];
+                    d[3] = dp[1];
+                    if (np == 3) {
+                        d[4] = vals[2 * branch_max + c];
+                        d[5] = dp[2];
+                    }
+                    memcpy(d + 2 * np, lf + 2 * np, 4 * sizeof(double));
+                    origins[o] = i;
+                    ++o;
+                }
+            }
+        }
+    }
+    free(vals);
+    return 0;
+}
+
+/* poly_taylor_resolve_accel_batch / _jerk_batch (lib/taylor.cpp:492-619). */
+void lko_taylor_resolve(const lko_plan* p, const double* leaves, uint64_t n, const double* co,
+                        uint64_t* param_idx, float* phase_shift) {
+    const uint32_t np = p->nparams;
+    const uint32_t L = p->n_levels - 1;
+    const uint64_t stride = (np + 2) * 2;
+    const uint64_t n_accel = p->param_counts[L][np - 2];
+    const uint64_t n_freq = p->param_counts[L][np - 1];
+    const double a_min = p->limits[2 * (np - 2)], a_max = p->limits[2 * (np - 2) + 1];
+    const double f_min = p->limits[2 * (np - 1)], f_max = p->limits[2 * (np - 1) + 1];
+    const double t0_add = co[0], t0_cur = co[2], t0_init = co[4];
+    const double dt_add = t0_add - t0_cur;
+    const double dt_init = t0_init - t0_cur;
+    if (np == 2) {
+        const double dt = dt_add - dt_init;
+        const double half_dt2 = 0.5 * ((dt_add * dt_add) - (dt_init * dt_init));
+        for (uint64_t i = 0; i < n; ++i) {
+            const double* lf = leaves + i * stride;
+            const double a_cur = lf[0], v_cur = lf[2], f0 = lf[6];
+            const double a_new = a_cur;
+            const double delta_v = a_cur * dt;
+            const double delta_d = (v_cur * dt) + (a_cur * half_dt2);
+            const double f_new = f0 * (1.0 - (delta_v * kInvCval));
+            const double delay_rel = delta_d * kInvCval;
+            const uint64_t ia = lko_nearest_idx(a_new, a_min, a_max, n_accel);
+            const uint64_t jf = lko_nearest_idx(f_new, f_min, f_max, n_freq);
+            param_idx[i] = (ia * n_freq) + jf;
+            phase_shift[i] = lko_phase_idx(dt, f0, p->nbins, delay_rel);
+        }
+    } else {
+        const double half_dt2_add = 0.5 * (dt_add * dt_add);
+        const double half_dt2_init = 0.5 * (dt_init * dt_init);
+        const double dt = dt_add - dt_init;
+        const double half_dt2 = half_dt2_add - half_dt2_init;
+        const double sixth_dt3 = ((half_dt2_add * dt_add) - (half_dt2_init * dt_init)) / 3.0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double* lf = leaves + i * stride;
+            const double j_cur = lf[0], a_cur = lf[2], v_cur = lf[4], f0 = lf[8];
+            const double a_new = a_cur + (j_cur * dt_add);
+            const double delta_v = (a_cur * dt) + (j_cur * half_dt2);
+            const double delta_d = (v_cur * dt) + (a_cur * half_dt2) + (j_cur * sixth_dt3);
+            const double f_new = f0 * (1.0 - (delta_v * kInvCval));
+            const double delay_rel = delta_d * kInvCval;
+            phase_shift[i] = lko_phase_idx(dt, f0, p->nbins, delay_rel);
+            const uint64_t ia = lko_nearest_idx(a_new, a_min, a_max, n_accel);
+            const uint64_t jf = lko_nearest_idx(f_new, f_min, f_max, n_freq);
+            param_idx[i] = (ia * n_freq) + jf;
+        }
+    }
+}
+
+/* poly_taylor_transform_{accel,jerk}_batch (lib/taylor.cpp:881-1005). */
+void lko_taylor_transform(double* leaves, const uint64_t* indices, uint64_t n, uint32_t np,
+                          double t_next, double t_cur, int conservative) {
+    const uint64_t stride = (np + 2) * 2;
+    const double dt = t_next - t_cur;
+    if (np == 2) {
+        const double half_dt2 = 0.5 * (dt * dt);
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + indices[i] * stride;
+            const double d2v = lf[0], d2e = lf[1], d1v = lf[2], d1e = lf[3], d0v = lf[4],
+                         d0e = lf[5];
+            const double d2v_j = d2v;
+            const double d1v_j = d1v + (d2v * dt);
+            const double d0v_j = d0v + (d1v * dt) + (d2v * half_dt2);
+            double d2e_j, d1e_j;
+            if (conservative) {
+                d2e_j = d2e;
+                d1e_j = sqrt((d1e * d1e) + (d2e * d2e * dt * dt));
+            } else {
+                d2e_j = d2e;
+                d1e_j = d1e;
+            }
+            lf[0] = d2v_j;
+            lf[1] = d2e_j;
+            lf[2] = d1v_j;
+            lf[3] = d1e_j;
+            lf[4] = d0v_j;
+            lf[5] = d0e;
+        }
+    } else {
+        const double dt2 = dt * dt;
+        const double half_dt2 = 0.5 * (dt2);
+        const double sixth_dt3 = dt2 * dt / 6.0;
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + indices[i] * stride;
+            const double d3v = lf[0], d3e = lf[1], d2v = lf[2], d2e = lf[3], d1v = lf[4],
+                         d1e = lf[5], d0v = lf[6], d0e = lf[7];
+            const double d3v_j = d3v;
+            const double d2v_j = d2v + (d3v * dt);
+            const double d1v_j = d1v + (d2v * dt) + (d3v * half_dt2);
+            const double d0v_j = d0v + (d1v * dt) + (d2v * half_dt2) + (d3v * sixth_dt3);
+            double d3e_j, d2e_j, d1e_j;
+            if (conservative) {
+                d3e_j = d3e;
+                d2e_j = sqrt((d2e * d2e) + (d3e * d3e * dt2));
+                d1e_j = sqrt((d1e * d1e) + (d2e * d2e * dt2) +
+                             (d3e * d3e * half_dt2 * half_dt2));
+            } else {
+                d3e_j = d3e;
+                d2e_j = d2e;
+                d1e_j = d1e;
+            }
+            lf[0] = d3v_j;
+            lf[1] = d3e_j;
+            lf[2] = d2v_j;
+            lf[3] = d2e_j;
+            lf[4] = d1v_j;
+            lf[5] = d1e_j;
+            lf[6] = d0v_j;
+            lf[7] = d0e;
+        }
+    }
+}
+
+/* kernels::shift_add_linear_batch + shift_add_linear_with_buffer
+ * (lib/kernels.cpp:118-146,1328-1355): tree fold unshifted, FFA fold rotated
+ * right by round(shift). The tree index is formed in 32 bits as there. */
+void lko_shift_add_batch(const float* folds_tree, const uint64_t* indices_tree,
+                         const float* folds_ffa, const uint64_t* indices_ffa,
+                         const float* phase_shift, float* folds_out, uint64_t nbins,
+                         uint64_t n_leaves, uint64_t physical_start_idx, uint64_t capacity) {
+    const uint64_t fs = 2 * nbins;
+    for (uint64_t i = 0; i < n_leaves; ++i) {
+        const uint32_t logical = (uint32_t)(indices_tree[i] + physical_start_idx);
+        const uint32_t phys = logical < capacity ? logical : (uint32_t)(logical - capacity);
+        const float* tail = folds_tree + (uint64_t)phys * fs;
+        const float* head = folds_ffa + indices_ffa[i] * fs;
+        float* o = folds_out + i * fs;
+        const uint64_t s = shift_bins(phase_shift[i], nbins);
+        for (uint64_t r = 0; r < 2; ++r) {
+            for (uint64_t j = 0; j < nbins; ++j) {
+                const uint64_t src = (j + nbins - s) % nbins;
+                o[r * nbins + j] = tail[r * nbins + j] + head[r * nbins + src];
+            }
+        }
+    }
+}
+
+uint64_t lko_score_filter(const float* folds, uint64_t n, uint64_t nbins, const uint64_t* widths,
+                          uint64_t nwidths, float threshold, float* scores, uint64_t* indices) {
+    snr_boxcar(1, 1, folds, n, nbins, widths, nwidths, 1.0F, scores);
+    uint64_t k = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (scores[i] >= threshold) {
+            indices[k++] = i;
+        }
+    }
+    return k;
+}
+
+/* ---- WorldTree (lib/world_tree.cpp) ----------------------------------------- */
+
+typedef struct wtree {
+    uint64_t cap, ls, fs, max_batch;
+    double* leaves;
+    float* folds;
+    float* scores;
+    float* scratch;    /* cap + max_batch */
+    uint64_t* pending; /* max_batch */
+    uint64_t head, size, size_old, write_head, write_start, read_consumed;
+    int updating;
+} wtree;
+
+static uint64_t wt_circ(uint64_t logical, uint64_t start, uint64_t cap) {
+    return (start + logical) % cap;
+}
+
+static uint64_t wt_space_left(const wtree* t) {
+    const int64_t remaining_old = (int64_t)t->size_old - (int64_t)t->read_consumed;
+    const int64_t space = (int64_t)t->cap - (remaining_old + (int64_t)t->size);
+    return space < 0 ? 0 : (uint64_t)space;
+}
+
+static uint64_t wt_start(const wtree* t) { return t->updating ? t->write_start : t->head; }
+
+/* prepare_in_place_update / finalize_in_place_update / consume_read
+ * (lib/world_tree.cpp:237-274). */
+static void wt_prepare(wtree* t) {
+    t->size_old = t->size;
+    t->write_start = wt_circ(t->size, t->head, t->cap);
+    t->write_head = t->write_start;
+    t->size = 0;
+    t->updating = 1;
+    t->read_consumed = 0;
+}
+
+static void wt_finalize(wtree* t) {
+    t->head = t->write_start;
+    t->size_old = 0;
+    t->updating = 0;
+    t->read_consumed = 0;
+    t->write_head = 0;
+    t->write_start = 0;
+}
+
+/* scatter_to_circular_copy (lib/world_tree.cpp:503-525). */
+static void wt_scatter(wtree* t, const double* lv, const float* fo, const float* sc,
+                       const uint64_t* idx, uint64_t n) {
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t s = idx[i], d = t->write_head;
+        memcpy(t->leaves + d * t->ls, lv + s * t->ls, t->ls * sizeof(double));
+        memcpy(t->folds + d * t->fs, fo + s * t->fs, t->fs * sizeof(float));
+        t->scores[d] = sc[s];
+        if (++t->write_head == t->cap) {
+            t->write_head = 0;
+        }
+    }
+    t->size += n;
+}
+
+static int cmp_desc(const void* a, const void* b) {
+    const float x = *(const float*)a, y = *(const float*)b;
+    return (x < y) - (x > y);
+}
+
+/* get_prune_threshold (lib/world_tree.cpp:570-618). With D the candidates
+ * sorted in descending order, N of them and K = size + space_left: the
+ * top-k value is D[K-1]; the second nth_element runs on the top K (or the
+ * remaining N-K) in ascending order, which selects D[K-1-N/2] when
+ * N/2 <= K-1 and D[N-1-N/2+K] otherwise. */
+static float wt_prune_threshold(wtree* t, const float* sc, const uint64_t* idx, uint64_t n,
+                                float cur) {
+    if (n == 0) {
+        return cur;
+    }
+    const uint64_t space = wt_space_left(t);
+    const uint64_t N = t->size + n;
+    const uint64_t K = t->size + space;
+    if (N <= K) {
+        return cur;
+    }
+    const uint64_t start = wt_start(t);
+    for (uint64_t i = 0; i < t->size; ++i) {
+        t->scratch[i] = t->scores[wt_circ(i, start, t->cap)];
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        t->scratch[t->size + i] = sc[idx[i]];
+    }
+    qsort(t->scratch, N, sizeof(float), cmp_desc);
+    const float topk = nextafterf(t->scratch[K - 1], FLT_MAX);
+    const uint64_t m = N / 2;
+    const float medv = (m <= K - 1) ? t->scratch[K - 1 - m] : t->scratch[N - 1 - m + K];
+    const float med = nextafterf(medv, FLT_MAX);
+    float eff = cur;
+    eff = (eff < topk) ? topk : eff;
+    eff = (eff < med) ? med : eff;
+    return eff;
+}
+
+/* prune_on_overload (lib/world_tree.cpp:620-669): keep score > threshold. */
+static void wt_prune_on_overload(wtree* t, float thr) {
+    if (t->size == 0) {
+        return;
+    }
+    uint64_t r = wt_start(t), w = r, kept = 0;
+    for (uint64_t i = 0; i < t->size; ++i) {
+        if (t->scores[r] > thr) {
+            if (r != w) {
+                memcpy(t->leaves + w * t->ls, t->leaves + r * t->ls, t->ls * sizeof(double));
+                memcpy(t->folds + w * t->fs, t->folds + r * t->fs, t->fs * sizeof(float));
+                t->scores[w] = t->scores[r];
+            }
+            ++kept;
+            if (++w == t->cap) {
+                w = 0;
+            }
+        }
+        if (++r == t->cap) {
+            r = 0;
+        }
+    }
+    t->size = kept;
+    t->write_head = w;
+}
+
+/* add_batch_scattered (lib/world_tree.cpp:361-422). */
+static float wt_add_batch(wtree* t, const double* lv, const float* fo, const float* sc,
+                          const uint64_t* idx, float cur, uint64_t n) {
+    if (n == 0) {
+        return cur;
+    }
+    uint64_t space = wt_space_left(t);
+    if (n <= space) {
+        wt_scatter(t, lv, fo, sc, idx, n);
+        return cur;
+    }
+    const float eff = wt_prune_threshold(t, sc, idx, n, cur);
+    wt_prune_on_overload(t, eff);
+    uint64_t pending = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (sc[idx[i]] >= eff) {
+            t->pending[pending++] = idx[i];
+        }
+    }
+    space = wt_space_left(t);
+    const uint64_t n_add = pending < space ? pending : space;
+    if (n_add == 0) {
+        return eff;
+    }
+    wt_scatter(t, lv, fo, sc, t->pending, n_add);
+    return eff;
+}
+
+/* PruneImpl::initialize + execute_iteration_batched (lib/prune.cpp:181-226,
+ * 429-620) for the Taylor basis, where validate is the identity
+ * (lib/dynamic.cpp:70-77). */
+int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
+                  const float* thresholds, uint64_t n_thresholds, uint64_t ref_seg,
+                  uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
+                  lko_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
+                  float* folds_out, float* scores_out, uint64_t cap_out, uint64_t* n_out) {
+    const uint32_t np = p->nparams;
+    if (np < 2 || np > 3) {
+        return fail("pruning supports nparams 2 or 3");
+    }
+    const uint32_t L = p->n_levels - 1;
+    const uint64_t nseg = p->nsegments[L];
+    const double tseg = p->tsegments[L];
+    const uint64_t nbins = p->nbins;
+    const uint64_t ncoords = p->ncoords[L];
+    const uint64_t ls = (np + 2) * 2, fs = 2 * nbins;
+    const uint64_t max_branched = batch_size * branch_max;
+    if (ref_seg >= nseg) {
+        return fail("ref_idx must be less than nsegments.");
+    }
+    if (ncoords > max_sugg) {
+        return fail("WorldTree: Suggestions too large to add.");
+    }
+    wtree t;
+    memset(&t, 0, sizeof(t));
+    t.cap = max_sugg;
+    t.ls = ls;
+    t.fs = fs;
+    t.max_batch = max_branched;
+    t.leaves = (double*)calloc(max_sugg * ls, sizeof(double));
+    t.folds = (float*)calloc(max_sugg * fs, sizeof(float));
+    t.scores = (float*)calloc(max_sugg, sizeof(float));
+    t.scratch = (float*)calloc(max_sugg + max_branched, sizeof(float));
+    t.pending = (uint64_t*)calloc(max_branched, sizeof(uint64_t));
+    uint64_t* order = (uint64_t*)malloc(sizeof(uint64_t) * nseg);
+    double* b_leaves = (double*)malloc(sizeof(double) * max_branched * ls);
+    uint64_t* b_org = (uint64_t*)malloc(sizeof(uint64_t) * max_branched);
+    uint64_t* b_pidx = (uint64_t*)malloc(sizeof(uint64_t) * max_branched);
+    float* b_shift = (float*)malloc(sizeof(float) * max_branched);
+    float* b_folds = (float*)malloc(sizeof(float) * max_branched * fs);
+    float* b_scores = (float*)malloc(sizeof(float) * max_branched);
+    uint64_t* b_idx = (uint64_t*)malloc(sizeof(uint64_t) * max_branched);
+    int rc = 0;
+    middle_out_order(nseg, ref_seg, order);
+
+    /* initialize: seed leaves, seed scores, add_initial */
+    const float* seg0 = ffa_fold + order[0] * ncoords * fs;
+    if (lko_taylor_seed(p, t.leaves) != ncoords) {
+        rc = 1;
+        goto done;
+    }
+    memcpy(t.folds, seg0, ncoords * fs * sizeof(float));
+    lko_snr_boxcar_3d_max(seg0, ncoords, nbins, p->widths, p->n_widths, t.scores);
+    t.size = ncoords;
+    uint64_t ns = 0;
+    {
+        float mn = t.scores[0], mx = t.scores[0];
+        for (uint64_t i = 1; i < ncoords; ++i) {
+            mn = (t.scores[i] < mn) ? t.scores[i] : mn;
+            mx = (mx < t.scores[i]) ? t.scores[i] : mx;
+        }
+        if (ncoords == 0) {
+            mn = mx = 0.0F;
+        }
+        lko_prune_stats s0 = {0, order[0], ncoords, ncoords, ncoords, ncoords, 0.0F, mn, mx, 0};
+        stats[ns++] = s0;
+    }
+
+    const uint64_t levels = (nseg - 1) < n_iters ? (nseg - 1) : n_iters;
+    for (uint64_t level = 1; level <= levels; ++level) {
+        if (level > n_thresholds) {
+            rc = fail("Pruning complete - exceeded threshold scheme length");
+            goto done;
+        }
+        wt_prepare(&t);
+        const uint64_t seg_idx = order[level];
+        const float threshold = thresholds[level - 1];
+        const uint64_t n_branches = t.size_old;
+        uint64_t n_leaves = 0, n_phy = 0;
+        float smin = FLT_MAX, smax = -FLT_MAX;
+        double ci[2], cn[2], cc[2], ca[2];
+        mo_coord(order, 0, tseg, &ci[0], &ci[1]);
+        mo_coord(order, level, tseg, &cn[0], &cn[1]);
+        mo_current_coord(order, level, tseg, &cc[0], &cc[1]);
+        mo_segment_coord(order, level, tseg, &ca[0], &ca[1]);
+        const double coords[6] = {ca[0], ca[1], cc[0], cc[1], ci[0], ci[1]};
+        const float* seg = ffa_fold + seg_idx * ncoords * fs;
+        float cur_thr = threshold;
+        uint64_t bsize = batch_size < n_branches ? batch_size : n_branches;
+        bsize = bsize < 1 ? 1 : bsize;
+        uint64_t processed = 0;
+        while (processed < n_branches) {
+            const uint64_t remaining = n_branches - processed;
+            const uint64_t want = bsize < remaining ? bsize : remaining;
+            /* get_leaves_span (lib/world_tree.cpp:148-163) */
+            const uint64_t pstart = wt_circ(t.read_consumed, t.head, t.cap);
+            const uint64_t nb = want < (t.cap - pstart) ? want : (t.cap - pstart);
+            if (nb == 0) {
+                rc = fail("Loaded batch size is 0");
+                goto done;
+            }
+            processed += nb;
+            uint64_t nl = 0;
+            const int brc = lko_taylor_branch(t.leaves + pstart * ls, nb, np, cc[0], cc[1], nbins,
+                                              p->eta, branch_max, b_leaves, b_org, max_branched,
+                                              &nl);
+            if (brc == 2) {
+                rc = fail("Branch factor exceeded workspace size:n_leaves_batch <= "
+                          "max_branched_leaves");
+                goto done;
+            }
+            if (brc != 0) {
+                rc = 1;
+                goto done;
+            }
+            n_leaves += nl;
+            n_phy += nl;
+            if (nl == 0) {
+                t.read_consumed += nb;
+                continue;
+            }
+            lko_taylor_resolve(p, b_leaves, nl, coords, b_pidx, b_shift);
+            lko_shift_add_batch(t.folds, b_org, seg, b_pidx, b_shift, b_folds, nbins, nl, pstart,
+                                t.cap);
+            const uint64_t npass =
+                lko_score_filter(b_folds, nl, nbins, p->widths, p->n_widths, cur_thr, b_scores, b_idx);
+            for (uint64_t i = 0; i < nl; ++i) {
+                smin = (b_scores[i] < smin) ? b_scores[i] : smin;
+                smax = (smax < b_scores[i]) ? b_scores[i] : smax;
+            }
+            if (npass == 0) {
+                t.read_consumed += nb;
+                continue;
+            }
+            lko_taylor_transform(b_leaves, b_idx, npass, np, cn[0], cc[0], conservative);
+            cur_thr = wt_add_batch(&t, b_leaves, b_folds, b_scores, b_idx, cur_thr, npass);
+            t.read_consumed += nb;
+        }
+        wt_finalize(&t);
+        lko_prune_stats sl = {level, seg_idx, n_branches, n_leaves, n_phy, t.size,
+                              threshold, smin, smax, 0};
+        stats[ns++] = sl;
+        if (t.size == 0) {
+            break;
+        }
+    }
+    *n_stats = ns;
+    *n_out = t.size;
+    if (t.size <= cap_out) {
+        for (uint64_t i = 0; i < t.size; ++i) {
+            const uint64_t ph = wt_circ(i, t.head, t.cap);
+            memcpy(leaves_out + i * ls, t.leaves + ph * ls, ls * sizeof(double));
+            memcpy(folds_out + i * fs, t.folds + ph * fs, fs * sizeof(float));
+            scores_out[i] = t.scores[ph];
+        }
+    }
+done:
+    free(t.leaves);
+    free(t.folds);
+    free(t.scores);
+    free(t.scratch);
+    free(t.pending);
+    free(order);
+    free(b_leaves);
+    free(b_org);
+    free(b_pidx);
+    free(b_shift);
+    free(b_folds);
+    free(b_scores);
+    free(b_idx);
+    return rc;
+}

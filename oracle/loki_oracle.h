@@ -135,6 +135,77 @@ void lko_circular_prefix_sum(const float* x, float* out, uint64_t nbins, uint64_
 uint64_t lko_compact(const float* scores, uint64_t n, float snr_min, uint32_t* idx_out,
                      float* score_out);
 
+/* ---- pruning leaf step (Taylor basis, nparams 2 or 3) ---------------------- */
+
+/* psr_utils::MiddleOutScheme (lib/loki/psr_utils.hpp:327-502) at one level:
+ * out[0] = segment index, out[1..2] = get_coord, out[3..4] =
+ * get_current_coord, out[5..6] = get_segment_coord. */
+int lko_middle_out(uint64_t nsegments, uint64_t ref_idx, double tsegment, uint64_t level,
+                   double* out);
+
+/* core::poly_taylor_seed (lib/taylor.cpp:1197-1257) over the final level of
+ * the plan: leaves [ncoords, nparams + 2, 2]. Returns the number of leaves
+ * (0 with lko_last_error() set on failure). */
+uint64_t lko_taylor_seed(const lko_plan* plan, double* leaves_out);
+
+/* poly_taylor_branch_{accel,jerk}_batch (lib/taylor.cpp:24-314). Children
+ * counts are computed first: *n_out receives the number of children, and
+ * nothing is written when it exceeds cap_out (returns 2). Returns 1 with the
+ * reference's message when a parameter needs more than branch_max points. */
+int lko_taylor_branch(const double* leaves, uint64_t n, uint32_t nparams, double t_cur,
+                      double scale_cur, uint64_t nbins, double eta, uint64_t branch_max,
+                      double* leaves_out, uint64_t* origins_out, uint64_t cap_out,
+                      uint64_t* n_out);
+
+/* poly_taylor_resolve_{accel,jerk}_batch (lib/taylor.cpp:492-619) against the
+ * final level of the plan. coords = {t_add, s_add, t_cur, s_cur, t_init,
+ * s_init}. */
+void lko_taylor_resolve(const lko_plan* plan, const double* leaves, uint64_t n,
+                        const double* coords, uint64_t* param_idx, float* phase_shift);
+
+/* poly_taylor_transform_{accel,jerk}_batch<Conservative> (lib/taylor.cpp:
+ * 881-1005), in place on the leaves named by indices. */
+void lko_taylor_transform(double* leaves, const uint64_t* indices, uint64_t n, uint32_t nparams,
+                          double t_next, double t_cur, int conservative);
+
+/* kernels::shift_add_linear_batch (lib/kernels.cpp:1328-1355). */
+void lko_shift_add_batch(const float* folds_tree, const uint64_t* indices_tree,
+                         const float* folds_ffa, const uint64_t* indices_ffa,
+                         const float* phase_shift, float* folds_out, uint64_t nbins,
+                         uint64_t n_leaves, uint64_t physical_start_idx, uint64_t capacity);
+
+/* detection::score_and_filter_max_with_cache (lib/score.cpp:213-259):
+ * returns the number of indices (input order) with score >= threshold. */
+uint64_t lko_score_filter(const float* folds, uint64_t n, uint64_t nbins,
+                          const uint64_t* widths, uint64_t nwidths, float threshold,
+                          float* scores, uint64_t* indices);
+
+/* cands::PruneStats fields of one level. */
+typedef struct lko_prune_stats {
+    uint64_t level;
+    uint64_t seg_idx;
+    uint64_t n_branches;
+    uint64_t n_leaves;
+    uint64_t n_leaves_phy;
+    uint64_t n_leaves_surv;
+    float threshold;
+    float score_min;
+    float score_max;
+    float pad;
+} lko_prune_stats;
+
+/* One pruning run (lib/prune.cpp:181-226 initialize, :429-620 levels) with
+ * the WorldTree circular buffer (lib/world_tree.cpp:237-276,361-422,
+ * 557-669). ffa_fold is the final FFA level [nsegments, ncoords, 2, nbins];
+ * thresholds[level - 1] is the level's threshold. stats receives n_iters + 1
+ * rows at most; the final tree (logical order) is copied out when it fits
+ * cap_out. */
+int lko_prune_run(const lko_plan* plan, int conservative, const float* ffa_fold,
+                  const float* thresholds, uint64_t n_thresholds, uint64_t ref_seg,
+                  uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
+                  lko_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
+                  float* folds_out, float* scores_out, uint64_t cap_out, uint64_t* n_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,16 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
         L.lkref_phase_idx.argtypes = [f64, f64, u64, f64]
         L.lkref_phase_idx_uint.restype = u32
         L.lkref_phase_idx_uint.argtypes = [f64, f64, u64, f64]
+        L.lkref_middle_out.argtypes = [u64, u64, f64, u64, vp]
+        L.lkref_taylor_seed.argtypes = [vp, vp, u64, vp]
+        L.lkref_taylor_branch.argtypes = [vp, u64, u32, f64, f64, u64, f64, u64, vp, vp, vp]
+        L.lkref_taylor_resolve.argtypes = [vp, vp, u64, vp, vp, vp]
+        L.lkref_taylor_transform.argtypes = [vp, u64, vp, u64, u32, f64, f64, f64, f64, ctypes.c_int]
+        L.lkref_shift_add_batch.argtypes = [vp, vp, vp, vp, vp, vp, u64, u64, u64, u64]
+        L.lkref_score_filter.argtypes = [vp, u64, u64, vp, u64, f32, vp, vp, vp]
+        L.lkref_branch_max.argtypes = [vp, ctypes.c_int, vp]
+        L.lkref_prune_run.argtypes = [vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64, u64,
+                                      vp, vp, vp, vp, vp, u64, vp]
         _libs[path] = L
     return _libs[path]
 
@@ -225,3 +235,125 @@ def phase_idx(t, f, nbins, delay=0.0) -> float:
 
 def phase_idx_uint(t, f, nbins, delay=0.0) -> int:
     return lib().lkref_phase_idx_uint(t, f, nbins, delay)
+
+
+# ---- pruning leaf step ----------------------------------------------------------
+
+PRUNE_STATS_DTYPE = np.dtype([
+    ("level", np.uint64), ("seg_idx", np.uint64), ("n_branches", np.uint64), ("n_leaves", np.uint64),
+    ("n_leaves_phy", np.uint64), ("n_leaves_surv", np.uint64), ("threshold", np.float32),
+    ("score_min", np.float32), ("score_max", np.float32), ("pad", np.float32)])
+
+
+def _check(L, rc):
+    if rc != 0:
+        raise RuntimeError(L.lkref_last_error().decode())
+
+
+def middle_out(nsegments, ref_idx, tsegment, level):
+    """(seg_idx, coord, current_coord, segment_coord) of MiddleOutScheme at a level."""
+    L = lib()
+    out = np.zeros(7, np.float64)
+    _check(L, L.lkref_middle_out(nsegments, ref_idx, tsegment, level, _p(out)))
+    return int(out[0]), (out[1], out[2]), (out[3], out[4]), (out[5], out[6])
+
+
+def taylor_seed(cfg: RefCfg, n_coords: int) -> np.ndarray:
+    L = lib()
+    stride = (cfg.nparams + 2) * 2
+    out = np.zeros(n_coords * stride, np.float64)
+    n = u64()
+    _check(L, L.lkref_taylor_seed(ctypes.byref(cfg), _p(out), n_coords, ctypes.byref(n)))
+    return out[: n.value * stride].reshape(n.value, cfg.nparams + 2, 2)
+
+
+def taylor_branch(leaves, nparams, coord_cur, nbins, eta, branch_max):
+    L = lib()
+    leaves = np.ascontiguousarray(leaves, np.float64)
+    stride = (nparams + 2) * 2
+    n = leaves.size // stride
+    out = np.zeros(n * branch_max * stride, np.float64)
+    org = np.zeros(n * branch_max, np.uint64)
+    nout = u64()
+    _check(L, L.lkref_taylor_branch(_p(leaves), n, nparams, coord_cur[0], coord_cur[1], nbins, eta,
+                                    branch_max, _p(out), _p(org), ctypes.byref(nout)))
+    k = nout.value
+    return out[: k * stride].reshape(k, nparams + 2, 2), org[:k]
+
+
+def taylor_resolve(cfg: RefCfg, leaves, coord_add, coord_cur, coord_init):
+    L = lib()
+    leaves = np.ascontiguousarray(leaves, np.float64)
+    n = leaves.size // ((cfg.nparams + 2) * 2)
+    coords = np.array([*coord_add, *coord_cur, *coord_init], np.float64)
+    idx = np.zeros(n, np.uint64)
+    sh = np.zeros(n, np.float32)
+    _check(L, L.lkref_taylor_resolve(ctypes.byref(cfg), _p(leaves), n, _p(coords), _p(idx), _p(sh)))
+    return idx, sh
+
+
+def taylor_transform(leaves, indices, nparams, coord_next, coord_cur, conservative=False):
+    """Returns a transformed copy of ``leaves`` (only rows named by indices change)."""
+    L = lib()
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    idx = np.ascontiguousarray(indices, np.uint64)
+    ntot = out.size // ((nparams + 2) * 2)
+    _check(L, L.lkref_taylor_transform(_p(out), ntot, _p(idx), idx.size, nparams, coord_next[0],
+                                       coord_next[1], coord_cur[0], coord_cur[1], int(conservative)))
+    return out
+
+
+def shift_add_batch(folds_tree, indices_tree, folds_ffa, indices_ffa, phase_shift, nbins,
+                    physical_start_idx, capacity):
+    L = lib()
+    ft = np.ascontiguousarray(folds_tree, np.float32)
+    it = np.ascontiguousarray(indices_tree, np.uint64)
+    ff = np.ascontiguousarray(folds_ffa, np.float32)
+    iff = np.ascontiguousarray(indices_ffa, np.uint64)
+    ps = np.ascontiguousarray(phase_shift, np.float32)
+    out = np.zeros((it.size, 2, nbins), np.float32)
+    _check(L, L.lkref_shift_add_batch(_p(ft), _p(it), _p(ff), _p(iff), _p(ps), _p(out), nbins, it.size,
+                                      physical_start_idx, capacity))
+    return out
+
+
+def score_filter(folds, nbins, widths, threshold):
+    L = lib()
+    folds = np.ascontiguousarray(folds, np.float32)
+    w = np.ascontiguousarray(widths, np.uint64)
+    n = folds.size // (2 * nbins)
+    scores = np.zeros(n, np.float32)
+    idx = np.zeros(n, np.uint64)
+    npass = u64()
+    _check(L, L.lkref_score_filter(_p(folds), n, nbins, _p(w), w.size, threshold, _p(scores), _p(idx),
+                                   ctypes.byref(npass)))
+    return scores, idx[: npass.value]
+
+
+def branch_max(cfg: RefCfg, conservative=False) -> int:
+    L = lib()
+    out = u64()
+    _check(L, L.lkref_branch_max(ctypes.byref(cfg), int(conservative), ctypes.byref(out)))
+    return out.value
+
+
+def prune_run(cfg: RefCfg, ffa_fold, thresholds, ref_seg, max_sugg, batch_size, branch_max_,
+              n_iters, nbins, conservative=False, kind="parity"):
+    """One reference pruning run: returns (stats, leaves, folds, scores) of the final tree."""
+    L = lib(kind)
+    ffa = np.ascontiguousarray(ffa_fold, np.float32).ravel()
+    thr = np.ascontiguousarray(thresholds, np.float32)
+    stats = np.zeros(n_iters + 1, PRUNE_STATS_DTYPE)
+    nstats = u64()
+    stride = (cfg.nparams + 2) * 2
+    leaves = np.zeros(max_sugg * stride, np.float64)
+    folds = np.zeros(max_sugg * 2 * nbins, np.float32)
+    scores = np.zeros(max_sugg, np.float32)
+    n = u64()
+    _check(L, L.lkref_prune_run(ctypes.byref(cfg), int(conservative), _p(ffa), ffa.size, _p(thr), thr.size,
+                                ref_seg, max_sugg, batch_size, branch_max_, n_iters, _p(stats),
+                                ctypes.byref(nstats), _p(leaves), _p(folds), _p(scores), max_sugg,
+                                ctypes.byref(n)))
+    k = n.value
+    return (stats[: nstats.value], leaves[: k * stride].reshape(k, cfg.nparams + 2, 2),
+            folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k])

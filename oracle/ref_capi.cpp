@@ -19,6 +19,19 @@
 //                            (lib/score.cpp:390-405)
 //   lkref_phase_idx*      -> psr_utils::get_phase_idx[_uint]
 //                            (lib/loki/psr_utils.hpp:32-63)
+//   lkref_middle_out      -> psr_utils::MiddleOutScheme (lib/loki/psr_utils.hpp:327-502)
+//   lkref_taylor_*        -> core::poly_taylor_{seed,branch,resolve,transform}_batch
+//                            (lib/taylor.cpp:24-314,492-619,881-1005,1197-1257)
+//   lkref_shift_add_batch -> kernels::shift_add_linear_batch (lib/kernels.cpp:1328-1355)
+//   lkref_score_filter    -> detection::score_and_filter_max_with_cache
+//                            (lib/score.cpp:213-259)
+//   lkref_branch_max      -> EPMultiPass's branch_max rule (lib/prune.cpp:648-651)
+//   lkref_prune_run       -> PruneImpl::initialize + execute_iteration[_batched]
+//                            (lib/prune.cpp:181-226,429-620), restated here
+//                            because prune.cpp itself needs HDF5 and a
+//                            thread pool; every step calls the reference's
+//                            own PruneDPFuncts (lib/dynamic.cpp) and
+//                            WorldTree (lib/world_tree.cpp).
 
 #include <cstdint>
 #include <cstring>
@@ -37,9 +50,14 @@
 #include "loki/common/coord.hpp"
 #include "loki/common/plans.hpp"
 #include "loki/common/types.hpp"
+#include "loki/core/dynamic.hpp"
+#include "loki/core/taylor.hpp"
 #include "loki/detection/score.hpp"
+#include "loki/kernels.hpp"
 #include "loki/psr_utils.hpp"
 #include "loki/search/configs.hpp"
+#include "loki/utils/workspace.hpp"
+#include "loki/utils/world_tree.hpp"
 
 namespace {
 
@@ -283,6 +301,312 @@ uint32_t lkref_phase_idx_uint(double proper_time,
                               uint64_t nbins,
                               double delay) {
     return loki::psr_utils::get_phase_idx_uint(proper_time, freq, nbins, delay);
+}
+
+// ---- pruning leaf step ------------------------------------------------------
+
+// MiddleOutScheme of (nsegments, ref_idx, tsegment) at one level: out[0] =
+// segment index, out[1..2] = get_coord, out[3..4] = get_current_coord,
+// out[5..6] = get_segment_coord.
+int lkref_middle_out(uint64_t nsegments, uint64_t ref_idx, double tsegment, uint64_t level,
+                     double* out) {
+    return guarded([&] {
+        const loki::psr_utils::MiddleOutScheme sc(nsegments, ref_idx, tsegment);
+        out[0]         = static_cast<double>(sc.get_segment_idx(level));
+        const auto c   = sc.get_coord(level);
+        const auto cur = sc.get_current_coord(level);
+        const auto seg = sc.get_segment_coord(level);
+        out[1] = c.first;
+        out[2] = c.second;
+        out[3] = cur.first;
+        out[4] = cur.second;
+        out[5] = seg.first;
+        out[6] = seg.second;
+    });
+}
+
+static loki::search::PulsarSearchConfig make_cfg_prune(const lkref_cfg* c, int conservative) {
+    std::vector<loki::ParamLimit> lims(c->nparams);
+    for (uint32_t i = 0; i < c->nparams; ++i) {
+        lims[i] = {.min = c->limits[2 * i], .max = c->limits[(2 * i) + 1]};
+    }
+    std::optional<loki::SizeType> bb;
+    std::optional<loki::SizeType> bf;
+    if (c->bseg_brute != 0) {
+        bb = c->bseg_brute;
+    }
+    if (c->bseg_ffa != 0) {
+        bf = c->bseg_ffa;
+    }
+    return {c->nsamps, c->tsamp, c->nbins, c->eta, lims, c->ducy_max, c->wtsp,
+            /*use_fourier=*/false, c->nthreads,
+            /*max_process_memory_gb=*/8.0, /*octave_scale=*/2.0,
+            /*nbins_max=*/1024, /*nbins_min_lossy_bf=*/64, bb, bf,
+            /*snr_min=*/5.0, /*max_passing_candidates=*/1U << 22U,
+            /*prune_poly_order=*/3, /*p_orb_min=*/1e-5, /*m_c_max=*/10.0,
+            /*m_p_min=*/1.4, /*minimum_snap_cells=*/5.0, conservative != 0};
+}
+
+// Seed leaves of the final FFA level ([ncoords, nparams + 2, 2] doubles).
+int lkref_taylor_seed(const lkref_cfg* c, double* leaves_out, uint64_t cap, uint64_t* n_out) {
+    return guarded([&] {
+        const auto cfg = make_cfg_prune(c, 0);
+        const loki::plans::FFAPlan<float> plan(cfg);
+        std::span<double> out(leaves_out, cap * (c->nparams + 2) * 2);
+        *n_out = loki::core::poly_taylor_seed(plan.get_param_counts().back(),
+                                              plan.get_dparams_actual().back(),
+                                              cfg.get_param_limits(), out, {0.0, 0.0},
+                                              c->nparams);
+    });
+}
+
+// Branch n parent leaves. leaves_out must hold n * branch_max leaves.
+int lkref_taylor_branch(const double* leaves_in, uint64_t n, uint32_t nparams, double t_cur,
+                        double scale_cur, uint64_t nbins, double eta, uint64_t branch_max,
+                        double* leaves_out, uint64_t* origins_out, uint64_t* n_out) {
+    return guarded([&] {
+        const uint64_t stride = (nparams + 2) * 2;
+        loki::memory::BranchingWorkspace ws(n, branch_max, nparams);
+        std::span<const double> in(leaves_in, n * stride);
+        std::span<double> out(leaves_out, n * branch_max * stride);
+        std::span<loki::SizeType> org(reinterpret_cast<loki::SizeType*>(origins_out),
+                                      n * branch_max);
+        *n_out = loki::core::poly_taylor_branch_batch(in, out, org, {t_cur, scale_cur}, nbins,
+                                                      eta, branch_max, n, nparams, ws);
+    });
+}
+
+// Resolve n leaves against the final FFA level of the configuration.
+// coords = {t_add, s_add, t_cur, s_cur, t_init, s_init}.
+int lkref_taylor_resolve(const lkref_cfg* c, const double* leaves, uint64_t n,
+                         const double* coords, uint64_t* param_idx, float* phase_shift) {
+    return guarded([&] {
+        const auto cfg = make_cfg_prune(c, 0);
+        const loki::plans::FFAPlan<float> plan(cfg);
+        const auto& counts = plan.get_param_counts().back();
+        const uint64_t stride = (c->nparams + 2) * 2;
+        loki::core::poly_taylor_resolve_batch(
+            std::span<const double>(leaves, n * stride),
+            std::span<loki::SizeType>(reinterpret_cast<loki::SizeType*>(param_idx), n),
+            std::span<float>(phase_shift, n), cfg.get_param_limits(), {coords[0], coords[1]},
+            {coords[2], coords[3]}, {coords[4], coords[5]}, counts[c->nparams - 2],
+            counts[c->nparams - 1], c->nbins, n, c->nparams);
+    });
+}
+
+// In-place transform of the leaves named by indices[0..n).
+int lkref_taylor_transform(double* leaves, uint64_t n_leaves_total, const uint64_t* indices,
+                           uint64_t n, uint32_t nparams, double t_next, double s_next,
+                           double t_cur, double s_cur, int conservative) {
+    return guarded([&] {
+        const uint64_t stride = (nparams + 2) * 2;
+        std::vector<loki::SizeType> idx(indices, indices + n);
+        loki::core::poly_taylor_transform_batch(std::span<double>(leaves, n_leaves_total * stride),
+                                                idx, {t_next, s_next}, {t_cur, s_cur}, n,
+                                                nparams, conservative != 0);
+    });
+}
+
+int lkref_shift_add_batch(const float* folds_tree, const uint64_t* indices_tree,
+                          const float* folds_ffa, const uint64_t* indices_ffa,
+                          const float* phase_shift, float* folds_out, uint64_t nbins,
+                          uint64_t n_leaves, uint64_t physical_start_idx, uint64_t capacity) {
+    return guarded([&] {
+        std::vector<float> tmp(2 * nbins);
+        loki::kernels::shift_add_linear_batch(
+            folds_tree, reinterpret_cast<const loki::SizeType*>(indices_tree), folds_ffa,
+            reinterpret_cast<const loki::SizeType*>(indices_ffa), phase_shift, folds_out,
+            tmp.data(), nbins, n_leaves, physical_start_idx, capacity);
+    });
+}
+
+int lkref_score_filter(const float* folds, uint64_t n, uint64_t nbins, const uint64_t* widths,
+                       uint64_t nwidths, float threshold, float* scores, uint64_t* indices,
+                       uint64_t* n_pass) {
+    return guarded([&] {
+        std::vector<loki::SizeType> w(widths, widths + nwidths);
+        loki::detection::BoxcarWidthsCache cache(w, nbins);
+        *n_pass = loki::detection::score_and_filter_max_with_cache(
+            std::span<const float>(folds, n * 2 * nbins), std::span<float>(scores, n),
+            std::span<loki::SizeType>(reinterpret_cast<loki::SizeType*>(indices), n),
+            threshold, n, nbins, cache);
+    });
+}
+
+// EPMultiPass's branch_max: max(ceil(2 * max branching pattern), 32).
+int lkref_branch_max(const lkref_cfg* c, int conservative, uint64_t* out) {
+    return guarded([&] {
+        const auto cfg = make_cfg_prune(c, conservative);
+        const loki::plans::FFAPlan<float> plan(cfg);
+        const auto bp = plan.get_branching_pattern("taylor");
+        const auto mx = *std::ranges::max_element(bp);
+        *out = std::max(static_cast<loki::SizeType>(std::ceil(mx * 2)), loki::SizeType{32});
+    });
+}
+
+// Per-level statistics (cands::PruneStats fields).
+struct lkref_prune_stats {
+    uint64_t level;
+    uint64_t seg_idx;
+    uint64_t n_branches;
+    uint64_t n_leaves;
+    uint64_t n_leaves_phy;
+    uint64_t n_leaves_surv;
+    float threshold;
+    float score_min;
+    float score_max;
+    float pad;
+};
+
+// One pruning run for ref_seg over the FFA fold of the final level
+// ([nsegments, ncoords, 2, nbins]): seed, then up to n_iters levels (each
+// uses thresholds[level - 1]). stats receives one row for the seed and one
+// per level run; the final tree is copied out in logical order.
+int lkref_prune_run(const lkref_cfg* c, int conservative, const float* ffa_fold,
+                    uint64_t ffa_fold_len, const float* thresholds, uint64_t n_thresholds,
+                    uint64_t ref_seg, uint64_t max_sugg, uint64_t batch_size,
+                    uint64_t branch_max, uint64_t n_iters, lkref_prune_stats* stats,
+                    uint64_t* n_stats, double* leaves_out, float* folds_out, float* scores_out,
+                    uint64_t cap_out, uint64_t* n_out) {
+    return guarded([&] {
+        using loki::SizeType;
+        const auto cfg = make_cfg_prune(c, conservative);
+        const loki::plans::FFAPlan<float> plan(cfg);
+        const SizeType nsegments = plan.get_nsegments().back();
+        const double tseg        = plan.get_tsegments().back();
+        const SizeType nparams   = cfg.get_nparams();
+        const SizeType nbins     = cfg.get_nbins();
+        auto funcs = loki::core::create_prune_dp_functs<float>(
+            "taylor", plan.get_param_counts().back(), plan.get_dparams_actual().back(),
+            nsegments, tseg, cfg, batch_size, branch_max);
+        loki::memory::EPWorkspace<float> ws(batch_size, branch_max, max_sugg,
+                                            plan.get_ncoords().back(), nparams, nbins,
+                                            nsegments);
+        auto& world_tree = ws.world_tree;
+        auto& prune_ws   = ws.prune;
+        auto& branch_ws  = ws.branch;
+        const std::span<const float> ffa(ffa_fold, ffa_fold_len);
+
+        // initialize (prune.cpp:181-226)
+        world_tree.reset();
+        const loki::psr_utils::MiddleOutScheme snail(nsegments, ref_seg, tseg);
+        const auto fold_segment = funcs->load_segment(ffa, snail.get_ref_idx());
+        const auto coord_init0  = snail.get_coord(0);
+        const SizeType n_seed   = plan.get_ncoords().back();
+        funcs->seed(fold_segment, ws.seed_leaves, ws.seed_scores, coord_init0);
+        world_tree.add_initial(ws.seed_leaves, fold_segment, ws.seed_scores, n_seed);
+        SizeType ns = 0;
+        stats[ns++] = {0, snail.get_segment_idx(0), world_tree.get_size(),
+                       world_tree.get_size(), world_tree.get_size(), world_tree.get_size(),
+                       0.0F, world_tree.get_score_min(), world_tree.get_score_max(), 0.0F};
+
+        // levels (prune.cpp:429-620)
+        const SizeType levels = std::min<SizeType>(nsegments - 1, n_iters);
+        for (SizeType prune_level = 1; prune_level <= levels; ++prune_level) {
+            if (prune_level > n_thresholds) {
+                throw std::runtime_error("Pruning complete - exceeded threshold scheme length");
+            }
+            world_tree.prepare_in_place_update();
+            const SizeType seg_idx_cur = snail.get_segment_idx(prune_level);
+            const float threshold      = thresholds[prune_level - 1];
+            const SizeType n_branches  = world_tree.get_size_old();
+            SizeType n_leaves = 0, n_leaves_phy = 0;
+            float score_min = std::numeric_limits<float>::max();
+            float score_max = std::numeric_limits<float>::lowest();
+
+            const auto coord_init = snail.get_coord(0);
+            const auto coord_prev = snail.get_coord(prune_level - 1);
+            const auto coord_next = snail.get_coord(prune_level);
+            const auto coord_cur  = snail.get_current_coord(prune_level);
+            const auto coord_add  = snail.get_segment_coord(prune_level);
+            const auto ffa_fold_segment = funcs->load_segment(ffa, seg_idx_cur);
+            auto current_threshold = threshold;
+            const SizeType bsize = std::max<SizeType>(1, std::min(batch_size, n_branches));
+            SizeType total_processed = 0;
+            while (total_processed < n_branches) {
+                const SizeType remaining       = n_branches - total_processed;
+                const SizeType this_batch_size = std::min(bsize, remaining);
+                auto [leaves_tree_span, current_batch_size] =
+                    world_tree.get_leaves_span(this_batch_size);
+                if (current_batch_size == 0) {
+                    throw std::runtime_error("Loaded batch size is 0");
+                }
+                total_processed += current_batch_size;
+                const auto n_leaves_batch = funcs->branch(
+                    leaves_tree_span, prune_ws.branched_leaves, prune_ws.branched_indices,
+                    coord_cur, coord_prev, current_batch_size, branch_ws);
+                n_leaves += n_leaves_batch;
+                if (n_leaves_batch == 0) {
+                    world_tree.consume_read(current_batch_size);
+                    continue;
+                }
+                if (n_leaves_batch > prune_ws.max_branched_leaves) {
+                    throw std::runtime_error("Branch factor exceeded workspace size");
+                }
+                const auto n_valid = funcs->validate(prune_ws.branched_leaves,
+                                                     prune_ws.branched_indices, coord_cur,
+                                                     n_leaves_batch);
+                n_leaves_phy += n_valid;
+                if (n_valid == 0) {
+                    world_tree.consume_read(current_batch_size);
+                    continue;
+                }
+                funcs->resolve(prune_ws.branched_leaves, prune_ws.branched_param_idx,
+                               prune_ws.branched_phase_shift, coord_add, coord_cur,
+                               coord_init, n_valid);
+                funcs->shift_add(world_tree.get_folds(), prune_ws.branched_indices,
+                                 ffa_fold_segment, prune_ws.branched_param_idx,
+                                 prune_ws.branched_phase_shift, prune_ws.branched_folds,
+                                 n_valid, world_tree.get_physical_start_idx(),
+                                 world_tree.get_capacity());
+                const SizeType n_pass = funcs->score_and_filter(
+                    prune_ws.branched_folds, prune_ws.branched_scores,
+                    prune_ws.branched_indices, current_threshold, n_valid);
+                const auto sc = std::span<const float>(prune_ws.branched_scores).first(n_valid);
+                const auto [mn, mx] = std::ranges::minmax_element(sc);
+                score_min = std::min(score_min, *mn);
+                score_max = std::max(score_max, *mx);
+                if (n_pass == 0) {
+                    world_tree.consume_read(current_batch_size);
+                    continue;
+                }
+                funcs->transform(prune_ws.branched_leaves, prune_ws.branched_indices,
+                                 coord_next, coord_cur, n_pass);
+                current_threshold = world_tree.add_batch_scattered(
+                    prune_ws.branched_leaves, prune_ws.branched_folds,
+                    prune_ws.branched_scores, prune_ws.branched_indices, current_threshold,
+                    n_pass);
+                world_tree.consume_read(current_batch_size);
+            }
+            world_tree.finalize_in_place_update();
+            stats[ns++] = {prune_level, seg_idx_cur, n_branches, n_leaves, n_leaves_phy,
+                           world_tree.get_size(), threshold, score_min, score_max, 0.0F};
+            if (world_tree.get_size() == 0) {
+                break;
+            }
+        }
+        *n_stats = ns;
+
+        // final tree in logical order
+        const SizeType n = world_tree.get_size();
+        *n_out = n;
+        if (n > cap_out) {
+            return;
+        }
+        const SizeType ls = world_tree.get_leaves_stride();
+        const SizeType fs = world_tree.get_folds_stride();
+        const auto lv = world_tree.get_leaves_circular_view();
+        const auto fv = world_tree.get_folds_circular_view();
+        const auto sv = world_tree.get_scores_circular_view();
+        std::copy(lv.first.begin(), lv.first.end(), leaves_out);
+        std::copy(lv.second.begin(), lv.second.end(), leaves_out + lv.first.size());
+        std::copy(fv.first.begin(), fv.first.end(), folds_out);
+        std::copy(fv.second.begin(), fv.second.end(), folds_out + fv.first.size());
+        std::copy(sv.first.begin(), sv.first.end(), scores_out);
+        std::copy(sv.second.begin(), sv.second.end(), scores_out + sv.first.size());
+        (void)ls;
+        (void)fs;
+    });
 }
 
 } // extern "C"
