@@ -21,6 +21,14 @@
  *   lk_brute_fold_*   algorithms::BruteFoldCUDA<float> (include/loki/algorithms/fold.hpp:78-134)
  *   lk_snr_boxcar_*   detection::snr_boxcar_{3d,3d_max,2d_max}_cuda (lib/score_cuda.cu:253-513)
  *   lk_compact_ge     score compaction of FFAFreqSweep (lib/ffa_freq_sweep.cpp:182-195)
+ *   lk_prune_*        PruneImpl / EPMultiPass per ref_seg run (lib/prune.cpp:40-226,429-620)
+ *                     and PruneCUDA (include/loki/algorithms/prune.hpp)
+ *   lk_taylor_*, lk_shift_add_batch, lk_score_filter
+ *                     the Taylor PruneDPFuncts steps (include/loki/core/dynamic.hpp:22-115):
+ *                     core::poly_taylor_{seed,branch,resolve,transform}_batch
+ *                     (include/loki/core/taylor.hpp:16-79), kernels::shift_add_linear_batch
+ *                     (lib/loki/kernels.hpp:100), detection::score_and_filter_max_with_cache
+ *                     (include/loki/detection/score.hpp:113-119)
  */
 #ifndef LOKI_B200_H
 #define LOKI_B200_H
@@ -231,6 +239,92 @@ int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
 int lk_compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
                           float* d_vals, uint64_t max_out, uint64_t* d_count,
                           lk_stream_t stream);
+
+/* ---- pruning leaf step (Taylor basis, nparams 2 or 3) ------------------ */
+/* Leaves are [n, nparams + 2, 2] doubles: (value, step) of each Taylor
+ * parameter from the highest derivative down to velocity, then (d0, 0) and
+ * (f0, basis flag), as core::poly_taylor_seed lays them out. Index arrays on
+ * the device are uint32 (the reference uses 64-bit SizeType on the host). */
+typedef struct lk_prune lk_prune;
+
+/* cands::PruneStats fields of one level. */
+typedef struct lk_prune_stats {
+    uint64_t level;
+    uint64_t seg_idx;
+    uint64_t n_branches;
+    uint64_t n_leaves;
+    uint64_t n_leaves_phy;
+    uint64_t n_leaves_surv;
+    float threshold;
+    float score_min;
+    float score_max;
+    float pad;
+} lk_prune_stats;
+
+/* One pruning search over the final FFA level of the plan (its nsegments
+ * segments, bseg_ffa samples each). max_sugg: world-tree capacity;
+ * batch_size: parents per batch (the reference's batch semantics, which
+ * decide when the threshold rises); branch_max: most child values of one
+ * parameter, 0 for EPMultiPass's rule max(ceil(2 * max branching), 32) over
+ * the branching pattern of ref_seg 0 (lib/prune.cpp:648-651);
+ * conservative: use_conservative_tile. */
+int lk_prune_create(const lk_plan* plan, uint64_t max_sugg, uint64_t batch_size,
+                    uint64_t branch_max, int conservative, int device, lk_prune** out);
+void lk_prune_destroy(lk_prune* pr);
+/* Seed from segment ref_seg of d_ffa_fold ([nsegments, ncoords, 2, nbins],
+ * the output of lk_ffa_execute) and run up to n_iters levels, level l using
+ * thresholds[l - 1] (host array). stats (host) receives one row for the seed
+ * and one per level run, *n_stats their number (stops when no leaf
+ * survives). Synchronises the stream several times per level. */
+int lk_prune_run(lk_prune* pr, const float* d_ffa_fold, uint64_t ref_seg,
+                 const float* thresholds, uint64_t n_thresholds, uint64_t n_iters,
+                 lk_prune_stats* stats, uint64_t max_stats, uint64_t* n_stats,
+                 lk_stream_t stream);
+/* core::generate_bp_poly_taylor (lib/taylor.cpp:1643-1741), the
+ * FFAPlan::get_branching_pattern("taylor", ref_seg) of the reference: the
+ * average branching factor of each of the nsegments - 1 pruning levels. */
+int lk_plan_branching_pattern(const lk_plan* plan, uint64_t ref_seg, int conservative,
+                              double* out, uint64_t max_out, uint64_t* n_out);
+/* Surviving leaves after lk_prune_run, in the world tree's logical order.
+ * Any of the device outputs may be NULL. */
+int lk_prune_tree_size(const lk_prune* pr, uint64_t* n);
+int lk_prune_get_tree(const lk_prune* pr, double* d_leaves, float* d_folds, float* d_scores,
+                      uint64_t max_out, lk_stream_t stream);
+
+/* Single steps, for callers composing their own level loop. */
+/* Seed leaves of the plan's final level, [ncoords, nparams + 2, 2]. */
+int lk_taylor_seed(const lk_plan* plan, double* d_leaves, lk_stream_t stream);
+/* Branch n parents with dt = scale of the current coordinate. Children are
+ * written in parent order (origins: parent index); *n_out (host) = children;
+ * nothing is written beyond max_out. Synchronises the stream. */
+int lk_taylor_branch(const lk_plan* plan, const double* d_leaves, uint64_t n, double scale_cur,
+                     uint64_t branch_max, double* d_out, uint32_t* d_origins, uint64_t max_out,
+                     uint64_t* n_out, lk_stream_t stream);
+/* coords = {t_add, scale_add, t_cur, scale_cur, t_init, scale_init} (host). */
+int lk_taylor_resolve(const lk_plan* plan, const double* d_leaves, uint64_t n,
+                      const double* coords, uint32_t* d_param_idx, float* d_phase_shift,
+                      lk_stream_t stream);
+/* In place on the leaves named by d_indices[0..n) of d_leaves[0..n_leaves);
+ * an index at or beyond n_leaves is rejected (LK_ERR_INVALID_ARG, after the
+ * other leaves are done). Synchronises the stream. */
+int lk_taylor_transform(const lk_plan* plan, double* d_leaves, uint64_t n_leaves,
+                        const uint32_t* d_indices, uint64_t n, double t_next, double t_cur,
+                        int conservative, lk_stream_t stream);
+/* out[i] = folds_tree[indices_tree[i] + physical_start, wrapped once at
+ *          capacity] + rotate_right(folds_ffa[indices_ffa[i]], round(phase_shift[i])).
+ * n_ffa: rows in d_folds_ffa. A tree index still >= capacity after the wrap
+ * or an FFA row >= n_ffa is rejected (LK_ERR_INVALID_ARG) and its output
+ * left unwritten. Synchronises the stream. */
+int lk_shift_add_batch(const float* d_folds_tree, const uint32_t* d_indices_tree,
+                       const float* d_folds_ffa, uint64_t n_ffa, const uint32_t* d_indices_ffa,
+                       const float* d_phase_shift, float* d_folds_out, uint32_t nbins,
+                       uint64_t n, uint64_t physical_start, uint64_t capacity,
+                       lk_stream_t stream);
+/* Max-width S/N of [n, 2, nbins] folds into d_scores; indices (input order)
+ * with score >= threshold into d_indices, their number into *d_count. */
+int lk_score_filter(const float* d_folds, uint64_t n, uint32_t nbins, const uint32_t* widths,
+                    uint32_t nwidths, float threshold, float* d_scores, uint32_t* d_indices,
+                    uint64_t* d_count, lk_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -103,6 +103,21 @@ class LkStageTime(ctypes.Structure):
 
 
 # (name, restype, argtypes) of every exported entry point, in header order.
+class LkPruneStats(ctypes.Structure):
+    _fields_ = [
+        ("level", u64),
+        ("seg_idx", u64),
+        ("n_branches", u64),
+        ("n_leaves", u64),
+        ("n_leaves_phy", u64),
+        ("n_leaves_surv", u64),
+        ("threshold", f32),
+        ("score_min", f32),
+        ("score_max", f32),
+        ("pad", f32),
+    ]
+
+
 SIGNATURES = [
     ("lk_last_error", ctypes.c_char_p, []),
     ("lk_version", i32, []),
@@ -130,6 +145,18 @@ SIGNATURES = [
     ("lk_compact_scratch_bytes", u64, [u64]),
     ("lk_compact_ge", i32, [vp, u64, f32, vp, vp, u64, vp, vp, vp]),
     ("lk_compact_ge_noalloc", i32, [vp, u64, f32, vp, vp, u64, vp, vp]),
+    ("lk_prune_create", i32, [vp, u64, u64, u64, i32, i32, vp]),
+    ("lk_prune_destroy", None, [vp]),
+    ("lk_plan_branching_pattern", i32, [vp, u64, i32, vp, u64, vp]),
+    ("lk_prune_run", i32, [vp, vp, u64, vp, u64, u64, vp, u64, vp, vp]),
+    ("lk_prune_tree_size", i32, [vp, vp]),
+    ("lk_prune_get_tree", i32, [vp, vp, vp, vp, u64, vp]),
+    ("lk_taylor_seed", i32, [vp, vp, vp]),
+    ("lk_taylor_branch", i32, [vp, vp, u64, f64, u64, vp, vp, u64, vp, vp]),
+    ("lk_taylor_resolve", i32, [vp, vp, u64, vp, vp, vp, vp]),
+    ("lk_taylor_transform", i32, [vp, vp, u64, vp, u64, f64, f64, i32, vp]),
+    ("lk_shift_add_batch", i32, [vp, vp, vp, u64, vp, vp, vp, u32, u64, u64, u64, vp]),
+    ("lk_score_filter", i32, [vp, u64, u32, vp, u32, f32, vp, vp, vp, vp]),
 ]
 
 _lib: ctypes.CDLL | None = None

@@ -9,12 +9,16 @@
 
 #include "lk_ffa.hpp"
 #include "lk_kernels.hpp"
+#include "lk_prune.hpp"
 
 struct lk_plan {
     lk::Plan plan;
 };
 struct lk_ffa {
     std::unique_ptr<lk::FFAExec> exec;
+};
+struct lk_prune {
+    std::unique_ptr<lk::PruneExec> exec;
 };
 struct lk_brute_fold {
     int device = 0;
@@ -365,6 +369,177 @@ int lk_compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t
         }
         lk::compact_ge_noalloc(d_scores, n, thr, d_idx, d_vals, max_out, d_count,
                                reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+// ---- pruning leaf step ------------------------------------------------------
+
+int lk_prune_create(const lk_plan* plan, uint64_t max_sugg, uint64_t batch_size,
+                    uint64_t branch_max, int conservative, int device, lk_prune** out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        auto h = std::make_unique<lk_prune>();
+        if (branch_max == 0) {
+            branch_max = plan->plan.prune_branch_max(conservative != 0);
+        }
+        h->exec = std::make_unique<lk::PruneExec>(plan->plan, max_sugg, batch_size, branch_max,
+                                                  conservative != 0, device);
+        *out = h.release();
+    });
+}
+
+void lk_prune_destroy(lk_prune* pr) { delete pr; }
+
+int lk_plan_branching_pattern(const lk_plan* plan, uint64_t ref_seg, int conservative,
+                              double* out, uint64_t max_out, uint64_t* n_out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(n_out, "n_out");
+        const auto bp = plan->plan.branching_pattern(ref_seg, conservative != 0);
+        *n_out = bp.size();
+        if (max_out > 0) {
+            need(out, "out");
+        }
+        std::copy_n(bp.begin(), std::min<uint64_t>(bp.size(), max_out), out);
+    });
+}
+
+int lk_prune_run(lk_prune* pr, const float* d_ffa_fold, uint64_t ref_seg,
+                 const float* thresholds, uint64_t n_thresholds, uint64_t n_iters,
+                 lk_prune_stats* stats, uint64_t max_stats, uint64_t* n_stats,
+                 lk_stream_t stream) {
+    return guarded([&] {
+        need(pr, "pr");
+        need(d_ffa_fold, "d_ffa_fold");
+        need(n_stats, "n_stats");
+        if (n_thresholds > 0) {
+            need(thresholds, "thresholds");
+        }
+        const auto st = pr->exec->run(d_ffa_fold, ref_seg, thresholds, n_thresholds, n_iters,
+                                      reinterpret_cast<cudaStream_t>(stream));
+        *n_stats = st.size();
+        if (max_stats > 0) {
+            need(stats, "stats");
+        }
+        std::copy_n(st.begin(), std::min<uint64_t>(st.size(), max_stats), stats);
+    });
+}
+
+int lk_prune_tree_size(const lk_prune* pr, uint64_t* n) {
+    return guarded([&] {
+        need(pr, "pr");
+        need(n, "n");
+        *n = pr->exec->tree_size();
+    });
+}
+
+int lk_prune_get_tree(const lk_prune* pr, double* d_leaves, float* d_folds, float* d_scores,
+                      uint64_t max_out, lk_stream_t stream) {
+    return guarded([&] {
+        need(pr, "pr");
+        lk::require(pr->exec->tree_size() <= max_out, "max_out is smaller than the tree size");
+        pr->exec->copy_tree(d_leaves, d_folds, d_scores, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_taylor_seed(const lk_plan* plan, double* d_leaves, lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(d_leaves, "d_leaves");
+        lk::taylor_seed(plan->plan, d_leaves, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_taylor_branch(const lk_plan* plan, const double* d_leaves, uint64_t n, double scale_cur,
+                     uint64_t branch_max, double* d_out, uint32_t* d_origins, uint64_t max_out,
+                     uint64_t* n_out, lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(n_out, "n_out");
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+        }
+        if (max_out > 0) {
+            need(d_out, "d_out");
+            need(d_origins, "d_origins");
+        }
+        *n_out = lk::taylor_branch(plan->plan, d_leaves, n, scale_cur, branch_max, d_out,
+                                   d_origins, max_out, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_taylor_resolve(const lk_plan* plan, const double* d_leaves, uint64_t n,
+                      const double* coords, uint32_t* d_param_idx, float* d_phase_shift,
+                      lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(coords, "coords");
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+            need(d_param_idx, "d_param_idx");
+            need(d_phase_shift, "d_phase_shift");
+        }
+        lk::taylor_resolve(plan->plan, d_leaves, n, coords, d_param_idx, d_phase_shift,
+                           reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_taylor_transform(const lk_plan* plan, double* d_leaves, uint64_t n_leaves,
+                        const uint32_t* d_indices, uint64_t n, double t_next, double t_cur,
+                        int conservative, lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+            need(d_indices, "d_indices");
+        }
+        lk::taylor_transform(plan->plan, d_leaves, n_leaves, d_indices, n, t_next, t_cur,
+                             conservative != 0, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_shift_add_batch(const float* d_folds_tree, const uint32_t* d_indices_tree,
+                       const float* d_folds_ffa, uint64_t n_ffa, const uint32_t* d_indices_ffa,
+                       const float* d_phase_shift, float* d_folds_out, uint32_t nbins,
+                       uint64_t n, uint64_t physical_start, uint64_t capacity,
+                       lk_stream_t stream) {
+    return guarded([&] {
+        if (n > 0) {
+            need(d_folds_tree, "d_folds_tree");
+            need(d_indices_tree, "d_indices_tree");
+            need(d_folds_ffa, "d_folds_ffa");
+            need(d_indices_ffa, "d_indices_ffa");
+            need(d_phase_shift, "d_phase_shift");
+            need(d_folds_out, "d_folds_out");
+        }
+        lk::shift_add_batch(d_folds_tree, d_indices_tree, d_folds_ffa, n_ffa, d_indices_ffa,
+                            d_phase_shift, d_folds_out, nbins, n, physical_start, capacity,
+                            reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_score_filter(const float* d_folds, uint64_t n, uint32_t nbins, const uint32_t* widths,
+                    uint32_t nwidths, float threshold, float* d_scores, uint32_t* d_indices,
+                    uint64_t* d_count, lk_stream_t stream) {
+    return guarded([&] {
+        need(widths, "widths");
+        need(d_count, "d_count");
+        const auto s = reinterpret_cast<cudaStream_t>(stream);
+        const auto sp = lk::make_score_params(widths, nwidths, nbins);
+        if (n == 0) {
+            LK_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), s));
+            return;
+        }
+        need(d_folds, "d_folds");
+        need(d_scores, "d_scores");
+        need(d_indices, "d_indices");
+        lk::score_folds(d_folds, n, nbins, true, 1.0f, sp, LK_SCORE_MAX, d_scores, s);
+        lk::DeviceBuffer scratch(lk::compact_scratch_bytes(n));
+        lk::DeviceBuffer vals(n * sizeof(float));
+        lk::compact_ge(d_scores, n, threshold, d_indices, vals.as<float>(), n, d_count,
+                       scratch.ptr, s);
+        LK_CUDA(cudaStreamSynchronize(s));
     });
 }
 

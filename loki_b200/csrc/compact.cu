@@ -4,6 +4,7 @@
 // of the counts, per-tile ordered scatter.
 #include <mutex>
 
+#include "lk_block.cuh"
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
 
@@ -15,42 +16,7 @@ constexpr uint32_t kThreads = 1024;
 constexpr uint32_t kPerThread = 4;
 constexpr uint32_t kTile = kThreads * kPerThread;
 
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums,
-                                                         uint32_t* total) {
-    const uint32_t lane = threadIdx.x % 32, warp = threadIdx.x / 32;
-    uint32_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
-        if (static_cast<int>(lane) >= o) {
-            x += t;
-        }
-    }
-    if (lane == 31) {
-        warp_sums[warp] = x;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t nw = blockDim.x / 32;
-        uint32_t y = lane < nw ? warp_sums[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, y, o);
-            if (static_cast<int>(lane) >= o) {
-                y += t;
-            }
-        }
-        if (lane < nw) {
-            warp_sums[lane] = y;  // inclusive
-        }
-    }
-    __syncthreads();
-    const uint32_t before = (warp == 0 ? 0 : warp_sums[warp - 1]) + x - v;
-    if (total != nullptr) {
-        *total = warp_sums[blockDim.x / 32 - 1];
-    }
-    return before;
-}
+using blk::block_exclusive_scan;
 
 __global__ void tile_count_kernel(const float* __restrict__ x, uint64_t n, float thr,
                                   uint32_t* __restrict__ counts) {

@@ -68,6 +68,8 @@ struct Plan {
     double t_ref0() const { return nparams == 1 ? 0.0 : tsegments[0] / 2.0; }
     std::vector<double> param_grid(uint32_t level, uint32_t iparam) const;
     std::vector<double> dparams_at(double tseg_cur, int kind) const;
+    std::vector<double> branching_pattern(uint64_t ref_seg, bool conservative) const;
+    uint64_t prune_branch_max(bool conservative) const;
 };
 
 Plan make_plan(const lk_config& cfg);

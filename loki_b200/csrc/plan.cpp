@@ -92,6 +92,148 @@ std::vector<double> Plan::param_grid(uint32_t level, uint32_t iparam) const {
     return range_param(lim_min(iparam), lim_max(iparam), dparams[level][iparam]);
 }
 
+// core::generate_bp_poly_taylor (lib/taylor.cpp:1643-1741): the average
+// branching factor of each pruning level for a run seeded at ref_seg,
+// weighted over the final level's frequency grid.
+std::vector<double> Plan::branching_pattern(uint64_t ref_seg, bool conservative) const {
+    require(nparams >= 2 && nparams <= 4, "branching pattern needs 2 <= nparams <= 4");
+    const uint32_t L = n_levels - 1;
+    const uint64_t nseg = nsegments[L];
+    require(ref_seg < nseg, "ref_idx must be less than nsegments.");
+    const double tseg = tsegments[L];
+    const uint32_t np = nparams;
+    const std::vector<double> f0 = param_grid(L, np - 1);
+    const uint64_t nf = f0.size();
+    // MiddleOutScheme order and coordinates (lib/loki/psr_utils.hpp:331-448)
+    std::vector<uint64_t> order{ref_seg};
+    for (uint64_t d = 1; order.size() < nseg; ++d) {
+        if (d <= ref_seg) {
+            order.push_back(ref_seg - d);
+        }
+        if (ref_seg + d < nseg && order.size() < nseg) {
+            order.push_back(ref_seg + d);
+        }
+    }
+    auto coord = [&](uint64_t level) {
+        uint64_t mn = order[0], mx = order[0];
+        for (uint64_t i = 1; i <= level; ++i) {
+            mn = std::min(mn, order[i]);
+            mx = std::max(mx, order[i]);
+        }
+        const double ref_val = (static_cast<double>(mn) + static_cast<double>(mx) + 1.0) / 2.0;
+        const double scale_val = ref_val - static_cast<double>(mn);
+        return std::pair<double, double>{ref_val * tseg, scale_val * tseg};
+    };
+    std::vector<double> weights(nf, 1.0), bp(nseg - 1, 0.0);
+    std::vector<double> cur(nf * np), nxt(nf * np, 0.0), dnew(nf * np, 0.0), shift(nf * np, 0.0);
+    std::vector<double> nbr(nf, 1.0), dvec(nf * (np + 1), 0.0);
+    for (uint64_t i = 0; i < nf; ++i) {
+        for (uint32_t j = 0; j < np; ++j) {
+            cur[i * np + j] = dparams_actual[L][j];
+        }
+        cur[i * np + np - 1] = cur[i * np + np - 1] * (kCval / f0[i]);
+    }
+    const double nbins_d = static_cast<double>(cfg.nbins);
+    for (uint64_t level = 1; level < nseg; ++level) {
+        const auto cn = coord(level);
+        const auto cc = std::pair<double, double>{coord(level - 1).first, coord(level).second};
+        const double tobs = cc.second;
+        // psr_utils::poly_taylor_step_d_vec with t_ref = 0 (lib/psr_utils.cpp:62-80)
+        const std::vector<double> df = poly_taylor_step_f(np, tobs, cfg.nbins, cfg.eta, 0.0);
+        for (uint64_t i = 0; i < nf; ++i) {
+            const double factor = kCval / f0[i];
+            for (uint32_t j = 0; j < np; ++j) {
+                dnew[i * np + j] = df[j] * factor;
+            }
+        }
+        // psr_utils::poly_taylor_shift_d_vec (lib/psr_utils.cpp:116-154)
+        std::vector<double> dtp(np), fac(np);
+        double dtpow = tobs;
+        for (uint32_t i = 0; i < np; ++i) {
+            dtp[i] = dtpow;
+            fac[i] = factorial_d(static_cast<double>(i + 1));
+            dtpow *= tobs;
+        }
+        for (uint32_t i = 0; i < np; ++i) {
+            const uint32_t k = np - 1 - i;
+            const double factor_base = dtp[k] * nbins_d / fac[k];
+            const double factor_opt = factor_base / std::pow(2.0, k);
+            const double scale = factor_opt / kCval;
+            for (uint64_t b = 0; b < nf; ++b) {
+                const uint64_t idx = b * np + i;
+                shift[idx] = std::abs(cur[idx] - dnew[idx]) * scale * f0[b];
+            }
+        }
+        std::fill(nbr.begin(), nbr.end(), 1.0);
+        for (uint64_t i = 0; i < nf; ++i) {
+            for (uint32_t j = 0; j < np; ++j) {
+                const uint64_t idx = i * np + j;
+                if (shift[idx] < (cfg.eta - kFloatEps)) {
+                    nxt[idx] = cur[idx];
+                    continue;
+                }
+                const double ratio = cur[idx] / dnew[idx];
+                const double c = std::ceil(ratio - kFloatEps);
+                const uint64_t num = c < 1.0 ? 1 : static_cast<uint64_t>(c);
+                nbr[i] *= static_cast<double>(num);
+                nxt[idx] = cur[idx] / static_cast<double>(num);
+            }
+        }
+        double children = 0.0, parents = 0.0;
+        for (uint64_t i = 0; i < nf; ++i) {
+            children += weights[i] * nbr[i];
+            parents += weights[i];
+            weights[i] *= nbr[i];
+        }
+        bp[level - 1] = children / parents;
+        // transforms::shift_taylor_errors_batch (lib/transforms.cpp:55-98)
+        const double delta_t = cn.first - cc.first;
+        const uint32_t npd = np + 1;
+        for (uint64_t i = 0; i < nf; ++i) {
+            for (uint32_t j = 0; j < np; ++j) {
+                dvec[i * npd + j] = nxt[i * np + j];
+            }
+        }
+        if (!conservative) {
+            for (uint64_t i = 0; i < nf; ++i) {
+                for (uint32_t j = 0; j < np; ++j) {
+                    cur[i * np + j] = dvec[i * npd + j];
+                }
+            }
+        } else {
+            std::vector<double> tsq(npd * npd, 0.0);
+            for (uint32_t i = 0; i < npd; ++i) {
+                for (uint32_t j = 0; j <= i; ++j) {
+                    const uint32_t k = i - j;
+                    const double t = std::pow(delta_t, k) / factorial_d(static_cast<double>(k));
+                    tsq[i * npd + j] = t * t;
+                }
+            }
+            for (uint64_t b = 0; b < nf; ++b) {
+                for (uint32_t i = 0; i < np; ++i) {
+                    double sum = 0.0;
+                    for (uint32_t j = 0; j <= i; ++j) {
+                        const double e = dvec[b * npd + j];
+                        sum += e * e * tsq[i * npd + j];
+                    }
+                    cur[b * np + i] = std::sqrt(sum);
+                }
+            }
+        }
+    }
+    return bp;
+}
+
+// EPMultiPass's branch_max (lib/prune.cpp:648-651): the pattern of ref_seg 0.
+uint64_t Plan::prune_branch_max(bool conservative) const {
+    const std::vector<double> bp = branching_pattern(0, conservative);
+    double mx = bp.empty() ? 0.0 : bp[0];
+    for (double v : bp) {
+        mx = std::max(mx, v);
+    }
+    return std::max<uint64_t>(static_cast<uint64_t>(std::ceil(mx * 2)), 32);
+}
+
 // PulsarSearchConfig::get_dparams / get_dparams_f / get_dparams_actual
 // (lib/configs.cpp:152-174).
 std::vector<double> Plan::dparams_at(double tseg_cur, int kind) const {

@@ -1,0 +1,1492 @@
+// Pruning leaf step on the GPU: seed, branch, resolve, shift-add, score and
+// filter, transform, and the world-tree update of one pruning level, for
+// Taylor-basis searches with nparams 2 (accel) or 3 (jerk).
+//
+// Reference: PruneImpl::initialize / execute_iteration_batched
+// (lib/prune.cpp:181-226,429-620) over the Taylor PruneDPFuncts
+// (lib/dynamic.cpp:155-310, lib/taylor.cpp:24-314,492-619,881-1005,
+// 1197-1257), kernels::shift_add_linear_batch (lib/kernels.cpp:1328-1355),
+// score_and_filter_max_with_cache (lib/score.cpp:213-259) and the WorldTree
+// circular buffer (lib/world_tree.cpp:237-276,361-422,557-669).
+//
+// The reference walks a level in batches of `batch_size` parents and, per
+// batch, branches, scores, filters with the current threshold and adds the
+// survivors to the world tree, whose overload pruning can raise that
+// threshold for the batches that follow. Here, the work that does not depend
+// on the threshold is done for the whole level at once:
+//   1. branch_count / scan / branch_emit: every parent's children, in parent
+//      order (the reference's concatenated batch outputs);
+//   2. leaf_kernel: resolve, shift-add and max-width S/N of every child, one
+//      child per thread for the FP64 and scoring parts and one warp per
+//      child for the fold rows; folds are kept only for children at or above
+//      the level's starting threshold, the lowest threshold any batch uses.
+// The threshold-dependent part keeps the reference's batch semantics exactly:
+// the host replays the WorldTree bookkeeping (sizes, space left, batch
+// boundaries at the circular buffer's wrap) from per-batch pass counts, and
+// the device holds the write region as an ordered list of (child, score).
+// Runs of batches that fit are appended with one ordered compaction; a batch
+// that overflows runs the reference's overload step on the device (exact
+// order statistics by radix select, threshold = max(current, next above the
+// k-th, next above the selected median), prune the list by score >
+// threshold, append the batch's children >= threshold up to the space left).
+// At the end of the level the surviving children are transformed and
+// gathered into the other of two tree buffers at the reference's physical
+// slots, so the next level's batch boundaries match the reference's.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lk_block.cuh"
+#include "lk_device.cuh"
+#include "lk_prune.hpp"
+#include "lk_score.cuh"
+
+namespace lk {
+
+namespace {
+
+constexpr uint32_t kWarp = 32;
+constexpr uint32_t kScanThreads = 1024;
+constexpr uint32_t kScanPer = 4;
+constexpr uint32_t kScanTile = kScanThreads * kScanPer;
+
+// Status bits (beside those of lk_device.cuh).
+constexpr uint32_t kStatusBranchMax = 1u << 8;   // a parameter needs > branch_max points
+constexpr uint32_t kStatusZeroStep = 1u << 9;    // non-positive step size when branching
+constexpr uint32_t kStatusBranchCount = 1u << 10;  // children of one parent exceed 2^32-1
+
+// Grid geometry of one search, by value in kernel arguments.
+struct LeafGeom {
+    uint32_t np;       // 2 (accel, freq) or 3 (jerk, accel, freq)
+    uint32_t nbins;
+    uint32_t ls;       // doubles per leaf: (np + 2) * 2
+    uint32_t n_accel;  // final FFA level counts used by resolve
+    uint32_t n_freq;
+    double eta;
+    double a_min, a_max, f_min, f_max;
+    uint64_t branch_max;
+};
+
+// Per-parameter branching of one parent: values base + i * step (i < count)
+// when `split`, else the parent value itself.
+struct ParamBranch {
+    double cur, first, act, dparam;
+    uint32_t count;
+    bool split;
+};
+
+// poly_taylor_branch_{accel,jerk}_batch steps and shifts (lib/taylor.cpp:
+// 64-85, 199-227), then branch_one_param_padded / branch_param_padded
+// (lib/loki/psr_utils.hpp:189-211, lib/psr_utils.cpp:226-259). Plain
+// double operators are IEEE round-to-nearest here (the library is built
+// with -fmad=false), in the reference's association.
+__device__ void branch_params(const double* lf, double dt, const LeafGeom& g, ParamBranch* pb,
+                              uint32_t* status) {
+    const double nbins_d = static_cast<double>(g.nbins);
+    const double dphi = g.eta / nbins_d;
+    const double dt2 = dt * dt;
+    const double inv_dt = 1.0 / dt;
+    const double inv_dt2 = inv_dt * inv_dt;
+    const double f0 = lf[(g.np + 1) * 2];
+    const double dfactor = kCval / f0;
+    double sig_new[3], shift[3];
+    if (g.np == 2) {
+        sig_new[0] = dphi * dfactor * 4.0 * inv_dt2;
+        sig_new[1] = dphi * dfactor * 1.0 * inv_dt;
+        shift[0] = fabs(lf[1] - sig_new[0]) * dt2 * nbins_d / (4.0 * dfactor);
+        shift[1] = fabs(lf[3] - sig_new[1]) * dt * nbins_d / (1.0 * dfactor);
+    } else {
+        const double dt3 = dt2 * dt;
+        const double inv_dt3 = inv_dt2 * inv_dt;
+        sig_new[0] = dphi * dfactor * 24.0 * inv_dt3;
+        sig_new[1] = dphi * dfactor * 4.0 * inv_dt2;
+        sig_new[2] = dphi * dfactor * 1.0 * inv_dt;
+        shift[0] = fabs(lf[1] - sig_new[0]) * dt3 * nbins_d / (24.0 * dfactor);
+        shift[1] = fabs(lf[3] - sig_new[1]) * dt2 * nbins_d / (4.0 * dfactor);
+        shift[2] = fabs(lf[5] - sig_new[2]) * dt * nbins_d / (1.0 * dfactor);
+    }
+    for (uint32_t k = 0; k < g.np; ++k) {
+        ParamBranch& b = pb[k];
+        const double cur = lf[2 * k], sig_cur = lf[2 * k + 1];
+        b.cur = cur;
+        if (!(shift[k] >= (g.eta - kFloatEps))) {
+            b.split = false;
+            b.count = 1;
+            b.dparam = sig_cur;
+            b.first = cur;
+            b.act = 0.0;
+            continue;
+        }
+        b.split = true;
+        if (sig_cur <= 1e-12 || sig_new[k] <= 1e-12) {  // utils::kZeroEps
+            atomicOr(status, kStatusZeroStep);
+            b.count = 1;
+            b.dparam = sig_cur;
+            b.first = cur;
+            b.act = 0.0;
+            continue;
+        }
+        const double ratio = sig_cur / sig_new[k];
+        const double c = ceil(ratio - kFloatEps);
+        uint64_t num = c < 1.0 ? 1 : static_cast<uint64_t>(c);
+        if (num > g.branch_max) {
+            atomicOr(status, kStatusBranchMax);
+            num = 1;
+        }
+        const double act = sig_cur / static_cast<double>(num);
+        const double parent_min = cur - (sig_cur / 2.0);
+        b.first = parent_min + (act / 2.0);
+        b.act = act;
+        b.dparam = act;
+        b.count = static_cast<uint32_t>(num);
+    }
+}
+
+__device__ __forceinline__ double branch_value(const ParamBranch& b, uint32_t i) {
+    return b.split ? b.first + (static_cast<double>(i) * b.act) : b.cur;
+}
+
+__global__ void branch_count_kernel(const double* __restrict__ tree_leaves, uint64_t head,
+                                    uint64_t cap, uint64_t n, double dt, LeafGeom g,
+                                    uint32_t* __restrict__ counts, uint32_t* status) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const double* lf = tree_leaves + ((head + i) % cap) * g.ls;
+    ParamBranch pb[3];
+    branch_params(lf, dt, g, pb, status);
+    uint64_t prod = 1;
+    for (uint32_t k = 0; k < g.np; ++k) {
+        prod *= pb[k].count;
+    }
+    if (prod > 0xffffffffull) {
+        atomicOr(status, kStatusBranchCount);
+        prod = 1;
+    }
+    counts[i] = static_cast<uint32_t>(prod);
+}
+
+// Children of parent i at offsets[i]..: Cartesian product with the highest
+// derivative outermost (lib/taylor.cpp:131-157, 282-311); d0 and f0 copied
+// from the parent.
+__global__ void branch_emit_kernel(const double* __restrict__ tree_leaves, uint64_t head,
+                                   uint64_t cap, uint64_t n, double dt, LeafGeom g,
+                                   const uint64_t* __restrict__ offsets,
+                                   double* __restrict__ out, uint32_t* __restrict__ parent,
+                                   uint32_t* status) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const double* lf = tree_leaves + ((head + i) % cap) * g.ls;
+    ParamBranch pb[3];
+    branch_params(lf, dt, g, pb, status);
+    uint64_t o = offsets[i];
+    const uint32_t c2 = g.np == 3 ? pb[2].count : 1;
+    for (uint32_t a = 0; a < pb[0].count; ++a) {
+        const double va = branch_value(pb[0], a);
+        for (uint32_t b = 0; b < pb[1].count; ++b) {
+            const double vb = branch_value(pb[1], b);
+            for (uint32_t c = 0; c < c2; ++c) {
+                double* d = out + o * g.ls;
+                d[0] = va;
+                d[1] = pb[0].dparam;
+                d[2] = vb;
+                d[3] = pb[1].dparam;
+                if (g.np == 3) {
+                    d[4] = branch_value(pb[2], c);
+                    d[5] = pb[2].dparam;
+                }
+                for (uint32_t q = 2 * g.np; q < g.ls; ++q) {
+                    d[q] = lf[q];
+                }
+                parent[o] = static_cast<uint32_t>(i);
+                ++o;
+            }
+        }
+    }
+}
+
+// core::poly_taylor_seed (lib/taylor.cpp:1197-1257): leaf (ia, jf) of the
+// final FFA level grid, accel-major.
+__global__ void seed_kernel(LeafGeom g, double dp0, double dp1, double dfreq, double* out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t n = static_cast<uint64_t>(g.n_accel) * g.n_freq;
+    if (i >= n) {
+        return;
+    }
+    const uint64_t ia = i / g.n_freq, jf = i - ia * g.n_freq;
+    const double accel = dev::param_val_at_idx(g.a_min, g.a_max, g.n_accel, ia);
+    const double freq = dev::param_val_at_idx(g.f_min, g.f_max, g.n_freq, jf);
+    double* o = out + i * g.ls;
+    const uint32_t np = g.np;
+    const double dps[2] = {dp0, dp1};
+    for (uint32_t j = 0; j + 1 < np; ++j) {
+        o[j * 2 + 0] = 0;
+        o[j * 2 + 1] = dps[j];
+    }
+    o[(np - 2) * 2 + 0] = accel;
+    o[(np - 1) * 2 + 0] = 0;
+    o[(np - 1) * 2 + 1] = dfreq * (kCval / freq);
+    o[np * 2 + 0] = 0;
+    o[np * 2 + 1] = 0;
+    o[(np + 1) * 2 + 0] = freq;
+    o[(np + 1) * 2 + 1] = 0;
+}
+
+// ---- exclusive scan of uint32 counts into uint64 offsets -------------------
+
+__global__ void scan_tile_sums_kernel(const uint32_t* __restrict__ x, uint64_t n,
+                                      uint32_t* __restrict__ sums) {
+    __shared__ uint32_t ws[32];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < kScanPer; ++q) {
+        c += (base + q < n) ? x[base + q] : 0u;
+    }
+    uint32_t total;
+    blk::block_exclusive_scan(c, ws, &total);
+    if (threadIdx.x == 0) {
+        sums[blockIdx.x] = total;
+    }
+}
+
+// Single block: exclusive scan of per-tile sums (uint32 each) into uint64.
+__global__ void scan_tiles_kernel(const uint32_t* __restrict__ sums, uint64_t ntiles,
+                                  uint64_t* __restrict__ offs, uint64_t* __restrict__ d_total) {
+    __shared__ uint32_t ws[32];
+    __shared__ uint64_t carry;
+    if (threadIdx.x == 0) {
+        carry = 0;
+    }
+    __syncthreads();
+    for (uint64_t c0 = 0; c0 < ntiles; c0 += blockDim.x) {
+        const uint64_t i = c0 + threadIdx.x;
+        const uint32_t v = i < ntiles ? sums[i] : 0;
+        uint32_t total;
+        const uint32_t before = blk::block_exclusive_scan(v, ws, &total);
+        if (i < ntiles) {
+            offs[i] = carry + before;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry += total;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *d_total = carry;
+    }
+}
+
+__global__ void scan_apply_kernel(const uint32_t* __restrict__ x, uint64_t n,
+                                  const uint64_t* __restrict__ tile_offs,
+                                  uint64_t* __restrict__ out) {
+    __shared__ uint32_t ws[32];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
+    uint32_t v[kScanPer];
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < kScanPer; ++q) {
+        v[q] = (base + q < n) ? x[base + q] : 0u;
+        c += v[q];
+    }
+    uint64_t pos = tile_offs[blockIdx.x] + blk::block_exclusive_scan(c, ws, nullptr);
+#pragma unroll
+    for (uint32_t q = 0; q < kScanPer; ++q) {
+        if (base + q < n) {
+            out[base + q] = pos;
+        }
+        pos += v[q];
+    }
+}
+
+// Child offsets at the batch boundaries (parent index -> first child).
+__global__ void batch_child_starts_kernel(const uint64_t* __restrict__ offsets, uint64_t n,
+                                          const uint64_t* __restrict__ d_total,
+                                          const uint64_t* __restrict__ parent_starts,
+                                          uint64_t nb1, uint64_t* __restrict__ child_starts) {
+    const uint64_t b = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (b < nb1) {
+        const uint64_t p = parent_starts[b];
+        child_starts[b] = p < n ? offsets[p] : *d_total;
+    }
+}
+
+// ---- resolve + shift-add + score ------------------------------------------
+
+// poly_taylor_resolve_{accel,jerk}_batch (lib/taylor.cpp:492-619).
+struct ResolveConsts {
+    double dt;          // dt_add - dt_init
+    double dt_add;      // t_add - t_cur (jerk's a_new)
+    double half_dt2;
+    double sixth_dt3;   // jerk only
+};
+
+__device__ __forceinline__ void resolve_leaf(const double* lf, const LeafGeom& g,
+                                             const ResolveConsts& rc, uint32_t* pidx,
+                                             float* phase) {
+    if (g.np == 2) {
+        const double a_cur = lf[0], v_cur = lf[2], f0 = lf[6];
+        const double a_new = a_cur;
+        const double delta_v = a_cur * rc.dt;
+        const double delta_d = (v_cur * rc.dt) + (a_cur * rc.half_dt2);
+        const double f_new = f0 * (1.0 - (delta_v * kInvCval));
+        const double delay_rel = delta_d * kInvCval;
+        const uint32_t ia = dev::nearest_idx(a_new, g.a_min, g.a_max, g.n_accel);
+        const uint32_t jf = dev::nearest_idx(f_new, g.f_min, g.f_max, g.n_freq);
+        *pidx = ia * g.n_freq + jf;
+        *phase = dev::phase_idx(rc.dt, f0, g.nbins, delay_rel);
+    } else {
+        const double j_cur = lf[0], a_cur = lf[2], v_cur = lf[4], f0 = lf[8];
+        const double a_new = a_cur + (j_cur * rc.dt_add);
+        const double delta_v = (a_cur * rc.dt) + (j_cur * rc.half_dt2);
+        const double delta_d = (v_cur * rc.dt) + (a_cur * rc.half_dt2) + (j_cur * rc.sixth_dt3);
+        const double f_new = f0 * (1.0 - (delta_v * kInvCval));
+        const double delay_rel = delta_d * kInvCval;
+        *phase = dev::phase_idx(rc.dt, f0, g.nbins, delay_rel);
+        const uint32_t ia = dev::nearest_idx(a_new, g.a_min, g.a_max, g.n_accel);
+        const uint32_t jf = dev::nearest_idx(f_new, g.f_min, g.f_max, g.n_freq);
+        *pidx = ia * g.n_freq + jf;
+    }
+}
+
+// Orderable uint32 key of a float: larger float <-> larger key.
+__device__ __forceinline__ uint32_t fkey(float x) {
+    const uint32_t u = __float_as_uint(x);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float fkey_inv(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// One block scores T consecutive children. Phase 0 (thread per child):
+// resolve in FP64. Phase 1 (warp per child): tree fold + rotated FFA fold,
+// normalised into shared memory (kernels::shift_add_linear_with_buffer,
+// lib/kernels.cpp:118-146: out[j] = tree[j] + ffa[(j - s) mod nbins]).
+// Phase 2 (thread per child): the reference's sequential prefix sum and
+// width maxima. Phase 3 (warp per child): children scoring at or above
+// thr_keep get their fold written for the world tree.
+template <int NW>
+__global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* __restrict__ parent,
+                            uint64_t n, const float* __restrict__ tree_folds, uint64_t head,
+                            uint64_t cap, const float* __restrict__ ffa_seg, LeafGeom g,
+                            ResolveConsts rc, uint32_t rs, ScoreParams sp, float thr_keep,
+                            float* __restrict__ scores, float* __restrict__ folds_out,
+                            uint32_t* __restrict__ minmax) {
+    extern __shared__ float rows[];
+    const uint32_t T = blockDim.x;
+    uint32_t* s_pidx = reinterpret_cast<uint32_t*>(rows + static_cast<size_t>(T) * rs);
+    uint32_t* s_shift = s_pidx + T;
+    uint32_t* s_tree = s_shift + T;
+    uint32_t* s_keep = s_tree + T;
+    __shared__ uint32_t s_min, s_max;
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * T;
+    const uint32_t nhere = static_cast<uint32_t>((n - c0) < T ? (n - c0) : T);
+    const uint32_t nb = g.nbins;
+    if (threadIdx.x == 0) {
+        s_min = 0xffffffffu;
+        s_max = 0u;
+    }
+    if (threadIdx.x < nhere) {
+        const uint64_t c = c0 + threadIdx.x;
+        uint32_t pidx;
+        float phase;
+        resolve_leaf(leaves + c * g.ls, g, rc, &pidx, &phase);
+        s_pidx[threadIdx.x] = pidx;
+        s_shift[threadIdx.x] = dev::shift_bins(phase, nb);
+        s_tree[threadIdx.x] = static_cast<uint32_t>((head + parent[c]) % cap);
+    }
+    __syncthreads();
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+        const float* tail = tree_folds + static_cast<uint64_t>(s_tree[p]) * 2 * nb;
+        const float* hd = ffa_seg + static_cast<uint64_t>(s_pidx[p]) * 2 * nb;
+        const uint32_t s = s_shift[p];
+        float* dst = rows + static_cast<size_t>(p) * rs;
+        for (uint32_t j = lane; j < nb; j += kWarp) {
+            const uint32_t jh = j >= s ? j - s : j + nb - s;
+            const float e = __fadd_rn(__ldg(tail + j), __ldg(hd + jh));
+            const float v = __fadd_rn(__ldg(tail + nb + j), __ldg(hd + nb + jh));
+            dst[j] = sc::normalise(e, v);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nhere) {
+        const uint64_t c = c0 + threadIdx.x;
+        float score;
+        sc::score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nb, 1.0f, sp,
+                          LK_SCORE_MAX, &score);
+        scores[c] = score;
+        s_keep[threadIdx.x] = score >= thr_keep ? 1u : 0u;
+        const uint32_t k = fkey(score);
+        atomicMin(&s_min, k);
+        atomicMax(&s_max, k);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && nhere > 0) {
+        atomicMin(&minmax[0], s_min);
+        atomicMax(&minmax[1], s_max);
+    }
+    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+        if (s_keep[p] == 0) {
+            continue;
+        }
+        const float* tail = tree_folds + static_cast<uint64_t>(s_tree[p]) * 2 * nb;
+        const float* hd = ffa_seg + static_cast<uint64_t>(s_pidx[p]) * 2 * nb;
+        const uint32_t s = s_shift[p];
+        float* o = folds_out + (c0 + p) * 2 * nb;
+        for (uint32_t j = lane; j < nb; j += kWarp) {
+            const uint32_t jh = j >= s ? j - s : j + nb - s;
+            o[j] = __fadd_rn(__ldg(tail + j), __ldg(hd + jh));
+            o[nb + j] = __fadd_rn(__ldg(tail + nb + j), __ldg(hd + nb + jh));
+        }
+    }
+}
+
+// ---- threshold-dependent steps --------------------------------------------
+
+// Children of batch b (child_starts[b0 + b] .. child_starts[b0 + b + 1]) with
+// score >= *d_thr (score_and_filter's test, lib/score.cpp:250).
+__global__ void batch_count_kernel(const float* __restrict__ scores,
+                                   const uint64_t* __restrict__ child_starts, uint64_t b0,
+                                   const float* __restrict__ d_thr,
+                                   uint32_t* __restrict__ counts) {
+    __shared__ uint32_t ws[32];
+    const uint64_t b = b0 + blockIdx.x;
+    const uint64_t lo = child_starts[b], hi = child_starts[b + 1];
+    const float thr = *d_thr;
+    uint32_t c = 0;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        c += scores[i] >= thr ? 1u : 0u;
+    }
+    uint32_t total;
+    blk::block_exclusive_scan(c, ws, &total);
+    if (threadIdx.x == 0) {
+        counts[blockIdx.x] = total;
+    }
+}
+
+// Ordered compaction of (id, score) pairs. Source kind CHILDREN: ids are
+// base + i and scores scores[base + i]; kind LIST: ids[i], scores[i].
+// Predicate: score >= *d_thr (GT = false) or score > *d_thr (GT = true).
+enum class Src { kChildren, kList };
+
+template <Src S>
+__device__ __forceinline__ void pc_load(const float* sc, const uint32_t* ids, uint64_t base,
+                                        uint64_t i, float* s, uint32_t* id) {
+    if constexpr (S == Src::kChildren) {
+        *s = sc[base + i];
+        *id = static_cast<uint32_t>(base + i);
+    } else {
+        *s = sc[i];
+        *id = ids[i];
+    }
+}
+
+template <bool GT>
+__device__ __forceinline__ bool pc_pred(float s, float thr) {
+    return GT ? (s > thr) : (s >= thr);
+}
+
+template <Src S, bool GT>
+__global__ void pc_count_kernel(const float* __restrict__ sc, const uint32_t* __restrict__ ids,
+                                uint64_t base, uint64_t n, const float* __restrict__ d_thr,
+                                uint32_t* __restrict__ tile_counts) {
+    __shared__ uint32_t ws[32];
+    const float thr = *d_thr;
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < kScanPer; ++q) {
+        if (t0 + q < n) {
+            float s;
+            uint32_t id;
+            pc_load<S>(sc, ids, base, t0 + q, &s, &id);
+            c += pc_pred<GT>(s, thr) ? 1u : 0u;
+        }
+    }
+    uint32_t total;
+    blk::block_exclusive_scan(c, ws, &total);
+    if (threadIdx.x == 0) {
+        tile_counts[blockIdx.x] = total;
+    }
+}
+
+// Writes kept pairs at *d_base + rank, skipping ranks at or beyond
+// limit - *d_base (the reference's min(pending, space_left)).
+template <Src S, bool GT>
+__global__ void pc_scatter_kernel(const float* __restrict__ sc, const uint32_t* __restrict__ ids,
+                                  uint64_t base, uint64_t n, const float* __restrict__ d_thr,
+                                  const uint64_t* __restrict__ tile_offs,
+                                  const uint64_t* __restrict__ d_base, uint64_t limit,
+                                  uint32_t* __restrict__ out_ids, float* __restrict__ out_sc) {
+    __shared__ uint32_t ws[32];
+    const float thr = *d_thr;
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanPer;
+    float s[kScanPer];
+    uint32_t id[kScanPer];
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < kScanPer; ++q) {
+        s[q] = 0.0f;
+        id[q] = 0;
+        if (t0 + q < n) {
+            pc_load<S>(sc, ids, base, t0 + q, &s[q], &id[q]);
+        }
+        c += (t0 + q < n && pc_pred<GT>(s[q], thr)) ? 1u : 0u;
+    }
+    uint64_t pos = *d_base + tile_offs[blockIdx.x] + blk::block_exclusive_scan(c, ws, nullptr);
+#pragma unroll
+    for (uint32_t q = 0; q < kScanPer; ++q) {
+        if (t0 + q < n && pc_pred<GT>(s[q], thr)) {
+            if (pos < limit) {
+                out_ids[pos] = id[q];
+                out_sc[pos] = s[q];
+            }
+            ++pos;
+        }
+    }
+}
+
+// *d_size_out = min(*d_base + *d_total, limit).
+__global__ void pc_finish_kernel(const uint64_t* d_base, const uint64_t* d_total, uint64_t limit,
+                                 uint64_t* d_size_out) {
+    const uint64_t v = *d_base + *d_total;
+    *d_size_out = v < limit ? v : limit;
+}
+
+// WorldTree::get_prune_threshold (lib/world_tree.cpp:570-618) on the
+// candidates {list scores} U {children of one batch with score >= *d_thr}:
+// N of them, K = size + space_left. The reference's two nth_element calls
+// select fixed order statistics: with D sorted in descending order, the
+// top-k value D[K-1] and the median value D[K-1-N/2] when N/2 <= K-1, else
+// D[N-1-N/2+K]. Both are found exactly by an 8-bit MSD radix select over
+// orderable keys (one block, four passes). The new threshold
+// max(current, nextafter(topk), nextafter(median)) replaces *d_thr.
+__global__ void select_threshold_kernel(const float* __restrict__ list_sc, uint64_t size,
+                                        const float* __restrict__ scores, uint64_t cb0,
+                                        uint64_t cb1, uint64_t N, uint64_t r_topk,
+                                        uint64_t r_med, float* d_thr, float* d_debug) {
+    __shared__ uint32_t hist[2][256];
+    __shared__ uint32_t prefix[2];
+    __shared__ uint64_t q[2];
+    const float thr = *d_thr;
+    if (threadIdx.x < 2) {
+        prefix[threadIdx.x] = 0;
+        // ascending rank of the wanted descending rank
+        q[threadIdx.x] = N - 1 - (threadIdx.x == 0 ? r_topk : r_med);
+    }
+    for (int pass = 0; pass < 4; ++pass) {
+        const uint32_t shift = 24u - 8u * static_cast<uint32_t>(pass);
+        const uint32_t hmask = pass == 0 ? 0u : (0xffffffffu << (shift + 8u));
+        for (uint32_t i = threadIdx.x; i < 512; i += blockDim.x) {
+            hist[i / 256][i % 256] = 0;
+        }
+        __syncthreads();
+        const uint32_t p0 = prefix[0] & hmask, p1 = prefix[1] & hmask;
+        for (uint64_t i = threadIdx.x; i < size; i += blockDim.x) {
+            const uint32_t k = fkey(list_sc[i]);
+            const uint32_t d = (k >> shift) & 0xffu;
+            if ((k & hmask) == p0) atomicAdd(&hist[0][d], 1u);
+            if ((k & hmask) == p1) atomicAdd(&hist[1][d], 1u);
+        }
+        for (uint64_t c = cb0 + threadIdx.x; c < cb1; c += blockDim.x) {
+            const float s = scores[c];
+            if (s >= thr) {
+                const uint32_t k = fkey(s);
+                const uint32_t d = (k >> shift) & 0xffu;
+                if ((k & hmask) == p0) atomicAdd(&hist[0][d], 1u);
+                if ((k & hmask) == p1) atomicAdd(&hist[1][d], 1u);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 2) {
+            const uint32_t r = threadIdx.x;
+            uint64_t acc = 0;
+            uint32_t d = 0;
+            for (; d < 255; ++d) {
+                if (q[r] < acc + hist[r][d]) {
+                    break;
+                }
+                acc += hist[r][d];
+            }
+            q[r] -= acc;
+            prefix[r] |= d << shift;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float topk = nextafterf(fkey_inv(prefix[0]), FLT_MAX);
+        const float med = nextafterf(fkey_inv(prefix[1]), FLT_MAX);
+        float eff = thr;
+        eff = (eff < topk) ? topk : eff;
+        eff = (eff < med) ? med : eff;
+        *d_thr = eff;
+        if (d_debug != nullptr) {
+            d_debug[0] = fkey_inv(prefix[0]);
+            d_debug[1] = fkey_inv(prefix[1]);
+        }
+    }
+    (void)N;
+}
+
+// Level end: transform (poly_taylor_transform_{accel,jerk}_batch,
+// lib/taylor.cpp:881-1005) and gather the survivors into the tree at
+// physical slots (write_start + i) mod cap. One warp per survivor.
+struct TransformConsts {
+    double dt, half_dt2, sixth_dt3, dt2;
+    int conservative;
+};
+
+__device__ __forceinline__ void transform_leaf(const double* in, double* o, uint32_t np,
+                                               const TransformConsts& tc) {
+    const double dt = tc.dt;
+    if (np == 2) {
+        const double d2v = in[0], d2e = in[1], d1v = in[2], d1e = in[3], d0v = in[4],
+                     d0e = in[5];
+        const double d1v_j = d1v + (d2v * dt);
+        const double d0v_j = d0v + (d1v * dt) + (d2v * tc.half_dt2);
+        const double d1e_j =
+            tc.conservative ? __dsqrt_rn((d1e * d1e) + (d2e * d2e * dt * dt)) : d1e;
+        o[0] = d2v;
+        o[1] = d2e;
+        o[2] = d1v_j;
+        o[3] = d1e_j;
+        o[4] = d0v_j;
+        o[5] = d0e;
+        o[6] = in[6];
+        o[7] = in[7];
+    } else {
+        const double d3v = in[0], d3e = in[1], d2v = in[2], d2e = in[3], d1v = in[4],
+                     d1e = in[5], d0v = in[6], d0e = in[7];
+        const double d2v_j = d2v + (d3v * dt);
+        const double d1v_j = d1v + (d2v * dt) + (d3v * tc.half_dt2);
+        const double d0v_j = d0v + (d1v * dt) + (d2v * tc.half_dt2) + (d3v * tc.sixth_dt3);
+        double d2e_j = d2e, d1e_j = d1e;
+        if (tc.conservative) {
+            d2e_j = __dsqrt_rn((d2e * d2e) + (d3e * d3e * tc.dt2));
+            d1e_j = __dsqrt_rn((d1e * d1e) + (d2e * d2e * tc.dt2) +
+                               (d3e * d3e * tc.half_dt2 * tc.half_dt2));
+        }
+        o[0] = d3v;
+        o[1] = d3e;
+        o[2] = d2v_j;
+        o[3] = d2e_j;
+        o[4] = d1v_j;
+        o[5] = d1e_j;
+        o[6] = d0v_j;
+        o[7] = d0e;
+        o[8] = in[8];
+        o[9] = in[9];
+    }
+}
+
+__global__ void gather_kernel(const uint32_t* __restrict__ list_ids,
+                              const float* __restrict__ list_sc, uint64_t size,
+                              const double* __restrict__ leaves, const float* __restrict__ folds,
+                              uint64_t write_start, uint64_t cap, uint32_t np, uint32_t nbins,
+                              TransformConsts tc, double* __restrict__ t_leaves,
+                              float* __restrict__ t_folds, float* __restrict__ t_scores) {
+    const uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
+    const uint32_t lane = threadIdx.x % kWarp;
+    if (w >= size) {
+        return;
+    }
+    const uint64_t c = list_ids[w];
+    const uint64_t ph = (write_start + w) % cap;
+    const uint32_t ls = (np + 2) * 2;
+    if (lane == 0) {
+        transform_leaf(leaves + c * ls, t_leaves + ph * ls, np, tc);
+        t_scores[ph] = list_sc[w];
+    }
+    const float* src = folds + c * 2 * nbins;
+    float* dst = t_folds + ph * 2 * nbins;
+    for (uint32_t j = lane; j < 2 * nbins; j += kWarp) {
+        dst[j] = src[j];
+    }
+}
+
+// In-place transform of leaves named by indices (the standalone entry
+// point); an index at or beyond n_leaves is skipped and flagged.
+__global__ void transform_kernel(double* __restrict__ leaves, uint64_t n_leaves,
+                                 const uint32_t* __restrict__ idx, uint64_t n, uint32_t np,
+                                 TransformConsts tc, uint32_t* status) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    if (idx[i] >= n_leaves) {
+        atomicOr(status, dev::kStatusBadTable);
+        return;
+    }
+    double* lf = leaves + static_cast<uint64_t>(idx[i]) * (np + 2) * 2;
+    double tmp[10];
+    transform_leaf(lf, tmp, np, tc);
+    for (uint32_t q = 0; q < (np + 2) * 2; ++q) {
+        lf[q] = tmp[q];
+    }
+}
+
+__global__ void set_f32_kernel(float* p, float v) { *p = v; }
+__global__ void set_u64_kernel(uint64_t* p, uint64_t v) { *p = v; }
+__global__ void init_minmax_kernel(uint32_t* mm) {
+    mm[0] = 0xffffffffu;
+    mm[1] = 0u;
+}
+
+}  // namespace
+
+namespace {
+
+// misc buffer layout (bytes)
+constexpr size_t kMiscThr = 0;      // float: current threshold
+constexpr size_t kMiscZero = 8;     // uint64: always 0
+constexpr size_t kMiscSize0 = 16;   // uint64: size of list 0
+constexpr size_t kMiscSize1 = 24;   // uint64: size of list 1
+constexpr size_t kMiscTotal = 32;   // uint64: scan / compaction total
+constexpr size_t kMiscMinMax = 40;  // uint32[2]: orderable min / max score keys
+constexpr size_t kMiscDebug = 48;   // float[2]: selected order statistics
+constexpr size_t kMiscBytes = 64;
+
+float key_to_float(uint32_t k) {
+    const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    float f;
+    std::memcpy(&f, &u, sizeof(f));
+    return f;
+}
+
+// np.argsort(|arange(nseg) - ref|, kind="stable") (lib/loki/psr_utils.hpp:331-347).
+std::vector<uint64_t> middle_out_order(uint64_t nseg, uint64_t ref) {
+    std::vector<uint64_t> order;
+    order.reserve(nseg);
+    order.push_back(ref);
+    for (uint64_t d = 1; order.size() < nseg; ++d) {
+        if (d <= ref) {
+            order.push_back(ref - d);
+        }
+        if (ref + d < nseg && order.size() < nseg) {
+            order.push_back(ref + d);
+        }
+    }
+    return order;
+}
+
+// MiddleOutScheme::get_coord / get_current_coord / get_segment_coord
+// (lib/loki/psr_utils.hpp:378-448).
+struct Coord {
+    double ref, scale;
+};
+Coord mo_coord(const std::vector<uint64_t>& order, uint64_t level, double tseg) {
+    uint64_t mn = order[0], mx = order[0];
+    for (uint64_t i = 1; i <= level; ++i) {
+        mn = std::min(mn, order[i]);
+        mx = std::max(mx, order[i]);
+    }
+    const double min_val = static_cast<double>(mn);
+    const double max_val = static_cast<double>(mx);
+    const double ref_val = (min_val + max_val + 1.0) / 2.0;
+    const double scale_val = ref_val - min_val;
+    return {ref_val * tseg, scale_val * tseg};
+}
+Coord mo_current_coord(const std::vector<uint64_t>& order, uint64_t level, double tseg) {
+    if (level == 0) {
+        return mo_coord(order, 0, tseg);
+    }
+    return {mo_coord(order, level - 1, tseg).ref, mo_coord(order, level, tseg).scale};
+}
+Coord mo_segment_coord(const std::vector<uint64_t>& order, uint64_t level, double tseg) {
+    const double idx = static_cast<double>(order[level]);
+    return {(idx + 0.5) * tseg, 0.5 * tseg};
+}
+
+LeafGeom make_geom(const Plan& p, uint64_t branch_max) {
+    const uint32_t np = p.nparams;
+    const uint32_t L = p.n_levels - 1;
+    LeafGeom g{};
+    g.np = np;
+    g.nbins = static_cast<uint32_t>(p.cfg.nbins);
+    g.ls = (np + 2) * 2;
+    g.n_accel = static_cast<uint32_t>(p.param_counts[L][np - 2]);
+    g.n_freq = static_cast<uint32_t>(p.param_counts[L][np - 1]);
+    g.eta = p.cfg.eta;
+    g.a_min = p.lim_min(np - 2);
+    g.a_max = p.lim_max(np - 2);
+    g.f_min = p.lim_min(np - 1);
+    g.f_max = p.lim_max(np - 1);
+    g.branch_max = branch_max;
+    return g;
+}
+
+TransformConsts make_transform(uint32_t np, double t_next, double t_cur, bool conservative) {
+    TransformConsts tc{};
+    tc.dt = t_next - t_cur;
+    tc.dt2 = tc.dt * tc.dt;
+    tc.half_dt2 = np == 2 ? 0.5 * (tc.dt * tc.dt) : 0.5 * (tc.dt2);
+    tc.sixth_dt3 = tc.dt2 * tc.dt / 6.0;
+    tc.conservative = conservative ? 1 : 0;
+    return tc;
+}
+
+ResolveConsts make_resolve(uint32_t np, double t_add, double t_cur, double t_init) {
+    ResolveConsts rc{};
+    const double dt_add = t_add - t_cur;
+    const double dt_init = t_init - t_cur;
+    rc.dt_add = dt_add;
+    if (np == 2) {
+        rc.dt = dt_add - dt_init;
+        rc.half_dt2 = 0.5 * ((dt_add * dt_add) - (dt_init * dt_init));
+    } else {
+        const double half_dt2_add = 0.5 * (dt_add * dt_add);
+        const double half_dt2_init = 0.5 * (dt_init * dt_init);
+        rc.dt = dt_add - dt_init;
+        rc.half_dt2 = half_dt2_add - half_dt2_init;
+        rc.sixth_dt3 = ((half_dt2_add * dt_add) - (half_dt2_init * dt_init)) / 3.0;
+    }
+    return rc;
+}
+
+unsigned grid_for(uint64_t n, uint32_t threads) {
+    const uint64_t b = (n + threads - 1) / threads;
+    require(b <= 0x7fffffffULL, "launch grid too large");
+    return static_cast<unsigned>(b < 1 ? 1 : b);
+}
+
+// Exclusive scan of n uint32 counts into uint64 offsets, total at d_total.
+void scan_counts(const uint32_t* d_x, uint64_t n, uint64_t* d_out, uint32_t* d_sums,
+                 uint64_t* d_offs, uint64_t* d_total, cudaStream_t s) {
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    if (n == 0) {
+        set_u64_kernel<<<1, 1, 0, s>>>(d_total, 0);
+        return;
+    }
+    scan_tile_sums_kernel<<<grid_for(ntiles, 1), kScanThreads, 0, s>>>(d_x, n, d_sums);
+    scan_tiles_kernel<<<1, kScanThreads, 0, s>>>(d_sums, ntiles, d_offs, d_total);
+    scan_apply_kernel<<<grid_for(ntiles, 1), kScanThreads, 0, s>>>(d_x, n, d_offs, d_out);
+    LK_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+PruneExec::PruneExec(const Plan& plan, uint64_t max_sugg, uint64_t batch_size,
+                     uint64_t branch_max, bool conservative, int device)
+    : m_plan(plan),
+      m_device(device),
+      m_cap(max_sugg),
+      m_batch(batch_size),
+      m_branch_max(branch_max),
+      m_conservative(conservative) {
+    m_np = plan.nparams;
+    require(m_np == 2 || m_np == 3,
+            "pruning is implemented for Taylor searches with nparams 2 (accel) or 3 (jerk)");
+    const uint32_t L = plan.n_levels - 1;
+    m_nbins = static_cast<uint32_t>(plan.cfg.nbins);
+    m_ls = (m_np + 2) * 2;
+    m_nseg = plan.nsegments[L];
+    m_tseg = plan.tsegments[L];
+    m_ncoords = plan.ncoords[L];
+    require(m_nseg >= 1, "pruning needs at least one FFA segment");
+    require(m_ncoords == plan.param_counts[L][m_np - 2] * plan.param_counts[L][m_np - 1],
+            "n_leaves mismatch: the final FFA level must have one cell in the higher "
+            "derivatives");
+    require(max_sugg >= 1 && max_sugg < (1ull << 31), "max_sugg must lie in [1, 2^31)");
+    require(m_ncoords <= max_sugg, "WorldTree: Suggestions too large to add.");
+    require(batch_size >= 1, "batch_size must be positive");
+    require(branch_max >= 1, "branch_max must be positive");
+    m_sp = make_score_params(plan.widths.data(), static_cast<uint32_t>(plan.widths.size()),
+                             m_nbins);
+    DeviceGuard g(device);
+    for (int i = 0; i < 2; ++i) {
+        m_tleaves[i].alloc(m_cap * m_ls * sizeof(double));
+        m_tfolds[i].alloc(m_cap * 2 * m_nbins * sizeof(float));
+        m_tscores[i].alloc(m_cap * sizeof(float));
+        m_lids[i].alloc(m_cap * sizeof(uint32_t));
+        m_lsc[i].alloc(m_cap * sizeof(float));
+    }
+    m_status.alloc(sizeof(uint32_t));
+    LK_CUDA(cudaMemset(m_status.ptr, 0, sizeof(uint32_t)));
+    m_misc.alloc(kMiscBytes);
+    LK_CUDA(cudaMemset(m_misc.ptr, 0, kMiscBytes));
+    m_host.alloc(64 * 1024);
+}
+
+uint64_t PruneExec::device_bytes() const {
+    uint64_t b = m_status.bytes + m_misc.bytes;
+    for (int i = 0; i < 2; ++i) {
+        b += m_tleaves[i].bytes + m_tfolds[i].bytes + m_tscores[i].bytes + m_lids[i].bytes +
+             m_lsc[i].bytes;
+    }
+    for (const DeviceBuffer* d : {&m_counts, &m_offsets, &m_scan_sums, &m_scan_offs, &m_bparents,
+                                  &m_bchild, &m_cleaves, &m_cparent, &m_cscores, &m_cfolds,
+                                  &m_bcounts}) {
+        b += d->bytes;
+    }
+    return b;
+}
+
+void PruneExec::ensure_level_buffers(uint64_t n_parents, uint64_t n_children) {
+    const uint64_t n_scan = std::max({n_parents, n_children, m_cap}) + 1;
+    const uint64_t ntiles = (n_scan + kScanTile - 1) / kScanTile + 1;
+    if (m_scan_sums.bytes < ntiles * sizeof(uint32_t)) {
+        m_scan_sums.alloc(ntiles * sizeof(uint32_t));
+        m_scan_offs.alloc(ntiles * sizeof(uint64_t));
+    }
+    if (n_parents > m_cap_parents) {
+        m_counts.alloc(n_parents * sizeof(uint32_t));
+        m_offsets.alloc(n_parents * sizeof(uint64_t));
+        m_cap_parents = n_parents;
+    }
+    if (n_children > m_cap_children) {
+        m_cleaves.alloc(n_children * m_ls * sizeof(double));
+        m_cparent.alloc(n_children * sizeof(uint32_t));
+        m_cscores.alloc(n_children * sizeof(float));
+        m_cfolds.alloc(n_children * 2 * m_nbins * sizeof(float));
+        m_cap_children = n_children;
+    }
+}
+
+void PruneExec::compact_children(uint64_t c_begin, uint64_t c_end, uint32_t* out_ids,
+                                 float* out_sc, const uint64_t* d_base, uint64_t limit,
+                                 uint64_t* d_size_out, cudaStream_t s) {
+    auto* misc = static_cast<char*>(m_misc.ptr);
+    auto* d_thr = reinterpret_cast<const float*>(misc + kMiscThr);
+    auto* d_total = reinterpret_cast<uint64_t*>(misc + kMiscTotal);
+    const uint64_t n = c_end - c_begin;
+    if (n == 0) {
+        set_u64_kernel<<<1, 1, 0, s>>>(d_total, 0);
+    } else {
+        const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+        const auto* sc = m_cscores.as<const float>();
+        pc_count_kernel<Src::kChildren, false><<<grid_for(ntiles, 1), kScanThreads, 0, s>>>(
+            sc, nullptr, c_begin, n, d_thr, m_scan_sums.as<uint32_t>());
+        scan_tiles_kernel<<<1, kScanThreads, 0, s>>>(m_scan_sums.as<uint32_t>(), ntiles,
+                                                     m_scan_offs.as<uint64_t>(), d_total);
+        pc_scatter_kernel<Src::kChildren, false><<<grid_for(ntiles, 1), kScanThreads, 0, s>>>(
+            sc, nullptr, c_begin, n, d_thr, m_scan_offs.as<uint64_t>(), d_base, limit, out_ids,
+            out_sc);
+    }
+    pc_finish_kernel<<<1, 1, 0, s>>>(d_base, d_total, limit, d_size_out);
+    LK_CUDA(cudaGetLastError());
+}
+
+void PruneExec::compact_list_gt(const uint32_t* ids, const float* sc, uint64_t n,
+                                uint32_t* out_ids, float* out_sc, const uint64_t* d_base,
+                                uint64_t* d_size_out, cudaStream_t s) {
+    auto* misc = static_cast<char*>(m_misc.ptr);
+    auto* d_thr = reinterpret_cast<const float*>(misc + kMiscThr);
+    auto* d_total = reinterpret_cast<uint64_t*>(misc + kMiscTotal);
+    if (n == 0) {
+        set_u64_kernel<<<1, 1, 0, s>>>(d_total, 0);
+    } else {
+        const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+        pc_count_kernel<Src::kList, true><<<grid_for(ntiles, 1), kScanThreads, 0, s>>>(
+            sc, ids, 0, n, d_thr, m_scan_sums.as<uint32_t>());
+        scan_tiles_kernel<<<1, kScanThreads, 0, s>>>(m_scan_sums.as<uint32_t>(), ntiles,
+                                                     m_scan_offs.as<uint64_t>(), d_total);
+        pc_scatter_kernel<Src::kList, true><<<grid_for(ntiles, 1), kScanThreads, 0, s>>>(
+            sc, ids, 0, n, d_thr, m_scan_offs.as<uint64_t>(), d_base, m_cap, out_ids, out_sc);
+    }
+    pc_finish_kernel<<<1, 1, 0, s>>>(d_base, d_total, m_cap, d_size_out);
+    LK_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+__global__ void minmax_kernel(const float* __restrict__ x, uint64_t n, uint32_t* mm) {
+    __shared__ uint32_t s_min, s_max;
+    if (threadIdx.x == 0) {
+        s_min = 0xffffffffu;
+        s_max = 0u;
+    }
+    __syncthreads();
+    uint32_t lo = 0xffffffffu, hi = 0u;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t k = fkey(x[i]);
+        lo = min(lo, k);
+        hi = max(hi, k);
+    }
+    atomicMin(&s_min, lo);
+    atomicMax(&s_max, hi);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicMin(&mm[0], s_min);
+        atomicMax(&mm[1], s_max);
+    }
+}
+
+}  // namespace
+
+std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref_seg,
+                                           const float* thresholds, uint64_t n_thresholds,
+                                           uint64_t n_iters, cudaStream_t s) {
+    require(d_ffa_fold != nullptr, "ffa_fold is null");
+    require(ref_seg < m_nseg, "ref_idx must be less than nsegments.");
+    DeviceGuard g(m_device);
+    const std::vector<uint64_t> order = middle_out_order(m_nseg, ref_seg);
+    const uint64_t seg_floats = m_ncoords * 2 * m_nbins;
+    auto* misc = static_cast<char*>(m_misc.ptr);
+    auto* d_mm = reinterpret_cast<uint32_t*>(misc + kMiscMinMax);
+    LK_CUDA(cudaMemsetAsync(m_status.ptr, 0, sizeof(uint32_t), s));
+
+    // initialize (lib/prune.cpp:181-226): seed leaves, fold segment, scores.
+    m_tree = TreeState{};
+    m_tree.cap = m_cap;
+    m_cur = 0;
+    const LeafGeom geom = make_geom(m_plan, m_branch_max);
+    const uint32_t L = m_plan.n_levels - 1;
+    const double dp0 = m_plan.dparams_actual[L][0];
+    const double dp1 = m_np == 3 ? m_plan.dparams_actual[L][1] : 0.0;
+    const double dfreq = m_plan.dparams_actual[L][m_np - 1];
+    seed_kernel<<<grid_for(m_ncoords, 256), 256, 0, s>>>(geom, dp0, dp1, dfreq,
+                                                         m_tleaves[0].as<double>());
+    const float* seg0 = d_ffa_fold + order[0] * seg_floats;
+    LK_CUDA(cudaMemcpyAsync(m_tfolds[0].ptr, seg0, seg_floats * sizeof(float),
+                            cudaMemcpyDeviceToDevice, s));
+    score_folds(seg0, m_ncoords, m_nbins, true, 1.0f, m_sp, LK_SCORE_MAX,
+                m_tscores[0].as<float>(), s);
+    init_minmax_kernel<<<1, 1, 0, s>>>(d_mm);
+    minmax_kernel<<<std::min<unsigned>(grid_for(m_ncoords, 256), 1184), 256, 0, s>>>(
+        m_tscores[0].as<float>(), m_ncoords, d_mm);
+    LK_CUDA(cudaGetLastError());
+    LK_CUDA(cudaMemcpyAsync(m_host.ptr, d_mm, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaStreamSynchronize(s));
+    m_tree.size = m_ncoords;
+    std::vector<lk_prune_stats> stats;
+    {
+        lk_prune_stats s0{};
+        s0.level = 0;
+        s0.seg_idx = order[0];
+        s0.n_branches = s0.n_leaves = s0.n_leaves_phy = s0.n_leaves_surv = m_ncoords;
+        s0.threshold = 0.0f;
+        s0.score_min = m_ncoords ? key_to_float(m_host.as<uint32_t>()[0]) : 0.0f;
+        s0.score_max = m_ncoords ? key_to_float(m_host.as<uint32_t>()[1]) : 0.0f;
+        stats.push_back(s0);
+    }
+    const uint64_t levels = std::min<uint64_t>(m_nseg - 1, n_iters);
+    for (uint64_t lv = 1; lv <= levels; ++lv) {
+        require(lv <= n_thresholds, "Pruning complete - exceeded threshold scheme length");
+        const float* d_seg = d_ffa_fold + order[lv] * seg_floats;
+        lk_prune_stats st{};
+        level(d_seg, order, lv, thresholds[lv - 1], &st, s);
+        stats.push_back(st);
+        if (m_tree.size == 0) {
+            break;
+        }
+    }
+    return stats;
+}
+
+void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, uint64_t lv,
+                      float threshold, lk_prune_stats* st, cudaStream_t s) {
+    TreeState& t = m_tree;
+    auto* misc = static_cast<char*>(m_misc.ptr);
+    auto* d_thr = reinterpret_cast<float*>(misc + kMiscThr);
+    auto* d_zero = reinterpret_cast<uint64_t*>(misc + kMiscZero);
+    uint64_t* d_size[2] = {reinterpret_cast<uint64_t*>(misc + kMiscSize0),
+                           reinterpret_cast<uint64_t*>(misc + kMiscSize1)};
+    auto* d_total = reinterpret_cast<uint64_t*>(misc + kMiscTotal);
+    auto* d_mm = reinterpret_cast<uint32_t*>(misc + kMiscMinMax);
+
+    // prepare_in_place_update (lib/world_tree.cpp:237-249)
+    t.size_old = t.size;
+    t.write_start = (t.head + t.size) % t.cap;
+    t.size = 0;
+    t.read_consumed = 0;
+    const uint64_t n_par = t.size_old;
+    const Coord ci = mo_coord(order, 0, m_tseg);
+    const Coord cn = mo_coord(order, lv, m_tseg);
+    const Coord cc = mo_current_coord(order, lv, m_tseg);
+    const Coord ca = mo_segment_coord(order, lv, m_tseg);
+
+    // Batches: get_leaves_span splits a batch at the buffer's wrap
+    // (lib/world_tree.cpp:148-163, lib/prune.cpp:509-530).
+    std::vector<uint64_t> bstart, bsize;
+    {
+        const uint64_t bs = std::max<uint64_t>(1, std::min(m_batch, n_par));
+        uint64_t done = 0;
+        while (done < n_par) {
+            const uint64_t want = std::min(bs, n_par - done);
+            const uint64_t phys = (t.head + done) % t.cap;
+            const uint64_t take = std::min(want, t.cap - phys);
+            bstart.push_back(done);
+            bsize.push_back(take);
+            done += take;
+        }
+    }
+    const uint64_t nbat = bstart.size();
+    const size_t host_need = 64 + (nbat + 1) * sizeof(uint64_t) * 2 + nbat * sizeof(uint32_t);
+    if (m_host.bytes < host_need) {
+        LK_CUDA(cudaStreamSynchronize(s));
+        m_host.alloc(host_need * 2);
+    }
+    if (m_cap_batches < nbat + 1) {
+        m_bparents.alloc((nbat + 1) * sizeof(uint64_t));
+        m_bchild.alloc((nbat + 1) * sizeof(uint64_t));
+        m_bcounts.alloc((nbat + 1) * sizeof(uint32_t));
+        m_cap_batches = nbat + 1;
+    }
+    auto* h = static_cast<char*>(m_host.ptr);
+    auto* h_bpar = reinterpret_cast<uint64_t*>(h + 64);
+    auto* h_bchild = h_bpar + (nbat + 1);
+    auto* h_counts = reinterpret_cast<uint32_t*>(h_bchild + (nbat + 1));
+    for (uint64_t b = 0; b < nbat; ++b) {
+        h_bpar[b] = bstart[b];
+    }
+    h_bpar[nbat] = n_par;
+    ensure_level_buffers(n_par, 0);
+
+    // 1. branch: counts, offsets, batch child ranges
+    const LeafGeom geom = make_geom(m_plan, m_branch_max);
+    const double* tree_leaves = m_tleaves[m_cur].as<double>();
+    LK_CUDA(cudaMemcpyAsync(m_bparents.ptr, h_bpar, (nbat + 1) * sizeof(uint64_t),
+                            cudaMemcpyHostToDevice, s));
+    branch_count_kernel<<<grid_for(n_par, 256), 256, 0, s>>>(
+        tree_leaves, t.head, t.cap, n_par, cc.scale, geom, m_counts.as<uint32_t>(),
+        m_status.as<uint32_t>());
+    scan_counts(m_counts.as<uint32_t>(), n_par, m_offsets.as<uint64_t>(),
+                m_scan_sums.as<uint32_t>(), m_scan_offs.as<uint64_t>(), d_total, s);
+    batch_child_starts_kernel<<<grid_for(nbat + 1, 256), 256, 0, s>>>(
+        m_offsets.as<uint64_t>(), n_par, d_total, m_bparents.as<uint64_t>(), nbat + 1,
+        m_bchild.as<uint64_t>());
+    LK_CUDA(cudaGetLastError());
+    LK_CUDA(cudaMemcpyAsync(h_bchild, m_bchild.ptr, (nbat + 1) * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaMemcpyAsync(h, m_status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaStreamSynchronize(s));
+    const uint32_t status = *reinterpret_cast<uint32_t*>(h);
+    if (status & kStatusBranchMax) {
+        fail(LK_ERR_INVALID_ARG, "num_points must be less than or equal to branch_max");
+    }
+    if (status & kStatusZeroStep) {
+        fail(LK_ERR_INVALID_ARG, "Both dparam_cur and dparam_new must be positive");
+    }
+    if (status & kStatusBranchCount) {
+        fail(LK_ERR_UNSUPPORTED, "a parent has more than 2^32-1 children");
+    }
+    const std::vector<uint64_t> cstart(h_bchild, h_bchild + nbat + 1);
+    const uint64_t n_child = cstart[nbat];
+    for (uint64_t b = 0; b < nbat; ++b) {
+        if (cstart[b + 1] - cstart[b] > m_batch * m_branch_max) {
+            fail(LK_ERR_INVALID_ARG,
+                 "Branch factor exceeded workspace size:n_leaves_batch <= max_branched_leaves");
+        }
+    }
+    require(n_child < (1ull << 32), "more than 2^32 children in one level");
+    ensure_level_buffers(n_par, n_child);
+
+    // 2. children: leaves, then resolve + shift-add + score (+ kept folds)
+    branch_emit_kernel<<<grid_for(n_par, 256), 256, 0, s>>>(
+        tree_leaves, t.head, t.cap, n_par, cc.scale, geom, m_offsets.as<uint64_t>(),
+        m_cleaves.as<double>(), m_cparent.as<uint32_t>(), m_status.as<uint32_t>());
+    init_minmax_kernel<<<1, 1, 0, s>>>(d_mm);
+    if (n_child > 0) {
+        const ResolveConsts rc = make_resolve(m_np, ca.ref, cc.ref, ci.ref);
+        const uint32_t rs = sc::row_stride(m_nbins, m_sp.wmax);
+        const uint32_t T = sc::profiles_per_block(rs + 4);
+        const size_t smem = static_cast<size_t>(T) * rs * sizeof(float) + 4 * T * sizeof(uint32_t);
+        auto launch = [&](auto kern) {
+            sc::set_smem(kern, smem);
+            kern<<<grid_for(n_child, T), T, smem, s>>>(
+                m_cleaves.as<double>(), m_cparent.as<uint32_t>(), n_child,
+                m_tfolds[m_cur].as<float>(), t.head, t.cap, d_seg, geom, rc, rs, m_sp,
+                threshold, m_cscores.as<float>(), m_cfolds.as<float>(), d_mm);
+        };
+        if (m_sp.nwidths <= 8) {
+            launch(leaf_kernel<8>);
+        } else if (m_sp.nwidths <= 16) {
+            launch(leaf_kernel<16>);
+        } else {
+            launch(leaf_kernel<32>);
+        }
+        LK_CUDA(cudaGetLastError());
+    }
+
+    // 3. filter + add, batch by batch in the reference's order
+    int li = 0;
+    set_f32_kernel<<<1, 1, 0, s>>>(d_thr, threshold);
+    set_u64_kernel<<<1, 1, 0, s>>>(d_size[0], 0);
+    uint64_t b = 0;
+    while (b < nbat) {
+        batch_count_kernel<<<static_cast<unsigned>(nbat - b), 256, 0, s>>>(
+            m_cscores.as<float>(), m_bchild.as<uint64_t>(), b, d_thr, m_bcounts.as<uint32_t>());
+        LK_CUDA(cudaGetLastError());
+        LK_CUDA(cudaMemcpyAsync(h_counts, m_bcounts.ptr, (nbat - b) * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, s));
+        LK_CUDA(cudaMemcpyAsync(h, d_size[li], sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        LK_CUDA(cudaStreamSynchronize(s));
+        t.size = *reinterpret_cast<uint64_t*>(h);
+        // fast path of add_batch_scattered (lib/world_tree.cpp:376-384)
+        uint64_t bf = b;
+        while (bf < nbat) {
+            const uint64_t cnt = h_counts[bf - b];
+            if (cnt > t.space_left()) {
+                break;
+            }
+            t.size += cnt;
+            t.read_consumed += bsize[bf];
+            ++bf;
+        }
+        if (bf > b) {
+            compact_children(cstart[b], cstart[bf], m_lids[li].as<uint32_t>(),
+                             m_lsc[li].as<float>(), d_size[li], m_cap, d_size[li], s);
+        }
+        if (bf == nbat) {
+            break;
+        }
+        // overload (lib/world_tree.cpp:386-421)
+        const uint64_t space = t.space_left();
+        const uint64_t K = t.size + space;
+        const uint64_t N = t.size + h_counts[bf - b];
+        const uint64_t m = N / 2;
+        const uint64_t r_med = (m <= K - 1) ? (K - 1 - m) : (N - 1 - m + K);
+        select_threshold_kernel<<<1, 1024, 0, s>>>(m_lsc[li].as<float>(), t.size,
+                                                   m_cscores.as<float>(), cstart[bf],
+                                                   cstart[bf + 1], N, K - 1, r_med, d_thr,
+                                                   reinterpret_cast<float*>(misc + kMiscDebug));
+        LK_CUDA(cudaGetLastError());
+        compact_list_gt(m_lids[li].as<uint32_t>(), m_lsc[li].as<float>(), t.size,
+                        m_lids[1 - li].as<uint32_t>(), m_lsc[1 - li].as<float>(), d_zero,
+                        d_size[1 - li], s);
+        compact_children(cstart[bf], cstart[bf + 1], m_lids[1 - li].as<uint32_t>(),
+                         m_lsc[1 - li].as<float>(), d_size[1 - li], K, d_size[1 - li], s);
+        li = 1 - li;
+        t.read_consumed += bsize[bf];
+        b = bf + 1;
+    }
+    LK_CUDA(cudaMemcpyAsync(h, d_size[li], sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaMemcpyAsync(h + 8, d_mm, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaStreamSynchronize(s));
+    t.size = *reinterpret_cast<uint64_t*>(h);
+    const uint32_t kmin = reinterpret_cast<uint32_t*>(h + 8)[0];
+    const uint32_t kmax = reinterpret_cast<uint32_t*>(h + 8)[1];
+
+    // 4. transform + gather into the other tree buffer; finalize_in_place_update
+    if (t.size > 0) {
+        const TransformConsts tc = make_transform(m_np, cn.ref, cc.ref, m_conservative);
+        const int nxt = 1 - m_cur;
+        gather_kernel<<<grid_for(t.size * kWarp, 256), 256, 0, s>>>(
+            m_lids[li].as<uint32_t>(), m_lsc[li].as<float>(), t.size, m_cleaves.as<double>(),
+            m_cfolds.as<float>(), t.write_start, t.cap, m_np, m_nbins, tc,
+            m_tleaves[nxt].as<double>(), m_tfolds[nxt].as<float>(), m_tscores[nxt].as<float>());
+        LK_CUDA(cudaGetLastError());
+        m_cur = nxt;
+    }
+    t.head = t.write_start;
+    t.size_old = 0;
+    t.read_consumed = 0;
+
+    st->level = lv;
+    st->seg_idx = order[lv];
+    st->n_branches = n_par;
+    st->n_leaves = n_child;
+    st->n_leaves_phy = n_child;
+    st->n_leaves_surv = t.size;
+    st->threshold = threshold;
+    st->score_min = n_child ? key_to_float(kmin) : FLT_MAX;
+    st->score_max = n_child ? key_to_float(kmax) : -FLT_MAX;
+}
+
+void PruneExec::copy_tree(double* d_leaves, float* d_folds, float* d_scores,
+                          cudaStream_t s) const {
+    DeviceGuard g(m_device);
+    const TreeState& t = m_tree;
+    const uint64_t first = std::min(t.size, t.cap - t.head);
+    const uint64_t second = t.size - first;
+    const size_t lb = m_ls * sizeof(double), fb = 2 * m_nbins * sizeof(float);
+    auto cp = [&](void* dst, const DeviceBuffer& src, size_t unit) {
+        if (dst == nullptr) {
+            return;
+        }
+        LK_CUDA(cudaMemcpyAsync(dst, static_cast<const char*>(src.ptr) + t.head * unit,
+                                first * unit, cudaMemcpyDeviceToDevice, s));
+        if (second > 0) {
+            LK_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + first * unit, src.ptr,
+                                    second * unit, cudaMemcpyDeviceToDevice, s));
+        }
+    };
+    cp(d_leaves, m_tleaves[m_cur], lb);
+    cp(d_folds, m_tfolds[m_cur], fb);
+    cp(d_scores, m_tscores[m_cur], sizeof(float));
+}
+
+}  // namespace lk
+
+// ---- single steps ----------------------------------------------------------
+
+namespace lk {
+
+namespace {
+
+__global__ void resolve_kernel(const double* __restrict__ leaves, uint64_t n, LeafGeom g,
+                               ResolveConsts rc, uint32_t* __restrict__ pidx,
+                               float* __restrict__ phase) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) {
+        resolve_leaf(leaves + i * g.ls, g, rc, pidx + i, phase + i);
+    }
+}
+
+// kernels::shift_add_linear_batch (lib/kernels.cpp:1328-1355), warp per leaf.
+// The reference wraps (index + start) once; an index that lands outside the
+// tree or an FFA row beyond n_ffa is skipped and flagged instead.
+__global__ void shift_add_kernel(const float* __restrict__ tree, const uint32_t* __restrict__ it,
+                                 const float* __restrict__ ffa, const uint32_t* __restrict__ iff,
+                                 const float* __restrict__ phase, float* __restrict__ out,
+                                 uint32_t nb, uint64_t n, uint64_t pstart, uint64_t cap,
+                                 uint64_t n_ffa, uint32_t* status) {
+    const uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
+    const uint32_t lane = threadIdx.x % kWarp;
+    if (w >= n) {
+        return;
+    }
+    const uint64_t logical = static_cast<uint64_t>(it[w]) + pstart;
+    const uint64_t phys = logical < cap ? logical : logical - cap;
+    const uint64_t row = iff[w];
+    if (phys >= cap || row >= n_ffa) {
+        if (lane == 0) {
+            atomicOr(status, dev::kStatusBadTable);
+        }
+        return;
+    }
+    const float* tail = tree + phys * 2 * nb;
+    const float* hd = ffa + row * 2 * nb;
+    const uint32_t s = dev::shift_bins(phase[w], nb);
+    float* o = out + w * 2 * nb;
+    for (uint32_t j = lane; j < nb; j += kWarp) {
+        const uint32_t jh = j >= s ? j - s : j + nb - s;
+        o[j] = __fadd_rn(tail[j], hd[jh]);
+        o[nb + j] = __fadd_rn(tail[nb + j], hd[nb + jh]);
+    }
+}
+
+void require_taylor(const Plan& plan) {
+    require(plan.nparams == 2 || plan.nparams == 3,
+            "pruning is implemented for Taylor searches with nparams 2 (accel) or 3 (jerk)");
+}
+
+}  // namespace
+
+void taylor_seed(const Plan& plan, double* d_leaves, cudaStream_t s) {
+    require_taylor(plan);
+    const uint32_t L = plan.n_levels - 1;
+    const uint32_t np = plan.nparams;
+    require(plan.ncoords[L] == plan.param_counts[L][np - 2] * plan.param_counts[L][np - 1],
+            "n_leaves mismatch");
+    const LeafGeom g = make_geom(plan, 1);
+    const double dp0 = plan.dparams_actual[L][0];
+    const double dp1 = np == 3 ? plan.dparams_actual[L][1] : 0.0;
+    seed_kernel<<<grid_for(plan.ncoords[L], 256), 256, 0, s>>>(
+        g, dp0, dp1, plan.dparams_actual[L][np - 1], d_leaves);
+    LK_CUDA(cudaGetLastError());
+}
+
+uint64_t taylor_branch(const Plan& plan, const double* d_leaves, uint64_t n, double scale_cur,
+                       uint64_t branch_max, double* d_out, uint32_t* d_origins, uint64_t max_out,
+                       cudaStream_t s) {
+    require_taylor(plan);
+    require(branch_max >= 1, "branch_max must be positive");
+    if (n == 0) {
+        return 0;
+    }
+    const LeafGeom g = make_geom(plan, branch_max);
+    DeviceBuffer counts(n * sizeof(uint32_t)), offsets(n * sizeof(uint64_t));
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    DeviceBuffer sums(ntiles * sizeof(uint32_t)), offs(ntiles * sizeof(uint64_t));
+    DeviceBuffer misc(16);
+    LK_CUDA(cudaMemsetAsync(misc.ptr, 0, 16, s));
+    auto* d_status = reinterpret_cast<uint32_t*>(static_cast<char*>(misc.ptr) + 8);
+    auto* d_total = misc.as<uint64_t>();
+    branch_count_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, 0, n, n, scale_cur, g,
+                                                         counts.as<uint32_t>(), d_status);
+    scan_counts(counts.as<uint32_t>(), n, offsets.as<uint64_t>(), sums.as<uint32_t>(),
+                offs.as<uint64_t>(), d_total, s);
+    uint64_t host[2] = {0, 0};
+    LK_CUDA(cudaMemcpyAsync(host, misc.ptr, 16, cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaStreamSynchronize(s));
+    const uint32_t status = static_cast<uint32_t>(host[1]);
+    if (status & kStatusBranchMax) {
+        fail(LK_ERR_INVALID_ARG, "num_points must be less than or equal to branch_max");
+    }
+    if (status & (kStatusZeroStep | kStatusBranchCount)) {
+        fail(LK_ERR_INVALID_ARG, "Both dparam_cur and dparam_new must be positive");
+    }
+    const uint64_t total = host[0];
+    if (total <= max_out && total > 0) {
+        branch_emit_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, 0, n, n, scale_cur, g,
+                                                            offsets.as<uint64_t>(), d_out,
+                                                            d_origins, d_status);
+        LK_CUDA(cudaGetLastError());
+        LK_CUDA(cudaStreamSynchronize(s));
+    }
+    return total;
+}
+
+void taylor_resolve(const Plan& plan, const double* d_leaves, uint64_t n, const double* coords,
+                    uint32_t* d_param_idx, float* d_phase_shift, cudaStream_t s) {
+    require_taylor(plan);
+    if (n == 0) {
+        return;
+    }
+    const LeafGeom g = make_geom(plan, 1);
+    const ResolveConsts rc = make_resolve(plan.nparams, coords[0], coords[2], coords[4]);
+    resolve_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, n, g, rc, d_param_idx,
+                                                    d_phase_shift);
+    LK_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+// Reads a one-word device status after the stream's work and turns a set
+// bad-index bit into an error.
+void check_index_status(const DeviceBuffer& st, cudaStream_t s, const char* what) {
+    uint32_t v = 0;
+    LK_CUDA(cudaMemcpyAsync(&v, st.ptr, sizeof(v), cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaStreamSynchronize(s));
+    if (v & dev::kStatusBadTable) {
+        fail(LK_ERR_INVALID_ARG, what);
+    }
+}
+
+}  // namespace
+
+void taylor_transform(const Plan& plan, double* d_leaves, uint64_t n_leaves,
+                      const uint32_t* d_indices, uint64_t n, double t_next, double t_cur,
+                      bool conservative, cudaStream_t s) {
+    require_taylor(plan);
+    if (n == 0) {
+        return;
+    }
+    const TransformConsts tc = make_transform(plan.nparams, t_next, t_cur, conservative);
+    DeviceBuffer st(sizeof(uint32_t));
+    LK_CUDA(cudaMemsetAsync(st.ptr, 0, sizeof(uint32_t), s));
+    transform_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, n_leaves, d_indices, n,
+                                                      plan.nparams, tc, st.as<uint32_t>());
+    LK_CUDA(cudaGetLastError());
+    check_index_status(st, s, "transform: an index is at or beyond n_leaves");
+}
+
+void shift_add_batch(const float* d_folds_tree, const uint32_t* d_indices_tree,
+                     const float* d_folds_ffa, uint64_t n_ffa, const uint32_t* d_indices_ffa,
+                     const float* d_phase_shift, float* d_out, uint32_t nbins, uint64_t n,
+                     uint64_t physical_start, uint64_t capacity, cudaStream_t s) {
+    require(nbins >= 1, "nbins must be positive");
+    require(capacity >= 1, "capacity must be positive");
+    if (n == 0) {
+        return;
+    }
+    DeviceBuffer st(sizeof(uint32_t));
+    LK_CUDA(cudaMemsetAsync(st.ptr, 0, sizeof(uint32_t), s));
+    shift_add_kernel<<<grid_for(n * kWarp, 256), 256, 0, s>>>(
+        d_folds_tree, d_indices_tree, d_folds_ffa, d_indices_ffa, d_phase_shift, d_out, nbins, n,
+        physical_start, capacity, n_ffa, st.as<uint32_t>());
+    LK_CUDA(cudaGetLastError());
+    check_index_status(st, s,
+                       "shift_add: a tree index (wrapped once) or an FFA row index is out of range");
+}
+
+}  // namespace lk

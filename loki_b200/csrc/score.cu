@@ -22,69 +22,14 @@
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
 #include "lk_merge.cuh"
+#include "lk_score.cuh"
 
 namespace lk {
 
 namespace {
 
 constexpr int kWarp = 32;
-
-// Odd row stride holding a profile and its circular extension.
-inline uint32_t row_stride(uint32_t nbins, uint32_t wmax) { return (nbins + wmax) | 1u; }
-
-__device__ __forceinline__ float normalise(float e, float v) {
-    // 1.0F / std::sqrt(v) then e * that (lib/score.cpp:134-136): both
-    // correctly rounded, so rcp_rn(sqrt_rn(v)) == 1.0F / sqrt(v) exactly.
-    return __fmul_rn(e, __frcp_rn(__fsqrt_rn(v)));
-}
-
-// Scores the normalised profile staged at r (in place). NW >= sp.nwidths is
-// the compile-time width capacity (8, 16 or 32): the width loops are
-// unrolled to NW, so a small NW avoids evaluating unused width slots.
-template <int NW>
-__device__ __forceinline__ void score_row(float* r, uint32_t nbins, float inv_stdnoise,
-                                          const ScoreParams& sp, int mode, float* out) {
-    float acc = r[0];
-    for (uint32_t j = 1; j < nbins; ++j) {
-        acc = __fadd_rn(acc, r[j]);
-        r[j] = acc;
-    }
-    const float sum = acc;
-    for (uint32_t k = 0; k < sp.wmax; ++k) {
-        r[nbins + k] = __fadd_rn(r[k], sum);
-    }
-    float dm[NW];
-#pragma unroll
-    for (int iw = 0; iw < NW; ++iw) {
-        dm[iw] = -FLT_MAX;
-    }
-    for (uint32_t i = 0; i < nbins; ++i) {
-        const float ri = r[i];
-#pragma unroll
-        for (int iw = 0; iw < NW; ++iw) {
-            if (iw < static_cast<int>(sp.nwidths)) {
-                const float d = __fsub_rn(r[i + sp.widths[iw]], ri);
-                dm[iw] = (dm[iw] < d) ? d : dm[iw];
-            }
-        }
-    }
-    float best = -FLT_MAX;
-#pragma unroll
-    for (int iw = 0; iw < NW; ++iw) {
-        if (iw < static_cast<int>(sp.nwidths)) {
-            const float base = __fsub_rn(__fmul_rn(sp.hb[iw], dm[iw]), __fmul_rn(sp.b[iw], sum));
-            const float snr = __fmul_rn(base, inv_stdnoise);
-            if (mode == LK_SCORE_PER_WIDTH) {
-                out[iw] = snr;
-            } else {
-                best = (best < snr) ? snr : best;
-            }
-        }
-    }
-    if (mode == LK_SCORE_MAX) {
-        out[0] = best;
-    }
-}
+using namespace sc;
 
 template <int NW>
 __global__ void score_kernel(const float* __restrict__ folds, uint64_t nprof, uint32_t nbins,
@@ -151,27 +96,6 @@ __global__ void merge_score_kernel(const float* __restrict__ in, const void* __r
         const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1;
         score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, 1.0f, sp, mode,
                       scores + c * nout);
-    }
-}
-
-// Profiles per block so that the staged rows fit comfortably in shared memory.
-uint32_t profiles_per_block(uint32_t rs) {
-    const size_t per = static_cast<size_t>(rs) * sizeof(float);
-    uint32_t T = 128;
-    while (T > 32 && T * per > 48 * 1024) {
-        T -= 32;
-    }
-    if (T * per > 200 * 1024) {
-        fail(LK_ERR_UNSUPPORTED, "nbins too large for the boxcar scorer");
-    }
-    return T;
-}
-
-template <class K>
-void set_smem(K kern, size_t smem) {
-    if (smem > 48 * 1024) {
-        LK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
     }
 }
 

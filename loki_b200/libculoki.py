@@ -8,6 +8,7 @@ reference reads the same:
     libculoki.fold.compute_brute_fold_time_cuda
     libculoki.scores.{snr_boxcar_3d, snr_boxcar_3d_max, snr_boxcar_2d_max,
                       generate_box_width_trials}
+    libculoki.prune.{EPMultiPassCUDA, PruneCUDA}
 """
 
-from . import configs, ffa, fold, plans, scores  # noqa: F401
+from . import configs, ffa, fold, plans, prune, scores  # noqa: F401

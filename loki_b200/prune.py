@@ -1,0 +1,189 @@
+"""Pruning tree on the GPU: ``PruneCUDA`` (one run for one reference segment)
+and ``EPMultiPassCUDA`` (FFA to ``bseg_ffa`` segments, then one pruning run per
+reference segment), mirroring ``libloki.prune.EPMultiPassTime`` of the
+reference (src/loki_templates.hpp:87-113, lib/prune.cpp:626-930).
+
+Each run seeds the world tree from the final FFA level of the reference
+segment and prunes level by level in middle-out segment order with the
+reference's batch, threshold and world-tree semantics (branch, resolve,
+shift-add, max-width boxcar S/N, filter ``score >= threshold``, transform,
+add with overload pruning). Results match the reference's CPU code bit for
+bit. The ascend / report stage and the HDF5 writer are not part of this
+module: runs return the final tree (leaves, folds, scores) and the per-level
+statistics, and ``execute`` can save them as ``.npz`` plus a text log.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _capi as C
+from . import _device as D
+from .configs import PulsarSearchConfig
+from .ffa import FFACUDA
+
+PRUNE_STATS_DTYPE = np.dtype([
+    ("level", np.uint64), ("seg_idx", np.uint64), ("n_branches", np.uint64), ("n_leaves", np.uint64),
+    ("n_leaves_phy", np.uint64), ("n_leaves_surv", np.uint64), ("threshold", np.float32),
+    ("score_min", np.float32), ("score_max", np.float32), ("pad", np.float32)])
+
+
+def branching_pattern(cfg: PulsarSearchConfig, ref_seg: int = 0, use_conservative_tile: bool = False) -> np.ndarray:
+    """FFAPlan.get_branching_pattern("taylor", ref_seg) (lib/taylor.cpp:1643-1741)."""
+    out = np.zeros(4096, np.float64)
+    n = ctypes.c_uint64()
+    C.check(C.lib().lk_plan_branching_pattern(cfg._plan_handle, int(ref_seg), int(use_conservative_tile),
+                                              out.ctypes.data, out.size, ctypes.byref(n)))
+    if n.value > out.size:
+        out = np.zeros(n.value, np.float64)
+        C.check(C.lib().lk_plan_branching_pattern(cfg._plan_handle, int(ref_seg), int(use_conservative_tile),
+                                                  out.ctypes.data, out.size, ctypes.byref(n)))
+    return out[: n.value].copy()
+
+
+def determine_ref_segs(nsegments: int, n_runs: int | None = None, ref_segs=None) -> list[int]:
+    """utils::determine_ref_segs_pareto (lib/utils.cpp:243-278)."""
+    if n_runs is not None:
+        if n_runs < 1 or n_runs > nsegments:
+            raise RuntimeError(f"n_runs must be between 1 and {nsegments}, got {n_runs}")
+        if n_runs == 1:
+            return [nsegments // 2]
+
+        def round_div(num, den):
+            return (num + den // 2) // den
+
+        margin = round_div(nsegments - 1, 2 * n_runs)
+        lo, hi, denom = margin, nsegments - 1 - margin, n_runs - 1
+        return [round_div((denom - i) * lo + i * hi, denom) for i in range(n_runs)]
+    if ref_segs is not None:
+        return [int(r) for r in ref_segs]
+    raise RuntimeError("Either n_runs or ref_segs must be provided")
+
+
+class PruneCUDA:
+    """One pruning search over the final FFA level of ``cfg`` on one device.
+
+    ``max_sugg`` is the world-tree capacity, ``batch_size`` the parents per
+    batch (it decides when overload pruning raises the threshold, exactly as
+    in the reference), ``branch_max`` the most child values of one parameter
+    (None: EPMultiPass's rule, max(ceil(2 * max branching), 32)).
+    """
+
+    def __init__(self, cfg: PulsarSearchConfig, max_sugg: int = 1 << 20, batch_size: int = 4096,
+                 branch_max: int | None = None, use_conservative_tile: bool = False, device_id: int = 0):
+        D.require_cuda(device_id)
+        if cfg.nparams not in (2, 3):
+            raise NotImplementedError("pruning is implemented for Taylor searches with nparams 2 or 3")
+        self._cfg = cfg
+        self._device = device_id
+        self._nparams = cfg.nparams
+        self._nbins = cfg.nbins
+        h = ctypes.c_void_p()
+        with D.torch().cuda.device(device_id):
+            C.check(C.lib().lk_prune_create(cfg._plan_handle, int(max_sugg), int(batch_size),
+                                            0 if branch_max is None else int(branch_max),
+                                            int(use_conservative_tile), device_id, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                C.lib().lk_prune_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def run(self, ffa_fold, ref_seg: int, thresholds, n_iters: int | None = None) -> np.ndarray:
+        """Seed from segment ``ref_seg`` of the final FFA fold (CUDA tensor or host
+        array, [nsegments, ncoords, 2, nbins]) and prune; returns the per-level
+        statistics (one row for the seed, then one per level run)."""
+        fold = D.to_device_f32(ffa_fold, self._device).reshape(-1)
+        thr = np.ascontiguousarray(thresholds, dtype=np.float32)
+        n_iters = thr.size if n_iters is None else int(n_iters)
+        stats = (C.LkPruneStats * (n_iters + 1))()
+        n = ctypes.c_uint64()
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_prune_run(self._h, D.ptr(fold), int(ref_seg), thr.ctypes.data, thr.size, n_iters,
+                                         stats, n_iters + 1, ctypes.byref(n), D.stream_ptr(self._device)))
+        out = np.zeros(n.value, PRUNE_STATS_DTYPE)
+        for i in range(n.value):
+            for name in PRUNE_STATS_DTYPE.names:
+                out[name][i] = getattr(stats[i], name)
+        return out
+
+    @property
+    def tree_size(self) -> int:
+        n = ctypes.c_uint64()
+        C.check(C.lib().lk_prune_tree_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    def tree(self, host: bool = True):
+        """Final tree in logical order: (leaves [n, nparams+2, 2] f64, folds
+        [n, 2, nbins] f32, scores [n] f32), as host arrays or CUDA tensors."""
+        t = D.torch()
+        n = self.tree_size
+        dev = f"cuda:{self._device}"
+        leaves = t.empty((max(n, 1), self._nparams + 2, 2), dtype=t.float64, device=dev)
+        folds = t.empty((max(n, 1), 2, self._nbins), dtype=t.float32, device=dev)
+        scores = t.empty(max(n, 1), dtype=t.float32, device=dev)
+        with t.cuda.device(self._device):
+            C.check(C.lib().lk_prune_get_tree(self._h, leaves.data_ptr(), folds.data_ptr(), scores.data_ptr(),
+                                              max(n, 1), D.stream_ptr(self._device)))
+        leaves, folds, scores = leaves[:n], folds[:n], scores[:n]
+        if host:
+            return leaves.cpu().numpy(), folds.cpu().numpy(), scores.cpu().numpy()
+        return leaves, folds, scores
+
+
+class EPMultiPassCUDA:
+    """FFA to ``bseg_ffa`` segments, then one pruning run per reference segment
+    (reference ``EPMultiPass``: same arguments; ``device_id`` added)."""
+
+    def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
+                 max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
+                 show_progress: bool = False, use_conservative_tile: bool = False, device_id: int = 0):
+        if poly_basis != "taylor":
+            raise NotImplementedError("only the Taylor basis is implemented")
+        self._cfg = cfg
+        self._thr = np.ascontiguousarray(threshold_scheme, dtype=np.float32)
+        self._n_runs = n_runs
+        self._ref_segs = ref_segs
+        self._ffa = FFACUDA(cfg, device_id)
+        self._prune = PruneCUDA(cfg, max_sugg, batch_size, None, use_conservative_tile, device_id)
+        self._device = device_id
+
+    @property
+    def ffa(self) -> FFACUDA:
+        return self._ffa
+
+    def execute(self, ts_e, ts_v, outdir: str | None = None, file_prefix: str = "test") -> dict:
+        """Returns {ref_seg: {"stats", "leaves", "folds", "scores"}}; with ``outdir``
+        also writes ``<prefix>_pruning_nstages_<n>_results.npz`` and a text log."""
+        fold = self._ffa.execute(D.to_device_f32(ts_e, self._device), D.to_device_f32(ts_v, self._device))
+        nseg = int(self._ffa.plan.nsegments[-1])
+        results = {}
+        for ref_seg in determine_ref_segs(nseg, self._n_runs, self._ref_segs):
+            stats = self._prune.run(fold, ref_seg, self._thr, n_iters=nseg - 1)
+            leaves, folds, scores = self._prune.tree()
+            results[ref_seg] = {"stats": stats, "leaves": leaves, "folds": folds, "scores": scores}
+        if outdir is not None:
+            os.makedirs(outdir, exist_ok=True)
+            base = os.path.join(outdir, f"{file_prefix}_pruning_nstages_{nseg}")
+            arrays = {}
+            with open(base + "_log.txt", "w") as log:
+                log.write("Pruning log\n")
+                for rs, r in results.items():
+                    log.write(f"Pruning log for ref segment: {rs}\n")
+                    for row in r["stats"]:
+                        log.write(f"level {int(row['level'])} seg {int(row['seg_idx'])} thr {row['threshold']:.3f} "
+                                  f"branches {int(row['n_branches'])} leaves {int(row['n_leaves'])} "
+                                  f"survivors {int(row['n_leaves_surv'])} "
+                                  f"score [{row['score_min']:.3f}, {row['score_max']:.3f}]\n")
+                    for k in ("stats", "leaves", "scores"):
+                        arrays[f"{rs:03d}_{k}"] = r[k]
+            np.savez(base + "_results.npz", **arrays)
+        return results

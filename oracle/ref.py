@@ -95,6 +95,7 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
         L.lkref_shift_add_batch.argtypes = [vp, vp, vp, vp, vp, vp, u64, u64, u64, u64]
         L.lkref_score_filter.argtypes = [vp, u64, u64, vp, u64, f32, vp, vp, vp]
         L.lkref_branch_max.argtypes = [vp, ctypes.c_int, vp]
+        L.lkref_branching_pattern.argtypes = [vp, ctypes.c_int, u64, vp, u64, vp]
         L.lkref_prune_run.argtypes = [vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64, u64,
                                       vp, vp, vp, vp, vp, u64, vp]
         _libs[path] = L
@@ -328,6 +329,15 @@ def score_filter(folds, nbins, widths, threshold):
     _check(L, L.lkref_score_filter(_p(folds), n, nbins, _p(w), w.size, threshold, _p(scores), _p(idx),
                                    ctypes.byref(npass)))
     return scores, idx[: npass.value]
+
+
+def branching_pattern(cfg: RefCfg, ref_seg=0, conservative=False) -> np.ndarray:
+    L = lib()
+    out = np.zeros(4096, np.float64)
+    n = u64()
+    _check(L, L.lkref_branching_pattern(ctypes.byref(cfg), int(conservative), ref_seg, _p(out), out.size,
+                                        ctypes.byref(n)))
+    return out[: n.value].copy()
 
 
 def branch_max(cfg: RefCfg, conservative=False) -> int:

@@ -444,6 +444,18 @@ int lkref_branch_max(const lkref_cfg* c, int conservative, uint64_t* out) {
     });
 }
 
+// FFAPlan::get_branching_pattern("taylor", ref_seg) (lib/plans.cpp:219-259).
+int lkref_branching_pattern(const lkref_cfg* c, int conservative, uint64_t ref_seg,
+                            double* out, uint64_t max_out, uint64_t* n_out) {
+    return guarded([&] {
+        const auto cfg = make_cfg_prune(c, conservative);
+        const loki::plans::FFAPlan<float> plan(cfg);
+        const auto bp = plan.get_branching_pattern("taylor", ref_seg);
+        *n_out = bp.size();
+        std::copy_n(bp.begin(), std::min<uint64_t>(bp.size(), max_out), out);
+    });
+}
+
 // Per-level statistics (cands::PruneStats fields).
 struct lkref_prune_stats {
     uint64_t level;

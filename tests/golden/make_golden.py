@@ -2,7 +2,8 @@
 
 Run from the repository root after ``make -C oracle ref``:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py prune    # the pruning fixtures only
 
 Every output comes from ``oracle/_ref/libloki_ref_parity.so`` -- the
 reference's CPU sources compiled unmodified with IEEE flags -- so the fixtures
@@ -104,5 +105,51 @@ def main() -> None:
     print("done")
 
 
+# Pruning runs: name -> (nsamps, tsamp, nbins, eta, param_limits, bseg_ffa, seed,
+# max_sugg, batch_size, thr_lo, thr_hi, conservative). The small world-tree
+# capacities force the overload path (threshold raised by order statistics).
+PRUNE_CASES = {
+    "prune_accel_nb16": (16384, 8e-3, 16, 1.0, [[-1000.0, 1000.0], [10.0, 10.3]], 2048, 5,
+                         64, 8, 1.0, 2.5, False),
+    "prune_jerk_nb16": (16384, 8e-3, 16, 1.0, [[-100.0, 100.0], [-900.0, 900.0], [10.0, 10.2]],
+                        2048, 6, 64, 8, 1.0, 2.5, True),
+}
+
+
+def prune_fixtures() -> None:
+    """Inputs (the reference's final FFA fold) and outputs of whole pruning
+    runs (PruneImpl over the reference's PruneDPFuncts and WorldTree), plus
+    branching patterns."""
+    for name, (ns, ts, nb, eta, lims, bf, seed, ms, bs, lo, hi, cons) in PRUNE_CASES.items():
+        cfg = ref.make_cfg(ns, ts, nb, eta, lims, bseg_ffa=bf)
+        ffa = ref.RefFFA(cfg)
+        ts_e, ts_v = series(ns, seed)
+        fold = ffa.execute(ts_e, ts_v).copy()
+        nseg = int(ffa.nsegments[-1])
+        bmax = ref.branch_max(cfg, cons)
+        thr = np.linspace(lo, hi, nseg - 1).astype(np.float32)
+        ref_seg = nseg // 2
+        stats, leaves, folds, scores = ref.prune_run(cfg, fold, thr, ref_seg, ms, bs, bmax, nseg - 1, nb, cons)
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"),
+            nsamps=ns, tsamp=ts, nbins=nb, eta=eta, param_limits=np.array(lims, dtype=np.float64),
+            bseg_ffa=bf, ffa_fold=fold, thresholds=thr, ref_seg=ref_seg, max_sugg=ms, batch_size=bs,
+            branch_max=bmax, conservative=int(cons),
+            stats=np.stack([stats[k].astype(np.float64) for k in
+                            ("level", "seg_idx", "n_branches", "n_leaves", "n_leaves_phy",
+                             "n_leaves_surv", "threshold", "score_min", "score_max")], axis=1),
+            leaves=leaves, folds=folds, scores=scores,
+            branching_pattern=ref.branching_pattern(cfg, 0, cons),
+            branching_pattern_ref=ref.branching_pattern(cfg, ref_seg, cons),
+        )
+        print(name, "nsegments", nseg, "survivors", leaves.shape[0])
+
+
 if __name__ == "__main__":
-    main()
+    if not ref.available():
+        raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` first")
+    if len(sys.argv) > 1 and sys.argv[1] == "prune":
+        prune_fixtures()
+    else:
+        main()
+        prune_fixtures()
