@@ -94,12 +94,10 @@ float* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t last,
     const bool taylor = plan.nparams > 1;
     const auto nbins = static_cast<uint32_t>(plan.cfg.nbins);
     float* in = (last == 0 && final_out != nullptr) ? final_out : buf[0].as<float>();
-    // Algorithmic bytes: the series in (E and V) for the transpose and the
-    // fold; each level reads the previous level and writes its own.
+    // Algorithmic bytes: the series in (E and V) and the level-0 fold out;
+    // each merge level reads the previous level and writes its own.
     const uint64_t series_bytes = 8 * plan.cfg.nsamps;
-    prof.begin(LK_STAGE_TRANSPOSE, -1, 1, 2 * series_bytes, s);
-    bf->transpose(ts_e, ts_v, s);
-    prof.end(s);
+    bf->bind_inputs(ts_e, ts_v, s);
     prof.begin(LK_STAGE_BRUTE_FOLD, 0, 1, series_bytes + 4 * plan.fold_size(0), s);
     bf->fold(in, s);
     prof.end(s);

@@ -41,22 +41,23 @@ struct DeviceBuffer {
 // Brute fold of a time series into [nseg, nfreq, 2, nbins] FP32.
 //
 // Plan-time tables: for every trial frequency the sample -> phase-bin map of
-// one segment (identical for all segments) is encoded as the runs of equal
-// bin in sample order, split at chunk boundaries. Replaying the runs in order
-// adds every sample to its bin in increasing sample order, which is the
-// reference's summation order (lib/kernels.cpp:550-580), so the fold is
-// bit-identical.
+// one segment (identical for all segments) is encoded as run-start bits per
+// 32 samples plus the bin of each run. Replaying the runs in order adds every
+// sample to its bin in increasing sample order, which is the reference's
+// summation order (lib/kernels.cpp:550-580), so the fold is bit-identical.
 class BruteFoldDevice {
 public:
     BruteFoldDevice(const std::vector<double>& freqs, uint64_t segment_len, uint64_t nbins,
                     uint64_t nsamps, double tsamp, double t_ref, uint32_t* d_status);
-    // Enqueue: transpose the input into the segment-interleaved scratch, then
-    // fold. d_fold must hold nseg * nfreq * 2 * nbins floats.
+    // Enqueue the fold of (d_ts_e, d_ts_v); d_fold must hold nseg * nfreq * 2 *
+    // nbins floats.
     void execute(const float* d_ts_e, const float* d_ts_v, float* d_fold, cudaStream_t s) {
-        transpose(d_ts_e, d_ts_v, s);
+        bind_inputs(d_ts_e, d_ts_v, s);
         fold(d_fold, s);
     }
-    void transpose(const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
+    // Points the input tensor maps at the series (host work; a misaligned
+    // series is first copied into an aligned buffer on `s`).
+    void bind_inputs(const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
     void fold(float* d_fold, cudaStream_t s);
     uint64_t nseg() const { return m_nseg; }
     uint64_t nfreq() const { return m_nfreq; }
@@ -64,18 +65,21 @@ public:
     uint64_t device_bytes() const;
 
 private:
-    uint64_t m_nfreq, m_seglen, m_nbins, m_nsamps, m_nseg = 0, m_nseg_pad = 0;
-    uint64_t m_chunk = 0, m_nchunks = 0;
-    uint32_t m_spl = 1;       // segments per lane (1, 2 or 4)
-    uint32_t m_rows = 2;      // rows (E, V) per consumer warp (1 or 2)
-    uint32_t m_warps = 0;     // consumer warps per block
-    size_t m_smem = 0;        // dynamic shared memory per block
+    uint64_t m_nfreq, m_seglen, m_nbins, m_nsamps, m_nseg = 0;
+    uint64_t m_nwords = 0;
+    bool m_wide_bins = false;  // uint16 run bins (nbins > 256)
+    uint32_t m_warps = 0;      // consumer warps (frequencies) per block
+    uint32_t m_stages = 0;     // shared-memory ring depth (32-sample words)
+    size_t m_smem = 0;         // dynamic shared memory per block
     uint32_t* m_status;
-    DeviceBuffer m_entries;   // uint32 (bin << 16 | run length), all frequencies
-    DeviceBuffer m_offsets;   // uint64 first entry of each frequency
-    DeviceBuffer m_counts;    // uint8 [nfreq][nchunks] entries per chunk
-    DeviceBuffer m_xT;        // float [2][seglen][nseg_pad]
-    CUtensorMap m_tmap{};
+    DeviceBuffer m_masks;      // uint32 [nfreq][ceil(seglen / 32)] run-start bits
+    DeviceBuffer m_bins;       // run bins, all frequencies
+    DeviceBuffer m_bin_off;    // uint64 first run of each frequency
+    DeviceBuffer m_nruns;      // uint64 runs of each frequency
+    DeviceBuffer m_stage;      // aligned copy of a misaligned series
+    CUtensorMap m_tmap_e{}, m_tmap_v{};
+    const float* m_map_e_ptr = nullptr;
+    const float* m_map_v_ptr = nullptr;
 };
 
 // One merge level: out[s, c] = rot(in[2s, tail(c)], st(c)) + rot(in[2s+1, head(c)], sh(c)).

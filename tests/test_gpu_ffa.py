@@ -65,6 +65,40 @@ def test_brute_fold_bit_exact(cuda, name):
     np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
+@pytest.mark.parametrize("seglen", [4, 16, 96, 160])
+def test_brute_fold_short_and_partial_segments(cuda, seglen):
+    """Segment lengths that are not whole 64-sample stages or 32-sample words."""
+    from loki_b200.fold import compute_brute_fold_time_cuda
+
+    n = seglen * 40
+    ts_e, ts_v = series(n, 31 + seglen)
+    freqs = np.linspace(90.0, 400.0, 13)
+    got = compute_brute_fold_time_cuda(ts_e, ts_v, freqs, seglen, 16, 1e-3, 0.0)
+    want = lko.brute_fold(ts_e, ts_v, freqs, seglen, 16, 1e-3, 0.0)
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_brute_fold_misaligned_and_rebound_inputs(cuda):
+    """Series views that are not 16-byte aligned go through an aligned copy;
+    switching between input buffers rebinds the tensor maps."""
+    from loki_b200.fold import BruteFoldCUDA
+
+    t = cuda
+    cfg, op, _ = make("accel_multi_nb32")
+    n = cfg.nsamps
+    seglen = int(op.segment_lens[0])
+    bf = BruteFoldCUDA(op.freqs0(), seglen, cfg.nbins, n, cfg.tsamp, op.t_ref0())
+    for seed, offset in ((21, 1), (22, 0), (23, 3)):
+        ts_e, ts_v = series(n, seed)
+        be = t.zeros(n + 4, dtype=t.float32, device="cuda")
+        bv = t.zeros(n + 4, dtype=t.float32, device="cuda")
+        be[offset:offset + n] = t.from_numpy(ts_e).cuda()
+        bv[offset:offset + n] = t.from_numpy(ts_v).cuda()
+        got = bf.execute(be[offset:offset + n], bv[offset:offset + n]).cpu().numpy()
+        want = lko.brute_fold(ts_e, ts_v, op.freqs0(), seglen, cfg.nbins, cfg.tsamp, op.t_ref0())
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_ffa_fold_and_scores_bit_exact(cuda, name):
     from loki_b200.ffa import FFACUDA
