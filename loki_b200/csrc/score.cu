@@ -18,6 +18,7 @@
 // of a different row, hit 32 different banks.
 #include <cfloat>
 #include <cmath>
+#include <type_traits>
 
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
@@ -61,7 +62,12 @@ __global__ void score_kernel(const float* __restrict__ folds, uint64_t nprof, ui
 // shared memory, then scored; the final fold never reaches global memory.
 // Block = up to T consecutive frequency cells of one outer row; blocks are
 // numbered frequency-tile-major (see merge.cu).
-template <bool TAYLOR, int NW>
+//
+// Phase 1 keeps many loads in flight: a warp takes PB profiles at a time,
+// loads their coordinates with one lane each, then issues every tail/head
+// load of the PB profiles (NJ = ceil(nbins / 32) bins per lane; NJ == 0
+// selects a generic loop for large nbins) before the first add.
+template <bool TAYLOR, int NW, int NJ, int PB>
 __global__ void merge_score_kernel(const float* __restrict__ in, const void* __restrict__ coords,
                                    uint32_t n_inner, uint32_t n_outer, uint64_t nprev,
                                    uint32_t nbins, uint32_t rs, ScoreParams sp, int mode,
@@ -76,18 +82,64 @@ __global__ void merge_score_kernel(const float* __restrict__ in, const void* __r
     const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
     const uint32_t plen = 2 * nbins;
     const float* head_base = in + nprev * plen;  // segment 1 of the previous level
+    if constexpr (NJ == 0) {
 #pragma unroll 2
-    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
-        const MergeCoord mc = load_merge_coord<TAYLOR>(coords, c0 + p, nbins);
-        const float* tail = in + static_cast<uint64_t>(mc.it) * plen;
-        const float* head = head_base + static_cast<uint64_t>(mc.ih) * plen;
-        float* dst = rows + static_cast<size_t>(p) * rs;
-        for (uint32_t j = lane; j < nbins; j += kWarp) {
-            const uint32_t jt = j >= mc.st ? j - mc.st : j + nbins - mc.st;
-            const uint32_t jh = j >= mc.sh ? j - mc.sh : j + nbins - mc.sh;
-            const float e = __fadd_rn(__ldg(tail + jt), __ldg(head + jh));
-            const float v = __fadd_rn(__ldg(tail + nbins + jt), __ldg(head + nbins + jh));
-            dst[j] = normalise(e, v);
+        for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+            const MergeCoord mc = load_merge_coord<TAYLOR>(coords, c0 + p, nbins);
+            const float* tail = in + static_cast<uint64_t>(mc.it) * plen;
+            const float* head = head_base + static_cast<uint64_t>(mc.ih) * plen;
+            float* dst = rows + static_cast<size_t>(p) * rs;
+            for (uint32_t j = lane; j < nbins; j += kWarp) {
+                const uint32_t jt = j >= mc.st ? j - mc.st : j + nbins - mc.st;
+                const uint32_t jh = j >= mc.sh ? j - mc.sh : j + nbins - mc.sh;
+                const float e = __fadd_rn(__ldg(tail + jt), __ldg(head + jh));
+                const float v = __fadd_rn(__ldg(tail + nbins + jt), __ldg(head + nbins + jh));
+                dst[j] = normalise(e, v);
+            }
+        }
+    } else {
+        for (uint32_t p0 = warp * PB; p0 < nhere; p0 += (T / kWarp) * PB) {
+            MergeCoord mine{0, 0, 0, 0};
+            if (lane < PB && p0 + lane < nhere) {
+                mine = load_merge_coord<TAYLOR>(coords, c0 + p0 + lane, nbins);
+            }
+            float te[PB][NJ], tv[PB][NJ], he[PB][NJ], hv[PB][NJ];
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+                const uint32_t it = __shfl_sync(0xffffffffu, mine.it, q);
+                const uint32_t ih = __shfl_sync(0xffffffffu, mine.ih, q);
+                const uint32_t st = __shfl_sync(0xffffffffu, mine.st, q);
+                const uint32_t sh = __shfl_sync(0xffffffffu, mine.sh, q);
+                const bool live = p0 + q < nhere;
+                const float* tail = in + static_cast<uint64_t>(it) * plen;
+                const float* head = head_base + static_cast<uint64_t>(ih) * plen;
+#pragma unroll
+                for (int u = 0; u < NJ; ++u) {
+                    const uint32_t jr = lane + 32u * u;
+                    const bool ok = live && jr < nbins;
+                    const uint32_t j = ok ? jr : 0u;  // keep every address inside the rows
+                    const uint32_t jt = j >= st ? j - st : j + nbins - st;
+                    const uint32_t jh = j >= sh ? j - sh : j + nbins - sh;
+                    te[q][u] = ok ? __ldg(tail + jt) : 0.0f;
+                    tv[q][u] = ok ? __ldg(tail + nbins + jt) : 1.0f;
+                    he[q][u] = ok ? __ldg(head + jh) : 0.0f;
+                    hv[q][u] = ok ? __ldg(head + nbins + jh) : 1.0f;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+                if (p0 + q < nhere) {
+                    float* dst = rows + static_cast<size_t>(p0 + q) * rs;
+#pragma unroll
+                    for (int u = 0; u < NJ; ++u) {
+                        const uint32_t j = lane + 32u * u;
+                        if (j < nbins) {
+                            dst[j] = normalise(__fadd_rn(te[q][u], he[q][u]),
+                                               __fadd_rn(tv[q][u], hv[q][u]));
+                        }
+                    }
+                }
+            }
         }
     }
     __syncthreads();
@@ -168,14 +220,26 @@ void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uin
                                      d_scores);
     };
     const int nwb = sp.nwidths <= 8 ? 8 : (sp.nwidths <= 16 ? 16 : 32);
+    const int nj = nbins <= 32 ? 1 : (nbins <= 64 ? 2 : (nbins <= 128 ? 4 : 0));
+    // Dispatch (taylor, width bucket, bins per lane); PB * NJ = 16 loads of
+    // each kind in flight per lane.
+    auto pick = [&](auto tg) {
+        constexpr bool TG = decltype(tg)::value;
+        auto by_nj = [&](auto nwc) {
+            constexpr int NWC = decltype(nwc)::value;
+            if (nj == 1) launch(merge_score_kernel<TG, NWC, 1, 16>);
+            else if (nj == 2) launch(merge_score_kernel<TG, NWC, 2, 8>);
+            else if (nj == 4) launch(merge_score_kernel<TG, NWC, 4, 4>);
+            else launch(merge_score_kernel<TG, NWC, 0, 1>);
+        };
+        if (nwb == 8) by_nj(std::integral_constant<int, 8>{});
+        else if (nwb == 16) by_nj(std::integral_constant<int, 16>{});
+        else by_nj(std::integral_constant<int, 32>{});
+    };
     if (taylor) {
-        if (nwb == 8) launch(merge_score_kernel<true, 8>);
-        else if (nwb == 16) launch(merge_score_kernel<true, 16>);
-        else launch(merge_score_kernel<true, 32>);
+        pick(std::true_type{});
     } else {
-        if (nwb == 8) launch(merge_score_kernel<false, 8>);
-        else if (nwb == 16) launch(merge_score_kernel<false, 16>);
-        else launch(merge_score_kernel<false, 32>);
+        pick(std::false_type{});
     }
     LK_CUDA(cudaGetLastError());
 }
