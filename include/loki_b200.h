@@ -29,6 +29,8 @@
  *                     (include/loki/core/taylor.hpp:16-79), kernels::shift_add_linear_batch
  *                     (lib/loki/kernels.hpp:100), detection::score_and_filter_max_with_cache
  *                     (include/loki/detection/score.hpp:113-119)
+ *   lk_mc_*           simulate_score_prune_fused of DynamicThresholdScheme
+ *                     (lib/thresholds.cpp:358-431)
  */
 #ifndef LOKI_B200_H
 #define LOKI_B200_H
@@ -325,6 +327,41 @@ int lk_shift_add_batch(const float* d_folds_tree, const uint32_t* d_indices_tree
 int lk_score_filter(const float* d_folds, uint64_t n, uint32_t nbins, const uint32_t* widths,
                     uint32_t nwidths, float threshold, float* d_scores, uint32_t* d_indices,
                     uint64_t* d_count, lk_stream_t stream);
+
+/* ---- Monte-Carlo threshold stage ------------------------------------------ */
+/* simulate_score_prune_fused of the reference's DynamicThresholdScheme
+ * (lib/thresholds.cpp:358-431) with detection::snr_boxcar_threshold_with_cache
+ * (lib/score.cpp:434-462), one launch sequence per stage:
+ *   out_i = (in[src_i] + noise[row_i]) + signal * signal_scale   (FP32, this order)
+ *   kept  = max over widths of S/N_w / sqrt(var_in + var_add) > threshold
+ * where row_i = rowmap[i] (NULL: i) selects the noise row and, when
+ * signal_per_trial, the signal row ([nbins] shared otherwise); src NULL
+ * means src_i = i. Kept trials' folds are written to d_folds_out in trial
+ * order, their noise rows to d_ids_out (may be NULL), their number to
+ * *d_count; d_counts[k] = trials whose maximum S/N > thresholds[k] (host
+ * array of n_thr <= 64 entries); with d_class (one byte per noise row, may
+ * be NULL) d_counts[n_thr + k] counts the same among trials whose row is
+ * flagged (e.g. the ones carrying a signal, for detection probabilities).
+ * d_max_snr (may be NULL) receives every trial's maximum S/N. The noise is
+ * the caller's (drawn on the host, so the CPU reference can use the same
+ * numbers). */
+typedef struct lk_mc lk_mc;
+int lk_mc_create(uint64_t max_trials, uint32_t nbins, const uint32_t* widths, uint32_t nwidths,
+                 int device, lk_mc** out);
+void lk_mc_destroy(lk_mc* mc);
+/* ntrials_in: rows of d_folds_in; nrows: rows of d_noise (and of d_signal
+ * when signal_per_trial). A src or rowmap entry outside them is read as row
+ * 0 and flagged; lk_mc_status reports (and clears) the flag. */
+int lk_mc_stage(lk_mc* mc, const float* d_folds_in, uint64_t ntrials_in, const uint32_t* d_src,
+                uint64_t ntrials, const float* d_noise, uint64_t nrows, const float* d_signal,
+                int signal_per_trial,
+                float signal_scale, const uint32_t* d_rowmap, float var_in, float var_add,
+                float threshold, const float* thresholds, uint32_t n_thr,
+                const uint8_t* d_class, float* d_folds_out, uint32_t* d_ids_out,
+                uint64_t* d_count, uint64_t* d_counts, float* d_max_snr, lk_stream_t stream);
+/* Synchronises the stream; *status = non-zero when an index was out of range
+ * since the last call (and clears it). */
+int lk_mc_status(lk_mc* mc, lk_stream_t stream, uint32_t* status);
 
 #ifdef __cplusplus
 }

@@ -145,6 +145,11 @@ SIGNATURES = [
     ("lk_compact_scratch_bytes", u64, [u64]),
     ("lk_compact_ge", i32, [vp, u64, f32, vp, vp, u64, vp, vp, vp]),
     ("lk_compact_ge_noalloc", i32, [vp, u64, f32, vp, vp, u64, vp, vp]),
+    ("lk_mc_create", i32, [u64, u32, vp, u32, i32, vp]),
+    ("lk_mc_destroy", None, [vp]),
+    ("lk_mc_stage", i32, [vp, vp, u64, vp, u64, vp, u64, vp, i32, f32, vp, f32, f32, f32, vp, u32, vp, vp, vp,
+                          vp, vp, vp, vp]),
+    ("lk_mc_status", i32, [vp, vp, vp]),
     ("lk_prune_create", i32, [vp, u64, u64, u64, i32, i32, vp]),
     ("lk_prune_destroy", None, [vp]),
     ("lk_plan_branching_pattern", i32, [vp, u64, i32, vp, u64, vp]),

@@ -9,6 +9,7 @@
 
 #include "lk_ffa.hpp"
 #include "lk_kernels.hpp"
+#include "lk_mc.hpp"
 #include "lk_prune.hpp"
 
 struct lk_plan {
@@ -16,6 +17,9 @@ struct lk_plan {
 };
 struct lk_ffa {
     std::unique_ptr<lk::FFAExec> exec;
+};
+struct lk_mc {
+    std::unique_ptr<lk::McExec> exec;
 };
 struct lk_prune {
     std::unique_ptr<lk::PruneExec> exec;
@@ -540,6 +544,74 @@ int lk_score_filter(const float* d_folds, uint64_t n, uint32_t nbins, const uint
         lk::compact_ge(d_scores, n, threshold, d_indices, vals.as<float>(), n, d_count,
                        scratch.ptr, s);
         LK_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+// ---- Monte-Carlo threshold stage ----------------------------------------------
+
+int lk_mc_create(uint64_t max_trials, uint32_t nbins, const uint32_t* widths, uint32_t nwidths,
+                 int device, lk_mc** out) {
+    return guarded([&] {
+        need(widths, "widths");
+        need(out, "out");
+        auto h = std::make_unique<lk_mc>();
+        h->exec = std::make_unique<lk::McExec>(max_trials, nbins, widths, nwidths, device);
+        *out = h.release();
+    });
+}
+
+void lk_mc_destroy(lk_mc* mc) { delete mc; }
+
+int lk_mc_stage(lk_mc* mc, const float* d_folds_in, uint64_t ntrials_in, const uint32_t* d_src,
+                uint64_t ntrials, const float* d_noise, uint64_t nrows, const float* d_signal,
+                int signal_per_trial,
+                float signal_scale, const uint32_t* d_rowmap, float var_in, float var_add,
+                float threshold, const float* thresholds, uint32_t n_thr,
+                const uint8_t* d_class, float* d_folds_out, uint32_t* d_ids_out,
+                uint64_t* d_count, uint64_t* d_counts, float* d_max_snr, lk_stream_t stream) {
+    return guarded([&] {
+        need(mc, "mc");
+        need(d_count, "d_count");
+        if (ntrials > 0) {
+            need(d_folds_in, "d_folds_in");
+            need(d_noise, "d_noise");
+            need(d_signal, "d_signal");
+            need(d_folds_out, "d_folds_out");
+        }
+        if (n_thr > 0) {
+            need(d_counts, "d_counts");
+        }
+        lk::McStage st;
+        st.d_folds_in = d_folds_in;
+        st.ntrials_in = ntrials_in;
+        st.d_src = d_src;
+        st.ntrials = ntrials;
+        st.d_noise = d_noise;
+        st.nrows = nrows;
+        st.d_signal = d_signal;
+        st.signal_per_trial = signal_per_trial != 0;
+        st.signal_scale = signal_scale;
+        st.d_rowmap = d_rowmap;
+        st.var_in = var_in;
+        st.var_add = var_add;
+        st.threshold = threshold;
+        st.thresholds = thresholds;
+        st.n_thr = n_thr;
+        st.d_class = d_class;
+        st.d_folds_out = d_folds_out;
+        st.d_ids_out = d_ids_out;
+        st.d_count = d_count;
+        st.d_counts = d_counts;
+        st.d_max_snr = d_max_snr;
+        mc->exec->stage(st, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_mc_status(lk_mc* mc, lk_stream_t stream, uint32_t* status) {
+    return guarded([&] {
+        need(mc, "mc");
+        need(status, "status");
+        *status = mc->exec->read_status(reinterpret_cast<cudaStream_t>(stream));
     });
 }
 

@@ -69,6 +69,48 @@ __device__ __forceinline__ void score_row(float* r, uint32_t nbins, float inv_st
     }
 }
 
+// Largest S/N of the (raw, 2-D) profile staged at r with every width's S/N
+// divided by stdnoise, as detection::snr_boxcar_threshold_with_cache does
+// (lib/score.cpp:434-462). Prefix sums are written in place.
+template <int NW>
+__device__ __forceinline__ float max_snr_div(float* r, uint32_t nbins, float stdnoise,
+                                             const ScoreParams& sp) {
+    float acc = r[0];
+    for (uint32_t j = 1; j < nbins; ++j) {
+        acc = __fadd_rn(acc, r[j]);
+        r[j] = acc;
+    }
+    const float sum = acc;
+    for (uint32_t k = 0; k < sp.wmax; ++k) {
+        r[nbins + k] = __fadd_rn(r[k], sum);
+    }
+    float dm[NW];
+#pragma unroll
+    for (int iw = 0; iw < NW; ++iw) {
+        dm[iw] = -FLT_MAX;
+    }
+    for (uint32_t i = 0; i < nbins; ++i) {
+        const float ri = r[i];
+#pragma unroll
+        for (int iw = 0; iw < NW; ++iw) {
+            if (iw < static_cast<int>(sp.nwidths)) {
+                const float d = __fsub_rn(r[i + sp.widths[iw]], ri);
+                dm[iw] = (dm[iw] < d) ? d : dm[iw];
+            }
+        }
+    }
+    float best = -FLT_MAX;
+#pragma unroll
+    for (int iw = 0; iw < NW; ++iw) {
+        if (iw < static_cast<int>(sp.nwidths)) {
+            const float base = __fsub_rn(__fmul_rn(sp.hb[iw], dm[iw]), __fmul_rn(sp.b[iw], sum));
+            const float snr = __fdiv_rn(base, stdnoise);
+            best = (best < snr) ? snr : best;
+        }
+    }
+    return best;
+}
+
 // Profiles per block so that the staged rows fit comfortably in shared memory.
 inline uint32_t profiles_per_block(uint32_t rs) {
     const size_t per = static_cast<size_t>(rs) * sizeof(float);

@@ -1,0 +1,237 @@
+// Monte-Carlo threshold stage on the GPU: one fused pass that builds every
+// trial's next-stage fold, scores it and counts it against a threshold grid,
+// then the ordered compaction of the trials above the pruning threshold.
+//
+// Reference: simulate_score_prune_fused (lib/thresholds.cpp:358-431) with
+// detection::snr_boxcar_threshold_with_cache (lib/score.cpp:434-462):
+//   out_i   = (in[src_i] + noise_i) + signal * scale      (FP32, this order)
+//   S/N_w   = ((h_w + b_w) * dmax_w - b_w * sum) / sqrt(var_in + var_add)
+//   survive = S/N_w > threshold for some w  (= max_w S/N_w > threshold)
+// The noise is drawn on the host (the reference's generator is seeded from
+// std::random_device, so its draws are not reproducible) and passed in, so
+// the device and the CPU oracle see the same numbers; survivors keep the
+// reference's trial order.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <limits>
+#include <type_traits>
+
+#include "lk_device.cuh"
+#include "lk_mc.hpp"
+#include "lk_score.cuh"
+
+namespace lk {
+
+namespace {
+
+constexpr uint32_t kWarp = 32;
+
+struct McArgs {
+    const float* in;
+    const uint32_t* src;      // NULL: trial i reads input row i
+    const float* noise;
+    const float* signal;
+    const uint32_t* rowmap;   // NULL: noise / per-trial signal row of trial i is i
+    uint64_t n;
+    uint64_t n_in;            // rows in `in`
+    uint64_t n_rows;          // rows in `noise` (and in `signal` when per_trial)
+    uint32_t nbins;
+    uint32_t* status;         // bad-index flag
+    int per_trial;
+    float scale;
+    float stdnoise;
+    const float* thr;         // threshold grid (device), n_thr entries
+    uint32_t n_thr;
+    const uint8_t* cls;       // optional: class flag of each noise row
+    float* max_snr;
+    unsigned long long* counts;
+};
+
+// Input row and noise row of trial i; an index outside its buffer is
+// replaced by row 0 and flagged (the entry point then reports an error).
+struct TrialRows {
+    uint64_t in, noise;
+};
+__device__ __forceinline__ TrialRows trial_rows(const McArgs& a, uint64_t i, bool flag) {
+    uint64_t s = a.src != nullptr ? a.src[i] : i;
+    uint64_t rw = a.rowmap != nullptr ? a.rowmap[i] : i;
+    if (s >= a.n_in || rw >= a.n_rows) {
+        if (flag) {
+            atomicOr(a.status, dev::kStatusBadTable);
+        }
+        s = s >= a.n_in ? 0 : s;
+        rw = rw >= a.n_rows ? 0 : rw;
+    }
+    return {s, rw};
+}
+
+__device__ __forceinline__ float stage_value(const McArgs& a, TrialRows t, uint32_t j) {
+    const float* sg = a.signal + (a.per_trial ? t.noise * a.nbins : 0);
+    return __fadd_rn(__fadd_rn(__ldg(a.in + t.in * a.nbins + j), __ldg(a.noise + t.noise * a.nbins + j)),
+                     __fmul_rn(__ldg(sg + j), a.scale));
+}
+
+// Block of T trials: warps build the folds in shared memory (lanes over
+// bins), then one thread per trial scores its fold; the block's threshold
+// counts are summed in shared memory and added to the global counts once.
+template <int NW>
+__global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
+    extern __shared__ float rows[];
+    __shared__ unsigned int s_cnt[2 * LK_MC_MAX_THRESHOLDS];
+    const uint32_t T = blockDim.x;
+    const uint64_t p0 = static_cast<uint64_t>(blockIdx.x) * T;
+    const uint32_t nhere = static_cast<uint32_t>((a.n - p0) < T ? (a.n - p0) : T);
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    for (uint32_t k = threadIdx.x; k < 2 * a.n_thr; k += T) {
+        s_cnt[k] = 0;
+    }
+#pragma unroll 2
+    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+        float* dst = rows + static_cast<size_t>(p) * rs;
+        const TrialRows tr = trial_rows(a, p0 + p, lane == 0);
+        for (uint32_t j = lane; j < a.nbins; j += kWarp) {
+            dst[j] = stage_value(a, tr, j);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nhere) {
+        const float m = sc::max_snr_div<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, a.nbins,
+                                            a.stdnoise, sp);
+        const uint64_t i = p0 + threadIdx.x;
+        a.max_snr[i] = m;
+        const bool flagged = a.cls != nullptr && a.cls[trial_rows(a, i, false).noise] != 0;
+        for (uint32_t k = 0; k < a.n_thr; ++k) {
+            if (m > a.thr[k]) {
+                atomicAdd(&s_cnt[k], 1u);
+                if (flagged) {
+                    atomicAdd(&s_cnt[a.n_thr + k], 1u);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t ncnt = a.cls != nullptr ? 2 * a.n_thr : a.n_thr;
+    for (uint32_t k = threadIdx.x; k < ncnt; k += T) {
+        if (s_cnt[k] != 0) {
+            atomicAdd(&a.counts[k], static_cast<unsigned long long>(s_cnt[k]));
+        }
+    }
+}
+
+// Survivor k (trial idx[k], k < *d_count): rebuild its fold into out[k] and
+// record its noise row. One warp per survivor, grid-stride.
+__global__ void mc_gather_kernel(McArgs a, const uint32_t* __restrict__ idx,
+                                 const uint64_t* __restrict__ d_count, float* __restrict__ out,
+                                 uint32_t* __restrict__ ids_out) {
+    const uint64_t n = *d_count;
+    const uint64_t wpb = blockDim.x / kWarp;
+    const uint32_t lane = threadIdx.x % kWarp;
+    for (uint64_t k = blockIdx.x * wpb + threadIdx.x / kWarp; k < n; k += gridDim.x * wpb) {
+        const uint64_t i = idx[k];
+        const TrialRows tr = trial_rows(a, i, false);
+        for (uint32_t j = lane; j < a.nbins; j += kWarp) {
+            out[k * a.nbins + j] = stage_value(a, tr, j);
+        }
+        if (lane == 0 && ids_out != nullptr) {
+            ids_out[k] = static_cast<uint32_t>(tr.noise);
+        }
+    }
+}
+
+}  // namespace
+
+McExec::McExec(uint64_t max_trials, uint32_t nbins, const uint32_t* widths, uint32_t nwidths,
+               int device)
+    : m_max(max_trials), m_nbins(nbins), m_device(device) {
+    require(max_trials >= 1 && max_trials <= 0xffffffffULL, "max_trials must lie in [1, 2^32)");
+    m_sp = make_score_params(widths, nwidths, nbins);
+    DeviceGuard g(device);
+    m_max_snr.alloc(max_trials * sizeof(float));
+    m_idx.alloc(max_trials * sizeof(uint32_t));
+    m_vals.alloc(max_trials * sizeof(float));
+    m_scratch.alloc(compact_scratch_bytes(max_trials));
+    m_thr.alloc(LK_MC_MAX_THRESHOLDS * sizeof(float));
+    m_status.alloc(sizeof(uint32_t));
+    LK_CUDA(cudaMemset(m_status.ptr, 0, sizeof(uint32_t)));
+}
+
+uint32_t McExec::read_status(cudaStream_t s) {
+    DeviceGuard g(m_device);
+    uint32_t v = 0;
+    LK_CUDA(cudaMemcpyAsync(&v, m_status.ptr, sizeof(v), cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaStreamSynchronize(s));
+    LK_CUDA(cudaMemsetAsync(m_status.ptr, 0, sizeof(uint32_t), s));
+    return v;
+}
+
+uint64_t McExec::device_bytes() const {
+    return m_max_snr.bytes + m_idx.bytes + m_vals.bytes + m_scratch.bytes + m_thr.bytes +
+           m_status.bytes;
+}
+
+void McExec::stage(const McStage& st, cudaStream_t s) {
+    require(st.ntrials <= m_max, "ntrials exceeds the executor's max_trials");
+    require(st.ntrials == 0 || (st.ntrials_in > 0 && st.nrows > 0),
+            "ntrials_in and nrows must be positive");
+    require(st.n_thr <= LK_MC_MAX_THRESHOLDS, "at most 64 thresholds in the grid");
+    require(st.n_thr == 0 || st.thresholds != nullptr, "thresholds must not be NULL");
+    require(!(st.var_in + st.var_add < 0.0f), "var_in + var_add must not be negative");
+    DeviceGuard g(m_device);
+    if (st.n_thr > 0) {
+        const uint32_t ncnt = st.d_class != nullptr ? 2 * st.n_thr : st.n_thr;
+        LK_CUDA(cudaMemsetAsync(st.d_counts, 0, ncnt * sizeof(uint64_t), s));
+        LK_CUDA(cudaMemcpyAsync(m_thr.ptr, st.thresholds, st.n_thr * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    }
+    if (st.ntrials == 0) {
+        LK_CUDA(cudaMemsetAsync(st.d_count, 0, sizeof(uint64_t), s));
+        return;
+    }
+    McArgs a{};
+    a.in = st.d_folds_in;
+    a.src = st.d_src;
+    a.noise = st.d_noise;
+    a.signal = st.d_signal;
+    a.rowmap = st.d_rowmap;
+    a.n = st.ntrials;
+    a.n_in = st.ntrials_in;
+    a.n_rows = st.nrows;
+    a.nbins = m_nbins;
+    a.status = m_status.as<uint32_t>();
+    a.per_trial = st.signal_per_trial ? 1 : 0;
+    a.scale = st.signal_scale;
+    a.stdnoise = std::sqrt(st.var_in + st.var_add);  // float, as sqrt(var_new) in the reference
+    a.thr = m_thr.as<float>();
+    a.n_thr = st.n_thr;
+    a.cls = st.d_class;
+    a.max_snr = st.d_max_snr != nullptr ? st.d_max_snr : m_max_snr.as<float>();
+    a.counts = reinterpret_cast<unsigned long long*>(st.d_counts);
+    const uint32_t rs = sc::row_stride(m_nbins, m_sp.wmax);
+    const uint32_t T = sc::profiles_per_block(rs);
+    const size_t smem = static_cast<size_t>(T) * rs * sizeof(float);
+    const uint64_t blocks = (st.ntrials + T - 1) / T;
+    require(blocks <= 0x7fffffffULL, "too many trials");
+    auto launch = [&](auto kern) {
+        sc::set_smem(kern, smem);
+        kern<<<static_cast<unsigned>(blocks), T, smem, s>>>(a, rs, m_sp);
+    };
+    if (m_sp.nwidths <= 8) {
+        launch(mc_score_kernel<8>);
+    } else if (m_sp.nwidths <= 16) {
+        launch(mc_score_kernel<16>);
+    } else {
+        launch(mc_score_kernel<32>);
+    }
+    LK_CUDA(cudaGetLastError());
+    // S/N > threshold  <=>  S/N >= the next float above the threshold.
+    const float thr_ge = std::nextafter(st.threshold, std::numeric_limits<float>::infinity());
+    compact_ge(a.max_snr, st.ntrials, thr_ge, m_idx.as<uint32_t>(), m_vals.as<float>(),
+               st.ntrials, st.d_count, m_scratch.ptr, s);
+    const uint64_t gblocks = std::min<uint64_t>((st.ntrials + 7) / 8, 148 * 16);
+    mc_gather_kernel<<<static_cast<unsigned>(gblocks), 256, 0, s>>>(
+        a, m_idx.as<uint32_t>(), st.d_count, st.d_folds_out, st.d_ids_out);
+    LK_CUDA(cudaGetLastError());
+}
+
+}  // namespace lk

@@ -94,3 +94,37 @@ def taylor_accel_workload(seed: int = 7, n_signals: int = 4):
     params = dict(nsamps=nsamps, tsamp=tsamp, nbins=nbins, eta=2.0,
                   param_limits=[[-200.0, 200.0], [5.0, 50.0]], score_widths=widths)
     return ts_e, ts_v, params, pulsars
+
+
+def mc_cascade_workload(ntrials: int = 1 << 20, nbins: int = 64, nstages: int = 8, seed: int = 99,
+                        n_grid: int = 64):
+    """Monte-Carlo cascade inputs: ntrials folded profiles of nbins float32 bins,
+    N(0, 1) per bin plus a von Mises pulse (duty ~ U(2 %, 20 %), random phase)
+    scaled to an injected S/N ~ U(0, 20) against unit-variance noise. Stage s
+    (0-based) adds fresh noise of the input's variance (so the variance
+    doubles) and the signal again times 2**s (a coherent signal doubles too);
+    its pruning threshold rises linearly from 2 to 6 and every stage is counted
+    against the same 64-threshold grid (0 .. 16). Trials with injected
+    S/N >= 8 are flagged for the detection counts. All arrays come from one
+    numpy generator (seed), so the CPU and GPU paths see the same numbers."""
+    rng = np.random.default_rng(seed)
+    duty = rng.uniform(0.02, 0.20, ntrials)
+    snr = rng.uniform(0.0, 20.0, ntrials).astype(np.float32)
+    phase = rng.random(ntrials)
+    x = (np.arange(nbins) + 0.5) / nbins
+    kappa = np.log(2.0) / (1.0 - np.cos(np.pi * duty))
+    shape = np.exp(kappa[:, None] * (np.cos(2 * np.pi * (x[None, :] - phase[:, None])) - 1.0))
+    shape /= np.sqrt((shape ** 2).sum(axis=1, keepdims=True))
+    signal = (shape * snr[:, None]).astype(np.float32)
+    folds0 = (rng.standard_normal((ntrials, nbins), dtype=np.float32) + signal).astype(np.float32)
+    cls = (snr >= 8.0).astype(np.uint8)
+    noises = []
+    var = 1.0
+    for _ in range(nstages):
+        nz = rng.standard_normal((ntrials, nbins), dtype=np.float32)
+        nz *= np.float32(np.sqrt(var))
+        noises.append(nz)
+        var *= 2.0
+    thresholds = np.linspace(2.0, 6.0, nstages).astype(np.float32)
+    grids = [np.linspace(0.0, 16.0, n_grid).astype(np.float32) for _ in range(nstages)]
+    return folds0, signal, cls, noises, thresholds, grids

@@ -113,6 +113,11 @@ def lib() -> ctypes.CDLL:
         L.lko_shift_add_batch.argtypes = [vp, vp, vp, vp, vp, vp, u64, u64, u64, u64]
         L.lko_score_filter.restype = u64
         L.lko_score_filter.argtypes = [vp, u64, u64, vp, u64, f32, vp, vp]
+        L.lko_snr_max_div.restype = f32
+        L.lko_snr_max_div.argtypes = [vp, u64, vp, u64, f32]
+        L.lko_mc_stage.restype = u64
+        L.lko_mc_stage.argtypes = [vp, vp, u64, u64, vp, vp, ctypes.c_int, f32, vp, f32, f32, vp, u64, f32, vp,
+                                   u64, vp, vp, vp, vp, vp]
         L.lko_prune_run.argtypes = [vp, ctypes.c_int, vp, vp, u64, u64, u64, u64, u64, u64, vp, vp,
                                     vp, vp, vp, u64, vp]
         _lib = L
@@ -449,3 +454,41 @@ def prune_run(plan: OraclePlan, ffa_fold, thresholds, ref_seg, max_sugg, batch_s
     k = n.value
     return (stats[: nstats.value], leaves[: k * stride].reshape(k, plan.nparams + 2, 2),
             folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k])
+
+
+# ---- Monte-Carlo threshold stage -------------------------------------------------
+
+def snr_max_div(profiles, nbins, widths, stdnoise) -> np.ndarray:
+    p = np.ascontiguousarray(profiles, np.float32).reshape(-1, nbins)
+    w = np.ascontiguousarray(widths, np.uint64)
+    return np.array([lib().lko_snr_max_div(_p(np.ascontiguousarray(r)), nbins, _p(w), w.size, stdnoise)
+                     for r in p], np.float32)
+
+
+def mc_stage(folds_in, noise, signal, var_in, var_add, widths, threshold, thresholds=(), src=None,
+             signal_scale=1.0, rowmap=None, ntrials=None, cls=None):
+    """simulate_score_prune_fused: returns (survivor folds, survivor noise rows,
+    counts per threshold of the grid (then of the flagged rows, with cls),
+    max S/N per trial)."""
+    fin = np.ascontiguousarray(folds_in, np.float32)
+    nz = np.ascontiguousarray(noise, np.float32)
+    nbins = nz.shape[-1]
+    rm = None if rowmap is None else np.ascontiguousarray(rowmap, np.uint32)
+    if ntrials is None:
+        ntrials = rm.size if rm is not None else nz.shape[0]
+    sg = np.ascontiguousarray(signal, np.float32)
+    per_trial = int(sg.ndim == 2)
+    w = np.ascontiguousarray(widths, np.uint64)
+    thr = np.ascontiguousarray(thresholds, np.float32)
+    s = None if src is None else np.ascontiguousarray(src, np.uint32)
+    out = np.zeros((ntrials, nbins), np.float32)
+    ids = np.zeros(ntrials, np.uint32)
+    c = None if cls is None else np.ascontiguousarray(cls, np.uint8)
+    ncnt = thr.size * (2 if c is not None else 1)
+    counts = np.zeros(max(ncnt, 1), np.uint64)
+    mx = np.zeros(ntrials, np.float32)
+    k = lib().lko_mc_stage(_p(fin), None if s is None else _p(s), ntrials, nbins, _p(nz), _p(sg), per_trial,
+                           signal_scale, None if rm is None else _p(rm), var_in, var_add, _p(w), w.size,
+                           threshold, _p(thr), thr.size, None if c is None else _p(c), _p(out), _p(ids),
+                           _p(counts), _p(mx))
+    return out[:k], ids[:k], counts[:ncnt], mx

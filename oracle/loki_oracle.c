@@ -1392,3 +1392,87 @@ done:
     free(b_idx);
     return rc;
 }
+
+/* ======================================================================== */
+/* Monte-Carlo threshold stage.                                              */
+/* ======================================================================== */
+
+/* detection::snr_boxcar_threshold_with_cache (lib/score.cpp:434-462): the
+ * largest boxcar S/N of one 2-D profile, each width's S/N divided by
+ * stdnoise; the reference returns (any S/N > threshold), which equals
+ * (this maximum > threshold). */
+float lko_snr_max_div(const float* prof, uint64_t nbins, const uint64_t* widths, uint64_t nw,
+                      float stdnoise) {
+    uint64_t wmax = 0;
+    for (uint64_t i = 0; i < nw; ++i) {
+        wmax = widths[i] > wmax ? widths[i] : wmax;
+    }
+    float* psum = (float*)malloc(sizeof(float) * (nbins + wmax));
+    lko_circular_prefix_sum(prof, psum, nbins, nbins + wmax);
+    const float sum = psum[nbins - 1];
+    float best = -FLT_MAX;
+    for (uint64_t iw = 0; iw < nw; ++iw) {
+        const uint64_t w = widths[iw];
+        const float h = sqrtf((float)(nbins - w) / (float)(nbins * w));
+        const float b = (float)w * h / (float)(nbins - w);
+        const float dmax = diff_max(psum + w, psum, nbins);
+        const float snr = (((h + b) * dmax) - (b * sum)) / stdnoise;
+        best = (best < snr) ? snr : best;
+    }
+    free(psum);
+    return best;
+}
+
+/* simulate_score_prune_fused (lib/thresholds.cpp:358-431): out_i =
+ * (in[src_i] + noise_i) + signal, stdnoise = sqrt(var_in + var_add), keep
+ * trials whose S/N exceeds the threshold, compacted in trial order.
+ * src == NULL: src_i = i (the reference draws src_i at random only for
+ * i >= ntrials_in). Noise row of trial i: rowmap[i] (NULL: i); signal:
+ * [nbins] shared, or per trial (row rowmap[i]) when signal_per_trial, times
+ * signal_scale (a power of two keeps it exact). ids_out receives the noise
+ * row of each kept trial. With cls (a flag per noise row), counts[n_thr + k]
+ * counts the flagged trials above thr[k].
+ * counts[k] (n_thr entries, may be NULL) = trials with maximum S/N > thr[k].
+ * Returns the number kept. */
+uint64_t lko_mc_stage(const float* folds_in, const uint32_t* src, uint64_t ntrials,
+                      uint64_t nbins, const float* noise, const float* signal,
+                      int signal_per_trial, float signal_scale, const uint32_t* rowmap,
+                      float var_in, float var_add, const uint64_t* widths, uint64_t nw,
+                      float threshold, const float* thr, uint64_t n_thr, const uint8_t* cls,
+                      float* folds_out, uint32_t* ids_out, uint64_t* counts, float* max_snr) {
+    const float stdnoise = sqrtf(var_in + var_add);
+    float* row = (float*)malloc(sizeof(float) * nbins);
+    for (uint64_t k = 0; k < (cls != NULL ? 2 : 1) * n_thr; ++k) {
+        counts[k] = 0;
+    }
+    uint64_t kept = 0;
+    for (uint64_t i = 0; i < ntrials; ++i) {
+        const uint64_t s = src != NULL ? src[i] : i;
+        const uint64_t rw = rowmap != NULL ? rowmap[i] : i;
+        const float* in = folds_in + s * nbins;
+        const float* nz = noise + rw * nbins;
+        const float* sg = signal + (signal_per_trial ? rw * nbins : 0);
+        for (uint64_t j = 0; j < nbins; ++j) {
+            row[j] = (in[j] + nz[j]) + (sg[j] * signal_scale);
+        }
+        const float m = lko_snr_max_div(row, nbins, widths, nw, stdnoise);
+        if (max_snr != NULL) {
+            max_snr[i] = m;
+        }
+        for (uint64_t k = 0; k < n_thr; ++k) {
+            counts[k] += (m > thr[k]) ? 1 : 0;
+            if (cls != NULL && cls[rw] != 0) {
+                counts[n_thr + k] += (m > thr[k]) ? 1 : 0;
+            }
+        }
+        if (m > threshold) {
+            memcpy(folds_out + kept * nbins, row, nbins * sizeof(float));
+            if (ids_out != NULL) {
+                ids_out[kept] = (uint32_t)rw;
+            }
+            ++kept;
+        }
+    }
+    free(row);
+    return kept;
+}

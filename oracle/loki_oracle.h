@@ -206,6 +206,23 @@ int lko_prune_run(const lko_plan* plan, int conservative, const float* ffa_fold,
                   lko_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
                   float* folds_out, float* scores_out, uint64_t cap_out, uint64_t* n_out);
 
+/* ---- Monte-Carlo threshold stage ------------------------------------------ */
+
+/* Largest boxcar S/N of one 2-D profile with every width's S/N divided by
+ * stdnoise (detection::snr_boxcar_threshold_with_cache, lib/score.cpp:434-462,
+ * decides S/N > threshold for some width, i.e. this maximum > threshold). */
+float lko_snr_max_div(const float* prof, uint64_t nbins, const uint64_t* widths, uint64_t nw,
+                      float stdnoise);
+
+/* One fused stage of simulate_score_prune_fused (lib/thresholds.cpp:358-431);
+ * see loki_oracle.c for the argument meanings. Returns the trials kept. */
+uint64_t lko_mc_stage(const float* folds_in, const uint32_t* src, uint64_t ntrials,
+                      uint64_t nbins, const float* noise, const float* signal,
+                      int signal_per_trial, float signal_scale, const uint32_t* rowmap,
+                      float var_in, float var_add, const uint64_t* widths, uint64_t nw,
+                      float threshold, const float* thr, uint64_t n_thr, const uint8_t* cls,
+                      float* folds_out, uint32_t* ids_out, uint64_t* counts, float* max_snr);
+
 #ifdef __cplusplus
 }
 #endif

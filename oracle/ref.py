@@ -95,6 +95,7 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
         L.lkref_shift_add_batch.argtypes = [vp, vp, vp, vp, vp, vp, u64, u64, u64, u64]
         L.lkref_score_filter.argtypes = [vp, u64, u64, vp, u64, f32, vp, vp, vp]
         L.lkref_branch_max.argtypes = [vp, ctypes.c_int, vp]
+        L.lkref_snr_threshold.argtypes = [vp, u64, u64, vp, u64, vp, f32, vp]
         L.lkref_branching_pattern.argtypes = [vp, ctypes.c_int, u64, vp, u64, vp]
         L.lkref_prune_run.argtypes = [vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64, u64,
                                       vp, vp, vp, vp, vp, u64, vp]
@@ -367,3 +368,15 @@ def prune_run(cfg: RefCfg, ffa_fold, thresholds, ref_seg, max_sugg, batch_size, 
     k = n.value
     return (stats[: nstats.value], leaves[: k * stride].reshape(k, cfg.nparams + 2, 2),
             folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k])
+
+
+def snr_threshold(profiles, nbins, widths, thresholds, stdnoise) -> np.ndarray:
+    """snr_boxcar_threshold_with_cache per profile (bool array)."""
+    L = lib()
+    p = np.ascontiguousarray(profiles, np.float32)
+    n = p.size // nbins
+    w = np.ascontiguousarray(widths, np.uint64)
+    t = np.ascontiguousarray(np.broadcast_to(np.asarray(thresholds, np.float32), (n,)))
+    out = np.zeros(n, np.uint8)
+    _check(L, L.lkref_snr_threshold(_p(p), n, nbins, _p(w), w.size, _p(t), stdnoise, _p(out)))
+    return out.astype(bool)

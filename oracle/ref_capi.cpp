@@ -26,6 +26,8 @@
 //   lkref_score_filter    -> detection::score_and_filter_max_with_cache
 //                            (lib/score.cpp:213-259)
 //   lkref_branch_max      -> EPMultiPass's branch_max rule (lib/prune.cpp:648-651)
+//   lkref_snr_threshold   -> detection::snr_boxcar_threshold_with_cache
+//                            (lib/score.cpp:434-462)
 //   lkref_prune_run       -> PruneImpl::initialize + execute_iteration[_batched]
 //                            (lib/prune.cpp:181-226,429-620), restated here
 //                            because prune.cpp itself needs HDF5 and a
@@ -301,6 +303,25 @@ uint32_t lkref_phase_idx_uint(double proper_time,
                               uint64_t nbins,
                               double delay) {
     return loki::psr_utils::get_phase_idx_uint(proper_time, freq, nbins, delay);
+}
+
+// detection::snr_boxcar_threshold_with_cache (lib/score.cpp:434-462) of n
+// 2-D profiles, thresholds[i] for profile i: out[i] = 1 if some width's
+// S/N / stdnoise > thresholds[i].
+int lkref_snr_threshold(const float* profiles, uint64_t n, uint64_t nbins,
+                        const uint64_t* widths, uint64_t nwidths, const float* thresholds,
+                        float stdnoise, uint8_t* out) {
+    return guarded([&] {
+        std::vector<loki::SizeType> w(widths, widths + nwidths);
+        loki::detection::BoxcarWidthsCache cache(w, nbins);
+        for (uint64_t i = 0; i < n; ++i) {
+            out[i] = loki::detection::snr_boxcar_threshold_with_cache(
+                         std::span<const float>(profiles + i * nbins, nbins), nbins, cache,
+                         thresholds[i], stdnoise)
+                         ? 1
+                         : 0;
+        }
+    });
 }
 
 // ---- pruning leaf step ------------------------------------------------------
