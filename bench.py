@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--storage", default="fp32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="taylor_accel",
+                    choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade"],
+                    help="taylor_accel (default): Taylor (f, fdot) FFA + S/N; freq_sweep: plain period "
+                         "sweep; prune_jerk: FFA to 32 segments + one pruning run; mc_cascade: 8-stage "
+                         "Monte-Carlo threshold cascade")
     return ap.parse_args()
 
 
@@ -391,6 +396,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload != "taylor_accel":
+        import bench_workloads
+
+        return bench_workloads.run(args, rank, world, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank)
     return run_ours(args, rank, world, local_rank)

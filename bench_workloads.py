@@ -1,0 +1,462 @@
+"""Benchmarks of the other hot-path workloads, run through ``bench.py
+--workload ...`` (same flags and JSON contract as the default line):
+
+  freq_sweep   plain FFA period sweep: 2^21 samples at 64 us, seed 42, one
+               47.3 ms pulsar; f in [5, 50] Hz (periods 20-200 ms), nbins 128,
+               widths {1,2,3,4,6,8,12,16}; scores of every final cell and width,
+               compacted at S/N >= 7. Metric: param-trials/s.
+  prune_jerk   2^23 samples at 64 us, seed 11, two circular binaries; FFA to 32
+               segments (bseg_ffa = 2^18) then one pruning run seeded at segment
+               16 over the 31 levels (thresholds 3 -> 8), world tree 2^20,
+               batches of 4096 parents. Metric: param-trials/s = leaves scored
+               (sum over levels of n_leaves_phy) x boxcar widths per second.
+  mc_cascade   2^20 profiles x 64 bins, seed 99, 8 Monte-Carlo stages (variance
+               doubling, pruning thresholds 2 -> 6) each counted against 64
+               thresholds. Metric: param-trials/s = alive profiles x 64
+               thresholds per second, summed over stages.
+
+Each step works on inputs already resident on the GPU (value); ``e2e`` repeats
+the step with the inputs copied from pinned host memory and the results read
+back inside the timed region. The CPU baseline runs the reference's own code
+(oracle/_ref, Release flags) where it can be linked, else the C oracle port,
+on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import time
+
+import numpy as np
+
+import bench as B
+
+UNIT = "param-trials/s"
+METRIC = "param-trials/s (FFA+S/N)"
+
+
+def _line(args, world, workload, value, step_ms, config, **extra):
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict({"workload": workload, "parallelism": "replicas",
+                            "l2": f"flushed: {B.FLUSH_BYTES >> 20} MiB written between timed steps"}, **config)}
+    line.update(extra)
+    return line
+
+
+def _timed(torch, step, steps, warmup, flush, dist=None):
+    """Warm-up, then `steps` steps bracketed by CUDA events (L2 flushed
+    between steps); returns (mean step ms (max over ranks), step outputs)."""
+    for _ in range(max(warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    outs = []
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record(stream)
+        outs.append(step())
+        stops[k].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / steps
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), outs
+
+
+def _init(local_rank, world):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local_rank}"))
+    return torch, dist
+
+
+def _finish(dist):
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _roofline(name, algo_bytes, ms):
+    peak, kind = B.hbm_peak()
+    ach = algo_bytes / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "peak_source": kind, "unit": "GB/s",
+            "frac": ach / peak, "traffic": B.ncu_traffic(name), "algorithmic_bytes": algo_bytes, "avg_ms": ms}
+
+
+# ---- freq_sweep -------------------------------------------------------------------
+
+def _freq_params():
+    from loki_b200.synthetic import Pulsar, make_series
+
+    nsamps, tsamp, nbins = 1 << 21, 64e-6, 128
+    widths = [1, 2, 3, 4, 6, 8, 12, 16]
+    ts_e, ts_v = make_series(nsamps, tsamp, 42, [Pulsar(f0=1.0 / 0.0473, duty=0.05, snr=15.0)], nbins, widths)
+    params = dict(nsamps=nsamps, tsamp=tsamp, nbins=nbins, eta=1.0, param_limits=[[5.0, 50.0]],
+                  score_widths=widths)
+    return ts_e, ts_v, params
+
+
+def run_freq(args, rank, world, local_rank):
+    ts_e, ts_v, params = _freq_params()
+    cfgd = {"nsamps": params["nsamps"], "tsamp": params["tsamp"], "nbins": params["nbins"],
+            "f_range_hz": params["param_limits"][0], "score_widths": params["score_widths"], "snr_min": B.SNR_MIN}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from oracle import ref
+
+        if not ref.available("timing"):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return 0
+        step, ntrials, nthreads = B.reference_runner(params)
+        for _ in range(max(args.warmup, 1)):
+            step(ts_e, ts_v)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(ts_e, ts_v)
+        total = time.perf_counter() - t0
+        v = ntrials * args.steps / total
+        print(json.dumps(_line(args, world, "freq_sweep_2^21x64us_nbins128", v, 1e3 * total / args.steps,
+                               dict(cfgd, cpu_threads=nthreads), impl="reference",
+                               cpu_baseline={"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                                             "sample": f"full workload, {args.steps} steps"},
+                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                    "d2h_bytes_per_step": 0})))
+        return 0
+    torch, dist = _init(local_rank, world)
+    from loki_b200 import _capi as C
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+
+    cfg = PulsarSearchConfig(params["nsamps"], params["tsamp"], params["nbins"], params["eta"],
+                             np.array(params["param_limits"]), use_fourier=False,
+                             score_widths=params["score_widths"], snr_min=B.SNR_MIN)
+    ffa = FFACUDA(cfg, device_id=local_rank)
+    ntrials = int(ffa.plan.ncoords[-1]) * cfg.n_scoring_widths
+    cap = 1 << 20
+    e = torch.from_numpy(ts_e).cuda()
+    v = torch.from_numpy(ts_v).cuda()
+    idx = torch.empty(cap, dtype=torch.int32, device="cuda")
+    snr = torch.empty(cap, dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+    L = C.lib()
+
+    def step():
+        C.check(L.lk_ffa_search(ffa._h, e.data_ptr(), v.data_ptr(), B.SNR_MIN, idx.data_ptr(), snr.data_ptr(),
+                                cap, cnt.data_ptr(), sp))
+
+    ffa.set_profiling(True)
+    clocks = B.ClockSampler(local_rank)
+    clocks.start()
+    ms, _ = _timed(torch, step, args.steps, args.warmup, flush, dist)
+    clk = clocks.stop()
+    prof = {}
+    launches = 0
+    for st in ffa.profile():
+        key = st["stage"] if st["level"] < 0 else f'{st["stage"]}_l{st["level"]}'
+        prof[key] = (st["ms"], st["bytes"])
+        launches += st["launches"]
+    ffa.set_profiling(False)
+    dom = max(prof, key=lambda k: prof[k][0])
+    value = ntrials * world / (ms / 1e3)
+    e2e = None
+    if not args.no_e2e:
+        he, hv = torch.from_numpy(ts_e).pin_memory(), torch.from_numpy(ts_v).pin_memory()
+        hc = torch.zeros(1, dtype=torch.int64).pin_memory()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(args.steps):
+            e.copy_(he, non_blocking=True)
+            v.copy_(hv, non_blocking=True)
+            step()
+            hc.copy_(cnt, non_blocking=True)
+            torch.cuda.synchronize()
+            n = min(int(hc.item()), cap)
+            _ = (idx[:n].cpu(), snr[:n].cpu())
+            d2h += 8 + 8 * n
+        el = time.perf_counter() - t0
+        e2e = {"value": ntrials * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": 8 * params["nsamps"],
+               "d2h_bytes_per_step": d2h // args.steps, "api": "FFACUDA.search (lk_ffa_search), host series"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = B.cpu_baseline(params, ts_e, ts_v)
+    if rank == 0:
+        print(json.dumps(_line(args, world, "freq_sweep_2^21x64us_nbins128", value, ms,
+                               dict(cfgd, final_coords=int(ffa.plan.ncoords[-1]), candidates=int(cnt.item())),
+                               roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
+                               gpu_launches=args.steps * launches, clocks=clk,
+                               stages={k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()})))
+    _finish(dist)
+    return 0
+
+
+# ---- prune_jerk -------------------------------------------------------------------
+
+PRUNE_MAX_SUGG = 1 << 20
+PRUNE_BATCH = 4096
+
+
+def _prune_setup():
+    from loki_b200.synthetic import jerk_prune_workload
+
+    ts_e, ts_v, p, thr, _ = jerk_prune_workload()
+    return ts_e, ts_v, p, thr
+
+
+def _prune_cfgd(p, nseg, ref_seg, widths):
+    return {"nsamps": p["nsamps"], "tsamp": p["tsamp"], "nbins": p["nbins"], "eta": p["eta"],
+            "param_limits": p["param_limits"], "bseg_ffa": p["bseg_ffa"], "nsegments": nseg, "ref_seg": ref_seg,
+            "thresholds": "linear 3 -> 8 over 31 levels", "max_sugg": PRUNE_MAX_SUGG, "batch_size": PRUNE_BATCH,
+            "score_widths": [int(w) for w in widths]}
+
+
+def _ref_prune_sample(p, fold, thr, ref_seg, nbins, kind, budget_s=20.0):
+    """The reference's pruning run (oracle/_ref: PruneDPFuncts + WorldTree over
+    prune.cpp's level loop) on the first k levels, k doubled while a run stays
+    within the budget; returns (trials/s, levels, seconds, stats)."""
+    from oracle import ref
+
+    cfg = ref.make_cfg(p["nsamps"], p["tsamp"], p["nbins"], p["eta"], p["param_limits"], bseg_ffa=p["bseg_ffa"])
+    bm = ref.branch_max(cfg)
+    widths = ref.box_widths(nbins)
+    k, best = 2, None
+    while True:
+        t0 = time.perf_counter()
+        st = ref.prune_run(cfg, fold, thr, ref_seg, PRUNE_MAX_SUGG, PRUNE_BATCH, bm, k, nbins, kind=kind)[0]
+        el = time.perf_counter() - t0
+        trials = int(st["n_leaves_phy"][1:].sum()) * widths.size
+        best = (trials / el, k, el, st)
+        if el * 2.5 > budget_s or k >= 31 or len(st) <= k:
+            return best
+        k *= 2
+
+
+def run_prune(args, rank, world, local_rank):
+    ts_e, ts_v, p, thr = _prune_setup()
+    nbins = p["nbins"]
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from oracle import lko, ref
+
+        if not ref.available("timing"):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return 0
+        cfg = ref.make_cfg(p["nsamps"], p["tsamp"], nbins, p["eta"], p["param_limits"], bseg_ffa=p["bseg_ffa"],
+                           nthreads=os.cpu_count() or 1)
+        fold = ref.RefFFA(cfg, kind="timing").execute(ts_e, ts_v).copy()
+        nseg = int(lko.plan_create(lko.make_cfg(p["nsamps"], p["tsamp"], nbins, p["eta"], p["param_limits"],
+                                                bseg_ffa=p["bseg_ffa"])).nsegments[-1])
+        v, k, el, st = _ref_prune_sample(p, fold, thr, nseg // 2, nbins, "timing")
+        widths = ref.box_widths(nbins)
+        sample = f"one pruning run (ref_seg {nseg // 2}) over its first {k} levels, {el:.1f} s, single thread"
+        print(json.dumps(_line(args, world, "prune_jerk_2^23x64us_nbins32", v, 1e3 * el,
+                               _prune_cfgd(p, nseg, nseg // 2, widths), impl="reference",
+                               cpu_baseline={"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                                             "sample": sample},
+                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})))
+        return 0
+    torch, dist = _init(local_rank, world)
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+    from loki_b200.prune import PruneCUDA
+
+    cfg = PulsarSearchConfig(p["nsamps"], p["tsamp"], nbins, p["eta"], np.array(p["param_limits"]),
+                             use_fourier=False, bseg_ffa=p["bseg_ffa"])
+    ffa = FFACUDA(cfg, device_id=local_rank)
+    nseg = int(ffa.plan.nsegments[-1])
+    ref_seg = nseg // 2
+    pr = PruneCUDA(cfg, max_sugg=PRUNE_MAX_SUGG, batch_size=PRUNE_BATCH, device_id=local_rank)
+    widths = cfg.score_widths
+    e = torch.from_numpy(ts_e).cuda()
+    v = torch.from_numpy(ts_v).cuda()
+    fold = torch.empty(ffa.plan.fold_size, dtype=torch.float32, device="cuda")
+    flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def step():
+        ffa.execute(e, v, fold)
+        ev[0].record()
+        st = pr.run(fold, ref_seg, thr, n_iters=nseg - 1)
+        ev[1].record()
+        return st
+
+    clocks = B.ClockSampler(local_rank)
+    clocks.start()
+    ms, outs = _timed(torch, step, args.steps, args.warmup, flush, dist)
+    clk = clocks.stop()
+    stats = outs[-1]
+    leaves = int(stats["n_leaves_phy"][1:].sum())
+    trials = leaves * len(widths)
+    value = trials * world / (ms / 1e3)
+    prune_ms = ev[0].elapsed_time(ev[1])
+    # algorithmic bytes of the leaf work: per child the parent fold and the FFA
+    # row read (2 x 2 x nbins floats) and the leaf read / written (10 doubles)
+    algo = leaves * (2 * 2 * nbins * 4 + 2 * 10 * 8)
+    e2e = None
+    if not args.no_e2e:
+        he, hv = torch.from_numpy(ts_e).pin_memory(), torch.from_numpy(ts_v).pin_memory()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(args.steps):
+            e.copy_(he, non_blocking=True)
+            v.copy_(hv, non_blocking=True)
+            ffa.execute(e, v, fold)
+            pr.run(fold, ref_seg, thr, n_iters=nseg - 1)
+            lv, fo, sc = pr.tree()
+            d2h += lv.nbytes + sc.nbytes
+        el = time.perf_counter() - t0
+        e2e = {"value": trials * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": 8 * p["nsamps"],
+               "d2h_bytes_per_step": d2h // args.steps,
+               "api": "FFACUDA.execute + PruneCUDA.run + tree read-back, host series"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+
+        if ref.available("timing"):
+            cv, k, el, _ = _ref_prune_sample(p, fold.cpu().numpy(), thr, ref_seg, nbins, "timing")
+            cpu = {"value": cv, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"reference pruning run (ref_seg {ref_seg}) over its first {k} levels "
+                             f"({el:.1f} s), single thread, on the same FFA fold"}
+    if rank == 0:
+        print(json.dumps(_line(
+            args, world, "prune_jerk_2^23x64us_nbins32", value, ms,
+            dict(_prune_cfgd(p, nseg, ref_seg, widths), leaves_scored=leaves,
+                 survivors=int(stats["n_leaves_surv"][-1]), levels_run=int(len(stats) - 1)),
+            roofline=_roofline("prune_run", algo, prune_ms), cpu_baseline=cpu, e2e=e2e,
+            clocks=clk, stages={"ffa_ms": ms - prune_ms, "prune_ms": prune_ms},
+            level_stats=[{k: (float(r[k]) if k in ("threshold", "score_min", "score_max") else int(r[k]))
+                          for k in ("level", "n_branches", "n_leaves", "n_leaves_surv", "threshold", "score_max")}
+                         for r in stats])))
+    _finish(dist)
+    return 0
+
+
+# ---- mc_cascade --------------------------------------------------------------------
+
+MC_WIDTHS = np.array([1, 2, 3, 4, 6, 8, 12, 16], np.uint32)
+
+
+def run_mc(args, rank, world, local_rank):
+    from loki_b200.synthetic import mc_cascade_workload
+
+    folds0, signal, cls, noises, thresholds, grids = mc_cascade_workload(ntrials=1 << 20, nstages=8, seed=99)
+    cfgd = {"ntrials": int(folds0.shape[0]), "nbins": int(folds0.shape[1]), "stages": len(noises),
+            "grid": "64 thresholds 0 .. 16 per stage", "pruning_thresholds": [float(x) for x in thresholds],
+            "score_widths": [int(w) for w in MC_WIDTHS]}
+
+    def port_sample(nsub=1 << 15):
+        from oracle import lko
+
+        f, rows, var, trials = folds0[:nsub], np.arange(nsub, dtype=np.uint32), 1.0, 0
+        t0 = time.perf_counter()
+        for s, nz in enumerate(noises):
+            trials += rows.size * len(grids[s])
+            f, rows, _, _ = lko.mc_stage(f, nz, signal, var, var, MC_WIDTHS.astype(np.uint64), thresholds[s],
+                                         grids[s], signal_scale=float(2 ** s), rowmap=rows, cls=cls)
+            var *= 2
+            if rows.size == 0:
+                break
+        el = time.perf_counter() - t0
+        return trials / el, el, nsub
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        v, el, nsub = port_sample()
+        print(json.dumps(_line(args, world, "mc_cascade_2^20x64_8stages", v, 1e3 * el, cfgd, impl="reference",
+                               cpu_baseline={"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                                             "sample": f"the first {nsub} profiles through all stages "
+                                                       f"({el:.1f} s), C oracle restatement, one thread"},
+                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})))
+        return 0
+    torch, dist = _init(local_rank, world)
+    from loki_b200.thresholds import MCStageCUDA
+
+    n0, nbins = folds0.shape
+    d_f0 = torch.from_numpy(folds0).cuda()
+    d_sig = torch.from_numpy(signal).cuda()
+    d_cls = torch.from_numpy(cls).cuda()
+    d_nz = [torch.from_numpy(nz).cuda() for nz in noises]
+    st = MCStageCUDA(n0, nbins, MC_WIDTHS, local_rank)
+    bufs = [torch.empty_like(d_f0), torch.empty_like(d_f0)]
+    rows0 = torch.arange(n0, dtype=torch.int32, device="cuda")
+    flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stage_bytes = []
+
+    def step():
+        rows, alive, var, fin, cur = rows0, n0, 1.0, d_f0, 0
+        trials = 0
+        stage_bytes.clear()
+        for s in range(len(noises)):
+            r = st.stage(fin, d_nz[s], d_sig, float(thresholds[s]), var, var, thresholds=grids[s],
+                         signal_scale=float(2 ** s), rowmap=rows[:alive], ntrials=alive, cls=d_cls,
+                         folds_out=bufs[cur])
+            trials += alive * len(grids[s])
+            kept = int(r["count"].item())
+            stage_bytes.append(alive * nbins * 4 * 3 + kept * nbins * 4 * 4)
+            rows, fin, cur, alive, var = r["ids"][:kept].clone(), bufs[cur], 1 - cur, kept, 2 * var
+            if alive == 0:
+                break
+        return trials
+
+    clocks = B.ClockSampler(local_rank)
+    clocks.start()
+    ms, outs = _timed(torch, step, args.steps, args.warmup, flush, dist)
+    clk = clocks.stop()
+    trials = outs[-1]
+    value = trials * world / (ms / 1e3)
+    e2e = None
+    if not args.no_e2e:
+        hf = torch.from_numpy(folds0).pin_memory()
+        hn = [torch.from_numpy(nz).pin_memory() for nz in noises]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            d_f0.copy_(hf, non_blocking=True)
+            for s in range(len(noises)):
+                d_nz[s].copy_(hn[s], non_blocking=True)
+            step()
+        el = time.perf_counter() - t0
+        e2e = {"value": trials * world * args.steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": folds0.nbytes + sum(nz.nbytes for nz in noises),
+               "d2h_bytes_per_step": len(noises) * (8 + 64 * 2 * 8),
+               "api": "MCStageCUDA.stage x 8 (lk_mc_stage), profiles and noise from pinned host memory"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cv, el, nsub = port_sample()
+        cpu = {"value": cv, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"the first {nsub} profiles through all stages ({el:.1f} s), C oracle restatement "
+                         f"(the reference's thresholds.cpp needs HDF5 and cannot be linked here), one thread"}
+    if rank == 0:
+        print(json.dumps(_line(args, world, "mc_cascade_2^20x64_8stages", value, ms,
+                               dict(cfgd, trials_per_step=trials),
+                               roofline=_roofline("mc_stage", sum(stage_bytes), ms), cpu_baseline=cpu, e2e=e2e,
+                               gpu_launches=args.steps * len(stage_bytes) * 5, clocks=clk)))
+    _finish(dist)
+    return 0
+
+
+def run(args, rank, world, local_rank):
+    return {"freq_sweep": run_freq, "prune_jerk": run_prune, "mc_cascade": run_mc}[args.workload](
+        args, rank, world, local_rank)

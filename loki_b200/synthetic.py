@@ -4,7 +4,8 @@ White N(0, 1) noise (variance series of ones) plus pulse trains with a von
 Mises pulse shape, exp(kappa (cos 2 pi phi - 1)) with
 kappa = ln 2 / (1 - cos(pi duty)) (duty = full width at half maximum as a
 fraction of the period), and a Taylor phase model about the middle of the
-observation: phi(t) = f0 (t - d(t)), d(t) = a t^2 / (2c) + j t^3 / (6c).
+observation: phi(t) = f0 (t - d(t)), d(t) = a t^2 / (2c) + j t^3 / (6c)
+(+ x sin(2 pi t / Pb + phi0) for a circular binary).
 Amplitudes are set so that the noiseless pulse folded at its true parameters
 and scored by the boxcar scorer reaches the requested S/N.
 """
@@ -25,6 +26,10 @@ class Pulsar:
     jerk: float = 0.0
     duty: float = 0.05
     snr: float = 10.0
+    # circular orbit: Roemer delay x sin(2 pi t / porb + phi0), x in light-seconds
+    porb: float = 0.0
+    x: float = 0.0
+    phi0: float = 0.0
 
 
 def von_mises_profile(nbins: int, duty: float, oversample: int = 32) -> np.ndarray:
@@ -64,6 +69,8 @@ def inject(ts: np.ndarray, tsamp: float, psr: Pulsar, nbins: int, widths, chunk:
     for i0 in range(0, n, chunk):
         t = (np.arange(i0, min(n, i0 + chunk)) * tsamp) - t_ref
         delay = psr.accel * t * t / (2 * C_LIGHT) + psr.jerk * t**3 / (6 * C_LIGHT)
+        if psr.porb > 0:
+            delay = delay + psr.x * np.sin(2 * np.pi * t / psr.porb + psr.phi0)
         phase = psr.f0 * (t - delay)
         ts[i0 : i0 + t.size] += (amp * np.exp(kappa * (np.cos(2 * np.pi * phase) - 1.0))).astype(np.float32)
 
@@ -128,3 +135,25 @@ def mc_cascade_workload(ntrials: int = 1 << 20, nbins: int = 64, nstages: int = 
     thresholds = np.linspace(2.0, 6.0, nstages).astype(np.float32)
     grids = [np.linspace(0.0, 16.0, n_grid).astype(np.float32) for _ in range(nstages)]
     return folds0, signal, cls, noises, thresholds, grids
+
+
+def jerk_prune_workload(seed: int = 11, n_signals: int = 2):
+    """Jerk search through the pruning tree: 2^23 samples at 64 us (537 s),
+    seed 11, two circular binaries (Pb ~ U(2, 6) h, x ~ U(0.5, 2) lt-s,
+    f ~ U(20, 200) Hz, fold S/N ~ U(10, 14)); FFA to 32 segments
+    (bseg_ffa = 2^18), jerk in [-0.4, 0.4] m/s^3, accel in [-457, 457] m/s^2,
+    f in [20, 200] Hz, nbins 32; per-level thresholds rising linearly from 3
+    to 8 over the 31 pruning levels."""
+    nsamps, tsamp, nbins = 1 << 23, 64e-6, 32
+    rng = np.random.default_rng(seed + 1000)
+    pulsars = [
+        Pulsar(f0=float(rng.uniform(20, 200)), duty=0.05, snr=float(rng.uniform(10, 14)),
+               porb=float(rng.uniform(2, 6)) * 3600.0, x=float(rng.uniform(0.5, 2.0)),
+               phi0=float(rng.uniform(0, 2 * np.pi)))
+        for _ in range(n_signals)
+    ]
+    ts_e, ts_v = make_series(nsamps, tsamp, seed, pulsars, nbins, (1, 2, 4, 8))
+    params = dict(nsamps=nsamps, tsamp=tsamp, nbins=nbins, eta=1.0, bseg_ffa=1 << 18,
+                  param_limits=[[-0.4, 0.4], [-457.0, 457.0], [20.0, 200.0]])
+    thresholds = np.linspace(3.0, 8.0, 31).astype(np.float32)
+    return ts_e, ts_v, params, thresholds, pulsars
