@@ -169,6 +169,25 @@ int lk_ffa_scores(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float* 
 int lk_ffa_search(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float snr_min,
                   uint32_t* d_idx, float* d_snr, uint64_t max_cands, uint64_t* d_count,
                   lk_stream_t stream);
+
+/* Batched executor: nbatch <= max_batch series of the plan's nsamps samples,
+ * stored back to back in d_ts_e / d_ts_v, folded and scored together (one
+ * launch per level for the whole batch; a batch is, level by level, one series
+ * with nbatch times the segments). Outputs are each series' single-series
+ * output, back to back: folds [nbatch][fold_size], scores [nbatch][ncoords]
+ * [nwidths], and search indices flat over [nbatch][ncoords][nwidths]
+ * (nbatch * ncoords * nwidths < 2^32). Intermediate buffers are sized for
+ * max_batch series. The single-series calls above are nbatch = 1. */
+int lk_ffa_create_batched(const lk_plan* plan, int device, int storage, uint64_t max_batch,
+                          lk_ffa** out);
+int lk_ffa_execute_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
+                         float* d_fold, uint64_t fold_len, lk_stream_t stream);
+int lk_ffa_scores_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
+                        float* d_scores, uint64_t scores_len, lk_stream_t stream);
+int lk_ffa_search_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
+                        float snr_min, uint32_t* d_idx, float* d_snr, uint64_t max_cands,
+                        uint64_t* d_count, lk_stream_t stream);
+
 /* Synchronises the stream and reports the executor's device status word
  * (0 = no bounded wait gave up). */
 int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status);

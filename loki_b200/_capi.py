@@ -133,6 +133,10 @@ SIGNATURES = [
     ("lk_ffa_execute", i32, [vp, vp, vp, vp, u64, vp]),
     ("lk_ffa_scores", i32, [vp, vp, vp, vp, u64, vp]),
     ("lk_ffa_search", i32, [vp, vp, vp, f32, vp, vp, u64, vp, vp]),
+    ("lk_ffa_create_batched", i32, [vp, i32, i32, u64, vp]),
+    ("lk_ffa_execute_batch", i32, [vp, vp, vp, u64, vp, u64, vp]),
+    ("lk_ffa_scores_batch", i32, [vp, vp, vp, u64, vp, u64, vp]),
+    ("lk_ffa_search_batch", i32, [vp, vp, vp, u64, f32, vp, vp, u64, vp, vp]),
     ("lk_ffa_status", i32, [vp, vp, vp]),
     ("lk_ffa_set_profiling", i32, [vp, i32]),
     ("lk_ffa_get_profile", i32, [vp, vp, vp, u32, vp]),

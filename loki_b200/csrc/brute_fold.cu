@@ -84,7 +84,11 @@ __device__ __forceinline__ uint32_t load_bins(const BinT* b, uint64_t n, uint64_
     return k < n ? static_cast<uint32_t>(__ldg(b + k)) : 0u;
 }
 
-template <class BinT>
+// ROWS = 2: a consumer warp owns one frequency and both rows (E and V share
+// the run mask and run bins); ROWS = 1: one (frequency, row) item per warp,
+// half the accumulator memory per warp, so twice the warps fit a block
+// (used for large nbins, where accumulators limit the warps per SM).
+template <class BinT, int ROWS>
 __global__ void __launch_bounds__(640, 1)
     brute_fold_mask_kernel(const __grid_constant__ CUtensorMap tmap_e,
                            const __grid_constant__ CUtensorMap tmap_v, FoldArgs a) {
@@ -100,8 +104,9 @@ __global__ void __launch_bounds__(640, 1)
     const int warp = threadIdx.x / kWarp;
     const int lane = threadIdx.x % kWarp;
     const int W = static_cast<int>(a.warps);
-    const uint32_t f0 = blockIdx.y * a.warps;  // first frequency of the block
-    const int nconsumers = static_cast<int>(min(a.warps, a.nfreq - f0));
+    const uint32_t q0 = blockIdx.y * a.warps;  // first work item of the block
+    const uint32_t nitems = (ROWS == 2 ? 1u : 2u) * a.nfreq;
+    const int nconsumers = static_cast<int>(min(a.warps, nitems - q0));
     const int seg0 = static_cast<int>(blockIdx.x * kWarp);
 
     // The 128-byte swizzle pattern is defined on 1024-byte aligned tiles.
@@ -153,12 +158,14 @@ __global__ void __launch_bounds__(640, 1)
         return;
     }
 
-    const uint32_t f = f0 + static_cast<uint32_t>(warp);
-    // Accumulators of this warp: E then V, each [nbins + 1][32 lanes]; slot
+    const uint32_t q = q0 + static_cast<uint32_t>(warp);
+    const uint32_t f = ROWS == 2 ? q : (q >> 1);
+    const uint32_t row0 = ROWS == 2 ? 0u : (q & 1u);
+    // Accumulators of this warp: ROWS rows of [nbins + 1][32 lanes]; slot
     // nbins is a scratch slot that absorbs the store before the first run.
     const uint32_t vrow = (a.nbins + 1) * kWarp;
-    float* A = accs + static_cast<size_t>(warp) * 2 * vrow + lane;
-    for (uint32_t b = 0; b < 2 * (a.nbins + 1); ++b) {
+    float* A = accs + static_cast<size_t>(warp) * ROWS * vrow + lane;
+    for (uint32_t b = 0; b < ROWS * (a.nbins + 1); ++b) {
         A[b * kWarp] = 0.0f;
     }
     const uint32_t* M = a.masks + static_cast<size_t>(f) * a.nwords;
@@ -166,7 +173,7 @@ __global__ void __launch_bounds__(640, 1)
     const uint64_t nr = a.nruns[f];
 
     uint32_t bin = a.nbins;   // current run's bin (scratch slot before the first run)
-    float acc_e = 0.0f, acc_v = 0.0f;
+    float acc0 = 0.0f, acc1 = 0.0f;
     uint64_t r = 0;           // runs started so far
     uint64_t rbase = 0;       // run index held by lane 0 of binbuf
     uint32_t binbuf = load_bins(B, nr, 0, lane);
@@ -180,12 +187,16 @@ __global__ void __launch_bounds__(640, 1)
     // measured slower on B200: 2.42 against 2.22 ms on the 2^22-sample
     // accelerated workload.)
     auto start_run = [&](uint32_t& rl) {
-        A[bin * kWarp] = acc_e;
-        A[vrow + bin * kWarp] = acc_v;
+        A[bin * kWarp] = acc0;
+        if constexpr (ROWS == 2) {
+            A[vrow + bin * kWarp] = acc1;
+        }
         bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
         ++rl;
-        acc_e = A[bin * kWarp];
-        acc_v = A[vrow + bin * kWarp];
+        acc0 = A[bin * kWarp];
+        if constexpr (ROWS == 2) {
+            acc1 = A[vrow + bin * kWarp];
+        }
     };
 
     uint32_t phase = 0;
@@ -195,7 +206,7 @@ __global__ void __launch_bounds__(640, 1)
             maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
         }
         const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
-        // binbuf must hold runs r .. r + popc(m) (the last one is the prefetch).
+        // binbuf must hold runs r .. r + popc(m) - 1.
         if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
             rbase = r;
             binbuf = load_bins(B, nr, rbase, lane);
@@ -205,21 +216,24 @@ __global__ void __launch_bounds__(640, 1)
                                         (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull))) {
             return;
         }
-        const unsigned char* te = ring + static_cast<size_t>(s) * kStageBytes + lrow;
-        float xe[32], xv[32];
+        const unsigned char* te =
+            ring + static_cast<size_t>(s) * kStageBytes + row0 * kTileBytes + lrow;
+        float x0[32], x1[ROWS == 2 ? 32 : 1];
 #pragma unroll
         for (uint32_t j = 0; j < 8; ++j) {
             const uint32_t o = (j ^ lsw) << 4;
-            const float4 ve = *reinterpret_cast<const float4*>(te + o);
-            const float4 vv = *reinterpret_cast<const float4*>(te + kTileBytes + o);
-            xe[4 * j + 0] = ve.x;
-            xe[4 * j + 1] = ve.y;
-            xe[4 * j + 2] = ve.z;
-            xe[4 * j + 3] = ve.w;
-            xv[4 * j + 0] = vv.x;
-            xv[4 * j + 1] = vv.y;
-            xv[4 * j + 2] = vv.z;
-            xv[4 * j + 3] = vv.w;
+            const float4 v0 = *reinterpret_cast<const float4*>(te + o);
+            x0[4 * j + 0] = v0.x;
+            x0[4 * j + 1] = v0.y;
+            x0[4 * j + 2] = v0.z;
+            x0[4 * j + 3] = v0.w;
+            if constexpr (ROWS == 2) {
+                const float4 v1 = *reinterpret_cast<const float4*>(te + kTileBytes + o);
+                x1[4 * j + 0] = v1.x;
+                x1[4 * j + 1] = v1.y;
+                x1[4 * j + 2] = v1.z;
+                x1[4 * j + 3] = v1.w;
+            }
         }
         // Release the stage as soon as its samples are in registers.
         ptx::mbar_arrive(&empty[s]);
@@ -233,8 +247,10 @@ __global__ void __launch_bounds__(640, 1)
             if (((m >> (4 * g)) & 0xfu) == 0) {
 #pragma unroll
                 for (int i = 4 * g; i < 4 * g + 4; ++i) {
-                    acc_e = __fadd_rn(acc_e, xe[i]);
-                    acc_v = __fadd_rn(acc_v, xv[i]);
+                    acc0 = __fadd_rn(acc0, x0[i]);
+                    if constexpr (ROWS == 2) {
+                        acc1 = __fadd_rn(acc1, x1[i]);
+                    }
                 }
             } else {
 #pragma unroll
@@ -242,15 +258,19 @@ __global__ void __launch_bounds__(640, 1)
                     if (m & (1u << i)) {
                         start_run(rl);
                     }
-                    acc_e = __fadd_rn(acc_e, xe[i]);
-                    acc_v = __fadd_rn(acc_v, xv[i]);
+                    acc0 = __fadd_rn(acc0, x0[i]);
+                    if constexpr (ROWS == 2) {
+                        acc1 = __fadd_rn(acc1, x1[i]);
+                    }
                 }
             }
         }
         r = rbase + rl;
     }
-    A[bin * kWarp] = acc_e;
-    A[vrow + bin * kWarp] = acc_v;
+    A[bin * kWarp] = acc0;
+    if constexpr (ROWS == 2) {
+        A[vrow + bin * kWarp] = acc1;
+    }
     if (r != nr) {
         atomicOr(a.status, dev::kStatusBadTable);
     }
@@ -258,8 +278,9 @@ __global__ void __launch_bounds__(640, 1)
     const uint32_t seg = static_cast<uint32_t>(seg0 + lane);
     if (seg < a.nseg) {
 #pragma unroll
-        for (uint32_t row = 0; row < 2; ++row) {
-            const float* R = A + row * vrow;
+        for (int k = 0; k < ROWS; ++k) {
+            const float* R = A + k * vrow;
+            const uint32_t row = row0 + static_cast<uint32_t>(k);
             float* out = a.fold + ((static_cast<size_t>(seg) * a.nfreq + f) * 2 + row) * a.nbins;
             if ((a.nbins & 3u) == 0) {
                 for (uint32_t b = 0; b < a.nbins; b += 4) {
@@ -345,7 +366,13 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
         m_stages = std::max<uint32_t>(2, std::min<uint32_t>(kMaxStages, std::atoi(env)));
     }
     const size_t ring = m_stages * kStageBytes + 2 * m_stages * sizeof(uint64_t);
-    const size_t per_warp = 2 * (m_nbins + 1) * kWarp * sizeof(float);
+    // Rows per warp: both when two rows' accumulators of nbins <= 64 leave
+    // room for >= 11 warps per block, else one (LOKI_B200_BF_ROWS overrides).
+    m_rows = m_nbins <= 64 ? 2 : 1;
+    if (const char* env = std::getenv("LOKI_B200_BF_ROWS")) {
+        m_rows = std::atoi(env) == 1 ? 1 : 2;
+    }
+    const size_t per_warp = m_rows * (m_nbins + 1) * kWarp * sizeof(float);
     require(ring + per_warp <= kSmemLimit,
             "BruteFold: nbins too large for the shared-memory accumulators");
     const uint32_t wmax = static_cast<uint32_t>(
@@ -353,7 +380,7 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
     int dev = 0, nsm = 148;
     LK_CUDA(cudaGetDevice(&dev));
     LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const uint64_t nitems = m_nfreq;
+    const uint64_t nitems = (m_rows == 2 ? 1 : 2) * m_nfreq;
     const uint64_t xblocks = (m_nseg + kWarp - 1) / kWarp;
     // The kernel is latency-bound per warp, so block time hardly depends on W:
     // take the fewest waves of blocks over the SMs among W >= 3/4 of the
@@ -440,27 +467,33 @@ uint64_t BruteFoldDevice::device_bytes() const {
 
 // The TMA maps read the series in place; a base address that is not 16-byte
 // aligned (a TMA requirement) is first copied into an aligned staging buffer.
-void BruteFoldDevice::bind_inputs(const float* d_ts_e, const float* d_ts_v, cudaStream_t s) {
+// A batch of nbatch series stored back to back is folded as one series of
+// nbatch * nseg segments: every segment is folded from its own start.
+void BruteFoldDevice::bind_inputs(const float* d_ts_e, const float* d_ts_v, cudaStream_t s,
+                                  uint64_t nbatch) {
+    require(nbatch >= 1, "BruteFold: nbatch must be positive");
+    const uint64_t n = nbatch * m_nsamps;
     const float* e = d_ts_e;
     const float* v = d_ts_v;
     const bool aligned = (reinterpret_cast<uintptr_t>(e) % 16 == 0) &&
                          (reinterpret_cast<uintptr_t>(v) % 16 == 0);
     if (!aligned) {
-        if (m_stage.bytes < 2 * m_nsamps * sizeof(float)) {
-            m_stage.alloc(2 * m_nsamps * sizeof(float));
+        if (m_stage.bytes < 2 * n * sizeof(float)) {
+            m_stage.alloc(2 * n * sizeof(float));
         }
         float* se = m_stage.as<float>();
-        float* sv = se + m_nsamps;
-        LK_CUDA(cudaMemcpyAsync(se, e, m_nsamps * sizeof(float), cudaMemcpyDeviceToDevice, s));
-        LK_CUDA(cudaMemcpyAsync(sv, v, m_nsamps * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        float* sv = se + n;
+        LK_CUDA(cudaMemcpyAsync(se, e, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        LK_CUDA(cudaMemcpyAsync(sv, v, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
         e = se;
         v = sv;
     }
-    if (e != m_map_e_ptr || v != m_map_v_ptr) {
-        encode_series_map(&m_tmap_e, e, m_seglen, m_nseg);
-        encode_series_map(&m_tmap_v, v, m_seglen, m_nseg);
+    if (e != m_map_e_ptr || v != m_map_v_ptr || nbatch != m_map_batch) {
+        encode_series_map(&m_tmap_e, e, m_seglen, nbatch * m_nseg);
+        encode_series_map(&m_tmap_v, v, m_seglen, nbatch * m_nseg);
         m_map_e_ptr = e;
         m_map_v_ptr = v;
+        m_map_batch = nbatch;
     }
 }
 
@@ -471,16 +504,18 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
     a.bins = m_bins.ptr;
     a.bin_off = m_bin_off.as<uint64_t>();
     a.nruns = m_nruns.as<uint64_t>();
+    const uint64_t nseg = m_map_batch * m_nseg;  // segments of the bound batch
+    require(nseg <= 0x7fffffffULL, "BruteFold: too many segments");
     a.nfreq = static_cast<uint32_t>(m_nfreq);
-    a.nseg = static_cast<uint32_t>(m_nseg);
+    a.nseg = static_cast<uint32_t>(nseg);
     a.nbins = static_cast<uint32_t>(m_nbins);
     a.nwords = static_cast<uint32_t>(m_nwords);
     a.warps = m_warps;
     a.stages = m_stages;
     a.fold = d_fold;
     a.status = m_status;
-    const uint64_t nitems = m_nfreq;
-    dim3 grid(static_cast<unsigned>((m_nseg + kWarp - 1) / kWarp),
+    const uint64_t nitems = (m_rows == 2 ? 1 : 2) * m_nfreq;
+    dim3 grid(static_cast<unsigned>((nseg + kWarp - 1) / kWarp),
               static_cast<unsigned>((nitems + m_warps - 1) / m_warps));
     auto launch = [&](auto kern) {
         LK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -488,9 +523,11 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
         kern<<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_e, m_tmap_v, a);
     };
     if (m_wide_bins) {
-        launch(brute_fold_mask_kernel<uint16_t>);
+        m_rows == 2 ? launch(brute_fold_mask_kernel<uint16_t, 2>)
+                    : launch(brute_fold_mask_kernel<uint16_t, 1>);
     } else {
-        launch(brute_fold_mask_kernel<uint8_t>);
+        m_rows == 2 ? launch(brute_fold_mask_kernel<uint8_t, 2>)
+                    : launch(brute_fold_mask_kernel<uint8_t, 1>);
     }
     LK_CUDA(cudaGetLastError());
 }

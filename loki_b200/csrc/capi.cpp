@@ -221,6 +221,58 @@ int lk_ffa_search(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, float s
     });
 }
 
+int lk_ffa_create_batched(const lk_plan* plan, int device, int storage, uint64_t max_batch,
+                          lk_ffa** out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        auto f = std::make_unique<lk_ffa>();
+        f->exec = std::make_unique<lk::FFAExec>(plan->plan, device, storage, max_batch);
+        *out = f.release();
+    });
+}
+
+int lk_ffa_execute_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
+                         float* d_fold, uint64_t fold_len, lk_stream_t stream) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_fold, "d_fold");
+        ffa->exec->execute(d_ts_e, d_ts_v, d_fold, fold_len, reinterpret_cast<cudaStream_t>(stream),
+                           nbatch);
+    });
+}
+
+int lk_ffa_scores_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
+                        float* d_scores, uint64_t scores_len, lk_stream_t stream) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_scores, "d_scores");
+        ffa->exec->scores(d_ts_e, d_ts_v, d_scores, scores_len,
+                          reinterpret_cast<cudaStream_t>(stream), nbatch);
+    });
+}
+
+int lk_ffa_search_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
+                        float snr_min, uint32_t* d_idx, float* d_snr, uint64_t max_cands,
+                        uint64_t* d_count, lk_stream_t stream) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_count, "d_count");
+        if (max_cands > 0) {
+            need(d_idx, "d_idx");
+            need(d_snr, "d_snr");
+        }
+        ffa->exec->search(d_ts_e, d_ts_v, snr_min, d_idx, d_snr, max_cands, d_count,
+                          reinterpret_cast<cudaStream_t>(stream), nbatch);
+    });
+}
+
 int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status) {
     return guarded([&] {
         need(ffa, "ffa");

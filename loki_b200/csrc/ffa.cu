@@ -46,7 +46,9 @@ StageProfiler::~StageProfiler() {
     }
 }
 
-FFAExec::FFAExec(const Plan& p, int device, int storage) : plan(p), device(device) {
+FFAExec::FFAExec(const Plan& p, int device, int storage, uint64_t max_batch_)
+    : plan(p), device(device), max_batch(max_batch_) {
+    require(max_batch >= 1 && max_batch <= 65535, "max_batch must lie in [1, 65535]");
     require(storage == LK_FP32, "only FP32 fold storage is implemented by this executor");
     require(plan.nparams <= 3, "the FFA executor supports nparams <= 3");
     require(plan.n_levels >= 2, "FFA::execute_unified: levels must be greater than or equal to 2");
@@ -68,8 +70,8 @@ FFAExec::FFAExec(const Plan& p, int device, int storage) : plan(p), device(devic
     for (uint32_t l = 0; l + 1 < plan.n_levels; ++l) {
         inter = std::max(inter, plan.fold_size(l));
     }
-    buf[0].alloc(sizeof(float) * inter);
-    buf[1].alloc(sizeof(float) * inter);
+    buf[0].alloc(sizeof(float) * inter * max_batch);
+    buf[1].alloc(sizeof(float) * inter * max_batch);
     sp = make_score_params(plan.widths.data(), static_cast<uint32_t>(plan.widths.size()),
                            static_cast<uint32_t>(plan.cfg.nbins));
 }
@@ -90,24 +92,27 @@ uint64_t FFAExec::coord_bytes(uint32_t l) const {
 }
 
 float* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t last,
-                           float* final_out, cudaStream_t s) {
+                           float* final_out, cudaStream_t s, uint64_t nbatch) {
+    require(nbatch >= 1 && nbatch <= max_batch, "nbatch must lie in [1, max_batch]");
     const bool taylor = plan.nparams > 1;
     const auto nbins = static_cast<uint32_t>(plan.cfg.nbins);
     float* in = (last == 0 && final_out != nullptr) ? final_out : buf[0].as<float>();
     // Algorithmic bytes: the series in (E and V) and the level-0 fold out;
-    // each merge level reads the previous level and writes its own.
-    const uint64_t series_bytes = 8 * plan.cfg.nsamps;
-    bf->bind_inputs(ts_e, ts_v, s);
-    prof.begin(LK_STAGE_BRUTE_FOLD, 0, 1, series_bytes + 4 * plan.fold_size(0), s);
+    // each merge level reads the previous level and writes its own. A batch of
+    // series is, level by level, one series with nbatch times the segments
+    // (merges pair segments 2s and 2s + 1, never across two series).
+    const uint64_t series_bytes = 8 * plan.cfg.nsamps * nbatch;
+    bf->bind_inputs(ts_e, ts_v, s, nbatch);
+    prof.begin(LK_STAGE_BRUTE_FOLD, 0, 1, series_bytes + 4 * plan.fold_size(0) * nbatch, s);
     bf->fold(in, s);
     prof.end(s);
     for (uint32_t l = 1; l <= last; ++l) {
         float* out = (l == last && final_out != nullptr) ? final_out : buf[l % 2].as<float>();
         prof.begin(LK_STAGE_MERGE, static_cast<int>(l), 1,
-                   4 * (plan.fold_size(l - 1) + plan.fold_size(l)) + coord_bytes(l), s);
+                   nbatch * (4 * (plan.fold_size(l - 1) + plan.fold_size(l))) + coord_bytes(l), s);
         const uint64_t n_inner = plan.param_counts[l][plan.nparams - 1];
         merge_level(in, out, level_coords(l), taylor, n_inner, plan.ncoords[l] / n_inner,
-                    plan.ncoords[l - 1], plan.nsegments[l], nbins, s);
+                    plan.ncoords[l - 1], plan.nsegments[l] * nbatch, nbins, s);
         prof.end(s);
         in = out;
     }
@@ -115,39 +120,41 @@ float* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t last,
 }
 
 void FFAExec::execute(const float* ts_e, const float* ts_v, float* fold, uint64_t fold_len,
-                      cudaStream_t s) {
+                      cudaStream_t s, uint64_t nbatch) {
     const uint32_t L = plan.n_levels;
-    require(fold_len >= plan.fold_size(L - 1), "fold must hold fold_size floats");
+    require(fold_len >= plan.fold_size(L - 1) * nbatch, "fold must hold fold_size floats");
     DeviceGuard g(device);
     prof.reset();
-    run_levels(ts_e, ts_v, L - 1, fold, s);
+    run_levels(ts_e, ts_v, L - 1, fold, s, nbatch);
 }
 
 void FFAExec::scores(const float* ts_e, const float* ts_v, float* d_scores, uint64_t len,
-                     cudaStream_t s) {
+                     cudaStream_t s, uint64_t nbatch) {
     const uint32_t L = plan.n_levels;
     require(plan.nsegments[L - 1] == 1, "compute_ffa_scores: nsegments must be 1 for scores");
-    require(len >= plan.ncoords[L - 1] * plan.widths.size(),
+    require(len >= plan.ncoords[L - 1] * plan.widths.size() * nbatch,
             "scores must hold ncoords * n_widths floats");
     DeviceGuard g(device);
     if (!in_search) {
         prof.reset();
     }
-    const float* in = run_levels(ts_e, ts_v, L - 2, nullptr, s);
+    const float* in = run_levels(ts_e, ts_v, L - 2, nullptr, s, nbatch);
     const uint64_t nscores = plan.ncoords[L - 1] * plan.widths.size();
     prof.begin(LK_STAGE_MERGE_SCORE, static_cast<int>(L - 1), 1,
-               4 * plan.fold_size(L - 2) + coord_bytes(L - 1) + 4 * nscores, s);
+               nbatch * (4 * plan.fold_size(L - 2) + 4 * nscores) + coord_bytes(L - 1), s);
     const uint64_t n_inner = plan.param_counts[L - 1][plan.nparams - 1];
     merge_score_level(in, level_coords(L - 1), plan.nparams > 1, n_inner,
                       plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
-                      static_cast<uint32_t>(plan.cfg.nbins), sp, LK_SCORE_PER_WIDTH, d_scores, s);
+                      static_cast<uint32_t>(plan.cfg.nbins), sp, LK_SCORE_PER_WIDTH, d_scores, s,
+                      nbatch);
     prof.end(s);
 }
 
 void FFAExec::search(const float* ts_e, const float* ts_v, float snr_min, uint32_t* d_idx,
-                     float* d_snr, uint64_t max_cands, uint64_t* d_count, cudaStream_t s) {
+                     float* d_snr, uint64_t max_cands, uint64_t* d_count, cudaStream_t s,
+                     uint64_t nbatch) {
     const uint32_t L = plan.n_levels;
-    const uint64_t n = plan.ncoords[L - 1] * plan.widths.size();
+    const uint64_t n = plan.ncoords[L - 1] * plan.widths.size() * nbatch;
     DeviceGuard g(device);
     if (scores_tmp.bytes < n * sizeof(float)) {
         scores_tmp.alloc(n * sizeof(float));
@@ -156,7 +163,7 @@ void FFAExec::search(const float* ts_e, const float* ts_v, float snr_min, uint32
     prof.reset();
     in_search = true;
     try {
-        scores(ts_e, ts_v, scores_tmp.as<float>(), n, s);
+        scores(ts_e, ts_v, scores_tmp.as<float>(), n, s, nbatch);
     } catch (...) {
         in_search = false;
         throw;

@@ -58,19 +58,24 @@ struct FFAExec {
     ScoreParams sp{};
     bool in_search = false;
 
-    FFAExec(const Plan& p, int device, int storage);
+    uint64_t max_batch = 1;  // series per call (buffers are sized for it)
+
+    FFAExec(const Plan& p, int device, int storage, uint64_t max_batch = 1);
     uint64_t device_bytes() const;
     const void* level_coords(uint32_t l) const;
     uint64_t coord_bytes(uint32_t l) const;
     std::vector<lk_stage_time> profile(cudaStream_t s);
+    // All entry points take nbatch series of nsamps samples stored back to
+    // back; outputs are the single-series outputs of each, back to back.
     float* run_levels(const float* ts_e, const float* ts_v, uint32_t last, float* final_out,
-                      cudaStream_t s);
+                      cudaStream_t s, uint64_t nbatch = 1);
     void execute(const float* ts_e, const float* ts_v, float* fold, uint64_t fold_len,
-                 cudaStream_t s);
+                 cudaStream_t s, uint64_t nbatch = 1);
     void scores(const float* ts_e, const float* ts_v, float* d_scores, uint64_t len,
-                cudaStream_t s);
+                cudaStream_t s, uint64_t nbatch = 1);
     void search(const float* ts_e, const float* ts_v, float snr_min, uint32_t* d_idx,
-                float* d_snr, uint64_t max_cands, uint64_t* d_count, cudaStream_t s);
+                float* d_snr, uint64_t max_cands, uint64_t* d_count, cudaStream_t s,
+                uint64_t nbatch = 1);
     uint32_t read_status(cudaStream_t s);
 };
 

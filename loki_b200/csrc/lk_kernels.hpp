@@ -55,9 +55,12 @@ public:
         bind_inputs(d_ts_e, d_ts_v, s);
         fold(d_fold, s);
     }
-    // Points the input tensor maps at the series (host work; a misaligned
-    // series is first copied into an aligned buffer on `s`).
-    void bind_inputs(const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
+    // Points the input tensor maps at the series, or at nbatch series of
+    // nsamps samples stored back to back (host work; a misaligned series is
+    // first copied into an aligned buffer on `s`). fold() then folds all of
+    // them: d_fold holds nbatch * fold_size() floats.
+    void bind_inputs(const float* d_ts_e, const float* d_ts_v, cudaStream_t s,
+                     uint64_t nbatch = 1);
     void fold(float* d_fold, cudaStream_t s);
     uint64_t nseg() const { return m_nseg; }
     uint64_t nfreq() const { return m_nfreq; }
@@ -68,7 +71,8 @@ private:
     uint64_t m_nfreq, m_seglen, m_nbins, m_nsamps, m_nseg = 0;
     uint64_t m_nwords = 0;
     bool m_wide_bins = false;  // uint16 run bins (nbins > 256)
-    uint32_t m_warps = 0;      // consumer warps (frequencies) per block
+    uint32_t m_rows = 2;       // rows (E, V) per consumer warp
+    uint32_t m_warps = 0;      // consumer warps per block
     uint32_t m_stages = 0;     // shared-memory ring depth (32-sample words)
     size_t m_smem = 0;         // dynamic shared memory per block
     uint32_t* m_status;
@@ -80,6 +84,7 @@ private:
     CUtensorMap m_tmap_e{}, m_tmap_v{};
     const float* m_map_e_ptr = nullptr;
     const float* m_map_v_ptr = nullptr;
+    uint64_t m_map_batch = 1;
 };
 
 // One merge level: out[s, c] = rot(in[2s, tail(c)], st(c)) + rot(in[2s+1, head(c)], sh(c)).
@@ -98,10 +103,13 @@ struct ScoreParams {
 };
 ScoreParams make_score_params(const uint32_t* widths, uint32_t nwidths, uint32_t nbins);
 
-// Final merge level fused with scoring (nsegments == 1).
+// Final merge level fused with scoring (one output segment per series;
+// nbatch series, the input holding 2 * nbatch segments of ncoords_prev cells,
+// scores [nbatch][ncoords][nout]).
 void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
                        uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
-                       const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s);
+                       const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s,
+                       uint64_t nbatch = 1);
 
 // Standalone scoring of [nprof, 2, nbins] (is3d) or [nprof, nbins] folds.
 void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d,

@@ -16,6 +16,8 @@
 // contiguous 128-byte span). Blocks are numbered frequency-tile-major, so the
 // outer rows that read the same parent rows run at the same time and share
 // them through L2.
+#include <algorithm>
+
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
 #include "lk_merge.cuh"
@@ -66,22 +68,31 @@ void merge_level(const float* d_in, float* d_out, const void* d_coords, bool tay
                  uint32_t nbins, cudaStream_t s) {
     require(n_inner > 0 && n_outer > 0, "empty merge level");
     const uint64_t tiles = (n_inner + kCoordsPerBlock - 1) / kCoordsPerBlock;
-    require(tiles * n_outer <= 0x7fffffffULL && nsegments <= 65535 && n_inner <= 0xffffffffULL &&
+    require(tiles * n_outer <= 0x7fffffffULL && n_inner <= 0xffffffffULL &&
                 n_outer <= 0xffffffffULL,
             "merge level too large for the launch grid");
-    dim3 grid(static_cast<unsigned>(tiles * n_outer), static_cast<unsigned>(nsegments));
-    if (taylor) {
-        merge_kernel<true><<<grid, kThreads, 0, s>>>(d_in, d_out, d_coords,
-                                                     static_cast<uint32_t>(n_inner),
-                                                     static_cast<uint32_t>(n_outer),
-                                                     ncoords_prev, nbins);
-    } else {
-        merge_kernel<false><<<grid, kThreads, 0, s>>>(d_in, d_out, d_coords,
-                                                      static_cast<uint32_t>(n_inner),
-                                                      static_cast<uint32_t>(n_outer),
-                                                      ncoords_prev, nbins);
+    // Output segments on grid.y, at most 65535 per launch (batched series can
+    // have more).
+    const uint64_t row = 2ull * nbins;
+    const uint64_t ncur = n_inner * n_outer;
+    for (uint64_t s0 = 0; s0 < nsegments; s0 += 65535) {
+        const uint64_t ns = std::min<uint64_t>(65535, nsegments - s0);
+        dim3 grid(static_cast<unsigned>(tiles * n_outer), static_cast<unsigned>(ns));
+        const float* in = d_in + s0 * 2 * ncoords_prev * row;
+        float* out = d_out + s0 * ncur * row;
+        if (taylor) {
+            merge_kernel<true><<<grid, kThreads, 0, s>>>(in, out, d_coords,
+                                                         static_cast<uint32_t>(n_inner),
+                                                         static_cast<uint32_t>(n_outer),
+                                                         ncoords_prev, nbins);
+        } else {
+            merge_kernel<false><<<grid, kThreads, 0, s>>>(in, out, d_coords,
+                                                          static_cast<uint32_t>(n_inner),
+                                                          static_cast<uint32_t>(n_outer),
+                                                          ncoords_prev, nbins);
+        }
+        LK_CUDA(cudaGetLastError());
     }
-    LK_CUDA(cudaGetLastError());
 }
 
 }  // namespace lk

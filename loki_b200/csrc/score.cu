@@ -73,6 +73,10 @@ __global__ void merge_score_kernel(const float* __restrict__ in, const void* __r
                                    uint32_t nbins, uint32_t rs, ScoreParams sp, int mode,
                                    float* __restrict__ scores) {
     extern __shared__ float rows[];
+    // Series of a batch on grid.y: input segments 2b and 2b + 1, scores b.
+    in += static_cast<uint64_t>(blockIdx.y) * 2 * nprev * 2 * nbins;
+    scores += static_cast<uint64_t>(blockIdx.y) * n_inner * n_outer *
+              (mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1);
     const uint32_t T = blockDim.x;
     const uint32_t tile = blockIdx.x / n_outer;
     const uint32_t outer = blockIdx.x - tile * n_outer;
@@ -201,7 +205,9 @@ void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d
 
 void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
                        uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
-                       const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s) {
+                       const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s,
+                       uint64_t nbatch) {
+    require(nbatch >= 1 && nbatch <= 65535, "nbatch must lie in [1, 65535]");
     if (n_inner == 0 || n_outer == 0) {
         return;
     }
@@ -216,8 +222,8 @@ void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uin
     const auto no = static_cast<uint32_t>(n_outer);
     auto launch = [&](auto kern) {
         set_smem(kern, smem);
-        kern<<<blocks, T, smem, s>>>(d_in, d_coords, ni, no, ncoords_prev, nbins, rs, sp, mode,
-                                     d_scores);
+        kern<<<dim3(blocks, static_cast<unsigned>(nbatch)), T, smem, s>>>(
+            d_in, d_coords, ni, no, ncoords_prev, nbins, rs, sp, mode, d_scores);
     };
     const int nwb = sp.nwidths <= 8 ? 8 : (sp.nwidths <= 16 ? 16 : 32);
     const int nj = nbins <= 32 ? 1 : (nbins <= 64 ? 2 : (nbins <= 128 ? 4 : 0));

@@ -36,16 +36,19 @@ class FFACUDA:
     intermediate fold buffers; it can be executed many times.
     """
 
-    def __init__(self, cfg: PulsarSearchConfig, device_id: int = 0, fold_storage: str = "fp32"):
+    def __init__(self, cfg: PulsarSearchConfig, device_id: int = 0, fold_storage: str = "fp32",
+                 max_batch: int = 1):
         D.require_cuda(device_id)
         self._cfg = cfg
         self._plan = FFAPlanTime(cfg)
         self._device = device_id
+        self._max_batch = int(max_batch)
         if fold_storage not in _STORAGE:
             raise ValueError(f"fold_storage must be one of {sorted(_STORAGE)}")
         h = ctypes.c_void_p()
         with D.torch().cuda.device(device_id):
-            C.check(C.lib().lk_ffa_create(cfg._plan_handle, device_id, _STORAGE[fold_storage], ctypes.byref(h)))
+            C.check(C.lib().lk_ffa_create_batched(cfg._plan_handle, device_id, _STORAGE[fold_storage],
+                                                  self._max_batch, ctypes.byref(h)))
         self._h = h
 
     def __del__(self):
@@ -127,6 +130,54 @@ class FFACUDA:
                                           cap, cnt.data_ptr(), D.stream_ptr(self._device)))
         total = int(cnt.item())
         k = min(total, cap)
+        return idx[:k].cpu().numpy().view(np.uint32), snr[:k].cpu().numpy(), total
+
+    # ---- batches of equal-length series ([nbatch, nsamps] CUDA tensors) -------------
+
+    def _batch_inputs(self, ts_e, ts_v):
+        n = self._cfg.nsamps
+        e = D.to_device_f32(ts_e, self._device).reshape(-1)
+        v = D.to_device_f32(ts_v, self._device).reshape(-1)
+        if e.numel() % n != 0 or e.numel() != v.numel():
+            raise RuntimeError("batch inputs must be [nbatch, nsamps] with matching ts_e / ts_v")
+        nb = e.numel() // n
+        if nb < 1 or nb > self._max_batch:
+            raise RuntimeError(f"nbatch must lie in [1, max_batch={self._max_batch}]")
+        return e, v, nb
+
+    def scores_batch(self, ts_e, ts_v, out=None):
+        """Boxcar S/N of each series of the batch: a [nbatch, ncoords_final *
+        n_widths] CUDA tensor (one launch per level for the whole batch)."""
+        e, v, nb = self._batch_inputs(ts_e, ts_v)
+        per = int(self._plan.ncoords[-1]) * self._cfg.n_scoring_widths
+        res = out if out is not None else D.empty_f32(nb * per, self._device)
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_ffa_scores_batch(self._h, D.ptr(e), D.ptr(v), nb, D.ptr(res), res.numel(),
+                                                D.stream_ptr(self._device)))
+        return res.reshape(nb, per) if out is None else res
+
+    def search_batch(self, ts_e, ts_v, snr_min: float | None = None, idx=None, snr=None, count=None):
+        """Scores of the batch compacted to S/N >= snr_min in flat
+        ((series * ncoords + coord) * n_widths + width) order. With idx / snr /
+        count CUDA tensors given, nothing is allocated (graph-capturable) and
+        they are returned; otherwise returns host (indices, snrs, total)."""
+        e, v, nb = self._batch_inputs(ts_e, ts_v)
+        thr = self._cfg.snr_min if snr_min is None else float(snr_min)
+        t = D.torch()
+        given = idx is not None
+        if not given:
+            cap = self._cfg.max_passing_candidates
+            idx = t.empty(cap, dtype=t.int32, device=f"cuda:{self._device}")
+            snr = D.empty_f32(cap, self._device)
+            count = t.zeros(1, dtype=t.int64, device=f"cuda:{self._device}")
+        with t.cuda.device(self._device):
+            C.check(C.lib().lk_ffa_search_batch(self._h, D.ptr(e), D.ptr(v), nb, thr, idx.data_ptr(),
+                                                D.ptr(snr), idx.numel(), count.data_ptr(),
+                                                D.stream_ptr(self._device)))
+        if given:
+            return idx, snr, count
+        total = int(count.item())
+        k = min(total, idx.numel())
         return idx[:k].cpu().numpy().view(np.uint32), snr[:k].cpu().numpy(), total
 
     def set_profiling(self, enable: bool = True) -> None:

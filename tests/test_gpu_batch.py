@@ -1,0 +1,104 @@
+"""Batched FFA executor on the GPU: every series of a batch gets exactly its
+single-series result (the batch is one launch per level), search indices are
+flat over the batch, and a CUDA-graph capture of a batch step replays to the
+same result; the multi-series driver pads, groups and matches the oracle."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import series
+from oracle import lko
+
+pytestmark = pytest.mark.gpu
+
+
+def _cfg(nsamps, nbins=32, lims=((-300.0, 300.0), (5.0, 8.0)), tsamp=1e-3, widths=(1, 2, 3, 4, 6)):
+    from loki_b200.configs import PulsarSearchConfig
+
+    return PulsarSearchConfig(nsamps, tsamp, nbins, 1.0, np.array(lims), use_fourier=False,
+                              score_widths=list(widths))
+
+
+@pytest.mark.parametrize("nbins,lims", [(32, ((-300.0, 300.0), (5.0, 8.0))), (128, ((20.0, 40.0),))])
+def test_batch_matches_single_series(cuda, nbins, lims):
+    from loki_b200.ffa import FFACUDA
+
+    t = cuda
+    n, nb = 1 << 17, 3
+    cfg = _cfg(n, nbins, lims, tsamp=1e-3 if len(lims) == 2 else 64e-6)
+    single = FFACUDA(cfg)
+    batched = FFACUDA(cfg, max_batch=4)
+    es, vs = zip(*(series(n, 40 + k) for k in range(nb)))
+    e = t.from_numpy(np.stack(es)).cuda()
+    v = t.from_numpy(np.stack(vs)).cuda()
+    got = batched.scores_batch(e, v).cpu().numpy()
+    for k in range(nb):
+        want = single.scores(es[k], vs[k])
+        np.testing.assert_array_equal(got[k].view(np.uint32), want.view(np.uint32))
+    # search indices flat over [series][coord][width]
+    thr = float(np.quantile(got, 0.999))
+    idx, snr, total = batched.search_batch(e, v, snr_min=thr)
+    flat = got.ravel()
+    want_idx = np.flatnonzero(flat >= thr)
+    assert total == want_idx.size
+    np.testing.assert_array_equal(idx, want_idx.astype(np.uint32))
+    np.testing.assert_array_equal(snr, flat[want_idx])
+
+
+def test_batch_graph_replay(cuda):
+    from loki_b200.ffa import FFACUDA
+
+    t = cuda
+    n, nb = 1 << 16, 2
+    cfg = _cfg(n)
+    ffa = FFACUDA(cfg, max_batch=nb)
+    e = t.empty((nb, n), dtype=t.float32, device="cuda")
+    v = t.empty((nb, n), dtype=t.float32, device="cuda")
+    idx = t.empty(1 << 16, dtype=t.int32, device="cuda")
+    snr = t.empty(1 << 16, dtype=t.float32, device="cuda")
+    cnt = t.zeros(1, dtype=t.int64, device="cuda")
+    es, vs = zip(*(series(n, 60 + k) for k in range(nb)))
+    e.copy_(t.from_numpy(np.stack(es)))
+    v.copy_(t.from_numpy(np.stack(vs)))
+    ffa.search_batch(e, v, 3.0, idx, snr, cnt)  # warm-up: allocations happen here
+    t.cuda.synchronize()
+    eager = (idx[: int(cnt.item())].clone(), snr[: int(cnt.item())].clone())
+    g = t.cuda.CUDAGraph()
+    with t.cuda.graph(g):
+        ffa.search_batch(e, v, 3.0, idx, snr, cnt)
+    for k in range(2):
+        es2, vs2 = zip(*(series(n, 70 + 10 * k + j) for j in range(nb)))
+        e.copy_(t.from_numpy(np.stack(es2)))
+        v.copy_(t.from_numpy(np.stack(vs2)))
+        g.replay()
+        t.cuda.synchronize()
+        got = (idx[: int(cnt.item())].cpu().numpy(), snr[: int(cnt.item())].cpu().numpy())
+        ffa.search_batch(e, v, 3.0, idx, snr, cnt)
+        t.cuda.synchronize()
+        np.testing.assert_array_equal(got[0], idx[: int(cnt.item())].cpu().numpy())
+        np.testing.assert_array_equal(got[1], snr[: int(cnt.item())].cpu().numpy())
+    assert eager[0].numel() > 0
+
+
+def test_multi_series_driver_matches_oracle(cuda):
+    from loki_b200.batched import MultiSeriesSearch
+
+    lengths = [3000, 5000, 9000, 16384, 20000, 70000]
+    rng = np.random.default_rng(5)
+    data = [(rng.standard_normal(L).astype(np.float32), np.ones(L, np.float32)) for L in lengths]
+    widths = [1, 2, 3, 4, 6, 8]
+    ms = MultiSeriesSearch(tsamp=1e-3, nbins=32, f_range=(5.0, 9.0), widths=widths, snr_min=3.5, max_batch=2)
+    res = ms.search(data)
+    for (e, v), r in zip(data, res):
+        L = 1 << int(np.ceil(np.log2(e.size)))
+        ep = np.zeros(L, np.float32)
+        vp = np.zeros(L, np.float32)
+        ep[: e.size] = e
+        vp[: e.size] = v
+        plan = lko.plan_create(lko.make_cfg(L, 1e-3, 32, 1.0, [[5.0, 9.0]]))
+        sc = lko.snr_boxcar_3d(lko.ffa(plan, ep, vp), np.array(widths, np.uint64), 32).ravel()
+        want = np.flatnonzero(sc >= 3.5)
+        np.testing.assert_array_equal(r["idx"], want.astype(np.uint32))
+        np.testing.assert_array_equal(r["snr"], sc[want])
