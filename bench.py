@@ -49,10 +49,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="taylor_accel",
-                    choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade"],
+                    choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade", "multi_series"],
                     help="taylor_accel (default): Taylor (f, fdot) FFA + S/N; freq_sweep: plain period "
                          "sweep; prune_jerk: FFA to 32 segments + one pruning run; mc_cascade: 8-stage "
-                         "Monte-Carlo threshold cascade")
+                         "Monte-Carlo threshold cascade; multi_series: 512 series of uneven length, "
+                         "batched with CUDA graphs")
     return ap.parse_args()
 
 

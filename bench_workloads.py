@@ -457,6 +457,111 @@ def run_mc(args, rank, world, local_rank):
     return 0
 
 
+# ---- multi_series -------------------------------------------------------------------
+
+def run_multi(args, rank, world, local_rank):
+    from loki_b200.synthetic import multi_series_workload
+
+    data, p = multi_series_workload()
+    lens = [int(e.size) for e, _ in data]
+    cfgd = {"nseries": len(data), "lengths": "log-uniform 2^18 .. 2^22 samples, padded to 2^k",
+            "tsamp": p["tsamp"], "nbins": p["nbins"], "f_range_hz": list(p["f_range"]),
+            "score_widths": p["widths"], "snr_min": B.SNR_MIN}
+
+    def trials_of(L, plan_ncoords):
+        return plan_ncoords * len(p["widths"])
+
+    def ref_sample(budget_s=20.0):
+        from oracle import ref
+
+        nthreads = os.cpu_count() or 1
+        picked = sorted(range(len(data)), key=lambda k: lens[k])[:: max(1, len(data) // 8)][:8]
+        trials, el = 0, 0.0
+        for k in picked:
+            e, v = data[k]
+            L = 1 << int(np.ceil(np.log2(e.size)))
+            ep, vp = np.zeros(L, np.float32), np.zeros(L, np.float32)
+            ep[: e.size], vp[: e.size] = e, v
+            params = dict(nsamps=L, tsamp=p["tsamp"], nbins=p["nbins"], eta=p["eta"],
+                          param_limits=[list(p["f_range"])], score_widths=p["widths"])
+            step, ntrials, _ = B.reference_runner(params)
+            step(ep, vp)
+            t0 = time.perf_counter()
+            step(ep, vp)
+            el += time.perf_counter() - t0
+            trials += ntrials
+            if el > budget_s:
+                break
+        return trials / el, el, len(picked), nthreads
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from oracle import ref
+
+        if not ref.available("timing"):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return 0
+        v, el, npick, nthreads = ref_sample()
+        print(json.dumps(_line(args, world, "multi_series_512x2^18..2^22_nbins128", v, 1e3 * el, cfgd,
+                               impl="reference",
+                               cpu_baseline={"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                                             "sample": f"{npick} series spread over the lengths, one FFA + "
+                                                       f"scores + compaction each ({el:.1f} s)"},
+                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})))
+        return 0
+    torch, dist = _init(local_rank, world)
+    from loki_b200.batched import MultiSeriesSearch, _pow2_ceil
+
+    ms = MultiSeriesSearch(tsamp=p["tsamp"], nbins=p["nbins"], f_range=p["f_range"], widths=p["widths"],
+                           snr_min=B.SNR_MIN, max_batch=16, device_id=local_rank)
+    d_data = [(torch.from_numpy(e).cuda(), torch.from_numpy(v).cuda()) for e, v in data]
+    flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ms.search(d_data[:1])
+
+    def step():
+        return ms.search(d_data)
+
+    clocks = B.ClockSampler(local_rank)
+    clocks.start()
+    ms_step, outs = _timed(torch, step, args.steps, args.warmup, flush, dist)
+    clk = clocks.stop()
+    trials = 0
+    for L in {_pow2_ceil(n) for n in lens}:
+        g = ms.groups[L]
+        trials += g.per * sum(1 for n in lens if _pow2_ceil(n) == L)
+    value = trials * world / (ms_step / 1e3)
+    ncand = sum(r["total"] for r in outs[-1])
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ms.search(data)
+        el = time.perf_counter() - t0
+        e2e = {"value": trials * world * args.steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": 8 * sum(lens), "d2h_bytes_per_step": 8 * ncand + 8 * len(ms.groups),
+               "api": "MultiSeriesSearch.search (lk_ffa_search_batch, graph replays) from host arrays"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+
+        if ref.available("timing"):
+            cv, el, npick, nthreads = ref_sample()
+            cpu = {"value": cv, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                   "sample": f"{npick} series spread over the lengths, one FFA + scores + compaction each "
+                             f"({el:.1f} s), reference CPU code with its Release flags"}
+    groups = {str(L): {"series": sum(1 for n in lens if _pow2_ceil(n) == L), "batch": ms.groups[L].nbatch,
+                       "trials_per_series": ms.groups[L].per} for L in sorted(ms.groups)}
+    if rank == 0:
+        print(json.dumps(_line(args, world, "multi_series_512x2^18..2^22_nbins128", value, ms_step,
+                               dict(cfgd, trials_per_step=trials, candidates=ncand, groups=groups,
+                                    graphs="one CUDA graph per length for full batches"),
+                               cpu_baseline=cpu, e2e=e2e, clocks=clk)))
+    _finish(dist)
+    return 0
+
+
 def run(args, rank, world, local_rank):
-    return {"freq_sweep": run_freq, "prune_jerk": run_prune, "mc_cascade": run_mc}[args.workload](
-        args, rank, world, local_rank)
+    return {"freq_sweep": run_freq, "prune_jerk": run_prune, "mc_cascade": run_mc,
+            "multi_series": run_multi}[args.workload](args, rank, world, local_rank)

@@ -157,3 +157,23 @@ def jerk_prune_workload(seed: int = 11, n_signals: int = 2):
                   param_limits=[[-0.4, 0.4], [-457.0, 457.0], [20.0, 200.0]])
     thresholds = np.linspace(3.0, 8.0, 31).astype(np.float32)
     return ts_e, ts_v, params, thresholds, pulsars
+
+
+def multi_series_workload(nseries: int = 512, seed: int = 3, tsamp: float = 64e-6):
+    """Many beams / DM trials: nseries float32 series with lengths
+    log-uniform in [2^18, 2^22] samples at 64 us, N(0, 1) noise (variance
+    series of ones); one in eight carries a pulsar with period ~ U(20, 500) ms
+    and fold S/N ~ U(6, 20). Searched over periods 20-500 ms (f 2-50 Hz) at
+    nbins 128 with widths {1,2,3,4,6,8,12,16}."""
+    rng = np.random.default_rng(seed)
+    lengths = np.exp(rng.uniform(np.log(2.0 ** 18), np.log(2.0 ** 22), nseries)).astype(np.int64)
+    widths = [1, 2, 3, 4, 6, 8, 12, 16]
+    data = []
+    for k, n in enumerate(lengths):
+        ts_e = rng.standard_normal(int(n), dtype=np.float32)
+        if k % 8 == 0:
+            psr = Pulsar(f0=1.0 / float(rng.uniform(0.020, 0.500)), duty=0.05, snr=float(rng.uniform(6, 20)))
+            inject(ts_e, tsamp, psr, 128, widths)
+        data.append((ts_e, np.ones(int(n), dtype=np.float32)))
+    params = dict(tsamp=tsamp, nbins=128, f_range=(2.0, 50.0), widths=widths, eta=1.0)
+    return data, params
