@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--storage", default="fp32")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "bf16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="taylor_accel",
@@ -310,6 +310,7 @@ def run_ours(args, rank, world, local_rank):
     step_ms_max = float(t.item())
     value = ntrials * world / (step_ms_max / 1e3)
     ncand = int(cnt.item())
+    rescored = ffa.rescored_cells() if args.storage == "bf16" else 0
 
     # roofline of the dominant stage
     dom = max(stage_ms, key=stage_ms.get)
@@ -381,7 +382,8 @@ def run_ours(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_dict(params, {"fold_storage": args.storage, "final_coords": nc, "n_widths": nw,
-                                           "candidates": ncand}),
+                                           "candidates": ncand, "rescored_cells": rescored,
+                                           "rescore_margin": list(ffa.rescore_margin)}),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "stages": stages, "wall_s": wall,
         }

@@ -147,7 +147,7 @@ def run_freq(args, rank, world, local_rank):
     cfg = PulsarSearchConfig(params["nsamps"], params["tsamp"], params["nbins"], params["eta"],
                              np.array(params["param_limits"]), use_fourier=False,
                              score_widths=params["score_widths"], snr_min=B.SNR_MIN)
-    ffa = FFACUDA(cfg, device_id=local_rank)
+    ffa = FFACUDA(cfg, device_id=local_rank, fold_storage=args.storage)
     ntrials = int(ffa.plan.ncoords[-1]) * cfg.n_scoring_widths
     cap = 1 << 20
     e = torch.from_numpy(ts_e).cuda()
@@ -201,7 +201,8 @@ def run_freq(args, rank, world, local_rank):
         cpu = B.cpu_baseline(params, ts_e, ts_v)
     if rank == 0:
         print(json.dumps(_line(args, world, "freq_sweep_2^21x64us_nbins128", value, ms,
-                               dict(cfgd, final_coords=int(ffa.plan.ncoords[-1]), candidates=int(cnt.item())),
+                               dict(cfgd, final_coords=int(ffa.plan.ncoords[-1]), candidates=int(cnt.item()),
+                                    fold_storage=args.storage),
                                roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
                                gpu_launches=args.steps * launches, clocks=clk,
                                stages={k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()})))
@@ -514,7 +515,7 @@ def run_multi(args, rank, world, local_rank):
     from loki_b200.batched import MultiSeriesSearch, _pow2_ceil
 
     ms = MultiSeriesSearch(tsamp=p["tsamp"], nbins=p["nbins"], f_range=p["f_range"], widths=p["widths"],
-                           snr_min=B.SNR_MIN, max_batch=16, device_id=local_rank)
+                           snr_min=B.SNR_MIN, max_batch=16, device_id=local_rank, fold_storage=args.storage)
     d_data = [(torch.from_numpy(e).cuda(), torch.from_numpy(v).cuda()) for e, v in data]
     flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     ms.search(d_data[:1])
@@ -556,7 +557,8 @@ def run_multi(args, rank, world, local_rank):
     if rank == 0:
         print(json.dumps(_line(args, world, "multi_series_512x2^18..2^22_nbins128", value, ms_step,
                                dict(cfgd, trials_per_step=trials, candidates=ncand, groups=groups,
-                                    graphs="one CUDA graph per length for full batches"),
+                                    graphs="one CUDA graph per length for full batches",
+                                    fold_storage=args.storage),
                                cpu_baseline=cpu, e2e=e2e, clocks=clk)))
     _finish(dist)
     return 0

@@ -147,7 +147,14 @@ int lk_plan_resolve_coords(const lk_plan* plan, void* d_coords, uint64_t n_coord
 
 /* ---- FFA executor (replaces FFACUDA<float>) ---------------------------- */
 /* Builds the device tables (coordinates, brute-fold run tables) and scratch
- * for `plan` on `device`. storage: lk_dtype of intermediate levels. */
+ * for `plan` on `device`. storage: lk_dtype of intermediate levels.
+ * LK_FP32: every level FP32 (the reference's FFACUDA<float>).
+ * LK_BF16: levels 1 .. L-2 stored as BF16, every add FP32; level 0 stays
+ *   FP32. Folds and scores then carry BF16 rounding error; lk_ffa_search
+ *   rescores every final cell within a margin of snr_min exactly (from the
+ *   FP32 level 0, same add tree) so its candidate set and S/N values are the
+ *   LK_FP32 ones. At most 8192 level-0 segments.
+ * LK_FP16: rejected (LK_ERR_UNSUPPORTED): V rows outgrow FP16's range. */
 int lk_ffa_create(const lk_plan* plan, int device, int storage, lk_ffa** out);
 void lk_ffa_destroy(lk_ffa* ffa);
 /* Device bytes owned by the executor. */
@@ -192,6 +199,16 @@ int lk_ffa_search_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, u
  * (0 = no bounded wait gave up). */
 int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status);
 
+/* LK_BF16 search margin (no reference counterpart): a search rescores every
+ * final cell whose approximate best S/N is >= (snr_min - margin_abs) /
+ * (1 + margin_rel). Defaults follow from the level count (12 standard
+ * deviations of the BF16 rounding error plus a bound for the V rows). Both
+ * must be finite and >= 0; calls on an LK_FP32 executor are no-ops. */
+int lk_ffa_set_rescore_margin(lk_ffa* ffa, float margin_abs, float margin_rel);
+int lk_ffa_get_rescore_margin(const lk_ffa* ffa, float* margin_abs, float* margin_rel);
+/* Synchronises the stream; final cells the last LK_BF16 search rescored. */
+int lk_ffa_rescored_cells(lk_ffa* ffa, lk_stream_t stream, uint64_t* n_cells);
+
 /* Per-stage timing with CUDA events recorded on the launching stream
  * (no reference counterpart; used by benchmarks). When enabled, every
  * execute/scores/search call records one event pair per kernel stage. */
@@ -200,7 +217,8 @@ enum lk_stage_kind {
     LK_STAGE_BRUTE_FOLD = 1,
     LK_STAGE_MERGE = 2,
     LK_STAGE_MERGE_SCORE = 3,
-    LK_STAGE_COMPACT = 4
+    LK_STAGE_COMPACT = 4,
+    LK_STAGE_RESCORE = 5  /* LK_BF16 search: exact rescoring of near-threshold cells */
 };
 typedef struct lk_stage_time {
     int32_t kind;       /* lk_stage_kind */

@@ -94,7 +94,7 @@ class LkPlanInfo(ctypes.Structure):
     ]
 
 
-STAGE_NAMES = {0: "transpose", 1: "brute_fold", 2: "merge", 3: "merge_score", 4: "compact"}
+STAGE_NAMES = {0: "transpose", 1: "brute_fold", 2: "merge", 3: "merge_score", 4: "compact", 5: "rescore"}
 
 
 class LkStageTime(ctypes.Structure):
@@ -138,6 +138,9 @@ SIGNATURES = [
     ("lk_ffa_scores_batch", i32, [vp, vp, vp, u64, vp, u64, vp]),
     ("lk_ffa_search_batch", i32, [vp, vp, vp, u64, f32, vp, vp, u64, vp, vp]),
     ("lk_ffa_status", i32, [vp, vp, vp]),
+    ("lk_ffa_set_rescore_margin", i32, [vp, ctypes.c_float, ctypes.c_float]),
+    ("lk_ffa_get_rescore_margin", i32, [vp, vp, vp]),
+    ("lk_ffa_rescored_cells", i32, [vp, vp, vp]),
     ("lk_ffa_set_profiling", i32, [vp, i32]),
     ("lk_ffa_get_profile", i32, [vp, vp, vp, u32, vp]),
     ("lk_brute_fold_create", i32, [vp, u64, u64, u64, u64, f64, f64, i32, vp]),

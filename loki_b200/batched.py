@@ -30,12 +30,13 @@ def _pow2_ceil(n: int) -> int:
 class _Group:
     """Executor, static buffers and captured graph for one padded length."""
 
-    def __init__(self, cfg: PulsarSearchConfig, nbatch: int, device: int, use_graph: bool, cap: int):
+    def __init__(self, cfg: PulsarSearchConfig, nbatch: int, device: int, use_graph: bool, cap: int,
+                 fold_storage: str = "fp32"):
         t = D.torch()
         dev = f"cuda:{device}"
         self.cfg = cfg
         self.nbatch = nbatch
-        self.ffa = FFACUDA(cfg, device_id=device, max_batch=nbatch)
+        self.ffa = FFACUDA(cfg, device_id=device, max_batch=nbatch, fold_storage=fold_storage)
         self.per = int(self.ffa.plan.ncoords[-1]) * cfg.n_scoring_widths
         n = cfg.nsamps
         self.e = t.zeros((nbatch, n), dtype=t.float32, device=dev)
@@ -64,11 +65,14 @@ class _Group:
 
 class MultiSeriesSearch:
     """FFA period search of many series (``tsamp``, ``nbins``, frequency range
-    ``f_range``, boxcar ``widths``, threshold ``snr_min``) on one device."""
+    ``f_range``, boxcar ``widths``, threshold ``snr_min``) on one device.
+    ``fold_storage="bf16"`` stores the intermediate levels in BF16 and
+    rescores near-threshold cells exactly (same candidates as FP32)."""
 
     def __init__(self, tsamp: float, nbins: int, f_range, widths, snr_min: float, max_batch: int = 8,
                  eta: float = 1.0, device_id: int = 0, use_graphs: bool = True, max_cands: int = 1 << 22,
-                 mem_fraction: float = 0.25):
+                 mem_fraction: float = 0.25, fold_storage: str = "fp32"):
+        self.fold_storage = fold_storage
         D.require_cuda(device_id)
         self.tsamp, self.nbins, self.eta = float(tsamp), int(nbins), float(eta)
         self.f_range = (float(f_range[0]), float(f_range[1]))
@@ -88,12 +92,15 @@ class MultiSeriesSearch:
     def _group(self, L: int) -> _Group:
         if L not in self.groups:
             cfg = self.config(L)
-            probe = FFACUDA(cfg, device_id=self.device, max_batch=1)
+            probe = FFACUDA(cfg, device_id=self.device, max_batch=1, fold_storage=self.fold_storage)
             per_series = probe.workspace_bytes + 8 * L + 4 * int(probe.plan.ncoords[-1]) * cfg.n_scoring_widths
+            if self.fold_storage == "bf16":
+                # per-cell best S/N, cell list and its values
+                per_series += 12 * int(probe.plan.ncoords[-1])
             del probe
             free, _ = D.torch().cuda.mem_get_info(self.device)
             nb = int(max(1, min(self.max_batch, (self.mem_fraction * free) // max(per_series, 1))))
-            self.groups[L] = _Group(cfg, nb, self.device, self.use_graphs, self.max_cands)
+            self.groups[L] = _Group(cfg, nb, self.device, self.use_graphs, self.max_cands, self.fold_storage)
         return self.groups[L]
 
     def search(self, data) -> list[dict]:

@@ -1,5 +1,6 @@
 // The C ABI (include/loki_b200.h): argument checks, exception-to-status
 // translation and the thread-local error message. No CUDA kernels here.
+#include <cmath>
 #include <algorithm>
 #include <cstring>
 #include <exception>
@@ -278,6 +279,37 @@ int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status) {
         need(ffa, "ffa");
         need(status, "status");
         *status = ffa->exec->read_status(reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_ffa_set_rescore_margin(lk_ffa* ffa, float margin_abs, float margin_rel) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        lk::require(std::isfinite(margin_abs) && std::isfinite(margin_rel) && margin_abs >= 0.0f &&
+                        margin_rel >= 0.0f,
+                    "rescore margins must be finite and >= 0");
+        if (ffa->exec->mixed) {
+            ffa->exec->margin_abs = margin_abs;
+            ffa->exec->margin_rel = margin_rel;
+        }
+    });
+}
+
+int lk_ffa_get_rescore_margin(const lk_ffa* ffa, float* margin_abs, float* margin_rel) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(margin_abs, "margin_abs");
+        need(margin_rel, "margin_rel");
+        *margin_abs = ffa->exec->margin_abs;
+        *margin_rel = ffa->exec->margin_rel;
+    });
+}
+
+int lk_ffa_rescored_cells(lk_ffa* ffa, lk_stream_t stream, uint64_t* n_cells) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(n_cells, "n_cells");
+        *n_cells = ffa->exec->rescored_cells(reinterpret_cast<cudaStream_t>(stream));
     });
 }
 

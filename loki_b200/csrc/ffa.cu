@@ -6,6 +6,7 @@
 // only), no stream synchronisation happens between levels, and the scores
 // entry point fuses the final merge level with the boxcar scorer.
 #include <algorithm>
+#include <cmath>
 #include <memory>
 
 #include "lk_ffa.hpp"
@@ -49,7 +50,15 @@ StageProfiler::~StageProfiler() {
 FFAExec::FFAExec(const Plan& p, int device, int storage, uint64_t max_batch_)
     : plan(p), device(device), max_batch(max_batch_) {
     require(max_batch >= 1 && max_batch <= 65535, "max_batch must lie in [1, 65535]");
-    require(storage == LK_FP32, "only FP32 fold storage is implemented by this executor");
+    require(storage == LK_FP32 || storage == LK_BF16 || storage == LK_FP16,
+            "fold storage must be LK_FP32, LK_BF16 or LK_FP16");
+    if (storage == LK_FP16) {
+        // Level L-2 holds sums of nsamps / 2 samples per bin: its V row
+        // exceeds FP16's largest finite value (65504) once nsamps / nbins
+        // passes about 2^17, so FP16 without a per-level scale is unsafe.
+        fail(LK_ERR_UNSUPPORTED, "FP16 fold storage is not implemented (use LK_BF16)");
+    }
+    mixed = storage == LK_BF16;
     require(plan.nparams <= 3, "the FFA executor supports nparams <= 3");
     require(plan.n_levels >= 2, "FFA::execute_unified: levels must be greater than or equal to 2");
     require(plan.cfg.nbins <= 0xffffffffULL, "nbins too large");
@@ -66,19 +75,58 @@ FFAExec::FFAExec(const Plan& p, int device, int storage, uint64_t max_batch_)
     bf = std::make_unique<BruteFoldDevice>(plan.param_grid(0, np - 1), plan.segment_lens[0],
                                            plan.cfg.nbins, plan.cfg.nsamps, plan.cfg.tsamp,
                                            plan.t_ref0(), status.as<uint32_t>());
-    uint64_t inter = 0;  // largest level that is not the final one
-    for (uint32_t l = 0; l + 1 < plan.n_levels; ++l) {
-        inter = std::max(inter, plan.fold_size(l));
+    if (!mixed) {
+        uint64_t inter = 0;  // largest level that is not the final one
+        for (uint32_t l = 0; l + 1 < plan.n_levels; ++l) {
+            inter = std::max(inter, plan.fold_size(l));
+        }
+        buf[0].alloc(sizeof(float) * inter * max_batch);
+        buf[1].alloc(sizeof(float) * inter * max_batch);
+    } else {
+        const uint32_t L = plan.n_levels;
+        require(L <= kRescoreMaxLevels && plan.nsegments[0] <= kRescoreMaxLeaves,
+                "BF16 storage supports at most 8192 level-0 segments");
+        uint64_t inter = 1;  // largest BF16 level (1 .. L-2)
+        for (uint32_t l = 1; l + 1 < L; ++l) {
+            inter = std::max(inter, plan.fold_size(l));
+        }
+        fold0.alloc(sizeof(float) * plan.fold_size(0) * max_batch);
+        buf[0].alloc(2 * inter * max_batch);  // BF16
+        buf[1].alloc(2 * inter * max_batch);
+        rtree.n_levels = L;
+        rtree.nbins = static_cast<uint32_t>(plan.cfg.nbins);
+        rtree.ncoords0 = plan.ncoords[0];
+        rtree.ncoords_final = plan.ncoords[L - 1];
+        rtree.fold0_size = plan.fold_size(0);
+        for (uint32_t l = 1; l < L; ++l) {
+            rtree.level_coords[l] = level_coords(l);
+        }
+        // Rounding model: each BF16 store moves a value by at most 2^-8 of
+        // its magnitude (round to nearest, 8-bit significand), uniformly
+        // distributed. Noise-dominated bins: the L-2 stored levels add
+        // independent errors whose S/N effect has RMS 2^-8 sqrt((L-2)/3);
+        // signal-dominated bins: RMS 2^-8 / sqrt(3) of the S/N. The V rows
+        // are positive, so their relative error is at most (L-2) 2^-8, and
+        // S/N depends on V through 1/sqrt(V). The margin takes 12 standard
+        // deviations of the random parts plus the V bound.
+        const double u = std::ldexp(1.0, -8);
+        const double nst = static_cast<double>(L >= 2 ? L - 2 : 0);
+        margin_abs = static_cast<float>(12.0 * u * std::sqrt(nst / 3.0));
+        margin_rel = static_cast<float>(0.5 * nst * u + (nst > 0 ? 12.0 * u / std::sqrt(3.0) : 0.0));
     }
-    buf[0].alloc(sizeof(float) * inter * max_batch);
-    buf[1].alloc(sizeof(float) * inter * max_batch);
     sp = make_score_params(plan.widths.data(), static_cast<uint32_t>(plan.widths.size()),
                            static_cast<uint32_t>(plan.cfg.nbins));
 }
 
 uint64_t FFAExec::device_bytes() const {
-    return status.bytes + coords.bytes + buf[0].bytes + buf[1].bytes + bf->device_bytes() +
-           scores_tmp.bytes + compact_scratch.bytes;
+    return status.bytes + coords.bytes + buf[0].bytes + buf[1].bytes + fold0.bytes +
+           bf->device_bytes() + scores_tmp.bytes + compact_scratch.bytes + cmax.bytes +
+           cells.bytes + cell_vals.bytes + cell_count.bytes + cell_scratch.bytes;
+}
+
+float FFAExec::rescore_threshold(float snr_min) const {
+    const float lo = (snr_min - margin_abs) / (1.0f + margin_rel);
+    return std::nextafter(lo, -INFINITY);
 }
 
 const void* FFAExec::level_coords(uint32_t l) const {
@@ -91,12 +139,19 @@ uint64_t FFAExec::coord_bytes(uint32_t l) const {
     return plan.ncoords[l] * (plan.nparams == 1 ? 8 : 16);
 }
 
-float* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t last,
-                           float* final_out, cudaStream_t s, uint64_t nbatch) {
+const void* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t last,
+                               float* final_out, cudaStream_t s, uint64_t nbatch,
+                               bool* last_bf16) {
     require(nbatch >= 1 && nbatch <= max_batch, "nbatch must lie in [1, max_batch]");
     const bool taylor = plan.nparams > 1;
     const auto nbins = static_cast<uint32_t>(plan.cfg.nbins);
-    float* in = (last == 0 && final_out != nullptr) ? final_out : buf[0].as<float>();
+    // Level l is BF16 when the storage is mixed, l >= 1, and it is not the
+    // caller's FP32 output.
+    auto is_bf16 = [&](uint32_t l) { return mixed && l >= 1 && !(l == last && final_out); };
+    auto elem = [&](uint32_t l) -> uint64_t { return is_bf16(l) ? 2 : 4; };
+    void* in = (last == 0 && final_out != nullptr) ? final_out
+               : mixed                             ? fold0.ptr
+                                                   : buf[0].ptr;
     // Algorithmic bytes: the series in (E and V) and the level-0 fold out;
     // each merge level reads the previous level and writes its own. A batch of
     // series is, level by level, one series with nbatch times the segments
@@ -104,18 +159,22 @@ float* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t last,
     const uint64_t series_bytes = 8 * plan.cfg.nsamps * nbatch;
     bf->bind_inputs(ts_e, ts_v, s, nbatch);
     prof.begin(LK_STAGE_BRUTE_FOLD, 0, 1, series_bytes + 4 * plan.fold_size(0) * nbatch, s);
-    bf->fold(in, s);
+    bf->fold(static_cast<float*>(in), s);
     prof.end(s);
     for (uint32_t l = 1; l <= last; ++l) {
-        float* out = (l == last && final_out != nullptr) ? final_out : buf[l % 2].as<float>();
+        void* out = (l == last && final_out != nullptr) ? final_out : buf[l % 2].ptr;
         prof.begin(LK_STAGE_MERGE, static_cast<int>(l), 1,
-                   nbatch * (4 * (plan.fold_size(l - 1) + plan.fold_size(l))) + coord_bytes(l), s);
+                   nbatch * (elem(l - 1) * plan.fold_size(l - 1) + elem(l) * plan.fold_size(l)) +
+                       coord_bytes(l),
+                   s);
         const uint64_t n_inner = plan.param_counts[l][plan.nparams - 1];
         merge_level(in, out, level_coords(l), taylor, n_inner, plan.ncoords[l] / n_inner,
-                    plan.ncoords[l - 1], plan.nsegments[l] * nbatch, nbins, s);
+                    plan.ncoords[l - 1], plan.nsegments[l] * nbatch, nbins, s, is_bf16(l - 1),
+                    is_bf16(l));
         prof.end(s);
         in = out;
     }
+    *last_bf16 = is_bf16(last);
     return in;
 }
 
@@ -125,7 +184,8 @@ void FFAExec::execute(const float* ts_e, const float* ts_v, float* fold, uint64_
     require(fold_len >= plan.fold_size(L - 1) * nbatch, "fold must hold fold_size floats");
     DeviceGuard g(device);
     prof.reset();
-    run_levels(ts_e, ts_v, L - 1, fold, s, nbatch);
+    bool bf16 = false;
+    run_levels(ts_e, ts_v, L - 1, fold, s, nbatch, &bf16);
 }
 
 void FFAExec::scores(const float* ts_e, const float* ts_v, float* d_scores, uint64_t len,
@@ -135,18 +195,25 @@ void FFAExec::scores(const float* ts_e, const float* ts_v, float* d_scores, uint
     require(len >= plan.ncoords[L - 1] * plan.widths.size() * nbatch,
             "scores must hold ncoords * n_widths floats");
     DeviceGuard g(device);
-    if (!in_search) {
-        prof.reset();
-    }
-    const float* in = run_levels(ts_e, ts_v, L - 2, nullptr, s, nbatch);
+    prof.reset();
+    scores_impl(ts_e, ts_v, d_scores, nullptr, s, nbatch);
+}
+
+void FFAExec::scores_impl(const float* ts_e, const float* ts_v, float* d_scores, float* d_cmax,
+                          cudaStream_t s, uint64_t nbatch) {
+    const uint32_t L = plan.n_levels;
+    bool in_bf16 = false;
+    const void* in = run_levels(ts_e, ts_v, L - 2, nullptr, s, nbatch, &in_bf16);
     const uint64_t nscores = plan.ncoords[L - 1] * plan.widths.size();
     prof.begin(LK_STAGE_MERGE_SCORE, static_cast<int>(L - 1), 1,
-               nbatch * (4 * plan.fold_size(L - 2) + 4 * nscores) + coord_bytes(L - 1), s);
+               nbatch * ((in_bf16 ? 2 : 4) * plan.fold_size(L - 2) + 4 * nscores) +
+                   coord_bytes(L - 1),
+               s);
     const uint64_t n_inner = plan.param_counts[L - 1][plan.nparams - 1];
     merge_score_level(in, level_coords(L - 1), plan.nparams > 1, n_inner,
                       plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
                       static_cast<uint32_t>(plan.cfg.nbins), sp, LK_SCORE_PER_WIDTH, d_scores, s,
-                      nbatch);
+                      nbatch, in_bf16, d_cmax);
     prof.end(s);
 }
 
@@ -154,25 +221,51 @@ void FFAExec::search(const float* ts_e, const float* ts_v, float snr_min, uint32
                      float* d_snr, uint64_t max_cands, uint64_t* d_count, cudaStream_t s,
                      uint64_t nbatch) {
     const uint32_t L = plan.n_levels;
-    const uint64_t n = plan.ncoords[L - 1] * plan.widths.size() * nbatch;
+    require(plan.nsegments[L - 1] == 1, "compute_ffa_scores: nsegments must be 1 for scores");
+    require(nbatch >= 1 && nbatch <= max_batch, "nbatch must lie in [1, max_batch]");
+    const uint64_t ncells = plan.ncoords[L - 1] * nbatch;
+    const uint64_t n = ncells * plan.widths.size();
     DeviceGuard g(device);
     if (scores_tmp.bytes < n * sizeof(float)) {
         scores_tmp.alloc(n * sizeof(float));
         compact_scratch.alloc(compact_scratch_bytes(n));
     }
-    prof.reset();
-    in_search = true;
-    try {
-        scores(ts_e, ts_v, scores_tmp.as<float>(), n, s, nbatch);
-    } catch (...) {
-        in_search = false;
-        throw;
+    if (mixed && cmax.bytes < ncells * sizeof(float)) {
+        cmax.alloc(ncells * sizeof(float));
+        cells.alloc(ncells * sizeof(uint32_t));
+        cell_vals.alloc(ncells * sizeof(float));
+        cell_count.alloc(sizeof(uint64_t));
+        cell_scratch.alloc(compact_scratch_bytes(ncells));
     }
-    in_search = false;
+    prof.reset();
+    scores_impl(ts_e, ts_v, scores_tmp.as<float>(), mixed ? cmax.as<float>() : nullptr, s, nbatch);
+    if (mixed) {
+        // Cells whose approximate best S/N is near or above snr_min get their
+        // exact FP32 scores; every other cell stays below snr_min.
+        prof.begin(LK_STAGE_COMPACT, static_cast<int>(L - 1), 3, 8 * ncells, s);
+        compact_ge(cmax.as<float>(), ncells, rescore_threshold(snr_min), cells.as<uint32_t>(),
+                   cell_vals.as<float>(), ncells, cell_count.as<uint64_t>(), cell_scratch.ptr, s);
+        prof.end(s);
+        prof.begin(LK_STAGE_RESCORE, -1, 1, 0, s);
+        rescore_cells(fold0.as<float>(), rtree, plan.nparams > 1, sp, cells.as<uint32_t>(),
+                      cell_count.as<uint64_t>(), ncells, scores_tmp.as<float>(), s);
+        prof.end(s);
+    }
     prof.begin(LK_STAGE_COMPACT, -1, 3, 8 * n, s);
     compact_ge(scores_tmp.as<float>(), n, snr_min, d_idx, d_snr, max_cands, d_count,
                compact_scratch.ptr, s);
     prof.end(s);
+}
+
+uint64_t FFAExec::rescored_cells(cudaStream_t s) {
+    if (!mixed || cell_count.ptr == nullptr) {
+        return 0;
+    }
+    DeviceGuard g(device);
+    LK_CUDA(cudaStreamSynchronize(s));
+    uint64_t c = 0;
+    LK_CUDA(cudaMemcpy(&c, cell_count.ptr, sizeof(c), cudaMemcpyDeviceToHost));
+    return c;
 }
 
 std::vector<lk_stage_time> FFAExec::profile(cudaStream_t s) {

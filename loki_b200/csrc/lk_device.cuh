@@ -10,6 +10,7 @@
 #include <cfloat>
 #include <cstdint>
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 namespace lk::dev {
@@ -92,10 +93,24 @@ __device__ __forceinline__ uint32_t shift_bins(float phase, uint32_t nbins) {
 }
 
 // ---- storage conversions ------------------------------------------------
+// Fold storage types: FP32, or BF16 (round to nearest even on store); every
+// arithmetic operation is FP32.
 template <class T> struct Store;
 template <> struct Store<float> {
     __device__ __forceinline__ static float load(const float* p) { return __ldg(p); }
     __device__ __forceinline__ static void store(float* p, float v) { *p = v; }
+    __device__ __forceinline__ static float from_float(float v) { return v; }
+};
+template <> struct Store<__nv_bfloat16> {
+    __device__ __forceinline__ static float load(const __nv_bfloat16* p) {
+        return __bfloat162float(__ldg(p));
+    }
+    __device__ __forceinline__ static void store(__nv_bfloat16* p, float v) {
+        *p = __float2bfloat16_rn(v);
+    }
+    __device__ __forceinline__ static __nv_bfloat16 from_float(float v) {
+        return __float2bfloat16_rn(v);
+    }
 };
 
 }  // namespace lk::dev

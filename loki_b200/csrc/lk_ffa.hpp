@@ -52,11 +52,23 @@ struct FFAExec {
     DeviceBuffer status;   // uint32 device status word
     DeviceBuffer coords;   // all levels, reference layout
     std::unique_ptr<BruteFoldDevice> bf;
-    DeviceBuffer buf[2];   // ping-pong intermediate levels
+    // Intermediate levels. FP32 storage: ping-pong buffers for every level
+    // before the last. BF16 storage: level 0 stays FP32 in fold0 (the exact
+    // rescorer rebuilds final cells from it) and levels 1 .. L-2 alternate
+    // between the two BF16 buffers.
+    DeviceBuffer buf[2];
+    DeviceBuffer fold0;
     DeviceBuffer scores_tmp;
     DeviceBuffer compact_scratch;
+    // BF16 search: per-cell best approximate S/N, the cells to rescore.
+    DeviceBuffer cmax, cells, cell_vals, cell_count, cell_scratch;
     ScoreParams sp{};
-    bool in_search = false;
+    bool mixed = false;  // BF16 storage of levels 1 .. L-2
+    // A BF16 search rescores every final cell whose approximate best S/N is
+    // at least (snr_min - margin_abs) / (1 + margin_rel).
+    float margin_abs = 0.0f;
+    float margin_rel = 0.0f;
+    RescoreTree rtree{};
 
     uint64_t max_batch = 1;  // series per call (buffers are sized for it)
 
@@ -65,10 +77,16 @@ struct FFAExec {
     const void* level_coords(uint32_t l) const;
     uint64_t coord_bytes(uint32_t l) const;
     std::vector<lk_stage_time> profile(cudaStream_t s);
+    // Lowest approximate best S/N that a BF16 search rescores for snr_min.
+    float rescore_threshold(float snr_min) const;
     // All entry points take nbatch series of nsamps samples stored back to
     // back; outputs are the single-series outputs of each, back to back.
-    float* run_levels(const float* ts_e, const float* ts_v, uint32_t last, float* final_out,
-                      cudaStream_t s, uint64_t nbatch = 1);
+    // run_levels runs levels 0 .. last (inclusive) and returns the buffer
+    // holding `last` (BF16 when *last_bf16 is set).
+    const void* run_levels(const float* ts_e, const float* ts_v, uint32_t last, float* final_out,
+                           cudaStream_t s, uint64_t nbatch, bool* last_bf16);
+    void scores_impl(const float* ts_e, const float* ts_v, float* d_scores, float* d_cmax,
+                     cudaStream_t s, uint64_t nbatch);
     void execute(const float* ts_e, const float* ts_v, float* fold, uint64_t fold_len,
                  cudaStream_t s, uint64_t nbatch = 1);
     void scores(const float* ts_e, const float* ts_v, float* d_scores, uint64_t len,
@@ -77,6 +95,8 @@ struct FFAExec {
                 float* d_snr, uint64_t max_cands, uint64_t* d_count, cudaStream_t s,
                 uint64_t nbatch = 1);
     uint32_t read_status(cudaStream_t s);
+    // Cells the last BF16 search rescored (synchronises s).
+    uint64_t rescored_cells(cudaStream_t s);
 };
 
 }  // namespace lk

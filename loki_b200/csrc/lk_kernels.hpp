@@ -89,9 +89,10 @@ private:
 
 // One merge level: out[s, c] = rot(in[2s, tail(c)], st(c)) + rot(in[2s+1, head(c)], sh(c)).
 // Coordinates are [n_outer][n_inner] (n_inner = frequency cells).
-void merge_level(const float* d_in, float* d_out, const void* d_coords, bool taylor,
+// Storage of input / output: FP32, or BF16 when the flag is set (adds are FP32).
+void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylor,
                  uint64_t n_inner, uint64_t n_outer, uint64_t ncoords_prev, uint64_t nsegments,
-                 uint32_t nbins, cudaStream_t s);
+                 uint32_t nbins, cudaStream_t s, bool in_bf16 = false, bool out_bf16 = false);
 
 // Boxcar scoring parameters shared by the score kernels.
 struct ScoreParams {
@@ -106,10 +107,32 @@ ScoreParams make_score_params(const uint32_t* widths, uint32_t nwidths, uint32_t
 // Final merge level fused with scoring (one output segment per series;
 // nbatch series, the input holding 2 * nbatch segments of ncoords_prev cells,
 // scores [nbatch][ncoords][nout]).
-void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
+void merge_score_level(const void* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
                        uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                        const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s,
-                       uint64_t nbatch = 1);
+                       uint64_t nbatch = 1, bool in_bf16 = false, float* d_cmax = nullptr);
+
+// Merge tree of the final FFA level: what the exact rescorer needs to rebuild
+// one final cell from the FP32 level-0 fold.
+constexpr uint32_t kRescoreMaxLevels = 24;
+constexpr uint64_t kRescoreMaxLeaves = 8192;  // level-0 segments (2^(levels-1))
+struct RescoreTree {
+    uint32_t n_levels = 0;
+    uint32_t nbins = 0;
+    uint64_t ncoords0 = 0;       // rows per level-0 segment
+    uint64_t ncoords_final = 0;  // final cells per series
+    uint64_t fold0_size = 0;     // floats of one series' level-0 fold
+    const void* level_coords[kRescoreMaxLevels] = {};  // device table of level l (l >= 1)
+};
+
+// For each of the *d_count final cells listed in d_cells (flat series *
+// ncoords_final + coord, at most max_cells of them), rebuilds the FP32 fold
+// of that cell from d_fold0 with the merge kernels' exact add tree and writes
+// its per-width S/N to d_scores[cell * nwidths ...]: bit-identical to the
+// all-FP32 path.
+void rescore_cells(const float* d_fold0, const RescoreTree& t, bool taylor, const ScoreParams& sp,
+                   const uint32_t* d_cells, const uint64_t* d_count, uint64_t max_cells,
+                   float* d_scores, cudaStream_t s);
 
 // Standalone scoring of [nprof, 2, nbins] (is3d) or [nprof, nbins] folds.
 void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d,

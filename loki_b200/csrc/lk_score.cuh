@@ -21,12 +21,13 @@ __device__ __forceinline__ float normalise(float e, float v) {
     return __fmul_rn(e, __frcp_rn(__fsqrt_rn(v)));
 }
 
-// Scores the normalised profile staged at r (in place). NW >= sp.nwidths is
-// the compile-time width capacity (8, 16 or 32): the width loops are
-// unrolled to NW, so a small NW avoids evaluating unused width slots.
+// Scores the normalised profile staged at r (in place) and returns the
+// largest S/N over the widths. NW >= sp.nwidths is the compile-time width
+// capacity (8, 16 or 32): the width loops are unrolled to NW, so a small NW
+// avoids evaluating unused width slots.
 template <int NW>
-__device__ __forceinline__ void score_row(float* r, uint32_t nbins, float inv_stdnoise,
-                                          const ScoreParams& sp, int mode, float* out) {
+__device__ __forceinline__ float score_row(float* r, uint32_t nbins, float inv_stdnoise,
+                                           const ScoreParams& sp, int mode, float* out) {
     float acc = r[0];
     for (uint32_t j = 1; j < nbins; ++j) {
         acc = __fadd_rn(acc, r[j]);
@@ -59,14 +60,14 @@ __device__ __forceinline__ void score_row(float* r, uint32_t nbins, float inv_st
             const float snr = __fmul_rn(base, inv_stdnoise);
             if (mode == LK_SCORE_PER_WIDTH) {
                 out[iw] = snr;
-            } else {
-                best = (best < snr) ? snr : best;
             }
+            best = (best < snr) ? snr : best;
         }
     }
     if (mode == LK_SCORE_MAX) {
         out[0] = best;
     }
+    return best;
 }
 
 // Largest S/N of the (raw, 2-D) profile staged at r with every width's S/N

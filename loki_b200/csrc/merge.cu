@@ -30,9 +30,10 @@ constexpr int kWarp = 32;
 constexpr int kThreads = 256;
 constexpr uint32_t kCoordsPerBlock = 64;
 
-template <bool TAYLOR>
+// TIn / TOut: float or __nv_bfloat16 storage; every add is FP32.
+template <bool TAYLOR, class TIn, class TOut>
 __global__ void __launch_bounds__(kThreads)
-    merge_kernel(const float* __restrict__ in, float* __restrict__ out,
+    merge_kernel(const TIn* __restrict__ in, TOut* __restrict__ out,
                  const void* __restrict__ coords, uint32_t n_inner, uint32_t n_outer,
                  uint64_t nprev, uint32_t nbins) {
     const uint32_t tiles = (n_inner + kCoordsPerBlock - 1) / kCoordsPerBlock;
@@ -48,24 +49,25 @@ __global__ void __launch_bounds__(kThreads)
     for (uint32_t jf = j0 + warp; jf < j1; jf += kThreads / kWarp) {
         const uint64_t c = static_cast<uint64_t>(outer) * n_inner + jf;
         const MergeCoord mc = load_merge_coord<TAYLOR>(coords, c, nbins);
-        const float* tail = in + ((2 * s) * nprev + mc.it) * row;
-        const float* head = in + ((2 * s + 1) * nprev + mc.ih) * row;
-        float* o = out + (s * ncur + c) * row;
+        const TIn* tail = in + ((2 * s) * nprev + mc.it) * row;
+        const TIn* head = in + ((2 * s + 1) * nprev + mc.ih) * row;
+        TOut* o = out + (s * ncur + c) * row;
         for (uint32_t e = lane; e < row; e += kWarp) {
             const uint32_t r = e >= nbins ? nbins : 0;
             const uint32_t j = e - r;
             const uint32_t jt = j >= mc.st ? j - mc.st : j + nbins - mc.st;
             const uint32_t jh = j >= mc.sh ? j - mc.sh : j + nbins - mc.sh;
-            o[e] = __fadd_rn(__ldg(tail + r + jt), __ldg(head + r + jh));
+            o[e] = dev::Store<TOut>::from_float(
+                __fadd_rn(dev::Store<TIn>::load(tail + r + jt), dev::Store<TIn>::load(head + r + jh)));
         }
     }
 }
 
 }  // namespace
 
-void merge_level(const float* d_in, float* d_out, const void* d_coords, bool taylor,
+void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylor,
                  uint64_t n_inner, uint64_t n_outer, uint64_t ncoords_prev, uint64_t nsegments,
-                 uint32_t nbins, cudaStream_t s) {
+                 uint32_t nbins, cudaStream_t s, bool in_bf16, bool out_bf16) {
     require(n_inner > 0 && n_outer > 0, "empty merge level");
     const uint64_t tiles = (n_inner + kCoordsPerBlock - 1) / kCoordsPerBlock;
     require(tiles * n_outer <= 0x7fffffffULL && n_inner <= 0xffffffffULL &&
@@ -78,18 +80,31 @@ void merge_level(const float* d_in, float* d_out, const void* d_coords, bool tay
     for (uint64_t s0 = 0; s0 < nsegments; s0 += 65535) {
         const uint64_t ns = std::min<uint64_t>(65535, nsegments - s0);
         dim3 grid(static_cast<unsigned>(tiles * n_outer), static_cast<unsigned>(ns));
-        const float* in = d_in + s0 * 2 * ncoords_prev * row;
-        float* out = d_out + s0 * ncur * row;
-        if (taylor) {
-            merge_kernel<true><<<grid, kThreads, 0, s>>>(in, out, d_coords,
-                                                         static_cast<uint32_t>(n_inner),
-                                                         static_cast<uint32_t>(n_outer),
-                                                         ncoords_prev, nbins);
+        const uint64_t in_off = s0 * 2 * ncoords_prev * row;
+        const uint64_t out_off = s0 * ncur * row;
+        auto launch = [&](auto tin, auto tout) {
+            using TIn = decltype(tin);
+            using TOut = decltype(tout);
+            const TIn* in = static_cast<const TIn*>(d_in) + in_off;
+            TOut* out = static_cast<TOut*>(d_out) + out_off;
+            const auto ni = static_cast<uint32_t>(n_inner);
+            const auto no = static_cast<uint32_t>(n_outer);
+            if (taylor) {
+                merge_kernel<true, TIn, TOut>
+                    <<<grid, kThreads, 0, s>>>(in, out, d_coords, ni, no, ncoords_prev, nbins);
+            } else {
+                merge_kernel<false, TIn, TOut>
+                    <<<grid, kThreads, 0, s>>>(in, out, d_coords, ni, no, ncoords_prev, nbins);
+            }
+        };
+        if (!in_bf16 && !out_bf16) {
+            launch(float{}, float{});
+        } else if (!in_bf16) {
+            launch(float{}, __nv_bfloat16{});
+        } else if (out_bf16) {
+            launch(__nv_bfloat16{}, __nv_bfloat16{});
         } else {
-            merge_kernel<false><<<grid, kThreads, 0, s>>>(in, out, d_coords,
-                                                          static_cast<uint32_t>(n_inner),
-                                                          static_cast<uint32_t>(n_outer),
-                                                          ncoords_prev, nbins);
+            launch(__nv_bfloat16{}, float{});
         }
         LK_CUDA(cudaGetLastError());
     }

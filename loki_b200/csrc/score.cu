@@ -67,16 +67,19 @@ __global__ void score_kernel(const float* __restrict__ folds, uint64_t nprof, ui
 // loads their coordinates with one lane each, then issues every tail/head
 // load of the PB profiles (NJ = ceil(nbins / 32) bins per lane; NJ == 0
 // selects a generic loop for large nbins) before the first add.
-template <bool TAYLOR, int NW, int NJ, int PB>
-__global__ void merge_score_kernel(const float* __restrict__ in, const void* __restrict__ coords,
+template <bool TAYLOR, int NW, int NJ, int PB, class TIn>
+__global__ void merge_score_kernel(const TIn* __restrict__ in, const void* __restrict__ coords,
                                    uint32_t n_inner, uint32_t n_outer, uint64_t nprev,
                                    uint32_t nbins, uint32_t rs, ScoreParams sp, int mode,
-                                   float* __restrict__ scores) {
+                                   float* __restrict__ scores, float* __restrict__ cmax) {
     extern __shared__ float rows[];
     // Series of a batch on grid.y: input segments 2b and 2b + 1, scores b.
     in += static_cast<uint64_t>(blockIdx.y) * 2 * nprev * 2 * nbins;
     scores += static_cast<uint64_t>(blockIdx.y) * n_inner * n_outer *
               (mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1);
+    if (cmax != nullptr) {
+        cmax += static_cast<uint64_t>(blockIdx.y) * n_inner * n_outer;
+    }
     const uint32_t T = blockDim.x;
     const uint32_t tile = blockIdx.x / n_outer;
     const uint32_t outer = blockIdx.x - tile * n_outer;
@@ -85,19 +88,21 @@ __global__ void merge_score_kernel(const float* __restrict__ in, const void* __r
     const uint64_t c0 = static_cast<uint64_t>(outer) * n_inner + j0;
     const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
     const uint32_t plen = 2 * nbins;
-    const float* head_base = in + nprev * plen;  // segment 1 of the previous level
+    const TIn* head_base = in + nprev * plen;  // segment 1 of the previous level
     if constexpr (NJ == 0) {
 #pragma unroll 2
         for (uint32_t p = warp; p < nhere; p += T / kWarp) {
             const MergeCoord mc = load_merge_coord<TAYLOR>(coords, c0 + p, nbins);
-            const float* tail = in + static_cast<uint64_t>(mc.it) * plen;
-            const float* head = head_base + static_cast<uint64_t>(mc.ih) * plen;
+            const TIn* tail = in + static_cast<uint64_t>(mc.it) * plen;
+            const TIn* head = head_base + static_cast<uint64_t>(mc.ih) * plen;
             float* dst = rows + static_cast<size_t>(p) * rs;
             for (uint32_t j = lane; j < nbins; j += kWarp) {
                 const uint32_t jt = j >= mc.st ? j - mc.st : j + nbins - mc.st;
                 const uint32_t jh = j >= mc.sh ? j - mc.sh : j + nbins - mc.sh;
-                const float e = __fadd_rn(__ldg(tail + jt), __ldg(head + jh));
-                const float v = __fadd_rn(__ldg(tail + nbins + jt), __ldg(head + nbins + jh));
+                const float e = __fadd_rn(dev::Store<TIn>::load(tail + jt),
+                                          dev::Store<TIn>::load(head + jh));
+                const float v = __fadd_rn(dev::Store<TIn>::load(tail + nbins + jt),
+                                          dev::Store<TIn>::load(head + nbins + jh));
                 dst[j] = normalise(e, v);
             }
         }
@@ -115,8 +120,8 @@ __global__ void merge_score_kernel(const float* __restrict__ in, const void* __r
                 const uint32_t st = __shfl_sync(0xffffffffu, mine.st, q);
                 const uint32_t sh = __shfl_sync(0xffffffffu, mine.sh, q);
                 const bool live = p0 + q < nhere;
-                const float* tail = in + static_cast<uint64_t>(it) * plen;
-                const float* head = head_base + static_cast<uint64_t>(ih) * plen;
+                const TIn* tail = in + static_cast<uint64_t>(it) * plen;
+                const TIn* head = head_base + static_cast<uint64_t>(ih) * plen;
 #pragma unroll
                 for (int u = 0; u < NJ; ++u) {
                     const uint32_t jr = lane + 32u * u;
@@ -124,10 +129,10 @@ __global__ void merge_score_kernel(const float* __restrict__ in, const void* __r
                     const uint32_t j = ok ? jr : 0u;  // keep every address inside the rows
                     const uint32_t jt = j >= st ? j - st : j + nbins - st;
                     const uint32_t jh = j >= sh ? j - sh : j + nbins - sh;
-                    te[q][u] = ok ? __ldg(tail + jt) : 0.0f;
-                    tv[q][u] = ok ? __ldg(tail + nbins + jt) : 1.0f;
-                    he[q][u] = ok ? __ldg(head + jh) : 0.0f;
-                    hv[q][u] = ok ? __ldg(head + nbins + jh) : 1.0f;
+                    te[q][u] = ok ? dev::Store<TIn>::load(tail + jt) : 0.0f;
+                    tv[q][u] = ok ? dev::Store<TIn>::load(tail + nbins + jt) : 1.0f;
+                    he[q][u] = ok ? dev::Store<TIn>::load(head + jh) : 0.0f;
+                    hv[q][u] = ok ? dev::Store<TIn>::load(head + nbins + jh) : 1.0f;
                 }
             }
 #pragma unroll
@@ -150,12 +155,21 @@ __global__ void merge_score_kernel(const float* __restrict__ in, const void* __r
     if (threadIdx.x < nhere) {
         const uint64_t c = c0 + threadIdx.x;
         const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1;
-        score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, 1.0f, sp, mode,
-                      scores + c * nout);
+        const float best = score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins,
+                                         1.0f, sp, mode, scores + c * nout);
+        if (cmax != nullptr) {
+            cmax[c] = best;
+        }
     }
 }
 
 }  // namespace
+
+// First parameter type of a merge_score_kernel instantiation.
+template <class K> struct KernelInput;
+template <class TIn, class... Rest> struct KernelInput<void (*)(const TIn*, Rest...)> {
+    using type = TIn;
+};
 
 ScoreParams make_score_params(const uint32_t* widths, uint32_t nwidths, uint32_t nbins) {
     require(nwidths >= 1 && nwidths <= LK_MAX_WIDTHS, "number of widths must be in [1, 32]");
@@ -203,10 +217,10 @@ void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d
     LK_CUDA(cudaGetLastError());
 }
 
-void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
+void merge_score_level(const void* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
                        uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                        const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s,
-                       uint64_t nbatch) {
+                       uint64_t nbatch, bool in_bf16, float* d_cmax) {
     require(nbatch >= 1 && nbatch <= 65535, "nbatch must lie in [1, 65535]");
     if (n_inner == 0 || n_outer == 0) {
         return;
@@ -222,30 +236,33 @@ void merge_score_level(const float* d_in, const void* d_coords, bool taylor, uin
     const auto no = static_cast<uint32_t>(n_outer);
     auto launch = [&](auto kern) {
         set_smem(kern, smem);
+        using TIn = typename KernelInput<decltype(kern)>::type;
         kern<<<dim3(blocks, static_cast<unsigned>(nbatch)), T, smem, s>>>(
-            d_in, d_coords, ni, no, ncoords_prev, nbins, rs, sp, mode, d_scores);
+            static_cast<const TIn*>(d_in), d_coords, ni, no, ncoords_prev, nbins, rs, sp, mode,
+            d_scores, d_cmax);
     };
     const int nwb = sp.nwidths <= 8 ? 8 : (sp.nwidths <= 16 ? 16 : 32);
     const int nj = nbins <= 32 ? 1 : (nbins <= 64 ? 2 : (nbins <= 128 ? 4 : 0));
     // Dispatch (taylor, width bucket, bins per lane); PB * NJ = 16 loads of
     // each kind in flight per lane.
-    auto pick = [&](auto tg) {
+    auto pick = [&](auto tg, auto tin) {
         constexpr bool TG = decltype(tg)::value;
+        using TI = decltype(tin);
         auto by_nj = [&](auto nwc) {
             constexpr int NWC = decltype(nwc)::value;
-            if (nj == 1) launch(merge_score_kernel<TG, NWC, 1, 16>);
-            else if (nj == 2) launch(merge_score_kernel<TG, NWC, 2, 8>);
-            else if (nj == 4) launch(merge_score_kernel<TG, NWC, 4, 4>);
-            else launch(merge_score_kernel<TG, NWC, 0, 1>);
+            if (nj == 1) launch(merge_score_kernel<TG, NWC, 1, 16, TI>);
+            else if (nj == 2) launch(merge_score_kernel<TG, NWC, 2, 8, TI>);
+            else if (nj == 4) launch(merge_score_kernel<TG, NWC, 4, 4, TI>);
+            else launch(merge_score_kernel<TG, NWC, 0, 1, TI>);
         };
         if (nwb == 8) by_nj(std::integral_constant<int, 8>{});
         else if (nwb == 16) by_nj(std::integral_constant<int, 16>{});
         else by_nj(std::integral_constant<int, 32>{});
     };
     if (taylor) {
-        pick(std::true_type{});
+        in_bf16 ? pick(std::true_type{}, __nv_bfloat16{}) : pick(std::true_type{}, float{});
     } else {
-        pick(std::false_type{});
+        in_bf16 ? pick(std::false_type{}, __nv_bfloat16{}) : pick(std::false_type{}, float{});
     }
     LK_CUDA(cudaGetLastError());
 }

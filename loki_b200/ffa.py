@@ -200,6 +200,23 @@ class FFACUDA:
         C.check(C.lib().lk_ffa_status(self._h, D.stream_ptr(self._device), ctypes.byref(st)))
         return st.value
 
+    @property
+    def rescore_margin(self) -> tuple[float, float]:
+        """BF16 search margin (abs, rel): cells with approximate best S/N >=
+        (snr_min - abs) / (1 + rel) are rescored exactly."""
+        a, r = ctypes.c_float(), ctypes.c_float()
+        C.check(C.lib().lk_ffa_get_rescore_margin(self._h, ctypes.byref(a), ctypes.byref(r)))
+        return float(a.value), float(r.value)
+
+    def set_rescore_margin(self, margin_abs: float, margin_rel: float) -> None:
+        C.check(C.lib().lk_ffa_set_rescore_margin(self._h, float(margin_abs), float(margin_rel)))
+
+    def rescored_cells(self) -> int:
+        """Final cells the last BF16 search rescored exactly."""
+        n = ctypes.c_uint64()
+        C.check(C.lib().lk_ffa_rescored_cells(self._h, D.stream_ptr(self._device), ctypes.byref(n)))
+        return int(n.value)
+
 
 def compute_ffa_time_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int = 0, quiet: bool = False):
     """Final-level time-domain fold and its plan (reference lib/ffa_cuda.cu:609-628)."""
