@@ -24,6 +24,12 @@
 //    ([row][bin][lane] in shared memory, conflict-free), fetches the next
 //    run's bin by warp shuffle and reloads that bin's accumulators. All lanes
 //    follow the same mask, so control flow is uniform.
+//
+// Packed form (both rows per warp, the default for nbins <= 64): the series
+// is first interleaved into (e, v) pairs, so one 16-byte shared-memory load
+// yields two samples' pairs in adjacent registers and each sample is one
+// add.rn.f32x2 (two IEEE round-to-nearest adds, E and V, in one
+// instruction); accumulators are float2 [bin][lane].
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -296,6 +302,214 @@ __global__ void __launch_bounds__(640, 1)
     }
 }
 
+// Two IEEE round-to-nearest FP32 adds (a.x + b.x, a.y + b.y) in one sm_100a
+// instruction; bit-identical to two __fadd_rn.
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
+    uint64_t ra, rb, rd;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(rd));
+    return r;
+}
+
+// Packed form: one frequency and both rows per consumer warp, input tiles of
+// (e, v) pairs. Same pipeline, tables and order of adds as the mask kernel.
+template <class BinT>
+__global__ void __launch_bounds__(640, 1)
+    brute_fold_pk_kernel(const __grid_constant__ CUtensorMap tmap_ev, FoldArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t S = a.stages;
+    unsigned char* ring = smem_raw;
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * kStageBytes);
+    uint64_t* empty = full + S;
+    float2* accs = reinterpret_cast<float2*>(empty + S);
+
+    const int warp = threadIdx.x / kWarp;
+    const int lane = threadIdx.x % kWarp;
+    const int W = static_cast<int>(a.warps);
+    const uint32_t q0 = blockIdx.y * a.warps;
+    const int nconsumers = static_cast<int>(min(a.warps, a.nfreq - q0));
+    const int seg0 = static_cast<int>(blockIdx.x * kWarp);
+
+    if ((ptx::smem_u32(ring) & 1023u) != 0) {
+        if (threadIdx.x == 0) {
+            atomicOr(a.status, dev::kStatusBadTable);
+        }
+        return;
+    }
+    if (threadIdx.x == 0) {
+        ptx::prefetch_tensormap(&tmap_ev);
+        for (uint32_t s = 0; s < S; ++s) {
+            ptx::mbar_init(&full[s], 1);
+            ptx::mbar_init(&empty[s], nconsumers * kWarp);
+        }
+        ptx::fence_barrier_init();
+    }
+    __syncthreads();
+
+    if (warp == W) {
+        // Producer: word k is samples 32k .. 32k+31, i.e. floats 64k ..
+        // 64k+63 of each segment's interleaved row, as two 32-float boxes.
+        if (lane == 0) {
+            uint32_t issued = 0;
+            for (uint32_t k = 0; k < a.nwords; ++k) {
+                const uint32_t s = k % S;
+                if (k >= S &&
+                    !ptx::mbar_wait_bounded(&empty[s], ((k / S) - 1) & 1u, a.status,
+                                            dev::kStatusWaitTimeout | dev::kStatusEmpty)) {
+                    break;
+                }
+                unsigned char* st = ring + static_cast<size_t>(s) * kStageBytes;
+                ptx::mbar_arrive_expect_tx(&full[s], kStageBytes);
+                const int x0 = static_cast<int>(k * 64);
+                ptx::tma_load_2d(st, &tmap_ev, &full[s], x0, seg0);
+                ptx::tma_load_2d(st + kTileBytes, &tmap_ev, &full[s], x0 + 32, seg0);
+                ++issued;
+            }
+            const uint32_t first = issued > S ? issued - S : 0;
+            for (uint32_t k = first; k < issued; ++k) {
+                ptx::mbar_wait_bounded(&full[k % S], (k / S) & 1u, a.status,
+                                       dev::kStatusWaitTimeout | dev::kStatusDrain);
+            }
+        }
+        return;
+    }
+    if (warp >= nconsumers) {
+        return;
+    }
+
+    const uint32_t f = q0 + static_cast<uint32_t>(warp);
+    // [nbins + 1][32 lanes] (E, V) sums; slot nbins absorbs the store before
+    // the first run.
+    float2* A = accs + static_cast<size_t>(warp) * (a.nbins + 1) * kWarp + lane;
+    for (uint32_t b = 0; b <= a.nbins; ++b) {
+        A[b * kWarp] = make_float2(0.0f, 0.0f);
+    }
+    const uint32_t* M = a.masks + static_cast<size_t>(f) * a.nwords;
+    const BinT* B = static_cast<const BinT*>(a.bins) + a.bin_off[f];
+    const uint64_t nr = a.nruns[f];
+
+    uint32_t bin = a.nbins;
+    float2 acc = make_float2(0.0f, 0.0f);
+    uint64_t r = 0;
+    uint64_t rbase = 0;
+    uint32_t binbuf = load_bins(B, nr, 0, lane);
+    uint32_t maskbuf = __ldg(M + min(static_cast<uint32_t>(lane), a.nwords - 1));
+    const uint32_t lrow = static_cast<uint32_t>(lane) * 128u;
+    const uint32_t lsw = static_cast<uint32_t>(lane) & 7u;
+
+    auto start_run = [&](uint32_t& rl) {
+        A[bin * kWarp] = acc;
+        bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
+        ++rl;
+        acc = A[bin * kWarp];
+    };
+
+    uint32_t phase = 0;
+    uint32_t s = 0;
+    for (uint32_t c = 0; c < a.nwords; ++c) {
+        if ((c & 31u) == 0 && c > 0) {
+            maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
+        }
+        const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
+        if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
+            rbase = r;
+            binbuf = load_bins(B, nr, rbase, lane);
+        }
+        if (!ptx::mbar_wait_bounded(&full[s], phase, a.status,
+                                    dev::kStatusWaitTimeout |
+                                        (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull))) {
+            return;
+        }
+        const unsigned char* t0 = ring + static_cast<size_t>(s) * kStageBytes + lrow;
+        float2 x[32];
+#pragma unroll
+        for (uint32_t h = 0; h < 2; ++h) {
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) {
+                const uint32_t o = (j ^ lsw) << 4;
+                const float4 v = *reinterpret_cast<const float4*>(t0 + h * kTileBytes + o);
+                x[16 * h + 2 * j] = make_float2(v.x, v.y);
+                x[16 * h + 2 * j + 1] = make_float2(v.z, v.w);
+            }
+        }
+        ptx::mbar_arrive(&empty[s]);
+        s = (s + 1 == S) ? 0 : s + 1;
+        if (s == 0) {
+            phase ^= 1u;
+        }
+        uint32_t rl = static_cast<uint32_t>(r - rbase);
+#pragma unroll
+        for (int g = 0; g < 8; ++g) {
+            if (((m >> (4 * g)) & 0xfu) == 0) {
+#pragma unroll
+                for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                    acc = add2_rn(acc, x[i]);
+                }
+            } else {
+#pragma unroll
+                for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                    if (m & (1u << i)) {
+                        start_run(rl);
+                    }
+                    acc = add2_rn(acc, x[i]);
+                }
+            }
+        }
+        r = rbase + rl;
+    }
+    A[bin * kWarp] = acc;
+    if (r != nr) {
+        atomicOr(a.status, dev::kStatusBadTable);
+    }
+
+    const uint32_t seg = static_cast<uint32_t>(seg0 + lane);
+    if (seg < a.nseg) {
+        float* out = a.fold + (static_cast<size_t>(seg) * a.nfreq + f) * 2 * a.nbins;
+        if ((a.nbins & 3u) == 0) {
+            for (uint32_t b = 0; b < a.nbins; b += 4) {
+                const float2 p0 = A[b * kWarp], p1 = A[(b + 1) * kWarp];
+                const float2 p2 = A[(b + 2) * kWarp], p3 = A[(b + 3) * kWarp];
+                reinterpret_cast<float4*>(out)[b / 4] = make_float4(p0.x, p1.x, p2.x, p3.x);
+                reinterpret_cast<float4*>(out + a.nbins)[b / 4] =
+                    make_float4(p0.y, p1.y, p2.y, p3.y);
+            }
+        } else {
+            for (uint32_t b = 0; b < a.nbins; ++b) {
+                const float2 p = A[b * kWarp];
+                out[b] = p.x;
+                out[a.nbins + b] = p.y;
+            }
+        }
+    }
+}
+
+// ev[i] = (e[i], v[i]) for i < n.
+__global__ void interleave_kernel(const float* __restrict__ e, const float* __restrict__ v,
+                                  float2* __restrict__ ev, uint64_t n, bool vec4) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (vec4) {
+        const uint64_t n4 = n / 4;
+        for (uint64_t i = t0; i < n4; i += stride) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(e) + i);
+            const float4 b = __ldg(reinterpret_cast<const float4*>(v) + i);
+            float4* o = reinterpret_cast<float4*>(ev) + 2 * i;
+            o[0] = make_float4(a.x, b.x, a.y, b.y);
+            o[1] = make_float4(a.z, b.z, a.w, b.w);
+        }
+        for (uint64_t i = 4 * n4 + t0; i < n; i += stride) {
+            ev[i] = make_float2(__ldg(e + i), __ldg(v + i));
+        }
+    } else {
+        for (uint64_t i = t0; i < n; i += stride) {
+            ev[i] = make_float2(__ldg(e + i), __ldg(v + i));
+        }
+    }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
@@ -319,6 +533,23 @@ void encode_series_map(CUtensorMap* map, const float* base, uint64_t seglen, uin
     cuuint32_t estr[2] = {1, 1};
     const CUresult r = tensor_map_encoder()(
         map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
+        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        fail(LK_ERR_CUDA, "cuTensorMapEncodeTiled failed for the brute-fold input");
+    }
+}
+
+// Interleaved series viewed as [nseg][2 * seglen] floats; box 32 floats
+// (16 samples' pairs) x 32 segments, 128-byte swizzle; reads past a row's end
+// or past nseg are zero.
+void encode_ev_map(CUtensorMap* map, const float2* base, uint64_t seglen, uint64_t nseg) {
+    cuuint64_t dims[2] = {2 * seglen, nseg};
+    cuuint64_t strides[1] = {2 * seglen * sizeof(float)};
+    cuuint32_t box[2] = {32, 32};
+    cuuint32_t estr[2] = {1, 1};
+    const CUresult r = tensor_map_encoder()(
+        map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float2*>(base), dims, strides, box,
         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -462,7 +693,8 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
 }
 
 uint64_t BruteFoldDevice::device_bytes() const {
-    return m_masks.bytes + m_bins.bytes + m_bin_off.bytes + m_nruns.bytes + m_stage.bytes;
+    return m_masks.bytes + m_bins.bytes + m_bin_off.bytes + m_nruns.bytes + m_stage.bytes +
+           m_ev.bytes;
 }
 
 // The TMA maps read the series in place; a base address that is not 16-byte
@@ -473,6 +705,28 @@ void BruteFoldDevice::bind_inputs(const float* d_ts_e, const float* d_ts_v, cuda
                                   uint64_t nbatch) {
     require(nbatch >= 1, "BruteFold: nbatch must be positive");
     const uint64_t n = nbatch * m_nsamps;
+    if (m_rows == 2) {
+        if (m_ev.bytes < n * sizeof(float2)) {
+            m_ev.alloc(n * sizeof(float2));
+        }
+        const bool vec4 = (reinterpret_cast<uintptr_t>(d_ts_e) % 16 == 0) &&
+                          (reinterpret_cast<uintptr_t>(d_ts_v) % 16 == 0);
+        int dev = 0, nsm = 148;
+        LK_CUDA(cudaGetDevice(&dev));
+        LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const uint64_t want = (n / (vec4 ? 4 : 1) + 255) / 256;
+        const auto blocks = static_cast<unsigned>(
+            std::max<uint64_t>(1, std::min<uint64_t>(want, static_cast<uint64_t>(nsm) * 8)));
+        interleave_kernel<<<blocks, 256, 0, s>>>(d_ts_e, d_ts_v, m_ev.as<float2>(), n, vec4);
+        LK_CUDA(cudaGetLastError());
+        if (m_ev.ptr != m_map_ev_ptr || nbatch != m_map_batch) {
+            encode_ev_map(&m_tmap_ev, m_ev.as<float2>(), m_seglen, nbatch * m_nseg);
+            m_map_ev_ptr = m_ev.ptr;
+            m_map_batch = nbatch;
+        }
+        m_map_e_ptr = d_ts_e;  // marks the inputs as bound
+        return;
+    }
     const float* e = d_ts_e;
     const float* v = d_ts_v;
     const bool aligned = (reinterpret_cast<uintptr_t>(e) % 16 == 0) &&
@@ -522,11 +776,16 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
                                      static_cast<int>(m_smem)));
         kern<<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_e, m_tmap_v, a);
     };
-    if (m_wide_bins) {
-        m_rows == 2 ? launch(brute_fold_mask_kernel<uint16_t, 2>)
-                    : launch(brute_fold_mask_kernel<uint16_t, 1>);
+    auto launch_pk = [&](auto kern) {
+        LK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(m_smem)));
+        kern<<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, a);
+    };
+    if (m_rows == 2) {
+        m_wide_bins ? launch_pk(brute_fold_pk_kernel<uint16_t>)
+                    : launch_pk(brute_fold_pk_kernel<uint8_t>);
     } else {
-        m_rows == 2 ? launch(brute_fold_mask_kernel<uint8_t, 2>)
+        m_wide_bins ? launch(brute_fold_mask_kernel<uint16_t, 1>)
                     : launch(brute_fold_mask_kernel<uint8_t, 1>);
     }
     LK_CUDA(cudaGetLastError());

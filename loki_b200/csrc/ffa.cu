@@ -157,7 +157,14 @@ const void* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t l
     // series is, level by level, one series with nbatch times the segments
     // (merges pair segments 2s and 2s + 1, never across two series).
     const uint64_t series_bytes = 8 * plan.cfg.nsamps * nbatch;
-    bf->bind_inputs(ts_e, ts_v, s, nbatch);
+    if (bf->interleaves()) {
+        // (e, v) pairs for the packed brute fold: series in, pairs out
+        prof.begin(LK_STAGE_TRANSPOSE, 0, 1, 2 * series_bytes, s);
+        bf->bind_inputs(ts_e, ts_v, s, nbatch);
+        prof.end(s);
+    } else {
+        bf->bind_inputs(ts_e, ts_v, s, nbatch);
+    }
     prof.begin(LK_STAGE_BRUTE_FOLD, 0, 1, series_bytes + 4 * plan.fold_size(0) * nbatch, s);
     bf->fold(static_cast<float*>(in), s);
     prof.end(s);

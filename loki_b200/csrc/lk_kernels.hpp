@@ -56,11 +56,15 @@ public:
         fold(d_fold, s);
     }
     // Points the input tensor maps at the series, or at nbatch series of
-    // nsamps samples stored back to back (host work; a misaligned series is
-    // first copied into an aligned buffer on `s`). fold() then folds all of
-    // them: d_fold holds nbatch * fold_size() floats.
+    // nsamps samples stored back to back. fold() then folds all of them:
+    // d_fold holds nbatch * fold_size() floats. With both rows per warp the
+    // series are first interleaved into (e, v) pairs on `s` (one kernel);
+    // otherwise the maps read them in place (a misaligned series is first
+    // copied into an aligned buffer on `s`).
     void bind_inputs(const float* d_ts_e, const float* d_ts_v, cudaStream_t s,
                      uint64_t nbatch = 1);
+    // True when bind_inputs launches the interleave kernel.
+    bool interleaves() const { return m_rows == 2; }
     void fold(float* d_fold, cudaStream_t s);
     uint64_t nseg() const { return m_nseg; }
     uint64_t nfreq() const { return m_nfreq; }
@@ -81,7 +85,10 @@ private:
     DeviceBuffer m_bin_off;    // uint64 first run of each frequency
     DeviceBuffer m_nruns;      // uint64 runs of each frequency
     DeviceBuffer m_stage;      // aligned copy of a misaligned series
+    DeviceBuffer m_ev;         // (e, v) interleaved series (both rows per warp)
     CUtensorMap m_tmap_e{}, m_tmap_v{};
+    CUtensorMap m_tmap_ev{};
+    const void* m_map_ev_ptr = nullptr;
     const float* m_map_e_ptr = nullptr;
     const float* m_map_v_ptr = nullptr;
     uint64_t m_map_batch = 1;

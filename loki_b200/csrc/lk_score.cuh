@@ -6,6 +6,7 @@
 
 #include <cfloat>
 #include <cstdint>
+#include <type_traits>
 
 #include "lk_internal.hpp"
 #include "lk_kernels.hpp"
@@ -110,6 +111,135 @@ __device__ __forceinline__ float max_snr_div(float* r, uint32_t nbins, float std
         }
     }
     return best;
+}
+
+// ---- compile-time nbins ------------------------------------------------
+// The same operations as score_row / max_snr_div (sequential prefix sum,
+// circular extension, window differences, maxima), with nbins a template
+// constant so every loop over bins unrolls and each shared-memory access is
+// one load with an immediate offset. Width slots at or beyond sp.nwidths
+// repeat width 0 and are ignored, so no slot needs a predicate.
+
+template <int NB, int NW>
+__device__ __forceinline__ float prefix_dmax_nb(float* r, const ScoreParams& sp, float (&dm)[NW]) {
+    float acc = r[0];
+#pragma unroll
+    for (int j = 1; j < NB; ++j) {
+        acc = __fadd_rn(acc, r[j]);
+        r[j] = acc;
+    }
+    const float sum = acc;
+    for (uint32_t k = 0; k < sp.wmax; ++k) {
+        r[NB + k] = __fadd_rn(r[k], sum);
+    }
+    const float* base[NW];
+#pragma unroll
+    for (int iw = 0; iw < NW; ++iw) {
+        base[iw] = r + (iw < static_cast<int>(sp.nwidths) ? sp.widths[iw] : sp.widths[0]);
+        dm[iw] = -FLT_MAX;
+    }
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        const float ri = r[i];
+#pragma unroll
+        for (int iw = 0; iw < NW; ++iw) {
+            const float d = __fsub_rn(base[iw][i], ri);
+            dm[iw] = (dm[iw] < d) ? d : dm[iw];
+        }
+    }
+    return sum;
+}
+
+template <int NB, int NW>
+__device__ __forceinline__ float score_row_nb(float* r, float inv_stdnoise, const ScoreParams& sp,
+                                              int mode, float* out) {
+    float dm[NW];
+    const float sum = prefix_dmax_nb<NB, NW>(r, sp, dm);
+    float best = -FLT_MAX;
+#pragma unroll
+    for (int iw = 0; iw < NW; ++iw) {
+        if (iw < static_cast<int>(sp.nwidths)) {
+            const float base = __fsub_rn(__fmul_rn(sp.hb[iw], dm[iw]), __fmul_rn(sp.b[iw], sum));
+            const float snr = __fmul_rn(base, inv_stdnoise);
+            if (mode == LK_SCORE_PER_WIDTH) {
+                out[iw] = snr;
+            }
+            best = (best < snr) ? snr : best;
+        }
+    }
+    if (mode == LK_SCORE_MAX) {
+        out[0] = best;
+    }
+    return best;
+}
+
+template <int NB, int NW>
+__device__ __forceinline__ float max_snr_div_nb(float* r, float stdnoise, const ScoreParams& sp) {
+    float dm[NW];
+    const float sum = prefix_dmax_nb<NB, NW>(r, sp, dm);
+    float best = -FLT_MAX;
+#pragma unroll
+    for (int iw = 0; iw < NW; ++iw) {
+        if (iw < static_cast<int>(sp.nwidths)) {
+            const float base = __fsub_rn(__fmul_rn(sp.hb[iw], dm[iw]), __fmul_rn(sp.b[iw], sum));
+            const float snr = __fdiv_rn(base, stdnoise);
+            best = (best < snr) ? snr : best;
+        }
+    }
+    return best;
+}
+
+// score_row with nbins dispatched to a compile-time constant when it is NB.
+template <int NB, int NW>
+__device__ __forceinline__ float score_row_any(float* r, uint32_t nbins, float inv_stdnoise,
+                                               const ScoreParams& sp, int mode, float* out) {
+    if constexpr (NB > 0) {
+        return score_row_nb<NB, NW>(r, inv_stdnoise, sp, mode, out);
+    } else {
+        return score_row<NW>(r, nbins, inv_stdnoise, sp, mode, out);
+    }
+}
+
+// Calls f(integral_constant<int, NW>, integral_constant<int, NB>) with NW the
+// width capacity (8, 16, 32) and NB = nbins when it is 32, 64 or 128 (and at
+// most 16 widths), else NB = 0 (runtime nbins).
+template <class F>
+void dispatch_nw_nb(uint32_t nwidths, uint32_t nbins, F&& f) {
+    auto by_nb = [&](auto nw) {
+        constexpr int NW = decltype(nw)::value;
+        if constexpr (NW <= 16) {
+            if (nbins == 32) {
+                f(nw, std::integral_constant<int, 32>{});
+                return;
+            }
+            if (nbins == 64) {
+                f(nw, std::integral_constant<int, 64>{});
+                return;
+            }
+            if (nbins == 128) {
+                f(nw, std::integral_constant<int, 128>{});
+                return;
+            }
+        }
+        f(nw, std::integral_constant<int, 0>{});
+    };
+    if (nwidths <= 8) {
+        by_nb(std::integral_constant<int, 8>{});
+    } else if (nwidths <= 16) {
+        by_nb(std::integral_constant<int, 16>{});
+    } else {
+        by_nb(std::integral_constant<int, 32>{});
+    }
+}
+
+template <int NB, int NW>
+__device__ __forceinline__ float max_snr_div_any(float* r, uint32_t nbins, float stdnoise,
+                                                 const ScoreParams& sp) {
+    if constexpr (NB > 0) {
+        return max_snr_div_nb<NB, NW>(r, stdnoise, sp);
+    } else {
+        return max_snr_div<NW>(r, nbins, stdnoise, sp);
+    }
 }
 
 // Profiles per block so that the staged rows fit comfortably in shared memory.

@@ -75,7 +75,7 @@ __device__ __forceinline__ float stage_value(const McArgs& a, TrialRows t, uint3
 // Block of T trials: warps build the folds in shared memory (lanes over
 // bins), then one thread per trial scores its fold; the block's threshold
 // counts are summed in shared memory and added to the global counts once.
-template <int NW>
+template <int NW, int NB>
 __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
     extern __shared__ float rows[];
     __shared__ unsigned int s_cnt[2 * LK_MC_MAX_THRESHOLDS];
@@ -96,8 +96,8 @@ __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
     }
     __syncthreads();
     if (threadIdx.x < nhere) {
-        const float m = sc::max_snr_div<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, a.nbins,
-                                            a.stdnoise, sp);
+        const float m = sc::max_snr_div_any<NB, NW>(rows + static_cast<size_t>(threadIdx.x) * rs,
+                                                    a.nbins, a.stdnoise, sp);
         const uint64_t i = p0 + threadIdx.x;
         a.max_snr[i] = m;
         const bool flagged = a.cls != nullptr && a.cls[trial_rows(a, i, false).noise] != 0;
@@ -216,13 +216,9 @@ void McExec::stage(const McStage& st, cudaStream_t s) {
         sc::set_smem(kern, smem);
         kern<<<static_cast<unsigned>(blocks), T, smem, s>>>(a, rs, m_sp);
     };
-    if (m_sp.nwidths <= 8) {
-        launch(mc_score_kernel<8>);
-    } else if (m_sp.nwidths <= 16) {
-        launch(mc_score_kernel<16>);
-    } else {
-        launch(mc_score_kernel<32>);
-    }
+    sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
+        launch(mc_score_kernel<decltype(nw)::value, decltype(nbc)::value>);
+    });
     LK_CUDA(cudaGetLastError());
     // S/N > threshold  <=>  S/N >= the next float above the threshold.
     const float thr_ge = std::nextafter(st.threshold, std::numeric_limits<float>::infinity());

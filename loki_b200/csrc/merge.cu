@@ -17,6 +17,7 @@
 // outer rows that read the same parent rows run at the same time and share
 // them through L2.
 #include <algorithm>
+#include <type_traits>
 
 #include "lk_device.cuh"
 #include "lk_kernels.hpp"
@@ -63,6 +64,73 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// Loads-in-flight form for nbins <= 32 * NJ (NJ = 1, 2, 4): a warp takes PB
+// output rows at a time, loads their coordinates with one lane each, issues
+// every tail and head load of the PB rows (NJ bins per lane and row), then
+// adds and stores. The first form keeps two loads in flight per lane and is
+// latency-bound; this one keeps 4 * PB * NJ.
+template <bool TAYLOR, class TIn, class TOut, int NJ, int PB>
+__global__ void __launch_bounds__(kThreads)
+    merge_kernel_mlp(const TIn* __restrict__ in, TOut* __restrict__ out,
+                     const void* __restrict__ coords, uint32_t n_inner, uint32_t n_outer,
+                     uint64_t nprev, uint32_t nbins) {
+    const uint32_t tile = blockIdx.x / n_outer;
+    const uint32_t outer = blockIdx.x - tile * n_outer;
+    const uint64_t s = blockIdx.y;
+    const uint64_t ncur = static_cast<uint64_t>(n_inner) * n_outer;
+    const uint32_t row = 2 * nbins;
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    const uint32_t j0 = tile * kCoordsPerBlock;
+    const uint32_t j1 = min(j0 + kCoordsPerBlock, n_inner);
+    const TIn* tail_base = in + (2 * s) * nprev * row;
+    const TIn* head_base = in + (2 * s + 1) * nprev * row;
+    TOut* out_base = out + (s * ncur + static_cast<uint64_t>(outer) * n_inner) * row;
+    for (uint32_t p0 = j0 + warp * PB; p0 < j1; p0 += (kThreads / kWarp) * PB) {
+        MergeCoord mine{0, 0, 0, 0};
+        if (lane < PB && p0 + lane < j1) {
+            mine = load_merge_coord<TAYLOR>(coords, static_cast<uint64_t>(outer) * n_inner + p0 + lane,
+                                            nbins);
+        }
+        float te[PB][NJ], tv[PB][NJ], he[PB][NJ], hv[PB][NJ];
+#pragma unroll
+        for (int q = 0; q < PB; ++q) {
+            const uint32_t it = __shfl_sync(0xffffffffu, mine.it, q);
+            const uint32_t ih = __shfl_sync(0xffffffffu, mine.ih, q);
+            const uint32_t st = __shfl_sync(0xffffffffu, mine.st, q);
+            const uint32_t sh = __shfl_sync(0xffffffffu, mine.sh, q);
+            const bool live = p0 + q < j1;
+            const TIn* tail = tail_base + static_cast<uint64_t>(it) * row;
+            const TIn* head = head_base + static_cast<uint64_t>(ih) * row;
+#pragma unroll
+            for (int u = 0; u < NJ; ++u) {
+                const uint32_t jr = lane + 32u * u;
+                const bool ok = live && jr < nbins;
+                const uint32_t j = ok ? jr : 0u;  // keep every address inside the rows
+                const uint32_t jt = j >= st ? j - st : j + nbins - st;
+                const uint32_t jh = j >= sh ? j - sh : j + nbins - sh;
+                te[q][u] = ok ? dev::Store<TIn>::load(tail + jt) : 0.0f;
+                tv[q][u] = ok ? dev::Store<TIn>::load(tail + nbins + jt) : 0.0f;
+                he[q][u] = ok ? dev::Store<TIn>::load(head + jh) : 0.0f;
+                hv[q][u] = ok ? dev::Store<TIn>::load(head + nbins + jh) : 0.0f;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PB; ++q) {
+            if (p0 + q < j1) {
+                TOut* o = out_base + static_cast<uint64_t>(p0 + q) * row;
+#pragma unroll
+                for (int u = 0; u < NJ; ++u) {
+                    const uint32_t j = lane + 32u * u;
+                    if (j < nbins) {
+                        o[j] = dev::Store<TOut>::from_float(__fadd_rn(te[q][u], he[q][u]));
+                        o[nbins + j] = dev::Store<TOut>::from_float(__fadd_rn(tv[q][u], hv[q][u]));
+                    }
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 
 void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylor,
@@ -89,12 +157,25 @@ void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylo
             TOut* out = static_cast<TOut*>(d_out) + out_off;
             const auto ni = static_cast<uint32_t>(n_inner);
             const auto no = static_cast<uint32_t>(n_outer);
+            auto go = [&](auto kern) {
+                kern<<<grid, kThreads, 0, s>>>(in, out, d_coords, ni, no, ncoords_prev, nbins);
+            };
+            auto pick = [&](auto tg) {
+                constexpr bool TG = decltype(tg)::value;
+                if (nbins <= 32) {
+                    go(merge_kernel_mlp<TG, TIn, TOut, 1, 8>);
+                } else if (nbins <= 64) {
+                    go(merge_kernel_mlp<TG, TIn, TOut, 2, 4>);
+                } else if (nbins <= 128) {
+                    go(merge_kernel_mlp<TG, TIn, TOut, 4, 2>);
+                } else {
+                    go(merge_kernel<TG, TIn, TOut>);
+                }
+            };
             if (taylor) {
-                merge_kernel<true, TIn, TOut>
-                    <<<grid, kThreads, 0, s>>>(in, out, d_coords, ni, no, ncoords_prev, nbins);
+                pick(std::true_type{});
             } else {
-                merge_kernel<false, TIn, TOut>
-                    <<<grid, kThreads, 0, s>>>(in, out, d_coords, ni, no, ncoords_prev, nbins);
+                pick(std::false_type{});
             }
         };
         if (!in_bf16 && !out_bf16) {

@@ -371,7 +371,7 @@ __device__ __forceinline__ float fkey_inv(uint32_t k) {
 // Phase 2 (thread per child): the reference's sequential prefix sum and
 // width maxima. Phase 3 (warp per child): children scoring at or above
 // thr_keep get their fold written for the world tree.
-template <int NW>
+template <int NW, int NB>
 __global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* __restrict__ parent,
                             uint64_t n, const float* __restrict__ tree_folds, uint64_t head,
                             uint64_t cap, const float* __restrict__ ffa_seg, LeafGeom g,
@@ -419,8 +419,8 @@ __global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* _
     if (threadIdx.x < nhere) {
         const uint64_t c = c0 + threadIdx.x;
         float score;
-        sc::score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nb, 1.0f, sp,
-                          LK_SCORE_MAX, &score);
+        sc::score_row_any<NB, NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nb, 1.0f, sp,
+                                  LK_SCORE_MAX, &score);
         scores[c] = score;
         s_keep[threadIdx.x] = score >= thr_keep ? 1u : 0u;
         const uint32_t k = fkey(score);
@@ -1196,13 +1196,9 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
                 m_tfolds[m_cur].as<float>(), t.head, t.cap, d_seg, geom, rc, rs, m_sp,
                 threshold, m_cscores.as<float>(), m_cfolds.as<float>(), d_mm);
         };
-        if (m_sp.nwidths <= 8) {
-            launch(leaf_kernel<8>);
-        } else if (m_sp.nwidths <= 16) {
-            launch(leaf_kernel<16>);
-        } else {
-            launch(leaf_kernel<32>);
-        }
+        sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
+            launch(leaf_kernel<decltype(nw)::value, decltype(nbc)::value>);
+        });
         LK_CUDA(cudaGetLastError());
     }
 

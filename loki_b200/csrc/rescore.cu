@@ -38,7 +38,7 @@ struct Leaf {
     uint32_t off;
 };
 
-template <bool TAYLOR, int NW>
+template <bool TAYLOR, int NW, int NB>
 __global__ void __launch_bounds__(kThreads)
     rescore_kernel(const float* __restrict__ fold0, RescoreTree t, ScoreParams sp, uint32_t rs,
                    const uint32_t* __restrict__ cells, const uint64_t* __restrict__ d_count,
@@ -137,8 +137,8 @@ __global__ void __launch_bounds__(kThreads)
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            sc::score_row<NW>(row, nbins, 1.0f, sp, LK_SCORE_PER_WIDTH,
-                              scores + cell * sp.nwidths);
+            sc::score_row_any<NB, NW>(row, nbins, 1.0f, sp, LK_SCORE_PER_WIDTH,
+                                      scores + cell * sp.nwidths);
         }
         __syncthreads();
     }
@@ -170,13 +170,9 @@ void rescore_cells(const float* d_fold0, const RescoreTree& t, bool taylor, cons
     };
     auto by_nw = [&](auto tg) {
         constexpr bool TG = decltype(tg)::value;
-        if (sp.nwidths <= 8) {
-            launch(rescore_kernel<TG, 8>);
-        } else if (sp.nwidths <= 16) {
-            launch(rescore_kernel<TG, 16>);
-        } else {
-            launch(rescore_kernel<TG, 32>);
-        }
+        sc::dispatch_nw_nb(sp.nwidths, t.nbins, [&](auto nw, auto nbc) {
+            launch(rescore_kernel<TG, decltype(nw)::value, decltype(nbc)::value>);
+        });
     };
     if (taylor) {
         by_nw(std::true_type{});

@@ -32,7 +32,7 @@ namespace {
 constexpr int kWarp = 32;
 using namespace sc;
 
-template <int NW>
+template <int NW, int NB>
 __global__ void score_kernel(const float* __restrict__ folds, uint64_t nprof, uint32_t nbins,
                              bool is3d, float inv_stdnoise, uint32_t rs, ScoreParams sp, int mode,
                              float* __restrict__ scores) {
@@ -53,8 +53,8 @@ __global__ void score_kernel(const float* __restrict__ folds, uint64_t nprof, ui
     if (threadIdx.x < nhere) {
         const uint64_t p = p0 + threadIdx.x;
         const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1;
-        score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, inv_stdnoise, sp, mode,
-                      scores + p * nout);
+        score_row_any<NB, NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins, inv_stdnoise, sp,
+                              mode, scores + p * nout);
     }
 }
 
@@ -67,7 +67,7 @@ __global__ void score_kernel(const float* __restrict__ folds, uint64_t nprof, ui
 // loads their coordinates with one lane each, then issues every tail/head
 // load of the PB profiles (NJ = ceil(nbins / 32) bins per lane; NJ == 0
 // selects a generic loop for large nbins) before the first add.
-template <bool TAYLOR, int NW, int NJ, int PB, class TIn>
+template <bool TAYLOR, int NW, int NJ, int PB, class TIn, int NB>
 __global__ void merge_score_kernel(const TIn* __restrict__ in, const void* __restrict__ coords,
                                    uint32_t n_inner, uint32_t n_outer, uint64_t nprev,
                                    uint32_t nbins, uint32_t rs, ScoreParams sp, int mode,
@@ -155,8 +155,8 @@ __global__ void merge_score_kernel(const TIn* __restrict__ in, const void* __res
     if (threadIdx.x < nhere) {
         const uint64_t c = c0 + threadIdx.x;
         const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? sp.nwidths : 1;
-        const float best = score_row<NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nbins,
-                                         1.0f, sp, mode, scores + c * nout);
+        const float best = score_row_any<NB, NW>(rows + static_cast<size_t>(threadIdx.x) * rs,
+                                                 nbins, 1.0f, sp, mode, scores + c * nout);
         if (cmax != nullptr) {
             cmax[c] = best;
         }
@@ -207,13 +207,9 @@ void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d
         kern<<<static_cast<unsigned>(blocks), T, smem, s>>>(d_folds, nprof, nbins, is3d,
                                                             inv_stdnoise, rs, sp, mode, d_scores);
     };
-    if (sp.nwidths <= 8) {
-        launch(score_kernel<8>);
-    } else if (sp.nwidths <= 16) {
-        launch(score_kernel<16>);
-    } else {
-        launch(score_kernel<32>);
-    }
+    dispatch_nw_nb(sp.nwidths, nbins, [&](auto nw, auto nbc) {
+        launch(score_kernel<decltype(nw)::value, decltype(nbc)::value>);
+    });
     LK_CUDA(cudaGetLastError());
 }
 
@@ -248,12 +244,24 @@ void merge_score_level(const void* d_in, const void* d_coords, bool taylor, uint
     auto pick = [&](auto tg, auto tin) {
         constexpr bool TG = decltype(tg)::value;
         using TI = decltype(tin);
+        // nbins of exactly 32, 64 or 128 (up to 16 widths) score with
+        // compile-time nbins.
+        const bool fixed = sp.nwidths <= 16 && (nbins == 32 || nbins == 64 || nbins == 128);
         auto by_nj = [&](auto nwc) {
             constexpr int NWC = decltype(nwc)::value;
-            if (nj == 1) launch(merge_score_kernel<TG, NWC, 1, 16, TI>);
-            else if (nj == 2) launch(merge_score_kernel<TG, NWC, 2, 8, TI>);
-            else if (nj == 4) launch(merge_score_kernel<TG, NWC, 4, 4, TI>);
-            else launch(merge_score_kernel<TG, NWC, 0, 1, TI>);
+            constexpr int FX = NWC <= 16 ? 1 : 0;
+            if (nj == 1) {
+                fixed ? launch(merge_score_kernel<TG, NWC, 1, 16, TI, 32 * FX>)
+                      : launch(merge_score_kernel<TG, NWC, 1, 16, TI, 0>);
+            } else if (nj == 2) {
+                fixed ? launch(merge_score_kernel<TG, NWC, 2, 8, TI, 64 * FX>)
+                      : launch(merge_score_kernel<TG, NWC, 2, 8, TI, 0>);
+            } else if (nj == 4) {
+                fixed ? launch(merge_score_kernel<TG, NWC, 4, 4, TI, 128 * FX>)
+                      : launch(merge_score_kernel<TG, NWC, 4, 4, TI, 0>);
+            } else {
+                launch(merge_score_kernel<TG, NWC, 0, 1, TI, 0>);
+            }
         };
         if (nwb == 8) by_nj(std::integral_constant<int, 8>{});
         else if (nwb == 16) by_nj(std::integral_constant<int, 16>{});
