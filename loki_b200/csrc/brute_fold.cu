@@ -29,7 +29,11 @@
 // is first interleaved into (e, v) pairs, so one 16-byte shared-memory load
 // yields two samples' pairs in adjacent registers and each sample is one
 // add.rn.f32x2 (two IEEE round-to-nearest adds, E and V, in one
-// instruction); accumulators are float2 [bin][lane].
+// instruction); accumulators are float2 [bin][lane]. Measured on B200
+// (2^22-sample accelerated workload, nbins 64): 1.95 ms against 2.23 ms for
+// two scalar adds. Loading the next run's sums one run ahead measured slower
+// here too (2.07 ms); for nbins 128 one row per warp stays faster (7.39
+// against 7.71 ms on the 2^21-sample frequency sweep).
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
