@@ -33,7 +33,10 @@
 // (2^22-sample accelerated workload, nbins 64): 1.95 ms against 2.23 ms for
 // two scalar adds. Loading the next run's sums one run ahead measured slower
 // here too (2.07 ms); for nbins 128 one row per warp stays faster (7.39
-// against 7.71 ms on the 2^21-sample frequency sweep).
+// against 7.71 ms on the 2^21-sample frequency sweep). Two frequencies per
+// warp sharing the sample registers (3.51 ms, half the warps fit) and each
+// frequency's bins split over two or four warps that skip words outside
+// their bins (2.55 / 3.64 ms) were slower as well.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
