@@ -131,6 +131,70 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// nbins = NB in {32, 64, 128}: rotations are (j - shift) & (NB - 1), every
+// lane's bins are in range, E and V of a row share one address register
+// (V at an immediate offset), and stores use immediate offsets from one
+// per-row base, which halves the integer work per element of
+// merge_kernel_mlp (that kernel is issue-bound on its index arithmetic).
+template <bool TAYLOR, class TIn, class TOut, int NB, int PB>
+__global__ void __launch_bounds__(kThreads)
+    merge_kernel_p2(const TIn* __restrict__ in, TOut* __restrict__ out,
+                    const void* __restrict__ coords, uint32_t n_inner, uint32_t n_outer,
+                    uint64_t nprev) {
+    constexpr int NJ = NB / 32;
+    constexpr uint32_t row = 2 * NB;
+    const uint32_t tile = blockIdx.x / n_outer;
+    const uint32_t outer = blockIdx.x - tile * n_outer;
+    const uint64_t s = blockIdx.y;
+    const uint64_t ncur = static_cast<uint64_t>(n_inner) * n_outer;
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    const uint32_t j0 = tile * kCoordsPerBlock;
+    const uint32_t j1 = min(j0 + kCoordsPerBlock, n_inner);
+    const TIn* tail_base = in + (2 * s) * nprev * row;
+    const TIn* head_base = in + (2 * s + 1) * nprev * row;
+    TOut* out_base = out + (s * ncur + static_cast<uint64_t>(outer) * n_inner) * row + lane;
+    for (uint32_t p0 = j0 + warp * PB; p0 < j1; p0 += (kThreads / kWarp) * PB) {
+        MergeCoord mine{0, 0, 0, 0};
+        if (lane < PB && p0 + lane < j1) {
+            mine = load_merge_coord<TAYLOR>(coords, static_cast<uint64_t>(outer) * n_inner + p0 + lane,
+                                            NB);
+        }
+        float te[PB][NJ], tv[PB][NJ], he[PB][NJ], hv[PB][NJ];
+#pragma unroll
+        for (int q = 0; q < PB; ++q) {
+            const uint32_t it = __shfl_sync(0xffffffffu, mine.it, q);
+            const uint32_t ih = __shfl_sync(0xffffffffu, mine.ih, q);
+            const uint32_t st = __shfl_sync(0xffffffffu, mine.st, q);
+            const uint32_t sh = __shfl_sync(0xffffffffu, mine.sh, q);
+            // rows of a coordinate past j1 read row 0 (in range) and are not stored
+            const bool live = p0 + q < j1;
+            const TIn* tail = tail_base + static_cast<uint64_t>(live ? it : 0u) * row;
+            const TIn* head = head_base + static_cast<uint64_t>(live ? ih : 0u) * row;
+#pragma unroll
+            for (int u = 0; u < NJ; ++u) {
+                const uint32_t j = lane + 32u * u;
+                const TIn* pt = tail + ((j - st) & (NB - 1));
+                const TIn* ph = head + ((j - sh) & (NB - 1));
+                te[q][u] = dev::Store<TIn>::load(pt);
+                tv[q][u] = dev::Store<TIn>::load(pt + NB);
+                he[q][u] = dev::Store<TIn>::load(ph);
+                hv[q][u] = dev::Store<TIn>::load(ph + NB);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PB; ++q) {
+            if (p0 + q < j1) {
+                TOut* o = out_base + static_cast<uint64_t>(p0 + q) * row;
+#pragma unroll
+                for (int u = 0; u < NJ; ++u) {
+                    o[32 * u] = dev::Store<TOut>::from_float(__fadd_rn(te[q][u], he[q][u]));
+                    o[NB + 32 * u] = dev::Store<TOut>::from_float(__fadd_rn(tv[q][u], hv[q][u]));
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 
 void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylor,
@@ -160,9 +224,18 @@ void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylo
             auto go = [&](auto kern) {
                 kern<<<grid, kThreads, 0, s>>>(in, out, d_coords, ni, no, ncoords_prev, nbins);
             };
+            auto go_p2 = [&](auto kern) {
+                kern<<<grid, kThreads, 0, s>>>(in, out, d_coords, ni, no, ncoords_prev);
+            };
             auto pick = [&](auto tg) {
                 constexpr bool TG = decltype(tg)::value;
-                if (nbins <= 32) {
+                if (nbins == 32) {
+                    go_p2(merge_kernel_p2<TG, TIn, TOut, 32, 8>);
+                } else if (nbins == 64) {
+                    go_p2(merge_kernel_p2<TG, TIn, TOut, 64, 4>);
+                } else if (nbins == 128) {
+                    go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 2>);
+                } else if (nbins <= 32) {
                     go(merge_kernel_mlp<TG, TIn, TOut, 1, 8>);
                 } else if (nbins <= 64) {
                     go(merge_kernel_mlp<TG, TIn, TOut, 2, 4>);

@@ -124,15 +124,27 @@ __global__ void merge_score_kernel(const TIn* __restrict__ in, const void* __res
                 const TIn* head = head_base + static_cast<uint64_t>(ih) * plen;
 #pragma unroll
                 for (int u = 0; u < NJ; ++u) {
-                    const uint32_t jr = lane + 32u * u;
-                    const bool ok = live && jr < nbins;
-                    const uint32_t j = ok ? jr : 0u;  // keep every address inside the rows
-                    const uint32_t jt = j >= st ? j - st : j + nbins - st;
-                    const uint32_t jh = j >= sh ? j - sh : j + nbins - sh;
-                    te[q][u] = ok ? dev::Store<TIn>::load(tail + jt) : 0.0f;
-                    tv[q][u] = ok ? dev::Store<TIn>::load(tail + nbins + jt) : 1.0f;
-                    he[q][u] = ok ? dev::Store<TIn>::load(head + jh) : 0.0f;
-                    hv[q][u] = ok ? dev::Store<TIn>::load(head + nbins + jh) : 1.0f;
+                    if constexpr (NB > 0) {
+                        // nbins == NB == 32 * NJ: every lane's bins are in range;
+                        // rows past nhere read row 0 (in range) and are not used
+                        const uint32_t j = lane + 32u * u;
+                        const TIn* pt = (live ? tail : in) + ((j - st) & (NB - 1));
+                        const TIn* ph = (live ? head : head_base) + ((j - sh) & (NB - 1));
+                        te[q][u] = dev::Store<TIn>::load(pt);
+                        tv[q][u] = dev::Store<TIn>::load(pt + NB);
+                        he[q][u] = dev::Store<TIn>::load(ph);
+                        hv[q][u] = dev::Store<TIn>::load(ph + NB);
+                    } else {
+                        const uint32_t jr = lane + 32u * u;
+                        const bool ok = live && jr < nbins;
+                        const uint32_t j = ok ? jr : 0u;  // keep every address inside the rows
+                        const uint32_t jt = j >= st ? j - st : j + nbins - st;
+                        const uint32_t jh = j >= sh ? j - sh : j + nbins - sh;
+                        te[q][u] = ok ? dev::Store<TIn>::load(tail + jt) : 0.0f;
+                        tv[q][u] = ok ? dev::Store<TIn>::load(tail + nbins + jt) : 1.0f;
+                        he[q][u] = ok ? dev::Store<TIn>::load(head + jh) : 0.0f;
+                        hv[q][u] = ok ? dev::Store<TIn>::load(head + nbins + jh) : 1.0f;
+                    }
                 }
             }
 #pragma unroll
