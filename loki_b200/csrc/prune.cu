@@ -408,11 +408,22 @@ __global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* _
         const float* hd = ffa_seg + static_cast<uint64_t>(s_pidx[p]) * 2 * nb;
         const uint32_t s = s_shift[p];
         float* dst = rows + static_cast<size_t>(p) * rs;
-        for (uint32_t j = lane; j < nb; j += kWarp) {
-            const uint32_t jh = j >= s ? j - s : j + nb - s;
-            const float e = __fadd_rn(__ldg(tail + j), __ldg(hd + jh));
-            const float v = __fadd_rn(__ldg(tail + nb + j), __ldg(hd + nb + jh));
-            dst[j] = sc::normalise(e, v);
+        if constexpr (NB > 0) {
+            // nbins == NB, a multiple of 32: masked rotation, no bounds test
+#pragma unroll
+            for (uint32_t j = lane; j < static_cast<uint32_t>(NB); j += kWarp) {
+                const float* ph = hd + ((j - s) & (NB - 1));
+                const float e = __fadd_rn(__ldg(tail + j), __ldg(ph));
+                const float v = __fadd_rn(__ldg(tail + NB + j), __ldg(ph + NB));
+                dst[j] = sc::normalise(e, v);
+            }
+        } else {
+            for (uint32_t j = lane; j < nb; j += kWarp) {
+                const uint32_t jh = j >= s ? j - s : j + nb - s;
+                const float e = __fadd_rn(__ldg(tail + j), __ldg(hd + jh));
+                const float v = __fadd_rn(__ldg(tail + nb + j), __ldg(hd + nb + jh));
+                dst[j] = sc::normalise(e, v);
+            }
         }
     }
     __syncthreads();

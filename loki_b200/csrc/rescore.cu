@@ -16,9 +16,11 @@
 // at row leaf_idx[s] and bin (j - leaf_off[s]) mod n, where leaf_off is the
 // sum of the shifts along the path. A block expands the path top-down once per
 // cell (leaf table in shared memory), then each thread reduces one (row, bin)
-// over the leaves bottom-up with a binary-counter stack, which groups the adds
-// exactly as the level-by-level merges do (IEEE addition is commutative, so
-// the operand order of each add does not matter; the grouping does).
+// over a quarter of the leaves (an aligned subtree) bottom-up with a
+// binary-counter stack, and the four subtree totals are added as the tree's
+// top two levels. This groups the adds exactly as the level-by-level merges
+// do (IEEE addition is commutative, so the operand order of each add does not
+// matter; the grouping does).
 #include <algorithm>
 
 #include "lk_device.cuh"
@@ -30,7 +32,9 @@ namespace lk {
 
 namespace {
 
-constexpr uint32_t kThreads = 128;
+constexpr uint32_t kThreads = 512;
+constexpr uint32_t kLane = 128;  // threads per leaf part
+constexpr uint32_t kParts = kThreads / kLane;
 constexpr uint32_t kGroup = 8;  // leaves loaded before their adds (ILP)
 
 struct Leaf {
@@ -48,8 +52,14 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t nleaves = 1u << (t.n_levels - 1);
     Leaf* la = reinterpret_cast<Leaf*>(smem_raw);
     Leaf* lb = la + nleaves;
-    float* ev = reinterpret_cast<float*>(lb + nleaves);  // [2 * nbins]
-    float* row = ev + 2 * nbins;                         // [rs]
+    float* ev = reinterpret_cast<float*>(lb + nleaves);  // [kParts][2 * nbins]
+    float* row = ev + kParts * 2 * nbins;                // [rs]
+    // The leaves split into nparts aligned subtrees (parts of >= kGroup
+    // leaves), each reduced by kLane threads; the part totals are then added
+    // pairwise, which is the top of the same tree.
+    const uint32_t nparts = nleaves >= kParts * kGroup ? kParts : 1;
+    const uint32_t pleaves = nleaves / nparts;
+    const uint32_t part = threadIdx.x / kLane;
     const uint64_t count = min(*d_count, max_cells);
     const uint32_t plen = 2 * nbins;
     for (uint64_t k = blockIdx.x; k < count; k += gridDim.x) {
@@ -81,19 +91,20 @@ __global__ void __launch_bounds__(kThreads)
         }
         // ---- bottom-up: FP32 add tree per (row, bin) ---------------------
         const float* base = fold0 + series * t.fold0_size;
-        for (uint32_t e = threadIdx.x; e < plen; e += blockDim.x) {
+        for (uint32_t e = threadIdx.x % kLane; part < nparts && e < plen; e += kLane) {
             const uint32_t r = e >= nbins ? nbins : 0;
             const uint32_t j = e - r;
             float stk[kRescoreMaxLevels];
-            auto leaf_value = [&](uint32_t s) {
+            auto leaf_value = [&](uint32_t sl) {
+                const uint32_t s = part * pleaves + sl;
                 const Leaf lf = cur[s];
                 const uint32_t jj = j >= lf.off ? j - lf.off : j + nbins - lf.off;
                 return __ldg(base + (static_cast<uint64_t>(s) * t.ncoords0 + lf.idx) * plen + r +
                              jj);
             };
             float total;
-            if (nleaves >= kGroup) {
-                const uint32_t ngroups = nleaves / kGroup;
+            if (pleaves >= kGroup) {
+                const uint32_t ngroups = pleaves / kGroup;
                 for (uint32_t g = 0; g < ngroups; ++g) {
                     float v[kGroup];
 #pragma unroll
@@ -118,7 +129,7 @@ __global__ void __launch_bounds__(kThreads)
                 }
                 total = stk[31 - __clz(ngroups)];
             } else {
-                for (uint32_t q = 0; q < nleaves; ++q) {
+                for (uint32_t q = 0; q < pleaves; ++q) {
                     float acc = leaf_value(q);
                     uint32_t b = 0;
                     while ((q >> b) & 1u) {
@@ -127,13 +138,24 @@ __global__ void __launch_bounds__(kThreads)
                     }
                     stk[b] = acc;
                 }
-                total = stk[31 - __clz(nleaves)];
+                total = stk[31 - __clz(pleaves)];
             }
-            ev[e] = total;
+            ev[part * plen + e] = total;
         }
         __syncthreads();
         for (uint32_t j = threadIdx.x; j < nbins; j += blockDim.x) {
-            row[j] = sc::normalise(ev[j], ev[nbins + j]);
+            float fe, fv;
+            if (nparts == kParts) {
+                static_assert(kParts == 4, "part totals are added as a 4-leaf tree");
+                fe = __fadd_rn(__fadd_rn(ev[j], ev[plen + j]),
+                               __fadd_rn(ev[2 * plen + j], ev[3 * plen + j]));
+                fv = __fadd_rn(__fadd_rn(ev[nbins + j], ev[plen + nbins + j]),
+                               __fadd_rn(ev[2 * plen + nbins + j], ev[3 * plen + nbins + j]));
+            } else {
+                fe = ev[j];
+                fv = ev[nbins + j];
+            }
+            row[j] = sc::normalise(fe, fv);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -156,13 +178,15 @@ void rescore_cells(const float* d_fold0, const RescoreTree& t, bool taylor, cons
     }
     const uint32_t nleaves = 1u << (t.n_levels - 1);
     const uint32_t rs = sc::row_stride(t.nbins, sp.wmax);
-    const size_t smem = 2 * nleaves * sizeof(Leaf) + (2 * t.nbins + rs) * sizeof(float);
+    const size_t smem = 2 * nleaves * sizeof(Leaf) + (kParts * 2 * t.nbins + rs) * sizeof(float);
     require(smem <= 200 * 1024, "rescore: nbins too large");
     int sms = 148;
     int dev = 0;
     LK_CUDA(cudaGetDevice(&dev));
     LK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const uint64_t blocks = std::min<uint64_t>(max_cells, static_cast<uint64_t>(sms) * 8);
+    // One block per listed cell up to 32 per SM (blocks past the device-side
+    // count exit at once); a block loops over further cells.
+    const uint64_t blocks = std::min<uint64_t>(max_cells, static_cast<uint64_t>(sms) * 32);
     auto launch = [&](auto kern) {
         sc::set_smem(kern, smem);
         kern<<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(d_fold0, t, sp, rs, d_cells,
