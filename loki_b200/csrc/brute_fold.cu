@@ -36,13 +36,18 @@
 // against 7.71 ms on the 2^21-sample frequency sweep). Two frequencies per
 // warp sharing the sample registers (3.51 ms, half the warps fit) and each
 // frequency's bins split over two or four warps that skip words outside
-// their bins (2.55 / 3.64 ms) were slower as well.
+// their bins (2.55 / 3.64 ms) were slower as well. Frequencies whose bins step
+// by one at every run (every frequency below 1 / (tsamp nbins)) take a path
+// without the bin table, with the next run's sums loaded a run ahead (1.82
+// ms); dispatching each four-sample group through a 16-way switch instead of
+// per-sample run-start tests measured slower (2.46 ms).
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
 #include <thread>
+#include <type_traits>
 
 #include <cudaTypedefs.h>
 
@@ -80,6 +85,7 @@ struct FoldArgs {
     const void* bins;          // run bins of all frequencies (uint8 or uint16)
     const uint64_t* bin_off;   // first run of each frequency
     const uint64_t* nruns;     // runs of each frequency
+    const uint8_t* seq;        // 1: frequency's run bins go b, b+1, b+2, ... (mod nbins)
     uint32_t nfreq;
     uint32_t nseg;
     uint32_t nbins;
@@ -397,79 +403,114 @@ __global__ void __launch_bounds__(640, 1)
     const uint32_t* M = a.masks + static_cast<size_t>(f) * a.nwords;
     const BinT* B = static_cast<const BinT*>(a.bins) + a.bin_off[f];
     const uint64_t nr = a.nruns[f];
-
-    uint32_t bin = a.nbins;
-    float2 acc = make_float2(0.0f, 0.0f);
-    uint64_t r = 0;
-    uint64_t rbase = 0;
-    uint32_t binbuf = load_bins(B, nr, 0, lane);
-    uint32_t maskbuf = __ldg(M + min(static_cast<uint32_t>(lane), a.nwords - 1));
     const uint32_t lrow = static_cast<uint32_t>(lane) * 128u;
     const uint32_t lsw = static_cast<uint32_t>(lane) & 7u;
 
-    auto start_run = [&](uint32_t& rl) {
-        A[bin * kWarp] = acc;
-        bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
-        ++rl;
-        acc = A[bin * kWarp];
-    };
+    // The word loop, for SEQ = run bins b, b+1, ... (mod nbins) or any order.
+    // SEQ: a run's bin is the previous one plus one, so no table read, and the
+    // next run's sums are loaded as soon as a run starts (the only store before
+    // they are used is the current bin's, and the next bin differs from it),
+    // which takes the load off the add chain. Other frequencies read each
+    // run's bin from the table by warp shuffle.
+    auto consume = [&](auto seq_tag) -> bool {
+        constexpr bool SEQ = decltype(seq_tag)::value;
+        uint32_t bin;
+        float2 acc = make_float2(0.0f, 0.0f);
+        float2 nacc = make_float2(0.0f, 0.0f);  // SEQ: sums of bin + 1
+        uint64_t r = 0;
+        uint64_t rbase = 0;
+        uint32_t binbuf = 0;
+        if constexpr (SEQ) {
+            // The first run (sample 0) starts at bin b0: begin "before" it at
+            // b0 - 1, whose sums are still zero, so the first run start
+            // stores a zero there and moves to b0 with zero sums.
+            const uint32_t b0 = static_cast<uint32_t>(__ldg(B));
+            bin = b0 == 0 ? a.nbins - 1 : b0 - 1;
+        } else {
+            bin = a.nbins;  // scratch slot before the first run
+            binbuf = load_bins(B, nr, 0, lane);
+        }
+        uint32_t maskbuf = __ldg(M + min(static_cast<uint32_t>(lane), a.nwords - 1));
 
-    uint32_t phase = 0;
-    uint32_t s = 0;
-    for (uint32_t c = 0; c < a.nwords; ++c) {
-        if ((c & 31u) == 0 && c > 0) {
-            maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
-        }
-        const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
-        if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
-            rbase = r;
-            binbuf = load_bins(B, nr, rbase, lane);
-        }
-        if (!ptx::mbar_wait_bounded(&full[s], phase, a.status,
-                                    dev::kStatusWaitTimeout |
-                                        (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull))) {
-            return;
-        }
-        const unsigned char* t0 = ring + static_cast<size_t>(s) * kStageBytes + lrow;
-        float2 x[32];
-#pragma unroll
-        for (uint32_t h = 0; h < 2; ++h) {
-#pragma unroll
-            for (uint32_t j = 0; j < 8; ++j) {
-                const uint32_t o = (j ^ lsw) << 4;
-                const float4 v = *reinterpret_cast<const float4*>(t0 + h * kTileBytes + o);
-                x[16 * h + 2 * j] = make_float2(v.x, v.y);
-                x[16 * h + 2 * j + 1] = make_float2(v.z, v.w);
-            }
-        }
-        ptx::mbar_arrive(&empty[s]);
-        s = (s + 1 == S) ? 0 : s + 1;
-        if (s == 0) {
-            phase ^= 1u;
-        }
-        uint32_t rl = static_cast<uint32_t>(r - rbase);
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-            if (((m >> (4 * g)) & 0xfu) == 0) {
-#pragma unroll
-                for (int i = 4 * g; i < 4 * g + 4; ++i) {
-                    acc = add2_rn(acc, x[i]);
-                }
+        auto start_run = [&](uint32_t& rl) {
+            A[bin * kWarp] = acc;
+            if constexpr (SEQ) {
+                bin = bin + 1 == a.nbins ? 0u : bin + 1;
+                acc = nacc;
+                const uint32_t nb = bin + 1 == a.nbins ? 0u : bin + 1;
+                nacc = A[nb * kWarp];
+                ++rl;
             } else {
-#pragma unroll
-                for (int i = 4 * g; i < 4 * g + 4; ++i) {
-                    if (m & (1u << i)) {
-                        start_run(rl);
-                    }
-                    acc = add2_rn(acc, x[i]);
+                bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
+                ++rl;
+                acc = A[bin * kWarp];
+            }
+        };
+
+        uint32_t phase = 0;
+        uint32_t s = 0;
+        for (uint32_t c = 0; c < a.nwords; ++c) {
+            if ((c & 31u) == 0 && c > 0) {
+                maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
+            }
+            const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
+            if constexpr (!SEQ) {
+                if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
+                    rbase = r;
+                    binbuf = load_bins(B, nr, rbase, lane);
                 }
             }
+            if (!ptx::mbar_wait_bounded(&full[s], phase, a.status,
+                                        dev::kStatusWaitTimeout |
+                                            (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull))) {
+                return false;
+            }
+            const unsigned char* t0 = ring + static_cast<size_t>(s) * kStageBytes + lrow;
+            float2 x[32];
+#pragma unroll
+            for (uint32_t h = 0; h < 2; ++h) {
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j) {
+                    const uint32_t o = (j ^ lsw) << 4;
+                    const float4 v = *reinterpret_cast<const float4*>(t0 + h * kTileBytes + o);
+                    x[16 * h + 2 * j] = make_float2(v.x, v.y);
+                    x[16 * h + 2 * j + 1] = make_float2(v.z, v.w);
+                }
+            }
+            ptx::mbar_arrive(&empty[s]);
+            s = (s + 1 == S) ? 0 : s + 1;
+            if (s == 0) {
+                phase ^= 1u;
+            }
+            uint32_t rl = static_cast<uint32_t>(r - rbase);
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                if (((m >> (4 * g)) & 0xfu) == 0) {
+#pragma unroll
+                    for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                        acc = add2_rn(acc, x[i]);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                        if (m & (1u << i)) {
+                            start_run(rl);
+                        }
+                        acc = add2_rn(acc, x[i]);
+                    }
+                }
+            }
+            r = rbase + rl;
         }
-        r = rbase + rl;
-    }
-    A[bin * kWarp] = acc;
-    if (r != nr) {
-        atomicOr(a.status, dev::kStatusBadTable);
+        A[bin * kWarp] = acc;
+        if (r != nr) {
+            atomicOr(a.status, dev::kStatusBadTable);
+        }
+        return true;
+    };
+    const bool ok = a.seq[f] != 0 ? consume(std::true_type{}) : consume(std::false_type{});
+    if (!ok) {
+        return;
     }
 
     const uint32_t seg = static_cast<uint32_t>(seg0 + lane);
@@ -671,6 +712,16 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
             t.join();
         }
     }
+    // Frequencies whose run bins step by one bin (mod nbins) at every run.
+    std::vector<uint8_t> seq(m_nfreq, 0);
+    for (uint64_t f = 0; f < m_nfreq; ++f) {
+        const auto& rb = per_f[f];
+        bool ok = !rb.empty();
+        for (size_t k = 1; ok && k < rb.size(); ++k) {
+            ok = rb[k] == (rb[k - 1] + 1) % nbins;
+        }
+        seq[f] = ok ? 1 : 0;
+    }
     std::vector<uint64_t> off(m_nfreq), nruns(m_nfreq);
     uint64_t total = 0;
     for (uint64_t f = 0; f < m_nfreq; ++f) {
@@ -697,11 +748,14 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
     LK_CUDA(cudaMemcpy(m_bin_off.ptr, off.data(), m_bin_off.bytes, cudaMemcpyHostToDevice));
     m_nruns.alloc(sizeof(uint64_t) * m_nfreq);
     LK_CUDA(cudaMemcpy(m_nruns.ptr, nruns.data(), m_nruns.bytes, cudaMemcpyHostToDevice));
+    m_seq.alloc(m_nfreq);
+    LK_CUDA(cudaMemcpy(m_seq.ptr, seq.data(), m_nfreq, cudaMemcpyHostToDevice));
+    m_nseq = static_cast<uint64_t>(std::count(seq.begin(), seq.end(), uint8_t{1}));
 }
 
 uint64_t BruteFoldDevice::device_bytes() const {
     return m_masks.bytes + m_bins.bytes + m_bin_off.bytes + m_nruns.bytes + m_stage.bytes +
-           m_ev.bytes;
+           m_ev.bytes + m_seq.bytes;
 }
 
 // The TMA maps read the series in place; a base address that is not 16-byte
@@ -765,6 +819,7 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
     a.bins = m_bins.ptr;
     a.bin_off = m_bin_off.as<uint64_t>();
     a.nruns = m_nruns.as<uint64_t>();
+    a.seq = m_seq.as<uint8_t>();
     const uint64_t nseg = m_map_batch * m_nseg;  // segments of the bound batch
     require(nseg <= 0x7fffffffULL, "BruteFold: too many segments");
     a.nfreq = static_cast<uint32_t>(m_nfreq);

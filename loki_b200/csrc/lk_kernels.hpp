@@ -84,6 +84,8 @@ private:
     DeviceBuffer m_bins;       // run bins, all frequencies
     DeviceBuffer m_bin_off;    // uint64 first run of each frequency
     DeviceBuffer m_nruns;      // uint64 runs of each frequency
+    DeviceBuffer m_seq;        // uint8 per frequency: run bins step by one
+    uint64_t m_nseq = 0;
     DeviceBuffer m_stage;      // aligned copy of a misaligned series
     DeviceBuffer m_ev;         // (e, v) interleaved series (both rows per warp)
     CUtensorMap m_tmap_e{}, m_tmap_v{};
