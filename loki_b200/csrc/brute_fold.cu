@@ -190,108 +190,139 @@ __global__ void __launch_bounds__(640, 1)
     const uint32_t* M = a.masks + static_cast<size_t>(f) * a.nwords;
     const BinT* B = static_cast<const BinT*>(a.bins) + a.bin_off[f];
     const uint64_t nr = a.nruns[f];
-
-    uint32_t bin = a.nbins;   // current run's bin (scratch slot before the first run)
-    float acc0 = 0.0f, acc1 = 0.0f;
-    uint64_t r = 0;           // runs started so far
-    uint64_t rbase = 0;       // run index held by lane 0 of binbuf
-    uint32_t binbuf = load_bins(B, nr, 0, lane);
-    uint32_t maskbuf = __ldg(M + min(static_cast<uint32_t>(lane), a.nwords - 1));
     // Swizzled tile offset of lane l's 16-byte chunk j: l*128 + ((j ^ (l & 7)) * 16).
     const uint32_t lrow = static_cast<uint32_t>(lane) * 128u;
     const uint32_t lsw = static_cast<uint32_t>(lane) & 7u;
 
-    // Starts run rl (relative to rbase): flush the current sums, fetch the
-    // run's bin and load its sums. (Loading the next run's sums one run ahead
-    // measured slower on B200: 2.42 against 2.22 ms on the 2^22-sample
-    // accelerated workload.)
-    auto start_run = [&](uint32_t& rl) {
+    // The word loop; SEQ as in the packed kernel (run bins step by one: no
+    // table, next run's sums loaded a run ahead).
+    auto consume = [&](auto seq_tag) -> bool {
+        constexpr bool SEQ = decltype(seq_tag)::value;
+        uint32_t bin;
+        float acc0 = 0.0f, acc1 = 0.0f;
+        float nacc0 = 0.0f, nacc1 = 0.0f;  // SEQ: sums of bin + 1
+        uint64_t r = 0;      // runs started so far
+        uint64_t rbase = 0;  // run index held by lane 0 of binbuf
+        uint32_t binbuf = 0;
+        if constexpr (SEQ) {
+            const uint32_t b0 = static_cast<uint32_t>(__ldg(B));
+            bin = b0 == 0 ? a.nbins - 1 : b0 - 1;
+        } else {
+            bin = a.nbins;  // scratch slot before the first run
+            binbuf = load_bins(B, nr, 0, lane);
+        }
+        uint32_t maskbuf = __ldg(M + min(static_cast<uint32_t>(lane), a.nwords - 1));
+
+        // Starts run rl (relative to rbase): flush the current sums, move to
+        // the run's bin and its sums.
+        auto start_run = [&](uint32_t& rl) {
+            A[bin * kWarp] = acc0;
+            if constexpr (ROWS == 2) {
+                A[vrow + bin * kWarp] = acc1;
+            }
+            if constexpr (SEQ) {
+                bin = bin + 1 == a.nbins ? 0u : bin + 1;
+                acc0 = nacc0;
+                acc1 = nacc1;
+                const uint32_t nb = bin + 1 == a.nbins ? 0u : bin + 1;
+                nacc0 = A[nb * kWarp];
+                if constexpr (ROWS == 2) {
+                    nacc1 = A[vrow + nb * kWarp];
+                }
+                ++rl;
+            } else {
+                bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
+                ++rl;
+                acc0 = A[bin * kWarp];
+                if constexpr (ROWS == 2) {
+                    acc1 = A[vrow + bin * kWarp];
+                }
+            }
+        };
+
+        uint32_t phase = 0;
+        uint32_t s = 0;
+        for (uint32_t c = 0; c < a.nwords; ++c) {
+            if ((c & 31u) == 0 && c > 0) {
+                maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
+            }
+            const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
+            if constexpr (!SEQ) {
+                // binbuf must hold runs r .. r + popc(m) - 1.
+                if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
+                    rbase = r;
+                    binbuf = load_bins(B, nr, rbase, lane);
+                }
+            }
+            if (!ptx::mbar_wait_bounded(&full[s], phase, a.status,
+                                        dev::kStatusWaitTimeout |
+                                            (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull))) {
+                return false;
+            }
+            const unsigned char* te =
+                ring + static_cast<size_t>(s) * kStageBytes + row0 * kTileBytes + lrow;
+            float x0[32];
+            [[maybe_unused]] float x1[ROWS == 2 ? 32 : 1];
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) {
+                const uint32_t o = (j ^ lsw) << 4;
+                const float4 v0 = *reinterpret_cast<const float4*>(te + o);
+                x0[4 * j + 0] = v0.x;
+                x0[4 * j + 1] = v0.y;
+                x0[4 * j + 2] = v0.z;
+                x0[4 * j + 3] = v0.w;
+                if constexpr (ROWS == 2) {
+                    const float4 v1 = *reinterpret_cast<const float4*>(te + kTileBytes + o);
+                    x1[4 * j + 0] = v1.x;
+                    x1[4 * j + 1] = v1.y;
+                    x1[4 * j + 2] = v1.z;
+                    x1[4 * j + 3] = v1.w;
+                }
+            }
+            // Release the stage as soon as its samples are in registers.
+            ptx::mbar_arrive(&empty[s]);
+            s = (s + 1 == S) ? 0 : s + 1;
+            if (s == 0) {
+                phase ^= 1u;
+            }
+            uint32_t rl = static_cast<uint32_t>(r - rbase);
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                if (((m >> (4 * g)) & 0xfu) == 0) {
+#pragma unroll
+                    for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                        acc0 = __fadd_rn(acc0, x0[i]);
+                        if constexpr (ROWS == 2) {
+                            acc1 = __fadd_rn(acc1, x1[i]);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                        if (m & (1u << i)) {
+                            start_run(rl);
+                        }
+                        acc0 = __fadd_rn(acc0, x0[i]);
+                        if constexpr (ROWS == 2) {
+                            acc1 = __fadd_rn(acc1, x1[i]);
+                        }
+                    }
+                }
+            }
+            r = rbase + rl;
+        }
         A[bin * kWarp] = acc0;
         if constexpr (ROWS == 2) {
             A[vrow + bin * kWarp] = acc1;
         }
-        bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
-        ++rl;
-        acc0 = A[bin * kWarp];
-        if constexpr (ROWS == 2) {
-            acc1 = A[vrow + bin * kWarp];
+        if (r != nr) {
+            atomicOr(a.status, dev::kStatusBadTable);
         }
+        return true;
     };
-
-    uint32_t phase = 0;
-    uint32_t s = 0;
-    for (uint32_t c = 0; c < a.nwords; ++c) {
-        if ((c & 31u) == 0 && c > 0) {
-            maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
-        }
-        const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
-        // binbuf must hold runs r .. r + popc(m) - 1.
-        if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
-            rbase = r;
-            binbuf = load_bins(B, nr, rbase, lane);
-        }
-        if (!ptx::mbar_wait_bounded(&full[s], phase, a.status,
-                                    dev::kStatusWaitTimeout |
-                                        (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull))) {
-            return;
-        }
-        const unsigned char* te =
-            ring + static_cast<size_t>(s) * kStageBytes + row0 * kTileBytes + lrow;
-        float x0[32], x1[ROWS == 2 ? 32 : 1];
-#pragma unroll
-        for (uint32_t j = 0; j < 8; ++j) {
-            const uint32_t o = (j ^ lsw) << 4;
-            const float4 v0 = *reinterpret_cast<const float4*>(te + o);
-            x0[4 * j + 0] = v0.x;
-            x0[4 * j + 1] = v0.y;
-            x0[4 * j + 2] = v0.z;
-            x0[4 * j + 3] = v0.w;
-            if constexpr (ROWS == 2) {
-                const float4 v1 = *reinterpret_cast<const float4*>(te + kTileBytes + o);
-                x1[4 * j + 0] = v1.x;
-                x1[4 * j + 1] = v1.y;
-                x1[4 * j + 2] = v1.z;
-                x1[4 * j + 3] = v1.w;
-            }
-        }
-        // Release the stage as soon as its samples are in registers.
-        ptx::mbar_arrive(&empty[s]);
-        s = (s + 1 == S) ? 0 : s + 1;
-        if (s == 0) {
-            phase ^= 1u;
-        }
-        uint32_t rl = static_cast<uint32_t>(r - rbase);
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-            if (((m >> (4 * g)) & 0xfu) == 0) {
-#pragma unroll
-                for (int i = 4 * g; i < 4 * g + 4; ++i) {
-                    acc0 = __fadd_rn(acc0, x0[i]);
-                    if constexpr (ROWS == 2) {
-                        acc1 = __fadd_rn(acc1, x1[i]);
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int i = 4 * g; i < 4 * g + 4; ++i) {
-                    if (m & (1u << i)) {
-                        start_run(rl);
-                    }
-                    acc0 = __fadd_rn(acc0, x0[i]);
-                    if constexpr (ROWS == 2) {
-                        acc1 = __fadd_rn(acc1, x1[i]);
-                    }
-                }
-            }
-        }
-        r = rbase + rl;
-    }
-    A[bin * kWarp] = acc0;
-    if constexpr (ROWS == 2) {
-        A[vrow + bin * kWarp] = acc1;
-    }
-    if (r != nr) {
-        atomicOr(a.status, dev::kStatusBadTable);
+    const bool ok = a.seq[f] != 0 ? consume(std::true_type{}) : consume(std::false_type{});
+    if (!ok) {
+        return;
     }
 
     const uint32_t seg = static_cast<uint32_t>(seg0 + lane);
