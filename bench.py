@@ -201,7 +201,7 @@ def run_reference(args, rank):
 
     ts_e, ts_v, params, _ = workload()
     if not ref.available("timing"):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
+        emit({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"})
         return 0
     step, ntrials, nthreads = reference_runner(params)
     for _ in range(max(args.warmup, 1)):
@@ -222,7 +222,7 @@ def run_reference(args, rank):
                          "sample": f"full workload per step, {args.steps} steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line))
+    emit(line)
     return 0
 
 
@@ -387,14 +387,38 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "stages": stages, "wall_s": wall,
         }
-        print(json.dumps(line))
+        emit(line)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
 
 
+_JSON_OUT = None
+
+
+def _reserve_stdout():
+    """Keep the process's stdout for the JSON line alone: the reference's
+    native CPU code writes progress-bar control sequences to stdout, so fd 1
+    is pointed at stderr and the JSON line goes to a saved copy of it."""
+    global _JSON_OUT
+    sys.stdout.flush()
+    _JSON_OUT = os.fdopen(os.dup(1), "w")
+    os.dup2(2, 1)
+
+
+def emit(obj):
+    """Print one JSON line on the real stdout."""
+    out = _JSON_OUT if _JSON_OUT is not None else sys.stdout
+    out.write(json.dumps(obj) + "\n")
+    out.flush()
+
+
 def main():
+    # bench_workloads imports this file as `bench`; share this instance (and
+    # its saved stdout) instead of loading a second copy.
+    sys.modules.setdefault("bench", sys.modules[__name__])
+    _reserve_stdout()
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

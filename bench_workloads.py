@@ -122,7 +122,7 @@ def run_freq(args, rank, world, local_rank):
         from oracle import ref
 
         if not ref.available("timing"):
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            B.emit({"impl": "reference", "unavailable": "oracle/_ref was not built"})
             return 0
         step, ntrials, nthreads = B.reference_runner(params)
         for _ in range(max(args.warmup, 1)):
@@ -132,12 +132,12 @@ def run_freq(args, rank, world, local_rank):
             step(ts_e, ts_v)
         total = time.perf_counter() - t0
         v = ntrials * args.steps / total
-        print(json.dumps(_line(args, world, "freq_sweep_2^21x64us_nbins128", v, 1e3 * total / args.steps,
+        B.emit(_line(args, world, "freq_sweep_2^21x64us_nbins128", v, 1e3 * total / args.steps,
                                dict(cfgd, cpu_threads=nthreads), impl="reference",
                                cpu_baseline={"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference",
                                              "sample": f"full workload, {args.steps} steps"},
                                e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
-                                    "d2h_bytes_per_step": 0})))
+                                    "d2h_bytes_per_step": 0}))
         return 0
     torch, dist = _init(local_rank, world)
     from loki_b200 import _capi as C
@@ -200,12 +200,12 @@ def run_freq(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = B.cpu_baseline(params, ts_e, ts_v)
     if rank == 0:
-        print(json.dumps(_line(args, world, "freq_sweep_2^21x64us_nbins128", value, ms,
+        B.emit(_line(args, world, "freq_sweep_2^21x64us_nbins128", value, ms,
                                dict(cfgd, final_coords=int(ffa.plan.ncoords[-1]), candidates=int(cnt.item()),
                                     fold_storage=args.storage),
                                roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
                                gpu_launches=args.steps * launches, clocks=clk,
-                               stages={k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()})))
+                               stages={k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()}))
     _finish(dist)
     return 0
 
@@ -260,7 +260,7 @@ def run_prune(args, rank, world, local_rank):
         from oracle import lko, ref
 
         if not ref.available("timing"):
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            B.emit({"impl": "reference", "unavailable": "oracle/_ref was not built"})
             return 0
         cfg = ref.make_cfg(p["nsamps"], p["tsamp"], nbins, p["eta"], p["param_limits"], bseg_ffa=p["bseg_ffa"],
                            nthreads=os.cpu_count() or 1)
@@ -270,11 +270,11 @@ def run_prune(args, rank, world, local_rank):
         v, k, el, st = _ref_prune_sample(p, fold, thr, nseg // 2, nbins, "timing")
         widths = ref.box_widths(nbins)
         sample = f"one pruning run (ref_seg {nseg // 2}) over its first {k} levels, {el:.1f} s, single thread"
-        print(json.dumps(_line(args, world, "prune_jerk_2^23x64us_nbins32", v, 1e3 * el,
+        B.emit(_line(args, world, "prune_jerk_2^23x64us_nbins32", v, 1e3 * el,
                                _prune_cfgd(p, nseg, nseg // 2, widths), impl="reference",
                                cpu_baseline={"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
                                              "sample": sample},
-                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})))
+                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}))
         return 0
     torch, dist = _init(local_rank, world)
     from loki_b200.configs import PulsarSearchConfig
@@ -340,7 +340,7 @@ def run_prune(args, rank, world, local_rank):
                    "sample": f"reference pruning run (ref_seg {ref_seg}) over its first {k} levels "
                              f"({el:.1f} s), single thread, on the same FFA fold"}
     if rank == 0:
-        print(json.dumps(_line(
+        B.emit(_line(
             args, world, "prune_jerk_2^23x64us_nbins32", value, ms,
             dict(_prune_cfgd(p, nseg, ref_seg, widths), leaves_scored=leaves,
                  survivors=int(stats["n_leaves_surv"][-1]), levels_run=int(len(stats) - 1)),
@@ -348,7 +348,7 @@ def run_prune(args, rank, world, local_rank):
             clocks=clk, stages={"ffa_ms": ms - prune_ms, "prune_ms": prune_ms},
             level_stats=[{k: (float(r[k]) if k in ("threshold", "score_min", "score_max") else int(r[k]))
                           for k in ("level", "n_branches", "n_leaves", "n_leaves_surv", "threshold", "score_max")}
-                         for r in stats])))
+                         for r in stats]))
     _finish(dist)
     return 0
 
@@ -385,11 +385,11 @@ def run_mc(args, rank, world, local_rank):
         if rank != 0:
             return 0
         v, el, nsub = port_sample()
-        print(json.dumps(_line(args, world, "mc_cascade_2^20x64_8stages", v, 1e3 * el, cfgd, impl="reference",
+        B.emit(_line(args, world, "mc_cascade_2^20x64_8stages", v, 1e3 * el, cfgd, impl="reference",
                                cpu_baseline={"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                                              "sample": f"the first {nsub} profiles through all stages "
                                                        f"({el:.1f} s), C oracle restatement, one thread"},
-                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})))
+                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}))
         return 0
     torch, dist = _init(local_rank, world)
     from loki_b200.thresholds import MCStageCUDA
@@ -450,10 +450,10 @@ def run_mc(args, rank, world, local_rank):
                "sample": f"the first {nsub} profiles through all stages ({el:.1f} s), C oracle restatement "
                          f"(the reference's thresholds.cpp needs HDF5 and cannot be linked here), one thread"}
     if rank == 0:
-        print(json.dumps(_line(args, world, "mc_cascade_2^20x64_8stages", value, ms,
+        B.emit(_line(args, world, "mc_cascade_2^20x64_8stages", value, ms,
                                dict(cfgd, trials_per_step=trials),
                                roofline=_roofline("mc_stage", sum(stage_bytes), ms), cpu_baseline=cpu, e2e=e2e,
-                               gpu_launches=args.steps * len(stage_bytes) * 5, clocks=clk)))
+                               gpu_launches=args.steps * len(stage_bytes) * 5, clocks=clk))
     _finish(dist)
     return 0
 
@@ -501,15 +501,15 @@ def run_multi(args, rank, world, local_rank):
         from oracle import ref
 
         if not ref.available("timing"):
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            B.emit({"impl": "reference", "unavailable": "oracle/_ref was not built"})
             return 0
         v, el, npick, nthreads = ref_sample()
-        print(json.dumps(_line(args, world, "multi_series_512x2^18..2^22_nbins128", v, 1e3 * el, cfgd,
+        B.emit(_line(args, world, "multi_series_512x2^18..2^22_nbins128", v, 1e3 * el, cfgd,
                                impl="reference",
                                cpu_baseline={"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference",
                                              "sample": f"{npick} series spread over the lengths, one FFA + "
                                                        f"scores + compaction each ({el:.1f} s)"},
-                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})))
+                               e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}))
         return 0
     torch, dist = _init(local_rank, world)
     from loki_b200.batched import MultiSeriesSearch, _pow2_ceil
@@ -555,11 +555,11 @@ def run_multi(args, rank, world, local_rank):
     groups = {str(L): {"series": sum(1 for n in lens if _pow2_ceil(n) == L), "batch": ms.groups[L].nbatch,
                        "trials_per_series": ms.groups[L].per} for L in sorted(ms.groups)}
     if rank == 0:
-        print(json.dumps(_line(args, world, "multi_series_512x2^18..2^22_nbins128", value, ms_step,
+        B.emit(_line(args, world, "multi_series_512x2^18..2^22_nbins128", value, ms_step,
                                dict(cfgd, trials_per_step=trials, candidates=ncand, groups=groups,
                                     graphs="one CUDA graph per length for full batches",
                                     fold_storage=args.storage),
-                               cpu_baseline=cpu, e2e=e2e, clocks=clk)))
+                               cpu_baseline=cpu, e2e=e2e, clocks=clk))
     _finish(dist)
     return 0
 
