@@ -338,39 +338,34 @@ def run_ours(args, rank, world, local_rank):
                   "gbs": stage_bytes[k] / (stage_ms[k] / args.steps / 1e3) / 1e9}
               for k in sorted(stage_ms, key=stage_ms.get, reverse=True)}
 
-    # end to end through the public API with host buffers
+    # end to end through the public API with host buffers: every step copies
+    # its series from pinned host memory and reads its candidates back; the
+    # pipeline overlaps step k + 1's copy and step k - 1's read-back with step
+    # k's search (two device input slots, a copy stream and a compute stream)
     e2e = None
     if not args.no_e2e:
+        from loki_b200.pipeline import SearchPipeline
+
         he = torch.from_numpy(ts_e).pin_memory()
         hv = torch.from_numpy(ts_v).pin_memory()
-        hcnt = torch.zeros(1, dtype=torch.int64).pin_memory()
-        hidx = torch.empty(cap, dtype=torch.int32).pin_memory()
-        hsnr = torch.empty(cap, dtype=torch.float32).pin_memory()
-        d2h = 0
-        for k in range(args.warmup + args.steps):
-            if k == args.warmup:
-                if dist is not None:
-                    dist.barrier()
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                d2h = 0
-            e.copy_(he, non_blocking=True)
-            v.copy_(hv, non_blocking=True)
-            step()
-            hcnt.copy_(cnt, non_blocking=True)
-            torch.cuda.synchronize()
-            n = min(int(hcnt.item()), cap)
-            hidx[:n].copy_(idx[:n], non_blocking=True)
-            hsnr[:n].copy_(snr[:n], non_blocking=True)
-            torch.cuda.synchronize()
-            d2h += 8 + 8 * n
+        pipe = SearchPipeline(ffa, SNR_MIN, max_cands=cap)
+        for _ in pipe.run([(he, hv)] * args.warmup):
+            pass
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        pipe.h2d_bytes = pipe.d2h_bytes = 0
+        t0 = time.perf_counter()
+        for _ in pipe.run([(he, hv)] * args.steps):
+            pass
         e2e_s = time.perf_counter() - t0
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         if dist is not None:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e = {"value": ntrials * world * args.steps / float(t.item()), "unit": UNIT,
-               "h2d_bytes_per_step": 2 * 4 * params["nsamps"], "d2h_bytes_per_step": d2h // args.steps,
-               "api": "loki_b200 FFACUDA executor (lk_ffa_search) with pinned host input and result read-back"}
+               "h2d_bytes_per_step": pipe.h2d_bytes // args.steps, "d2h_bytes_per_step": pipe.d2h_bytes // args.steps,
+               "api": "loki_b200.pipeline.SearchPipeline over FFACUDA (lk_ffa_search): pinned host series in, "
+                      "candidates out, copies overlapped with the previous/next search"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -18,7 +18,7 @@ from ._capi import LokiError, lib
 # Fail loudly at import time if the native library is missing.
 lib()
 
-from . import batched, configs, ffa, fold, plans, prune, scores, thresholds  # noqa: E402
+from . import batched, configs, ffa, fold, pipeline, plans, prune, scores, thresholds  # noqa: E402
 from . import libculoki  # noqa: E402
 
 __all__ = ["configs", "plans", "ffa", "fold", "prune", "scores", "thresholds", "batched", "libculoki",

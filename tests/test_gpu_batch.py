@@ -102,3 +102,25 @@ def test_multi_series_driver_matches_oracle(cuda):
         want = np.flatnonzero(sc >= 3.5)
         np.testing.assert_array_equal(r["idx"], want.astype(np.uint32))
         np.testing.assert_array_equal(r["snr"], sc[want])
+
+
+def test_search_pipeline_matches_search(cuda):
+    """SearchPipeline (copies overlapped with searches) returns per series
+    exactly what FFACUDA.search returns."""
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+    from loki_b200.pipeline import SearchPipeline
+
+    cfg = PulsarSearchConfig(2**18, 1e-3, 32, 1.0, np.array([[-300.0, 300.0], [5.0, 8.0]]), use_fourier=False,
+                             score_widths=[1, 2, 3, 4])
+    ffa = FFACUDA(cfg)
+    data = [series(cfg.nsamps, 70 + k) for k in range(5)]
+    s0 = ffa.scores(*data[0])
+    thr = float(np.quantile(s0, 0.999))
+    want = [ffa.search(e, v, snr_min=thr) for e, v in data]
+    got = list(SearchPipeline(ffa, thr, max_cands=1 << 16).run(data))
+    assert len(got) == len(want)
+    for (gi, gs, gn), (wi, ws, wn) in zip(got, want):
+        assert gn == wn
+        np.testing.assert_array_equal(gi, wi)
+        np.testing.assert_array_equal(gs.view(np.uint32), ws.view(np.uint32))

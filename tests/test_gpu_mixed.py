@@ -149,3 +149,55 @@ def test_margin_api_and_fp16_refused(cuda):
     assert plain.rescore_margin == (0.0, 0.0)
     with pytest.raises(C.LokiError):
         FFACUDA(cfg, fold_storage="fp16")
+
+
+def _error_statement(nsamps: int):
+    """FP32 and BF16-stored S/N and folds against the FP64 oracle on the
+    accelerated-search workload (seed 7, four signals) at nsamps samples."""
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+    from loki_b200.synthetic import Pulsar, make_series
+
+    tsamp, nbins, eta = 64e-6, 64, 2.0
+    lims = [[-200.0, 200.0], [5.0, 50.0]]
+    widths = [1, 2, 3, 4, 6, 8, 12, 16]
+    rng = np.random.default_rng(7 + 1000)
+    psrs = [Pulsar(f0=float(rng.uniform(5, 50)), accel=float(rng.uniform(-150, 150)), duty=0.05,
+                   snr=float(rng.uniform(8, 20))) for _ in range(4)]
+    ts_e, ts_v = make_series(nsamps, tsamp, 7, psrs, nbins, widths)
+    cfg = PulsarSearchConfig(nsamps, tsamp, nbins, eta, np.array(lims), use_fourier=False, score_widths=widths)
+    op = lko.plan_create(lko.make_cfg(nsamps, tsamp, nbins, eta, lims))
+    plain = FFACUDA(cfg, fold_storage="fp32")
+    mixed = FFACUDA(cfg, fold_storage="bf16")
+    s64 = fp64.ffa_scores64(op, ts_e, ts_v, widths).ravel()
+    s32 = plain.scores(ts_e, ts_v).astype(np.float64)
+    s16 = mixed.scores(ts_e, ts_v).astype(np.float64)
+    thr = 7.0
+    i32, v32, n32 = plain.search(ts_e, ts_v, snr_min=thr)
+    i16, v16, n16 = mixed.search(ts_e, ts_v, snr_min=thr)
+    assert n16 == n32 and np.array_equal(i16, i32) and np.array_equal(v16.view(np.uint32), v32.view(np.uint32))
+    e16 = s16 - s64
+    stat = {
+        "nsamps": nsamps, "cells": int(s64.size), "candidates": int(n32),
+        "rescored_cells": mixed.rescored_cells(),
+        "fp32_snr_max_abs_err": float(np.max(np.abs(s32 - s64))),
+        "bf16_snr_rms_err": float(np.sqrt(np.mean(e16**2))),
+        "bf16_snr_max_abs_err": float(np.max(np.abs(e16))),
+        "bf16_snr_max_abs_err_at_or_above_6": float(np.max(np.abs(e16[s64 >= 6.0]))) if np.any(s64 >= 6.0) else 0.0,
+        "candidate_snr_max_abs_err": float(np.max(np.abs(v16.astype(np.float64) - s64[i16]))) if n16 else 0.0,
+        "margin": list(mixed.rescore_margin),
+    }
+    print("ERRSTAT", stat)
+    assert stat["fp32_snr_max_abs_err"] < 1e-4
+    assert stat["candidate_snr_max_abs_err"] < 1e-3
+    return stat
+
+
+def test_error_statement_accel_2p20(cuda):
+    _error_statement(1 << 20)
+
+
+@pytest.mark.skipif(not __import__("os").environ.get("LOKI_B200_FULL_ERRSTAT"),
+                    reason="full-size FP64 statement (2^22 samples, minutes of numpy): set LOKI_B200_FULL_ERRSTAT=1")
+def test_error_statement_accel_2p22(cuda):
+    _error_statement(1 << 22)
