@@ -120,6 +120,13 @@ def lib() -> ctypes.CDLL:
                                    u64, vp, vp, vp, vp, vp]
         L.lko_prune_run.argtypes = [vp, ctypes.c_int, vp, vp, u64, u64, u64, u64, u64, u64, vp, vp,
                                     vp, vp, vp, u64, vp]
+        L.lko_prune_run_basis.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, u64, u64, u64, u64, u64,
+                                          u64, vp, vp, vp, vp, vp, u64, vp]
+        L.lko_taylor_to_cheby.argtypes = [vp, u64, u32, f64]
+        L.lko_cheby_to_taylor.argtypes = [vp, u64, u32, f64]
+        L.lko_cheby_transform.argtypes = [vp, vp, u64, u32, f64, f64, f64, f64]
+        L.lko_cheby_branch.argtypes = [vp, u64, u32, f64, f64, f64, f64, u64, f64, u64, vp, vp, u64, vp]
+        L.lko_cheby_resolve.argtypes = [vp, vp, u64, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -435,8 +442,61 @@ def score_filter(folds, nbins, widths, threshold):
     return scores, idx[:k]
 
 
+# ---- Chebyshev basis (lib/chebyshev.cpp) --------------------------------------
+
+def taylor_to_cheby(leaves, nparams, coord_init):
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    n = out.size // ((nparams + 2) * 2)
+    lib().lko_taylor_to_cheby(_p(out), n, nparams, coord_init[1])
+    return out
+
+
+def cheby_to_taylor(leaves, nparams, coord_report):
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    n = out.size // ((nparams + 2) * 2)
+    lib().lko_cheby_to_taylor(_p(out), n, nparams, coord_report[1])
+    return out
+
+
+def cheby_transform(leaves, indices, nparams, coord_next, coord_cur):
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    idx = np.ascontiguousarray(indices, np.uint64)
+    lib().lko_cheby_transform(_p(out), _p(idx), idx.size, nparams, coord_next[0], coord_next[1],
+                              coord_cur[0], coord_cur[1])
+    return out
+
+
+def cheby_branch(leaves, nparams, coord_cur, coord_prev, nbins, eta, branch_max, cap=None):
+    """Returns (children, origins, parents transformed to coord_cur)."""
+    par = np.array(leaves, np.float64, copy=True, order="C")
+    stride = (nparams + 2) * 2
+    n = par.size // stride
+    cap = n * branch_max if cap is None else cap
+    out = np.zeros(cap * stride, np.float64)
+    org = np.zeros(cap, np.uint64)
+    nout = u64()
+    work = par.copy()
+    rc = lib().lko_cheby_branch(_p(work), n, nparams, coord_cur[0], coord_cur[1], coord_prev[0], coord_prev[1],
+                                nbins, eta, branch_max, _p(out), _p(org), cap, ctypes.byref(nout))
+    if rc == 2:
+        return cheby_branch(leaves, nparams, coord_cur, coord_prev, nbins, eta, branch_max, cap=nout.value)
+    _check(rc)
+    k = nout.value
+    return out[: k * stride].reshape(k, nparams + 2, 2), org[:k], work.reshape(n, nparams + 2, 2)
+
+
+def cheby_resolve(plan: OraclePlan, leaves, coord_add, coord_cur, coord_init):
+    leaves = np.ascontiguousarray(leaves, np.float64)
+    n = leaves.size // ((plan.nparams + 2) * 2)
+    coords = np.array([*coord_add, *coord_cur, *coord_init], np.float64)
+    idx = np.zeros(n, np.uint64)
+    sh = np.zeros(n, np.float32)
+    lib().lko_cheby_resolve(ctypes.byref(plan.raw), _p(leaves), n, _p(coords), _p(idx), _p(sh))
+    return idx, sh
+
+
 def prune_run(plan: OraclePlan, ffa_fold, thresholds, ref_seg, max_sugg, batch_size, branch_max,
-              n_iters, conservative=False):
+              n_iters, conservative=False, basis="taylor"):
     """One pruning run: returns (stats, leaves, folds, scores) of the final tree."""
     ffa = np.ascontiguousarray(ffa_fold, np.float32).ravel()
     thr = np.ascontiguousarray(thresholds, np.float32)
@@ -448,9 +508,10 @@ def prune_run(plan: OraclePlan, ffa_fold, thresholds, ref_seg, max_sugg, batch_s
     folds = np.zeros(max_sugg * 2 * nbins, np.float32)
     scores = np.zeros(max_sugg, np.float32)
     n = u64()
-    _check(lib().lko_prune_run(ctypes.byref(plan.raw), int(conservative), _p(ffa), _p(thr), thr.size, ref_seg,
-                               max_sugg, batch_size, branch_max, n_iters, _p(stats), ctypes.byref(nstats),
-                               _p(leaves), _p(folds), _p(scores), max_sugg, ctypes.byref(n)))
+    _check(lib().lko_prune_run_basis(ctypes.byref(plan.raw), 1 if basis == "chebyshev" else 0, int(conservative),
+                                     _p(ffa), _p(thr), thr.size, ref_seg, max_sugg, batch_size, branch_max,
+                                     n_iters, _p(stats), ctypes.byref(nstats), _p(leaves), _p(folds), _p(scores),
+                                     max_sugg, ctypes.byref(n)))
     k = n.value
     return (stats[: nstats.value], leaves[: k * stride].reshape(k, plan.nparams + 2, 2),
             folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k])

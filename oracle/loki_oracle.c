@@ -1029,6 +1029,292 @@ void lko_taylor_transform(double* leaves, const uint64_t* indices, uint64_t n, u
     }
 }
 
+/* ======================================================================== */
+/* Chebyshev basis of the pruning leaf step (lib/chebyshev.cpp).            */
+/* Leaves keep the Taylor layout [np + 2][value, error]: rows 0 .. np-1 the  */
+/* Chebyshev coefficients alpha_np .. alpha_1, row np alpha_0, row np+1 f0.  */
+/* ======================================================================== */
+
+/* poly_taylor_to_cheby_{accel,jerk}_batch (lib/chebyshev.cpp:58-93,145-189),
+ * ts = coord_init.second. */
+void lko_taylor_to_cheby(double* leaves, uint64_t n, uint32_t np, double ts) {
+    const uint64_t stride = (np + 2) * 2;
+    const double ts2 = ts * ts;
+    if (np == 2) {
+        const double w2_2 = (ts2 / 2.0) * 0.5;
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + i * stride;
+            const double d2v = lf[0], d2e = lf[1], d1v = lf[2], d1e = lf[3], d0v = lf[4],
+                         d0e = lf[5];
+            lf[0] = d2v * w2_2;
+            lf[2] = d1v * ts;
+            lf[4] = d0v + (d2v * w2_2);
+            const double e2 = d2e * w2_2;
+            const double e1_ts = d1e * ts;
+            lf[1] = e2;
+            lf[3] = e1_ts;
+            lf[5] = sqrt((d0e * d0e) + (e2 * e2));
+        }
+    } else {
+        const double ts3 = ts2 * ts;
+        const double w3_3 = (ts3 / 6.0) * 0.25;
+        const double w2_2 = (ts2 / 2.0) * 0.5;
+        const double w3_1 = (ts3 / 6.0) * 0.75;
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + i * stride;
+            const double d3v = lf[0], d3e = lf[1], d2v = lf[2], d2e = lf[3], d1v = lf[4],
+                         d1e = lf[5], d0v = lf[6], d0e = lf[7];
+            lf[0] = d3v * w3_3;
+            lf[2] = d2v * w2_2;
+            lf[4] = (d1v * ts) + (d3v * w3_1);
+            lf[6] = d0v + (d2v * w2_2);
+            const double e3_3 = d3e * w3_3;
+            const double e2_2 = d2e * w2_2;
+            const double e3_1 = d3e * w3_1;
+            const double e1_ts = d1e * ts;
+            lf[1] = e3_3;
+            lf[3] = e2_2;
+            lf[5] = sqrt((e1_ts * e1_ts) + (e3_1 * e3_1));
+            lf[7] = sqrt((d0e * d0e) + (e2_2 * e2_2));
+        }
+    }
+}
+
+/* poly_cheby_to_taylor_{accel,jerk}_batch (lib/chebyshev.cpp:21-56,95-143),
+ * ts = coord_report.second. */
+void lko_cheby_to_taylor(double* leaves, uint64_t n, uint32_t np, double ts) {
+    const uint64_t stride = (np + 2) * 2;
+    const double inv_ts = 1.0 / ts;
+    const double inv_ts2 = inv_ts * inv_ts;
+    if (np == 2) {
+        const double w2_2 = 4.0 * inv_ts2;
+        const double w1_1 = inv_ts;
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + i * stride;
+            const double a2v = lf[0], a2e = lf[1], a1v = lf[2], a1e = lf[3], a0v = lf[4],
+                         a0e = lf[5];
+            lf[0] = a2v * w2_2;
+            lf[2] = a1v * w1_1;
+            lf[4] = a0v - a2v;
+            lf[1] = a2e * w2_2;
+            lf[3] = a1e * w1_1;
+            lf[5] = sqrt((a0e * a0e) + (a2e * a2e));
+        }
+    } else {
+        const double inv_ts3 = inv_ts2 * inv_ts;
+        const double w3_3 = 24.0 * inv_ts3;
+        const double w2_2 = 4.0 * inv_ts2;
+        const double w1_1 = inv_ts;
+        const double w3_1 = 3.0 * inv_ts;
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + i * stride;
+            const double a3v = lf[0], a3e = lf[1], a2v = lf[2], a2e = lf[3], a1v = lf[4],
+                         a1e = lf[5], a0v = lf[6], a0e = lf[7];
+            lf[0] = a3v * w3_3;
+            lf[2] = a2v * w2_2;
+            lf[4] = (a1v * w1_1) - (a3v * w3_1);
+            lf[6] = a0v - a2v;
+            const double e3_3 = a3e * w3_3;
+            const double e2_2 = a2e * w2_2;
+            const double e1_1 = a1e * w1_1;
+            const double e3_1 = a3e * w3_1;
+            lf[1] = e3_3;
+            lf[3] = e2_2;
+            lf[5] = sqrt((e1_1 * e1_1) + (e3_1 * e3_1));
+            lf[7] = sqrt((a0e * a0e) + (a2e * a2e));
+        }
+    }
+}
+
+/* poly_chebyshev_transform_{accel,jerk}_batch (lib/chebyshev.cpp:316-409):
+ * re-centre from coord_cur (t_cur, s_cur) to coord_next (t_next, s_next);
+ * errors scaled by the diagonal (non-conservative). */
+void lko_cheby_transform(double* leaves, const uint64_t* indices, uint64_t n, uint32_t np,
+                         double t_next, double s_next, double t_cur, double s_cur) {
+    const uint64_t stride = (np + 2) * 2;
+    const double dt = t_next - t_cur;
+    const double p = s_next / s_cur;
+    const double q = dt / s_cur;
+    const double p2 = p * p;
+    const double q2 = q * q;
+    if (np == 2) {
+        const double pq = p * q;
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + indices[i] * stride;
+            const double a2v = lf[0], a2e = lf[1], a1v = lf[2], a1e = lf[3], a0v = lf[4];
+            lf[0] = p2 * a2v;
+            lf[2] = (p * a1v) + (4.0 * pq * a2v);
+            lf[4] = a0v + (q * a1v) + ((p2 + (2.0 * q2) - 1.0) * a2v);
+            lf[1] = p2 * a2e;
+            lf[3] = p * a1e;
+        }
+    } else {
+        const double p3 = p2 * p;
+        for (uint64_t i = 0; i < n; ++i) {
+            double* lf = leaves + indices[i] * stride;
+            const double a3v = lf[0], a3e = lf[1], a2v = lf[2], a2e = lf[3], a1v = lf[4],
+                         a1e = lf[5], a0v = lf[6];
+            lf[0] = p3 * a3v;
+            lf[2] = (6.0 * p2 * q * a3v) + (p2 * a2v);
+            lf[4] = (3.0 * p * (p2 + (4.0 * q2) - 1.0) * a3v) + (4.0 * p * q * a2v) + (p * a1v);
+            lf[6] = (q * ((6.0 * p2) + (4.0 * q2) - 3.0) * a3v) + ((p2 + (2.0 * q2) - 1.0) * a2v) +
+                    (q * a1v) + a0v;
+            lf[1] = p3 * a3e;
+            lf[3] = p2 * a2e;
+            lf[5] = p * a1e;
+        }
+    }
+}
+
+/* Steps and shifts of one (transformed) parent in the Chebyshev basis
+ * (lib/chebyshev.cpp:530-551, 677-702): one step dphi C / f0 for every
+ * coefficient, shift |sigma_cur - step| nbins / (C / f0). */
+static void cheby_steps(const double* lf, uint32_t np, double nbins_d, double dphi,
+                        double* sig_new, double* shift) {
+    const double f0 = lf[(np + 1) * 2];
+    const double dfactor = kCval / f0;
+    const double base_step = dphi * dfactor;
+    const double inv_base = nbins_d / dfactor;
+    for (uint32_t k = 0; k < np; ++k) {
+        sig_new[k] = base_step;
+        shift[k] = fabs(lf[2 * k + 1] - base_step) * inv_base;
+    }
+}
+
+/* poly_chebyshev_branch_{accel,jerk}_batch (lib/chebyshev.cpp:475-779): the
+ * parents are first transformed in place from coord_prev to coord_cur, then
+ * branched as in the Taylor basis (branch_one_param_padded, Cartesian
+ * product with the highest coefficient outermost, alpha_0 and f0 copied). */
+int lko_cheby_branch(double* leaves, uint64_t n, uint32_t np, double t_cur, double s_cur,
+                     double t_prev, double s_prev, uint64_t nbins, double eta,
+                     uint64_t branch_max, double* out, uint64_t* origins, uint64_t cap_out,
+                     uint64_t* n_out) {
+    if (np < 2 || np > 3) {
+        return fail("pruning supports nparams 2 or 3");
+    }
+    const uint64_t stride = (np + 2) * 2;
+    const double nbins_d = (double)nbins;
+    const double dphi = eta / nbins_d;
+    {
+        uint64_t* ident = (uint64_t*)malloc(sizeof(uint64_t) * (n > 0 ? n : 1));
+        for (uint64_t i = 0; i < n; ++i) {
+            ident[i] = i;
+        }
+        lko_cheby_transform(leaves, ident, n, np, t_cur, s_cur, t_prev, s_prev);
+        free(ident);
+    }
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double* lf = leaves + i * stride;
+        double sig_new[3], shift[3], dp;
+        cheby_steps(lf, np, nbins_d, dphi, sig_new, shift);
+        uint64_t prod = 1;
+        for (uint32_t k = 0; k < np; ++k) {
+            uint64_t cnt;
+            if (branch_one(lf[2 * k], lf[2 * k + 1], sig_new[k], shift[k], eta, branch_max, NULL,
+                           &dp, &cnt) != 0) {
+                return 1;
+            }
+            prod *= cnt;
+        }
+        total += prod;
+    }
+    *n_out = total;
+    if (total > cap_out) {
+        return 2;
+    }
+    double* vals = (double*)malloc(sizeof(double) * 3 * (branch_max > 0 ? branch_max : 1));
+    uint64_t o = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double* lf = leaves + i * stride;
+        double sig_new[3], shift[3], dp[3];
+        uint64_t cnt[3] = {1, 1, 1};
+        cheby_steps(lf, np, nbins_d, dphi, sig_new, shift);
+        for (uint32_t k = 0; k < np; ++k) {
+            branch_one(lf[2 * k], lf[2 * k + 1], sig_new[k], shift[k], eta, branch_max,
+                       vals + k * branch_max, &dp[k], &cnt[k]);
+        }
+        for (uint64_t a = 0; a < cnt[0]; ++a) {
+            for (uint64_t b = 0; b < cnt[1]; ++b) {
+                for (uint64_t c = 0; c < (np == 3 ? cnt[2] : 1); ++c) {
+                    double* d = out + o * stride;
+                    d[0] = vals[a];
+                    d[1] = dp[0];
+                    d[2] = vals[branch_max + b];
+                    d[3] = dp[1];
+                    if (np == 3) {
+                        d[4] = vals[2 * branch_max + c];
+                        d[5] = dp[2];
+                    }
+                    memcpy(d + 2 * np, lf + 2 * np, 4 * sizeof(double));
+                    origins[o] = i;
+                    ++o;
+                }
+            }
+        }
+    }
+    free(vals);
+    return 0;
+}
+
+/* poly_chebyshev_resolve_{accel,jerk}_batch (lib/chebyshev.cpp:961-1097);
+ * co = {t_add, s_add, t_cur, s_cur, t_init, s_init}. */
+void lko_cheby_resolve(const lko_plan* p, const double* leaves, uint64_t n, const double* co,
+                       uint64_t* param_idx, float* phase_shift) {
+    const uint32_t np = p->nparams;
+    const uint32_t L = p->n_levels - 1;
+    const uint64_t stride = (np + 2) * 2;
+    const uint64_t n_accel = p->param_counts[L][np - 2];
+    const uint64_t n_freq = p->param_counts[L][np - 1];
+    const double a_min = p->limits[2 * (np - 2)], a_max = p->limits[2 * (np - 2) + 1];
+    const double f_min = p->limits[2 * (np - 1)], f_max = p->limits[2 * (np - 1) + 1];
+    const double t0_add = co[0], t0_cur = co[2], scale_cur = co[3], t0_init = co[4];
+    const double dt_add = t0_add - t0_cur;
+    const double dt_init = t0_init - t0_cur;
+    const double inv_ts = 1.0 / scale_cur;
+    const double inv_ts2 = inv_ts * inv_ts;
+    if (np == 2) {
+        const double dt = dt_add - dt_init;
+        const double dt2 = ((dt_add * dt_add) - (dt_init * dt_init));
+        for (uint64_t i = 0; i < n; ++i) {
+            const double* lf = leaves + i * stride;
+            const double alpha_2 = lf[0], alpha_1 = lf[2], f0 = lf[6];
+            const double a_new = 4.0 * alpha_2 * inv_ts2;
+            const double delta_v = 4.0 * alpha_2 * inv_ts2 * dt;
+            const double delta_d = (alpha_1 * inv_ts * dt) + (2.0 * alpha_2 * inv_ts2 * dt2);
+            const double f_new = f0 * (1.0 - (delta_v * kInvCval));
+            const double delay_rel = delta_d * kInvCval;
+            const uint64_t ia = lko_nearest_idx(a_new, a_min, a_max, n_accel);
+            const uint64_t jf = lko_nearest_idx(f_new, f_min, f_max, n_freq);
+            param_idx[i] = (ia * n_freq) + jf;
+            phase_shift[i] = lko_phase_idx(dt, f0, p->nbins, delay_rel);
+        }
+    } else {
+        const double dt2_add = dt_add * dt_add;
+        const double dt2_init = dt_init * dt_init;
+        const double dt = dt_add - dt_init;
+        const double dt2 = dt2_add - dt2_init;
+        const double dt3 = (dt2_add * dt_add) - (dt2_init * dt_init);
+        const double inv_ts3 = inv_ts2 * inv_ts;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double* lf = leaves + i * stride;
+            const double alpha_3 = lf[0], alpha_2 = lf[2], alpha_1 = lf[4], f0 = lf[8];
+            const double a_new = (4.0 * alpha_2 * inv_ts2) + (24.0 * alpha_3 * dt_add * inv_ts3);
+            const double delta_v =
+                ((4.0 * alpha_2 * inv_ts2) * dt) + ((12.0 * alpha_3 * inv_ts3) * dt2);
+            const double delta_d = ((alpha_1 - (3.0 * alpha_3)) * inv_ts * dt) +
+                                   ((2.0 * alpha_2 * inv_ts2) * dt2) +
+                                   ((4.0 * alpha_3 * inv_ts3) * dt3);
+            const double f_new = f0 * (1.0 - (delta_v * kInvCval));
+            const double delay_rel = delta_d * kInvCval;
+            phase_shift[i] = lko_phase_idx(dt, f0, p->nbins, delay_rel);
+            const uint64_t ia = lko_nearest_idx(a_new, a_min, a_max, n_accel);
+            const uint64_t jf = lko_nearest_idx(f_new, f_min, f_max, n_freq);
+            param_idx[i] = (ia * n_freq) + jf;
+        }
+    }
+}
+
 /* kernels::shift_add_linear_batch + shift_add_linear_with_buffer
  * (lib/kernels.cpp:118-146,1328-1355): tree fold unshifted, FFA fold rotated
  * right by round(shift). The tree index is formed in 32 bits as there. */
@@ -1226,9 +1512,28 @@ int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
                   uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
                   lko_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
                   float* folds_out, float* scores_out, uint64_t cap_out, uint64_t* n_out) {
+    return lko_prune_run_basis(p, 0, conservative, ffa_fold, thresholds, n_thresholds, ref_seg,
+                               max_sugg, batch_size, branch_max, n_iters, stats, n_stats,
+                               leaves_out, folds_out, scores_out, cap_out, n_out);
+}
+
+/* basis 0: Taylor (lib/dynamic.cpp:155-310); basis 1: Chebyshev
+ * (BaseChebyshevPruneDPFuncts / PrunePolyChebyshevDPFuncts,
+ * lib/dynamic.cpp:203-240,381-450): seeds converted to the Chebyshev basis,
+ * the branch transforms the parents from coord_prev to coord_cur, and the
+ * conservative tile is rejected. */
+int lko_prune_run_basis(const lko_plan* p, int basis, int conservative, const float* ffa_fold,
+                        const float* thresholds, uint64_t n_thresholds, uint64_t ref_seg,
+                        uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max,
+                        uint64_t n_iters, lko_prune_stats* stats, uint64_t* n_stats,
+                        double* leaves_out, float* folds_out, float* scores_out, uint64_t cap_out,
+                        uint64_t* n_out) {
     const uint32_t np = p->nparams;
     if (np < 2 || np > 3) {
         return fail("pruning supports nparams 2 or 3");
+    }
+    if (basis == 1 && conservative) {
+        return fail("Conservative tile not implemented for Chebyshev basis");
     }
     const uint32_t L = p->n_levels - 1;
     const uint64_t nseg = p->nsegments[L];
@@ -1271,6 +1576,11 @@ int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
         rc = 1;
         goto done;
     }
+    if (basis == 1) {
+        double ci0, cs0;
+        mo_coord(order, 0, tseg, &ci0, &cs0);
+        lko_taylor_to_cheby(t.leaves, ncoords, np, cs0);
+    }
     memcpy(t.folds, seg0, ncoords * fs * sizeof(float));
     lko_snr_boxcar_3d_max(seg0, ncoords, nbins, p->widths, p->n_widths, t.scores);
     t.size = ncoords;
@@ -1300,8 +1610,9 @@ int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
         const uint64_t n_branches = t.size_old;
         uint64_t n_leaves = 0, n_phy = 0;
         float smin = FLT_MAX, smax = -FLT_MAX;
-        double ci[2], cn[2], cc[2], ca[2];
+        double ci[2], cn[2], cc[2], ca[2], cp[2];
         mo_coord(order, 0, tseg, &ci[0], &ci[1]);
+        mo_coord(order, level - 1, tseg, &cp[0], &cp[1]);
         mo_coord(order, level, tseg, &cn[0], &cn[1]);
         mo_current_coord(order, level, tseg, &cc[0], &cc[1]);
         mo_segment_coord(order, level, tseg, &ca[0], &ca[1]);
@@ -1323,9 +1634,13 @@ int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
             }
             processed += nb;
             uint64_t nl = 0;
-            const int brc = lko_taylor_branch(t.leaves + pstart * ls, nb, np, cc[0], cc[1], nbins,
-                                              p->eta, branch_max, b_leaves, b_org, max_branched,
-                                              &nl);
+            const int brc =
+                basis == 1 ? lko_cheby_branch(t.leaves + pstart * ls, nb, np, cc[0], cc[1], cp[0],
+                                              cp[1], nbins, p->eta, branch_max, b_leaves, b_org,
+                                              max_branched, &nl)
+                           : lko_taylor_branch(t.leaves + pstart * ls, nb, np, cc[0], cc[1],
+                                               nbins, p->eta, branch_max, b_leaves, b_org,
+                                               max_branched, &nl);
             if (brc == 2) {
                 rc = fail("Branch factor exceeded workspace size:n_leaves_batch <= "
                           "max_branched_leaves");
@@ -1341,7 +1656,11 @@ int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
                 t.read_consumed += nb;
                 continue;
             }
-            lko_taylor_resolve(p, b_leaves, nl, coords, b_pidx, b_shift);
+            if (basis == 1) {
+                lko_cheby_resolve(p, b_leaves, nl, coords, b_pidx, b_shift);
+            } else {
+                lko_taylor_resolve(p, b_leaves, nl, coords, b_pidx, b_shift);
+            }
             lko_shift_add_batch(t.folds, b_org, seg, b_pidx, b_shift, b_folds, nbins, nl, pstart,
                                 t.cap);
             const uint64_t npass =
@@ -1354,7 +1673,11 @@ int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
                 t.read_consumed += nb;
                 continue;
             }
-            lko_taylor_transform(b_leaves, b_idx, npass, np, cn[0], cc[0], conservative);
+            if (basis == 1) {
+                lko_cheby_transform(b_leaves, b_idx, npass, np, cn[0], cn[1], cc[0], cc[1]);
+            } else {
+                lko_taylor_transform(b_leaves, b_idx, npass, np, cn[0], cc[0], conservative);
+            }
             cur_thr = wt_add_batch(&t, b_leaves, b_folds, b_scores, b_idx, cur_thr, npass);
             t.read_consumed += nb;
         }

@@ -200,6 +200,26 @@ typedef struct lko_prune_stats {
  * thresholds[level - 1] is the level's threshold. stats receives n_iters + 1
  * rows at most; the final tree (logical order) is copied out when it fits
  * cap_out. */
+/* Chebyshev basis of the pruning leaf step (lib/chebyshev.cpp). Leaves keep
+ * the Taylor layout; co for resolve = {t_add, s_add, t_cur, s_cur, t_init,
+ * s_init}. lko_cheby_branch transforms `leaves` in place (coord_prev ->
+ * coord_cur) before branching, as the reference does. */
+void lko_taylor_to_cheby(double* leaves, uint64_t n, uint32_t nparams, double ts);
+void lko_cheby_to_taylor(double* leaves, uint64_t n, uint32_t nparams, double ts);
+void lko_cheby_transform(double* leaves, const uint64_t* indices, uint64_t n, uint32_t nparams,
+                         double t_next, double s_next, double t_cur, double s_cur);
+int lko_cheby_branch(double* leaves, uint64_t n, uint32_t nparams, double t_cur, double s_cur,
+                     double t_prev, double s_prev, uint64_t nbins, double eta,
+                     uint64_t branch_max, double* out, uint64_t* origins, uint64_t cap_out,
+                     uint64_t* n_out);
+void lko_cheby_resolve(const lko_plan* plan, const double* leaves, uint64_t n, const double* co,
+                       uint64_t* param_idx, float* phase_shift);
+int lko_prune_run_basis(const lko_plan* plan, int basis, int conservative, const float* ffa_fold,
+                        const float* thresholds, uint64_t n_thresholds, uint64_t ref_seg,
+                        uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max,
+                        uint64_t n_iters, lko_prune_stats* stats, uint64_t* n_stats,
+                        double* leaves_out, float* folds_out, float* scores_out, uint64_t cap_out,
+                        uint64_t* n_out);
 int lko_prune_run(const lko_plan* plan, int conservative, const float* ffa_fold,
                   const float* thresholds, uint64_t n_thresholds, uint64_t ref_seg,
                   uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,

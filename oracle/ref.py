@@ -97,7 +97,15 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
         L.lkref_branch_max.argtypes = [vp, ctypes.c_int, vp]
         L.lkref_snr_threshold.argtypes = [vp, u64, u64, vp, u64, vp, f32, vp]
         L.lkref_branching_pattern.argtypes = [vp, ctypes.c_int, u64, vp, u64, vp]
+        L.lkref_branching_pattern_basis.argtypes = [vp, ctypes.c_int, ctypes.c_int, u64, vp, u64, vp]
+        L.lkref_taylor_to_cheby.argtypes = [vp, u64, u32, f64, f64]
+        L.lkref_cheby_to_taylor.argtypes = [vp, u64, u32, f64, f64]
+        L.lkref_cheby_branch.argtypes = [vp, u64, u32, f64, f64, f64, f64, u64, f64, u64, vp, vp, vp]
+        L.lkref_cheby_resolve.argtypes = [vp, vp, u64, vp, vp, vp]
+        L.lkref_cheby_transform.argtypes = [vp, u64, vp, u64, u32, f64, f64, f64, f64]
         L.lkref_prune_run.argtypes = [vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64, u64,
+                                      vp, vp, vp, vp, vp, u64, vp]
+        L.lkref_prune_run_basis.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64, u64,
                                       vp, vp, vp, vp, vp, u64, vp]
         _libs[path] = L
     return _libs[path]
@@ -341,6 +349,67 @@ def branching_pattern(cfg: RefCfg, ref_seg=0, conservative=False) -> np.ndarray:
     return out[: n.value].copy()
 
 
+def branching_pattern_basis(cfg: RefCfg, basis="taylor", ref_seg=0, conservative=False) -> np.ndarray:
+    L = lib()
+    out = np.zeros(4096, np.float64)
+    n = u64()
+    _check(L, L.lkref_branching_pattern_basis(ctypes.byref(cfg), 1 if basis == "chebyshev" else 0,
+                                              int(conservative), ref_seg, _p(out), out.size, ctypes.byref(n)))
+    return out[: n.value].copy()
+
+
+def taylor_to_cheby(leaves, nparams, coord_init):
+    L = lib()
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    n = out.size // ((nparams + 2) * 2)
+    _check(L, L.lkref_taylor_to_cheby(_p(out), n, nparams, coord_init[0], coord_init[1]))
+    return out
+
+
+def cheby_to_taylor(leaves, nparams, coord_report):
+    L = lib()
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    n = out.size // ((nparams + 2) * 2)
+    _check(L, L.lkref_cheby_to_taylor(_p(out), n, nparams, coord_report[0], coord_report[1]))
+    return out
+
+
+def cheby_branch(leaves, nparams, coord_cur, coord_prev, nbins, eta, branch_max):
+    """Returns (children, origins, parents transformed to coord_cur)."""
+    L = lib()
+    work = np.array(leaves, np.float64, copy=True, order="C")
+    stride = (nparams + 2) * 2
+    n = work.size // stride
+    out = np.zeros(n * branch_max * stride, np.float64)
+    org = np.zeros(n * branch_max, np.uint64)
+    nout = u64()
+    _check(L, L.lkref_cheby_branch(_p(work), n, nparams, coord_cur[0], coord_cur[1], coord_prev[0],
+                                   coord_prev[1], nbins, eta, branch_max, _p(out), _p(org), ctypes.byref(nout)))
+    k = nout.value
+    return out[: k * stride].reshape(k, nparams + 2, 2), org[:k], work.reshape(n, nparams + 2, 2)
+
+
+def cheby_resolve(cfg: RefCfg, leaves, coord_add, coord_cur, coord_init):
+    L = lib()
+    leaves = np.ascontiguousarray(leaves, np.float64)
+    n = leaves.size // ((cfg.nparams + 2) * 2)
+    coords = np.array([*coord_add, *coord_cur, *coord_init], np.float64)
+    idx = np.zeros(n, np.uint64)
+    sh = np.zeros(n, np.float32)
+    _check(L, L.lkref_cheby_resolve(ctypes.byref(cfg), _p(leaves), n, _p(coords), _p(idx), _p(sh)))
+    return idx, sh
+
+
+def cheby_transform(leaves, indices, nparams, coord_next, coord_cur):
+    L = lib()
+    out = np.array(leaves, np.float64, copy=True, order="C")
+    idx = np.ascontiguousarray(indices, np.uint64)
+    ntot = out.size // ((nparams + 2) * 2)
+    _check(L, L.lkref_cheby_transform(_p(out), ntot, _p(idx), idx.size, nparams, coord_next[0], coord_next[1],
+                                      coord_cur[0], coord_cur[1]))
+    return out
+
+
 def branch_max(cfg: RefCfg, conservative=False) -> int:
     L = lib()
     out = u64()
@@ -349,7 +418,7 @@ def branch_max(cfg: RefCfg, conservative=False) -> int:
 
 
 def prune_run(cfg: RefCfg, ffa_fold, thresholds, ref_seg, max_sugg, batch_size, branch_max_,
-              n_iters, nbins, conservative=False, kind="parity"):
+              n_iters, nbins, conservative=False, kind="parity", basis="taylor"):
     """One reference pruning run: returns (stats, leaves, folds, scores) of the final tree."""
     L = lib(kind)
     ffa = np.ascontiguousarray(ffa_fold, np.float32).ravel()
@@ -361,10 +430,10 @@ def prune_run(cfg: RefCfg, ffa_fold, thresholds, ref_seg, max_sugg, batch_size, 
     folds = np.zeros(max_sugg * 2 * nbins, np.float32)
     scores = np.zeros(max_sugg, np.float32)
     n = u64()
-    _check(L, L.lkref_prune_run(ctypes.byref(cfg), int(conservative), _p(ffa), ffa.size, _p(thr), thr.size,
-                                ref_seg, max_sugg, batch_size, branch_max_, n_iters, _p(stats),
-                                ctypes.byref(nstats), _p(leaves), _p(folds), _p(scores), max_sugg,
-                                ctypes.byref(n)))
+    _check(L, L.lkref_prune_run_basis(1 if basis == "chebyshev" else 0, ctypes.byref(cfg), int(conservative),
+                                      _p(ffa), ffa.size, _p(thr), thr.size, ref_seg, max_sugg, batch_size,
+                                      branch_max_, n_iters, _p(stats), ctypes.byref(nstats), _p(leaves),
+                                      _p(folds), _p(scores), max_sugg, ctypes.byref(n)))
     k = n.value
     return (stats[: nstats.value], leaves[: k * stride].reshape(k, cfg.nparams + 2, 2),
             folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k])

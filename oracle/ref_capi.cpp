@@ -53,6 +53,7 @@
 #include "loki/common/plans.hpp"
 #include "loki/common/types.hpp"
 #include "loki/core/dynamic.hpp"
+#include "loki/core/chebyshev.hpp"
 #include "loki/core/taylor.hpp"
 #include "loki/detection/score.hpp"
 #include "loki/kernels.hpp"
@@ -477,6 +478,85 @@ int lkref_branching_pattern(const lkref_cfg* c, int conservative, uint64_t ref_s
     });
 }
 
+// ---- Chebyshev basis (lib/chebyshev.cpp) -----------------------------------
+
+int lkref_taylor_to_cheby(double* leaves, uint64_t n, uint32_t nparams, double t_init,
+                          double s_init) {
+    return guarded([&] {
+        loki::core::poly_taylor_to_cheby_batch(
+            std::span<double>(leaves, n * (nparams + 2) * 2), {t_init, s_init}, n, nparams);
+    });
+}
+
+int lkref_cheby_to_taylor(double* leaves, uint64_t n, uint32_t nparams, double t_report,
+                          double s_report) {
+    return guarded([&] {
+        loki::core::poly_cheby_to_taylor_batch(
+            std::span<double>(leaves, n * (nparams + 2) * 2), {t_report, s_report}, n, nparams);
+    });
+}
+
+// Branch n parents; leaves_in is transformed in place (coord_prev ->
+// coord_cur) as the reference does. leaves_out must hold n * branch_max.
+int lkref_cheby_branch(double* leaves_in, uint64_t n, uint32_t nparams, double t_cur,
+                       double s_cur, double t_prev, double s_prev, uint64_t nbins, double eta,
+                       uint64_t branch_max, double* leaves_out, uint64_t* origins_out,
+                       uint64_t* n_out) {
+    return guarded([&] {
+        const uint64_t stride = (nparams + 2) * 2;
+        loki::memory::BranchingWorkspace ws(n, branch_max, nparams);
+        std::span<double> in(leaves_in, n * stride);
+        std::span<double> out(leaves_out, n * branch_max * stride);
+        std::span<loki::SizeType> org(reinterpret_cast<loki::SizeType*>(origins_out),
+                                      n * branch_max);
+        *n_out = loki::core::poly_chebyshev_branch_batch(in, out, org, {t_cur, s_cur},
+                                                         {t_prev, s_prev}, nbins, eta,
+                                                         branch_max, n, nparams, ws);
+    });
+}
+
+// coords = {t_add, s_add, t_cur, s_cur, t_init, s_init}.
+int lkref_cheby_resolve(const lkref_cfg* c, const double* leaves, uint64_t n,
+                        const double* coords, uint64_t* param_idx, float* phase_shift) {
+    return guarded([&] {
+        const auto cfg = make_cfg_prune(c, 0);
+        const loki::plans::FFAPlan<float> plan(cfg);
+        const auto& counts = plan.get_param_counts().back();
+        const uint64_t stride = (c->nparams + 2) * 2;
+        loki::core::poly_chebyshev_resolve_batch(
+            std::span<const double>(leaves, n * stride),
+            std::span<loki::SizeType>(reinterpret_cast<loki::SizeType*>(param_idx), n),
+            std::span<float>(phase_shift, n), cfg.get_param_limits(), {coords[0], coords[1]},
+            {coords[2], coords[3]}, {coords[4], coords[5]}, counts[c->nparams - 2],
+            counts[c->nparams - 1], c->nbins, n, c->nparams);
+    });
+}
+
+int lkref_cheby_transform(double* leaves, uint64_t n_leaves_total, const uint64_t* indices,
+                          uint64_t n, uint32_t nparams, double t_next, double s_next,
+                          double t_cur, double s_cur) {
+    return guarded([&] {
+        const uint64_t stride = (nparams + 2) * 2;
+        std::vector<loki::SizeType> idx(indices, indices + n);
+        loki::core::poly_chebyshev_transform_batch(
+            std::span<double>(leaves, n_leaves_total * stride), idx, {t_next, s_next},
+            {t_cur, s_cur}, n, nparams);
+    });
+}
+
+// FFAPlan::get_branching_pattern(basis, ref_seg), basis 0 taylor / 1 chebyshev.
+int lkref_branching_pattern_basis(const lkref_cfg* c, int basis, int conservative,
+                                  uint64_t ref_seg, double* out, uint64_t max_out,
+                                  uint64_t* n_out) {
+    return guarded([&] {
+        const auto cfg = make_cfg_prune(c, conservative);
+        const loki::plans::FFAPlan<float> plan(cfg);
+        const auto bp = plan.get_branching_pattern(basis == 1 ? "chebyshev" : "taylor", ref_seg);
+        *n_out = bp.size();
+        std::copy_n(bp.begin(), std::min<uint64_t>(bp.size(), max_out), out);
+    });
+}
+
 // Per-level statistics (cands::PruneStats fields).
 struct lkref_prune_stats {
     uint64_t level;
@@ -495,12 +575,46 @@ struct lkref_prune_stats {
 // ([nsegments, ncoords, 2, nbins]): seed, then up to n_iters levels (each
 // uses thresholds[level - 1]). stats receives one row for the seed and one
 // per level run; the final tree is copied out in logical order.
+static int prune_run_basis(const char* basis, const lkref_cfg* c, int conservative,
+                           const float* ffa_fold, uint64_t ffa_fold_len, const float* thresholds,
+                           uint64_t n_thresholds, uint64_t ref_seg, uint64_t max_sugg,
+                           uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
+                           lkref_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
+                           float* folds_out, float* scores_out, uint64_t cap_out,
+                           uint64_t* n_out);
+
 int lkref_prune_run(const lkref_cfg* c, int conservative, const float* ffa_fold,
                     uint64_t ffa_fold_len, const float* thresholds, uint64_t n_thresholds,
                     uint64_t ref_seg, uint64_t max_sugg, uint64_t batch_size,
                     uint64_t branch_max, uint64_t n_iters, lkref_prune_stats* stats,
                     uint64_t* n_stats, double* leaves_out, float* folds_out, float* scores_out,
                     uint64_t cap_out, uint64_t* n_out) {
+    return prune_run_basis("taylor", c, conservative, ffa_fold, ffa_fold_len, thresholds,
+                           n_thresholds, ref_seg, max_sugg, batch_size, branch_max, n_iters,
+                           stats, n_stats, leaves_out, folds_out, scores_out, cap_out, n_out);
+}
+
+// The same run with poly_basis "taylor" (basis 0) or "chebyshev" (basis 1).
+int lkref_prune_run_basis(int basis, const lkref_cfg* c, int conservative,
+                          const float* ffa_fold, uint64_t ffa_fold_len, const float* thresholds,
+                          uint64_t n_thresholds, uint64_t ref_seg, uint64_t max_sugg,
+                          uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
+                          lkref_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
+                          float* folds_out, float* scores_out, uint64_t cap_out,
+                          uint64_t* n_out) {
+    return prune_run_basis(basis == 1 ? "chebyshev" : "taylor", c, conservative, ffa_fold,
+                           ffa_fold_len, thresholds, n_thresholds, ref_seg, max_sugg, batch_size,
+                           branch_max, n_iters, stats, n_stats, leaves_out, folds_out,
+                           scores_out, cap_out, n_out);
+}
+
+static int prune_run_basis(const char* basis, const lkref_cfg* c, int conservative,
+                           const float* ffa_fold, uint64_t ffa_fold_len, const float* thresholds,
+                           uint64_t n_thresholds, uint64_t ref_seg, uint64_t max_sugg,
+                           uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
+                           lkref_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
+                           float* folds_out, float* scores_out, uint64_t cap_out,
+                           uint64_t* n_out) {
     return guarded([&] {
         using loki::SizeType;
         const auto cfg = make_cfg_prune(c, conservative);
@@ -510,7 +624,7 @@ int lkref_prune_run(const lkref_cfg* c, int conservative, const float* ffa_fold,
         const SizeType nparams   = cfg.get_nparams();
         const SizeType nbins     = cfg.get_nbins();
         auto funcs = loki::core::create_prune_dp_functs<float>(
-            "taylor", plan.get_param_counts().back(), plan.get_dparams_actual().back(),
+            basis, plan.get_param_counts().back(), plan.get_dparams_actual().back(),
             nsegments, tseg, cfg, batch_size, branch_max);
         loki::memory::EPWorkspace<float> ws(batch_size, branch_max, max_sugg,
                                             plan.get_ncoords().back(), nparams, nbins,

@@ -116,20 +116,35 @@ PRUNE_CASES = {
 }
 
 
+# The same runs in the Chebyshev basis (poly_basis "chebyshev"; the
+# reference rejects the conservative tile there).
+CHEBY_CASES = {
+    "prune_cheby_accel_nb16": (16384, 8e-3, 16, 1.0, [[-1000.0, 1000.0], [10.0, 10.3]], 2048, 5,
+                               64, 8, 1.0, 2.5, False),
+    "prune_cheby_jerk_nb16": (16384, 8e-3, 16, 1.0, [[-100.0, 100.0], [-900.0, 900.0], [10.0, 10.2]],
+                              2048, 6, 64, 8, 1.0, 2.5, False),
+}
+
+
 def prune_fixtures() -> None:
     """Inputs (the reference's final FFA fold) and outputs of whole pruning
     runs (PruneImpl over the reference's PruneDPFuncts and WorldTree), plus
     branching patterns."""
-    for name, (ns, ts, nb, eta, lims, bf, seed, ms, bs, lo, hi, cons) in PRUNE_CASES.items():
+    cases = [(n, c, "taylor") for n, c in PRUNE_CASES.items()] + [(n, c, "chebyshev") for n, c in CHEBY_CASES.items()]
+    for name, (ns, ts, nb, eta, lims, bf, seed, ms, bs, lo, hi, cons), basis in cases:
         cfg = ref.make_cfg(ns, ts, nb, eta, lims, bseg_ffa=bf)
         ffa = ref.RefFFA(cfg)
         ts_e, ts_v = series(ns, seed)
         fold = ffa.execute(ts_e, ts_v).copy()
         nseg = int(ffa.nsegments[-1])
-        bmax = ref.branch_max(cfg, cons)
+        bp0 = ref.branching_pattern_basis(cfg, basis, 0, cons)
+        bmax = max(int(np.ceil(bp0.max() * 2)), 32)
+        if basis == "taylor":
+            assert bmax == ref.branch_max(cfg, cons)
         thr = np.linspace(lo, hi, nseg - 1).astype(np.float32)
         ref_seg = nseg // 2
-        stats, leaves, folds, scores = ref.prune_run(cfg, fold, thr, ref_seg, ms, bs, bmax, nseg - 1, nb, cons)
+        stats, leaves, folds, scores = ref.prune_run(cfg, fold, thr, ref_seg, ms, bs, bmax, nseg - 1, nb, cons,
+                                                     basis=basis)
         np.savez_compressed(
             os.path.join(OUT, f"{name}.npz"),
             nsamps=ns, tsamp=ts, nbins=nb, eta=eta, param_limits=np.array(lims, dtype=np.float64),
@@ -138,9 +153,9 @@ def prune_fixtures() -> None:
             stats=np.stack([stats[k].astype(np.float64) for k in
                             ("level", "seg_idx", "n_branches", "n_leaves", "n_leaves_phy",
                              "n_leaves_surv", "threshold", "score_min", "score_max")], axis=1),
-            leaves=leaves, folds=folds, scores=scores,
-            branching_pattern=ref.branching_pattern(cfg, 0, cons),
-            branching_pattern_ref=ref.branching_pattern(cfg, ref_seg, cons),
+            leaves=leaves, folds=folds, scores=scores, basis=basis,
+            branching_pattern=bp0,
+            branching_pattern_ref=ref.branching_pattern_basis(cfg, basis, ref_seg, cons),
         )
         print(name, "nsegments", nseg, "survivors", leaves.shape[0])
 
