@@ -324,6 +324,22 @@ int lk_prune_run(lk_prune* pr, const float* d_ffa_fold, uint64_t ref_seg,
  * average branching factor of each of the nsegments - 1 pruning levels. */
 int lk_plan_branching_pattern(const lk_plan* plan, uint64_t ref_seg, int conservative,
                               double* out, uint64_t max_out, uint64_t* n_out);
+/* Polynomial basis of a pruning search (the reference's poly_basis):
+ * Taylor (PrunePolyTaylorDPFuncts) or Chebyshev (PrunePolyChebyshevDPFuncts,
+ * lib/dynamic.cpp:381-450; lib/chebyshev.cpp). */
+enum lk_poly_basis { LK_BASIS_TAYLOR = 0, LK_BASIS_CHEBYSHEV = 1 };
+/* lk_prune_create with a basis. Chebyshev: seeds converted to the basis,
+ * parents re-centred (coord_prev -> coord_cur) in the branch, and
+ * conservative = 1 rejected (the reference throws); branch_max 0 applies
+ * EPMultiPass's rule to the basis's branching pattern. */
+int lk_prune_create_basis(const lk_plan* plan, uint64_t max_sugg, uint64_t batch_size,
+                          uint64_t branch_max, int conservative, int poly_basis, int device,
+                          lk_prune** out);
+/* FFAPlan::get_branching_pattern(basis, ref_seg): generate_bp_poly_taylor or
+ * generate_bp_poly_chebyshev (lib/chebyshev.cpp:1796-1890). */
+int lk_plan_branching_pattern_basis(const lk_plan* plan, uint64_t ref_seg, int conservative,
+                                    int poly_basis, double* out, uint64_t max_out,
+                                    uint64_t* n_out);
 /* Surviving leaves after lk_prune_run, in the world tree's logical order.
  * Any of the device outputs may be NULL. */
 int lk_prune_tree_size(const lk_prune* pr, uint64_t* n);
@@ -349,6 +365,31 @@ int lk_taylor_resolve(const lk_plan* plan, const double* d_leaves, uint64_t n,
 int lk_taylor_transform(const lk_plan* plan, double* d_leaves, uint64_t n_leaves,
                         const uint32_t* d_indices, uint64_t n, double t_next, double t_cur,
                         int conservative, lk_stream_t stream);
+/* Chebyshev-basis steps (lib/chebyshev.cpp). Leaves keep the Taylor layout:
+ * rows 0 .. nparams-1 the coefficients alpha_nparams .. alpha_1, row nparams
+ * alpha_0, row nparams + 1 f0, each (value, error). */
+/* poly_taylor_to_cheby_batch (ts = scale of coord_init) and
+ * poly_cheby_to_taylor_batch (ts = scale of coord_report), in place. */
+int lk_taylor_to_cheby(double* d_leaves, uint64_t n, uint32_t nparams, double ts,
+                       lk_stream_t stream);
+int lk_cheby_to_taylor(double* d_leaves, uint64_t n, uint32_t nparams, double ts,
+                       lk_stream_t stream);
+/* poly_chebyshev_branch_batch: d_leaves (n parents) are re-centred in place
+ * from (t_prev, s_prev) to (t_cur, s_cur), then branched as lk_taylor_branch
+ * with the Chebyshev steps. Synchronises the stream. */
+int lk_cheby_branch(const lk_plan* plan, double* d_leaves, uint64_t n, double t_cur, double s_cur,
+                    double t_prev, double s_prev, uint64_t branch_max, double* d_out,
+                    uint32_t* d_origins, uint64_t max_out, uint64_t* n_out, lk_stream_t stream);
+/* poly_chebyshev_resolve_batch; coords as for lk_taylor_resolve. */
+int lk_cheby_resolve(const lk_plan* plan, const double* d_leaves, uint64_t n,
+                     const double* coords, uint32_t* d_param_idx, float* d_phase_shift,
+                     lk_stream_t stream);
+/* poly_chebyshev_transform_batch from (t_cur, s_cur) to (t_next, s_next),
+ * in place on the leaves named by d_indices (checked as lk_taylor_transform).
+ * Synchronises the stream. */
+int lk_cheby_transform(const lk_plan* plan, double* d_leaves, uint64_t n_leaves,
+                       const uint32_t* d_indices, uint64_t n, double t_next, double s_next,
+                       double t_cur, double s_cur, lk_stream_t stream);
 /* out[i] = folds_tree[indices_tree[i] + physical_start, wrapped once at
  *          capacity] + rotate_right(folds_ffa[indices_ffa[i]], round(phase_shift[i])).
  * n_ffa: rows in d_folds_ffa. A tree index still >= capacity after the wrap

@@ -167,6 +167,13 @@ SIGNATURES = [
     ("lk_taylor_branch", i32, [vp, vp, u64, f64, u64, vp, vp, u64, vp, vp]),
     ("lk_taylor_resolve", i32, [vp, vp, u64, vp, vp, vp, vp]),
     ("lk_taylor_transform", i32, [vp, vp, u64, vp, u64, f64, f64, i32, vp]),
+    ("lk_prune_create_basis", i32, [vp, u64, u64, u64, i32, i32, i32, vp]),
+    ("lk_plan_branching_pattern_basis", i32, [vp, u64, i32, i32, vp, u64, vp]),
+    ("lk_taylor_to_cheby", i32, [vp, u64, u32, f64, vp]),
+    ("lk_cheby_to_taylor", i32, [vp, u64, u32, f64, vp]),
+    ("lk_cheby_branch", i32, [vp, vp, u64, f64, f64, f64, f64, u64, vp, vp, u64, vp, vp]),
+    ("lk_cheby_resolve", i32, [vp, vp, u64, vp, vp, vp, vp]),
+    ("lk_cheby_transform", i32, [vp, vp, u64, vp, u64, f64, f64, f64, f64, vp]),
     ("lk_shift_add_batch", i32, [vp, vp, vp, u64, vp, vp, vp, u32, u64, u64, u64, vp]),
     ("lk_score_filter", i32, [vp, u64, u32, vp, u32, f32, vp, vp, vp, vp]),
 ]

@@ -477,6 +477,50 @@ int lk_prune_create(const lk_plan* plan, uint64_t max_sugg, uint64_t batch_size,
     });
 }
 
+int lk_prune_create_basis(const lk_plan* plan, uint64_t max_sugg, uint64_t batch_size,
+                          uint64_t branch_max, int conservative, int poly_basis, int device,
+                          lk_prune** out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        lk::require(poly_basis == LK_BASIS_TAYLOR || poly_basis == LK_BASIS_CHEBYSHEV,
+                    "Unknown poly_basis. Valid options: 'taylor', 'chebyshev'");
+        lk::require(!(poly_basis == LK_BASIS_CHEBYSHEV && conservative != 0),
+                    "Conservative tile not implemented for Chebyshev basis");
+        auto h = std::make_unique<lk_prune>();
+        if (branch_max == 0) {
+            branch_max = plan->plan.prune_branch_max(conservative != 0, poly_basis);
+        }
+        h->exec = std::make_unique<lk::PruneExec>(plan->plan, max_sugg, batch_size, branch_max,
+                                                  conservative != 0, device, poly_basis);
+        *out = h.release();
+    });
+}
+
+int lk_plan_branching_pattern_basis(const lk_plan* plan, uint64_t ref_seg, int conservative,
+                                    int poly_basis, double* out, uint64_t max_out,
+                                    uint64_t* n_out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(n_out, "n_out");
+        lk::require(poly_basis == LK_BASIS_TAYLOR || poly_basis == LK_BASIS_CHEBYSHEV,
+                    "Invalid poly_basis for branching pattern generation");
+        if (poly_basis == LK_BASIS_CHEBYSHEV) {
+            lk::require(conservative == 0,
+                        "Conservative tile is not supported for chebyshev branching pattern "
+                        "generation");
+        }
+        const auto bp = poly_basis == LK_BASIS_CHEBYSHEV
+                            ? plan->plan.branching_pattern_cheby(ref_seg)
+                            : plan->plan.branching_pattern(ref_seg, conservative != 0);
+        *n_out = bp.size();
+        if (max_out > 0) {
+            need(out, "out");
+        }
+        std::copy_n(bp.begin(), std::min<uint64_t>(bp.size(), max_out), out);
+    });
+}
+
 void lk_prune_destroy(lk_prune* pr) { delete pr; }
 
 int lk_plan_branching_pattern(const lk_plan* plan, uint64_t ref_seg, int conservative,
@@ -584,6 +628,75 @@ int lk_taylor_transform(const lk_plan* plan, double* d_leaves, uint64_t n_leaves
         }
         lk::taylor_transform(plan->plan, d_leaves, n_leaves, d_indices, n, t_next, t_cur,
                              conservative != 0, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_taylor_to_cheby(double* d_leaves, uint64_t n, uint32_t nparams, double ts,
+                       lk_stream_t stream) {
+    return guarded([&] {
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+        }
+        lk::basis_convert(d_leaves, n, nparams, ts, true, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_cheby_to_taylor(double* d_leaves, uint64_t n, uint32_t nparams, double ts,
+                       lk_stream_t stream) {
+    return guarded([&] {
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+        }
+        lk::basis_convert(d_leaves, n, nparams, ts, false, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_cheby_branch(const lk_plan* plan, double* d_leaves, uint64_t n, double t_cur, double s_cur,
+                    double t_prev, double s_prev, uint64_t branch_max, double* d_out,
+                    uint32_t* d_origins, uint64_t max_out, uint64_t* n_out, lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(n_out, "n_out");
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+        }
+        if (max_out > 0) {
+            need(d_out, "d_out");
+            need(d_origins, "d_origins");
+        }
+        *n_out = lk::cheby_branch(plan->plan, d_leaves, n, t_cur, s_cur, t_prev, s_prev,
+                                  branch_max, d_out, d_origins, max_out,
+                                  reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_cheby_resolve(const lk_plan* plan, const double* d_leaves, uint64_t n,
+                     const double* coords, uint32_t* d_param_idx, float* d_phase_shift,
+                     lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(coords, "coords");
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+            need(d_param_idx, "d_param_idx");
+            need(d_phase_shift, "d_phase_shift");
+        }
+        lk::cheby_resolve(plan->plan, d_leaves, n, coords, d_param_idx, d_phase_shift,
+                          reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_cheby_transform(const lk_plan* plan, double* d_leaves, uint64_t n_leaves,
+                       const uint32_t* d_indices, uint64_t n, double t_next, double s_next,
+                       double t_cur, double s_cur, lk_stream_t stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        if (n > 0) {
+            need(d_leaves, "d_leaves");
+            need(d_indices, "d_indices");
+        }
+        lk::cheby_transform(plan->plan, d_leaves, n_leaves, d_indices, n, t_next, s_next, t_cur,
+                            s_cur, reinterpret_cast<cudaStream_t>(stream));
     });
 }
 

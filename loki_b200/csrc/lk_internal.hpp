@@ -69,7 +69,8 @@ struct Plan {
     std::vector<double> param_grid(uint32_t level, uint32_t iparam) const;
     std::vector<double> dparams_at(double tseg_cur, int kind) const;
     std::vector<double> branching_pattern(uint64_t ref_seg, bool conservative) const;
-    uint64_t prune_branch_max(bool conservative) const;
+    std::vector<double> branching_pattern_cheby(uint64_t ref_seg) const;
+    uint64_t prune_branch_max(bool conservative, int basis = 0) const;
 };
 
 Plan make_plan(const lk_config& cfg);

@@ -44,8 +44,9 @@ struct TreeState {
 // ref_seg PruneImpl, lib/prune.cpp:40-226,429-620).
 class PruneExec {
 public:
+    // basis: 0 Taylor, 1 Chebyshev (PrunePolyChebyshevDPFuncts, lib/dynamic.cpp:381-450).
     PruneExec(const Plan& plan, uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max,
-              bool conservative, int device);
+              bool conservative, int device, int basis = 0);
     // Seeds from segment ref_seg of d_ffa_fold ([nsegments, ncoords, 2, nbins])
     // and runs up to n_iters levels with thresholds[level - 1]. Returns one
     // stats row for the seed and one per level run (stops early when no
@@ -74,6 +75,7 @@ private:
     int m_device;
     uint64_t m_cap, m_batch, m_branch_max;
     bool m_conservative;
+    int m_basis = 0;
     uint32_t m_np, m_nbins, m_ls;
     uint64_t m_ncoords, m_nseg;
     double m_tseg;
@@ -101,6 +103,20 @@ void taylor_resolve(const Plan& plan, const double* d_leaves, uint64_t n, const 
 void taylor_transform(const Plan& plan, double* d_leaves, uint64_t n_leaves,
                       const uint32_t* d_indices, uint64_t n, double t_next, double t_cur,
                       bool conservative, cudaStream_t s);
+// Chebyshev basis (lib/chebyshev.cpp). cheby_branch re-centres d_leaves in
+// place (coord_prev -> coord_cur) before branching, as the reference does;
+// coords for resolve = {t_add, s_add, t_cur, s_cur, t_init, s_init}.
+uint64_t cheby_branch(const Plan& plan, double* d_leaves, uint64_t n, double t_cur, double s_cur,
+                      double t_prev, double s_prev, uint64_t branch_max, double* d_out,
+                      uint32_t* d_origins, uint64_t max_out, cudaStream_t s);
+void cheby_resolve(const Plan& plan, const double* d_leaves, uint64_t n, const double* coords,
+                   uint32_t* d_param_idx, float* d_phase_shift, cudaStream_t s);
+void cheby_transform(const Plan& plan, double* d_leaves, uint64_t n_leaves,
+                     const uint32_t* d_indices, uint64_t n, double t_next, double s_next,
+                     double t_cur, double s_cur, cudaStream_t s);
+// poly_taylor_to_cheby (to_cheby, ts = coord_init scale) / poly_cheby_to_taylor.
+void basis_convert(double* d_leaves, uint64_t n, uint32_t nparams, double ts, bool to_cheby,
+                   cudaStream_t s);
 void shift_add_batch(const float* d_folds_tree, const uint32_t* d_indices_tree,
                      const float* d_folds_ffa, uint64_t n_ffa, const uint32_t* d_indices_ffa,
                      const float* d_phase_shift, float* d_out, uint32_t nbins, uint64_t n,

@@ -224,9 +224,147 @@ std::vector<double> Plan::branching_pattern(uint64_t ref_seg, bool conservative)
     return bp;
 }
 
-// EPMultiPass's branch_max (lib/prune.cpp:648-651): the pattern of ref_seg 0.
-uint64_t Plan::prune_branch_max(bool conservative) const {
-    const std::vector<double> bp = branching_pattern(0, conservative);
+// generate_bp_poly_chebyshev (lib/chebyshev.cpp:1796-1890): the branching
+// pattern of a pruning run in the Chebyshev basis, with the errors converted by
+// transforms::taylor_to_cheby_errors_batch and rescaled between coordinates by
+// shift_cheb_errors_batch (lib/transforms.cpp:164-235), steps and shifts from
+// poly_cheb_step_vec / poly_cheb_shift_vec (lib/psr_utils.cpp:157-194).
+std::vector<double> Plan::branching_pattern_cheby(uint64_t ref_seg) const {
+    require(nparams >= 2 && nparams <= 4, "branching pattern needs 2 <= nparams <= 4");
+    const uint32_t L = n_levels - 1;
+    const uint64_t nseg = nsegments[L];
+    require(ref_seg < nseg, "ref_idx must be less than nsegments.");
+    const double tseg = tsegments[L];
+    const uint32_t np = nparams;
+    const std::vector<double> f0 = param_grid(L, np - 1);
+    const uint64_t nf = f0.size();
+    std::vector<uint64_t> order{ref_seg};
+    for (uint64_t d = 1; order.size() < nseg; ++d) {
+        if (d <= ref_seg) {
+            order.push_back(ref_seg - d);
+        }
+        if (ref_seg + d < nseg && order.size() < nseg) {
+            order.push_back(ref_seg + d);
+        }
+    }
+    auto coord = [&](uint64_t level) {
+        uint64_t mn = order[0], mx = order[0];
+        for (uint64_t i = 1; i <= level; ++i) {
+            mn = std::min(mn, order[i]);
+            mx = std::max(mx, order[i]);
+        }
+        const double ref_val = (static_cast<double>(mn) + static_cast<double>(mx) + 1.0) / 2.0;
+        const double scale_val = ref_val - static_cast<double>(mn);
+        return std::pair<double, double>{ref_val * tseg, scale_val * tseg};
+    };
+    std::vector<double> weights(nf, 1.0), bp(nseg - 1, 0.0);
+    std::vector<double> cur(nf * np), nxt(nf * np, 0.0), dnew(nf * np, 0.0), shift(nf * np, 0.0);
+    std::vector<double> nbr(nf, 1.0);
+    for (uint64_t i = 0; i < nf; ++i) {
+        for (uint32_t j = 0; j < np; ++j) {
+            cur[i * np + j] = dparams_actual[L][j];
+        }
+        cur[i * np + np - 1] = cur[i * np + np - 1] * (kCval / f0[i]);
+    }
+    {  // taylor_to_cheby_errors_batch at coord_init's scale
+        const double ts = coord(0).second;
+        const double ts2 = ts * ts;
+        const double ts3 = ts2 * ts;
+        const double ts4 = ts3 * ts;
+        const double w2_2 = (ts2 / 2.0) * 0.5;
+        const double w4_4 = (ts4 / 24.0) * 0.125;
+        const double w3_3 = (ts3 / 6.0) * 0.25;
+        const double w4_2 = (ts4 / 24.0) * 0.5;
+        const double w3_1 = (ts3 / 6.0) * 0.75;
+        for (uint64_t i = 0; i < nf; ++i) {
+            double* e = cur.data() + i * np;
+            if (np == 2) {
+                const double d2 = e[0], d1 = e[1];
+                e[0] = d2 * w2_2;
+                e[1] = d1 * ts;
+            } else if (np == 3) {
+                const double d3 = e[0], d2 = e[1], d1 = e[2];
+                const double e3_1 = d3 * w3_1;
+                const double e1_ts = d1 * ts;
+                e[0] = d3 * w3_3;
+                e[1] = d2 * w2_2;
+                e[2] = std::sqrt((e1_ts * e1_ts) + (e3_1 * e3_1));
+            } else {
+                const double d4 = e[0], d3 = e[1], d2 = e[2], d1 = e[3];
+                const double e4_2 = d4 * w4_2;
+                const double e2_2 = d2 * w2_2;
+                const double e3_1 = d3 * w3_1;
+                const double e1_ts = d1 * ts;
+                e[0] = d4 * w4_4;
+                e[1] = d3 * w3_3;
+                e[2] = std::sqrt((e2_2 * e2_2) + (e4_2 * e4_2));
+                e[3] = std::sqrt((e1_ts * e1_ts) + (e3_1 * e3_1));
+            }
+        }
+    }
+    // shift_cheb_errors_batch: error j scaled by (scale_next / scale_cur)^(np - j)
+    auto rescale = [&](std::vector<double>& v, double scale_next, double scale_cur) {
+        const double p = scale_next / scale_cur;
+        for (uint64_t i = 0; i < nf; ++i) {
+            for (uint32_t j = 0; j < np; ++j) {
+                v[i * np + j] = v[i * np + j] * std::pow(p, static_cast<double>(np - j));
+            }
+        }
+    };
+    const double nbins_d = static_cast<double>(cfg.nbins);
+    const double dphi = cfg.eta / nbins_d;
+    for (uint64_t level = 1; level < nseg; ++level) {
+        const auto cp = coord(level - 1);
+        const auto cn = coord(level);
+        const auto cc = std::pair<double, double>{cp.first, cn.second};
+        rescale(cur, cc.second, cp.second);
+        for (uint64_t i = 0; i < nf; ++i) {
+            const double factor = kCval / f0[i];
+            for (uint32_t j = 0; j < np; ++j) {
+                dnew[i * np + j] = dphi * factor;
+            }
+        }
+        const double scale_factor = nbins_d / kCval;
+        for (uint32_t j = 0; j < np; ++j) {
+            for (uint64_t b = 0; b < nf; ++b) {
+                const uint64_t idx = b * np + j;
+                const double diff = std::abs(cur[idx] - dnew[idx]);
+                shift[idx] = diff * scale_factor * f0[b];
+            }
+        }
+        std::fill(nbr.begin(), nbr.end(), 1.0);
+        for (uint64_t i = 0; i < nf; ++i) {
+            for (uint32_t j = 0; j < np; ++j) {
+                const uint64_t idx = i * np + j;
+                if (shift[idx] < (cfg.eta - kFloatEps)) {
+                    nxt[idx] = cur[idx];
+                    continue;
+                }
+                const double ratio = cur[idx] / dnew[idx];
+                const double c = std::ceil(ratio - kFloatEps);
+                const uint64_t num = c < 1.0 ? 1 : static_cast<uint64_t>(c);
+                nbr[i] *= static_cast<double>(num);
+                nxt[idx] = cur[idx] / static_cast<double>(num);
+            }
+        }
+        double children = 0.0, parents = 0.0;
+        for (uint64_t i = 0; i < nf; ++i) {
+            children += weights[i] * nbr[i];
+            parents += weights[i];
+            weights[i] *= nbr[i];
+        }
+        bp[level - 1] = children / parents;
+        rescale(nxt, cn.second, cc.second);
+        cur = nxt;
+    }
+    return bp;
+}
+
+// EPMultiPass's branch_max (lib/prune.cpp:648-651): the pattern of ref_seg 0,
+// in the run's basis (1: Chebyshev).
+uint64_t Plan::prune_branch_max(bool conservative, int basis) const {
+    const std::vector<double> bp =
+        basis == 1 ? branching_pattern_cheby(0) : branching_pattern(0, conservative);
     double mx = bp.empty() ? 0.0 : bp[0];
     for (double v : bp) {
         mx = std::max(mx, v);

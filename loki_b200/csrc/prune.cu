@@ -67,6 +67,7 @@ struct LeafGeom {
     double eta;
     double a_min, a_max, f_min, f_max;
     uint64_t branch_max;
+    uint32_t basis;    // 0 Taylor, 1 Chebyshev
 };
 
 // Per-parameter branching of one parent: values base + i * step (i < count)
@@ -92,7 +93,17 @@ __device__ void branch_params(const double* lf, double dt, const LeafGeom& g, Pa
     const double f0 = lf[(g.np + 1) * 2];
     const double dfactor = kCval / f0;
     double sig_new[3], shift[3];
-    if (g.np == 2) {
+    if (g.basis == 1) {
+        // poly_chebyshev_branch_{accel,jerk}_batch (lib/chebyshev.cpp:
+        // 530-551, 677-702): one step dphi C / f0 for every coefficient,
+        // shift |sigma_cur - step| nbins / (C / f0).
+        const double base_step = dphi * dfactor;
+        const double inv_base = nbins_d / dfactor;
+        for (uint32_t k = 0; k < g.np; ++k) {
+            sig_new[k] = base_step;
+            shift[k] = fabs(lf[2 * k + 1] - base_step) * inv_base;
+        }
+    } else if (g.np == 2) {
         sig_new[0] = dphi * dfactor * 4.0 * inv_dt2;
         sig_new[1] = dphi * dfactor * 1.0 * inv_dt;
         shift[0] = fabs(lf[1] - sig_new[0]) * dt2 * nbins_d / (4.0 * dfactor);
@@ -237,6 +248,95 @@ __global__ void seed_kernel(LeafGeom g, double dp0, double dp1, double dfreq, do
     o[(np + 1) * 2 + 1] = 0;
 }
 
+// poly_taylor_to_cheby_{accel,jerk}_batch (lib/chebyshev.cpp:58-93,145-189),
+// in place, ts = coord_init.second.
+__device__ __forceinline__ void taylor_to_cheby_leaf(double* lf, uint32_t np, double ts) {
+    const double ts2 = ts * ts;
+    if (np == 2) {
+        const double w2_2 = (ts2 / 2.0) * 0.5;
+        const double d2v = lf[0], d2e = lf[1], d1v = lf[2], d1e = lf[3], d0v = lf[4], d0e = lf[5];
+        lf[0] = d2v * w2_2;
+        lf[2] = d1v * ts;
+        lf[4] = d0v + (d2v * w2_2);
+        const double e2 = d2e * w2_2;
+        const double e1_ts = d1e * ts;
+        lf[1] = e2;
+        lf[3] = e1_ts;
+        lf[5] = __dsqrt_rn((d0e * d0e) + (e2 * e2));
+    } else {
+        const double ts3 = ts2 * ts;
+        const double w3_3 = (ts3 / 6.0) * 0.25;
+        const double w2_2 = (ts2 / 2.0) * 0.5;
+        const double w3_1 = (ts3 / 6.0) * 0.75;
+        const double d3v = lf[0], d3e = lf[1], d2v = lf[2], d2e = lf[3], d1v = lf[4], d1e = lf[5],
+                     d0v = lf[6], d0e = lf[7];
+        lf[0] = d3v * w3_3;
+        lf[2] = d2v * w2_2;
+        lf[4] = (d1v * ts) + (d3v * w3_1);
+        lf[6] = d0v + (d2v * w2_2);
+        const double e3_3 = d3e * w3_3;
+        const double e2_2 = d2e * w2_2;
+        const double e3_1 = d3e * w3_1;
+        const double e1_ts = d1e * ts;
+        lf[1] = e3_3;
+        lf[3] = e2_2;
+        lf[5] = __dsqrt_rn((e1_ts * e1_ts) + (e3_1 * e3_1));
+        lf[7] = __dsqrt_rn((d0e * d0e) + (e2_2 * e2_2));
+    }
+}
+
+// poly_cheby_to_taylor_{accel,jerk}_batch (lib/chebyshev.cpp:21-56,95-143),
+// in place, ts = coord_report.second.
+__device__ __forceinline__ void cheby_to_taylor_leaf(double* lf, uint32_t np, double ts) {
+    const double inv_ts = 1.0 / ts;
+    const double inv_ts2 = inv_ts * inv_ts;
+    if (np == 2) {
+        const double w2_2 = 4.0 * inv_ts2;
+        const double w1_1 = inv_ts;
+        const double a2v = lf[0], a2e = lf[1], a1v = lf[2], a1e = lf[3], a0v = lf[4], a0e = lf[5];
+        lf[0] = a2v * w2_2;
+        lf[2] = a1v * w1_1;
+        lf[4] = a0v - a2v;
+        lf[1] = a2e * w2_2;
+        lf[3] = a1e * w1_1;
+        lf[5] = __dsqrt_rn((a0e * a0e) + (a2e * a2e));
+    } else {
+        const double inv_ts3 = inv_ts2 * inv_ts;
+        const double w3_3 = 24.0 * inv_ts3;
+        const double w2_2 = 4.0 * inv_ts2;
+        const double w1_1 = inv_ts;
+        const double w3_1 = 3.0 * inv_ts;
+        const double a3v = lf[0], a3e = lf[1], a2v = lf[2], a2e = lf[3], a1v = lf[4], a1e = lf[5],
+                     a0v = lf[6], a0e = lf[7];
+        lf[0] = a3v * w3_3;
+        lf[2] = a2v * w2_2;
+        lf[4] = (a1v * w1_1) - (a3v * w3_1);
+        lf[6] = a0v - a2v;
+        const double e3_3 = a3e * w3_3;
+        const double e2_2 = a2e * w2_2;
+        const double e1_1 = a1e * w1_1;
+        const double e3_1 = a3e * w3_1;
+        lf[1] = e3_3;
+        lf[3] = e2_2;
+        lf[5] = __dsqrt_rn((e1_1 * e1_1) + (e3_1 * e3_1));
+        lf[7] = __dsqrt_rn((a0e * a0e) + (a2e * a2e));
+    }
+}
+
+__global__ void basis_convert_kernel(double* __restrict__ leaves, uint64_t n, uint32_t np,
+                                     double ts, int to_cheby) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    double* lf = leaves + i * (np + 2) * 2;
+    if (to_cheby) {
+        taylor_to_cheby_leaf(lf, np, ts);
+    } else {
+        cheby_to_taylor_leaf(lf, np, ts);
+    }
+}
+
 // ---- exclusive scan of uint32 counts into uint64 offsets -------------------
 
 __global__ void scan_tile_sums_kernel(const uint32_t* __restrict__ x, uint64_t n,
@@ -325,11 +425,42 @@ struct ResolveConsts {
     double dt_add;      // t_add - t_cur (jerk's a_new)
     double half_dt2;
     double sixth_dt3;   // jerk only
+    // Chebyshev (lib/chebyshev.cpp:961-1097)
+    uint32_t basis;
+    double dt2, dt3;    // dt_add^k - dt_init^k
+    double inv_ts, inv_ts2, inv_ts3;
 };
 
 __device__ __forceinline__ void resolve_leaf(const double* lf, const LeafGeom& g,
                                              const ResolveConsts& rc, uint32_t* pidx,
                                              float* phase) {
+    if (rc.basis == 1) {
+        // poly_chebyshev_resolve_{accel,jerk}_batch
+        double a_new, delta_v, delta_d, f0;
+        if (g.np == 2) {
+            const double alpha_2 = lf[0], alpha_1 = lf[2];
+            f0 = lf[6];
+            a_new = 4.0 * alpha_2 * rc.inv_ts2;
+            delta_v = 4.0 * alpha_2 * rc.inv_ts2 * rc.dt;
+            delta_d = (alpha_1 * rc.inv_ts * rc.dt) + (2.0 * alpha_2 * rc.inv_ts2 * rc.dt2);
+        } else {
+            const double alpha_3 = lf[0], alpha_2 = lf[2], alpha_1 = lf[4];
+            f0 = lf[8];
+            a_new = (4.0 * alpha_2 * rc.inv_ts2) + (24.0 * alpha_3 * rc.dt_add * rc.inv_ts3);
+            delta_v = ((4.0 * alpha_2 * rc.inv_ts2) * rc.dt) +
+                      ((12.0 * alpha_3 * rc.inv_ts3) * rc.dt2);
+            delta_d = ((alpha_1 - (3.0 * alpha_3)) * rc.inv_ts * rc.dt) +
+                      ((2.0 * alpha_2 * rc.inv_ts2) * rc.dt2) +
+                      ((4.0 * alpha_3 * rc.inv_ts3) * rc.dt3);
+        }
+        const double f_new = f0 * (1.0 - (delta_v * kInvCval));
+        const double delay_rel = delta_d * kInvCval;
+        *phase = dev::phase_idx(rc.dt, f0, g.nbins, delay_rel);
+        const uint32_t ia = dev::nearest_idx(a_new, g.a_min, g.a_max, g.n_accel);
+        const uint32_t jf = dev::nearest_idx(f_new, g.f_min, g.f_max, g.n_freq);
+        *pidx = ia * g.n_freq + jf;
+        return;
+    }
     if (g.np == 2) {
         const double a_cur = lf[0], v_cur = lf[2], f0 = lf[6];
         const double a_new = a_cur;
@@ -652,10 +783,47 @@ __global__ void select_threshold_kernel(const float* __restrict__ list_sc, uint6
 struct TransformConsts {
     double dt, half_dt2, sixth_dt3, dt2;
     int conservative;
+    // Chebyshev (lib/chebyshev.cpp:316-409): p = s_next / s_cur, q = dt / s_cur
+    int basis;
+    double p, q, p2, q2, pq, p3;
 };
+
+// poly_chebyshev_transform_{accel,jerk}_batch: values through the
+// re-centring matrix, errors times its diagonal (non-conservative).
+__device__ __forceinline__ void cheby_transform_leaf(const double* in, double* o, uint32_t np,
+                                                     const TransformConsts& tc) {
+    const double p = tc.p, q = tc.q, p2 = tc.p2, q2 = tc.q2;
+    for (uint32_t k = 0; k < (np + 2) * 2; ++k) {
+        o[k] = in[k];
+    }
+    if (np == 2) {
+        const double a2v = in[0], a2e = in[1], a1v = in[2], a1e = in[3], a0v = in[4];
+        o[0] = p2 * a2v;
+        o[2] = (p * a1v) + (4.0 * tc.pq * a2v);
+        o[4] = a0v + (q * a1v) + ((p2 + (2.0 * q2) - 1.0) * a2v);
+        o[1] = p2 * a2e;
+        o[3] = p * a1e;
+    } else {
+        const double p3 = tc.p3;
+        const double a3v = in[0], a3e = in[1], a2v = in[2], a2e = in[3], a1v = in[4],
+                     a1e = in[5], a0v = in[6];
+        o[0] = p3 * a3v;
+        o[2] = (6.0 * p2 * q * a3v) + (p2 * a2v);
+        o[4] = (3.0 * p * (p2 + (4.0 * q2) - 1.0) * a3v) + (4.0 * p * q * a2v) + (p * a1v);
+        o[6] = (q * ((6.0 * p2) + (4.0 * q2) - 3.0) * a3v) + ((p2 + (2.0 * q2) - 1.0) * a2v) +
+               (q * a1v) + a0v;
+        o[1] = p3 * a3e;
+        o[3] = p2 * a2e;
+        o[5] = p * a1e;
+    }
+}
 
 __device__ __forceinline__ void transform_leaf(const double* in, double* o, uint32_t np,
                                                const TransformConsts& tc) {
+    if (tc.basis == 1) {
+        cheby_transform_leaf(in, o, np, tc);
+        return;
+    }
     const double dt = tc.dt;
     if (np == 2) {
         const double d2v = in[0], d2e = in[1], d1v = in[2], d1e = in[3], d0v = in[4],
@@ -743,6 +911,24 @@ __global__ void transform_kernel(double* __restrict__ leaves, uint64_t n_leaves,
     }
 }
 
+// Chebyshev branch, first step (lib/chebyshev.cpp:516-522, 660-666): the
+// level's parents, at physical slots (head + i) mod cap, re-centred in place
+// from coord_prev to coord_cur.
+__global__ void parent_transform_kernel(double* __restrict__ tree_leaves, uint64_t head,
+                                        uint64_t cap, uint64_t n, uint32_t np,
+                                        TransformConsts tc) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    double* lf = tree_leaves + ((head + i) % cap) * (np + 2) * 2;
+    double tmp[10];
+    transform_leaf(lf, tmp, np, tc);
+    for (uint32_t q = 0; q < (np + 2) * 2; ++q) {
+        lf[q] = tmp[q];
+    }
+}
+
 __global__ void set_f32_kernel(float* p, float v) { *p = v; }
 __global__ void set_u64_kernel(uint64_t* p, uint64_t v) { *p = v; }
 __global__ void init_minmax_kernel(uint32_t* mm) {
@@ -815,7 +1001,7 @@ Coord mo_segment_coord(const std::vector<uint64_t>& order, uint64_t level, doubl
     return {(idx + 0.5) * tseg, 0.5 * tseg};
 }
 
-LeafGeom make_geom(const Plan& p, uint64_t branch_max) {
+LeafGeom make_geom(const Plan& p, uint64_t branch_max, int basis = 0) {
     const uint32_t np = p.nparams;
     const uint32_t L = p.n_levels - 1;
     LeafGeom g{};
@@ -830,7 +1016,44 @@ LeafGeom make_geom(const Plan& p, uint64_t branch_max) {
     g.f_min = p.lim_min(np - 1);
     g.f_max = p.lim_max(np - 1);
     g.branch_max = branch_max;
+    g.basis = basis == 1 ? 1u : 0u;
     return g;
+}
+
+// poly_chebyshev_transform_*: from (t_cur, s_cur) to (t_next, s_next).
+TransformConsts make_transform_cheby(Coord next, Coord cur) {
+    TransformConsts tc{};
+    tc.basis = 1;
+    tc.dt = next.ref - cur.ref;
+    tc.p = next.scale / cur.scale;
+    tc.q = tc.dt / cur.scale;
+    tc.p2 = tc.p * tc.p;
+    tc.q2 = tc.q * tc.q;
+    tc.pq = tc.p * tc.q;
+    tc.p3 = tc.p2 * tc.p;
+    return tc;
+}
+
+// poly_chebyshev_resolve_*: coordinates add, cur, init.
+ResolveConsts make_resolve_cheby(uint32_t np, Coord add, Coord cur, Coord init) {
+    ResolveConsts rc{};
+    rc.basis = 1;
+    const double dt_add = add.ref - cur.ref;
+    const double dt_init = init.ref - cur.ref;
+    rc.dt_add = dt_add;
+    rc.inv_ts = 1.0 / cur.scale;
+    rc.inv_ts2 = rc.inv_ts * rc.inv_ts;
+    rc.dt = dt_add - dt_init;
+    if (np == 2) {
+        rc.dt2 = ((dt_add * dt_add) - (dt_init * dt_init));
+    } else {
+        const double dt2_add = dt_add * dt_add;
+        const double dt2_init = dt_init * dt_init;
+        rc.dt2 = dt2_add - dt2_init;
+        rc.dt3 = (dt2_add * dt_add) - (dt2_init * dt_init);
+        rc.inv_ts3 = rc.inv_ts2 * rc.inv_ts;
+    }
+    return rc;
 }
 
 TransformConsts make_transform(uint32_t np, double t_next, double t_cur, bool conservative) {
@@ -884,16 +1107,20 @@ void scan_counts(const uint32_t* d_x, uint64_t n, uint64_t* d_out, uint32_t* d_s
 }  // namespace
 
 PruneExec::PruneExec(const Plan& plan, uint64_t max_sugg, uint64_t batch_size,
-                     uint64_t branch_max, bool conservative, int device)
+                     uint64_t branch_max, bool conservative, int device, int basis)
     : m_plan(plan),
       m_device(device),
       m_cap(max_sugg),
       m_batch(batch_size),
       m_branch_max(branch_max),
-      m_conservative(conservative) {
+      m_conservative(conservative),
+      m_basis(basis) {
     m_np = plan.nparams;
     require(m_np == 2 || m_np == 3,
-            "pruning is implemented for Taylor searches with nparams 2 (accel) or 3 (jerk)");
+            "pruning is implemented for searches with nparams 2 (accel) or 3 (jerk)");
+    require(basis == 0 || basis == 1, "poly_basis must be taylor (0) or chebyshev (1)");
+    require(!(basis == 1 && conservative),
+            "Conservative tile not implemented for Chebyshev basis");
     const uint32_t L = plan.n_levels - 1;
     m_nbins = static_cast<uint32_t>(plan.cfg.nbins);
     m_ls = (m_np + 2) * 2;
@@ -1048,13 +1275,18 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
     m_tree = TreeState{};
     m_tree.cap = m_cap;
     m_cur = 0;
-    const LeafGeom geom = make_geom(m_plan, m_branch_max);
+    const LeafGeom geom = make_geom(m_plan, m_branch_max, m_basis);
     const uint32_t L = m_plan.n_levels - 1;
     const double dp0 = m_plan.dparams_actual[L][0];
     const double dp1 = m_np == 3 ? m_plan.dparams_actual[L][1] : 0.0;
     const double dfreq = m_plan.dparams_actual[L][m_np - 1];
     seed_kernel<<<grid_for(m_ncoords, 256), 256, 0, s>>>(geom, dp0, dp1, dfreq,
                                                          m_tleaves[0].as<double>());
+    if (m_basis == 1) {
+        // BaseChebyshevPruneDPFuncts::seed (lib/dynamic.cpp:203-218)
+        basis_convert_kernel<<<grid_for(m_ncoords, 256), 256, 0, s>>>(
+            m_tleaves[0].as<double>(), m_ncoords, m_np, mo_coord(order, 0, m_tseg).scale, 1);
+    }
     const float* seg0 = d_ffa_fold + order[0] * seg_floats;
     LK_CUDA(cudaMemcpyAsync(m_tfolds[0].ptr, seg0, seg_floats * sizeof(float),
                             cudaMemcpyDeviceToDevice, s));
@@ -1110,6 +1342,7 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
     t.read_consumed = 0;
     const uint64_t n_par = t.size_old;
     const Coord ci = mo_coord(order, 0, m_tseg);
+    const Coord cp = mo_coord(order, lv - 1, m_tseg);
     const Coord cn = mo_coord(order, lv, m_tseg);
     const Coord cc = mo_current_coord(order, lv, m_tseg);
     const Coord ca = mo_segment_coord(order, lv, m_tseg);
@@ -1151,8 +1384,15 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
     h_bpar[nbat] = n_par;
     ensure_level_buffers(n_par, 0);
 
-    // 1. branch: counts, offsets, batch child ranges
-    const LeafGeom geom = make_geom(m_plan, m_branch_max);
+    // 1. branch: counts, offsets, batch child ranges. In the Chebyshev basis
+    // the parents are first re-centred in place from coord_prev to
+    // coord_cur (every batch's branch does this to its parents).
+    const LeafGeom geom = make_geom(m_plan, m_branch_max, m_basis);
+    if (m_basis == 1 && n_par > 0) {
+        parent_transform_kernel<<<grid_for(n_par, 256), 256, 0, s>>>(
+            m_tleaves[m_cur].as<double>(), t.head, t.cap, n_par, m_np,
+            make_transform_cheby(cc, cp));
+    }
     const double* tree_leaves = m_tleaves[m_cur].as<double>();
     LK_CUDA(cudaMemcpyAsync(m_bparents.ptr, h_bpar, (nbat + 1) * sizeof(uint64_t),
                             cudaMemcpyHostToDevice, s));
@@ -1196,7 +1436,8 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
         m_cleaves.as<double>(), m_cparent.as<uint32_t>(), m_status.as<uint32_t>());
     init_minmax_kernel<<<1, 1, 0, s>>>(d_mm);
     if (n_child > 0) {
-        const ResolveConsts rc = make_resolve(m_np, ca.ref, cc.ref, ci.ref);
+        const ResolveConsts rc = m_basis == 1 ? make_resolve_cheby(m_np, ca, cc, ci)
+                                              : make_resolve(m_np, ca.ref, cc.ref, ci.ref);
         const uint32_t rs = sc::row_stride(m_nbins, m_sp.wmax);
         const uint32_t T = sc::profiles_per_block(rs + 4);
         const size_t smem = static_cast<size_t>(T) * rs * sizeof(float) + 4 * T * sizeof(uint32_t);
@@ -1274,7 +1515,8 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
 
     // 4. transform + gather into the other tree buffer; finalize_in_place_update
     if (t.size > 0) {
-        const TransformConsts tc = make_transform(m_np, cn.ref, cc.ref, m_conservative);
+        const TransformConsts tc = m_basis == 1 ? make_transform_cheby(cn, cc)
+                                                : make_transform(m_np, cn.ref, cc.ref, m_conservative);
         const int nxt = 1 - m_cur;
         gather_kernel<<<grid_for(t.size * kWarp, 256), 256, 0, s>>>(
             m_lids[li].as<uint32_t>(), m_lsc[li].as<float>(), t.size, m_cleaves.as<double>(),
@@ -1373,8 +1615,12 @@ __global__ void shift_add_kernel(const float* __restrict__ tree, const uint32_t*
 
 void require_taylor(const Plan& plan) {
     require(plan.nparams == 2 || plan.nparams == 3,
-            "pruning is implemented for Taylor searches with nparams 2 (accel) or 3 (jerk)");
+            "pruning is implemented for searches with nparams 2 (accel) or 3 (jerk)");
 }
+
+uint64_t branch_impl(const Plan& plan, const double* d_leaves, uint64_t n, double scale_cur,
+                     uint64_t branch_max, double* d_out, uint32_t* d_origins, uint64_t max_out,
+                     cudaStream_t s, int basis);
 
 }  // namespace
 
@@ -1395,12 +1641,60 @@ void taylor_seed(const Plan& plan, double* d_leaves, cudaStream_t s) {
 uint64_t taylor_branch(const Plan& plan, const double* d_leaves, uint64_t n, double scale_cur,
                        uint64_t branch_max, double* d_out, uint32_t* d_origins, uint64_t max_out,
                        cudaStream_t s) {
+    return branch_impl(plan, d_leaves, n, scale_cur, branch_max, d_out, d_origins, max_out, s, 0);
+}
+
+uint64_t cheby_branch(const Plan& plan, double* d_leaves, uint64_t n, double t_cur, double s_cur,
+                      double t_prev, double s_prev, uint64_t branch_max, double* d_out,
+                      uint32_t* d_origins, uint64_t max_out, cudaStream_t s) {
+    require_taylor(plan);
+    if (n > 0) {
+        parent_transform_kernel<<<grid_for(n, 256), 256, 0, s>>>(
+            d_leaves, 0, n, n, plan.nparams,
+            make_transform_cheby(Coord{t_cur, s_cur}, Coord{t_prev, s_prev}));
+        LK_CUDA(cudaGetLastError());
+    }
+    return branch_impl(plan, d_leaves, n, 0.0, branch_max, d_out, d_origins, max_out, s, 1);
+}
+
+void cheby_resolve(const Plan& plan, const double* d_leaves, uint64_t n, const double* coords,
+                   uint32_t* d_param_idx, float* d_phase_shift, cudaStream_t s) {
+    require_taylor(plan);
+    if (n == 0) {
+        return;
+    }
+    const LeafGeom g = make_geom(plan, 1, 1);
+    const ResolveConsts rc = make_resolve_cheby(plan.nparams, Coord{coords[0], coords[1]},
+                                                Coord{coords[2], coords[3]},
+                                                Coord{coords[4], coords[5]});
+    resolve_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, n, g, rc, d_param_idx,
+                                                    d_phase_shift);
+    LK_CUDA(cudaGetLastError());
+}
+
+void basis_convert(double* d_leaves, uint64_t n, uint32_t nparams, double ts, bool to_cheby,
+                   cudaStream_t s) {
+    require(nparams == 2 || nparams == 3, "basis conversion supports nparams 2 or 3");
+    require(ts > 0.0, "the coordinate scale must be positive");
+    if (n == 0) {
+        return;
+    }
+    basis_convert_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, n, nparams, ts,
+                                                          to_cheby ? 1 : 0);
+    LK_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+uint64_t branch_impl(const Plan& plan, const double* d_leaves, uint64_t n, double scale_cur,
+                     uint64_t branch_max, double* d_out, uint32_t* d_origins, uint64_t max_out,
+                     cudaStream_t s, int basis) {
     require_taylor(plan);
     require(branch_max >= 1, "branch_max must be positive");
     if (n == 0) {
         return 0;
     }
-    const LeafGeom g = make_geom(plan, branch_max);
+    const LeafGeom g = make_geom(plan, branch_max, basis);
     DeviceBuffer counts(n * sizeof(uint32_t)), offsets(n * sizeof(uint64_t));
     const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
     DeviceBuffer sums(ntiles * sizeof(uint32_t)), offs(ntiles * sizeof(uint64_t));
@@ -1432,6 +1726,8 @@ uint64_t taylor_branch(const Plan& plan, const double* d_leaves, uint64_t n, dou
     }
     return total;
 }
+
+}  // namespace
 
 void taylor_resolve(const Plan& plan, const double* d_leaves, uint64_t n, const double* coords,
                     uint32_t* d_param_idx, float* d_phase_shift, cudaStream_t s) {
@@ -1469,6 +1765,22 @@ void taylor_transform(const Plan& plan, double* d_leaves, uint64_t n_leaves,
         return;
     }
     const TransformConsts tc = make_transform(plan.nparams, t_next, t_cur, conservative);
+    DeviceBuffer st(sizeof(uint32_t));
+    LK_CUDA(cudaMemsetAsync(st.ptr, 0, sizeof(uint32_t), s));
+    transform_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, n_leaves, d_indices, n,
+                                                      plan.nparams, tc, st.as<uint32_t>());
+    LK_CUDA(cudaGetLastError());
+    check_index_status(st, s, "transform: an index is at or beyond n_leaves");
+}
+
+void cheby_transform(const Plan& plan, double* d_leaves, uint64_t n_leaves,
+                     const uint32_t* d_indices, uint64_t n, double t_next, double s_next,
+                     double t_cur, double s_cur, cudaStream_t s) {
+    require_taylor(plan);
+    if (n == 0) {
+        return;
+    }
+    const TransformConsts tc = make_transform_cheby(Coord{t_next, s_next}, Coord{t_cur, s_cur});
     DeviceBuffer st(sizeof(uint32_t));
     LK_CUDA(cudaMemsetAsync(st.ptr, 0, sizeof(uint32_t), s));
     transform_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_leaves, n_leaves, d_indices, n,

@@ -31,16 +31,28 @@ PRUNE_STATS_DTYPE = np.dtype([
     ("score_min", np.float32), ("score_max", np.float32), ("pad", np.float32)])
 
 
-def branching_pattern(cfg: PulsarSearchConfig, ref_seg: int = 0, use_conservative_tile: bool = False) -> np.ndarray:
-    """FFAPlan.get_branching_pattern("taylor", ref_seg) (lib/taylor.cpp:1643-1741)."""
+_BASES = {"taylor": 0, "chebyshev": 1}
+
+
+def _basis(poly_basis: str) -> int:
+    if poly_basis not in _BASES:
+        raise ValueError(f"Unknown poly_basis: '{poly_basis}'. Valid options: 'taylor', 'chebyshev'")
+    return _BASES[poly_basis]
+
+
+def branching_pattern(cfg: PulsarSearchConfig, ref_seg: int = 0, use_conservative_tile: bool = False,
+                      poly_basis: str = "taylor") -> np.ndarray:
+    """FFAPlan.get_branching_pattern(poly_basis, ref_seg): generate_bp_poly_taylor
+    (lib/taylor.cpp:1643-1741) or generate_bp_poly_chebyshev (lib/chebyshev.cpp:1796-1890)."""
+    b = _basis(poly_basis)
     out = np.zeros(4096, np.float64)
     n = ctypes.c_uint64()
-    C.check(C.lib().lk_plan_branching_pattern(cfg._plan_handle, int(ref_seg), int(use_conservative_tile),
-                                              out.ctypes.data, out.size, ctypes.byref(n)))
+    C.check(C.lib().lk_plan_branching_pattern_basis(cfg._plan_handle, int(ref_seg), int(use_conservative_tile), b,
+                                                    out.ctypes.data, out.size, ctypes.byref(n)))
     if n.value > out.size:
         out = np.zeros(n.value, np.float64)
-        C.check(C.lib().lk_plan_branching_pattern(cfg._plan_handle, int(ref_seg), int(use_conservative_tile),
-                                                  out.ctypes.data, out.size, ctypes.byref(n)))
+        C.check(C.lib().lk_plan_branching_pattern_basis(cfg._plan_handle, int(ref_seg), int(use_conservative_tile),
+                                                        b, out.ctypes.data, out.size, ctypes.byref(n)))
     return out[: n.value].copy()
 
 
@@ -69,23 +81,27 @@ class PruneCUDA:
     ``max_sugg`` is the world-tree capacity, ``batch_size`` the parents per
     batch (it decides when overload pruning raises the threshold, exactly as
     in the reference), ``branch_max`` the most child values of one parameter
-    (None: EPMultiPass's rule, max(ceil(2 * max branching), 32)).
+    (None: EPMultiPass's rule, max(ceil(2 * max branching), 32)) and
+    ``poly_basis`` "taylor" or "chebyshev" (lib/dynamic.cpp:381-450).
     """
 
     def __init__(self, cfg: PulsarSearchConfig, max_sugg: int = 1 << 20, batch_size: int = 4096,
-                 branch_max: int | None = None, use_conservative_tile: bool = False, device_id: int = 0):
+                 branch_max: int | None = None, use_conservative_tile: bool = False, device_id: int = 0,
+                 poly_basis: str = "taylor"):
         D.require_cuda(device_id)
         if cfg.nparams not in (2, 3):
-            raise NotImplementedError("pruning is implemented for Taylor searches with nparams 2 or 3")
+            raise NotImplementedError("pruning is implemented for searches with nparams 2 or 3")
+        self.poly_basis = poly_basis
+        basis = _basis(poly_basis)
         self._cfg = cfg
         self._device = device_id
         self._nparams = cfg.nparams
         self._nbins = cfg.nbins
         h = ctypes.c_void_p()
         with D.torch().cuda.device(device_id):
-            C.check(C.lib().lk_prune_create(cfg._plan_handle, int(max_sugg), int(batch_size),
-                                            0 if branch_max is None else int(branch_max),
-                                            int(use_conservative_tile), device_id, ctypes.byref(h)))
+            C.check(C.lib().lk_prune_create_basis(cfg._plan_handle, int(max_sugg), int(batch_size),
+                                                  0 if branch_max is None else int(branch_max),
+                                                  int(use_conservative_tile), basis, device_id, ctypes.byref(h)))
         self._h = h
 
     def __del__(self):
@@ -146,14 +162,14 @@ class EPMultiPassCUDA:
     def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
                  max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
                  show_progress: bool = False, use_conservative_tile: bool = False, device_id: int = 0):
-        if poly_basis != "taylor":
-            raise NotImplementedError("only the Taylor basis is implemented")
+        _basis(poly_basis)
         self._cfg = cfg
         self._thr = np.ascontiguousarray(threshold_scheme, dtype=np.float32)
         self._n_runs = n_runs
         self._ref_segs = ref_segs
         self._ffa = FFACUDA(cfg, device_id)
-        self._prune = PruneCUDA(cfg, max_sugg, batch_size, None, use_conservative_tile, device_id)
+        self._prune = PruneCUDA(cfg, max_sugg, batch_size, None, use_conservative_tile, device_id,
+                                poly_basis=poly_basis)
         self._device = device_id
 
     @property

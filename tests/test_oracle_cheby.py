@@ -112,3 +112,32 @@ def test_oracle_cheby_prune_matches_reference_directly(case):
     b = lko.prune_run(plan, fold, thr, ref_seg, ms, bs, bm, nseg - 1, basis="chebyshev")
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("name", CHEBY_FIXTURES)
+def test_library_cheby_branching_pattern_matches_reference_fixture(name):
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.prune import branching_pattern
+
+    g = golden(name)
+    cfg = PulsarSearchConfig(int(g["nsamps"]), float(g["tsamp"]), int(g["nbins"]), float(g["eta"]),
+                             g["param_limits"], use_fourier=False, bseg_ffa=int(g["bseg_ffa"]))
+    np.testing.assert_array_equal(branching_pattern(cfg, 0, poly_basis="chebyshev"), g["branching_pattern"])
+    np.testing.assert_array_equal(branching_pattern(cfg, int(g["ref_seg"]), poly_basis="chebyshev"),
+                                  g["branching_pattern_ref"])
+    assert max(int(np.ceil(g["branching_pattern"].max() * 2)), 32) == int(g["branch_max"])
+
+
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref (the reference build) is not present")
+@pytest.mark.parametrize("case", range(len(CHEBY_REF_CASES)))
+def test_library_cheby_branching_pattern_matches_reference_directly(case):
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.prune import branching_pattern
+
+    ns, ts, nb, eta, lim, bf = CHEBY_REF_CASES[case][:6]
+    rc = R.make_cfg(ns, ts, nb, eta, lim, bseg_ffa=bf)
+    cfg = PulsarSearchConfig(ns, ts, nb, eta, np.array(lim), use_fourier=False, bseg_ffa=bf)
+    nseg = len(branching_pattern(cfg, 0)) + 1
+    for rs in (0, nseg // 2, nseg - 1):
+        np.testing.assert_array_equal(branching_pattern(cfg, rs, poly_basis="chebyshev"),
+                                      R.branching_pattern_basis(rc, "chebyshev", rs))
