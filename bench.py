@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--basis", default="taylor", choices=["taylor", "chebyshev"],
+                    help="polynomial basis of the pruning workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="taylor_accel",

@@ -230,19 +230,20 @@ def _prune_cfgd(p, nseg, ref_seg, widths):
             "score_widths": [int(w) for w in widths]}
 
 
-def _ref_prune_sample(p, fold, thr, ref_seg, nbins, kind, budget_s=20.0):
+def _ref_prune_sample(p, fold, thr, ref_seg, nbins, kind, budget_s=20.0, basis="taylor"):
     """The reference's pruning run (oracle/_ref: PruneDPFuncts + WorldTree over
     prune.cpp's level loop) on the first k levels, k doubled while a run stays
     within the budget; returns (trials/s, levels, seconds, stats)."""
     from oracle import ref
 
     cfg = ref.make_cfg(p["nsamps"], p["tsamp"], p["nbins"], p["eta"], p["param_limits"], bseg_ffa=p["bseg_ffa"])
-    bm = ref.branch_max(cfg)
+    bm = max(int(np.ceil(ref.branching_pattern_basis(cfg, basis, 0).max() * 2)), 32)
     widths = ref.box_widths(nbins)
     k, best = 2, None
     while True:
         t0 = time.perf_counter()
-        st = ref.prune_run(cfg, fold, thr, ref_seg, PRUNE_MAX_SUGG, PRUNE_BATCH, bm, k, nbins, kind=kind)[0]
+        st = ref.prune_run(cfg, fold, thr, ref_seg, PRUNE_MAX_SUGG, PRUNE_BATCH, bm, k, nbins, kind=kind,
+                           basis=basis)[0]
         el = time.perf_counter() - t0
         trials = int(st["n_leaves_phy"][1:].sum()) * widths.size
         best = (trials / el, k, el, st)
@@ -267,11 +268,13 @@ def run_prune(args, rank, world, local_rank):
         fold = ref.RefFFA(cfg, kind="timing").execute(ts_e, ts_v).copy()
         nseg = int(lko.plan_create(lko.make_cfg(p["nsamps"], p["tsamp"], nbins, p["eta"], p["param_limits"],
                                                 bseg_ffa=p["bseg_ffa"])).nsegments[-1])
-        v, k, el, st = _ref_prune_sample(p, fold, thr, nseg // 2, nbins, "timing")
+        v, k, el, st = _ref_prune_sample(p, fold, thr, nseg // 2, nbins, "timing", basis=args.basis)
         widths = ref.box_widths(nbins)
-        sample = f"one pruning run (ref_seg {nseg // 2}) over its first {k} levels, {el:.1f} s, single thread"
+        sample = (f"one {args.basis}-basis pruning run (ref_seg {nseg // 2}) over its first {k} levels, "
+                  f"{el:.1f} s, single thread")
         B.emit(_line(args, world, "prune_jerk_2^23x64us_nbins32", v, 1e3 * el,
-                               _prune_cfgd(p, nseg, nseg // 2, widths), impl="reference",
+                               dict(_prune_cfgd(p, nseg, nseg // 2, widths), poly_basis=args.basis),
+                               impl="reference",
                                cpu_baseline={"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
                                              "sample": sample},
                                e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}))
@@ -286,7 +289,8 @@ def run_prune(args, rank, world, local_rank):
     ffa = FFACUDA(cfg, device_id=local_rank)
     nseg = int(ffa.plan.nsegments[-1])
     ref_seg = nseg // 2
-    pr = PruneCUDA(cfg, max_sugg=PRUNE_MAX_SUGG, batch_size=PRUNE_BATCH, device_id=local_rank)
+    pr = PruneCUDA(cfg, max_sugg=PRUNE_MAX_SUGG, batch_size=PRUNE_BATCH, device_id=local_rank,
+                   poly_basis=args.basis)
     widths = cfg.score_widths
     e = torch.from_numpy(ts_e).cuda()
     v = torch.from_numpy(ts_v).cuda()
@@ -335,14 +339,15 @@ def run_prune(args, rank, world, local_rank):
         from oracle import ref
 
         if ref.available("timing"):
-            cv, k, el, _ = _ref_prune_sample(p, fold.cpu().numpy(), thr, ref_seg, nbins, "timing")
+            cv, k, el, _ = _ref_prune_sample(p, fold.cpu().numpy(), thr, ref_seg, nbins, "timing",
+                                             basis=args.basis)
             cpu = {"value": cv, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": f"reference pruning run (ref_seg {ref_seg}) over its first {k} levels "
                              f"({el:.1f} s), single thread, on the same FFA fold"}
     if rank == 0:
         B.emit(_line(
             args, world, "prune_jerk_2^23x64us_nbins32", value, ms,
-            dict(_prune_cfgd(p, nseg, ref_seg, widths), leaves_scored=leaves,
+            dict(_prune_cfgd(p, nseg, ref_seg, widths), poly_basis=args.basis, leaves_scored=leaves,
                  survivors=int(stats["n_leaves_surv"][-1]), levels_run=int(len(stats) - 1)),
             roofline=_roofline("prune_run", algo, prune_ms), cpu_baseline=cpu, e2e=e2e,
             clocks=clk, stages={"ffa_ms": ms - prune_ms, "prune_ms": prune_ms},
