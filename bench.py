@@ -50,6 +50,8 @@ def parse():
                     help="polynomial basis of the pruning workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--workload", default="taylor_accel",
                     choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade", "multi_series"],
                     help="taylor_accel (default): Taylor (f, fdot) FFA + S/N; freq_sweep: plain period "
@@ -271,6 +273,10 @@ def run_ours(args, rank, world, local_rank):
         C.check(L.lk_ffa_search(ffa._h, e.data_ptr(), v.data_ptr(), SNR_MIN, idx.data_ptr(), snr.data_ptr(),
                                 cap, cnt.data_ptr(), sp))
 
+    tuning = None
+    if not args.no_autotune:
+        # launch shapes timed on this series before the warm-up (not timed)
+        tuning = ffa.autotune(e, v, reps=3)
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
@@ -380,7 +386,8 @@ def run_ours(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_dict(params, {"fold_storage": args.storage, "final_coords": nc, "n_widths": nw,
                                            "candidates": ncand, "rescored_cells": rescored,
-                                           "rescore_margin": list(ffa.rescore_margin)}),
+                                           "rescore_margin": list(ffa.rescore_margin),
+                                           "tuning": tuning}),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "stages": stages, "wall_s": wall,
         }

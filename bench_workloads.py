@@ -158,6 +158,7 @@ def run_freq(args, rank, world, local_rank):
     flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     sp = torch.cuda.current_stream().cuda_stream
     L = C.lib()
+    tuning = None if args.no_autotune else ffa.autotune(e, v, reps=3)
 
     def step():
         C.check(L.lk_ffa_search(ffa._h, e.data_ptr(), v.data_ptr(), B.SNR_MIN, idx.data_ptr(), snr.data_ptr(),
@@ -202,7 +203,7 @@ def run_freq(args, rank, world, local_rank):
     if rank == 0:
         B.emit(_line(args, world, "freq_sweep_2^21x64us_nbins128", value, ms,
                                dict(cfgd, final_coords=int(ffa.plan.ncoords[-1]), candidates=int(cnt.item()),
-                                    fold_storage=args.storage),
+                                    fold_storage=args.storage, tuning=tuning),
                                roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
                                gpu_launches=args.steps * launches, clocks=clk,
                                stages={k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()}))

@@ -206,6 +206,32 @@ int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status);
  * must be finite and >= 0; calls on an LK_FP32 executor are no-ops. */
 int lk_ffa_set_rescore_margin(lk_ffa* ffa, float margin_abs, float margin_rel);
 int lk_ffa_get_rescore_margin(const lk_ffa* ffa, float* margin_abs, float* margin_rel);
+/* Launch-shape tuning (north-star "autotuner"; no reference counterpart).
+ * bf_*: brute fold rows (E, V) per consumer warp (1 or 2), consumer warps
+ * per block (0: the wave-count rule), shared-memory ring depth in 32-sample
+ * words; merge_rows_in_flight: output rows per warp whose loads are issued
+ * together in a merge level (0: the default for nbins); score_cells_per_block:
+ * final cells per block of the fused final level (0: the most that fit). */
+typedef struct lk_tuning {
+    uint32_t bf_rows;
+    uint32_t bf_warps;
+    uint32_t bf_stages;
+    int32_t merge_rows_in_flight;
+    uint32_t score_cells_per_block;
+    uint32_t candidates; /* configurations lk_ffa_autotune timed */
+    float bf_ms;         /* best median stage times (ms): brute fold (+ interleave), */
+    float merge_ms;      /* all merge levels, */
+    float score_ms;      /* fused final level */
+} lk_tuning;
+/* Times the candidates on the given device series (one search's inputs;
+ * reps timed passes each, median) and keeps the fastest shape of each stage.
+ * Results of every later call are unchanged (same sums, same order).
+ * Synchronises the stream; needs a plan with one final segment. */
+int lk_ffa_autotune(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint32_t reps,
+                    lk_tuning* out, lk_stream_t stream);
+int lk_ffa_get_tuning(const lk_ffa* ffa, lk_tuning* out);
+/* Applies a saved tuning (validated against the plan). */
+int lk_ffa_set_tuning(lk_ffa* ffa, const lk_tuning* tuning);
 /* Synchronises the stream; final cells the last LK_BF16 search rescored. */
 int lk_ffa_rescored_cells(lk_ffa* ffa, lk_stream_t stream, uint64_t* n_cells);
 

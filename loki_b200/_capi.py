@@ -102,6 +102,12 @@ class LkStageTime(ctypes.Structure):
                 ("bytes", u64)]
 
 
+class LkTuning(ctypes.Structure):
+    _fields_ = [("bf_rows", u32), ("bf_warps", u32), ("bf_stages", u32), ("merge_rows_in_flight", ctypes.c_int32),
+                ("score_cells_per_block", u32), ("candidates", u32), ("bf_ms", f32), ("merge_ms", f32),
+                ("score_ms", f32)]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 class LkPruneStats(ctypes.Structure):
     _fields_ = [
@@ -141,6 +147,9 @@ SIGNATURES = [
     ("lk_ffa_set_rescore_margin", i32, [vp, ctypes.c_float, ctypes.c_float]),
     ("lk_ffa_get_rescore_margin", i32, [vp, vp, vp]),
     ("lk_ffa_rescored_cells", i32, [vp, vp, vp]),
+    ("lk_ffa_autotune", i32, [vp, vp, vp, u32, vp, vp]),
+    ("lk_ffa_get_tuning", i32, [vp, vp]),
+    ("lk_ffa_set_tuning", i32, [vp, vp]),
     ("lk_ffa_set_profiling", i32, [vp, i32]),
     ("lk_ffa_get_profile", i32, [vp, vp, vp, u32, vp]),
     ("lk_brute_fold_create", i32, [vp, u64, u64, u64, u64, f64, f64, i32, vp]),

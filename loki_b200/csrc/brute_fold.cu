@@ -671,46 +671,22 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
     // 2 .. 16 words on the 2^22-sample accelerated workload changed nothing
     // but the shared memory left for accumulators), so 3 words leave the
     // most for accumulator warps. LOKI_B200_BF_STAGES overrides it (2 .. 16).
-    m_stages = 3;
+    uint32_t stages = 3;
     if (const char* env = std::getenv("LOKI_B200_BF_STAGES")) {
-        m_stages = std::max<uint32_t>(2, std::min<uint32_t>(kMaxStages, std::atoi(env)));
+        stages = std::max<uint32_t>(2, std::min<uint32_t>(kMaxStages, std::atoi(env)));
     }
-    const size_t ring = m_stages * kStageBytes + 2 * m_stages * sizeof(uint64_t);
     // Rows per warp: both when two rows' accumulators of nbins <= 64 leave
     // room for >= 11 warps per block, else one (LOKI_B200_BF_ROWS overrides).
-    m_rows = m_nbins <= 64 ? 2 : 1;
+    uint32_t rows = m_nbins <= 64 ? 2 : 1;
     if (const char* env = std::getenv("LOKI_B200_BF_ROWS")) {
-        m_rows = std::atoi(env) == 1 ? 1 : 2;
+        rows = std::atoi(env) == 1 ? 1 : 2;
     }
-    const size_t per_warp = m_rows * (m_nbins + 1) * kWarp * sizeof(float);
-    require(ring + per_warp <= kSmemLimit,
-            "BruteFold: nbins too large for the shared-memory accumulators");
-    const uint32_t wmax = static_cast<uint32_t>(
-        std::min<size_t>((kSmemLimit - ring) / per_warp, kMaxConsumers));
-    int dev = 0, nsm = 148;
-    LK_CUDA(cudaGetDevice(&dev));
-    LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const uint64_t nitems = (m_rows == 2 ? 1 : 2) * m_nfreq;
-    const uint64_t xblocks = (m_nseg + kWarp - 1) / kWarp;
-    // The kernel is latency-bound per warp, so block time hardly depends on W:
-    // take the fewest waves of blocks over the SMs among W >= 3/4 of the
-    // maximum, the larger W on a tie. LOKI_B200_BF_WARPS overrides it.
-    m_warps = wmax;
+    uint32_t warps = 0;  // 0: the wave-count rule below
     if (const char* env = std::getenv("LOKI_B200_BF_WARPS")) {
-        m_warps = std::max<uint32_t>(1, std::min<uint32_t>(wmax, std::atoi(env)));
-    } else {
-        uint64_t best = ~0ull;
-        for (uint32_t w = std::max<uint32_t>(1, (3 * wmax + 3) / 4); w <= wmax; ++w) {
-            const uint64_t blocks = xblocks * ((nitems + w - 1) / w);
-            const uint64_t waves = (blocks + nsm - 1) / nsm;
-            if (waves <= best) {
-                best = waves;
-                m_warps = w;
-            }
-        }
+        warps = static_cast<uint32_t>(std::max(1, std::atoi(env)));
     }
-    m_smem = ring + m_warps * per_warp;
-    require((nitems + m_warps - 1) / m_warps <= 65535, "BruteFold: too many frequencies");
+    require(configure(rows, warps, stages),
+            "BruteFold: nbins too large for the shared-memory accumulators");
 
     // Run tables, one frequency per task (host threads; same arithmetic as
     // the reference's BruteFold::compute_phase_time_domain, lib/fold.cpp:113-142).
@@ -782,6 +758,60 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
     m_seq.alloc(m_nfreq);
     LK_CUDA(cudaMemcpy(m_seq.ptr, seq.data(), m_nfreq, cudaMemcpyHostToDevice));
     m_nseq = static_cast<uint64_t>(std::count(seq.begin(), seq.end(), uint8_t{1}));
+}
+
+// Launch shape: rows (E, V) per consumer warp, consumer warps per block
+// (0: the fewest waves of blocks over the SMs among W >= 3/4 of the most that
+// fit, the larger W on a tie -- the kernel is latency-bound per warp, so
+// block time hardly depends on W) and the depth of the shared-memory ring.
+// Returns false (and changes nothing) when the shape does not fit.
+bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages) {
+    if ((rows != 1 && rows != 2) || stages < 2 || stages > kMaxStages) {
+        return false;
+    }
+    const size_t ring = stages * kStageBytes + 2 * stages * sizeof(uint64_t);
+    const size_t per_warp = rows * (m_nbins + 1) * kWarp * sizeof(float);
+    if (ring + per_warp > kSmemLimit) {
+        return false;
+    }
+    const uint32_t wmax = static_cast<uint32_t>(
+        std::min<size_t>((kSmemLimit - ring) / per_warp, kMaxConsumers));
+    const uint64_t nitems = (rows == 2 ? 1 : 2) * m_nfreq;
+    uint32_t w = warps;
+    if (w == 0) {
+        int dev = 0, nsm = 148;
+        LK_CUDA(cudaGetDevice(&dev));
+        LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const uint64_t xblocks = (m_nseg + kWarp - 1) / kWarp;
+        uint64_t best = ~0ull;
+        for (uint32_t c = std::max<uint32_t>(1, (3 * wmax + 3) / 4); c <= wmax; ++c) {
+            const uint64_t blocks = xblocks * ((nitems + c - 1) / c);
+            const uint64_t waves = (blocks + nsm - 1) / nsm;
+            if (waves <= best) {
+                best = waves;
+                w = c;
+            }
+        }
+    }
+    if (w < 1 || w > wmax || (nitems + w - 1) / w > 65535) {
+        return false;
+    }
+    m_rows = rows;
+    m_warps = w;
+    m_stages = stages;
+    m_smem = ring + w * per_warp;
+    m_map_e_ptr = nullptr;  // the input binding depends on the rows
+    m_map_ev_ptr = nullptr;
+    return true;
+}
+
+uint32_t BruteFoldDevice::max_warps(uint32_t rows, uint32_t stages) const {
+    const size_t ring = stages * kStageBytes + 2 * stages * sizeof(uint64_t);
+    const size_t per_warp = rows * (m_nbins + 1) * kWarp * sizeof(float);
+    if (ring + per_warp > kSmemLimit) {
+        return 0;
+    }
+    return static_cast<uint32_t>(std::min<size_t>((kSmemLimit - ring) / per_warp, kMaxConsumers));
 }
 
 uint64_t BruteFoldDevice::device_bytes() const {

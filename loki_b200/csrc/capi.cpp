@@ -313,6 +313,42 @@ int lk_ffa_rescored_cells(lk_ffa* ffa, lk_stream_t stream, uint64_t* n_cells) {
     });
 }
 
+int lk_ffa_autotune(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint32_t reps,
+                    lk_tuning* out, lk_stream_t stream) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        const lk_tuning t =
+            ffa->exec->autotune(d_ts_e, d_ts_v, reps, reinterpret_cast<cudaStream_t>(stream));
+        if (out != nullptr) {
+            *out = t;
+        }
+    });
+}
+
+int lk_ffa_get_tuning(const lk_ffa* ffa, lk_tuning* out) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(out, "out");
+        lk_tuning t = ffa->exec->tuning;
+        t.bf_rows = ffa->exec->bf->rows();
+        t.bf_warps = ffa->exec->bf->warps();
+        t.bf_stages = ffa->exec->bf->stages();
+        t.merge_rows_in_flight = ffa->exec->merge_pb;
+        t.score_cells_per_block = ffa->exec->score_cells;
+        *out = t;
+    });
+}
+
+int lk_ffa_set_tuning(lk_ffa* ffa, const lk_tuning* tuning) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        need(tuning, "tuning");
+        ffa->exec->apply_tuning(*tuning);
+    });
+}
+
 int lk_ffa_set_profiling(lk_ffa* ffa, int enable) {
     return guarded([&] {
         need(ffa, "ffa");

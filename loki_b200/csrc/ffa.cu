@@ -10,6 +10,7 @@
 #include <memory>
 
 #include "lk_ffa.hpp"
+#include "lk_score.cuh"
 
 namespace lk {
 
@@ -177,7 +178,7 @@ const void* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t l
         const uint64_t n_inner = plan.param_counts[l][plan.nparams - 1];
         merge_level(in, out, level_coords(l), taylor, n_inner, plan.ncoords[l] / n_inner,
                     plan.ncoords[l - 1], plan.nsegments[l] * nbatch, nbins, s, is_bf16(l - 1),
-                    is_bf16(l));
+                    is_bf16(l), merge_pb);
         prof.end(s);
         in = out;
     }
@@ -220,7 +221,7 @@ void FFAExec::scores_impl(const float* ts_e, const float* ts_v, float* d_scores,
     merge_score_level(in, level_coords(L - 1), plan.nparams > 1, n_inner,
                       plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
                       static_cast<uint32_t>(plan.cfg.nbins), sp, LK_SCORE_PER_WIDTH, d_scores, s,
-                      nbatch, in_bf16, d_cmax);
+                      nbatch, in_bf16, d_cmax, score_cells);
     prof.end(s);
 }
 
@@ -273,6 +274,168 @@ uint64_t FFAExec::rescored_cells(cudaStream_t s) {
     uint64_t c = 0;
     LK_CUDA(cudaMemcpy(&c, cell_count.ptr, sizeof(c), cudaMemcpyDeviceToHost));
     return c;
+}
+
+namespace {
+
+// Sum of the recorded stage times of the given kinds (after a synchronise).
+float stage_ms(const StageProfiler& prof, std::initializer_list<int> kinds) {
+    float total = 0.0f;
+    for (size_t i = 0; i < prof.used; ++i) {
+        const auto& st = prof.stages[i];
+        for (int k : kinds) {
+            if (st.kind == k) {
+                float ms = 0.0f;
+                LK_CUDA(cudaEventElapsedTime(&ms, st.start, st.stop));
+                total += ms;
+            }
+        }
+    }
+    return total;
+}
+
+}  // namespace
+
+void FFAExec::apply_tuning(const lk_tuning& t) {
+    DeviceGuard g(device);
+    require(t.merge_rows_in_flight >= 0 && t.merge_rows_in_flight <= 16,
+            "merge rows in flight must lie in [0, 16]");
+    if (t.bf_rows != 0 || t.bf_warps != 0 || t.bf_stages != 0) {
+        require(bf->configure(t.bf_rows != 0 ? t.bf_rows : bf->rows(), t.bf_warps,
+                              t.bf_stages != 0 ? t.bf_stages : bf->stages()),
+                "brute-fold launch shape does not fit this plan");
+    }
+    merge_pb = t.merge_rows_in_flight;
+    score_cells = t.score_cells_per_block;
+    tuning = t;
+    tuning.bf_rows = bf->rows();
+    tuning.bf_warps = bf->warps();
+    tuning.bf_stages = bf->stages();
+}
+
+lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
+                            cudaStream_t s) {
+    require(plan.nsegments[plan.n_levels - 1] == 1,
+            "autotune needs a plan whose final level has one segment (a scoring plan)");
+    DeviceGuard g(device);
+    reps = std::max<uint32_t>(1, std::min<uint32_t>(reps, 20));
+    const uint64_t n = plan.ncoords[plan.n_levels - 1] * plan.widths.size();
+    if (scores_tmp.bytes < n * sizeof(float)) {
+        scores_tmp.alloc(n * sizeof(float));
+        compact_scratch.alloc(compact_scratch_bytes(n));
+    }
+    const bool was_enabled = prof.enabled;
+    prof.enabled = true;
+    lk_tuning best{};
+    uint32_t tried = 0;
+    // Median of reps timed passes (after one untimed pass) of the stages.
+    auto time_stages = [&](std::initializer_list<int> kinds) {
+        std::vector<float> t;
+        for (uint32_t r = 0; r <= reps; ++r) {
+            prof.reset();
+            scores_impl(ts_e, ts_v, scores_tmp.as<float>(), nullptr, s, 1);
+            LK_CUDA(cudaStreamSynchronize(s));
+            if (r > 0) {
+                t.push_back(stage_ms(prof, kinds));
+            }
+        }
+        std::sort(t.begin(), t.end());
+        ++tried;
+        return t[t.size() / 2];
+    };
+    try {
+        // 1. brute fold (with the interleave pass when both rows share a warp)
+        const uint32_t rows0 = bf->rows(), warps0 = bf->warps(), stages0 = bf->stages();
+        float bf_best = INFINITY;
+        uint32_t br = rows0, bw = warps0, bs = stages0;
+        for (uint32_t rows = 1; rows <= 2; ++rows) {
+            if (rows == 2 && plan.cfg.nbins > 128) {
+                continue;
+            }
+            for (uint32_t stages = 2; stages <= 4; ++stages) {
+                const uint32_t wmax = bf->max_warps(rows, stages);
+                if (wmax == 0) {
+                    continue;
+                }
+                std::vector<uint32_t> ws{0};
+                for (uint32_t w = wmax; w >= std::max<uint32_t>(1, (3 * wmax + 3) / 4); --w) {
+                    ws.push_back(w);
+                    if (w == 1) {
+                        break;
+                    }
+                }
+                for (uint32_t w : ws) {
+                    if (!bf->configure(rows, w, stages)) {
+                        continue;
+                    }
+                    const float ms = time_stages({LK_STAGE_TRANSPOSE, LK_STAGE_BRUTE_FOLD});
+                    if (ms < bf_best) {
+                        bf_best = ms;
+                        br = rows;
+                        bw = bf->warps();
+                        bs = stages;
+                    }
+                }
+            }
+        }
+        require(bf->configure(br, bw, bs), "autotune: lost the brute-fold shape");
+        // 2. merges
+        const uint32_t nb = static_cast<uint32_t>(plan.cfg.nbins);
+        std::vector<int> pbs{0};
+        if (nb == 32) {
+            pbs = {4, 8, 16};
+        } else if (nb == 64) {
+            pbs = {2, 4, 8};
+        } else if (nb == 128) {
+            pbs = {1, 2, 4};
+        }
+        float merge_best = INFINITY;
+        int bpb = 0;
+        if (plan.n_levels > 2) {
+            for (int pb : pbs) {
+                merge_pb = pb;
+                const float ms = time_stages({LK_STAGE_MERGE});
+                if (ms < merge_best) {
+                    merge_best = ms;
+                    bpb = pb;
+                }
+            }
+        } else {
+            merge_best = 0.0f;
+        }
+        merge_pb = bpb;
+        // 3. fused final level: cells per block
+        const uint32_t rs = sc::row_stride(nb, sp.wmax);
+        const uint32_t tmax = sc::profiles_per_block(rs);
+        float score_best = INFINITY;
+        uint32_t bcells = 0;
+        for (uint32_t cells = 32; cells <= tmax; cells += 32) {
+            score_cells = cells;
+            const float ms = time_stages({LK_STAGE_MERGE_SCORE});
+            if (ms < score_best) {
+                score_best = ms;
+                bcells = cells;
+            }
+        }
+        score_cells = bcells;
+        best.bf_rows = br;
+        best.bf_warps = bf->warps();
+        best.bf_stages = bs;
+        best.merge_rows_in_flight = bpb;
+        best.score_cells_per_block = bcells;
+        best.candidates = tried;
+        best.bf_ms = bf_best;
+        best.merge_ms = merge_best;
+        best.score_ms = score_best;
+    } catch (...) {
+        prof.enabled = was_enabled;
+        prof.reset();
+        throw;
+    }
+    prof.enabled = was_enabled;
+    prof.reset();
+    tuning = best;
+    return best;
 }
 
 std::vector<lk_stage_time> FFAExec::profile(cudaStream_t s) {

@@ -71,6 +71,18 @@ struct FFAExec {
     RescoreTree rtree{};
 
     uint64_t max_batch = 1;  // series per call (buffers are sized for it)
+    // Tuned launch shapes (0: defaults); see autotune.
+    int merge_pb = 0;            // merge: output rows per warp in flight
+    uint32_t score_cells = 0;    // final level + score: cells per block
+    lk_tuning tuning{};          // last autotune result / applied shapes
+
+    // Times launch-shape candidates of the brute fold (rows per warp,
+    // consumer warps per block, ring depth), the merges (rows in flight per
+    // warp) and the fused final level (cells per block) on the given series,
+    // stage by stage, and keeps the fastest of each. Every candidate computes
+    // the same sums in the same order, so results do not change.
+    lk_tuning autotune(const float* ts_e, const float* ts_v, uint32_t reps, cudaStream_t s);
+    void apply_tuning(const lk_tuning& t);
 
     FFAExec(const Plan& p, int device, int storage, uint64_t max_batch = 1);
     uint64_t device_bytes() const;

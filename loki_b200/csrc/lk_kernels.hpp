@@ -65,6 +65,12 @@ public:
                      uint64_t nbatch = 1);
     // True when bind_inputs launches the interleave kernel.
     bool interleaves() const { return m_rows == 2; }
+    // Launch shape (see brute_fold.cu); false when it does not fit.
+    bool configure(uint32_t rows, uint32_t warps, uint32_t stages);
+    uint32_t max_warps(uint32_t rows, uint32_t stages) const;
+    uint32_t rows() const { return m_rows; }
+    uint32_t warps() const { return m_warps; }
+    uint32_t stages() const { return m_stages; }
     void fold(float* d_fold, cudaStream_t s);
     uint64_t nseg() const { return m_nseg; }
     uint64_t nfreq() const { return m_nfreq; }
@@ -101,7 +107,8 @@ private:
 // Storage of input / output: FP32, or BF16 when the flag is set (adds are FP32).
 void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylor,
                  uint64_t n_inner, uint64_t n_outer, uint64_t ncoords_prev, uint64_t nsegments,
-                 uint32_t nbins, cudaStream_t s, bool in_bf16 = false, bool out_bf16 = false);
+                 uint32_t nbins, cudaStream_t s, bool in_bf16 = false, bool out_bf16 = false,
+                 int pb = 0);
 
 // Boxcar scoring parameters shared by the score kernels.
 struct ScoreParams {
@@ -119,7 +126,8 @@ ScoreParams make_score_params(const uint32_t* widths, uint32_t nwidths, uint32_t
 void merge_score_level(const void* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
                        uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                        const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s,
-                       uint64_t nbatch = 1, bool in_bf16 = false, float* d_cmax = nullptr);
+                       uint64_t nbatch = 1, bool in_bf16 = false, float* d_cmax = nullptr,
+                       uint32_t cells_per_block = 0);
 
 // Merge tree of the final FFA level: what the exact rescorer needs to rebuild
 // one final cell from the FP32 level-0 fold.

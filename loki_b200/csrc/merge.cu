@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kThreads)
 
 void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylor,
                  uint64_t n_inner, uint64_t n_outer, uint64_t ncoords_prev, uint64_t nsegments,
-                 uint32_t nbins, cudaStream_t s, bool in_bf16, bool out_bf16) {
+                 uint32_t nbins, cudaStream_t s, bool in_bf16, bool out_bf16, int pb) {
     require(n_inner > 0 && n_outer > 0, "empty merge level");
     const uint64_t tiles = (n_inner + kCoordsPerBlock - 1) / kCoordsPerBlock;
     require(tiles * n_outer <= 0x7fffffffULL && n_inner <= 0xffffffffULL &&
@@ -229,12 +229,20 @@ void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylo
             };
             auto pick = [&](auto tg) {
                 constexpr bool TG = decltype(tg)::value;
+                // pb: output rows per warp in flight (0: 8 / 4 / 2 for nbins
+                // 32 / 64 / 128, i.e. 16 loads of each kind per lane)
                 if (nbins == 32) {
-                    go_p2(merge_kernel_p2<TG, TIn, TOut, 32, 8>);
+                    pb == 4    ? go_p2(merge_kernel_p2<TG, TIn, TOut, 32, 4>)
+                    : pb == 16 ? go_p2(merge_kernel_p2<TG, TIn, TOut, 32, 16>)
+                               : go_p2(merge_kernel_p2<TG, TIn, TOut, 32, 8>);
                 } else if (nbins == 64) {
-                    go_p2(merge_kernel_p2<TG, TIn, TOut, 64, 4>);
+                    pb == 2   ? go_p2(merge_kernel_p2<TG, TIn, TOut, 64, 2>)
+                    : pb == 8 ? go_p2(merge_kernel_p2<TG, TIn, TOut, 64, 8>)
+                              : go_p2(merge_kernel_p2<TG, TIn, TOut, 64, 4>);
                 } else if (nbins == 128) {
-                    go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 2>);
+                    pb == 1   ? go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 1>)
+                    : pb == 4 ? go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 4>)
+                              : go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 2>);
                 } else if (nbins <= 32) {
                     go(merge_kernel_mlp<TG, TIn, TOut, 1, 8>);
                 } else if (nbins <= 64) {

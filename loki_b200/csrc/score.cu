@@ -228,13 +228,17 @@ void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d
 void merge_score_level(const void* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
                        uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                        const ScoreParams& sp, int mode, float* d_scores, cudaStream_t s,
-                       uint64_t nbatch, bool in_bf16, float* d_cmax) {
+                       uint64_t nbatch, bool in_bf16, float* d_cmax, uint32_t cells_per_block) {
     require(nbatch >= 1 && nbatch <= 65535, "nbatch must lie in [1, 65535]");
     if (n_inner == 0 || n_outer == 0) {
         return;
     }
     const uint32_t rs = row_stride(nbins, sp.wmax);
-    const uint32_t T = profiles_per_block(rs);
+    // cells per block: a multiple of 32 up to the shared-memory default
+    const uint32_t Tmax = profiles_per_block(rs);
+    const uint32_t T = (cells_per_block >= 32 && cells_per_block % 32 == 0 && cells_per_block <= Tmax)
+                           ? cells_per_block
+                           : Tmax;
     const size_t smem = static_cast<size_t>(T) * rs * sizeof(float);
     const uint64_t tiles = (n_inner + T - 1) / T;
     require(tiles * n_outer <= 0x7fffffffULL && n_inner <= 0xffffffffULL,

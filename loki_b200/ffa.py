@@ -200,6 +200,33 @@ class FFACUDA:
         C.check(C.lib().lk_ffa_status(self._h, D.stream_ptr(self._device), ctypes.byref(st)))
         return st.value
 
+    _TUNING_FIELDS = ("bf_rows", "bf_warps", "bf_stages", "merge_rows_in_flight", "score_cells_per_block")
+
+    def autotune(self, ts_e, ts_v, reps: int = 3) -> dict:
+        """Time launch-shape candidates of the brute fold, the merges and the
+        fused final level on this series (CUDA tensors or host arrays) and keep
+        the fastest of each; results are unchanged. Returns the tuning with
+        the best stage times (ms)."""
+        e, v = self._inputs(ts_e, ts_v)
+        t = C.LkTuning()
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_ffa_autotune(self._h, D.ptr(e), D.ptr(v), int(reps), ctypes.byref(t),
+                                            D.stream_ptr(self._device)))
+        return {name: getattr(t, name) for name, _ in C.LkTuning._fields_}
+
+    @property
+    def tuning(self) -> dict:
+        t = C.LkTuning()
+        C.check(C.lib().lk_ffa_get_tuning(self._h, ctypes.byref(t)))
+        return {name: getattr(t, name) for name, _ in C.LkTuning._fields_}
+
+    def set_tuning(self, tuning: dict) -> None:
+        """Apply a tuning returned by ``autotune`` / ``tuning`` (launch shapes only)."""
+        t = C.LkTuning()
+        for name in self._TUNING_FIELDS:
+            setattr(t, name, int(tuning.get(name, 0)))
+        C.check(C.lib().lk_ffa_set_tuning(self._h, ctypes.byref(t)))
+
     @property
     def rescore_margin(self) -> tuple[float, float]:
         """BF16 search margin (abs, rel): cells with approximate best S/N >=

@@ -124,3 +124,39 @@ def test_search_pipeline_matches_search(cuda):
         assert gn == wn
         np.testing.assert_array_equal(gi, wi)
         np.testing.assert_array_equal(gs.view(np.uint32), ws.view(np.uint32))
+
+
+@pytest.mark.parametrize("nbins,lims,storage", [(64, [[-200.0, 200.0], [5.0, 50.0]], "fp32"),
+                                                (32, [[-300.0, 300.0], [5.0, 8.0]], "bf16"),
+                                                (128, [[20.0, 60.0]], "fp32")])
+def test_autotune_keeps_results(cuda, nbins, lims, storage):
+    """The autotuner only changes launch shapes: scores stay bit-exact with
+    the oracle and a BF16 search keeps the FP32 candidates."""
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+
+    ns = 2**18
+    cfg = PulsarSearchConfig(ns, 1e-3 if len(lims) == 2 and nbins == 32 else 64e-6, nbins, 1.0, np.array(lims),
+                             use_fourier=False, score_widths=[1, 2, 3, 4])
+    op = lko.plan_create(lko.make_cfg(ns, cfg.tsamp, nbins, 1.0, lims))
+    e, v = series(ns, 91)
+    ffa = FFACUDA(cfg, fold_storage=storage)
+    t = ffa.autotune(e, v, reps=1)
+    assert t["candidates"] > 3 and t["bf_rows"] in (1, 2) and t["bf_warps"] >= 1 and t["bf_stages"] >= 2
+    assert ffa.tuning["bf_warps"] == t["bf_warps"]
+    if storage == "fp32":
+        want = lko.snr_boxcar_3d(lko.ffa(op, e, v), np.array([1, 2, 3, 4], np.uint64), nbins).ravel()
+        got = ffa.scores(e, v)
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    else:
+        plain = FFACUDA(cfg)
+        thr = float(np.quantile(plain.scores(e, v), 0.999))
+        a = plain.search(e, v, snr_min=thr)
+        b = ffa.search(e, v, snr_min=thr)
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+    # a saved tuning applies to a fresh executor
+    other = FFACUDA(cfg, fold_storage=storage)
+    other.set_tuning(t)
+    for k in ("bf_rows", "bf_warps", "bf_stages", "merge_rows_in_flight", "score_cells_per_block"):
+        assert other.tuning[k] == t[k]
