@@ -206,6 +206,59 @@ int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status);
  * must be finite and >= 0; calls on an LK_FP32 executor are no-ops. */
 int lk_ffa_set_rescore_margin(lk_ffa* ffa, float margin_abs, float margin_rel);
 int lk_ffa_get_rescore_margin(const lk_ffa* ffa, float* margin_abs, float* margin_rel);
+/* ---- FFAFreqSweep (replaces algorithms::FFAFreqSweep) ------------------- */
+/* The reference's production caller (lib/ffa_freq_sweep.cpp:76-269,
+ * lib/regions.cpp:31-514): octave regions of growing nbins, each cut into
+ * chunks that fit max_memory_gb (bisection over the chunk width, frequency
+ * ranges widened by the largest Doppler drift), then per chunk FFA + boxcar
+ * scores + `>= snr_min` compaction and the parameter decode of every passing
+ * (coordinate, width). The base configuration supplies nsamps, tsamp, the
+ * smallest nbins, eta, the parameter limits (frequency last), widths and
+ * snr_min. Results replace the HDF5 writer: per candidate nparams + 1
+ * doubles (parameter values, then the width) and its S/N, in region order. */
+typedef struct lk_sweep lk_sweep;
+typedef struct lk_sweep_options {
+    double max_memory_gb;             /* max_process_memory_gb (reference default 8.0) */
+    double octave_scale;              /* 2.0 */
+    uint64_t nbins_max;               /* 1024 */
+    uint64_t max_passing_candidates;  /* 1 << 22 */
+    /* 0: decode every chunk's candidates with the base configuration's width
+     * list, as save_results does (lib/ffa_freq_sweep.cpp:202-233), which
+     * mislabels candidates of a chunk whose nbins gives another width count;
+     * 1: decode with the chunk's own widths. */
+    int32_t decode_chunk_widths;
+    /* 1: the device memory model of FFAFreqSweepCUDA (input series, scores and
+     * indices, fold buffers, coordinates; lib/regions.cpp:136-149); 0: the
+     * process model of FFAFreqSweep (fold buffers, coordinates, scores,
+     * indices, write batch; lib/regions.cpp:101-135). */
+    int32_t device_memory_model;
+} lk_sweep_options;
+/* regions::generate_ffa_regions (lib/regions.cpp:31-78): rows of (f_start,
+ * f_end, nbins, eta); *n_out regions, rows written up to cap. */
+int lk_generate_ffa_regions(double p_min, double p_max, double tsamp, uint64_t nbins_min,
+                            double eta_min, double octave_scale, uint64_t nbins_max,
+                            double* rows, uint64_t cap, uint64_t* n_out);
+typedef struct lk_sweep_chunk {
+    double f_min, f_max;              /* drift-widened frequency limits */
+    double nominal_f_start, nominal_f_end;
+    uint64_t nbins;
+    double eta;
+    uint64_t buffer_size, coord_size, ncoords, n_levels;
+    double memory_gb;                 /* this chunk alone */
+    double allocated_gb;              /* with the largest sizes of the chunks up to it */
+} lk_sweep_chunk;
+int lk_sweep_create(const lk_config* base, const lk_sweep_options* opt, int device, int storage,
+                    lk_sweep** out);
+void lk_sweep_destroy(lk_sweep* sw);
+int lk_sweep_nchunks(const lk_sweep* sw, uint64_t* n);
+int lk_sweep_chunk_info(const lk_sweep* sw, uint64_t i, lk_sweep_chunk* out);
+/* Device series (nsamps floats each). Synchronises the stream. */
+int lk_sweep_execute(lk_sweep* sw, const float* d_ts_e, const float* d_ts_v, lk_stream_t stream);
+/* Host outputs of the last execute: *n_out candidates; params [n][nparams + 1]
+ * and scores [n] written up to max_out; region_counts [nchunks] may be NULL. */
+int lk_sweep_results(const lk_sweep* sw, double* params, float* scores, uint64_t max_out,
+                     uint64_t* n_out, uint64_t* region_counts);
+
 /* Launch-shape tuning (north-star "autotuner"; no reference counterpart).
  * bf_*: brute fold rows (E, V) per consumer warp (1 or 2), consumer warps
  * per block (0: the wave-count rule), shared-memory ring depth in 32-sample

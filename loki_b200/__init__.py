@@ -18,8 +18,8 @@ from ._capi import LokiError, lib
 # Fail loudly at import time if the native library is missing.
 lib()
 
-from . import batched, configs, ffa, fold, pipeline, plans, prune, scores, thresholds  # noqa: E402
+from . import batched, configs, ffa, fold, pipeline, plans, prune, scores, sweep, thresholds  # noqa: E402
 from . import libculoki  # noqa: E402
 
-__all__ = ["configs", "plans", "ffa", "fold", "prune", "scores", "thresholds", "batched", "libculoki",
+__all__ = ["configs", "plans", "ffa", "fold", "prune", "scores", "sweep", "thresholds", "batched", "libculoki",
            "LokiError", "lib"]

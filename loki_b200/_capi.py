@@ -108,6 +108,18 @@ class LkTuning(ctypes.Structure):
                 ("score_ms", f32)]
 
 
+class LkSweepOptions(ctypes.Structure):
+    _fields_ = [("max_memory_gb", f64), ("octave_scale", f64), ("nbins_max", u64),
+                ("max_passing_candidates", u64), ("decode_chunk_widths", ctypes.c_int32),
+                ("device_memory_model", ctypes.c_int32)]
+
+
+class LkSweepChunk(ctypes.Structure):
+    _fields_ = [("f_min", f64), ("f_max", f64), ("nominal_f_start", f64), ("nominal_f_end", f64),
+                ("nbins", u64), ("eta", f64), ("buffer_size", u64), ("coord_size", u64), ("ncoords", u64),
+                ("n_levels", u64), ("memory_gb", f64), ("allocated_gb", f64)]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 class LkPruneStats(ctypes.Structure):
     _fields_ = [
@@ -147,6 +159,13 @@ SIGNATURES = [
     ("lk_ffa_set_rescore_margin", i32, [vp, ctypes.c_float, ctypes.c_float]),
     ("lk_ffa_get_rescore_margin", i32, [vp, vp, vp]),
     ("lk_ffa_rescored_cells", i32, [vp, vp, vp]),
+    ("lk_sweep_create", i32, [vp, vp, i32, i32, vp]),
+    ("lk_sweep_destroy", None, [vp]),
+    ("lk_sweep_nchunks", i32, [vp, vp]),
+    ("lk_sweep_chunk_info", i32, [vp, u64, vp]),
+    ("lk_sweep_execute", i32, [vp, vp, vp, vp]),
+    ("lk_sweep_results", i32, [vp, vp, vp, u64, vp, vp]),
+    ("lk_generate_ffa_regions", i32, [f64, f64, f64, u64, f64, f64, u64, vp, u64, vp]),
     ("lk_ffa_autotune", i32, [vp, vp, vp, u32, vp, vp]),
     ("lk_ffa_get_tuning", i32, [vp, vp]),
     ("lk_ffa_set_tuning", i32, [vp, vp]),

@@ -12,6 +12,7 @@
 #include "lk_kernels.hpp"
 #include "lk_mc.hpp"
 #include "lk_prune.hpp"
+#include "lk_sweep.hpp"
 
 struct lk_plan {
     lk::Plan plan;
@@ -24,6 +25,9 @@ struct lk_mc {
 };
 struct lk_prune {
     std::unique_ptr<lk::PruneExec> exec;
+};
+struct lk_sweep {
+    std::unique_ptr<lk::FreqSweepExec> exec;
 };
 struct lk_brute_fold {
     int device = 0;
@@ -74,7 +78,7 @@ int lk_plan_create(const lk_config* cfg, lk_plan** out) {
         need(cfg, "cfg");
         need(out, "out");
         auto p = std::make_unique<lk_plan>();
-        p->plan = lk::make_plan(*cfg);
+        p->plan = lk::make_plan(*cfg, /*sizes_only=*/true);
         *out = p.release();
     });
 }
@@ -310,6 +314,113 @@ int lk_ffa_rescored_cells(lk_ffa* ffa, lk_stream_t stream, uint64_t* n_cells) {
         need(ffa, "ffa");
         need(n_cells, "n_cells");
         *n_cells = ffa->exec->rescored_cells(reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_sweep_create(const lk_config* base, const lk_sweep_options* opt, int device, int storage,
+                    lk_sweep** out) {
+    return guarded([&] {
+        need(base, "base");
+        need(out, "out");
+        lk::SweepOptions o;
+        if (opt != nullptr) {
+            o.max_memory_gb = opt->max_memory_gb;
+            o.octave_scale = opt->octave_scale;
+            o.nbins_max = opt->nbins_max;
+            o.max_passing_candidates = opt->max_passing_candidates;
+            o.decode_chunk_widths = opt->decode_chunk_widths != 0;
+            o.device_memory_model = opt->device_memory_model != 0;
+        }
+        lk::require(o.max_memory_gb > 0, "max_process_memory_gb must be positive");
+        auto h = std::make_unique<lk_sweep>();
+        h->exec = std::make_unique<lk::FreqSweepExec>(*base, o, device, storage);
+        *out = h.release();
+    });
+}
+
+void lk_sweep_destroy(lk_sweep* sw) { delete sw; }
+
+int lk_generate_ffa_regions(double p_min, double p_max, double tsamp, uint64_t nbins_min,
+                            double eta_min, double octave_scale, uint64_t nbins_max,
+                            double* rows, uint64_t cap, uint64_t* n_out) {
+    return guarded([&] {
+        need(n_out, "n_out");
+        const auto rg = lk::generate_ffa_regions(p_min, p_max, tsamp, nbins_min, eta_min,
+                                                 octave_scale, nbins_max);
+        *n_out = rg.size();
+        if (cap > 0) {
+            need(rows, "rows");
+        }
+        for (size_t i = 0; i < rg.size() && i < cap; ++i) {
+            rows[4 * i + 0] = rg[i].f_start;
+            rows[4 * i + 1] = rg[i].f_end;
+            rows[4 * i + 2] = static_cast<double>(rg[i].nbins);
+            rows[4 * i + 3] = rg[i].eta;
+        }
+    });
+}
+
+int lk_sweep_nchunks(const lk_sweep* sw, uint64_t* n) {
+    return guarded([&] {
+        need(sw, "sw");
+        need(n, "n");
+        *n = sw->exec->chunks().size();
+    });
+}
+
+int lk_sweep_chunk_info(const lk_sweep* sw, uint64_t i, lk_sweep_chunk* out) {
+    return guarded([&] {
+        need(sw, "sw");
+        need(out, "out");
+        const auto& ch = sw->exec->chunks();
+        lk::require(i < ch.size(), "chunk index out of range");
+        const auto& c = ch[i];
+        const uint32_t np = c.cfg.nparams;
+        out->f_min = c.cfg.param_limits[2 * (np - 1)];
+        out->f_max = c.cfg.param_limits[2 * (np - 1) + 1];
+        out->nominal_f_start = c.nominal_f_start;
+        out->nominal_f_end = c.nominal_f_end;
+        out->nbins = c.cfg.nbins;
+        out->eta = c.cfg.eta;
+        out->buffer_size = c.buffer_size;
+        out->coord_size = c.coord_size;
+        out->ncoords = c.ncoords;
+        out->n_levels = c.n_levels;
+        out->memory_gb = c.memory_gb;
+        out->allocated_gb = c.allocated_gb;
+    });
+}
+
+int lk_sweep_execute(lk_sweep* sw, const float* d_ts_e, const float* d_ts_v, lk_stream_t stream) {
+    return guarded([&] {
+        need(sw, "sw");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        sw->exec->execute(d_ts_e, d_ts_v, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_sweep_results(const lk_sweep* sw, double* params, float* scores, uint64_t max_out,
+                     uint64_t* n_out, uint64_t* region_counts) {
+    return guarded([&] {
+        need(sw, "sw");
+        need(n_out, "n_out");
+        const auto& sc = sw->exec->scores();
+        const auto& pr = sw->exec->params();
+        const uint64_t n = sc.size();
+        const uint64_t k = std::min(n, max_out);
+        const uint64_t stride = sw->exec->nparams() + 1;
+        *n_out = n;
+        if (k > 0) {
+            need(params, "params");
+            need(scores, "scores");
+            std::copy_n(pr.begin(), k * stride, params);
+            std::copy_n(sc.begin(), k, scores);
+        }
+        if (region_counts != nullptr) {
+            const auto& rc = sw->exec->region_counts();
+            std::copy(rc.begin(), rc.end(), region_counts);
+        }
     });
 }
 

@@ -50,6 +50,7 @@ StageProfiler::~StageProfiler() {
 
 FFAExec::FFAExec(const Plan& p, int device, int storage, uint64_t max_batch_)
     : plan(p), device(device), max_batch(max_batch_) {
+    require(!plan.offsets_overflow, "coordinate offsets exceed 32 bits");
     require(max_batch >= 1 && max_batch <= 65535, "max_batch must lie in [1, 65535]");
     require(storage == LK_FP32 || storage == LK_BF16 || storage == LK_FP16,
             "fold storage must be LK_FP32, LK_BF16 or LK_FP16");

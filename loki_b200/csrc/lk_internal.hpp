@@ -52,6 +52,7 @@ struct Plan {
     std::vector<uint64_t> segment_lens, nsegments, ncoords;
     std::vector<double> tsegments;
     std::vector<uint32_t> ncoords_offsets;
+    bool offsets_overflow = false;  // offsets or final ncoords past 32 bits (sizes-only plan)
     std::vector<std::vector<uint64_t>> param_counts;
     std::vector<std::vector<double>> dparams, dparams_actual;
     std::vector<uint32_t> widths;
@@ -73,7 +74,7 @@ struct Plan {
     uint64_t prune_branch_max(bool conservative, int basis = 0) const;
 };
 
-Plan make_plan(const lk_config& cfg);
+Plan make_plan(const lk_config& cfg, bool sizes_only = false);
 std::vector<uint32_t> box_width_trials(uint64_t nbins, double ducy_max, double wtsp);
 
 // psr_utils::range_param (lib/loki/psr_utils.hpp:254-270).

@@ -1,0 +1,73 @@
+// FFAFreqSweep: region planner and executor (sweep.cpp).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "lk_internal.hpp"
+#include "lk_kernels.hpp"
+
+namespace lk {
+
+struct FFAExec;
+
+// coord::FFARegion (include/loki/common/coord.hpp): one octave of the sweep.
+struct SweepRegion {
+    double f_start, f_end;
+    uint64_t nbins;
+    double eta;
+};
+
+// The planner's knobs (PulsarSearchConfig defaults of the reference).
+struct SweepOptions {
+    double max_memory_gb = 8.0;           // max_process_memory_gb
+    double octave_scale = 2.0;
+    uint64_t nbins_max = 1024;
+    uint64_t max_passing_candidates = 1ull << 22;
+    bool decode_chunk_widths = false;  // false: the reference's decode (base widths)
+    bool device_memory_model = true;   // FFAFreqSweepCUDA's model; false: FFAFreqSweep's
+};
+
+// One chunk: its configuration (drift-widened frequency limits, the region's
+// nbins and eta), nominal range and the plan sizes behind the memory model.
+struct SweepChunk {
+    lk_config cfg;
+    double nominal_f_start, nominal_f_end;
+    uint64_t buffer_size, coord_size, ncoords, n_levels;
+    double memory_gb;     // this chunk alone
+    double allocated_gb;  // with the largest sizes of the chunks before it
+};
+
+std::vector<SweepRegion> generate_ffa_regions(double p_min, double p_max, double tsamp,
+                                              uint64_t nbins_min, double eta_min,
+                                              double octave_scale, uint64_t nbins_max);
+std::vector<SweepChunk> plan_freq_sweep(const lk_config& base, const SweepOptions& opt);
+
+class FreqSweepExec {
+public:
+    FreqSweepExec(const lk_config& base, const SweepOptions& opt, int device, int storage);
+    ~FreqSweepExec();
+    // Every chunk: FFA + scores + compaction `>= snr_min` + parameter decode.
+    // Synchronises the stream once per chunk.
+    void execute(const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
+    const std::vector<SweepChunk>& chunks() const { return m_chunks; }
+    const std::vector<double>& params() const { return m_params; }   // [n][nparams + 1]
+    const std::vector<float>& scores() const { return m_scores; }
+    const std::vector<uint64_t>& region_counts() const { return m_region_counts; }
+    uint32_t nparams() const { return m_base.nparams; }
+
+private:
+    FFAExec& exec(size_t i);
+    lk_config m_base;
+    SweepOptions m_opt;
+    int m_device, m_storage;
+    std::vector<SweepChunk> m_chunks;
+    std::vector<uint32_t> m_base_widths;
+    std::vector<std::unique_ptr<FFAExec>> m_execs;
+    DeviceBuffer m_idx, m_snr, m_cnt;
+    std::vector<double> m_params;
+    std::vector<float> m_scores;
+    std::vector<uint64_t> m_region_counts;
+};
+
+}  // namespace lk

@@ -390,7 +390,7 @@ std::vector<double> Plan::dparams_at(double tseg_cur, int kind) const {
     return d;
 }
 
-Plan make_plan(const lk_config& cfg) {
+Plan make_plan(const lk_config& cfg, bool sizes_only) {
     Plan p;
     p.cfg = cfg;
     const uint32_t np = cfg.nparams;
@@ -473,7 +473,13 @@ Plan make_plan(const lk_config& cfg) {
             nc *= c;
         }
         p.ncoords[l] = nc;
-        require(offset + nc <= 0xffffffffULL, "coordinate offsets exceed 32 bits");
+        // The level offsets are 32-bit (as the reference's). A plan made for
+        // its sizes only (a configuration, the sweep planner's probes) may
+        // exceed that; executors and coordinate resolution refuse it.
+        if (offset + nc > 0xffffffffULL) {
+            require(sizes_only, "coordinate offsets exceed 32 bits");
+            p.offsets_overflow = true;
+        }
         p.ncoords_offsets[l] = static_cast<uint32_t>(offset);
         offset += nc;
         p.buffer_size = std::max(p.buffer_size, p.fold_size(l));
@@ -486,8 +492,12 @@ Plan make_plan(const lk_config& cfg) {
                 "FFAPlan::validate_plan: Only one parameter for higher order derivatives is "
                 "supported for the initialization for the first level");
     }
-    // Final coordinates index the fold with 32-bit values.
-    require(p.ncoords[L - 1] <= 0xffffffffULL, "too many final coordinates");
+    // Final coordinates index the fold with 32-bit values (sizes-only plans
+    // are flagged instead, like the offsets).
+    if (p.ncoords[L - 1] > 0xffffffffULL) {
+        require(sizes_only, "too many final coordinates");
+        p.offsets_overflow = true;
+    }
     return p;
 }
 

@@ -1116,6 +1116,7 @@ PruneExec::PruneExec(const Plan& plan, uint64_t max_sugg, uint64_t batch_size,
       m_conservative(conservative),
       m_basis(basis) {
     m_np = plan.nparams;
+    require(!plan.offsets_overflow, "coordinate offsets exceed 32 bits");
     require(m_np == 2 || m_np == 3,
             "pruning is implemented for searches with nparams 2 (accel) or 3 (jerk)");
     require(basis == 0 || basis == 1, "poly_basis must be taylor (0) or chebyshev (1)");

@@ -134,6 +134,7 @@ __global__ void resolve_jerk_kernel(LevelArgs a, CoordTaylor* __restrict__ out) 
 }  // namespace
 
 void resolve_coords_device(const Plan& plan, void* d_coords, cudaStream_t stream) {
+    require(!plan.offsets_overflow, "coordinate offsets exceed 32 bits");
     const uint32_t np = plan.nparams;
     if (np > 3) {
         fail(LK_ERR_UNSUPPORTED, "coordinate resolution supports nparams <= 3");

@@ -257,3 +257,6 @@ def compute_ffa_scores_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int 
     _check_time_domain(cfg)
     ffa = FFACUDA(cfg, device_id)
     return ffa.scores(np.asarray(ts_e, dtype=np.float32), np.asarray(ts_v, dtype=np.float32)), ffa.plan
+
+
+from .sweep import FFAFreqSweepCUDA  # noqa: E402  (the reference binds it in the ffa submodule)

@@ -3,8 +3,8 @@
 reference reads the same:
 
     libculoki.configs.PulsarSearchConfig
-    libculoki.plans.FFAPlanTime
-    libculoki.ffa.{FFACUDA, compute_ffa_time_cuda, compute_ffa_scores_cuda}
+    libculoki.plans.{FFAPlanTime, FFARegionPlannerTime, generate_ffa_regions}
+    libculoki.ffa.{FFACUDA, FFAFreqSweepCUDA, compute_ffa_time_cuda, compute_ffa_scores_cuda}
     libculoki.fold.compute_brute_fold_time_cuda
     libculoki.scores.{snr_boxcar_3d, snr_boxcar_3d_max, snr_boxcar_2d_max,
                       generate_box_width_trials}

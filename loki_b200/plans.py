@@ -191,3 +191,7 @@ class FFAPlanTime:
     def resolve_coordinates_flat(self, device_id: int = 0) -> np.ndarray:
         """All levels in one array (coord_size entries, level 0 zeroed)."""
         return self._resolve(device_id)
+
+
+# The reference binds the region planner in the plans submodule.
+from .sweep import FFARegionPlannerTime, generate_ffa_regions  # noqa: E402

@@ -107,6 +107,7 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
                                       vp, vp, vp, vp, vp, u64, vp]
         L.lkref_prune_run_basis.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64, u64,
                                       vp, vp, vp, vp, vp, u64, vp]
+        L.lkref_region_plan.argtypes = [vp, f64, f64, u64, u64, ctypes.c_int, vp, u64, vp, vp]
         _libs[path] = L
     return _libs[path]
 
@@ -449,3 +450,20 @@ def snr_threshold(profiles, nbins, widths, thresholds, stdnoise) -> np.ndarray:
     out = np.zeros(n, np.uint8)
     _check(L, L.lkref_snr_threshold(_p(p), n, nbins, _p(w), w.size, _p(t), stdnoise, _p(out)))
     return out.astype(bool)
+
+
+def region_plan(cfg: RefCfg, max_memory_gb=8.0, octave_scale=2.0, nbins_max=1024, max_passing=1 << 22,
+                use_gpu=False):
+    """FFARegionPlanner<float> of the reference: (chunks [n, 6] = f_min, f_max,
+    nbins, eta, bseg_brute, bseg_ffa; stats [5] = max buffer size, max coord
+    size, max ncoords, max levels, sweep memory usage in GB -- the device
+    model when use_gpu)."""
+    L = lib()
+    cap = 4096
+    rows = np.zeros(cap * 6, np.float64)
+    stats = np.zeros(5, np.float64)
+    n = u64()
+    _check(L, L.lkref_region_plan(ctypes.byref(cfg), max_memory_gb, octave_scale, nbins_max, max_passing,
+                                  int(use_gpu), _p(rows), cap, ctypes.byref(n), _p(stats)))
+    k = min(n.value, cap)
+    return rows[: k * 6].reshape(k, 6), stats

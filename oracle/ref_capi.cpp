@@ -49,6 +49,7 @@
 
 #include "loki/algorithms/ffa.hpp"
 #include "loki/algorithms/fold.hpp"
+#include "loki/algorithms/regions.hpp"
 #include "loki/common/coord.hpp"
 #include "loki/common/plans.hpp"
 #include "loki/common/types.hpp"
@@ -592,6 +593,53 @@ int lkref_prune_run(const lkref_cfg* c, int conservative, const float* ffa_fold,
     return prune_run_basis("taylor", c, conservative, ffa_fold, ffa_fold_len, thresholds,
                            n_thresholds, ref_seg, max_sugg, batch_size, branch_max, n_iters,
                            stats, n_stats, leaves_out, folds_out, scores_out, cap_out, n_out);
+}
+
+// FFARegionPlanner<float> (lib/regions.cpp:157-514) on a base configuration
+// with the given planner knobs. Per chunk, 6 doubles: f_min, f_max (the
+// drift-widened frequency limits), nbins, eta, bseg_brute, bseg_ffa. stats_out
+// (5 doubles): max buffer size, max coord size, max ncoords, max FFA levels,
+// get_freq_sweep_memory_usage() in GB (the device model when use_gpu).
+int lkref_region_plan(const lkref_cfg* c, double max_memory_gb, double octave_scale,
+                      uint64_t nbins_max, uint64_t max_passing, int use_gpu, double* chunks_out,
+                      uint64_t cap, uint64_t* n_out, double* stats_out) {
+    return guarded([&] {
+        std::vector<loki::ParamLimit> lims(c->nparams);
+        for (uint32_t i = 0; i < c->nparams; ++i) {
+            lims[i] = {.min = c->limits[2 * i], .max = c->limits[(2 * i) + 1]};
+        }
+        std::optional<loki::SizeType> bb;
+        std::optional<loki::SizeType> bf;
+        if (c->bseg_brute != 0) {
+            bb = c->bseg_brute;
+        }
+        if (c->bseg_ffa != 0) {
+            bf = c->bseg_ffa;
+        }
+        const loki::search::PulsarSearchConfig cfg(
+            c->nsamps, c->tsamp, c->nbins, c->eta, lims, c->ducy_max, c->wtsp,
+            /*use_fourier=*/false, c->nthreads, max_memory_gb, octave_scale, nbins_max,
+            /*nbins_min_lossy_bf=*/64, bb, bf, /*snr_min=*/5.0, max_passing);
+        const loki::regions::FFARegionPlanner<float> planner(cfg, use_gpu != 0);
+        const auto& cfgs = planner.get_cfgs();
+        *n_out = cfgs.size();
+        for (std::size_t i = 0; i < cfgs.size() && i < cap; ++i) {
+            const auto pl = cfgs[i].get_param_limits();
+            double* row = chunks_out + (6 * i);
+            row[0] = pl.back().min;
+            row[1] = pl.back().max;
+            row[2] = static_cast<double>(cfgs[i].get_nbins());
+            row[3] = cfgs[i].get_eta();
+            row[4] = static_cast<double>(cfgs[i].get_bseg_brute());
+            row[5] = static_cast<double>(cfgs[i].get_bseg_ffa());
+        }
+        const auto& st = planner.get_stats();
+        stats_out[0] = static_cast<double>(st.get_max_buffer_size());
+        stats_out[1] = static_cast<double>(st.get_max_coord_size());
+        stats_out[2] = static_cast<double>(st.get_max_ncoords());
+        stats_out[3] = static_cast<double>(st.get_max_ffa_levels());
+        stats_out[4] = static_cast<double>(st.get_freq_sweep_memory_usage());
+    });
 }
 
 // The same run with poly_basis "taylor" (basis 0) or "chebyshev" (basis 1).

@@ -4,6 +4,7 @@ Run from the repository root after ``make -C oracle ref``:
 
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py prune    # the pruning fixtures only
+    python tests/golden/make_golden.py sweep    # the frequency-sweep fixtures only
 
 Every output comes from ``oracle/_ref/libloki_ref_parity.so`` -- the
 reference's CPU sources compiled unmodified with IEEE flags -- so the fixtures
@@ -160,11 +161,83 @@ def prune_fixtures() -> None:
         print(name, "nsegments", nseg, "survivors", leaves.shape[0])
 
 
+# Frequency-sweep chunk plans: name -> (nsamps, tsamp, nbins, eta, param_limits,
+# max_process_memory_gb, max_passing_candidates, use_gpu). The small memory
+# limits force the bisection, sliver and drift-widening paths.
+SWEEP_PLAN_CASES = {
+    "accel_2p22_8gb_cpu": (1 << 22, 64e-6, 64, 2.0, [[-200.0, 200.0], [1.0, 500.0]], 8.0, 1 << 22, False),
+    "accel_2p22_8gb_gpu": (1 << 22, 64e-6, 64, 2.0, [[-200.0, 200.0], [1.0, 500.0]], 8.0, 1 << 22, True),
+    "freq_2p22_2gb_gpu": (1 << 22, 64e-6, 32, 1.0, [[0.5, 800.0]], 2.0, 1 << 22, True),
+    "jerk_2p20_3gb_cpu": (1 << 20, 64e-6, 32, 2.0, [[-30.0, 30.0], [-300.0, 300.0], [5.0, 200.0]], 3.0, 1 << 20,
+                          False),
+    "freq_2p16_tight_gpu": (1 << 16, 1e-3, 32, 1.0, [[1.0, 40.0]], 0.508, 4096, True),
+    "freq_2p16_tight_cpu": (1 << 16, 1e-3, 32, 1.0, [[1.0, 40.0]], 0.508, 4096, False),
+    "accel_2p16_tight_gpu": (1 << 16, 1e-3, 32, 2.0, [[-50.0, 50.0], [2.0, 30.0]], 0.503, 4096, True),
+    "jerk_2p15_tight_gpu": (1 << 15, 2e-3, 16, 2.0, [[-2.0, 2.0], [-20.0, 20.0], [2.0, 12.0]], 0.5004, 4096,
+                            True),
+}
+
+# Whole sweeps (reference planner + reference FFA and scores per chunk +
+# compaction + save_results decode): name -> (plan case, snr_min, seed,
+# pulsars (f0, amplitude, duty)).
+SWEEP_RUN_CASES = {
+    "sweep_freq_2p16": ("freq_2p16_tight_gpu", 6.0, 21, [(3.3, 0.6, 0.05), (17.9, 0.5, 0.03)]),
+    "sweep_accel_2p16": ("accel_2p16_tight_gpu", 6.0, 22, [(5.1, 0.5, 0.05), (24.4, 0.5, 0.04)]),
+    "sweep_jerk_2p15": ("jerk_2p15_tight_gpu", 4.5, 23, [(7.7, 0.6, 0.05), (3.2, 0.5, 0.05)]),
+}
+
+
+def _ref_backend(nsamps, tsamp, nbins, eta, lims, ts_e, ts_v, widths=None):
+    cfg = ref.make_cfg(nsamps, tsamp, nbins, eta, lims)
+    ffa = ref.RefFFA(cfg)
+    w = ref.box_widths(nbins) if widths is None else np.asarray(widths, np.uint64)
+    fold = ffa.execute(ts_e, ts_v).copy()
+    return ref.snr_boxcar_3d(fold, w, nbins).ravel(), ffa.param_counts[-1].copy(), w
+
+
+def sweep_fixtures() -> None:
+    from oracle import sweep as osweep
+
+    plans = {}
+    for name, (nsamps, tsamp, nbins, eta, lims, mem, mp, gpu) in SWEEP_PLAN_CASES.items():
+        rows, stats = ref.region_plan(ref.make_cfg(nsamps, tsamp, nbins, eta, lims), mem, 2.0, 1024, mp, gpu)
+        plans[f"{name}__rows"] = rows
+        plans[f"{name}__stats"] = stats
+        plans[f"{name}__inputs"] = np.array([nsamps, tsamp, nbins, eta, mem, mp, float(gpu)], np.float64)
+        plans[f"{name}__lims"] = np.array(lims, np.float64)
+        print(name, "chunks", rows.shape[0])
+    np.savez_compressed(os.path.join(OUT, "sweep_plans.npz"), **plans)
+
+    for name, (pcase, snr_min, seed, psrs) in SWEEP_RUN_CASES.items():
+        nsamps, tsamp, nbins, eta, lims, mem, mp, gpu = SWEEP_PLAN_CASES[pcase]
+        ts_e, ts_v = series(nsamps, seed)
+        t = np.arange(nsamps) * tsamp
+        for f0, amp, duty in psrs:
+            ts_e += (amp * (np.mod(t * f0, 1.0) < duty)).astype(np.float32)
+        rows, _ = ref.region_plan(ref.make_cfg(nsamps, tsamp, nbins, eta, lims), mem, 2.0, 1024, mp, gpu)
+        base = (nsamps, tsamp, nbins, eta, lims)
+        out = {}
+        for tag, chunk_w in (("base_widths", False), ("chunk_widths", True)):
+            params, snr, counts = osweep.run(base, rows[:, :4], ts_e, ts_v, snr_min, backend=_ref_backend,
+                                             chunk_widths=chunk_w)
+            out[f"params_{tag}"] = params
+            out[f"snr_{tag}"] = snr
+            out["region_counts"] = counts
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), ts_e=ts_e, ts_v=ts_v, nsamps=nsamps, tsamp=tsamp,
+                            nbins=nbins, eta=eta, param_limits=np.array(lims, np.float64), max_memory_gb=mem,
+                            max_passing=mp, snr_min=snr_min, chunks=rows, **out)
+        print(name, "chunks", rows.shape[0], "candidates", out["snr_base_widths"].size,
+              out["region_counts"].tolist())
+
+
 if __name__ == "__main__":
     if not ref.available():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` first")
     if len(sys.argv) > 1 and sys.argv[1] == "prune":
         prune_fixtures()
+    elif len(sys.argv) > 1 and sys.argv[1] == "sweep":
+        sweep_fixtures()
     else:
         main()
         prune_fixtures()
+        sweep_fixtures()
