@@ -419,6 +419,17 @@ int lk_prune_create_basis(const lk_plan* plan, uint64_t max_sugg, uint64_t batch
 int lk_plan_branching_pattern_basis(const lk_plan* plan, uint64_t ref_seg, int conservative,
                                     int poly_basis, double* out, uint64_t max_out,
                                     uint64_t* n_out);
+/* The end of a pruning run (PruneImpl::run, lib/prune.cpp:136-139,
+ * ascend_survivors_batched and report_survivors, lib/prune.cpp:228-334):
+ * every survivor's fold rebuilt over all segments searched so far and
+ * rescored (the run's scores kept as scores_ep), then its leaf reported at
+ * the middle of the data (observer-frame Taylor parameters; Chebyshev leaves
+ * converted first). Once per lk_prune_run; d_ffa_fold as given to the run. */
+int lk_prune_finalize(lk_prune* pr, const float* d_ffa_fold, lk_stream_t stream);
+/* scores_ep of the finalized tree, logical order (max_out >= tree size). */
+int lk_prune_get_scores_ep(const lk_prune* pr, float* d_scores_ep, uint64_t max_out,
+                           lk_stream_t stream);
+
 /* Surviving leaves after lk_prune_run, in the world tree's logical order.
  * Any of the device outputs may be NULL. */
 int lk_prune_tree_size(const lk_prune* pr, uint64_t* n);

@@ -189,6 +189,8 @@ SIGNATURES = [
     ("lk_prune_destroy", None, [vp]),
     ("lk_plan_branching_pattern", i32, [vp, u64, i32, vp, u64, vp]),
     ("lk_prune_run", i32, [vp, vp, u64, vp, u64, u64, vp, u64, vp, vp]),
+    ("lk_prune_finalize", i32, [vp, vp, vp]),
+    ("lk_prune_get_scores_ep", i32, [vp, vp, u64, vp]),
     ("lk_prune_tree_size", i32, [vp, vp]),
     ("lk_prune_get_tree", i32, [vp, vp, vp, vp, u64, vp]),
     ("lk_taylor_seed", i32, [vp, vp, vp]),

@@ -705,6 +705,23 @@ int lk_prune_run(lk_prune* pr, const float* d_ffa_fold, uint64_t ref_seg,
     });
 }
 
+int lk_prune_finalize(lk_prune* pr, const float* d_ffa_fold, lk_stream_t stream) {
+    return guarded([&] {
+        need(pr, "pr");
+        need(d_ffa_fold, "d_ffa_fold");
+        pr->exec->finalize(d_ffa_fold, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_prune_get_scores_ep(const lk_prune* pr, float* d_scores_ep, uint64_t max_out,
+                           lk_stream_t stream) {
+    return guarded([&] {
+        need(pr, "pr");
+        lk::require(pr->exec->tree_size() <= max_out, "max_out is smaller than the tree size");
+        pr->exec->copy_scores_ep(d_scores_ep, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 int lk_prune_tree_size(const lk_prune* pr, uint64_t* n) {
     return guarded([&] {
         need(pr, "pr");

@@ -54,6 +54,13 @@ public:
     std::vector<lk_prune_stats> run(const float* d_ffa_fold, uint64_t ref_seg,
                                     const float* thresholds, uint64_t n_thresholds,
                                     uint64_t n_iters, cudaStream_t s);
+    // The end of PruneImpl::run (lib/prune.cpp:136-139): the survivors
+    // ascended to the middle of the data (folds over every segment searched,
+    // scores of those folds; the run's scores kept as scores_ep) and their
+    // leaves reported there (observer-frame Taylor parameters). Once per run.
+    void finalize(const float* d_ffa_fold, cudaStream_t s);
+    void copy_scores_ep(float* d_scores_ep, cudaStream_t s) const;
+    bool finalized() const { return m_finalized; }
     uint64_t tree_size() const { return m_tree.size; }
     // Final tree in logical order into caller device buffers.
     void copy_tree(double* d_leaves, float* d_folds, float* d_scores, cudaStream_t s) const;
@@ -90,6 +97,11 @@ private:
     DeviceBuffer m_cleaves, m_cparent, m_cscores, m_cfolds, m_bcounts;
     uint64_t m_cap_parents = 0, m_cap_children = 0, m_cap_batches = 0;
     PinnedBuffer m_host;
+    // the last run, for finalize
+    std::vector<uint64_t> m_order;
+    uint64_t m_level = 0;
+    bool m_ran = false, m_finalized = false;
+    DeviceBuffer m_segs, m_tscores_ep;
 };
 
 // Single steps (the Taylor PruneDPFuncts interface, include/loki/core/

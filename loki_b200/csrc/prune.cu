@@ -590,6 +590,163 @@ __global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* _
     }
 }
 
+// ---- end of a run: ascend and report --------------------------------------
+
+// Ascend resolve of one leaf for one segment (poly_taylor_ascend_resolve_
+// {accel,jerk}_batch, lib/taylor.cpp:693-813; poly_chebyshev_ascend_resolve_
+// {accel,jerk}_batch, lib/chebyshev.cpp:1181-1312): the leaf carried from the
+// middle coordinate (t_mid, scale s_mid) to the segment centre, in the
+// reference's association.
+__device__ __forceinline__ void ascend_resolve_leaf(const double* lf, const LeafGeom& g,
+                                                    double dt, double inv_ts, uint32_t* pidx,
+                                                    float* phase) {
+    double a_new, v_new, d_new, f0;
+    if (g.basis == 0 && g.np == 2) {
+        const double half_dt2 = 0.5 * (dt * dt);
+        const double a_cur = lf[0], v_cur = lf[2], d_cur = lf[4];
+        f0 = lf[6];
+        a_new = a_cur;
+        v_new = v_cur + (a_cur * dt);
+        d_new = d_cur + (v_cur * dt) + (a_cur * half_dt2);
+    } else if (g.basis == 0) {
+        const double half_dt2 = 0.5 * (dt * dt);
+        const double sixth_dt3 = (half_dt2 * dt) / 3.0;
+        const double j_cur = lf[0], a_cur = lf[2], v_cur = lf[4], d_cur = lf[6];
+        f0 = lf[8];
+        a_new = a_cur + (j_cur * dt);
+        v_new = v_cur + (a_cur * dt) + (j_cur * half_dt2);
+        d_new = d_cur + (v_cur * dt) + (a_cur * half_dt2) + (j_cur * sixth_dt3);
+    } else if (g.np == 2) {
+        const double dt2 = dt * dt;
+        const double inv_ts2 = inv_ts * inv_ts;
+        const double alpha_2 = lf[0], alpha_1 = lf[2], alpha_0 = lf[4];
+        f0 = lf[6];
+        a_new = 4.0 * alpha_2 * inv_ts2;
+        v_new = (alpha_1 * inv_ts) + (4.0 * alpha_2 * inv_ts2 * dt);
+        d_new = (alpha_0 - alpha_2) + (alpha_1 * inv_ts * dt) + (2.0 * alpha_2 * inv_ts2 * dt2);
+    } else {
+        const double dt2 = dt * dt;
+        const double dt3 = dt2 * dt;
+        const double inv_ts2 = inv_ts * inv_ts;
+        const double inv_ts3 = inv_ts2 * inv_ts;
+        const double alpha_3 = lf[0], alpha_2 = lf[2], alpha_1 = lf[4], alpha_0 = lf[6];
+        f0 = lf[8];
+        a_new = (4.0 * alpha_2 * inv_ts2) + (24.0 * alpha_3 * dt * inv_ts3);
+        v_new = ((alpha_1 - (3.0 * alpha_3)) * inv_ts) + (4.0 * alpha_2 * inv_ts2 * dt) +
+                (12.0 * alpha_3 * inv_ts3 * dt2);
+        d_new = (alpha_0 - alpha_2) + ((alpha_1 - (3.0 * alpha_3)) * dt * inv_ts) +
+                (2.0 * alpha_2 * inv_ts2 * dt2) + (4.0 * alpha_3 * inv_ts3 * dt3);
+    }
+    const double f_new = f0 * (1.0 - (v_new * kInvCval));
+    const double delay_rel = d_new * kInvCval;
+    *phase = dev::phase_idx(dt, f0, g.nbins, delay_rel);
+    const uint32_t ia = dev::nearest_idx(a_new, g.a_min, g.a_max, g.n_accel);
+    const uint32_t jf = dev::nearest_idx(f_new, g.f_min, g.f_max, g.n_freq);
+    *pidx = ia * g.n_freq + jf;
+}
+
+// ascend (PrunePoly{Taylor,Chebyshev}DPFuncts::ascend, lib/dynamic.cpp:
+// 311-371,450-508): each survivor's fold rebuilt over the segments searched
+// so far -- zero, then every segment in middle-out order rotated right by
+// round(shift) and added (shift_add_ascend_linear_batch, lib/kernels.cpp:
+// 1390-1416) -- and rescored; the previous score moves to scores_ep. A warp
+// per survivor: lanes resolve 32 segments at a time in double precision and
+// the warp adds the segments' rows in order, each lane owning the bins
+// j = lane mod 32 of a shared-memory accumulator. Then a thread per survivor
+// scores its normalised row (the leaf step's scorer).
+template <int NW, int NB>
+__global__ void ascend_kernel(const double* __restrict__ leaves, uint64_t head, uint64_t cap,
+                              uint64_t n, const float* __restrict__ ffa, uint64_t ncoords,
+                              const uint32_t* __restrict__ seg_order, uint32_t nsegs, double tseg,
+                              double t_mid, double inv_ts_mid, LeafGeom g, uint32_t rs,
+                              ScoreParams sp, float* __restrict__ folds, float* __restrict__ scores,
+                              float* __restrict__ scores_ep) {
+    extern __shared__ float rows[];
+    const uint32_t T = blockDim.x;
+    const uint32_t nb = g.nbins;
+    const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
+    float* acc = rows + static_cast<size_t>(T) * rs + static_cast<size_t>(warp) * 2 * nb;
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * T;
+    const uint32_t nhere = static_cast<uint32_t>((n - c0) < T ? (n - c0) : T);
+    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+        const uint64_t phys = (head + c0 + p) % cap;
+        const double* lf = leaves + phys * g.ls;
+        // each lane touches only its own bins (E row j and V row nb + j)
+        for (uint32_t j = lane; j < nb; j += kWarp) {
+            acc[j] = 0.0f;
+            acc[nb + j] = 0.0f;
+        }
+        for (uint32_t base = 0; base < nsegs; base += kWarp) {
+            uint32_t my_pidx = 0, my_shift = 0;
+            if (base + lane < nsegs) {
+                const double t_seg = (static_cast<double>(seg_order[base + lane]) + 0.5) * tseg;
+                float ph;
+                ascend_resolve_leaf(lf, g, t_seg - t_mid, inv_ts_mid, &my_pidx, &ph);
+                my_shift = dev::shift_bins(ph, nb);
+            }
+            const uint32_t cnt = (nsegs - base) < kWarp ? (nsegs - base) : kWarp;
+            for (uint32_t q = 0; q < cnt; ++q) {
+                const uint32_t pidx = __shfl_sync(0xffffffffu, my_pidx, q);
+                const uint32_t sh = __shfl_sync(0xffffffffu, my_shift, q);
+                const float* src =
+                    ffa + (static_cast<uint64_t>(seg_order[base + q]) * ncoords + pidx) * 2 * nb;
+                for (uint32_t j = lane; j < nb; j += kWarp) {
+                    const uint32_t jh = j >= sh ? j - sh : j + nb - sh;
+                    acc[j] = __fadd_rn(acc[j], __ldg(src + jh));
+                    acc[nb + j] = __fadd_rn(acc[nb + j], __ldg(src + nb + jh));
+                }
+            }
+        }
+        float* o = folds + phys * 2 * nb;
+        float* dst = rows + static_cast<size_t>(p) * rs;
+        for (uint32_t j = lane; j < nb; j += kWarp) {
+            o[j] = acc[j];
+            o[nb + j] = acc[nb + j];
+            dst[j] = sc::normalise(acc[j], acc[nb + j]);
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    if (threadIdx.x < nhere) {
+        const uint64_t phys = (head + c0 + threadIdx.x) % cap;
+        float score;
+        sc::score_row_any<NB, NW>(rows + static_cast<size_t>(threadIdx.x) * rs, nb, 1.0f, sp,
+                                  LK_SCORE_MAX, &score);
+        scores_ep[phys] = scores[phys];
+        scores[phys] = score;
+    }
+}
+
+// report (PrunePoly{Taylor,Chebyshev}DPFuncts::report, lib/dynamic.cpp:
+// 373-379,510-519): Chebyshev leaves to Taylor at the middle coordinate, then
+// poly_taylor_report_batch (lib/taylor.cpp:1529-1564), the gauge transform to
+// the observer frame with first-order error propagation.
+__global__ void report_kernel(double* __restrict__ leaves, uint64_t head, uint64_t cap, uint64_t n,
+                              uint32_t np, uint32_t basis, double ts_mid) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    double* lf = leaves + ((head + i) % cap) * ((np + 2) * 2);
+    if (basis == 1) {
+        cheby_to_taylor_leaf(lf, np, ts_mid);
+    }
+    const double v_final = lf[(np - 1) * 2 + 0];
+    const double dv_final = lf[(np - 1) * 2 + 1];
+    const double f0_batch = lf[(np + 1) * 2 + 0];
+    const double s_factor = 1.0 - (v_final * kInvCval);
+    for (uint32_t j = 0; j + 1 < np; ++j) {
+        const double val = lf[j * 2 + 0];
+        const double err = lf[j * 2 + 1];
+        lf[j * 2 + 0] = val / s_factor;
+        lf[j * 2 + 1] = sqrt(((err / s_factor) * (err / s_factor)) +
+                             ((val * kInvCval / (s_factor * s_factor)) *
+                              (val * kInvCval / (s_factor * s_factor)) * (dv_final * dv_final)));
+    }
+    lf[(np - 1) * 2 + 0] = f0_batch * s_factor;
+    lf[(np - 1) * 2 + 1] = f0_batch * dv_final * kInvCval;
+}
+
 // ---- threshold-dependent steps --------------------------------------------
 
 // Children of batch b (child_starts[b0 + b] .. child_starts[b0 + b + 1]) with
@@ -1311,6 +1468,10 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
         s0.score_max = m_ncoords ? key_to_float(m_host.as<uint32_t>()[1]) : 0.0f;
         stats.push_back(s0);
     }
+    m_order = order;
+    m_level = 0;
+    m_ran = true;
+    m_finalized = false;
     const uint64_t levels = std::min<uint64_t>(m_nseg - 1, n_iters);
     for (uint64_t lv = 1; lv <= levels; ++lv) {
         require(lv <= n_thresholds, "Pruning complete - exceeded threshold scheme length");
@@ -1318,6 +1479,7 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
         lk_prune_stats st{};
         level(d_seg, order, lv, thresholds[lv - 1], &st, s);
         stats.push_back(st);
+        m_level = lv;
         if (m_tree.size == 0) {
             break;
         }
@@ -1539,6 +1701,71 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
     st->threshold = threshold;
     st->score_min = n_child ? key_to_float(kmin) : FLT_MAX;
     st->score_max = n_child ? key_to_float(kmax) : -FLT_MAX;
+}
+
+void PruneExec::finalize(const float* d_ffa_fold, cudaStream_t s) {
+    require(d_ffa_fold != nullptr, "ffa_fold is null");
+    require(m_ran, "finalize needs a pruning run first");
+    require(!m_finalized, "the run's survivors are already ascended and reported");
+    DeviceGuard g(m_device);
+    m_finalized = true;
+    const TreeState& t = m_tree;
+    if (t.size == 0) {
+        return;  // ascend_survivors_batched returns on an empty tree
+    }
+    const uint64_t nsegs = m_level + 1;
+    std::vector<uint32_t> segs(nsegs);
+    for (uint64_t k = 0; k < nsegs; ++k) {
+        segs[k] = static_cast<uint32_t>(m_order[k]);
+    }
+    if (m_segs.bytes < m_nseg * sizeof(uint32_t)) {
+        m_segs.alloc(m_nseg * sizeof(uint32_t));
+    }
+    if (m_tscores_ep.bytes < m_cap * sizeof(float)) {
+        m_tscores_ep.alloc(m_cap * sizeof(float));
+    }
+    // the copy reads pageable host memory: it completes before returning
+    LK_CUDA(cudaMemcpyAsync(m_segs.ptr, segs.data(), nsegs * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s));
+    const Coord mid = mo_coord(m_order, m_level, m_tseg);
+    const LeafGeom geom = make_geom(m_plan, m_branch_max, m_basis);
+    const uint32_t rs = sc::row_stride(m_nbins, m_sp.wmax);
+    // per thread: its scoring row and its share of the warp accumulators
+    const uint32_t T = sc::profiles_per_block(rs + (2 * m_nbins + kWarp - 1) / kWarp);
+    const size_t smem = (static_cast<size_t>(T) * rs + static_cast<size_t>(T / kWarp) * 2 * m_nbins) *
+                        sizeof(float);
+    auto launch = [&](auto kern) {
+        sc::set_smem(kern, smem);
+        kern<<<grid_for(t.size, T), T, smem, s>>>(
+            m_tleaves[m_cur].as<double>(), t.head, t.cap, t.size, d_ffa_fold, m_ncoords,
+            m_segs.as<uint32_t>(), static_cast<uint32_t>(nsegs), m_tseg, mid.ref, 1.0 / mid.scale,
+            geom, rs, m_sp, m_tfolds[m_cur].as<float>(), m_tscores[m_cur].as<float>(),
+            m_tscores_ep.as<float>());
+    };
+    sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
+        launch(ascend_kernel<decltype(nw)::value, decltype(nbc)::value>);
+    });
+    report_kernel<<<grid_for(t.size, 256), 256, 0, s>>>(m_tleaves[m_cur].as<double>(), t.head,
+                                                        t.cap, t.size, m_np,
+                                                        static_cast<uint32_t>(m_basis), mid.scale);
+    LK_CUDA(cudaGetLastError());
+}
+
+void PruneExec::copy_scores_ep(float* d_scores_ep, cudaStream_t s) const {
+    require(m_finalized, "scores_ep exist after finalize");
+    DeviceGuard g(m_device);
+    const TreeState& t = m_tree;
+    if (d_scores_ep == nullptr || t.size == 0) {
+        return;
+    }
+    const uint64_t first = std::min(t.size, t.cap - t.head);
+    const uint64_t second = t.size - first;
+    LK_CUDA(cudaMemcpyAsync(d_scores_ep, m_tscores_ep.as<float>() + t.head, first * sizeof(float),
+                            cudaMemcpyDeviceToDevice, s));
+    if (second > 0) {
+        LK_CUDA(cudaMemcpyAsync(d_scores_ep + first, m_tscores_ep.ptr, second * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+    }
 }
 
 void PruneExec::copy_tree(double* d_leaves, float* d_folds, float* d_scores,

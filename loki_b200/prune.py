@@ -56,6 +56,12 @@ def branching_pattern(cfg: PulsarSearchConfig, ref_seg: int = 0, use_conservativ
     return out[: n.value].copy()
 
 
+def middle_out_order(nsegments: int, ref_seg: int) -> list[int]:
+    """MiddleOutScheme's segment order (lib/loki/psr_utils.hpp:331-347):
+    stable argsort of |i - ref_seg|."""
+    return sorted(range(nsegments), key=lambda i: (abs(i - ref_seg), i))
+
+
 def determine_ref_segs(nsegments: int, n_runs: int | None = None, ref_segs=None) -> list[int]:
     """utils::determine_ref_segs_pareto (lib/utils.cpp:243-278)."""
     if n_runs is not None:
@@ -131,6 +137,26 @@ class PruneCUDA:
                 out[name][i] = getattr(stats[i], name)
         return out
 
+    def finalize(self, ffa_fold) -> None:
+        """Ascend the run's survivors to the middle of the data and report them
+        there (the end of the reference's PruneImpl::run): folds over every
+        segment searched, their scores, the run's scores kept as scores_ep,
+        leaves as observer-frame Taylor parameters."""
+        fold = D.to_device_f32(ffa_fold, self._device).reshape(-1)
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_prune_finalize(self._h, D.ptr(fold), D.stream_ptr(self._device)))
+
+    def scores_ep(self, host: bool = True):
+        """scores_ep of the finalized tree, logical order."""
+        t = D.torch()
+        n = self.tree_size
+        out = t.empty(max(n, 1), dtype=t.float32, device=f"cuda:{self._device}")
+        with t.cuda.device(self._device):
+            C.check(C.lib().lk_prune_get_scores_ep(self._h, out.data_ptr(), max(n, 1),
+                                                   D.stream_ptr(self._device)))
+        out = out[:n]
+        return out.cpu().numpy() if host else out
+
     @property
     def tree_size(self) -> int:
         n = ctypes.c_uint64()
@@ -177,15 +203,23 @@ class EPMultiPassCUDA:
         return self._ffa
 
     def execute(self, ts_e, ts_v, outdir: str | None = None, file_prefix: str = "test") -> dict:
-        """Returns {ref_seg: {"stats", "leaves", "folds", "scores"}}; with ``outdir``
-        also writes ``<prefix>_pruning_nstages_<n>_results.npz`` and a text log."""
+        """Runs every reference segment as the reference's PruneImpl::run does
+        (levels, then survivors ascended and reported at the middle of the
+        data). Returns {ref_seg: {"stats", "leaves", "folds", "scores",
+        "scores_ep", "snail_scheme"}}; with ``outdir`` also writes
+        ``<prefix>_pruning_nstages_<n>_results.npz`` (per run ``<ref_seg>_00``:
+        param_sets, scores, scores_ep, snail_scheme, level_stats -- the
+        reference's HDF5 run group) and a text log."""
         fold = self._ffa.execute(D.to_device_f32(ts_e, self._device), D.to_device_f32(ts_v, self._device))
         nseg = int(self._ffa.plan.nsegments[-1])
         results = {}
         for ref_seg in determine_ref_segs(nseg, self._n_runs, self._ref_segs):
             stats = self._prune.run(fold, ref_seg, self._thr, n_iters=nseg - 1)
+            self._prune.finalize(fold)
             leaves, folds, scores = self._prune.tree()
-            results[ref_seg] = {"stats": stats, "leaves": leaves, "folds": folds, "scores": scores}
+            results[ref_seg] = {"stats": stats, "leaves": leaves, "folds": folds, "scores": scores,
+                                "scores_ep": self._prune.scores_ep(),
+                                "snail_scheme": np.array(middle_out_order(nseg, ref_seg), np.uint64)}
         if outdir is not None:
             os.makedirs(outdir, exist_ok=True)
             base = os.path.join(outdir, f"{file_prefix}_pruning_nstages_{nseg}")
@@ -199,7 +233,11 @@ class EPMultiPassCUDA:
                                   f"branches {int(row['n_branches'])} leaves {int(row['n_leaves'])} "
                                   f"survivors {int(row['n_leaves_surv'])} "
                                   f"score [{row['score_min']:.3f}, {row['score_max']:.3f}]\n")
-                    for k in ("stats", "leaves", "scores"):
-                        arrays[f"{rs:03d}_{k}"] = r[k]
+                    run = f"{rs:03d}_00"
+                    arrays[f"{run}/param_sets"] = r["leaves"]
+                    arrays[f"{run}/scores"] = r["scores"]
+                    arrays[f"{run}/scores_ep"] = r["scores_ep"]
+                    arrays[f"{run}/snail_scheme"] = r["snail_scheme"]
+                    arrays[f"{run}/level_stats"] = r["stats"]
             np.savez(base + "_results.npz", **arrays)
         return results

@@ -120,6 +120,7 @@ def lib() -> ctypes.CDLL:
                                    u64, vp, vp, vp, vp, vp]
         L.lko_prune_run.argtypes = [vp, ctypes.c_int, vp, vp, u64, u64, u64, u64, u64, u64, vp, vp,
                                     vp, vp, vp, u64, vp]
+        L.lko_prune_finalize.argtypes = [vp, ctypes.c_int, vp, u64, u64, vp, vp, vp, vp, u64]
         L.lko_prune_run_basis.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, u64, u64, u64, u64, u64,
                                           u64, vp, vp, vp, vp, vp, u64, vp]
         L.lko_taylor_to_cheby.argtypes = [vp, u64, u32, f64]
@@ -515,6 +516,19 @@ def prune_run(plan: OraclePlan, ffa_fold, thresholds, ref_seg, max_sugg, batch_s
     k = n.value
     return (stats[: nstats.value], leaves[: k * stride].reshape(k, plan.nparams + 2, 2),
             folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k])
+
+
+def prune_finalize(plan: OraclePlan, ffa_fold, ref_seg, prune_level, leaves, folds, scores, basis="taylor"):
+    """Ascend + report of a run's survivors (copies): returns (leaves, folds,
+    scores, scores_ep)."""
+    ffa = np.ascontiguousarray(ffa_fold, np.float32).ravel()
+    lv = np.ascontiguousarray(leaves, np.float64).copy()
+    fo = np.ascontiguousarray(folds, np.float32).copy()
+    sc = np.ascontiguousarray(scores, np.float32).copy()
+    ep = np.zeros_like(sc)
+    _check(lib().lko_prune_finalize(ctypes.byref(plan.raw), 1 if basis == "chebyshev" else 0, _p(ffa), ref_seg,
+                                    prune_level, _p(lv), _p(fo), _p(sc), _p(ep), sc.size))
+    return lv, fo, sc, ep
 
 
 # ---- Monte-Carlo threshold stage -------------------------------------------------

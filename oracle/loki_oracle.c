@@ -1507,6 +1507,148 @@ static float wt_add_batch(wtree* t, const double* lv, const float* fo, const flo
 /* PruneImpl::initialize + execute_iteration_batched (lib/prune.cpp:181-226,
  * 429-620) for the Taylor basis, where validate is the identity
  * (lib/dynamic.cpp:70-77). */
+/* Ascend resolve for one segment (poly_taylor_ascend_resolve_{accel,jerk}_batch,
+ * lib/taylor.cpp:693-813; poly_chebyshev_ascend_resolve_{accel,jerk}_batch,
+ * lib/chebyshev.cpp:1181-1312): the leaf's parameters carried from coord_cur
+ * to the segment's centre t0_seg, nearest final-level grid cell and phase
+ * shift. */
+static void ascend_resolve_one(const lko_plan* p, int basis, const double* lf, double t0_seg,
+                               double t0_cur, double scale_cur, uint64_t* pidx, float* shift) {
+    const uint32_t np = p->nparams;
+    const uint32_t L = p->n_levels - 1;
+    const uint64_t n_accel = p->param_counts[L][np - 2];
+    const uint64_t n_freq = p->param_counts[L][np - 1];
+    const double a_min = p->limits[2 * (np - 2)], a_max = p->limits[2 * (np - 2) + 1];
+    const double f_min = p->limits[2 * (np - 1)], f_max = p->limits[2 * (np - 1) + 1];
+    const double dt = t0_seg - t0_cur;
+    double a_new, v_new, d_new, f0;
+    if (basis == 0 && np == 2) {
+        const double half_dt2 = 0.5 * (dt * dt);
+        const double a_cur = lf[0], v_cur = lf[2], d_cur = lf[4];
+        f0 = lf[6];
+        a_new = a_cur;
+        v_new = v_cur + (a_cur * dt);
+        d_new = d_cur + (v_cur * dt) + (a_cur * half_dt2);
+    } else if (basis == 0) {
+        const double half_dt2 = 0.5 * (dt * dt);
+        const double sixth_dt3 = (half_dt2 * dt) / 3.0;
+        const double j_cur = lf[0], a_cur = lf[2], v_cur = lf[4], d_cur = lf[6];
+        f0 = lf[8];
+        a_new = a_cur + (j_cur * dt);
+        v_new = v_cur + (a_cur * dt) + (j_cur * half_dt2);
+        d_new = d_cur + (v_cur * dt) + (a_cur * half_dt2) + (j_cur * sixth_dt3);
+    } else if (np == 2) {
+        const double dt2 = dt * dt;
+        const double inv_ts = 1.0 / scale_cur;
+        const double inv_ts2 = inv_ts * inv_ts;
+        const double alpha_2 = lf[0], alpha_1 = lf[2], alpha_0 = lf[4];
+        f0 = lf[6];
+        a_new = 4.0 * alpha_2 * inv_ts2;
+        v_new = (alpha_1 * inv_ts) + (4.0 * alpha_2 * inv_ts2 * dt);
+        d_new = (alpha_0 - alpha_2) + (alpha_1 * inv_ts * dt) + (2.0 * alpha_2 * inv_ts2 * dt2);
+    } else {
+        const double dt2 = dt * dt;
+        const double dt3 = dt2 * dt;
+        const double inv_ts = 1.0 / scale_cur;
+        const double inv_ts2 = inv_ts * inv_ts;
+        const double inv_ts3 = inv_ts2 * inv_ts;
+        const double alpha_3 = lf[0], alpha_2 = lf[2], alpha_1 = lf[4], alpha_0 = lf[6];
+        f0 = lf[8];
+        a_new = (4.0 * alpha_2 * inv_ts2) + (24.0 * alpha_3 * dt * inv_ts3);
+        v_new = ((alpha_1 - (3.0 * alpha_3)) * inv_ts) + (4.0 * alpha_2 * inv_ts2 * dt) +
+                (12.0 * alpha_3 * inv_ts3 * dt2);
+        d_new = (alpha_0 - alpha_2) + ((alpha_1 - (3.0 * alpha_3)) * dt * inv_ts) +
+                (2.0 * alpha_2 * inv_ts2 * dt2) + (4.0 * alpha_3 * inv_ts3 * dt3);
+    }
+    const double f_new = f0 * (1.0 - (v_new * kInvCval));
+    const double delay_rel = d_new * kInvCval;
+    *shift = lko_phase_idx(dt, f0, p->nbins, delay_rel);
+    const uint64_t ia = lko_nearest_idx(a_new, a_min, a_max, n_accel);
+    const uint64_t jf = lko_nearest_idx(f_new, f_min, f_max, n_freq);
+    *pidx = (ia * n_freq) + jf;
+}
+
+/* poly_taylor_report_batch (lib/taylor.cpp:1529-1564): gauge transform of
+ * the leaf to the observer frame with first-order error propagation. */
+static void taylor_report_one(double* lf, uint32_t np) {
+    const double v_final = lf[(np - 1) * 2 + 0];
+    const double dv_final = lf[(np - 1) * 2 + 1];
+    const double f0_batch = lf[(np + 1) * 2 + 0];
+    const double s_factor = 1.0 - (v_final * kInvCval);
+    for (uint32_t j = 0; j + 1 < np; ++j) {
+        const double val = lf[j * 2 + 0];
+        const double err = lf[j * 2 + 1];
+        lf[j * 2 + 0] = val / s_factor;
+        lf[j * 2 + 1] = sqrt(((err / s_factor) * (err / s_factor)) +
+                             ((val * kInvCval / (s_factor * s_factor)) *
+                              (val * kInvCval / (s_factor * s_factor)) * (dv_final * dv_final)));
+    }
+    lf[(np - 1) * 2 + 0] = f0_batch * s_factor;
+    lf[(np - 1) * 2 + 1] = f0_batch * dv_final * kInvCval;
+}
+
+int lko_prune_finalize(const lko_plan* p, int basis, const float* ffa_fold, uint64_t ref_seg,
+                       uint64_t prune_level, double* leaves, float* folds, float* scores,
+                       float* scores_ep, uint64_t n) {
+    const uint32_t np = p->nparams;
+    if (np < 2 || np > 3) {
+        return fail("pruning supports nparams 2 or 3");
+    }
+    const uint32_t L = p->n_levels - 1;
+    const uint64_t nseg = p->nsegments[L];
+    const double tseg = p->tsegments[L];
+    const uint64_t nbins = p->nbins;
+    const uint64_t ncoords = p->ncoords[L];
+    const uint64_t ls = (np + 2) * 2, fs = 2 * nbins;
+    if (ref_seg >= nseg || prune_level >= nseg) {
+        return fail("MiddleOutScheme: invalid ref_idx / level");
+    }
+    uint64_t* order = (uint64_t*)malloc(sizeof(uint64_t) * nseg);
+    middle_out_order(nseg, ref_seg, order);
+    double t0_mid, s_mid;
+    mo_coord(order, prune_level, tseg, &t0_mid, &s_mid);
+    for (uint64_t i = 0; i < n; ++i) {
+        double* lf = leaves + i * ls;
+        float* out = folds + i * fs;
+        /* shift_add_ascend_linear_batch (lib/kernels.cpp:1390-1416): zero,
+         * then every segment so far, in middle-out order, rotated right by
+         * round(shift) and added (shift_add_linear_with_buffer_inplace,
+         * lib/kernels.cpp:149-176). */
+        for (uint64_t j = 0; j < fs; ++j) {
+            out[j] = 0.0F;
+        }
+        for (uint64_t k = 0; k <= prune_level; ++k) {
+            double t_seg, s_seg;
+            mo_segment_coord(order, k, tseg, &t_seg, &s_seg);
+            uint64_t pidx;
+            float ph;
+            ascend_resolve_one(p, basis, lf, t_seg, t0_mid, s_mid, &pidx, &ph);
+            uint64_t sh = (uint64_t)(ph + 0.5F);
+            if (sh == nbins) {
+                sh = 0;
+            }
+            const float* src = ffa_fold + (order[k] * ncoords + pidx) * fs;
+            for (uint64_t j = 0; j < nbins; ++j) {
+                const uint64_t jj = (j + nbins - sh) % nbins;
+                out[j] += src[jj];
+                out[nbins + j] += src[nbins + jj];
+            }
+        }
+        scores_ep[i] = scores[i];
+    }
+    lko_snr_boxcar_3d_max(folds, n, nbins, p->widths, p->n_widths, scores);
+    /* report: Chebyshev leaves to Taylor at coord_mid first
+     * (PrunePolyChebyshevDPFuncts::report, lib/dynamic.cpp:510-519). */
+    if (basis == 1) {
+        lko_cheby_to_taylor(leaves, n, np, s_mid);
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        taylor_report_one(leaves + i * ls, np);
+    }
+    free(order);
+    return 0;
+}
+
 int lko_prune_run(const lko_plan* p, int conservative, const float* ffa_fold,
                   const float* thresholds, uint64_t n_thresholds, uint64_t ref_seg,
                   uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,

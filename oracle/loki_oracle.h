@@ -220,6 +220,14 @@ int lko_prune_run_basis(const lko_plan* plan, int basis, int conservative, const
                         uint64_t n_iters, lko_prune_stats* stats, uint64_t* n_stats,
                         double* leaves_out, float* folds_out, float* scores_out, uint64_t cap_out,
                         uint64_t* n_out);
+/* The end of a pruning run (PruneImpl::run, lib/prune.cpp:136-139): the n
+ * surviving leaves (logical order, after prune_level levels from ref_seg)
+ * ascended to the middle of the data -- folds rebuilt over every segment so
+ * far, scores_ep = the scores before, scores = the new folds' scores -- and
+ * the leaves reported there. */
+int lko_prune_finalize(const lko_plan* plan, int basis, const float* ffa_fold, uint64_t ref_seg,
+                       uint64_t prune_level, double* leaves, float* folds, float* scores,
+                       float* scores_ep, uint64_t n);
 int lko_prune_run(const lko_plan* plan, int conservative, const float* ffa_fold,
                   const float* thresholds, uint64_t n_thresholds, uint64_t ref_seg,
                   uint64_t max_sugg, uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,

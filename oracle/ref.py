@@ -107,6 +107,8 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
                                       vp, vp, vp, vp, vp, u64, vp]
         L.lkref_prune_run_basis.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64, u64,
                                       vp, vp, vp, vp, vp, u64, vp]
+        L.lkref_prune_run_full.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64,
+                                           u64, vp, vp, vp, vp, vp, vp, u64, vp]
         L.lkref_region_plan.argtypes = [vp, f64, f64, u64, u64, ctypes.c_int, vp, u64, vp, vp]
         _libs[path] = L
     return _libs[path]
@@ -467,3 +469,27 @@ def region_plan(cfg: RefCfg, max_memory_gb=8.0, octave_scale=2.0, nbins_max=1024
                                   int(use_gpu), _p(rows), cap, ctypes.byref(n), _p(stats)))
     k = min(n.value, cap)
     return rows[: k * 6].reshape(k, 6), stats
+
+
+def prune_run_full(cfg: RefCfg, ffa_fold, thresholds, ref_seg, max_sugg, batch_size, branch_max_, n_iters,
+                   nbins, conservative=False, basis="taylor"):
+    """A whole reference pruning run with the survivors ascended and reported:
+    (stats, leaves, folds, scores, scores_ep)."""
+    L = lib()
+    ffa = np.ascontiguousarray(ffa_fold, np.float32).ravel()
+    thr = np.ascontiguousarray(thresholds, np.float32)
+    stats = np.zeros(n_iters + 1, PRUNE_STATS_DTYPE)
+    nstats = u64()
+    stride = (cfg.nparams + 2) * 2
+    leaves = np.zeros(max_sugg * stride, np.float64)
+    folds = np.zeros(max_sugg * 2 * nbins, np.float32)
+    scores = np.zeros(max_sugg, np.float32)
+    scores_ep = np.zeros(max_sugg, np.float32)
+    n = u64()
+    _check(L, L.lkref_prune_run_full(1 if basis == "chebyshev" else 0, ctypes.byref(cfg), int(conservative),
+                                     _p(ffa), ffa.size, _p(thr), thr.size, ref_seg, max_sugg, batch_size,
+                                     branch_max_, n_iters, _p(stats), ctypes.byref(nstats), _p(leaves),
+                                     _p(folds), _p(scores), _p(scores_ep), max_sugg, ctypes.byref(n)))
+    k = n.value
+    return (stats[: nstats.value], leaves[: k * stride].reshape(k, cfg.nparams + 2, 2),
+            folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k], scores_ep[:k])

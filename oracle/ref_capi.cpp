@@ -582,7 +582,7 @@ static int prune_run_basis(const char* basis, const lkref_cfg* c, int conservati
                            uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
                            lkref_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
                            float* folds_out, float* scores_out, uint64_t cap_out,
-                           uint64_t* n_out);
+                           uint64_t* n_out, int finalize = 0, float* scores_ep_out = nullptr);
 
 int lkref_prune_run(const lkref_cfg* c, int conservative, const float* ffa_fold,
                     uint64_t ffa_fold_len, const float* thresholds, uint64_t n_thresholds,
@@ -656,13 +656,30 @@ int lkref_prune_run_basis(int basis, const lkref_cfg* c, int conservative,
                            scores_out, cap_out, n_out);
 }
 
+// A whole EPMultiPass run for one ref_seg as PruneImpl::run does it: the
+// levels, then the survivors ascended to the middle of the data (folds and
+// scores over every segment so far; scores_ep = the scores before) and
+// reported there (prune.cpp:136-139,228-334).
+int lkref_prune_run_full(int basis, const lkref_cfg* c, int conservative, const float* ffa_fold,
+                         uint64_t ffa_fold_len, const float* thresholds, uint64_t n_thresholds,
+                         uint64_t ref_seg, uint64_t max_sugg, uint64_t batch_size,
+                         uint64_t branch_max, uint64_t n_iters, lkref_prune_stats* stats,
+                         uint64_t* n_stats, double* leaves_out, float* folds_out,
+                         float* scores_out, float* scores_ep_out, uint64_t cap_out,
+                         uint64_t* n_out) {
+    return prune_run_basis(basis == 1 ? "chebyshev" : "taylor", c, conservative, ffa_fold,
+                           ffa_fold_len, thresholds, n_thresholds, ref_seg, max_sugg, batch_size,
+                           branch_max, n_iters, stats, n_stats, leaves_out, folds_out,
+                           scores_out, cap_out, n_out, 1, scores_ep_out);
+}
+
 static int prune_run_basis(const char* basis, const lkref_cfg* c, int conservative,
                            const float* ffa_fold, uint64_t ffa_fold_len, const float* thresholds,
                            uint64_t n_thresholds, uint64_t ref_seg, uint64_t max_sugg,
                            uint64_t batch_size, uint64_t branch_max, uint64_t n_iters,
                            lkref_prune_stats* stats, uint64_t* n_stats, double* leaves_out,
                            float* folds_out, float* scores_out, uint64_t cap_out,
-                           uint64_t* n_out) {
+                           uint64_t* n_out, int finalize, float* scores_ep_out) {
     return guarded([&] {
         using loki::SizeType;
         const auto cfg = make_cfg_prune(c, conservative);
@@ -782,6 +799,44 @@ static int prune_run_basis(const char* basis, const lkref_cfg* c, int conservati
         }
         *n_stats = ns;
 
+        // ascend_survivors_batched + report_survivors (prune.cpp:136-139,
+        // 228-334): survivors of a run that kept any are ascended to the
+        // middle of the data and reported there.
+        if (finalize != 0 && world_tree.get_size() > 0) {
+            const SizeType prune_level = ns - 1;
+            const auto coord_mid = snail.get_coord(prune_level);
+            const auto [idx_segments, coord_segments] =
+                snail.get_segment_coords_so_far(prune_level);
+            const SizeType n_surv  = world_tree.get_size();
+            const SizeType cap_b   = std::max(SizeType{1}, std::min(batch_size, n_surv));
+            const SizeType lstride = world_tree.get_leaves_stride();
+            const SizeType fstride = world_tree.get_folds_stride();
+            auto lv = world_tree.get_leaves_circular_view();
+            auto fv = world_tree.get_folds_circular_view();
+            auto sv = world_tree.get_scores_circular_view();
+            auto ev = world_tree.get_scores_ep_circular_view();
+            auto region = [&](std::span<double> l, std::span<float> f, std::span<float> sc,
+                              std::span<float> ep) {
+                const SizeType nreg = l.size() / lstride;
+                for (SizeType off = 0; off < nreg; off += cap_b) {
+                    const SizeType chunk = std::min(cap_b, nreg - off);
+                    funcs->ascend(ffa, l.subspan(off * lstride, chunk * lstride),
+                                  f.subspan(off * fstride, chunk * fstride),
+                                  sc.subspan(off, chunk), ep.subspan(off, chunk), idx_segments,
+                                  coord_segments, coord_mid, prune_ws.branched_param_idx,
+                                  prune_ws.branched_phase_shift, chunk);
+                }
+            };
+            region(lv.first, fv.first, sv.first, ev.first);
+            region(lv.second, fv.second, sv.second, ev.second);
+            const SizeType n1 = lv.first.size() / lstride;
+            const SizeType n2 = lv.second.size() / lstride;
+            funcs->report(lv.first, coord_mid, n1);
+            if (n2 > 0) {
+                funcs->report(lv.second, coord_mid, n2);
+            }
+        }
+
         // final tree in logical order
         const SizeType n = world_tree.get_size();
         *n_out = n;
@@ -799,6 +854,11 @@ static int prune_run_basis(const char* basis, const lkref_cfg* c, int conservati
         std::copy(fv.second.begin(), fv.second.end(), folds_out + fv.first.size());
         std::copy(sv.first.begin(), sv.first.end(), scores_out);
         std::copy(sv.second.begin(), sv.second.end(), scores_out + sv.first.size());
+        if (scores_ep_out != nullptr) {
+            const auto ev = world_tree.get_scores_ep_circular_view();
+            std::copy(ev.first.begin(), ev.first.end(), scores_ep_out);
+            std::copy(ev.second.begin(), ev.second.end(), scores_ep_out + ev.first.size());
+        }
         (void)ls;
         (void)fs;
     });

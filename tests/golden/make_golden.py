@@ -146,6 +146,15 @@ def prune_fixtures() -> None:
         ref_seg = nseg // 2
         stats, leaves, folds, scores = ref.prune_run(cfg, fold, thr, ref_seg, ms, bs, bmax, nseg - 1, nb, cons,
                                                      basis=basis)
+        # whole runs as PruneImpl::run ends them: survivors ascended to the
+        # middle of the data and reported there, after every level and after
+        # half of them
+        fin = ref.prune_run_full(cfg, fold, thr, ref_seg, ms, bs, bmax, nseg - 1, nb, cons, basis=basis)
+        half = ref.prune_run_full(cfg, fold, thr, ref_seg, ms, bs, bmax, (nseg - 1) // 2, nb, cons, basis=basis)
+        finals = {}
+        for tag, (st, lv, fo, sc, ep) in (("final", fin), ("half", half)):
+            finals.update({f"{tag}_levels": st.size - 1, f"{tag}_leaves": lv, f"{tag}_folds": fo,
+                           f"{tag}_scores": sc, f"{tag}_scores_ep": ep})
         np.savez_compressed(
             os.path.join(OUT, f"{name}.npz"),
             nsamps=ns, tsamp=ts, nbins=nb, eta=eta, param_limits=np.array(lims, dtype=np.float64),
@@ -157,6 +166,7 @@ def prune_fixtures() -> None:
             leaves=leaves, folds=folds, scores=scores, basis=basis,
             branching_pattern=bp0,
             branching_pattern_ref=ref.branching_pattern_basis(cfg, basis, ref_seg, cons),
+            **finals,
         )
         print(name, "nsegments", nseg, "survivors", leaves.shape[0])
 

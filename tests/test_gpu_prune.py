@@ -118,8 +118,63 @@ def test_ep_multipass_end_to_end(cuda):
     for rs, r in res.items():
         want = lko.prune_run(plan, fold, thr, rs, ms, bs, bm, nseg - 1)
         np.testing.assert_array_equal(_stats_matrix(r["stats"]), _stats_matrix(want[0]))
-        np.testing.assert_array_equal(r["leaves"], want[1])
-        np.testing.assert_array_equal(r["scores"], want[3])
+        # survivors ascended and reported as PruneImpl::run ends
+        lv, fo, sc, ep = lko.prune_finalize(plan, fold, rs, want[0].size - 1, *want[1:])
+        np.testing.assert_array_equal(r["leaves"], lv)
+        np.testing.assert_array_equal(r["folds"], fo)
+        np.testing.assert_array_equal(r["scores"], sc)
+        np.testing.assert_array_equal(r["scores_ep"], ep)
+        assert r["snail_scheme"][0] == rs
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_prune_finalize_bit_exact(cuda, name):
+    """Ascend + report (the end of PruneImpl::run) after full and partial runs."""
+    from loki_b200.prune import PruneCUDA
+
+    plan, cfg, _, fold, nseg, ref_seg, thr, ms, bs, cons = _setup(name)
+    bm = _branch_max(cfg, cons)
+    pr = PruneCUDA(cfg, max_sugg=ms, batch_size=bs, branch_max=None, use_conservative_tile=cons)
+    for n_iters in (nseg - 1, max(1, (nseg - 1) // 3)):
+        want = lko.prune_run(plan, fold, thr, ref_seg, ms, bs, bm, n_iters, conservative=cons)
+        lv, fo, sc, ep = lko.prune_finalize(plan, fold, ref_seg, want[0].size - 1, *want[1:])
+        pr.run(fold, ref_seg, thr, n_iters=n_iters)
+        pr.finalize(fold)
+        leaves, folds, scores = pr.tree()
+        np.testing.assert_array_equal(leaves.view(np.uint64), lv.view(np.uint64))
+        np.testing.assert_array_equal(folds.view(np.uint32), fo.view(np.uint32))
+        np.testing.assert_array_equal(scores.view(np.uint32), sc.view(np.uint32))
+        np.testing.assert_array_equal(pr.scores_ep().view(np.uint32), ep.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["prune_accel_nb16.npz", "prune_jerk_nb16.npz", "prune_cheby_accel_nb16.npz",
+                                  "prune_cheby_jerk_nb16.npz"])
+@pytest.mark.parametrize("tag", ["final", "half"])
+def test_prune_finalize_reference_golden_fixtures(cuda, name, tag):
+    from loki_b200 import _capi as C
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.prune import PruneCUDA
+
+    g = golden(name)
+    cfg = PulsarSearchConfig(int(g["nsamps"]), float(g["tsamp"]), int(g["nbins"]), float(g["eta"]),
+                             g["param_limits"], use_fourier=False, bseg_ffa=int(g["bseg_ffa"]))
+    pr = PruneCUDA(cfg, max_sugg=int(g["max_sugg"]), batch_size=int(g["batch_size"]),
+                   branch_max=int(g["branch_max"]), use_conservative_tile=bool(g["conservative"]),
+                   poly_basis=str(g["basis"]))
+    nseg = g["thresholds"].size + 1
+    n_iters = nseg - 1 if tag == "final" else (nseg - 1) // 2
+    with pytest.raises(C.LokiError):
+        pr.finalize(g["ffa_fold"])  # no run yet
+    stats = pr.run(g["ffa_fold"], int(g["ref_seg"]), g["thresholds"], n_iters=n_iters)
+    assert stats.size - 1 == int(g[f"{tag}_levels"])
+    pr.finalize(g["ffa_fold"])
+    with pytest.raises(C.LokiError):
+        pr.finalize(g["ffa_fold"])  # once per run
+    leaves, folds, scores = pr.tree()
+    np.testing.assert_array_equal(leaves.view(np.uint64), g[f"{tag}_leaves"].view(np.uint64))
+    np.testing.assert_array_equal(folds.view(np.uint32), g[f"{tag}_folds"].view(np.uint32))
+    np.testing.assert_array_equal(scores.view(np.uint32), g[f"{tag}_scores"].view(np.uint32))
+    np.testing.assert_array_equal(pr.scores_ep().view(np.uint32), g[f"{tag}_scores_ep"].view(np.uint32))
 
 
 # ---- single steps ---------------------------------------------------------------

@@ -79,6 +79,27 @@ def test_cheby_prune_run_bit_exact(cuda, name):
     np.testing.assert_array_equal(scores, want[3])
 
 
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_cheby_finalize_bit_exact(cuda, name):
+    """Ascend + report in the Chebyshev basis (leaves converted to Taylor at
+    the middle coordinate before the report)."""
+    from loki_b200.prune import PruneCUDA
+
+    plan, cfg, fold, nseg, ref_seg, thr, ms, bs = _setup(name)
+    bm = _branch_max(cfg)
+    pr = PruneCUDA(cfg, max_sugg=ms, batch_size=bs, poly_basis="chebyshev")
+    for n_iters in (nseg - 1, max(1, (nseg - 1) // 2)):
+        want = lko.prune_run(plan, fold, thr, ref_seg, ms, bs, bm, n_iters, basis="chebyshev")
+        lv, fo, sc, ep = lko.prune_finalize(plan, fold, ref_seg, want[0].size - 1, *want[1:], basis="chebyshev")
+        pr.run(fold, ref_seg, thr, n_iters=n_iters)
+        pr.finalize(fold)
+        leaves, folds, scores = pr.tree()
+        np.testing.assert_array_equal(leaves.view(np.uint64), lv.view(np.uint64))
+        np.testing.assert_array_equal(folds.view(np.uint32), fo.view(np.uint32))
+        np.testing.assert_array_equal(scores.view(np.uint32), sc.view(np.uint32))
+        np.testing.assert_array_equal(pr.scores_ep().view(np.uint32), ep.view(np.uint32))
+
+
 @pytest.mark.parametrize("name", ["prune_cheby_accel_nb16.npz", "prune_cheby_jerk_nb16.npz"])
 def test_cheby_prune_reference_golden_fixtures(cuda, name):
     from loki_b200.configs import PulsarSearchConfig

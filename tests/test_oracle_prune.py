@@ -115,3 +115,53 @@ def test_oracle_prune_matches_reference_directly(case):
     b = lko.prune_run(plan, fold, thr, ref_seg, ms, bs, bm, nseg - 1, cons)
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
+
+
+FINAL_FIXTURES = PRUNE_FIXTURES + ["prune_cheby_accel_nb16.npz", "prune_cheby_jerk_nb16.npz"]
+
+
+@pytest.mark.parametrize("name", FINAL_FIXTURES)
+@pytest.mark.parametrize("tag", ["final", "half"])
+def test_oracle_ascend_report_matches_reference_fixture(name, tag):
+    """The end of a run (PruneImpl::run, lib/prune.cpp:136-139): survivors
+    ascended to the middle of the data (folds over every segment so far,
+    scores_ep = the scores before) and reported there."""
+    g = golden(name)
+    plan = _plan(g)
+    basis = str(g["basis"])
+    nseg = int(plan.nsegments[-1])
+    n_iters = nseg - 1 if tag == "final" else (nseg - 1) // 2
+    st, lv, fo, sc = lko.prune_run(plan, g["ffa_fold"], g["thresholds"], int(g["ref_seg"]), int(g["max_sugg"]),
+                                   int(g["batch_size"]), int(g["branch_max"]), n_iters, bool(g["conservative"]),
+                                   basis=basis)
+    assert st.size - 1 == int(g[f"{tag}_levels"])
+    lv2, fo2, sc2, ep = lko.prune_finalize(plan, g["ffa_fold"], int(g["ref_seg"]), st.size - 1, lv, fo, sc,
+                                           basis=basis)
+    np.testing.assert_array_equal(lv2.view(np.uint64), g[f"{tag}_leaves"].view(np.uint64))
+    np.testing.assert_array_equal(fo2.view(np.uint32), g[f"{tag}_folds"].view(np.uint32))
+    np.testing.assert_array_equal(sc2.view(np.uint32), g[f"{tag}_scores"].view(np.uint32))
+    np.testing.assert_array_equal(ep.view(np.uint32), g[f"{tag}_scores_ep"].view(np.uint32))
+    assert lv2.shape[0] > 0
+
+
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref (the reference build) is not present")
+@pytest.mark.parametrize("case", range(len(REF_CASES)))
+@pytest.mark.parametrize("basis", ["taylor", "chebyshev"])
+def test_oracle_ascend_report_matches_reference_directly(case, basis):
+    ns, ts, nb, eta, lim, bf, seed, ms, bs, lo, hi, rf, cons = REF_CASES[case]
+    if basis == "chebyshev" and cons:
+        pytest.skip("the conservative tile has no Chebyshev form")
+    rc = R.make_cfg(ns, ts, nb, eta, lim, bseg_ffa=bf)
+    plan = lko.plan_create(lko.make_cfg(ns, ts, nb, eta, lim, bseg_ffa=bf))
+    e, v = _series(ns, seed)
+    fold = lko.ffa(plan, e, v)
+    nseg = int(plan.nsegments[-1])
+    ref_seg = min(int(nseg * rf), nseg - 1)
+    bm = max(R.branch_max(rc, cons), int(np.ceil(R.branching_pattern_basis(rc, basis, 0, cons).max() * 2)), 32)
+    thr = np.linspace(lo, hi, nseg - 1).astype(np.float32)
+    for n_iters in (nseg - 1, 2):
+        st, lv, fo, sc, ep = R.prune_run_full(rc, fold, thr, ref_seg, ms, bs, bm, n_iters, nb, cons, basis=basis)
+        st2, lv2, fo2, sc2 = lko.prune_run(plan, fold, thr, ref_seg, ms, bs, bm, n_iters, cons, basis=basis)
+        out = lko.prune_finalize(plan, fold, ref_seg, st2.size - 1, lv2, fo2, sc2, basis=basis)
+        for x, y in zip((lv, fo, sc, ep), out):
+            np.testing.assert_array_equal(x.view(np.uint8), y.view(np.uint8))
