@@ -53,11 +53,13 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--workload", default="taylor_accel",
-                    choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade", "multi_series"],
+                    choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade", "multi_series",
+                             "octave_sweep"],
                     help="taylor_accel (default): Taylor (f, fdot) FFA + S/N; freq_sweep: plain period "
                          "sweep; prune_jerk: FFA to 32 segments + one pruning run; mc_cascade: 8-stage "
                          "Monte-Carlo threshold cascade; multi_series: 512 series of uneven length, "
-                         "batched with CUDA graphs")
+                         "batched with CUDA graphs; octave_sweep: the frequency sweep over octave "
+                         "regions (FFAFreqSweep) on the freq_sweep series")
     return ap.parse_args()
 
 

@@ -10,6 +10,11 @@
                16 over the 31 levels (thresholds 3 -> 8), world tree 2^20,
                batches of 4096 parents. Metric: param-trials/s = leaves scored
                (sum over levels of n_leaves_phy) x boxcar widths per second.
+  octave_sweep the frequency sweep (FFAFreqSweep) over config 1's series: f
+               5-50 Hz in octave regions of 128 / 256 / 512 / 1024 bins, each
+               cut into chunks for 8 GB under the device memory model; per
+               chunk FFA + scores + `>= 7` compaction + parameter decode.
+               Metric: param-trials/s summed over chunks.
   mc_cascade   2^20 profiles x 64 bins, seed 99, 8 Monte-Carlo stages (variance
                doubling, pruning thresholds 2 -> 6) each counted against 64
                thresholds. Metric: param-trials/s = alive profiles x 64
@@ -207,6 +212,144 @@ def run_freq(args, rank, world, local_rank):
                                roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
                                gpu_launches=args.steps * launches, clocks=clk,
                                stages={k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()}))
+    _finish(dist)
+    return 0
+
+
+# ---- octave_sweep -----------------------------------------------------------------
+
+def _octave_cfg(params, storage_snr_min):
+    from loki_b200.configs import PulsarSearchConfig
+
+    return PulsarSearchConfig(params["nsamps"], params["tsamp"], params["nbins"], params["eta"],
+                              np.array(params["param_limits"]), use_fourier=False,
+                              score_widths=params["score_widths"], snr_min=storage_snr_min)
+
+
+def _ref_octave_runner(params, rows):
+    """The reference's per-chunk work (FFA::execute + snr_boxcar_3d + `>=`
+    compaction) over the chunk list, with all host threads."""
+    from oracle import ref
+
+    nthreads = os.cpu_count() or 1
+    widths = np.array(params["score_widths"], dtype=np.uint64)
+    chunks = []
+    for f_min, f_max, nb, eta in rows:
+        cfg = ref.make_cfg(params["nsamps"], params["tsamp"], int(nb), float(eta), [[f_min, f_max]],
+                           nthreads=nthreads)
+        chunks.append((ref.RefFFA(cfg, kind="timing"), int(nb)))
+
+    def step(ts_e, ts_v):
+        out = []
+        for ffa, nb in chunks:
+            fold = ffa.execute(ts_e, ts_v)
+            scores = ref.snr_boxcar_3d(fold, widths, nb, nthreads=nthreads, kind="timing").ravel()
+            idx = np.flatnonzero(scores >= B.SNR_MIN)
+            out.append((idx, scores[idx]))
+        return out
+
+    return step, nthreads
+
+
+def run_octaves(args, rank, world, local_rank):
+    """FFAFreqSweep over octave regions on config 1's series (the reference's
+    production caller): f 5-50 Hz from nbins 128, regions of 128 / 256 / 512 /
+    1024 bins, chunked for 8 GB under the device memory model."""
+    from loki_b200.sweep import FFARegionPlannerTime
+
+    ts_e, ts_v, params = _freq_params()
+    cfg = _octave_cfg(params, B.SNR_MIN)
+    planner = FFARegionPlannerTime(cfg, use_gpu=True)
+    rows = [(c["f_min"], c["f_max"], c["nbins"], c["eta"]) for c in planner.chunks]
+    nw = len(params["score_widths"])
+    ntrials = sum(int(c["ncoords"]) for c in planner.chunks) * nw
+    name = "octave_sweep_2^21x64us_f5-50Hz_nbins128-1024"
+    cfgd = {"nsamps": params["nsamps"], "tsamp": params["tsamp"], "nbins_min": params["nbins"],
+            "f_range_hz": params["param_limits"][0], "score_widths": params["score_widths"],
+            "snr_min": B.SNR_MIN, "chunks": [{"nbins": int(r[2]), "f_hz": [r[0], r[1]]} for r in rows],
+            "max_process_memory_gb": cfg.max_process_memory_gb}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from oracle import ref
+
+        if not ref.available("timing"):
+            B.emit({"impl": "reference", "unavailable": "oracle/_ref was not built"})
+            return 0
+        step, nthreads = _ref_octave_runner(params, rows)
+        for _ in range(max(args.warmup, 1)):
+            step(ts_e, ts_v)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(ts_e, ts_v)
+        total = time.perf_counter() - t0
+        v = ntrials * args.steps / total
+        B.emit(_line(args, world, name, v, 1e3 * total / args.steps, dict(cfgd, cpu_threads=nthreads),
+                     impl="reference",
+                     cpu_baseline={"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                                   "sample": f"full sweep, {args.steps} steps"},
+                     e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}))
+        return 0
+    torch, dist = _init(local_rank, world)
+    from loki_b200 import _capi as C
+    from loki_b200.sweep import FFAFreqSweepCUDA
+
+    sw = FFAFreqSweepCUDA(cfg, device_id=local_rank, fold_storage=args.storage)
+    e = torch.from_numpy(ts_e).cuda()
+    v = torch.from_numpy(ts_v).cuda()
+    flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+    L = C.lib()
+
+    def step():
+        C.check(L.lk_sweep_execute(sw._h, e.data_ptr(), v.data_ptr(), sp))
+
+    sw.set_profiling(True)
+    clocks = B.ClockSampler(local_rank)
+    clocks.start()
+    ms, _ = _timed(torch, step, args.steps, args.warmup, flush, dist)
+    clk = clocks.stop()
+    prof = {st["stage"]: (st["ms"], st["bytes"], st["launches"]) for st in sw.profile()}
+    sw.set_profiling(False)
+    launches = sum(p[2] for p in prof.values())
+    dom = max(prof, key=lambda k: prof[k][0])
+    value = ntrials * world / (ms / 1e3)
+    params_out, snr_out = sw.run(e, v)
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(args.steps):
+            p_, s_ = sw.run(ts_e, ts_v)
+            d2h += 8 * sum(int(c) for c in sw.region_counts) + 8 * len(rows)
+        el = time.perf_counter() - t0
+        e2e = {"value": ntrials * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": 8 * params["nsamps"],
+               "d2h_bytes_per_step": d2h // args.steps,
+               "api": "FFAFreqSweepCUDA.run (lk_sweep_execute + lk_sweep_results), host series, decoded "
+                      "parameter sets on the host"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+
+        if ref.available("timing"):
+            rstep, nthreads = _ref_octave_runner(params, rows)
+            rstep(ts_e, ts_v)
+            times = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                rstep(ts_e, ts_v)
+                times.append(time.perf_counter() - t0)
+            med = sorted(times)[1]
+            cpu = {"value": ntrials / med, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                   "sample": f"full sweep, median of 3 runs ({med:.3f} s each) of the reference's FFA::execute + "
+                             "snr_boxcar_3d + compaction per chunk, Release flags"}
+    if rank == 0:
+        B.emit(_line(args, world, name, value, ms,
+                     dict(cfgd, final_cells=ntrials // nw, candidates=int(snr_out.size), fold_storage=args.storage),
+                     roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
+                     gpu_launches=args.steps * launches, clocks=clk,
+                     stages={k: {"ms": p[0], "bytes": p[1], "launches": p[2]} for k, p in prof.items()}))
     _finish(dist)
     return 0
 
@@ -572,4 +715,4 @@ def run_multi(args, rank, world, local_rank):
 
 def run(args, rank, world, local_rank):
     return {"freq_sweep": run_freq, "prune_jerk": run_prune, "mc_cascade": run_mc,
-            "multi_series": run_multi}[args.workload](args, rank, world, local_rank)
+            "multi_series": run_multi, "octave_sweep": run_octaves}[args.workload](args, rank, world, local_rank)

@@ -310,6 +310,10 @@ int lk_ffa_set_profiling(lk_ffa* ffa, int enable);
 /* Synchronises the stream, then reports the stages of the last call. */
 int lk_ffa_get_profile(lk_ffa* ffa, lk_stream_t stream, lk_stage_time* out, uint32_t max_out,
                        uint32_t* n_out);
+/* Stage timing of the chunks' executors; the profile of the last execute is
+ * summed by stage kind over levels and chunks (level -1). */
+int lk_sweep_set_profiling(lk_sweep* sw, int enable);
+int lk_sweep_get_profile(lk_sweep* sw, lk_stage_time* out, uint32_t max_out, uint32_t* n_out);
 
 /* ---- brute fold (replaces BruteFoldCUDA<float>) ------------------------ */
 int lk_brute_fold_create(const double* freqs, uint64_t nfreqs, uint64_t segment_len,

@@ -165,6 +165,8 @@ SIGNATURES = [
     ("lk_sweep_chunk_info", i32, [vp, u64, vp]),
     ("lk_sweep_execute", i32, [vp, vp, vp, vp]),
     ("lk_sweep_results", i32, [vp, vp, vp, u64, vp, vp]),
+    ("lk_sweep_set_profiling", i32, [vp, i32]),
+    ("lk_sweep_get_profile", i32, [vp, vp, u32, vp]),
     ("lk_generate_ffa_regions", i32, [f64, f64, f64, u64, f64, f64, u64, vp, u64, vp]),
     ("lk_ffa_autotune", i32, [vp, vp, vp, u32, vp, vp]),
     ("lk_ffa_get_tuning", i32, [vp, vp]),

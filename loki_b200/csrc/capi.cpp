@@ -340,6 +340,27 @@ int lk_sweep_create(const lk_config* base, const lk_sweep_options* opt, int devi
 
 void lk_sweep_destroy(lk_sweep* sw) { delete sw; }
 
+int lk_sweep_set_profiling(lk_sweep* sw, int enable) {
+    return guarded([&] {
+        need(sw, "sw");
+        sw->exec->set_profiling(enable != 0);
+    });
+}
+
+int lk_sweep_get_profile(lk_sweep* sw, lk_stage_time* out, uint32_t max_out, uint32_t* n_out) {
+    return guarded([&] {
+        need(sw, "sw");
+        need(n_out, "n_out");
+        const auto st = sw->exec->profile(nullptr);
+        const auto n = static_cast<uint32_t>(std::min<size_t>(st.size(), max_out));
+        if (n > 0) {
+            need(out, "out");
+            std::copy(st.begin(), st.begin() + n, out);
+        }
+        *n_out = static_cast<uint32_t>(st.size());
+    });
+}
+
 int lk_generate_ffa_regions(double p_min, double p_max, double tsamp, uint64_t nbins_min,
                             double eta_min, double octave_scale, uint64_t nbins_max,
                             double* rows, uint64_t cap, uint64_t* n_out) {

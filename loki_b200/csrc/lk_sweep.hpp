@@ -55,6 +55,10 @@ public:
     const std::vector<float>& scores() const { return m_scores; }
     const std::vector<uint64_t>& region_counts() const { return m_region_counts; }
     uint32_t nparams() const { return m_base.nparams; }
+    // Stage timing of every chunk's executor (CUDA events); profile() sums
+    // the last execute's stages by kind over levels and chunks (level -1).
+    void set_profiling(bool enable);
+    std::vector<lk_stage_time> profile(cudaStream_t s);
 
 private:
     FFAExec& exec(size_t i);
@@ -68,6 +72,8 @@ private:
     std::vector<double> m_params;
     std::vector<float> m_scores;
     std::vector<uint64_t> m_region_counts;
+    bool m_profiling = false;
+    std::vector<lk_stage_time> m_prof;  // summed by kind during execute
 };
 
 }  // namespace lk

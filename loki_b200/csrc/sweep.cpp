@@ -256,9 +256,23 @@ FreqSweepExec::~FreqSweepExec() = default;
 FFAExec& FreqSweepExec::exec(size_t i) {
     if (!m_execs[i]) {
         m_execs[i] = std::make_unique<FFAExec>(make_plan(m_chunks[i].cfg), m_device, m_storage);
+        m_execs[i]->prof.enabled = m_profiling;
     }
     return *m_execs[i];
 }
+
+void FreqSweepExec::set_profiling(bool enable) {
+    m_profiling = enable;
+    for (auto& e : m_execs) {
+        if (e) {
+            e->prof.enabled = enable;
+            e->prof.reset();
+        }
+    }
+    m_prof.clear();
+}
+
+std::vector<lk_stage_time> FreqSweepExec::profile(cudaStream_t /*s*/) { return m_prof; }
 
 void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream_t s) {
     DeviceGuard g(m_device);
@@ -281,6 +295,22 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
     m_params.clear();
     m_scores.clear();
     m_region_counts.assign(m_chunks.size(), 0);
+    m_prof.clear();
+    auto add_profile = [&](FFAExec& ex) {
+        for (const lk_stage_time& st : ex.profile(s)) {
+            auto it = std::find_if(m_prof.begin(), m_prof.end(),
+                                   [&](const lk_stage_time& a) { return a.kind == st.kind; });
+            if (it == m_prof.end()) {
+                lk_stage_time a = st;
+                a.level = -1;
+                m_prof.push_back(a);
+            } else {
+                it->launches += st.launches;
+                it->ms += st.ms;
+                it->bytes += st.bytes;
+            }
+        }
+    };
     std::vector<uint32_t> h_idx;
     std::vector<float> h_snr;
     // `score >= snr_min` compares the float score promoted to double: the
@@ -314,6 +344,9 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
             LK_CUDA(cudaStreamSynchronize(s));
         }
         m_region_counts[i] = total;
+        if (m_profiling) {
+            add_profile(ex);
+        }
         // save_results (lib/ffa_freq_sweep.cpp:202-250): decode with the
         // chunk plan's final-level counts and Cartesian strides and (by
         // default) the base configuration's width list, as the reference

@@ -190,6 +190,18 @@ class FFAFreqSweepCUDA(_SweepHandle):
         self._region_counts = counts
         return self._param_sets, self._snr
 
+    def set_profiling(self, enable: bool = True) -> None:
+        """Record CUDA events around every kernel stage of every chunk."""
+        C.check(C.lib().lk_sweep_set_profiling(self._h, 1 if enable else 0))
+
+    def profile(self) -> list[dict]:
+        """Stages of the last run summed by kind over levels and chunks."""
+        arr = (C.LkStageTime * 16)()
+        n = ctypes.c_uint32()
+        C.check(C.lib().lk_sweep_get_profile(self._h, arr, 16, ctypes.byref(n)))
+        return [{"stage": C.STAGE_NAMES.get(arr[i].kind, str(arr[i].kind)), "launches": arr[i].launches,
+                 "ms": float(arr[i].ms), "bytes": int(arr[i].bytes)} for i in range(min(n.value, 16))]
+
     @property
     def region_counts(self) -> np.ndarray:
         """Passing candidates per chunk of the last run."""

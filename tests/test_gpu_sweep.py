@@ -114,3 +114,31 @@ def test_sweep_larger_chunked_vs_oracle(cuda):
     # the injected signals are found at their frequencies
     for f0 in (9.3, 41.7, 88.8):
         assert np.any(np.abs(params[:, 1] - f0) < 0.05 * f0)
+
+
+def test_sweep_octaves_to_nbins_max_vs_oracle(cuda):
+    """A plain period sweep over 1-250 Hz whose octaves grow from 62 to the
+    1024-bin cap (the brute fold's widest accumulators, the generic merge and
+    scoring paths), against the oracle composition."""
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.sweep import FFAFreqSweepCUDA
+
+    nsamps, tsamp = 1 << 17, 64e-6
+    lims = [[1.0, 250.0]]
+    ts_e, ts_v = series(nsamps, 5)
+    tt = np.arange(nsamps) * tsamp
+    for f0 in (2.3, 37.0, 180.0):
+        ts_e += (0.3 * (np.mod(tt * f0, 1.0) < 0.03)).astype(np.float32)
+    cfg = PulsarSearchConfig(nsamps, tsamp, 64, 1.0, np.array(lims), use_fourier=False,
+                             max_passing_candidates=1 << 16, snr_min=6.0)
+    for storage in ("fp32", "bf16"):
+        sw = FFAFreqSweepCUDA(cfg, fold_storage=storage, decode_chunk_widths=True)
+        assert [int(c["nbins"]) for c in sw.chunks] == [62, 124, 248, 496, 992, 1024]
+        params, snr = sw.run(ts_e, ts_v)
+        rows = np.array([[c["f_min"], c["f_max"], c["nbins"], c["eta"]] for c in sw.chunks])
+        o_params, o_snr, o_counts = osweep.run((nsamps, tsamp, 64, 1.0, lims), rows, ts_e, ts_v, 6.0,
+                                               chunk_widths=True)
+        np.testing.assert_array_equal(sw.region_counts, o_counts)
+        np.testing.assert_array_equal(params, o_params)
+        np.testing.assert_array_equal(snr.view(np.uint32), o_snr.view(np.uint32))
+        assert snr.size > 0
