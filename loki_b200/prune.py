@@ -183,20 +183,39 @@ class PruneCUDA:
 
 class EPMultiPassCUDA:
     """FFA to ``bseg_ffa`` segments, then one pruning run per reference segment
-    (reference ``EPMultiPass``: same arguments; ``device_id`` added)."""
+    (reference ``EPMultiPass``: same arguments; ``device_id`` added).
+
+    ``n_workers`` runs that many reference segments at once on the device, each
+    on its own executor, CUDA stream and host thread (the reference runs its
+    segments on a thread pool of ``nthreads`` workspaces); a pruning level is a
+    few small launches between host synchronisations, so concurrent runs fill
+    the GPU that one run leaves idle. Results do not depend on it."""
 
     def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
                  max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
-                 show_progress: bool = False, use_conservative_tile: bool = False, device_id: int = 0):
+                 show_progress: bool = False, use_conservative_tile: bool = False, device_id: int = 0,
+                 n_workers: int = 1):
         _basis(poly_basis)
         self._cfg = cfg
         self._thr = np.ascontiguousarray(threshold_scheme, dtype=np.float32)
         self._n_runs = n_runs
         self._ref_segs = ref_segs
         self._ffa = FFACUDA(cfg, device_id)
-        self._prune = PruneCUDA(cfg, max_sugg, batch_size, None, use_conservative_tile, device_id,
-                                poly_basis=poly_basis)
+        self._workers = max(1, int(n_workers))
+        self._prunes = [PruneCUDA(cfg, max_sugg, batch_size, None, use_conservative_tile, device_id,
+                                  poly_basis=poly_basis) for _ in range(self._workers)]
+        self._prune = self._prunes[0]
         self._device = device_id
+
+    def _run_one(self, pr: "PruneCUDA", fold, ref_seg: int, nseg: int, stream) -> dict:
+        t = D.torch()
+        with t.cuda.device(self._device), t.cuda.stream(stream):
+            stats = pr.run(fold, ref_seg, self._thr, n_iters=nseg - 1)
+            pr.finalize(fold)
+            leaves, folds, scores = pr.tree()
+            return {"stats": stats, "leaves": leaves, "folds": folds, "scores": scores,
+                    "scores_ep": pr.scores_ep(),
+                    "snail_scheme": np.array(middle_out_order(nseg, ref_seg), np.uint64)}
 
     @property
     def ffa(self) -> FFACUDA:
@@ -210,16 +229,35 @@ class EPMultiPassCUDA:
         ``<prefix>_pruning_nstages_<n>_results.npz`` (per run ``<ref_seg>_00``:
         param_sets, scores, scores_ep, snail_scheme, level_stats -- the
         reference's HDF5 run group) and a text log."""
+        t = D.torch()
         fold = self._ffa.execute(D.to_device_f32(ts_e, self._device), D.to_device_f32(ts_v, self._device))
         nseg = int(self._ffa.plan.nsegments[-1])
-        results = {}
-        for ref_seg in determine_ref_segs(nseg, self._n_runs, self._ref_segs):
-            stats = self._prune.run(fold, ref_seg, self._thr, n_iters=nseg - 1)
-            self._prune.finalize(fold)
-            leaves, folds, scores = self._prune.tree()
-            results[ref_seg] = {"stats": stats, "leaves": leaves, "folds": folds, "scores": scores,
-                                "scores_ep": self._prune.scores_ep(),
-                                "snail_scheme": np.array(middle_out_order(nseg, ref_seg), np.uint64)}
+        segs = determine_ref_segs(nseg, self._n_runs, self._ref_segs)
+        t.cuda.synchronize(self._device)  # the fold is complete before other streams read it
+        if self._workers == 1:
+            stream = t.cuda.current_stream(self._device)
+            runs = [self._run_one(self._prune, fold, rs, nseg, stream) for rs in segs]
+        else:
+            from concurrent.futures import ThreadPoolExecutor
+
+            streams = [t.cuda.Stream(device=self._device) for _ in range(self._workers)]
+            free = list(range(self._workers))
+            import threading
+
+            lock = threading.Lock()
+
+            def work(rs):
+                with lock:
+                    k = free.pop()
+                try:
+                    return self._run_one(self._prunes[k], fold, rs, nseg, streams[k])
+                finally:
+                    with lock:
+                        free.append(k)
+
+            with ThreadPoolExecutor(self._workers) as pool:
+                runs = list(pool.map(work, segs))
+        results = dict(zip(segs, runs))
         if outdir is not None:
             os.makedirs(outdir, exist_ok=True)
             base = os.path.join(outdir, f"{file_prefix}_pruning_nstages_{nseg}")

@@ -127,6 +127,27 @@ def test_ep_multipass_end_to_end(cuda):
         assert r["snail_scheme"][0] == rs
 
 
+def test_ep_multipass_concurrent_runs_identical(cuda, tmp_path):
+    """Reference segments run on 3 executors at once (own streams and host
+    threads) give exactly the sequential results, and the .npz holds one run
+    group per segment."""
+    from loki_b200.prune import EPMultiPassCUDA
+
+    plan, cfg, (e, v), fold, nseg, _, thr, ms, bs, cons = _setup("accel_nb32_many_batches")
+    seq = EPMultiPassCUDA(cfg, thr, n_runs=5, max_sugg=ms, batch_size=bs).execute(e, v)
+    par = EPMultiPassCUDA(cfg, thr, n_runs=5, max_sugg=ms, batch_size=bs, n_workers=3).execute(
+        e, v, outdir=str(tmp_path), file_prefix="t")
+    assert sorted(seq) == sorted(par) and len(seq) == 5
+    for rs in seq:
+        for k in ("leaves", "folds", "scores", "scores_ep"):
+            np.testing.assert_array_equal(par[rs][k].view(np.uint8), seq[rs][k].view(np.uint8))
+        np.testing.assert_array_equal(_stats_matrix(par[rs]["stats"]), _stats_matrix(seq[rs]["stats"]))
+    z = np.load(tmp_path / f"t_pruning_nstages_{nseg}_results.npz")
+    for rs in seq:
+        np.testing.assert_array_equal(z[f"{rs:03d}_00/param_sets"], seq[rs]["leaves"])
+        np.testing.assert_array_equal(z[f"{rs:03d}_00/scores_ep"], seq[rs]["scores_ep"])
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_prune_finalize_bit_exact(cuda, name):
     """Ascend + report (the end of PruneImpl::run) after full and partial runs."""
