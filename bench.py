@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
+    ap.add_argument("--pipeline-execs", type=int, default=2,
+                    help="executors (own compute streams) the end-to-end search pipeline alternates between")
     ap.add_argument("--workload", default="taylor_accel",
                     choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade", "multi_series",
                              "octave_sweep"],
@@ -351,14 +353,16 @@ def run_ours(args, rank, world, local_rank):
     # end to end through the public API with host buffers: every step copies
     # its series from pinned host memory and reads its candidates back; the
     # pipeline overlaps step k + 1's copy and step k - 1's read-back with step
-    # k's search (two device input slots, a copy stream and a compute stream)
+    # k's search, and alternates consecutive steps between two executors on
+    # their own compute streams (one step's brute fold beside the previous
+    # step's merges and scoring)
     e2e = None
     if not args.no_e2e:
         from loki_b200.pipeline import SearchPipeline
 
         he = torch.from_numpy(ts_e).pin_memory()
         hv = torch.from_numpy(ts_v).pin_memory()
-        pipe = SearchPipeline(ffa, SNR_MIN, max_cands=cap)
+        pipe = SearchPipeline(ffa, SNR_MIN, max_cands=cap, n_exec=args.pipeline_execs)
         for _ in pipe.run([(he, hv)] * args.warmup):
             pass
         torch.cuda.synchronize()
@@ -375,7 +379,8 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": ntrials * world * args.steps / float(t.item()), "unit": UNIT,
                "h2d_bytes_per_step": pipe.h2d_bytes // args.steps, "d2h_bytes_per_step": pipe.d2h_bytes // args.steps,
                "api": "loki_b200.pipeline.SearchPipeline over FFACUDA (lk_ffa_search): pinned host series in, "
-                      "candidates out, copies overlapped with the previous/next search"}
+                      "candidates out, copies overlapped with the previous/next search, "
+                      f"{args.pipeline_execs} executors on their own compute streams"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -43,6 +43,7 @@ class FFACUDA:
         self._plan = FFAPlanTime(cfg)
         self._device = device_id
         self._max_batch = int(max_batch)
+        self._storage = fold_storage
         if fold_storage not in _STORAGE:
             raise ValueError(f"fold_storage must be one of {sorted(_STORAGE)}")
         h = ctypes.c_void_p()
@@ -63,6 +64,19 @@ class FFACUDA:
     @property
     def plan(self) -> FFAPlanTime:
         return self._plan
+
+    @property
+    def fold_storage(self) -> str:
+        return self._storage
+
+    def clone(self) -> "FFACUDA":
+        """A second executor of the same configuration, storage and tuning
+        (its own buffers, so the two can search on different streams)."""
+        other = FFACUDA(self._cfg, self._device, self._storage, self._max_batch)
+        other.set_tuning(self.tuning)
+        if self._storage == "bf16":
+            other.set_rescore_margin(*self.rescore_margin)
+        return other
 
     @property
     def device_id(self) -> int:

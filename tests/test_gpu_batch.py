@@ -118,12 +118,13 @@ def test_search_pipeline_matches_search(cuda):
     s0 = ffa.scores(*data[0])
     thr = float(np.quantile(s0, 0.999))
     want = [ffa.search(e, v, snr_min=thr) for e, v in data]
-    got = list(SearchPipeline(ffa, thr, max_cands=1 << 16).run(data))
-    assert len(got) == len(want)
-    for (gi, gs, gn), (wi, ws, wn) in zip(got, want):
-        assert gn == wn
-        np.testing.assert_array_equal(gi, wi)
-        np.testing.assert_array_equal(gs.view(np.uint32), ws.view(np.uint32))
+    for n_exec in (1, 2, 3):
+        got = list(SearchPipeline(ffa, thr, max_cands=1 << 16, n_exec=n_exec).run(data))
+        assert len(got) == len(want)
+        for (gi, gs, gn), (wi, ws, wn) in zip(got, want):
+            assert gn == wn
+            np.testing.assert_array_equal(gi, wi)
+            np.testing.assert_array_equal(gs.view(np.uint32), ws.view(np.uint32))
 
 
 @pytest.mark.parametrize("nbins,lims,storage", [(64, [[-200.0, 200.0], [5.0, 50.0]], "fp32"),
