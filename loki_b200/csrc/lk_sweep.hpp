@@ -48,7 +48,8 @@ public:
     FreqSweepExec(const lk_config& base, const SweepOptions& opt, int device, int storage);
     ~FreqSweepExec();
     // Every chunk: FFA + scores + compaction `>= snr_min` + parameter decode.
-    // Synchronises the stream once per chunk.
+    // Chunks run on two internal streams after the work already queued on
+    // `s`; synchronises `s` twice (counts, then candidates).
     void execute(const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
     const std::vector<SweepChunk>& chunks() const { return m_chunks; }
     const std::vector<double>& params() const { return m_params; }   // [n][nparams + 1]
@@ -74,6 +75,10 @@ private:
     std::vector<uint64_t> m_region_counts;
     bool m_profiling = false;
     std::vector<lk_stage_time> m_prof;  // summed by kind during execute
+    static constexpr int kSweepStreams = 2;  // chunks alternate between them
+    std::vector<cudaStream_t> m_streams;
+    std::vector<cudaEvent_t> m_done;
+    cudaEvent_t m_ready = nullptr;
 };
 
 }  // namespace lk

@@ -251,8 +251,6 @@ FreqSweepExec::FreqSweepExec(const lk_config& base, const SweepOptions& opt, int
     m_execs.resize(m_chunks.size());
 }
 
-FreqSweepExec::~FreqSweepExec() = default;
-
 FFAExec& FreqSweepExec::exec(size_t i) {
     if (!m_execs[i]) {
         m_execs[i] = std::make_unique<FFAExec>(make_plan(m_chunks[i].cfg), m_device, m_storage);
@@ -277,90 +275,125 @@ std::vector<lk_stage_time> FreqSweepExec::profile(cudaStream_t /*s*/) { return m
 void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream_t s) {
     DeviceGuard g(m_device);
     const uint32_t np = m_base.nparams;
-    // Room for every cell of the largest chunk (the reference's scores buffer
-    // is max(max_ncoords * n_widths, max_passing_candidates)), so a chunk
-    // never overflows it.
-    uint64_t cap = std::max<uint64_t>(1, m_opt.max_passing_candidates);
-    for (const auto& c : m_chunks) {
+    const size_t nch = m_chunks.size();
+    // Every chunk gets room for all of its cells (the reference's scores
+    // buffer holds max(max_ncoords * n_widths, max_passing_candidates)), so a
+    // chunk never overflows; chunks are searched concurrently, each into its
+    // own region.
+    std::vector<uint64_t> off(nch + 1, 0), cap(nch, 0);
+    for (size_t i = 0; i < nch; ++i) {
+        const auto& c = m_chunks[i];
         const uint64_t nw = m_base.n_score_widths > 0
                                 ? m_base.n_score_widths
                                 : box_width_trials(c.cfg.nbins, c.cfg.ducy_max, c.cfg.wtsp).size();
-        cap = std::max(cap, c.ncoords * nw);
+        cap[i] = std::max<uint64_t>(1, c.ncoords * nw);
+        off[i + 1] = off[i] + cap[i];
     }
-    if (m_idx.bytes < cap * sizeof(uint32_t)) {
-        m_idx.alloc(cap * sizeof(uint32_t));
-        m_snr.alloc(cap * sizeof(float));
-        m_cnt.alloc(sizeof(uint64_t));
+    if (m_idx.bytes < off[nch] * sizeof(uint32_t)) {
+        m_idx.alloc(off[nch] * sizeof(uint32_t));
+        m_snr.alloc(off[nch] * sizeof(float));
+    }
+    if (m_cnt.bytes < std::max<size_t>(1, nch) * sizeof(uint64_t)) {
+        m_cnt.alloc(std::max<size_t>(1, nch) * sizeof(uint64_t));
+    }
+    if (m_streams.empty()) {
+        m_streams.resize(kSweepStreams);
+        m_done.resize(kSweepStreams);
+        for (int k = 0; k < kSweepStreams; ++k) {
+            LK_CUDA(cudaStreamCreateWithFlags(&m_streams[k], cudaStreamNonBlocking));
+            LK_CUDA(cudaEventCreateWithFlags(&m_done[k], cudaEventDisableTiming));
+        }
+        LK_CUDA(cudaEventCreateWithFlags(&m_ready, cudaEventDisableTiming));
     }
     m_params.clear();
     m_scores.clear();
-    m_region_counts.assign(m_chunks.size(), 0);
+    m_region_counts.assign(nch, 0);
     m_prof.clear();
-    auto add_profile = [&](FFAExec& ex) {
-        for (const lk_stage_time& st : ex.profile(s)) {
-            auto it = std::find_if(m_prof.begin(), m_prof.end(),
-                                   [&](const lk_stage_time& a) { return a.kind == st.kind; });
-            if (it == m_prof.end()) {
-                lk_stage_time a = st;
-                a.level = -1;
-                m_prof.push_back(a);
-            } else {
-                it->launches += st.launches;
-                it->ms += st.ms;
-                it->bytes += st.bytes;
-            }
-        }
-    };
-    std::vector<uint32_t> h_idx;
-    std::vector<float> h_snr;
     // `score >= snr_min` compares the float score promoted to double: the
     // same set as `score >= thr` with thr the smallest float not below snr_min.
     float thr = static_cast<float>(m_base.snr_min);
     if (static_cast<double>(thr) < m_base.snr_min) {
         thr = std::nextafter(thr, std::numeric_limits<float>::infinity());
     }
-    for (size_t i = 0; i < m_chunks.size(); ++i) {
+    // Chunks alternate between two streams: one chunk's brute fold runs
+    // beside the previous chunk's merges and scoring. The executors are built
+    // first (allocations synchronise the device).
+    for (size_t i = 0; i < nch; ++i) {
         FFAExec& ex = exec(i);
-        const Plan& pl = ex.plan;
-        const std::vector<uint32_t>& dec_widths =
-            m_opt.decode_chunk_widths ? pl.widths : m_base_widths;
-        const uint64_t nw_dec = dec_widths.size();
-        const uint32_t L = pl.n_levels - 1;
-        require(pl.nsegments[L] == 1,
+        require(ex.plan.nsegments[ex.plan.n_levels - 1] == 1,
                 "FFAFreqSweep::execute_ffa_region: nsegments must be 1 to call scoring function");
-        ex.search(d_ts_e, d_ts_v, thr, m_idx.as<uint32_t>(),
-                  m_snr.as<float>(), cap, m_cnt.as<uint64_t>(), s);
-        uint64_t total = 0;
-        LK_CUDA(cudaMemcpyAsync(&total, m_cnt.ptr, sizeof(total), cudaMemcpyDeviceToHost, s));
-        LK_CUDA(cudaStreamSynchronize(s));
-        require(total <= cap, "FFAFreqSweep: candidate buffer overflow");
-        h_idx.resize(total);
-        h_snr.resize(total);
-        if (total > 0) {
-            LK_CUDA(cudaMemcpyAsync(h_idx.data(), m_idx.ptr, total * sizeof(uint32_t),
-                                    cudaMemcpyDeviceToHost, s));
-            LK_CUDA(cudaMemcpyAsync(h_snr.data(), m_snr.ptr, total * sizeof(float),
-                                    cudaMemcpyDeviceToHost, s));
-            LK_CUDA(cudaStreamSynchronize(s));
+    }
+    LK_CUDA(cudaEventRecord(m_ready, s));
+    for (int k = 0; k < kSweepStreams; ++k) {
+        LK_CUDA(cudaStreamWaitEvent(m_streams[k], m_ready, 0));
+    }
+    for (size_t i = 0; i < nch; ++i) {
+        m_execs[i]->search(d_ts_e, d_ts_v, thr, m_idx.as<uint32_t>() + off[i],
+                           m_snr.as<float>() + off[i], cap[i], m_cnt.as<uint64_t>() + i,
+                           m_streams[i % kSweepStreams]);
+    }
+    for (int k = 0; k < kSweepStreams; ++k) {
+        LK_CUDA(cudaEventRecord(m_done[k], m_streams[k]));
+        LK_CUDA(cudaStreamWaitEvent(s, m_done[k], 0));
+    }
+    std::vector<uint64_t> counts(nch, 0);
+    if (nch > 0) {
+        LK_CUDA(cudaMemcpyAsync(counts.data(), m_cnt.ptr, nch * sizeof(uint64_t),
+                                cudaMemcpyDeviceToHost, s));
+    }
+    LK_CUDA(cudaStreamSynchronize(s));
+    std::vector<std::vector<uint32_t>> h_idx(nch);
+    std::vector<std::vector<float>> h_snr(nch);
+    for (size_t i = 0; i < nch; ++i) {
+        require(counts[i] <= cap[i], "FFAFreqSweep: candidate buffer overflow");
+        h_idx[i].resize(counts[i]);
+        h_snr[i].resize(counts[i]);
+        if (counts[i] > 0) {
+            LK_CUDA(cudaMemcpyAsync(h_idx[i].data(), m_idx.as<uint32_t>() + off[i],
+                                    counts[i] * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            LK_CUDA(cudaMemcpyAsync(h_snr[i].data(), m_snr.as<float>() + off[i],
+                                    counts[i] * sizeof(float), cudaMemcpyDeviceToHost, s));
         }
-        m_region_counts[i] = total;
+    }
+    LK_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < nch; ++i) {
+        FFAExec& ex = *m_execs[i];
         if (m_profiling) {
-            add_profile(ex);
+            for (const lk_stage_time& st : ex.profile(m_streams[i % kSweepStreams])) {
+                auto it = std::find_if(m_prof.begin(), m_prof.end(),
+                                       [&](const lk_stage_time& a) { return a.kind == st.kind; });
+                if (it == m_prof.end()) {
+                    lk_stage_time a = st;
+                    a.level = -1;
+                    m_prof.push_back(a);
+                } else {
+                    it->launches += st.launches;
+                    it->ms += st.ms;
+                    it->bytes += st.bytes;
+                }
+            }
         }
+        const Plan& pl = ex.plan;
+        const uint32_t L = pl.n_levels - 1;
+        const uint64_t total = counts[i];
+        m_region_counts[i] = total;
         // save_results (lib/ffa_freq_sweep.cpp:202-250): decode with the
         // chunk plan's final-level counts and Cartesian strides and (by
         // default) the base configuration's width list, as the reference
         // does.
-        std::vector<uint64_t> counts(np), strides(np);
+        const std::vector<uint32_t>& dec_widths =
+            m_opt.decode_chunk_widths ? pl.widths : m_base_widths;
+        const uint64_t nw_dec = dec_widths.size();
+        std::vector<uint64_t> pc(np), strides(np);
         for (uint32_t j = 0; j < np; ++j) {
-            counts[j] = pl.param_counts[L][j];
+            pc[j] = pl.param_counts[L][j];
         }
         strides[np - 1] = 1;
         for (int j = static_cast<int>(np) - 2; j >= 0; --j) {
-            strides[j] = strides[j + 1] * counts[j + 1];
+            strides[j] = strides[j + 1] * pc[j + 1];
         }
         for (uint64_t k = 0; k < total; ++k) {
-            const uint64_t score_idx = h_idx[k];
+            const uint64_t score_idx = h_idx[i][k];
             const uint64_t coord_idx = score_idx / nw_dec;
             const uint64_t width_idx = score_idx % nw_dec;
             uint64_t rem = coord_idx;
@@ -369,17 +402,29 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
                 rem -= pidx * strides[j];
                 const double vmin = pl.lim_min(j), vmax = pl.lim_max(j);
                 double val;
-                if (counts[j] <= 1) {
+                if (pc[j] <= 1) {
                     val = (vmax + vmin) / 2.0;
                 } else {
-                    const double dv = (vmax - vmin) / static_cast<double>(counts[j]);
+                    const double dv = (vmax - vmin) / static_cast<double>(pc[j]);
                     val = vmin + (dv * (static_cast<double>(pidx) + 0.5));
                 }
                 m_params.push_back(val);
             }
             m_params.push_back(static_cast<double>(dec_widths[width_idx]));
-            m_scores.push_back(h_snr[k]);
+            m_scores.push_back(h_snr[i][k]);
         }
+    }
+}
+
+FreqSweepExec::~FreqSweepExec() {
+    if (!m_streams.empty()) {
+        DeviceGuard g(m_device);
+        for (int k = 0; k < kSweepStreams; ++k) {
+            cudaStreamSynchronize(m_streams[k]);
+            cudaEventDestroy(m_done[k]);
+            cudaStreamDestroy(m_streams[k]);
+        }
+        cudaEventDestroy(m_ready);
     }
 }
 
