@@ -678,7 +678,7 @@ def run_multi(args, rank, world, local_rank):
     clk = clocks.stop()
     trials = 0
     for L in {_pow2_ceil(n) for n in lens}:
-        g = ms.groups[L]
+        g = ms.groups[L][0]
         trials += g.per * sum(1 for n in lens if _pow2_ceil(n) == L)
     value = trials * world / (ms_step / 1e3)
     ncand = sum(r["total"] for r in outs[-1])
@@ -701,8 +701,9 @@ def run_multi(args, rank, world, local_rank):
             cpu = {"value": cv, "unit": UNIT, "cores": nthreads, "kind": "reference",
                    "sample": f"{npick} series spread over the lengths, one FFA + scores + compaction each "
                              f"({el:.1f} s), reference CPU code with its Release flags"}
-    groups = {str(L): {"series": sum(1 for n in lens if _pow2_ceil(n) == L), "batch": ms.groups[L].nbatch,
-                       "trials_per_series": ms.groups[L].per} for L in sorted(ms.groups)}
+    groups = {str(L): {"series": sum(1 for n in lens if _pow2_ceil(n) == L), "batch": ms.groups[L][0].nbatch,
+                       "slots": len(ms.groups[L]), "trials_per_series": ms.groups[L][0].per}
+              for L in sorted(ms.groups)}
     if rank == 0:
         B.emit(_line(args, world, "multi_series_512x2^18..2^22_nbins128", value, ms_step,
                                dict(cfgd, trials_per_step=trials, candidates=ncand, groups=groups,

@@ -161,3 +161,28 @@ def test_autotune_keeps_results(cuda, nbins, lims, storage):
     other.set_tuning(t)
     for k in ("bf_rows", "bf_warps", "bf_stages", "merge_rows_in_flight", "score_cells_per_block"):
         assert other.tuning[k] == t[k]
+
+
+def test_multi_series_slots_identical(cuda):
+    """Batches alternating over two executor slots (own streams, own graphs)
+    give exactly the one-slot results; device inputs, several batches per
+    length, partial last batches."""
+    from loki_b200.batched import MultiSeriesSearch
+
+    t = cuda
+    rng = np.random.default_rng(8)
+    lengths = [8192] * 7 + [5000] * 3 + [16384] * 4
+    data = [(t.from_numpy(rng.standard_normal(L).astype(np.float32)).cuda(),
+             t.from_numpy((1.0 + 0.2 * rng.random(L)).astype(np.float32)).cuda()) for L in lengths]
+    kw = dict(tsamp=1e-3, nbins=32, f_range=(5.0, 9.0), widths=[1, 2, 3, 4], snr_min=3.0, max_batch=2)
+    one = MultiSeriesSearch(n_slots=1, **kw).search(data)
+    two = MultiSeriesSearch(n_slots=2, **kw).search(data)
+    again = MultiSeriesSearch(n_slots=2, **kw)
+    again.search(data[:3])
+    three = again.search(data)  # graphs captured, slots reused
+    for a, b, c in zip(one, two, three):
+        for r in (b, c):
+            assert r["total"] == a["total"] and r["nsamps"] == a["nsamps"]
+            np.testing.assert_array_equal(r["idx"], a["idx"])
+            np.testing.assert_array_equal(r["snr"].view(np.uint32), a["snr"].view(np.uint32))
+    assert sum(r["total"] for r in one) > 0
