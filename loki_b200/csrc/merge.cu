@@ -243,6 +243,14 @@ void merge_level(const void* d_in, void* d_out, const void* d_coords, bool taylo
                     pb == 1   ? go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 1>)
                     : pb == 4 ? go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 4>)
                               : go_p2(merge_kernel_p2<TG, TIn, TOut, 128, 2>);
+                } else if (nbins == 256) {
+                    // the octave sweep's wider regions: one row per warp in
+                    // flight (32 / 64 / 128 loads per lane)
+                    go_p2(merge_kernel_p2<TG, TIn, TOut, 256, 1>);
+                } else if (nbins == 512) {
+                    go_p2(merge_kernel_p2<TG, TIn, TOut, 512, 1>);
+                } else if (nbins == 1024) {
+                    go_p2(merge_kernel_p2<TG, TIn, TOut, 1024, 1>);
                 } else if (nbins <= 32) {
                     go(merge_kernel_mlp<TG, TIn, TOut, 1, 8>);
                 } else if (nbins <= 64) {

@@ -254,7 +254,7 @@ void merge_score_level(const void* d_in, const void* d_coords, bool taylor, uint
             d_scores, d_cmax);
     };
     const int nwb = sp.nwidths <= 8 ? 8 : (sp.nwidths <= 16 ? 16 : 32);
-    const int nj = nbins <= 32 ? 1 : (nbins <= 64 ? 2 : (nbins <= 128 ? 4 : 0));
+    const int nj = nbins <= 32 ? 1 : (nbins <= 64 ? 2 : (nbins <= 128 ? 4 : (nbins <= 256 ? 8 : 0)));
     // Dispatch (taylor, width bucket, bins per lane); PB * NJ = 16 loads of
     // each kind in flight per lane.
     auto pick = [&](auto tg, auto tin) {
@@ -275,6 +275,8 @@ void merge_score_level(const void* d_in, const void* d_coords, bool taylor, uint
             } else if (nj == 4) {
                 fixed ? launch(merge_score_kernel<TG, NWC, 4, 4, TI, 128 * FX>)
                       : launch(merge_score_kernel<TG, NWC, 4, 4, TI, 0>);
+            } else if (nj == 8) {
+                launch(merge_score_kernel<TG, NWC, 8, 2, TI, 0>);
             } else {
                 launch(merge_score_kernel<TG, NWC, 0, 1, TI, 0>);
             }
