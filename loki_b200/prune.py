@@ -189,7 +189,9 @@ class EPMultiPassCUDA:
     on its own executor, CUDA stream and host thread (the reference runs its
     segments on a thread pool of ``nthreads`` workspaces); a pruning level is a
     few small launches between host synchronisations, so concurrent runs fill
-    the GPU that one run leaves idle. Results do not depend on it."""
+    the GPU that one run leaves idle. Results do not depend on it. Two workers
+    measured 1.5x one on the jerk search; four were slower than one (the
+    host threads' stream waits contend)."""
 
     def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
                  max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
