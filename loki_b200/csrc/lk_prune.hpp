@@ -102,6 +102,7 @@ private:
     uint64_t m_level = 0;
     bool m_ran = false, m_finalized = false;
     DeviceBuffer m_segs, m_tscores_ep;
+    DeviceBuffer m_level_mm;  // per level: orderable min / max score keys
 };
 
 // Single steps (the Taylor PruneDPFuncts interface, include/loki/core/

@@ -1473,6 +1473,11 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
     m_ran = true;
     m_finalized = false;
     const uint64_t levels = std::min<uint64_t>(m_nseg - 1, n_iters);
+    // Each level's score minimum / maximum stays in its own device slot and
+    // is read back once, after the last level.
+    if (m_level_mm.bytes < 2 * (levels + 1) * sizeof(uint32_t)) {
+        m_level_mm.alloc(2 * (levels + 1) * sizeof(uint32_t));
+    }
     for (uint64_t lv = 1; lv <= levels; ++lv) {
         require(lv <= n_thresholds, "Pruning complete - exceeded threshold scheme length");
         const float* d_seg = d_ffa_fold + order[lv] * seg_floats;
@@ -1482,6 +1487,17 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
         m_level = lv;
         if (m_tree.size == 0) {
             break;
+        }
+    }
+    if (stats.size() > 1) {
+        std::vector<uint32_t> mm(2 * stats.size());
+        LK_CUDA(cudaMemcpyAsync(mm.data(), m_level_mm.ptr, mm.size() * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, s));
+        LK_CUDA(cudaStreamSynchronize(s));
+        for (size_t k = 1; k < stats.size(); ++k) {
+            const bool any = stats[k].n_leaves > 0;
+            stats[k].score_min = any ? key_to_float(mm[2 * k]) : FLT_MAX;
+            stats[k].score_max = any ? key_to_float(mm[2 * k + 1]) : -FLT_MAX;
         }
     }
     return stats;
@@ -1496,7 +1512,7 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
     uint64_t* d_size[2] = {reinterpret_cast<uint64_t*>(misc + kMiscSize0),
                            reinterpret_cast<uint64_t*>(misc + kMiscSize1)};
     auto* d_total = reinterpret_cast<uint64_t*>(misc + kMiscTotal);
-    auto* d_mm = reinterpret_cast<uint32_t*>(misc + kMiscMinMax);
+    auto* d_mm = m_level_mm.as<uint32_t>() + 2 * lv;  // this level's min / max keys
 
     // prepare_in_place_update (lib/world_tree.cpp:237-249)
     t.size_old = t.size;
@@ -1622,6 +1638,7 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
     set_f32_kernel<<<1, 1, 0, s>>>(d_thr, threshold);
     set_u64_kernel<<<1, 1, 0, s>>>(d_size[0], 0);
     uint64_t b = 0;
+    bool size_known = true;  // t.size (0 here) matches the device's list size
     while (b < nbat) {
         batch_count_kernel<<<static_cast<unsigned>(nbat - b), 256, 0, s>>>(
             m_cscores.as<float>(), m_bchild.as<uint64_t>(), b, d_thr, m_bcounts.as<uint32_t>());
@@ -1631,6 +1648,7 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
         LK_CUDA(cudaMemcpyAsync(h, d_size[li], sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         LK_CUDA(cudaStreamSynchronize(s));
         t.size = *reinterpret_cast<uint64_t*>(h);
+        size_known = true;
         // fast path of add_batch_scattered (lib/world_tree.cpp:376-384)
         uint64_t bf = b;
         while (bf < nbat) {
@@ -1668,13 +1686,13 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
         li = 1 - li;
         t.read_consumed += bsize[bf];
         b = bf + 1;
+        size_known = false;  // the overload step's size is on the device
     }
-    LK_CUDA(cudaMemcpyAsync(h, d_size[li], sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    LK_CUDA(cudaMemcpyAsync(h + 8, d_mm, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    LK_CUDA(cudaStreamSynchronize(s));
-    t.size = *reinterpret_cast<uint64_t*>(h);
-    const uint32_t kmin = reinterpret_cast<uint32_t*>(h + 8)[0];
-    const uint32_t kmax = reinterpret_cast<uint32_t*>(h + 8)[1];
+    if (!size_known) {
+        LK_CUDA(cudaMemcpyAsync(h, d_size[li], sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        LK_CUDA(cudaStreamSynchronize(s));
+        t.size = *reinterpret_cast<uint64_t*>(h);
+    }
 
     // 4. transform + gather into the other tree buffer; finalize_in_place_update
     if (t.size > 0) {
@@ -1699,8 +1717,9 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
     st->n_leaves_phy = n_child;
     st->n_leaves_surv = t.size;
     st->threshold = threshold;
-    st->score_min = n_child ? key_to_float(kmin) : FLT_MAX;
-    st->score_max = n_child ? key_to_float(kmax) : -FLT_MAX;
+    // score_min / score_max: filled by run() from this level's device slot
+    st->score_min = FLT_MAX;
+    st->score_max = -FLT_MAX;
 }
 
 void PruneExec::finalize(const float* d_ffa_fold, cudaStream_t s) {
