@@ -1086,9 +1086,16 @@ __global__ void parent_transform_kernel(double* __restrict__ tree_leaves, uint64
     }
 }
 
-__global__ void set_f32_kernel(float* p, float v) { *p = v; }
 __global__ void set_u64_kernel(uint64_t* p, uint64_t v) { *p = v; }
 __global__ void init_minmax_kernel(uint32_t* mm) {
+    mm[0] = 0xffffffffu;
+    mm[1] = 0u;
+}
+// A level's starting state in one launch: its threshold, an empty write
+// list and its score min / max slot.
+__global__ void level_init_kernel(float* thr, float v, uint64_t* size, uint32_t* mm) {
+    *thr = v;
+    *size = 0;
     mm[0] = 0xffffffffu;
     mm[1] = 0u;
 }
@@ -1573,6 +1580,9 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
             make_transform_cheby(cc, cp));
     }
     const double* tree_leaves = m_tleaves[m_cur].as<double>();
+    // nothing before the batch replay reads the threshold or the list size,
+    // and nothing before the leaf kernel the min / max slot
+    level_init_kernel<<<1, 1, 0, s>>>(d_thr, threshold, d_size[0], d_mm);
     LK_CUDA(cudaMemcpyAsync(m_bparents.ptr, h_bpar, (nbat + 1) * sizeof(uint64_t),
                             cudaMemcpyHostToDevice, s));
     branch_count_kernel<<<grid_for(n_par, 256), 256, 0, s>>>(
@@ -1613,7 +1623,6 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
     branch_emit_kernel<<<grid_for(n_par, 256), 256, 0, s>>>(
         tree_leaves, t.head, t.cap, n_par, cc.scale, geom, m_offsets.as<uint64_t>(),
         m_cleaves.as<double>(), m_cparent.as<uint32_t>(), m_status.as<uint32_t>());
-    init_minmax_kernel<<<1, 1, 0, s>>>(d_mm);
     if (n_child > 0) {
         const ResolveConsts rc = m_basis == 1 ? make_resolve_cheby(m_np, ca, cc, ci)
                                               : make_resolve(m_np, ca.ref, cc.ref, ci.ref);
@@ -1635,8 +1644,6 @@ void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, ui
 
     // 3. filter + add, batch by batch in the reference's order
     int li = 0;
-    set_f32_kernel<<<1, 1, 0, s>>>(d_thr, threshold);
-    set_u64_kernel<<<1, 1, 0, s>>>(d_size[0], 0);
     uint64_t b = 0;
     bool size_known = true;  // t.size (0 here) matches the device's list size
     while (b < nbat) {
