@@ -232,6 +232,12 @@ typedef struct lk_sweep_options {
      * process model of FFAFreqSweep (fold buffers, coordinates, scores,
      * indices, write batch; lib/regions.cpp:101-135). */
     int32_t device_memory_model;
+    /* Chunk executors: 0 decides at the first execute (every chunk's executor
+     * kept resident, chunks overlapping on two streams, when their planned
+     * memory fits in free device memory with room to spare; else one chunk at
+     * a time, each executor released after its chunk), 1 resident, 2 one at a
+     * time. Results do not depend on it. */
+    int32_t executor_mode;
 } lk_sweep_options;
 /* regions::generate_ffa_regions (lib/regions.cpp:31-78): rows of (f_start,
  * f_end, nbins, eta); *n_out regions, rows written up to cap. */

@@ -330,6 +330,9 @@ int lk_sweep_create(const lk_config* base, const lk_sweep_options* opt, int devi
             o.max_passing_candidates = opt->max_passing_candidates;
             o.decode_chunk_widths = opt->decode_chunk_widths != 0;
             o.device_memory_model = opt->device_memory_model != 0;
+            lk::require(opt->executor_mode >= 0 && opt->executor_mode <= 2,
+                        "executor_mode must be 0 (auto), 1 (resident) or 2 (one chunk at a time)");
+            o.executor_mode = opt->executor_mode;
         }
         lk::require(o.max_memory_gb > 0, "max_process_memory_gb must be positive");
         auto h = std::make_unique<lk_sweep>();

@@ -26,6 +26,7 @@ struct SweepOptions {
     uint64_t max_passing_candidates = 1ull << 22;
     bool decode_chunk_widths = false;  // false: the reference's decode (base widths)
     bool device_memory_model = true;   // FFAFreqSweepCUDA's model; false: FFAFreqSweep's
+    int executor_mode = 0;             // 0 auto, 1 resident, 2 one chunk at a time
 };
 
 // One chunk: its configuration (drift-widened frequency limits, the region's
@@ -74,6 +75,7 @@ private:
     std::vector<float> m_scores;
     std::vector<uint64_t> m_region_counts;
     bool m_profiling = false;
+    int m_mode = 0;  // 0 undecided, 1 every chunk's executor resident, 2 one chunk at a time
     std::vector<lk_stage_time> m_prof;  // summed by kind during execute
     static constexpr int kSweepStreams = 2;  // chunks alternate between them
     std::vector<cudaStream_t> m_streams;

@@ -289,9 +289,32 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
         cap[i] = std::max<uint64_t>(1, c.ncoords * nw);
         off[i + 1] = off[i] + cap[i];
     }
-    if (m_idx.bytes < off[nch] * sizeof(uint32_t)) {
-        m_idx.alloc(off[nch] * sizeof(uint32_t));
-        m_snr.alloc(off[nch] * sizeof(float));
+    // Every chunk's executor stays resident (its tables reused by the next
+    // sweep, chunks overlapping on two streams) when all of them fit in free
+    // device memory with room to spare; otherwise the chunks run one at a
+    // time, each executor released after its chunk, so the device never holds
+    // more than one chunk's workspace (the planner's memory budget).
+    if (m_mode == 0 && (m_opt.executor_mode == 1 || m_opt.executor_mode == 2)) {
+        m_mode = m_opt.executor_mode;
+    }
+    if (m_mode == 0) {
+        double total_gb = 0.0;
+        for (const auto& c : m_chunks) {
+            total_gb += c.memory_gb;
+        }
+        size_t free_b = 0, total_b = 0;
+        LK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const double free_gb = static_cast<double>(free_b) / static_cast<double>(1ull << 30);
+        m_mode = (1.25 * total_gb <= 0.8 * free_gb) ? 1 : 2;
+    }
+    const bool resident = m_mode == 1;
+    uint64_t need = 0;
+    for (size_t i = 0; i < nch; ++i) {
+        need = resident ? off[i + 1] : std::max(need, cap[i]);
+    }
+    if (m_idx.bytes < std::max<uint64_t>(1, need) * sizeof(uint32_t)) {
+        m_idx.alloc(std::max<uint64_t>(1, need) * sizeof(uint32_t));
+        m_snr.alloc(std::max<uint64_t>(1, need) * sizeof(float));
     }
     if (m_cnt.bytes < std::max<size_t>(1, nch) * sizeof(uint64_t)) {
         m_cnt.alloc(std::max<size_t>(1, nch) * sizeof(uint64_t));
@@ -315,65 +338,92 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
     if (static_cast<double>(thr) < m_base.snr_min) {
         thr = std::nextafter(thr, std::numeric_limits<float>::infinity());
     }
-    // Chunks alternate between two streams: one chunk's brute fold runs
-    // beside the previous chunk's merges and scoring. The executors are built
-    // first (allocations synchronise the device).
-    for (size_t i = 0; i < nch; ++i) {
-        FFAExec& ex = exec(i);
-        require(ex.plan.nsegments[ex.plan.n_levels - 1] == 1,
-                "FFAFreqSweep::execute_ffa_region: nsegments must be 1 to call scoring function");
-    }
-    LK_CUDA(cudaEventRecord(m_ready, s));
-    for (int k = 0; k < kSweepStreams; ++k) {
-        LK_CUDA(cudaStreamWaitEvent(m_streams[k], m_ready, 0));
-    }
-    for (size_t i = 0; i < nch; ++i) {
-        m_execs[i]->search(d_ts_e, d_ts_v, thr, m_idx.as<uint32_t>() + off[i],
-                           m_snr.as<float>() + off[i], cap[i], m_cnt.as<uint64_t>() + i,
-                           m_streams[i % kSweepStreams]);
-    }
-    for (int k = 0; k < kSweepStreams; ++k) {
-        LK_CUDA(cudaEventRecord(m_done[k], m_streams[k]));
-        LK_CUDA(cudaStreamWaitEvent(s, m_done[k], 0));
-    }
     std::vector<uint64_t> counts(nch, 0);
-    if (nch > 0) {
-        LK_CUDA(cudaMemcpyAsync(counts.data(), m_cnt.ptr, nch * sizeof(uint64_t),
-                                cudaMemcpyDeviceToHost, s));
-    }
-    LK_CUDA(cudaStreamSynchronize(s));
     std::vector<std::vector<uint32_t>> h_idx(nch);
     std::vector<std::vector<float>> h_snr(nch);
-    for (size_t i = 0; i < nch; ++i) {
-        require(counts[i] <= cap[i], "FFAFreqSweep: candidate buffer overflow");
-        h_idx[i].resize(counts[i]);
-        h_snr[i].resize(counts[i]);
-        if (counts[i] > 0) {
-            LK_CUDA(cudaMemcpyAsync(h_idx[i].data(), m_idx.as<uint32_t>() + off[i],
-                                    counts[i] * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-            LK_CUDA(cudaMemcpyAsync(h_snr[i].data(), m_snr.as<float>() + off[i],
-                                    counts[i] * sizeof(float), cudaMemcpyDeviceToHost, s));
-        }
-    }
-    LK_CUDA(cudaStreamSynchronize(s));
-    for (size_t i = 0; i < nch; ++i) {
-        FFAExec& ex = *m_execs[i];
-        if (m_profiling) {
-            for (const lk_stage_time& st : ex.profile(m_streams[i % kSweepStreams])) {
-                auto it = std::find_if(m_prof.begin(), m_prof.end(),
-                                       [&](const lk_stage_time& a) { return a.kind == st.kind; });
-                if (it == m_prof.end()) {
-                    lk_stage_time a = st;
-                    a.level = -1;
-                    m_prof.push_back(a);
-                } else {
-                    it->launches += st.launches;
-                    it->ms += st.ms;
-                    it->bytes += st.bytes;
-                }
+    std::vector<Plan> plans(nch);
+    auto add_profile = [&](FFAExec& ex, cudaStream_t st_of) {
+        for (const lk_stage_time& st : ex.profile(st_of)) {
+            auto it = std::find_if(m_prof.begin(), m_prof.end(),
+                                   [&](const lk_stage_time& a) { return a.kind == st.kind; });
+            if (it == m_prof.end()) {
+                lk_stage_time a = st;
+                a.level = -1;
+                m_prof.push_back(a);
+            } else {
+                it->launches += st.launches;
+                it->ms += st.ms;
+                it->bytes += st.bytes;
             }
         }
-        const Plan& pl = ex.plan;
+    };
+    // Counts and candidates of chunks [i0, i1), region off[i] - base.
+    auto read_back = [&](size_t i0, size_t i1, uint64_t base) {
+        LK_CUDA(cudaMemcpyAsync(counts.data() + i0, m_cnt.as<uint64_t>() + i0,
+                                (i1 - i0) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        LK_CUDA(cudaStreamSynchronize(s));
+        for (size_t i = i0; i < i1; ++i) {
+            require(counts[i] <= cap[i], "FFAFreqSweep: candidate buffer overflow");
+            h_idx[i].resize(counts[i]);
+            h_snr[i].resize(counts[i]);
+            if (counts[i] > 0) {
+                LK_CUDA(cudaMemcpyAsync(h_idx[i].data(), m_idx.as<uint32_t>() + (off[i] - base),
+                                        counts[i] * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                LK_CUDA(cudaMemcpyAsync(h_snr[i].data(), m_snr.as<float>() + (off[i] - base),
+                                        counts[i] * sizeof(float), cudaMemcpyDeviceToHost, s));
+            }
+        }
+        LK_CUDA(cudaStreamSynchronize(s));
+    };
+    auto check_plan = [](const FFAExec& ex) {
+        require(ex.plan.nsegments[ex.plan.n_levels - 1] == 1,
+                "FFAFreqSweep::execute_ffa_region: nsegments must be 1 to call scoring function");
+    };
+    if (resident) {
+        // Chunks alternate between two streams: one chunk's brute fold runs
+        // beside the previous chunk's merges and scoring. The executors are
+        // built first (allocations synchronise the device).
+        for (size_t i = 0; i < nch; ++i) {
+            check_plan(exec(i));
+        }
+        LK_CUDA(cudaEventRecord(m_ready, s));
+        for (int k = 0; k < kSweepStreams; ++k) {
+            LK_CUDA(cudaStreamWaitEvent(m_streams[k], m_ready, 0));
+        }
+        for (size_t i = 0; i < nch; ++i) {
+            m_execs[i]->search(d_ts_e, d_ts_v, thr, m_idx.as<uint32_t>() + off[i],
+                               m_snr.as<float>() + off[i], cap[i], m_cnt.as<uint64_t>() + i,
+                               m_streams[i % kSweepStreams]);
+        }
+        for (int k = 0; k < kSweepStreams; ++k) {
+            LK_CUDA(cudaEventRecord(m_done[k], m_streams[k]));
+            LK_CUDA(cudaStreamWaitEvent(s, m_done[k], 0));
+        }
+        if (nch > 0) {
+            read_back(0, nch, 0);
+        }
+        for (size_t i = 0; i < nch; ++i) {
+            if (m_profiling) {
+                add_profile(*m_execs[i], m_streams[i % kSweepStreams]);
+            }
+            plans[i] = m_execs[i]->plan;
+        }
+    } else {
+        for (size_t i = 0; i < nch; ++i) {
+            FFAExec& ex = exec(i);
+            check_plan(ex);
+            ex.search(d_ts_e, d_ts_v, thr, m_idx.as<uint32_t>(), m_snr.as<float>(), cap[i],
+                      m_cnt.as<uint64_t>() + i, s);
+            read_back(i, i + 1, off[i]);
+            if (m_profiling) {
+                add_profile(ex, s);
+            }
+            plans[i] = ex.plan;
+            m_execs[i].reset();  // release this chunk's workspace
+        }
+    }
+    for (size_t i = 0; i < nch; ++i) {
+        const Plan& pl = plans[i];
         const uint32_t L = pl.n_levels - 1;
         const uint64_t total = counts[i];
         m_region_counts[i] = total;

@@ -46,6 +46,22 @@ def test_sweep_matches_reference_fixture(cuda, name, storage):
         np.testing.assert_array_equal(snr.view(np.uint32), g[f"snr_{tag}"].view(np.uint32))
 
 
+@pytest.mark.parametrize("executors", ["resident", "one_at_a_time"])
+def test_sweep_executor_modes_identical(cuda, executors):
+    """Chunk executors kept on the device (chunks on two streams) or one chunk
+    at a time (each executor released after its chunk): the reference's
+    results either way, over two sweeps in a row."""
+    from loki_b200.sweep import FFAFreqSweepCUDA
+
+    g = golden("sweep_freq_2p16.npz")
+    sw = FFAFreqSweepCUDA(_cfg(g), executors=executors)
+    for _ in range(2):
+        params, snr = sw.run(g["ts_e"], g["ts_v"])
+        np.testing.assert_array_equal(sw.region_counts, g["region_counts"])
+        np.testing.assert_array_equal(params, g["params_base_widths"])
+        np.testing.assert_array_equal(snr.view(np.uint32), g["snr_base_widths"].view(np.uint32))
+
+
 def test_sweep_execute_writes_results(cuda, tmp_path):
     from loki_b200 import libculoki
 
