@@ -236,6 +236,22 @@ def run_reference(args, rank):
 
 # ---- our path -------------------------------------------------------------------
 
+def job_throughput(units_per_rank, local_ms, dist=None, device=None):
+    """Whole-job throughput of N replicas (one process per GPU): every rank
+    processed units_per_rank in local_ms (its own device time); the job took
+    the slowest rank's time, so value = units over all ranks / max time.
+    Returns (value per second, max ms)."""
+    import torch
+
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    world = 1
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        world = dist.get_world_size()
+    ms_max = float(t.item())
+    return units_per_rank * world / (ms_max / 1e3), ms_max
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -316,11 +332,7 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     ffa.set_profiling(False)
     step_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / args.steps
-    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms_max = float(t.item())
-    value = ntrials * world / (step_ms_max / 1e3)
+    value, step_ms_max = job_throughput(ntrials, step_ms, dist, dev)
     ncand = int(cnt.item())
     rescored = ffa.rescored_cells() if args.storage == "bf16" else 0
 
