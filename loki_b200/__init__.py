@@ -1,5 +1,7 @@
-"""loki_b200: B200-native (sm_100a) FFA folding, boxcar scoring and pruning
-leaf step for pulsar searches.
+"""loki_b200: B200-native (sm_100a) FFA folding, boxcar scoring, the
+frequency sweep over octave regions, the pruning tree (leaf step, whole runs
+and their ascend / report end) and the Monte-Carlo threshold stage for pulsar
+searches.
 
 The compute path is ``libloki_b200.so`` (hand-written CUDA kernels behind the
 C ABI in ``include/loki_b200.h``); this package is its Python face, with the
