@@ -664,7 +664,8 @@ def run_multi(args, rank, world, local_rank):
     from loki_b200.batched import MultiSeriesSearch, _pow2_ceil
 
     ms = MultiSeriesSearch(tsamp=p["tsamp"], nbins=p["nbins"], f_range=p["f_range"], widths=p["widths"],
-                           snr_min=B.SNR_MIN, max_batch=16, device_id=local_rank, fold_storage=args.storage)
+                           snr_min=B.SNR_MIN, max_batch=16, device_id=local_rank, fold_storage=args.storage,
+                           autotune=not args.no_autotune)
     d_data = [(torch.from_numpy(e).cuda(), torch.from_numpy(v).cuda()) for e, v in data]
     flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     ms.search(d_data[:1])

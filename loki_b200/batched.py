@@ -83,7 +83,8 @@ class MultiSeriesSearch:
 
     def __init__(self, tsamp: float, nbins: int, f_range, widths, snr_min: float, max_batch: int = 8,
                  eta: float = 1.0, device_id: int = 0, use_graphs: bool = True, max_cands: int = 1 << 22,
-                 mem_fraction: float = 0.25, fold_storage: str = "fp32", n_slots: int = 1):
+                 mem_fraction: float = 0.25, fold_storage: str = "fp32", n_slots: int = 1,
+                 autotune: bool = False):
         self.fold_storage = fold_storage
         D.require_cuda(device_id)
         self.tsamp, self.nbins, self.eta = float(tsamp), int(nbins), float(eta)
@@ -96,6 +97,8 @@ class MultiSeriesSearch:
         self.max_cands = int(max_cands)
         self.mem_fraction = float(mem_fraction)
         self.n_slots = max(1, int(n_slots))
+        self.autotune = bool(autotune)
+        self._tuned: set[int] = set()
         self.groups: dict[int, list[_Group]] = {}
 
     def config(self, nsamps: int) -> PulsarSearchConfig:
@@ -117,6 +120,21 @@ class MultiSeriesSearch:
             self.groups[L] = [_Group(cfg, nb, self.device, self.use_graphs, self.max_cands, self.fold_storage)
                               for _ in range(self.n_slots)]
         return self.groups[L]
+
+    def _tune(self, slots: list, L: int, e, v) -> None:
+        """Launch shapes timed on the first series of a length (results are
+        unchanged), applied to every slot of that length before any capture."""
+        if not self.autotune or L in self._tuned:
+            return
+        t = D.torch()
+        e1 = t.zeros(L, dtype=t.float32, device=f"cuda:{self.device}")
+        v1 = t.zeros(L, dtype=t.float32, device=f"cuda:{self.device}")
+        e1[: e.shape[-1]].copy_(e if isinstance(e, t.Tensor) else t.from_numpy(np.ascontiguousarray(e, np.float32)))
+        v1[: v.shape[-1]].copy_(v if isinstance(v, t.Tensor) else t.from_numpy(np.ascontiguousarray(v, np.float32)))
+        tuning = slots[0].ffa.autotune(e1, v1, reps=3)
+        for g in slots:
+            g.ffa.set_tuning(tuning)
+        self._tuned.add(L)
 
     @staticmethod
     def _collect(g: _Group, out: list) -> None:
@@ -152,6 +170,7 @@ class MultiSeriesSearch:
         for L in sorted(order):
             slots = self._group(L)
             ks = order[L]
+            self._tune(slots, L, *data[ks[0]])
             nbatch = slots[0].nbatch
             for bi, b0 in enumerate(range(0, len(ks), nbatch)):
                 g = slots[bi % len(slots)]
