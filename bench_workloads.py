@@ -294,7 +294,7 @@ def run_octaves(args, rank, world, local_rank):
     from loki_b200 import _capi as C
     from loki_b200.sweep import FFAFreqSweepCUDA
 
-    sw = FFAFreqSweepCUDA(cfg, device_id=local_rank, fold_storage=args.storage)
+    sw = FFAFreqSweepCUDA(cfg, device_id=local_rank, fold_storage=args.storage, autotune=not args.no_autotune)
     e = torch.from_numpy(ts_e).cuda()
     v = torch.from_numpy(ts_v).cuda()
     flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")

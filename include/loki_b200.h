@@ -238,6 +238,10 @@ typedef struct lk_sweep_options {
      * a time, each executor released after its chunk), 1 resident, 2 one at a
      * time. Results do not depend on it. */
     int32_t executor_mode;
+    /* 1: time each chunk executor's launch shapes on the first execute's
+     * series (lk_ffa_autotune) and keep them, also for executors re-created
+     * in mode 2; results do not change. */
+    int32_t autotune;
 } lk_sweep_options;
 /* regions::generate_ffa_regions (lib/regions.cpp:31-78): rows of (f_start,
  * f_end, nbins, eta); *n_out regions, rows written up to cap. */

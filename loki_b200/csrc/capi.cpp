@@ -333,6 +333,7 @@ int lk_sweep_create(const lk_config* base, const lk_sweep_options* opt, int devi
             lk::require(opt->executor_mode >= 0 && opt->executor_mode <= 2,
                         "executor_mode must be 0 (auto), 1 (resident) or 2 (one chunk at a time)");
             o.executor_mode = opt->executor_mode;
+            o.autotune = opt->autotune != 0;
         }
         lk::require(o.max_memory_gb > 0, "max_process_memory_gb must be positive");
         auto h = std::make_unique<lk_sweep>();

@@ -27,6 +27,7 @@ struct SweepOptions {
     bool decode_chunk_widths = false;  // false: the reference's decode (base widths)
     bool device_memory_model = true;   // FFAFreqSweepCUDA's model; false: FFAFreqSweep's
     int executor_mode = 0;             // 0 auto, 1 resident, 2 one chunk at a time
+    bool autotune = false;             // tune each chunk executor's launch shapes once
 };
 
 // One chunk: its configuration (drift-widened frequency limits, the region's
@@ -64,6 +65,8 @@ public:
 
 private:
     FFAExec& exec(size_t i);
+    // exec(i), its launch shapes tuned on (or restored for) these series
+    FFAExec& tuned_exec(size_t i, const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
     lk_config m_base;
     SweepOptions m_opt;
     int m_device, m_storage;
@@ -76,6 +79,8 @@ private:
     std::vector<uint64_t> m_region_counts;
     bool m_profiling = false;
     int m_mode = 0;  // 0 undecided, 1 every chunk's executor resident, 2 one chunk at a time
+    std::vector<lk_tuning> m_tunings;  // per chunk, once tuned
+    std::vector<bool> m_tuned;
     std::vector<lk_stage_time> m_prof;  // summed by kind during execute
     static constexpr int kSweepStreams = 2;  // chunks alternate between them
     std::vector<cudaStream_t> m_streams;

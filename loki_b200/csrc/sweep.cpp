@@ -259,6 +259,26 @@ FFAExec& FreqSweepExec::exec(size_t i) {
     return *m_execs[i];
 }
 
+FFAExec& FreqSweepExec::tuned_exec(size_t i, const float* d_ts_e, const float* d_ts_v,
+                                   cudaStream_t s) {
+    const bool fresh = !m_execs[i];
+    FFAExec& ex = exec(i);
+    if (!m_opt.autotune) {
+        return ex;
+    }
+    if (m_tuned.size() != m_chunks.size()) {
+        m_tuned.assign(m_chunks.size(), false);
+        m_tunings.assign(m_chunks.size(), lk_tuning{});
+    }
+    if (!m_tuned[i]) {
+        m_tunings[i] = ex.autotune(d_ts_e, d_ts_v, 3, s);
+        m_tuned[i] = true;
+    } else if (fresh) {
+        ex.apply_tuning(m_tunings[i]);
+    }
+    return ex;
+}
+
 void FreqSweepExec::set_profiling(bool enable) {
     m_profiling = enable;
     for (auto& e : m_execs) {
@@ -384,7 +404,7 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
         // beside the previous chunk's merges and scoring. The executors are
         // built first (allocations synchronise the device).
         for (size_t i = 0; i < nch; ++i) {
-            check_plan(exec(i));
+            check_plan(tuned_exec(i, d_ts_e, d_ts_v, s));
         }
         LK_CUDA(cudaEventRecord(m_ready, s));
         for (int k = 0; k < kSweepStreams; ++k) {
@@ -410,7 +430,7 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
         }
     } else {
         for (size_t i = 0; i < nch; ++i) {
-            FFAExec& ex = exec(i);
+            FFAExec& ex = tuned_exec(i, d_ts_e, d_ts_v, s);
             check_plan(ex);
             ex.search(d_ts_e, d_ts_v, thr, m_idx.as<uint32_t>(), m_snr.as<float>(), cap[i],
                       m_cnt.as<uint64_t>() + i, s);

@@ -61,7 +61,7 @@ _EXECUTORS = {None: 0, "auto": 0, "resident": 1, "one_at_a_time": 2}
 
 
 def _options(cfg: PulsarSearchConfig, device_model: bool, decode_chunk_widths: bool,
-             executors=None) -> C.LkSweepOptions:
+             executors=None, autotune: bool = False) -> C.LkSweepOptions:
     o = C.LkSweepOptions()
     o.max_memory_gb = cfg.max_process_memory_gb
     o.octave_scale = cfg.octave_scale
@@ -72,15 +72,16 @@ def _options(cfg: PulsarSearchConfig, device_model: bool, decode_chunk_widths: b
     if executors not in _EXECUTORS:
         raise ValueError(f"executors must be one of {sorted(k for k in _EXECUTORS if k)}")
     o.executor_mode = _EXECUTORS[executors]
+    o.autotune = int(bool(autotune))
     return o
 
 
 class _SweepHandle:
     def __init__(self, cfg: PulsarSearchConfig, device_id: int, storage: int, device_model: bool,
-                 decode_chunk_widths: bool, executors=None):
+                 decode_chunk_widths: bool, executors=None, autotune: bool = False):
         _check_time_domain(cfg)
         self._cfg = cfg
-        self._opt = _options(cfg, device_model, decode_chunk_widths, executors)
+        self._opt = _options(cfg, device_model, decode_chunk_widths, executors, autotune)
         h = ctypes.c_void_p()
         C.check(C.lib().lk_sweep_create(ctypes.byref(cfg.c_config), ctypes.byref(self._opt), device_id, storage,
                                         ctypes.byref(h)))
@@ -163,18 +164,21 @@ class FFAFreqSweepCUDA(_SweepHandle):
     ``executors`` (None / "auto": every chunk's executor kept on the device when
     they all fit in free memory with room to spare, else one chunk at a time;
     "resident"; "one_at_a_time": at most one chunk's workspace on the device,
-    the planner's budget). The results do not depend on ``executors``.
+    the planner's budget) and ``autotune`` (each chunk executor's launch
+    shapes timed on the first run's series and kept). The results depend on
+    neither.
     """
 
     def __init__(self, cfg: PulsarSearchConfig, device_id: int = 0, fold_storage: str = "fp32",
-                 decode_chunk_widths: bool = False, device_memory_model: bool = True, executors=None):
+                 decode_chunk_widths: bool = False, device_memory_model: bool = True, executors=None,
+                 autotune: bool = False):
         D.require_cuda(device_id)
         if fold_storage not in _STORAGE:
             raise ValueError(f"fold_storage must be one of {sorted(_STORAGE)}")
         self._device = device_id
         with D.torch().cuda.device(device_id):
             super().__init__(cfg, device_id, _STORAGE[fold_storage], device_memory_model, decode_chunk_widths,
-                             executors)
+                             executors, autotune)
         self._param_sets = np.zeros((0, cfg.nparams + 1))
         self._snr = np.zeros(0, np.float32)
         self._region_counts = np.zeros(self.nregions, np.uint64)

@@ -46,15 +46,16 @@ def test_sweep_matches_reference_fixture(cuda, name, storage):
         np.testing.assert_array_equal(snr.view(np.uint32), g[f"snr_{tag}"].view(np.uint32))
 
 
-@pytest.mark.parametrize("executors", ["resident", "one_at_a_time"])
-def test_sweep_executor_modes_identical(cuda, executors):
+@pytest.mark.parametrize("executors,autotune", [("resident", False), ("one_at_a_time", False),
+                                                ("resident", True), ("one_at_a_time", True)])
+def test_sweep_executor_modes_identical(cuda, executors, autotune):
     """Chunk executors kept on the device (chunks on two streams) or one chunk
     at a time (each executor released after its chunk): the reference's
     results either way, over two sweeps in a row."""
     from loki_b200.sweep import FFAFreqSweepCUDA
 
     g = golden("sweep_freq_2p16.npz")
-    sw = FFAFreqSweepCUDA(_cfg(g), executors=executors)
+    sw = FFAFreqSweepCUDA(_cfg(g), executors=executors, autotune=autotune)
     for _ in range(2):
         params, snr = sw.run(g["ts_e"], g["ts_v"])
         np.testing.assert_array_equal(sw.region_counts, g["region_counts"])
