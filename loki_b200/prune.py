@@ -185,7 +185,8 @@ class EPMultiPassCUDA:
     """FFA to ``bseg_ffa`` segments, then one pruning run per reference segment
     (reference ``EPMultiPass``: same arguments; ``device_id`` added).
 
-    ``n_workers`` runs that many reference segments at once on the device, each
+    ``n_workers`` (default ``cfg.nthreads``, the reference's number of pruning
+    workspaces) runs that many reference segments at once on the device, each
     on its own executor, CUDA stream and host thread (the reference runs its
     segments on a thread pool of ``nthreads`` workspaces); a pruning level is a
     few small launches between host synchronisations, so concurrent runs fill
@@ -197,14 +198,15 @@ class EPMultiPassCUDA:
     def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
                  max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
                  show_progress: bool = False, use_conservative_tile: bool = False, device_id: int = 0,
-                 n_workers: int = 1):
+                 n_workers: int | None = None):
         _basis(poly_basis)
         self._cfg = cfg
         self._thr = np.ascontiguousarray(threshold_scheme, dtype=np.float32)
         self._n_runs = n_runs
         self._ref_segs = ref_segs
         self._ffa = FFACUDA(cfg, device_id)
-        self._workers = max(1, int(n_workers))
+        # the reference runs its segments on cfg.nthreads workspaces
+        self._workers = max(1, int(cfg.nthreads if n_workers is None else n_workers))
         self._prunes = [PruneCUDA(cfg, max_sugg, batch_size, None, use_conservative_tile, device_id,
                                   poly_basis=poly_basis) for _ in range(self._workers)]
         self._prune = self._prunes[0]
