@@ -10,7 +10,7 @@
                16 over the 31 levels (thresholds 3 -> 8), world tree 2^20,
                batches of 4096 parents. Metric: param-trials/s = leaves scored
                (sum over levels of n_leaves_phy) x boxcar widths per second.
-  octave_sweep the frequency sweep (FFAFreqSweep) over config 1's series: f
+  octave_sweep the frequency sweep (FFAFreqSweep) over the freq_sweep series: f
                5-50 Hz in octave regions of 128 / 256 / 512 / 1024 bins, each
                cut into chunks for 8 GB under the device memory model; per
                chunk FFA + scores + `>= 7` compaction + parameter decode.
@@ -252,7 +252,7 @@ def _ref_octave_runner(params, rows):
 
 
 def run_octaves(args, rank, world, local_rank):
-    """FFAFreqSweep over octave regions on config 1's series (the reference's
+    """FFAFreqSweep over octave regions on the freq_sweep series (the reference's
     production caller): f 5-50 Hz from nbins 128, regions of 128 / 256 / 512 /
     1024 bins, chunked for 8 GB under the device memory model."""
     from loki_b200.sweep import FFARegionPlannerTime

@@ -269,7 +269,7 @@ int lk_sweep_execute(lk_sweep* sw, const float* d_ts_e, const float* d_ts_v, lk_
 int lk_sweep_results(const lk_sweep* sw, double* params, float* scores, uint64_t max_out,
                      uint64_t* n_out, uint64_t* region_counts);
 
-/* Launch-shape tuning (north-star "autotuner"; no reference counterpart).
+/* Launch-shape tuning (an autotuner of this library; no reference counterpart).
  * bf_*: brute fold rows (E, V) per consumer warp (1 or 2), consumer warps
  * per block (0: the wave-count rule), shared-memory ring depth in 32-sample
  * words; merge_rows_in_flight: output rows per warp whose loads are issued
