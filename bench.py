@@ -50,6 +50,8 @@ def parse():
                     help="polynomial basis of the pruning workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the comparison of the candidates with the reference's CPU code")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--pipeline-execs", type=int, default=2,
@@ -162,6 +164,46 @@ def ncu_traffic(stage: str):
         return None
 
 
+def smem_peak_gbs(device_index, clk):
+    """Nominal shared-memory bandwidth: 128 B/clock/SM x SMs x max SM clock."""
+    import torch
+
+    props = torch.cuda.get_device_properties(device_index)
+    mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+    return 128 * props.multi_processor_count * mhz * 1e6 / 1e9
+
+
+def stage_roofline(stage_ms, stage_bytes, steps, clk, device_index, brute_adds):
+    """Roofline object of the dominant stage.
+
+    HBM-bound stages (merges, merge+score, compaction) report algorithmic HBM
+    bytes per launch / average launch time against the measured copy peak.
+    The level-0 brute fold reads little HBM data: its bound is shared memory
+    (one 4-byte read per sample x level-0 frequency x row from the staged
+    series tile, brute_adds = those reads), so it is reported as "smem"
+    against the nominal shared-memory bandwidth, with its HBM fraction kept as
+    a second field. Every merge level's HBM fraction is listed too."""
+    dom = max(stage_ms, key=stage_ms.get)
+    dom_ms = stage_ms[dom] / steps
+    peak, peak_kind = hbm_peak()
+    hbm_ach = stage_bytes[dom] / (dom_ms / 1e3) / 1e9
+    levels = {k: (stage_bytes[k] / (stage_ms[k] / steps / 1e3) / 1e9) / peak
+              for k in sorted(stage_ms) if k.startswith("merge")}
+    hbm = {"achieved": hbm_ach, "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": hbm_ach / peak,
+           "algorithmic_bytes": stage_bytes[dom]}
+    if dom.startswith("brute_fold"):
+        smem_bytes = 4 * brute_adds
+        speak = smem_peak_gbs(device_index, clk)
+        sach = smem_bytes / (dom_ms / 1e3) / 1e9
+        return {"bound": "smem", "kernel": dom, "achieved": sach, "peak": speak, "unit": "GB/s",
+                "frac": sach / speak, "peak_source": "nominal 128 B/clock/SM x SMs at the max SM clock",
+                "algorithmic_bytes": smem_bytes, "adds": brute_adds, "avg_ms": dom_ms,
+                "traffic": ncu_traffic(dom), "hbm": hbm, "merge_hbm_frac": levels}
+    return {"bound": "hbm", "kernel": dom, "achieved": hbm_ach, "peak": peak, "peak_source": peak_kind,
+            "unit": "GB/s", "frac": hbm_ach / peak, "traffic": ncu_traffic(dom),
+            "algorithmic_bytes": stage_bytes[dom], "avg_ms": dom_ms, "merge_hbm_frac": levels}
+
+
 # ---- reference CPU path -------------------------------------------------------
 
 def reference_runner(params, kind="timing"):
@@ -200,6 +242,31 @@ def cpu_baseline(params, ts_e, ts_v, budget_s=20.0):
     return {"value": ntrials / med, "unit": UNIT, "cores": nthreads, "kind": "reference",
             "sample": f"full workload, median of {len(times)} runs of FFA::execute + snr_boxcar_3d + "
                       f"compaction ({med:.3f} s each), reference CPU code built with its Release flags"}
+
+
+def candidate_parity(params, ts_e, ts_v, idx, snr):
+    """Compares a search's candidates (flat cell x width indices in increasing
+    order, S/N) with the reference's own CPU code on the same series: the IEEE
+    build of the reference (FFA<float>::execute + snr_boxcar_3d, then the
+    FFAFreqSweep compaction score >= snr_min in flat order)."""
+    from oracle import ref
+
+    if not ref.available("parity"):
+        return {"checked": False, "why": "oracle/_ref was not built"}
+    step, _, nthreads = reference_runner(params, kind="parity")
+    t0 = time.perf_counter()
+    r_idx, r_snr = step(ts_e, ts_v)
+    secs = time.perf_counter() - t0
+    idx = np.asarray(idx, dtype=np.int64)
+    snr = np.asarray(snr, dtype=np.float32)
+    same_idx = idx.shape == r_idx.shape and bool(np.array_equal(idx, r_idx))
+    same_bits = same_idx and bool(np.array_equal(snr.view(np.uint32), r_snr.astype(np.float32).view(np.uint32)))
+    max_diff = float(np.max(np.abs(snr - r_snr))) if same_idx and snr.size else None
+    return {"checked": True, "candidates_equal": same_idx, "snr_bits_equal": same_bits,
+            "candidates_match": same_idx and (max_diff is None or max_diff <= 1e-4),
+            "snr_max_abs_diff": max_diff, "n": int(idx.size), "n_ref": int(r_idx.size),
+            "vs": "oracle/_ref/libloki_ref_parity.so (the reference's CPU code, IEEE build)",
+            "ref_threads": nthreads, "ref_seconds": secs}
 
 
 def run_reference(args, rank):
@@ -269,6 +336,7 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device(f"cuda:{local_rank}"))
 
+    status = 0
     ts_e, ts_v, params, _ = workload()
     cfg = PulsarSearchConfig(params["nsamps"], params["tsamp"], params["nbins"], params["eta"],
                              np.array(params["param_limits"]), use_fourier=False,
@@ -337,27 +405,8 @@ def run_ours(args, rank, world, local_rank):
     rescored = ffa.rescored_cells() if args.storage == "bf16" else 0
 
     # roofline of the dominant stage
-    dom = max(stage_ms, key=stage_ms.get)
-    dom_ms = stage_ms[dom] / args.steps
-    achieved = stage_bytes[dom] / (dom_ms / 1e3) / 1e9
-    peak, peak_kind = hbm_peak()
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic(dom),
-                "algorithmic_bytes": stage_bytes[dom], "avg_ms": dom_ms}
-    if dom == "brute_fold_l0":
-        # The brute fold moves little HBM data; its floor is one 4-byte
-        # shared-memory read per (sample, level-0 frequency, row) from the
-        # staged series tile. Peak: 128 B/clock/SM x SMs x max SM clock.
-        nfreq0 = int(ffa.plan.param_counts[0][-1])
-        smem_bytes = 4 * 2 * params["nsamps"] * nfreq0
-        props = torch.cuda.get_device_properties(local_rank)
-        mhz = (clk or {}).get("sm_max_mhz") or 1965.0
-        smem_peak = 128 * props.multi_processor_count * mhz * 1e6 / 1e9
-        smem_ach = smem_bytes / (dom_ms / 1e3) / 1e9
-        roofline["shared_memory"] = {
-            "achieved": smem_ach, "peak": smem_peak, "unit": "GB/s", "frac": smem_ach / smem_peak,
-            "peak_source": "nominal 128 B/clock/SM at the max SM clock",
-            "algorithmic_bytes": smem_bytes, "adds": 2 * params["nsamps"] * nfreq0}
+    roofline = stage_roofline(stage_ms, stage_bytes, args.steps, clk, local_rank,
+                              2 * params["nsamps"] * int(ffa.plan.param_counts[0][-1]))
     stages = {k: {"avg_ms": stage_ms[k] / args.steps, "bytes": stage_bytes[k],
                   "gbs": stage_bytes[k] / (stage_ms[k] / args.steps / 1e3) / 1e9}
               for k in sorted(stage_ms, key=stage_ms.get, reverse=True)}
@@ -397,6 +446,10 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(params, ts_e, ts_v)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        # the last timed step's candidates against the reference's, full size
+        parity = candidate_parity(params, ts_e, ts_v, idx[:ncand].cpu().numpy(), snr[:ncand].cpu().numpy())
 
     if rank == 0:
         line = {
@@ -408,13 +461,16 @@ def run_ours(args, rank, world, local_rank):
                                            "rescore_margin": list(ffa.rescore_margin),
                                            "tuning": tuning}),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "stages": stages, "wall_s": wall,
+            "clocks": clk, "stages": stages, "wall_s": wall, "parity": parity,
         }
         emit(line)
+        if parity is not None and parity.get("checked") and not parity["candidates_match"]:
+            print("bench: the search's candidates differ from the reference's", file=sys.stderr)
+            status = 1
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
+    return status
 
 
 _JSON_OUT = None

@@ -205,15 +205,24 @@ def run_freq(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = B.cpu_baseline(params, ts_e, ts_v)
+    ncand = int(cnt.item())
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = B.candidate_parity(params, ts_e, ts_v, idx[:ncand].cpu().numpy(), snr[:ncand].cpu().numpy())
+    roof = B.stage_roofline({k: v[0] for k, v in prof.items()}, {k: v[1] for k, v in prof.items()}, 1, clk,
+                            local_rank, 2 * params["nsamps"] * int(ffa.plan.param_counts[0][-1]))
+    status = 0
     if rank == 0:
         B.emit(_line(args, world, "freq_sweep_2^21x64us_nbins128", value, ms,
-                               dict(cfgd, final_coords=int(ffa.plan.ncoords[-1]), candidates=int(cnt.item()),
+                               dict(cfgd, final_coords=int(ffa.plan.ncoords[-1]), candidates=ncand,
                                     fold_storage=args.storage, tuning=tuning),
-                               roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
-                               gpu_launches=args.steps * launches, clocks=clk,
+                               roofline=roof, cpu_baseline=cpu, e2e=e2e,
+                               gpu_launches=args.steps * launches, clocks=clk, parity=parity,
                                stages={k: {"ms": v[0], "bytes": v[1]} for k, v in prof.items()}))
+        if parity is not None and parity.get("checked") and not parity["candidates_match"]:
+            status = 1
     _finish(dist)
-    return 0
+    return status
 
 
 # ---- octave_sweep -----------------------------------------------------------------

@@ -302,7 +302,7 @@ int lk_ffa_rescored_cells(lk_ffa* ffa, lk_stream_t stream, uint64_t* n_cells);
  * (no reference counterpart; used by benchmarks). When enabled, every
  * execute/scores/search call records one event pair per kernel stage. */
 enum lk_stage_kind {
-    LK_STAGE_TRANSPOSE = 0,
+    LK_STAGE_INTERLEAVE = 0,  /* series packed into (e, v) pairs for the brute fold */
     LK_STAGE_BRUTE_FOLD = 1,
     LK_STAGE_MERGE = 2,
     LK_STAGE_MERGE_SCORE = 3,
@@ -357,6 +357,16 @@ uint64_t lk_compact_scratch_bytes(uint64_t n);
 int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
                   float* d_vals, uint64_t max_out, uint64_t* d_count, void* d_scratch,
                   lk_stream_t stream);
+/* ---- bounded device-side waits ----------------------------------------- */
+/* Check of the bounded mbarrier wait the pipelined kernels use (no reference
+ * counterpart; the reference's waits are unbounded). One warp waits up to
+ * limit_us (1000 .. 500000) on an mbarrier that one arrival completes
+ * (complete != 0) or that nothing completes (complete == 0); no asynchronous
+ * copy is in flight. Synchronises the stream and writes the status word.
+ * Returns LK_ERR_DEVICE_TIMEOUT when the wait gave up (bit 0 of *status
+ * set), LK_OK when the barrier completed; the context stays usable. */
+int lk_wait_check(uint32_t limit_us, int complete, uint32_t* status, lk_stream_t stream);
+
 /* Allocation-free variant of lk_compact_ge; it has no counterpart in the
  * reference. For callers that may not call cudaMalloc or any allocating
  * routine where they compact (a host framework that owns all device memory
@@ -367,7 +377,9 @@ int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
  * LK_ERR_INVALID_ARG); calls whose work overlaps on the GPU race on that
  * array and must be serialised. The first call on a device looks up the
  * array's device address with that device current; make that first call
- * before any stream capture. Same results as lk_compact_ge. */
+ * before any stream capture. The address is cached per device and context:
+ * the first call after the device's context was reset (cudaDeviceReset)
+ * looks it up again. Same results as lk_compact_ge. */
 int lk_compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
                           float* d_vals, uint64_t max_out, uint64_t* d_count,
                           lk_stream_t stream);

@@ -10,18 +10,29 @@ names of the reference's ``libloki`` / ``libculoki`` modules:
     from loki_b200 import libculoki
     cfg = libculoki.configs.PulsarSearchConfig(...)
     scores, plan = libculoki.ffa.compute_ffa_scores_cuda(ts_e, ts_v, cfg)
+
+Submodules are imported on first use. Every module that computes imports
+``_capi``, which loads the native library when it is imported and raises
+``ImportError`` if it is missing (there is no fallback path); the synthetic
+input generators (``loki_b200.synthetic``) need no native code and do not
+load it.
 """
 
 from __future__ import annotations
 
-from . import _capi
-from ._capi import LokiError, lib
+import importlib
 
-# Fail loudly at import time if the native library is missing.
-lib()
+_SUBMODULES = ("batched", "configs", "ffa", "fold", "pipeline", "plans", "prune", "scores", "sweep",
+               "thresholds", "libculoki", "synthetic")
 
-from . import batched, configs, ffa, fold, pipeline, plans, prune, scores, sweep, thresholds  # noqa: E402
-from . import libculoki  # noqa: E402
+__all__ = list(_SUBMODULES) + ["LokiError", "lib"]
 
-__all__ = ["configs", "plans", "ffa", "fold", "prune", "scores", "sweep", "thresholds", "batched", "libculoki",
-           "LokiError", "lib"]
+
+def __getattr__(name: str):
+    if name in _SUBMODULES:
+        return importlib.import_module(f".{name}", __name__)
+    if name in ("LokiError", "lib"):
+        from . import _capi
+
+        return getattr(_capi, name)
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")

@@ -94,7 +94,7 @@ class LkPlanInfo(ctypes.Structure):
     ]
 
 
-STAGE_NAMES = {0: "transpose", 1: "brute_fold", 2: "merge", 3: "merge_score", 4: "compact", 5: "rescore"}
+STAGE_NAMES = {0: "interleave", 1: "brute_fold", 2: "merge", 3: "merge_score", 4: "compact", 5: "rescore"}
 
 
 class LkStageTime(ctypes.Structure):
@@ -209,6 +209,7 @@ SIGNATURES = [
     ("lk_cheby_transform", i32, [vp, vp, u64, vp, u64, f64, f64, f64, f64, vp]),
     ("lk_shift_add_batch", i32, [vp, vp, vp, u64, vp, vp, vp, u32, u64, u64, u64, vp]),
     ("lk_score_filter", i32, [vp, u64, u32, vp, u32, f32, vp, vp, vp, vp]),
+    ("lk_wait_check", i32, [u32, i32, vp, vp]),
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -238,3 +239,7 @@ def check(rc: int) -> None:
         if rc == LK_ERR_OOM:
             raise MemoryError(msg)
         raise LokiError(rc, msg)
+
+
+# Fail loudly when a computing module is imported without the native library.
+lib()

@@ -8,6 +8,7 @@
 #include <new>
 #include <string>
 
+#include "lk_device.cuh"
 #include "lk_ffa.hpp"
 #include "lk_kernels.hpp"
 #include "lk_mc.hpp"
@@ -613,6 +614,26 @@ int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
         lk::compact_ge(d_scores, n, thr, d_idx, d_vals, max_out, d_count, d_scratch,
                        reinterpret_cast<cudaStream_t>(stream));
     });
+}
+
+int lk_wait_check(uint32_t limit_us, int complete, uint32_t* status, lk_stream_t stream) {
+    int rc = LK_OK;
+    const int g = guarded([&] {
+        need(status, "status");
+        lk::DeviceBuffer word(sizeof(uint32_t));
+        *status = lk::wait_check(static_cast<uint64_t>(limit_us) * 1000ull, complete != 0,
+                                 word.as<uint32_t>(), reinterpret_cast<cudaStream_t>(stream));
+        if ((*status & lk::dev::kStatusWaitTimeout) != 0) {
+            rc = LK_ERR_DEVICE_TIMEOUT;
+        }
+    });
+    if (g != LK_OK) {
+        return g;
+    }
+    if (rc != LK_OK) {
+        g_error = "a bounded device-side wait gave up (status word " + std::to_string(*status) + ")";
+    }
+    return rc;
 }
 
 int lk_compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,

@@ -2,6 +2,8 @@
 // i -- the order FFAFreqSweep produces (lib/ffa_freq_sweep.cpp:182-195).
 // Three passes, no atomics, deterministic: per-tile counts, one exclusive scan
 // of the counts, per-tile ordered scatter.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "lk_block.cuh"
@@ -119,20 +121,56 @@ static __device__ __align__(256) unsigned char g_compact_noalloc_scratch[kNoAllo
 
 namespace {
 
+// Identifier of the calling thread's current CUDA context (cuCtxGetId), 0 if
+// the driver cannot report one. A context created after cudaDeviceReset (or
+// any teardown of the primary context) has a new identifier.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static const std::pair<GetCurrent, GetId> fns = [] {
+        void* cur = nullptr;
+        void* id = nullptr;
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &cur, 12000, cudaEnableDefault, &q1) !=
+                cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess) {
+            cur = nullptr;
+        }
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &id, 12000, cudaEnableDefault, &q2) !=
+                cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess) {
+            id = nullptr;
+        }
+        return std::make_pair(reinterpret_cast<GetCurrent>(cur), reinterpret_cast<GetId>(id));
+    }();
+    CUcontext ctx = nullptr;
+    unsigned long long ident = 0;
+    if (fns.first == nullptr || fns.second == nullptr || fns.first(&ctx) != CUDA_SUCCESS ||
+        ctx == nullptr || fns.second(ctx, &ident) != CUDA_SUCCESS) {
+        return 0;
+    }
+    return ident;
+}
+
 // Device address of g_compact_noalloc_scratch for the current device. In host
 // code the symbol's name is only a host-side stand-in, so the address is
-// looked up once per device (with that device current) and cached.
+// looked up with the device current and cached per device together with the
+// identifier of the context it was looked up in; a call in a different
+// context (the device's context was reset and re-created) looks it up again.
 void* noalloc_scratch_for_current_device() {
     static std::mutex mu;
     static void* addr[64] = {};
+    static unsigned long long ctx_of[64] = {};
     int dev = -1;
     LK_CUDA(cudaGetDevice(&dev));
     require(dev >= 0 && dev < 64, "device ordinal out of range");
+    const unsigned long long ctx = current_context_id();  // 0 before the context exists
     std::lock_guard<std::mutex> lock(mu);
-    if (addr[dev] == nullptr) {
+    if (addr[dev] == nullptr || ctx == 0 || ctx != ctx_of[dev]) {
         void* p = nullptr;
-        LK_CUDA(cudaGetSymbolAddress(&p, g_compact_noalloc_scratch));
+        LK_CUDA(cudaGetSymbolAddress(&p, g_compact_noalloc_scratch));  // creates the context if needed
         addr[dev] = p;
+        ctx_of[dev] = current_context_id();
     }
     return addr[dev];
 }

@@ -161,7 +161,7 @@ const void* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t l
     const uint64_t series_bytes = 8 * plan.cfg.nsamps * nbatch;
     if (bf->interleaves()) {
         // (e, v) pairs for the packed brute fold: series in, pairs out
-        prof.begin(LK_STAGE_TRANSPOSE, 0, 1, 2 * series_bytes, s);
+        prof.begin(LK_STAGE_INTERLEAVE, 0, 1, 2 * series_bytes, s);
         bf->bind_inputs(ts_e, ts_v, s, nbatch);
         prof.end(s);
     } else {
@@ -369,7 +369,7 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
                     if (!bf->configure(rows, w, stages)) {
                         continue;
                     }
-                    const float ms = time_stages({LK_STAGE_TRANSPOSE, LK_STAGE_BRUTE_FOLD});
+                    const float ms = time_stages({LK_STAGE_INTERLEAVE, LK_STAGE_BRUTE_FOLD});
                     if (ms < bf_best) {
                         bf_best = ms;
                         br = rows;

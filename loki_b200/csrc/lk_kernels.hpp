@@ -161,6 +161,10 @@ uint64_t compact_scratch_bytes(uint64_t n);
 void compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx, float* d_vals,
                 uint64_t max_out, uint64_t* d_count, void* d_scratch, cudaStream_t s);
 // Same compaction with its scratch in a static device array (n <= 2^28).
+// Bounded-wait check: one warp waits (limit_ns) on an mbarrier that is
+// completed or never completed; returns the status word (synchronises s).
+uint32_t wait_check(uint64_t limit_ns, bool complete, uint32_t* d_status, cudaStream_t s);
+
 void compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
                         float* d_vals, uint64_t max_out, uint64_t* d_count, cudaStream_t s);
 

@@ -60,7 +60,8 @@ constexpr uint64_t kWaitLimitNs = 500000000ull;  // 0.5 s
 constexpr uint32_t kSpinLimit = 1u << 20;
 
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  uint32_t* status, uint32_t bit) {
+                                                  uint32_t* status, uint32_t bit,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) {
         return true;
     }
@@ -69,7 +70,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (mbar_try_wait(bar, parity)) {
             return true;
         }
-        if ((it & 255u) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) {
+        if ((it & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) {
             break;
         }
     }

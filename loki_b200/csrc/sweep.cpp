@@ -326,6 +326,25 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
         LK_CUDA(cudaMemGetInfo(&free_b, &total_b));
         const double free_gb = static_cast<double>(free_b) / static_cast<double>(1ull << 30);
         m_mode = (1.25 * total_gb <= 0.8 * free_gb) ? 1 : 2;
+    } else if (m_mode == 1 && m_opt.executor_mode == 0) {
+        // Chosen automatically on an earlier execute: executors that are not
+        // resident yet (an earlier execute stopped part-way) are checked
+        // against the free memory of now; once all are resident, nothing more
+        // is allocated and the mode stays.
+        double missing_gb = 0.0;
+        for (size_t i = 0; i < nch; ++i) {
+            if (i >= m_execs.size() || !m_execs[i]) {
+                missing_gb += m_chunks[i].memory_gb;
+            }
+        }
+        if (missing_gb > 0.0) {
+            size_t free_b = 0, total_b = 0;
+            LK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            const double free_gb = static_cast<double>(free_b) / static_cast<double>(1ull << 30);
+            if (1.25 * missing_gb > 0.8 * free_gb) {
+                m_mode = 2;
+            }
+        }
     }
     const bool resident = m_mode == 1;
     uint64_t need = 0;

@@ -192,8 +192,11 @@ class EPMultiPassCUDA:
     few small launches between host synchronisations, so concurrent runs fill
     the GPU that one run leaves idle. Results do not depend on it. Each worker
     takes a fixed share of the segments (its executor's buffers then stop
-    growing after the first execute). Eight segments of the jerk search:
-    one worker 29.2 ms, four 15.6 ms, eight 11.4 ms."""
+    growing after the first execute). No more workers run than there are
+    reference segments to prune, and each worker's executor (device buffers
+    sized for ``max_sugg`` leaves) is created when the worker first runs.
+    Eight segments of the jerk search: one worker 29.2 ms, four 15.6 ms,
+    eight 11.4 ms."""
 
     def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
                  max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
@@ -207,10 +210,16 @@ class EPMultiPassCUDA:
         self._ffa = FFACUDA(cfg, device_id)
         # the reference runs its segments on cfg.nthreads workspaces
         self._workers = max(1, int(cfg.nthreads if n_workers is None else n_workers))
-        self._prunes = [PruneCUDA(cfg, max_sugg, batch_size, None, use_conservative_tile, device_id,
-                                  poly_basis=poly_basis) for _ in range(self._workers)]
-        self._prune = self._prunes[0]
+        self._prune_args = (cfg, max_sugg, batch_size, None, use_conservative_tile, device_id)
+        self._poly_basis = poly_basis
+        self._prunes: list[PruneCUDA] = []
         self._device = device_id
+
+    def _executor(self, k: int) -> "PruneCUDA":
+        """Worker k's pruning executor, created on first use."""
+        while len(self._prunes) <= k:
+            self._prunes.append(PruneCUDA(*self._prune_args, poly_basis=self._poly_basis))
+        return self._prunes[k]
 
     def _run_one(self, pr: "PruneCUDA", fold, ref_seg: int, nseg: int, stream) -> dict:
         t = D.torch()
@@ -239,24 +248,27 @@ class EPMultiPassCUDA:
         nseg = int(self._ffa.plan.nsegments[-1])
         segs = determine_ref_segs(nseg, self._n_runs, self._ref_segs)
         t.cuda.synchronize(self._device)  # the fold is complete before other streams read it
-        if self._workers == 1:
+        workers = max(1, min(self._workers, len(segs)))
+        if workers == 1:
             stream = t.cuda.current_stream(self._device)
-            runs = [self._run_one(self._prune, fold, rs, nseg, stream) for rs in segs]
+            pr = self._executor(0)
+            runs = [self._run_one(pr, fold, rs, nseg, stream) for rs in segs]
         else:
             from concurrent.futures import ThreadPoolExecutor
 
-            streams = [t.cuda.Stream(device=self._device) for _ in range(self._workers)]
+            prunes = [self._executor(k) for k in range(workers)]
+            streams = [t.cuda.Stream(device=self._device) for _ in range(workers)]
             # A fixed share of the segments per worker: each executor sees the
             # same runs on every execute, so its buffers stop growing after the
             # first (a growth frees device memory, which waits for the device).
-            shares = [segs[k::self._workers] for k in range(self._workers)]
+            shares = [segs[k::workers] for k in range(workers)]
 
             def work(k):
-                return [self._run_one(self._prunes[k], fold, rs, nseg, streams[k]) for rs in shares[k]]
+                return [self._run_one(prunes[k], fold, rs, nseg, streams[k]) for rs in shares[k]]
 
-            with ThreadPoolExecutor(self._workers) as pool:
-                done = list(pool.map(work, range(self._workers)))
-            by_seg = {rs: r for k in range(self._workers) for rs, r in zip(shares[k], done[k])}
+            with ThreadPoolExecutor(workers) as pool:
+                done = list(pool.map(work, range(workers)))
+            by_seg = {rs: r for k in range(workers) for rs, r in zip(shares[k], done[k])}
             runs = [by_seg[rs] for rs in segs]
         results = dict(zip(segs, runs))
         if outdir is not None:

@@ -98,6 +98,7 @@ def lib() -> ctypes.CDLL:
         L.lko_merge_freq.argtypes = [vp, vp, vp, u64, u64, u64, u64]
         L.lko_merge_taylor.argtypes = [vp, vp, vp, u64, u64, u64, u64]
         L.lko_ffa.argtypes = [vp, vp, vp, u32, vp]
+        L.lko_ffa_scores64.argtypes = [vp, vp, vp, vp, u64, vp]
         L.lko_snr_boxcar_3d.argtypes = [vp, u64, u64, vp, u64, vp]
         L.lko_snr_boxcar_3d_max.argtypes = [vp, u64, u64, vp, u64, vp]
         L.lko_snr_boxcar_2d_max.argtypes = [vp, u64, u64, vp, u64, f32, vp]
@@ -276,6 +277,18 @@ def ffa(plan: OraclePlan, ts_e, ts_v, level: int | None = None) -> np.ndarray:
     ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
     out = np.zeros(plan.fold_size(l), dtype=np.float32)
     _check(lib().lko_ffa(ctypes.byref(plan.raw), _p(ts_e), _p(ts_v), l, _p(out)))
+    return out
+
+
+def ffa_scores64(plan: OraclePlan, ts_e, ts_v, widths) -> np.ndarray:
+    """FP64 FFA + boxcar S/N of every final cell and width, [ncoords, nwidths]
+    float64 (the FP32 path's phase map, coordinates and shifts; every sum in
+    double)."""
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    w = np.ascontiguousarray(widths, dtype=np.uint64)
+    out = np.zeros((int(plan.ncoords[-1]), w.size), dtype=np.float64)
+    _check(lib().lko_ffa_scores64(ctypes.byref(plan.raw), _p(ts_e), _p(ts_v), _p(w), w.size, _p(out)))
     return out
 
 

@@ -447,8 +447,11 @@ static uint64_t shift_bins(float phase, uint64_t nbins) {
 void lko_merge_freq(const float* in, float* out, const lko_coord_freq* coords,
                     uint64_t ncur, uint64_t nprev, uint64_t nseg, uint64_t nbins) {
     const uint64_t fs = 2 * nbins;
-    for (uint64_t s = 0; s < nseg; ++s) {
-        for (uint64_t c = 0; c < ncur; ++c) {
+    /* every output row is independent: rows are split over threads */
+#pragma omp parallel for schedule(static)
+    for (int64_t sc = 0; sc < (int64_t)(nseg * ncur); ++sc) {
+        const uint64_t s = (uint64_t)sc / ncur, c = (uint64_t)sc % ncur;
+        {
             const float* tail = in + ((2 * s) * nprev + coords[c].idx) * fs;
             const float* head = in + ((2 * s + 1) * nprev + coords[c].idx) * fs;
             float* o = out + (s * ncur + c) * fs;
@@ -469,8 +472,10 @@ void lko_merge_freq(const float* in, float* out, const lko_coord_freq* coords,
 void lko_merge_taylor(const float* in, float* out, const lko_coord* coords, uint64_t ncur,
                       uint64_t nprev, uint64_t nseg, uint64_t nbins) {
     const uint64_t fs = 2 * nbins;
-    for (uint64_t s = 0; s < nseg; ++s) {
-        for (uint64_t c = 0; c < ncur; ++c) {
+#pragma omp parallel for schedule(static)
+    for (int64_t sc = 0; sc < (int64_t)(nseg * ncur); ++sc) {
+        const uint64_t s = (uint64_t)sc / ncur, c = (uint64_t)sc % ncur;
+        {
             const float* tail = in + ((2 * s) * nprev + coords[c].i_tail) * fs;
             const float* head = in + ((2 * s + 1) * nprev + coords[c].i_head) * fs;
             float* o = out + (s * ncur + c) * fs;
@@ -660,6 +665,146 @@ uint64_t lko_compact(const float* scores, uint64_t n, float snr_min, uint32_t* i
         }
     }
     return k;
+}
+
+/* ======================================================================== */
+/* FP64 statement of the FFA + boxcar S/N (the error reference of the FP32    */
+/* and BF16-stored device paths): the same algorithm with every sum in        */
+/* double -- the FP32 path's phase map and coordinate tables (so the same    */
+/* samples land in the same bins and the same rows are merged with the same  */
+/* shifts), brute fold and merges as lko_brute_fold / lko_merge_*, scores as */
+/* snr_boxcar (lib/score.cpp:95-172) with double prefix sums and constants.  */
+/* ======================================================================== */
+
+static void merge64(const double* in, double* out, const void* coords, int taylor, uint64_t ncur,
+                    uint64_t nprev, uint64_t nseg, uint64_t nbins) {
+    const uint64_t fs = 2 * nbins;
+#pragma omp parallel for schedule(static)
+    for (int64_t sc = 0; sc < (int64_t)(nseg * ncur); ++sc) {
+        const uint64_t s = (uint64_t)sc / ncur, c = (uint64_t)sc % ncur;
+        uint64_t it, ih, st, sh;
+        if (taylor) {
+            const lko_coord* cc = (const lko_coord*)coords + c;
+            it = cc->i_tail;
+            ih = cc->i_head;
+            st = shift_bins(cc->shift_tail, nbins);
+            sh = shift_bins(cc->shift_head, nbins);
+        } else {
+            const lko_coord_freq* cc = (const lko_coord_freq*)coords + c;
+            it = ih = cc->idx;
+            st = 0;
+            sh = shift_bins(cc->shift, nbins);
+        }
+        const double* tail = in + ((2 * s) * nprev + it) * fs;
+        const double* head = in + ((2 * s + 1) * nprev + ih) * fs;
+        double* o = out + (s * ncur + c) * fs;
+        for (uint64_t r = 0; r < 2; ++r) {
+            for (uint64_t j = 0; j < nbins; ++j) {
+                o[r * nbins + j] =
+                    tail[r * nbins + (j + nbins - st) % nbins] + head[r * nbins + (j + nbins - sh) % nbins];
+            }
+        }
+    }
+}
+
+int lko_ffa_scores64(const lko_plan* p, const float* ts_e, const float* ts_v,
+                     const uint64_t* widths, uint64_t nw, double* scores) {
+    if (p->n_levels < 2 || p->nsegments[p->n_levels - 1] != 1) {
+        return fail("lko_ffa_scores64: the final level must have one segment");
+    }
+    if (nw == 0 || nw > LKO_MAX_WIDTHS) {
+        return fail("lko_ffa_scores64: number of widths out of range");
+    }
+    const uint32_t np = p->nparams;
+    const uint64_t nbins = p->nbins;
+    const uint64_t nfreq0 = p->param_counts[0][np - 1];
+    const uint64_t seglen = p->segment_lens[0];
+    const uint64_t nseg0 = p->nsegments[0];
+    double* freqs = (double*)malloc(sizeof(double) * nfreq0);
+    uint32_t* map = (uint32_t*)malloc(sizeof(uint32_t) * nfreq0 * seglen);
+    double* a = (double*)malloc(sizeof(double) * p->buffer_size);
+    double* b = (double*)malloc(sizeof(double) * p->buffer_size);
+    void* coords = malloc((np == 1 ? sizeof(lko_coord_freq) : sizeof(lko_coord)) * p->coord_size);
+    int rc = 0;
+    if (freqs == NULL || map == NULL || a == NULL || b == NULL || coords == NULL) {
+        rc = fail("out of memory");
+        goto done;
+    }
+    lko_range_param(p->limits[2 * (np - 1)], p->limits[2 * (np - 1) + 1], p->dparams[0][np - 1], freqs,
+                    nfreq0);
+    rc = (np == 1) ? lko_resolve_freq(p, (lko_coord_freq*)coords)
+                   : lko_resolve_taylor(p, (lko_coord*)coords);
+    if (rc != 0) {
+        goto done;
+    }
+    lko_phase_map(freqs, nfreq0, seglen, nbins, p->tsamp, (np == 1) ? 0.0 : p->tsegments[0] / 2.0, map);
+    memset(a, 0, sizeof(double) * nseg0 * nfreq0 * 2 * nbins);
+#pragma omp parallel for schedule(static)
+    for (int64_t sf = 0; sf < (int64_t)(nseg0 * nfreq0); ++sf) {
+        const uint64_t s = (uint64_t)sf / nfreq0, f = (uint64_t)sf % nfreq0;
+        const float* e = ts_e + s * seglen;
+        const float* v = ts_v + s * seglen;
+        double* fe = a + (s * nfreq0 + f) * 2 * nbins;
+        double* fv = fe + nbins;
+        const uint32_t* m = map + f * seglen;
+        for (uint64_t i = 0; i < seglen; ++i) {
+            fe[m[i]] += (double)e[i];
+            fv[m[i]] += (double)v[i];
+        }
+    }
+    for (uint32_t l = 1; l < p->n_levels; ++l) {
+        const void* cl = (np == 1) ? (const void*)((const lko_coord_freq*)coords + p->ncoords_offsets[l])
+                                   : (const void*)((const lko_coord*)coords + p->ncoords_offsets[l]);
+        merge64(a, b, cl, np > 1, p->ncoords[l], p->ncoords[l - 1], p->nsegments[l], nbins);
+        double* t = a;
+        a = b;
+        b = t;
+    }
+    {
+        uint64_t wmax = 0;
+        double hb[LKO_MAX_WIDTHS], bb[LKO_MAX_WIDTHS];
+        for (uint64_t k = 0; k < nw; ++k) {
+            const double w = (double)widths[k];
+            const double h = sqrt(((double)nbins - w) / ((double)nbins * w));
+            bb[k] = w * h / ((double)nbins - w);
+            hb[k] = h + bb[k];
+            wmax = widths[k] > wmax ? widths[k] : wmax;
+        }
+        const uint64_t nc = p->ncoords[p->n_levels - 1];
+#pragma omp parallel
+        {
+            double* ps = (double*)malloc(sizeof(double) * (nbins + wmax));
+#pragma omp for schedule(static)
+            for (int64_t ci = 0; ci < (int64_t)nc; ++ci) {
+                const double* e = a + (uint64_t)ci * 2 * nbins;
+                const double* v = e + nbins;
+                double acc = 0.0;
+                for (uint64_t j = 0; j < nbins; ++j) {
+                    acc += e[j] / sqrt(v[j]);
+                    ps[j] = acc;
+                }
+                for (uint64_t k = 0; k < wmax; ++k) {
+                    ps[nbins + k] = ps[k] + acc;
+                }
+                for (uint64_t k = 0; k < nw; ++k) {
+                    double dm = -DBL_MAX;
+                    for (uint64_t j = 0; j < nbins; ++j) {
+                        const double d = ps[j + widths[k]] - ps[j];
+                        dm = d > dm ? d : dm;
+                    }
+                    scores[(uint64_t)ci * nw + k] = hb[k] * dm - bb[k] * acc;
+                }
+            }
+            free(ps);
+        }
+    }
+done:
+    free(freqs);
+    free(map);
+    free(a);
+    free(b);
+    free(coords);
+    return rc;
 }
 
 /* ======================================================================== */

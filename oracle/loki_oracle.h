@@ -132,6 +132,11 @@ void lko_circular_prefix_sum(const float* x, float* out, uint64_t nbins, uint64_
 
 /* Threshold compaction `score >= snr_min` in flat order
  * (lib/ffa_freq_sweep.cpp:182-195). Returns the number kept. */
+/* FP64 FFA + boxcar S/N of every final cell and width, [ncoords, nw]
+ * doubles (same phase map, coordinates and shifts as the FP32 path). */
+int lko_ffa_scores64(const lko_plan* plan, const float* ts_e, const float* ts_v,
+                     const uint64_t* widths, uint64_t nw, double* scores);
+
 uint64_t lko_compact(const float* scores, uint64_t n, float snr_min, uint32_t* idx_out,
                      float* score_out);
 

@@ -169,7 +169,7 @@ def _error_statement(nsamps: int):
     op = lko.plan_create(lko.make_cfg(nsamps, tsamp, nbins, eta, lims))
     plain = FFACUDA(cfg, fold_storage="fp32")
     mixed = FFACUDA(cfg, fold_storage="bf16")
-    s64 = fp64.ffa_scores64(op, ts_e, ts_v, widths).ravel()
+    s64 = lko.ffa_scores64(op, ts_e, ts_v, np.array(widths, np.uint64)).ravel()
     s32 = plain.scores(ts_e, ts_v).astype(np.float64)
     s16 = mixed.scores(ts_e, ts_v).astype(np.float64)
     thr = 7.0
@@ -197,7 +197,5 @@ def test_error_statement_accel_2p20(cuda):
     _error_statement(1 << 20)
 
 
-@pytest.mark.skipif(not __import__("os").environ.get("LOKI_B200_FULL_ERRSTAT"),
-                    reason="full-size FP64 statement (2^22 samples, minutes of numpy): set LOKI_B200_FULL_ERRSTAT=1")
 def test_error_statement_accel_2p22(cuda):
     _error_statement(1 << 22)
