@@ -189,6 +189,16 @@ void compact_ge_noalloc(const float* d_scores, uint64_t n, float thr, uint32_t* 
                noalloc_scratch_for_current_device(), s);
 }
 
+void scan_counts(const uint32_t* d_counts, uint64_t n, uint64_t* d_offsets, uint64_t* d_total,
+                 cudaStream_t s) {
+    if (n == 0) {
+        LK_CUDA(cudaMemsetAsync(d_total, 0, sizeof(uint64_t), s));
+        return;
+    }
+    tile_scan_kernel<<<1, kThreads, 0, s>>>(d_counts, n, d_offsets, d_total);
+    LK_CUDA(cudaGetLastError());
+}
+
 uint64_t compact_scratch_bytes(uint64_t n) {
     const uint64_t ntiles = (n + kTile - 1) / kTile;
     return ntiles * (sizeof(uint32_t) + sizeof(uint64_t)) + 16;

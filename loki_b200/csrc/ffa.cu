@@ -118,12 +118,20 @@ FFAExec::FFAExec(const Plan& p, int device, int storage, uint64_t max_batch_)
     }
     sp = make_score_params(plan.widths.data(), static_cast<uint32_t>(plan.widths.size()),
                            static_cast<uint32_t>(plan.cfg.nbins));
+    if (plan.nsegments[plan.n_levels - 1] == 1 &&
+        make_mask_score_params(sp, static_cast<uint32_t>(plan.cfg.nbins), &mp)) {
+        wm = true;
+        normtab.alloc(sizeof(float) * kNormTableSize);
+        norm_table_fill(normtab.as<float>(), nullptr);
+        LK_CUDA(cudaDeviceSynchronize());
+    }
 }
 
 uint64_t FFAExec::device_bytes() const {
     return status.bytes + coords.bytes + buf[0].bytes + buf[1].bytes + fold0.bytes +
            bf->device_bytes() + scores_tmp.bytes + compact_scratch.bytes + cmax.bytes +
-           cells.bytes + cell_vals.bytes + cell_count.bytes + cell_scratch.bytes;
+           cells.bytes + cell_vals.bytes + cell_count.bytes + cell_scratch.bytes + normtab.bytes +
+           blk_counts.bytes + blk_offsets.bytes;
 }
 
 float FFAExec::rescore_threshold(float snr_min) const {
@@ -209,7 +217,7 @@ void FFAExec::scores(const float* ts_e, const float* ts_v, float* d_scores, uint
 }
 
 void FFAExec::scores_impl(const float* ts_e, const float* ts_v, float* d_scores, float* d_cmax,
-                          cudaStream_t s, uint64_t nbatch) {
+                          cudaStream_t s, uint64_t nbatch, float count_thr, uint32_t* d_counts) {
     const uint32_t L = plan.n_levels;
     bool in_bf16 = false;
     const void* in = run_levels(ts_e, ts_v, L - 2, nullptr, s, nbatch, &in_bf16);
@@ -219,10 +227,19 @@ void FFAExec::scores_impl(const float* ts_e, const float* ts_v, float* d_scores,
                    coord_bytes(L - 1),
                s);
     const uint64_t n_inner = plan.param_counts[L - 1][plan.nparams - 1];
-    merge_score_level(in, level_coords(L - 1), plan.nparams > 1, n_inner,
-                      plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
-                      static_cast<uint32_t>(plan.cfg.nbins), sp, LK_SCORE_PER_WIDTH, d_scores, s,
-                      nbatch, in_bf16, d_cmax, score_cells);
+    if (use_wm()) {
+        merge_score_level_wm(in, level_coords(L - 1), plan.nparams > 1, n_inner,
+                             plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
+                             static_cast<uint32_t>(plan.cfg.nbins), mp, LK_SCORE_PER_WIDTH,
+                             d_scores, s, nbatch, in_bf16, d_cmax, normtab.as<float>(), count_thr,
+                             d_counts);
+    } else {
+        require(d_counts == nullptr, "internal: block counts need the masked final level");
+        merge_score_level(in, level_coords(L - 1), plan.nparams > 1, n_inner,
+                          plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
+                          static_cast<uint32_t>(plan.cfg.nbins), sp, LK_SCORE_PER_WIDTH, d_scores,
+                          s, nbatch, in_bf16, d_cmax, score_cells);
+    }
     prof.end(s);
 }
 
@@ -247,6 +264,25 @@ void FFAExec::search(const float* ts_e, const float* ts_v, float snr_min, uint32
         cell_scratch.alloc(compact_scratch_bytes(ncells));
     }
     prof.reset();
+    if (!mixed && use_wm()) {
+        // The final level counts each block's candidates; the list is the
+        // scan of the counts and a scatter of the blocks that have any.
+        const uint64_t n_inner = plan.param_counts[L - 1][plan.nparams - 1];
+        const uint64_t n_outer = plan.ncoords[L - 1] / n_inner;
+        const uint64_t nblk = final_level_blocks(n_inner, n_outer, nbatch);
+        if (blk_counts.bytes < nblk * sizeof(uint32_t)) {
+            blk_counts.alloc(nblk * sizeof(uint32_t));
+            blk_offsets.alloc(nblk * sizeof(uint64_t));
+        }
+        scores_impl(ts_e, ts_v, scores_tmp.as<float>(), nullptr, s, nbatch, snr_min,
+                    blk_counts.as<uint32_t>());
+        prof.begin(LK_STAGE_COMPACT, -1, 2, 12 * nblk, s);
+        compact_ranges(scores_tmp.as<float>(), blk_counts.as<uint32_t>(), blk_offsets.as<uint64_t>(),
+                       n_inner, n_outer, nbatch, static_cast<uint32_t>(plan.widths.size()), snr_min,
+                       d_idx, d_snr, max_cands, d_count, s);
+        prof.end(s);
+        return;
+    }
     scores_impl(ts_e, ts_v, scores_tmp.as<float>(), mixed ? cmax.as<float>() : nullptr, s, nbatch);
     if (mixed) {
         // Cells whose approximate best S/N is near or above snr_min get their
@@ -410,6 +446,10 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         const uint32_t tmax = sc::profiles_per_block(rs);
         float score_best = INFINITY;
         uint32_t bcells = 0;
+        if (wm) {
+            score_cells = 0;  // masked final level (final_level.cu)
+            score_best = time_stages({LK_STAGE_MERGE_SCORE});
+        }
         for (uint32_t cells = 32; cells <= tmax; cells += 32) {
             score_cells = cells;
             const float ms = time_stages({LK_STAGE_MERGE_SCORE});

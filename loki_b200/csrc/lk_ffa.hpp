@@ -63,6 +63,15 @@ struct FFAExec {
     // BF16 search: per-cell best approximate S/N, the cells to rescore.
     DeviceBuffer cmax, cells, cell_vals, cell_count, cell_scratch;
     ScoreParams sp{};
+    // Final level for 32 / 64 / 128 bins and strictly increasing widths <= 32
+    // (final_level.cu): width mask, 1 / sqrt(n) table, per-block candidate
+    // counts and their offsets (FP32 search).
+    bool wm = false;
+    MaskScoreParams mp{};
+    DeviceBuffer normtab, blk_counts, blk_offsets;
+    // The masked final level runs unless a tuning picked the generic kernel
+    // (score_cells != 0).
+    bool use_wm() const { return wm && score_cells == 0; }
     bool mixed = false;  // BF16 storage of levels 1 .. L-2
     // A BF16 search rescores every final cell whose approximate best S/N is
     // at least (snr_min - margin_abs) / (1 + margin_rel).
@@ -97,8 +106,11 @@ struct FFAExec {
     // holding `last` (BF16 when *last_bf16 is set).
     const void* run_levels(const float* ts_e, const float* ts_v, uint32_t last, float* final_out,
                            cudaStream_t s, uint64_t nbatch, bool* last_bf16);
+    // With d_counts (masked final level only), per-block counts of scores >=
+    // count_thr are written too.
     void scores_impl(const float* ts_e, const float* ts_v, float* d_scores, float* d_cmax,
-                     cudaStream_t s, uint64_t nbatch);
+                     cudaStream_t s, uint64_t nbatch, float count_thr = 0.0f,
+                     uint32_t* d_counts = nullptr);
     void execute(const float* ts_e, const float* ts_v, float* fold, uint64_t fold_len,
                  cudaStream_t s, uint64_t nbatch = 1);
     void scores(const float* ts_e, const float* ts_v, float* d_scores, uint64_t len,

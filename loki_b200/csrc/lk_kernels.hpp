@@ -120,6 +120,46 @@ struct ScoreParams {
 };
 ScoreParams make_score_params(const uint32_t* widths, uint32_t nwidths, uint32_t nbins);
 
+// ---- final level for 32 / 64 / 128 bins (final_level.cu) -----------------
+// 1 / sqrt(n) table for exact integer variance sums n < kNormTableSize
+// (rcp_rn(sqrt_rn(n)), the direct computation's bits).
+constexpr uint32_t kNormTableSize = 1u << 19;
+void norm_table_fill(float* d_tab, cudaStream_t s);
+// Scoring widths as a bit mask (bit w for width w <= 32) with the per-width
+// constants and output slots, for strictly increasing widths.
+struct MaskScoreParams {
+    uint64_t wmask;
+    uint32_t nwidths;
+    uint32_t wmax;
+    float hb[33];
+    float b[33];
+    uint8_t slot[33];
+};
+// False when the masked path does not apply (nbins not 32 / 64 / 128, widths
+// not strictly increasing or wider than 32 bins).
+bool make_mask_score_params(const ScoreParams& sp, uint32_t nbins, MaskScoreParams* mp);
+uint32_t final_level_cells_per_block();
+// Blocks (count slots) of one final-level launch.
+uint64_t final_level_blocks(uint64_t n_inner, uint64_t n_outer, uint64_t nbatch);
+// Final merge level fused with scoring (same results as merge_score_level).
+// With d_counts, each block also writes its number of scores >= count_thr
+// (per-width mode) to d_counts[final_level_blocks order].
+void merge_score_level_wm(const void* d_in, const void* d_coords, bool taylor, uint64_t n_inner,
+                          uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
+                          const MaskScoreParams& mp, int mode, float* d_scores, cudaStream_t s,
+                          uint64_t nbatch, bool in_bf16, float* d_cmax, const float* d_tab,
+                          float count_thr, uint32_t* d_counts);
+// Ordered compaction of scores >= thr from the block counts of
+// merge_score_level_wm: exclusive scan of the counts (d_offsets: one uint64
+// per block), then a scatter of the blocks that have candidates.
+void compact_ranges(const float* d_scores, const uint32_t* d_counts, uint64_t* d_offsets,
+                    uint64_t n_inner, uint64_t n_outer, uint64_t nbatch, uint32_t nw, float thr,
+                    uint32_t* d_idx, float* d_vals, uint64_t max_out, uint64_t* d_count,
+                    cudaStream_t s);
+// Exclusive scan of n uint32 counts into uint64 offsets (one block); *d_total = sum.
+void scan_counts(const uint32_t* d_counts, uint64_t n, uint64_t* d_offsets, uint64_t* d_total,
+                 cudaStream_t s);
+
 // Final merge level fused with scoring (one output segment per series;
 // nbatch series, the input holding 2 * nbatch segments of ncoords_prev cells,
 // scores [nbatch][ncoords][nout]).
