@@ -724,6 +724,132 @@ def run_multi(args, rank, world, local_rank):
     return 0
 
 
+# ---- beam_scheme -------------------------------------------------------------------
+
+DTS_NSTAGES = 16
+
+
+def _dts_params():
+    """The reference's DynamicThresholdScheme defaults (nbins 64, 1024 trials,
+    100 thresholds, 10 probability bins, snr_final 8, beam width 0.7, ducy_max
+    0.3, wtsp 1) over 16 stages of a branching pattern rising from 1.5 to 4,
+    profile duty 0.1, ten neighbouring thresholds per transition."""
+    bp = np.linspace(1.5, 4.0, DTS_NSTAGES).astype(np.float32)
+    return bp, dict(ref_ducy=0.1), 10
+
+
+def _dts_transitions(states, bp, neigh, nthr=100, nprobs=10, ntrials=1024, snr_final=8.0, beam_width=0.7,
+                     stages=None):
+    """Transitions a run simulated, from its states: a transition runs when
+    its previous state is non-empty and kept H0 and H1 survivors (recovered
+    exactly from the success fractions)."""
+    from oracle import lko
+
+    ns = bp.size
+    st = states.reshape(ns, nthr, nprobs)
+    thr = lko.dts_thresholds(0.1, snr_final, nthr)
+    guess = lko.dts_guess(ns, snr_final, bp)
+
+    def beam(s):
+        lo = max(np.float32(0.0), np.float32(guess[s] - np.float32(beam_width)))
+        hi = min(thr[-1], np.float32(guess[s] + np.float32(beam_width)))
+        return [i for i in range(nthr) if lo <= thr[i] <= hi]
+
+    total = len(beam(0))
+    prev = beam(0)
+    for s in range(1, ns if stages is None else stages):
+        cur = beam(s)
+        p = st[s - 1]
+        ok = (~p["is_empty"]) & (np.rint(p["success_h0"] * ntrials) > 0) & (np.rint(p["success_h1"] * ntrials) > 0)
+        for i in cur:
+            for j in lko.dts_neighbours(prev, i, neigh):
+                total += int(ok[j].sum())
+        prev = cur
+    return total
+
+
+def run_dts(args, rank, world, local_rank):
+    """Metric: trial folds built and scored per second (each simulated
+    transition builds and scores 1024 H0 and 1024 H1 folds of 64 bins)."""
+    bp, kw, neigh = _dts_params()
+    unit = "trial-folds/s"
+    metric = "trial-folds/s (beam-search simulate+score+survive)"
+    cfgd = {"nstages": int(bp.size), "branching": "linear 1.5 -> 4", "ref_ducy": 0.1, "nbins": 64,
+            "ntrials": 1024, "nthresholds": 100, "nprobs": 10, "thres_neigh": neigh}
+
+    def cpu_sample(nst=4, kind="timing"):
+        """The reference's stage loop restated over its own pieces
+        (oracle/_ref; thresholds.cpp itself needs HDF5), else the C oracle, on
+        the first nst stages; returns (transitions/s x 2 x 1024, seconds, kind)."""
+        from oracle import lko, ref
+
+        t0 = time.perf_counter()
+        if ref.available(kind):
+            st = ref.dts_run(bp, kw["ref_ducy"], lko.dts_guess(bp.size, 8.0, bp), lko.dts_normal_lut(),
+                             lko.DTS_STATE_DTYPE, thres_neigh=neigh, stages_run=nst, kind=kind)
+            how = "reference pieces (oracle/_ref)"
+        else:
+            st = lko.dts_run(bp, **kw, thres_neigh=neigh, stages_run=nst)
+            how = "C oracle"
+        el = time.perf_counter() - t0
+        return _dts_transitions(st, bp, neigh, stages=nst) * 2 * 1024 / el, el, how
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        v, el, how = cpu_sample()
+        B.emit({"impl": "reference", "metric": metric, "value": v, "unit": unit, "n_gpus": world,
+                "steps": 1, "warmup": 0, "ms_per_step": 1e3 * el, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(cfgd, workload="beam_scheme_16stages_nbins64_1024trials"),
+                "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "port",
+                                 "sample": f"first 4 stages, {how}, single thread, {el:.1f} s"},
+                "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return 0
+    torch, dist = _init(local_rank, world)
+    from loki_b200.thresholds import DynamicThresholdSchemeCUDA
+
+    dts = DynamicThresholdSchemeCUDA(bp, **kw)
+    flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        dts.run(thres_neigh=neigh)
+        return dts.transitions()
+
+    clocks = B.ClockSampler(local_rank)
+    clocks.start()
+    ms, outs = _timed(torch, step, args.steps, args.warmup, flush, dist)
+    clk = clocks.stop()
+    trials = outs[-1] * 2 * 1024
+    value = trials * world / (ms / 1e3)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, el, how = cpu_sample()
+        cpu = {"value": v, "unit": unit, "cores": 1, "kind": "port",
+               "sample": f"the first 4 stages through the reference's stage loop restated over its own pieces "
+                         f"({how}; thresholds.cpp itself needs HDF5), single thread, {el:.1f} s"}
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            dts.run(thres_neigh=neigh)
+            states = dts.get_states()
+            dts.get_best_path_thresholds(0.1)
+        el = time.perf_counter() - t0
+        e2e = {"value": trials * world * args.steps / el, "unit": unit, "h2d_bytes_per_step": 0,
+               "d2h_bytes_per_step": int(states.nbytes),
+               "api": "DynamicThresholdSchemeCUDA.run + get_states + get_best_path_thresholds"}
+    if rank == 0:
+        line = _line(args, world, "beam_scheme_16stages_nbins64_1024trials", value, ms,
+                     dict(cfgd, transitions=int(outs[-1])), cpu_baseline=cpu, e2e=e2e, clocks=clk,
+                     gpu_launches=1 + 4 * int(bp.size))
+        line["metric"], line["unit"] = metric, unit
+        B.emit(line)
+    _finish(dist)
+    return 0
+
+
 def run(args, rank, world, local_rank):
     return {"freq_sweep": run_freq, "prune_jerk": run_prune, "mc_cascade": run_mc,
-            "multi_series": run_multi, "octave_sweep": run_octaves}[args.workload](args, rank, world, local_rank)
+            "multi_series": run_multi, "octave_sweep": run_octaves,
+            "beam_scheme": run_dts}[args.workload](args, rank, world, local_rank)

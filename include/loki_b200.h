@@ -557,6 +557,78 @@ int lk_mc_stage(lk_mc* mc, const float* d_folds_in, uint64_t ntrials_in, const u
  * since the last call (and clears it). */
 int lk_mc_status(lk_mc* mc, lk_stream_t stream, uint32_t* status);
 
+/* ---- DynamicThresholdScheme beam search ---------------------------------- */
+/* Replaces detection::DynamicThresholdScheme / DynamicThresholdSchemeCUDA
+ * (include/loki/detection/thresholds.hpp:65-164, lib/thresholds.cpp:560-907,
+ * lib/thresholds_cuda.cu): for every stage and every threshold of the
+ * stage's beam, every neighbouring previous state is advanced by simulating
+ * ntrials H0 and H1 folds, scoring them and keeping the survivors; each
+ * (threshold, probability bin) cell keeps the first transition with the
+ * smallest cumulative complexity. Noise comes from a counter-based generator
+ * (Philox4x32-10 words through the reference's normal quantile table), so a
+ * run is reproducible from `seed`. */
+typedef struct lk_dts lk_dts;
+/* detection::State (include/loki/detection/thresholds.hpp:17-29), same fields
+ * and order; is_empty is 1 for a cell no transition reached. */
+typedef struct lk_dts_state {
+    float success_h0;
+    float success_h1;
+    float complexity;
+    float complexity_cumul;
+    float success_h1_cumul;
+    float nbranches;
+    float threshold;
+    float cost;
+    float threshold_prev;
+    float success_h1_cumul_prev;
+    uint8_t is_empty;
+    uint8_t pad[3];
+} lk_dts_state;
+/* The reference constructor's arguments (defaults there: nbins 64, ntrials
+ * 1024, nprobs 10, prob_min 0.05, snr_final 8, nthresholds 100, ducy_max 0.3,
+ * wtsp 1, beam_width 0.7, trials_start 1) plus the generator seed. */
+typedef struct lk_dts_config {
+    const float* branching_pattern; /* host, nstages entries */
+    uint32_t nstages;
+    float ref_ducy;
+    uint32_t nbins;
+    uint32_t ntrials;
+    uint32_t nprobs;
+    float prob_min;
+    float snr_final;
+    uint32_t nthresholds;
+    float ducy_max;
+    float wtsp;
+    float beam_width;
+    uint32_t trials_start;
+    uint64_t seed;
+} lk_dts_config;
+int lk_dts_create(const lk_dts_config* cfg, int device, lk_dts** out);
+void lk_dts_destroy(lk_dts* dts);
+/* DynamicThresholdScheme::run(thres_neigh): the whole scheme on `stream`;
+ * synchronises it and keeps the states on the host. */
+int lk_dts_run(lk_dts* dts, uint32_t thres_neigh, lk_stream_t stream);
+int lk_dts_info(const lk_dts* dts, uint32_t* nstages, uint32_t* nthresholds, uint32_t* nprobs,
+                uint32_t* nbins, uint32_t* nwidths);
+/* Host arrays (NULL skips one): profile [nbins], thresholds [nthresholds],
+ * probs [nprobs], guess path [nstages], box widths [nwidths]. */
+int lk_dts_arrays(const lk_dts* dts, float* profile, float* thresholds, float* probs,
+                  float* guess_path, uint32_t* widths);
+/* Transitions the last lk_dts_run simulated (each: ntrials H0 and ntrials
+ * H1 folds built and scored). */
+int lk_dts_transitions(const lk_dts* dts, uint64_t* n);
+/* get_states: [nstages][nthresholds][nprobs] after lk_dts_run; n = capacity. */
+int lk_dts_states(const lk_dts* dts, lk_dts_state* out, uint64_t n);
+/* get_best_path_thresholds(min_pd): *n thresholds (0 when no final state
+ * reaches min_pd); out holds nstages entries. */
+int lk_dts_best_path(const lk_dts* dts, float min_pd, float* out, uint32_t* n);
+/* Host-only set-up (no device): the arrays lk_dts_arrays reports for cfg
+ * (each output may be NULL; widths holds up to 32 entries, *nwidths set). */
+int lk_dts_plan(const lk_dts_config* cfg, float* profile, float* thresholds, float* probs,
+                float* guess_path, uint32_t* widths, uint32_t* nwidths);
+/* The normal quantile table of the generator (n >= 131073 entries). */
+int lk_dts_normal_lut(float* out, uint64_t n);
+
 #ifdef __cplusplus
 }
 #endif

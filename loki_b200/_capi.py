@@ -210,6 +210,16 @@ SIGNATURES = [
     ("lk_shift_add_batch", i32, [vp, vp, vp, u64, vp, vp, vp, u32, u64, u64, u64, vp]),
     ("lk_score_filter", i32, [vp, u64, u32, vp, u32, f32, vp, vp, vp, vp]),
     ("lk_wait_check", i32, [u32, i32, vp, vp]),
+    ("lk_dts_create", i32, [vp, i32, vp]),
+    ("lk_dts_destroy", None, [vp]),
+    ("lk_dts_run", i32, [vp, u32, vp]),
+    ("lk_dts_info", i32, [vp, vp, vp, vp, vp, vp]),
+    ("lk_dts_arrays", i32, [vp, vp, vp, vp, vp, vp]),
+    ("lk_dts_states", i32, [vp, vp, u64]),
+    ("lk_dts_best_path", i32, [vp, f32, vp, vp]),
+    ("lk_dts_normal_lut", i32, [vp, u64]),
+    ("lk_dts_plan", i32, [vp, vp, vp, vp, vp, vp, vp]),
+    ("lk_dts_transitions", i32, [vp, vp]),
 ]
 
 _lib: ctypes.CDLL | None = None

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "lk_device.cuh"
+#include "lk_dts.hpp"
 #include "lk_ffa.hpp"
 #include "lk_kernels.hpp"
 #include "lk_mc.hpp"
@@ -29,6 +30,9 @@ struct lk_prune {
 };
 struct lk_sweep {
     std::unique_ptr<lk::FreqSweepExec> exec;
+};
+struct lk_dts {
+    std::unique_ptr<lk::DtsExec> exec;
 };
 struct lk_brute_fold {
     int device = 0;
@@ -613,6 +617,125 @@ int lk_compact_ge(const float* d_scores, uint64_t n, float thr, uint32_t* d_idx,
         }
         lk::compact_ge(d_scores, n, thr, d_idx, d_vals, max_out, d_count, d_scratch,
                        reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_dts_create(const lk_dts_config* cfg, int device, lk_dts** out) {
+    return guarded([&] {
+        need(cfg, "cfg");
+        need(out, "out");
+        auto d = std::make_unique<lk_dts>();
+        d->exec = std::make_unique<lk::DtsExec>(*cfg, device);
+        *out = d.release();
+    });
+}
+
+void lk_dts_destroy(lk_dts* dts) { delete dts; }
+
+int lk_dts_run(lk_dts* dts, uint32_t thres_neigh, lk_stream_t stream) {
+    return guarded([&] {
+        need(dts, "dts");
+        dts->exec->run(thres_neigh, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_dts_info(const lk_dts* dts, uint32_t* nstages, uint32_t* nthresholds, uint32_t* nprobs,
+                uint32_t* nbins, uint32_t* nwidths) {
+    return guarded([&] {
+        need(dts, "dts");
+        const lk::DtsExec& e = *dts->exec;
+        if (nstages) *nstages = e.nstages();
+        if (nthresholds) *nthresholds = e.nthresholds();
+        if (nprobs) *nprobs = e.nprobs();
+        if (nbins) *nbins = e.nbins();
+        if (nwidths) *nwidths = static_cast<uint32_t>(e.m_widths.size());
+    });
+}
+
+int lk_dts_arrays(const lk_dts* dts, float* profile, float* thresholds, float* probs,
+                  float* guess_path, uint32_t* widths) {
+    return guarded([&] {
+        need(dts, "dts");
+        const lk::DtsExec& e = *dts->exec;
+        if (profile) std::copy(e.m_profile.begin(), e.m_profile.end(), profile);
+        if (thresholds) std::copy(e.m_thresholds.begin(), e.m_thresholds.end(), thresholds);
+        if (probs) std::copy(e.m_probs.begin(), e.m_probs.end(), probs);
+        if (guess_path) std::copy(e.m_guess.begin(), e.m_guess.end(), guess_path);
+        if (widths) std::copy(e.m_widths.begin(), e.m_widths.end(), widths);
+    });
+}
+
+int lk_dts_transitions(const lk_dts* dts, uint64_t* n) {
+    return guarded([&] {
+        need(dts, "dts");
+        need(n, "n");
+        *n = dts->exec->m_transitions;
+    });
+}
+
+int lk_dts_states(const lk_dts* dts, lk_dts_state* out, uint64_t n) {
+    return guarded([&] {
+        need(dts, "dts");
+        need(out, "out");
+        const auto& st = dts->exec->m_states;
+        lk::require(!st.empty(), "run the scheme before reading its states");
+        lk::require(n >= st.size(), "out must hold nstages * nthresholds * nprobs states");
+        std::copy(st.begin(), st.end(), out);
+    });
+}
+
+int lk_dts_best_path(const lk_dts* dts, float min_pd, float* out, uint32_t* n) {
+    return guarded([&] {
+        need(dts, "dts");
+        need(out, "out");
+        need(n, "n");
+        const std::vector<float> p = dts->exec->best_path(min_pd);
+        std::copy(p.begin(), p.end(), out);
+        *n = static_cast<uint32_t>(p.size());
+    });
+}
+
+int lk_dts_plan(const lk_dts_config* cfg, float* profile, float* thresholds, float* probs,
+                float* guess_path, uint32_t* widths, uint32_t* nwidths) {
+    return guarded([&] {
+        need(cfg, "cfg");
+        need(cfg->branching_pattern, "branching_pattern");
+        lk::require(cfg->nstages >= 1 && cfg->nthresholds >= 2 && cfg->nprobs >= 2 && cfg->nbins >= 4,
+                    "invalid scheme configuration");
+        const std::vector<float> bp(cfg->branching_pattern, cfg->branching_pattern + cfg->nstages);
+        if (profile) {
+            const auto v = lk::dts_profile(cfg->nbins, cfg->ref_ducy, 0.5F);
+            std::copy(v.begin(), v.end(), profile);
+        }
+        if (thresholds) {
+            const auto v = lk::dts_thresholds(0.1F, cfg->snr_final, cfg->nthresholds);
+            std::copy(v.begin(), v.end(), thresholds);
+        }
+        if (probs) {
+            const auto v = lk::dts_probs(cfg->nprobs, cfg->prob_min);
+            std::copy(v.begin(), v.end(), probs);
+        }
+        if (guess_path) {
+            const auto v = lk::dts_guess_scheme(cfg->nstages, cfg->snr_final, bp, cfg->trials_start, 1E10F);
+            std::copy(v.begin(), v.end(), guess_path);
+        }
+        const auto w = lk::box_width_trials(cfg->nbins, cfg->ducy_max, cfg->wtsp);
+        if (widths) {
+            lk::require(w.size() <= LK_MAX_WIDTHS, "too many widths");
+            std::copy(w.begin(), w.end(), widths);
+        }
+        if (nwidths) {
+            *nwidths = static_cast<uint32_t>(w.size());
+        }
+    });
+}
+
+int lk_dts_normal_lut(float* out, uint64_t n) {
+    return guarded([&] {
+        need(out, "out");
+        lk::require(n >= lk::kDtsLutSize, "out must hold 131073 floats");
+        const std::vector<float> lut = lk::normal_lut();
+        std::copy(lut.begin(), lut.end(), out);
     });
 }
 

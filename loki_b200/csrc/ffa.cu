@@ -232,7 +232,7 @@ void FFAExec::scores_impl(const float* ts_e, const float* ts_v, float* d_scores,
                              plan.ncoords[L - 1] / n_inner, plan.ncoords[L - 2],
                              static_cast<uint32_t>(plan.cfg.nbins), mp, LK_SCORE_PER_WIDTH,
                              d_scores, s, nbatch, in_bf16, d_cmax, normtab.as<float>(), count_thr,
-                             d_counts);
+                             d_counts, score_cells == 0);
     } else {
         require(d_counts == nullptr, "internal: block counts need the masked final level");
         merge_score_level(in, level_coords(L - 1), plan.nparams > 1, n_inner,
@@ -447,8 +447,15 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         float score_best = INFINITY;
         uint32_t bcells = 0;
         if (wm) {
-            score_cells = 0;  // masked final level (final_level.cu)
-            score_best = time_stages({LK_STAGE_MERGE_SCORE});
+            // masked final level (final_level.cu), with and without the table
+            for (uint32_t v : {0u, 1u}) {
+                score_cells = v;
+                const float ms = time_stages({LK_STAGE_MERGE_SCORE});
+                if (ms < score_best) {
+                    score_best = ms;
+                    bcells = v;
+                }
+            }
         }
         for (uint32_t cells = 32; cells <= tmax; cells += 32) {
             score_cells = cells;

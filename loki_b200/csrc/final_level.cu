@@ -16,13 +16,13 @@
 //    is the same correctly rounded rcp(sqrt(n)) the direct path computes, so
 //    the product is the same; other V take the direct path;
 //  * each thread scores one cell from its staged prefix row: the row is read
-//    into registers a chunk of 32 positions (+ 32 ahead) at a time and every
-//    width w in 1..32 is a compile-time register offset, taken when bit w of
-//    the width mask is set; window differences are the same IEEE subtracts,
-//    and the maxima use fmaxf, which returns the same value as the
-//    reference's `(m < d) ? d : m` except for the sign of a zero maximum
-//    (fmaxf may prefer +0 where the reference keeps the first of -0 / +0), so
-//    a zero maximum is recomputed with the reference's rule;
+//    into registers 16 positions (plus the widest width) at a time and every
+//    width w up to the bucket WM (8, 16 or 32) is a compile-time register
+//    offset, taken when bit w of the width mask is set; window differences
+//    are the same IEEE subtracts, reduced by a pairwise fmaxf tree. fmaxf
+//    returns the same value as the reference's `(m < d) ? d : m` scan (NaN
+//    differences are skipped by both) except possibly for the sign of a zero
+//    maximum, so a zero maximum is recomputed with the reference's rule;
 //  * with a count target, each block counts its scores >= thr; a block's
 //    cells are contiguous in flat score order, so the candidate list is an
 //    exclusive scan of the block counts plus an ordered scatter of the blocks
@@ -50,16 +50,6 @@ __global__ void norm_table_kernel(float* __restrict__ tab, uint32_t n) {
     }
 }
 
-// e * (1 / sqrt(v)) exactly as sc::normalise, the reciprocal square root
-// taken from the table when v is an exact integer inside it.
-__device__ __forceinline__ float normalise_tab(float e, float v, const float* __restrict__ tab) {
-    const uint32_t n = __float2uint_rz(v);
-    if (n < kNormTableSize && __float_as_uint(__uint2float_rn(n)) == __float_as_uint(v)) {
-        return __fmul_rn(e, __ldg(tab + n));
-    }
-    return sc::normalise(e, v);
-}
-
 // Exact reference maximum (first maximum kept) of p[i + w] - p[i].
 __device__ __noinline__ float dmax_exact(const float* r, uint32_t w, uint32_t nbins) {
     float m = -FLT_MAX;
@@ -70,15 +60,19 @@ __device__ __noinline__ float dmax_exact(const float* r, uint32_t w, uint32_t nb
     return m;
 }
 
-template <bool TAYLOR, int NB, int PB, class TIn>
-__global__ void __launch_bounds__(128, 4)
+// WM: largest width the kernel handles (8, 16 or 32; the width mask has no
+// bit above it), so only WM width bodies are generated. CH: window chunk.
+// TAB: 1 / sqrt(V) from the table where V is an exact integer inside it.
+template <bool TAYLOR, int NB, int PB, class TIn, int WM, bool TAB>
+__global__ void __launch_bounds__(128, 5)
     merge_score_wm_kernel(const TIn* __restrict__ in, const void* __restrict__ coords,
                           uint32_t n_inner, uint32_t n_outer, uint64_t nprev, MaskScoreParams mp,
                           int mode, float* __restrict__ scores, float* __restrict__ cmax,
                           const float* __restrict__ tab, float thr, uint32_t* __restrict__ counts) {
-    constexpr int NJ = NB / kWarp;     // bins per lane in phase 1
-    constexpr int RS = NB + kMaxW + 1;  // odd row stride, room for every window read
-    constexpr int CH = NB < 32 ? NB : 32;
+    constexpr int NJ = NB / kWarp;      // bins per lane in phase 1
+    constexpr int RS = NB + WM + 1;  // odd row stride, room for every window read
+    constexpr int CH = 16;
+    static_assert(NB % CH == 0 && WM <= kMaxW, "chunking");
     extern __shared__ float rows[];
     const uint32_t nout = mode == LK_SCORE_PER_WIDTH ? mp.nwidths : 1;
     in += static_cast<uint64_t>(blockIdx.y) * 2 * nprev * 2 * NB;
@@ -104,36 +98,78 @@ __global__ void __launch_bounds__(128, 4)
         if (lane < PB && p0 + lane < nhere) {
             mine = load_merge_coord<TAYLOR>(coords, c0 + p0 + lane, NB);
         }
-        float te[PB][NJ], tv[PB][NJ], he[PB][NJ], hv[PB][NJ];
+        float se[PB][NJ], sv[PB][NJ];
+        {
+            float te[PB][NJ], tv[PB][NJ], he[PB][NJ], hv[PB][NJ];
 #pragma unroll
-        for (int q = 0; q < PB; ++q) {
-            const uint32_t it = __shfl_sync(0xffffffffu, mine.it, q);
-            const uint32_t ih = __shfl_sync(0xffffffffu, mine.ih, q);
-            const uint32_t st = __shfl_sync(0xffffffffu, mine.st, q);
-            const uint32_t sh = __shfl_sync(0xffffffffu, mine.sh, q);
-            const bool live = p0 + q < nhere;
-            // rows past nhere read row 0 (in range) and are not used
-            const TIn* tail = live ? in + static_cast<uint64_t>(it) * plen : in;
-            const TIn* head = live ? head_base + static_cast<uint64_t>(ih) * plen : head_base;
-#pragma unroll
-            for (int u = 0; u < NJ; ++u) {
-                const uint32_t j = lane + 32u * u;
-                const TIn* pt = tail + ((j - st) & (NB - 1));
-                const TIn* ph = head + ((j - sh) & (NB - 1));
-                te[q][u] = dev::Store<TIn>::load(pt);
-                tv[q][u] = dev::Store<TIn>::load(pt + NB);
-                he[q][u] = dev::Store<TIn>::load(ph);
-                hv[q][u] = dev::Store<TIn>::load(ph + NB);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < PB; ++q) {
-            if (p0 + q < nhere) {
-                float* dst = rows + static_cast<size_t>(p0 + q) * RS;
+            for (int q = 0; q < PB; ++q) {
+                const uint32_t it = __shfl_sync(0xffffffffu, mine.it, q);
+                const uint32_t ih = __shfl_sync(0xffffffffu, mine.ih, q);
+                const uint32_t st = __shfl_sync(0xffffffffu, mine.st, q);
+                const uint32_t sh = __shfl_sync(0xffffffffu, mine.sh, q);
+                const bool live = p0 + q < nhere;
+                // rows past nhere read row 0 (in range) and are not used
+                const TIn* tail = live ? in + static_cast<uint64_t>(it) * plen : in;
+                const TIn* head = live ? head_base + static_cast<uint64_t>(ih) * plen : head_base;
 #pragma unroll
                 for (int u = 0; u < NJ; ++u) {
-                    dst[lane + 32u * u] = normalise_tab(__fadd_rn(te[q][u], he[q][u]),
-                                                        __fadd_rn(tv[q][u], hv[q][u]), tab);
+                    const uint32_t j = lane + 32u * u;
+                    const TIn* pt = tail + ((j - st) & (NB - 1));
+                    const TIn* ph = head + ((j - sh) & (NB - 1));
+                    te[q][u] = dev::Store<TIn>::load(pt);
+                    tv[q][u] = dev::Store<TIn>::load(pt + NB);
+                    he[q][u] = dev::Store<TIn>::load(ph);
+                    hv[q][u] = dev::Store<TIn>::load(ph + NB);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+#pragma unroll
+                for (int u = 0; u < NJ; ++u) {
+                    se[q][u] = __fadd_rn(te[q][u], he[q][u]);
+                    sv[q][u] = __fadd_rn(tv[q][u], hv[q][u]);
+                }
+            }
+        }
+        if constexpr (TAB) {
+            // every table read in flight before the first product
+            float inv[PB][NJ];
+            bool ok[PB][NJ];
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+#pragma unroll
+                for (int u = 0; u < NJ; ++u) {
+                    const uint32_t n = __float2uint_rz(sv[q][u]);
+                    ok[q][u] = n < kNormTableSize &&
+                               __float_as_uint(__uint2float_rn(n)) == __float_as_uint(sv[q][u]);
+                    inv[q][u] = __ldg(tab + (ok[q][u] ? n : 0u));
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+                if (p0 + q < nhere) {
+                    float* dst = rows + static_cast<size_t>(p0 + q) * RS;
+#pragma unroll
+                    for (int u = 0; u < NJ; ++u) {
+                        float x;
+                        if (ok[q][u]) {
+                            x = __fmul_rn(se[q][u], inv[q][u]);
+                        } else {
+                            x = sc::normalise(se[q][u], sv[q][u]);
+                        }
+                        dst[lane + 32u * u] = x;
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+                if (p0 + q < nhere) {
+                    float* dst = rows + static_cast<size_t>(p0 + q) * RS;
+#pragma unroll
+                    for (int u = 0; u < NJ; ++u) {
+                        dst[lane + 32u * u] = sc::normalise(se[q][u], sv[q][u]);
+                    }
                 }
             }
         }
@@ -154,34 +190,45 @@ __global__ void __launch_bounds__(128, 4)
         for (uint32_t k = 0; k < mp.wmax; ++k) {
             r[NB + k] = __fadd_rn(r[k], sum);
         }
-        float dm[kMaxW + 1];
+        float dm[WM + 1];
 #pragma unroll
-        for (int w = 1; w <= kMaxW; ++w) {
+        for (int w = 1; w <= WM; ++w) {
             dm[w] = -FLT_MAX;
         }
 #pragma unroll 1
         for (int c = 0; c < NB; c += CH) {
-            // positions c .. c + CH + 31; those past NB + wmax - 1 are read
-            // (inside the row) but only widths above wmax would use them
-            float win[CH + kMaxW];
+            // positions c .. c + CH + WM - 1 (inside the row); those past
+            // NB + wmax - 1 are only used by widths above wmax (not taken)
+            float win[CH + WM];
 #pragma unroll
-            for (int k = 0; k < CH + kMaxW; ++k) {
+            for (int k = 0; k < CH + WM; ++k) {
                 win[k] = r[c + k];
             }
 #pragma unroll
-            for (int w = 1; w <= kMaxW; ++w) {
+            for (int w = 1; w <= WM; ++w) {
                 if ((mp.wmask >> w) & 1ull) {
+                    // pairwise tree of the chunk's differences (short
+                    // dependency chains), then the running maximum
+                    float d[CH];
 #pragma unroll
                     for (int k = 0; k < CH; ++k) {
-                        dm[w] = fmaxf(dm[w], __fsub_rn(win[k + w], win[k]));
+                        d[k] = __fsub_rn(win[k + w], win[k]);
                     }
+#pragma unroll
+                    for (int h = CH / 2; h >= 1; h /= 2) {
+#pragma unroll
+                        for (int k = 0; k < h; ++k) {
+                            d[k] = fmaxf(d[k], d[k + h]);
+                        }
+                    }
+                    dm[w] = fmaxf(dm[w], d[0]);
                 }
             }
         }
         const uint64_t c = c0 + threadIdx.x;
         float best = -FLT_MAX;
 #pragma unroll
-        for (int w = 1; w <= kMaxW; ++w) {
+        for (int w = 1; w <= WM; ++w) {
             if ((mp.wmask >> w) & 1ull) {
                 float d = dm[w];
                 if (d == 0.0f) {
@@ -298,7 +345,7 @@ void merge_score_level_wm(const void* d_in, const void* d_coords, bool taylor, u
                           uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                           const MaskScoreParams& mp, int mode, float* d_scores, cudaStream_t s,
                           uint64_t nbatch, bool in_bf16, float* d_cmax, const float* d_tab,
-                          float count_thr, uint32_t* d_counts) {
+                          float count_thr, uint32_t* d_counts, bool use_table) {
     require(nbatch >= 1 && nbatch <= 65535, "nbatch must lie in [1, 65535]");
     if (n_inner == 0 || n_outer == 0) {
         return;
@@ -308,18 +355,33 @@ void merge_score_level_wm(const void* d_in, const void* d_coords, bool taylor, u
     require(tiles * n_outer <= 0x7fffffffULL && n_inner <= 0xffffffffULL,
             "final level too large for the launch grid");
     const auto blocks = static_cast<unsigned>(tiles * n_outer);
-    auto go = [&](auto tg, auto tin, auto nbc) {
+    require(d_tab != nullptr || !use_table, "internal: no normalisation table");
+    auto go2 = [&](auto tg, auto tin, auto nbc, auto wmc, auto tabc) {
         constexpr bool TG = decltype(tg)::value;
         using TI = decltype(tin);
         constexpr int NB = decltype(nbc)::value;
-        constexpr int PB = NB == 32 ? 16 : (NB == 64 ? 8 : 4);
-        auto kern = merge_score_wm_kernel<TG, NB, PB, TI>;
-        const size_t smem = static_cast<size_t>(T) * (NB + kMaxW + 1) * sizeof(float);
+        constexpr int WM = decltype(wmc)::value;
+        constexpr bool TB = decltype(tabc)::value;
+        constexpr int PB = NB == 128 ? 4 : 8;
+        auto kern = merge_score_wm_kernel<TG, NB, PB, TI, WM, TB>;
+        const size_t smem = static_cast<size_t>(T) * (NB + WM + 1) * sizeof(float);
         sc::set_smem(kern, smem);
         kern<<<dim3(blocks, static_cast<unsigned>(nbatch)), T, smem, s>>>(
             static_cast<const TI*>(d_in), d_coords, static_cast<uint32_t>(n_inner),
             static_cast<uint32_t>(n_outer), ncoords_prev, mp, mode, d_scores, d_cmax, d_tab,
             count_thr, d_counts);
+    };
+    auto go = [&](auto tg, auto tin, auto nbc) {
+        auto by_tab = [&](auto wmc) {
+            use_table ? go2(tg, tin, nbc, wmc, std::true_type{}) : go2(tg, tin, nbc, wmc, std::false_type{});
+        };
+        if (mp.wmax <= 8) {
+            by_tab(std::integral_constant<int, 8>{});
+        } else if (mp.wmax <= 16) {
+            by_tab(std::integral_constant<int, 16>{});
+        } else {
+            by_tab(std::integral_constant<int, 32>{});
+        }
     };
     auto by_nb = [&](auto tg, auto tin) {
         if (nbins == 32) {

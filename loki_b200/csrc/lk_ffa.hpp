@@ -70,8 +70,9 @@ struct FFAExec {
     MaskScoreParams mp{};
     DeviceBuffer normtab, blk_counts, blk_offsets;
     // The masked final level runs unless a tuning picked the generic kernel
-    // (score_cells != 0).
-    bool use_wm() const { return wm && score_cells == 0; }
+    // (score_cells >= 32: cells per block of the generic kernel); score_cells
+    // 1 selects the masked kernel without the 1 / sqrt table.
+    bool use_wm() const { return wm && score_cells < 32; }
     bool mixed = false;  // BF16 storage of levels 1 .. L-2
     // A BF16 search rescores every final cell whose approximate best S/N is
     // at least (snr_min - margin_abs) / (1 + margin_rel).

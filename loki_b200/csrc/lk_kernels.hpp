@@ -148,7 +148,7 @@ void merge_score_level_wm(const void* d_in, const void* d_coords, bool taylor, u
                           uint64_t n_outer, uint64_t ncoords_prev, uint32_t nbins,
                           const MaskScoreParams& mp, int mode, float* d_scores, cudaStream_t s,
                           uint64_t nbatch, bool in_bf16, float* d_cmax, const float* d_tab,
-                          float count_thr, uint32_t* d_counts);
+                          float count_thr, uint32_t* d_counts, bool use_table = true);
 // Ordered compaction of scores >= thr from the block counts of
 // merge_score_level_wm: exclusive scan of the counts (d_offsets: one uint64
 // per block), then a scatter of the blocks that have candidates.

@@ -151,3 +151,137 @@ def mc_cascade(folds0, signal, noises, cls, widths, thresholds, grids, var0: flo
         if alive == 0:
             break
     return out
+
+
+# detection::State (include/loki/detection/thresholds.hpp:17-29); the
+# reference's pybind module exposes get_states() with these fields.
+STATE_DTYPE = np.dtype([("success_h0", np.float32), ("success_h1", np.float32), ("complexity", np.float32),
+                        ("complexity_cumul", np.float32), ("success_h1_cumul", np.float32),
+                        ("nbranches", np.float32), ("threshold", np.float32), ("cost", np.float32),
+                        ("threshold_prev", np.float32), ("success_h1_cumul_prev", np.float32),
+                        ("is_empty", np.bool_), ("_pad", np.uint8, 3)])
+
+
+class _DtsConfig(ctypes.Structure):
+    _fields_ = [("branching_pattern", ctypes.c_void_p), ("nstages", ctypes.c_uint32), ("ref_ducy", ctypes.c_float),
+                ("nbins", ctypes.c_uint32), ("ntrials", ctypes.c_uint32), ("nprobs", ctypes.c_uint32),
+                ("prob_min", ctypes.c_float), ("snr_final", ctypes.c_float), ("nthresholds", ctypes.c_uint32),
+                ("ducy_max", ctypes.c_float), ("wtsp", ctypes.c_float), ("beam_width", ctypes.c_float),
+                ("trials_start", ctypes.c_uint32), ("seed", ctypes.c_uint64)]
+
+
+DEFAULT_SEED = 0x10C1B200
+
+
+class DynamicThresholdSchemeCUDA:
+    """The reference's ``DynamicThresholdSchemeCUDA`` / ``DynamicThresholdScheme``
+    (lib/thresholds.cpp:560-907): beam search over (stage x threshold x
+    probability bin) with simulated H0 / H1 folds. Same arguments
+    (``batch_size`` is accepted and unused: every transition of a stage runs
+    in one launch); ``seed`` fixes the counter-based noise, so a run is
+    reproducible and matches the CPU oracle's."""
+
+    def __init__(self, branching_pattern, ref_ducy: float, nbins: int = 64, ntrials: int = 1024, nprobs: int = 10,
+                 prob_min: float = 0.05, snr_final: float = 8.0, nthresholds: int = 100, ducy_max: float = 0.3,
+                 wtsp: float = 1.0, beam_width: float = 0.7, trials_start: int = 1, batch_size: int = 256,
+                 device_id: int = 0, seed: int = DEFAULT_SEED):
+        D.require_cuda(device_id)
+        self._bp = np.ascontiguousarray(branching_pattern, dtype=np.float32)
+        if self._bp.size == 0:
+            raise ValueError("Branching pattern is empty")
+        cfg = _DtsConfig(self._bp.ctypes.data, self._bp.size, float(ref_ducy), int(nbins), int(ntrials), int(nprobs),
+                         float(prob_min), float(snr_final), int(nthresholds), float(ducy_max), float(wtsp),
+                         float(beam_width), int(trials_start), int(seed))
+        self._device = device_id
+        h = ctypes.c_void_p()
+        with D.torch().cuda.device(device_id):
+            C.check(C.lib().lk_dts_create(ctypes.byref(cfg), device_id, ctypes.byref(h)))
+        self._h = h
+        ns, nt, npb, nb, nw = (ctypes.c_uint32() for _ in range(5))
+        C.check(C.lib().lk_dts_info(h, ctypes.byref(ns), ctypes.byref(nt), ctypes.byref(npb), ctypes.byref(nb),
+                                    ctypes.byref(nw)))
+        self.nstages, self.nthresholds, self.nprobs = ns.value, nt.value, npb.value
+        self._nbins, self._nw = nb.value, nw.value
+        self.profile = np.zeros(self._nbins, np.float32)
+        self.thresholds = np.zeros(self.nthresholds, np.float32)
+        self.probs = np.zeros(self.nprobs, np.float32)
+        self.guess_path = np.zeros(self.nstages, np.float32)
+        self.box_score_widths = np.zeros(self._nw, np.uint32)
+        C.check(C.lib().lk_dts_arrays(h, self.profile.ctypes.data, self.thresholds.ctypes.data,
+                                      self.probs.ctypes.data, self.guess_path.ctypes.data,
+                                      self.box_score_widths.ctypes.data))
+        self._ran = False
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            C.lib().lk_dts_destroy(h)
+            self._h = None
+
+    @property
+    def branching_pattern(self) -> np.ndarray:
+        return self._bp.copy()
+
+    def run(self, thres_neigh: int = 10) -> None:
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_dts_run(self._h, int(thres_neigh), D.stream_ptr(self._device)))
+        self._ran = True
+
+    def transitions(self) -> int:
+        """Transitions the last run simulated (each: ntrials H0 and ntrials H1
+        folds built and scored)."""
+        n = ctypes.c_uint64()
+        C.check(C.lib().lk_dts_transitions(self._h, ctypes.byref(n)))
+        return n.value
+
+    def get_states(self) -> np.ndarray:
+        """States [nstages * nthresholds * nprobs] (the reference's flat layout)."""
+        n = self.nstages * self.nthresholds * self.nprobs
+        out = np.zeros(n, STATE_DTYPE)
+        C.check(C.lib().lk_dts_states(self._h, out.ctypes.data, n))
+        return out
+
+    def get_best_path_thresholds(self, min_pd: float = 0.1) -> np.ndarray:
+        out = np.zeros(self.nstages, np.float32)
+        n = ctypes.c_uint32()
+        C.check(C.lib().lk_dts_best_path(self._h, float(min_pd), out.ctypes.data, ctypes.byref(n)))
+        return out[: n.value].copy()
+
+    def save(self, outdir: str = "./") -> str:
+        """The reference's HDF5 file as ``.npz`` (same name stem and datasets)."""
+        import os
+
+        os.makedirs(outdir, exist_ok=True)
+        name = (f"dynscheme_nstages_{self.nstages:03d}_nthresh_{self.nthresholds:03d}_nprobs_{self.nprobs:03d}_"
+                f"snr_{float(self.thresholds[-1]):04.1f}.npz")
+        path = os.path.join(outdir, name)
+        np.savez(path, branching_pattern=self._bp, profile=self.profile, thresholds=self.thresholds,
+                 probs=self.probs, guess_path=self.guess_path,
+                 states=self.get_states().reshape(self.nstages, self.nthresholds, self.nprobs))
+        return path
+
+
+def dts_plan(branching_pattern, ref_ducy: float, nbins: int = 64, nprobs: int = 10, prob_min: float = 0.05,
+             snr_final: float = 8.0, nthresholds: int = 100, ducy_max: float = 0.3, wtsp: float = 1.0,
+             trials_start: int = 1) -> dict:
+    """Host-only set-up of a scheme (no device): profile, thresholds, probs,
+    guess path and box widths."""
+    bp = np.ascontiguousarray(branching_pattern, dtype=np.float32)
+    cfg = _DtsConfig(bp.ctypes.data, bp.size, float(ref_ducy), int(nbins), 1, int(nprobs), float(prob_min),
+                     float(snr_final), int(nthresholds), float(ducy_max), float(wtsp), 0.7, int(trials_start), 0)
+    out = {"profile": np.zeros(nbins, np.float32), "thresholds": np.zeros(nthresholds, np.float32),
+           "probs": np.zeros(nprobs, np.float32), "guess_path": np.zeros(bp.size, np.float32),
+           "widths": np.zeros(32, np.uint32)}
+    nw = ctypes.c_uint32()
+    C.check(C.lib().lk_dts_plan(ctypes.byref(cfg), out["profile"].ctypes.data, out["thresholds"].ctypes.data,
+                                out["probs"].ctypes.data, out["guess_path"].ctypes.data, out["widths"].ctypes.data,
+                                ctypes.byref(nw)))
+    out["widths"] = out["widths"][: nw.value].copy()
+    return out
+
+
+def normal_lut() -> np.ndarray:
+    """The generator's table of normal quantiles (2^17 + 1 floats)."""
+    out = np.zeros((1 << 17) + 1, np.float32)
+    C.check(C.lib().lk_dts_normal_lut(out.ctypes.data, out.size))
+    return out

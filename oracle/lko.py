@@ -580,3 +580,106 @@ def mc_stage(folds_in, noise, signal, var_in, var_add, widths, threshold, thresh
                            threshold, _p(thr), thr.size, None if c is None else _p(c), _p(out), _p(ids),
                            _p(counts), _p(mx))
     return out[:k], ids[:k], counts[:ncnt], mx
+
+
+# ---- DynamicThresholdScheme beam search -------------------------------------
+
+DTS_STATE_DTYPE = np.dtype([("success_h0", np.float32), ("success_h1", np.float32), ("complexity", np.float32),
+                            ("complexity_cumul", np.float32), ("success_h1_cumul", np.float32),
+                            ("nbranches", np.float32), ("threshold", np.float32), ("cost", np.float32),
+                            ("threshold_prev", np.float32), ("success_h1_cumul_prev", np.float32),
+                            ("is_empty", np.bool_), ("_pad", np.uint8, 3)])
+DTS_LUT_SIZE = (1 << 17) + 1
+
+
+class DtsCfg(ctypes.Structure):
+    _fields_ = [("branching_pattern", vp), ("nstages", u32), ("ref_ducy", f32), ("nbins", u32), ("ntrials", u32),
+                ("nprobs", u32), ("prob_min", f32), ("snr_final", f32), ("nthresholds", u32), ("ducy_max", f32),
+                ("wtsp", f32), ("beam_width", f32), ("trials_start", u32), ("seed", u64)]
+
+
+def _dts_lib():
+    L = lib()
+    if not hasattr(L, "_dts_ready"):
+        L.lko_normal_quantile.restype = f64
+        L.lko_normal_quantile.argtypes = [f64]
+        L.lko_dts_normal_lut.argtypes = [vp]
+        L.lko_dts_thresholds.argtypes = [f32, f32, u32, vp]
+        L.lko_dts_probs.argtypes = [u32, f32, vp]
+        L.lko_dts_profile.argtypes = [u32, f32, f32, vp]
+        L.lko_dts_guess.argtypes = [u32, f32, vp, u32, f32, vp]
+        L.lko_dts_neighbours.restype = u32
+        L.lko_dts_neighbours.argtypes = [vp, u32, u32, u32, vp]
+        L.lko_dts_lower_bin.restype = ctypes.c_int64
+        L.lko_dts_lower_bin.argtypes = [vp, u32, f32]
+        L.lko_philox4x32_10.argtypes = [vp, u32, u32, vp]
+        L.lko_dts_normal.restype = f32
+        L.lko_dts_normal.argtypes = [u32, vp]
+        L.lko_dts_resample.restype = u32
+        L.lko_dts_resample.argtypes = [u32, u32, u32, u32, u32, u32]
+        L.lko_dts_run.argtypes = [vp, u32, u32, vp]
+        L._dts_ready = True
+    return L
+
+
+def dts_normal_lut() -> np.ndarray:
+    out = np.zeros(DTS_LUT_SIZE, np.float32)
+    _dts_lib().lko_dts_normal_lut(_p(out))
+    return out
+
+
+def dts_thresholds(snr_start, snr_final, n) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    _dts_lib().lko_dts_thresholds(snr_start, snr_final, n, _p(out))
+    return out
+
+
+def dts_probs(n, prob_min) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    _dts_lib().lko_dts_probs(n, prob_min, _p(out))
+    return out
+
+
+def dts_profile(nbins, ducy, center=0.5) -> np.ndarray:
+    out = np.zeros(nbins, np.float32)
+    _dts_lib().lko_dts_profile(nbins, ducy, center, _p(out))
+    return out
+
+
+def dts_guess(nstages, snr_bound, branching, trials_start=1, min_trials=1e10) -> np.ndarray:
+    b = np.ascontiguousarray(branching, np.float32)
+    out = np.zeros(nstages, np.float32)
+    _dts_lib().lko_dts_guess(nstages, snr_bound, _p(b), trials_start, min_trials, _p(out))
+    return out
+
+
+def dts_neighbours(indices, target, num) -> np.ndarray:
+    idx = np.ascontiguousarray(indices, np.uint32)
+    out = np.zeros(num + 1, np.uint32)
+    n = _dts_lib().lko_dts_neighbours(_p(idx), idx.size, target, num, _p(out))
+    return out[:n].copy()
+
+
+def dts_lower_bin(range_, value) -> int:
+    r = np.ascontiguousarray(range_, np.float32)
+    return int(_dts_lib().lko_dts_lower_bin(_p(r), r.size, value))
+
+
+def philox4x32_10(ctr, seed) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, np.uint32)
+    out = np.zeros(4, np.uint32)
+    _dts_lib().lko_philox4x32_10(_p(c), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, _p(out))
+    return out
+
+
+def dts_run(branching, ref_ducy, nbins=64, ntrials=1024, nprobs=10, prob_min=0.05, snr_final=8.0, nthresholds=100,
+            ducy_max=0.3, wtsp=1.0, beam_width=0.7, trials_start=1, seed=0x10C1B200, thres_neigh=10,
+            stages_run=0) -> np.ndarray:
+    """The beam search (its first stages_run stages; 0: all); states
+    [nstages * nthresholds * nprobs]."""
+    b = np.ascontiguousarray(branching, np.float32)
+    cfg = DtsCfg(_p(b), b.size, ref_ducy, nbins, ntrials, nprobs, prob_min, snr_final, nthresholds, ducy_max, wtsp,
+                 beam_width, trials_start, seed)
+    out = np.zeros(b.size * nthresholds * nprobs, DTS_STATE_DTYPE)
+    _check(_dts_lib().lko_dts_run(ctypes.byref(cfg), thres_neigh, stages_run, _p(out)))
+    return out

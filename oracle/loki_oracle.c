@@ -2086,3 +2086,412 @@ uint64_t lko_mc_stage(const float* folds_in, const uint32_t* src, uint64_t ntria
     free(row);
     return kept;
 }
+
+/* ======================================================================== */
+/* DynamicThresholdScheme beam search (lib/thresholds.cpp:560-907): host     */
+/* set-up (lib/scheme.cpp, lib/simulation.cpp:12-50, lib/utils.cpp:138-185), */
+/* State::gen_next (include/loki/detection/thresholds.hpp:32-58) and the      */
+/* stage loop, sequential in the reference's order. The noise is the          */
+/* reference's table method (lib/loki/math.hpp:363-390: a 32-bit uniform     */
+/* through a 2^17 + 1 entry normal quantile table, fmaf interpolation) and    */
+/* its Lemire resampling (math.hpp:267-285), fed by Philox4x32-10 words of    */
+/* the counter (trial, bin / 4, transition * 2 + hypothesis, stage + 1) --    */
+/* the reference's thread-local PCG32 streams seeded from random_device       */
+/* cannot be reproduced.                                                      */
+/* ======================================================================== */
+
+#define LKO_DTS_LUT ((1u << 17) + 1u)
+
+/* Acklam's inverse normal CDF (2003) with one Halley step on erfc. */
+double lko_normal_quantile(double p) {
+    static const double a[6] = {-3.969683028665376e+01, 2.209460984245205e+02,
+                                -2.759285104469687e+02, 1.383577518672690e+02,
+                                -3.066479806614716e+01, 2.506628277459239e+00};
+    static const double b[5] = {-5.447609879822406e+01, 1.615858368580409e+02,
+                                -1.556989798598866e+02, 6.680131188771972e+01,
+                                -1.328068155288572e+01};
+    static const double c[6] = {-7.784894002430293e-03, -3.223964580411365e-01,
+                                -2.400758277161838e+00, -2.549732539343734e+00,
+                                4.374664141464968e+00, 2.938163982698783e+00};
+    static const double d[4] = {7.784695709041462e-03, 3.224671290700398e-01,
+                                2.445134137142996e+00, 3.754408661907416e+00};
+    const double p_low = 0.02425;
+    double x;
+    if (p < p_low) {
+        const double q = sqrt(-2.0 * log(p));
+        x = (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+            ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0);
+    } else if (p <= 1.0 - p_low) {
+        const double q = p - 0.5;
+        const double r = q * q;
+        x = (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+            (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1.0);
+    } else {
+        const double q = sqrt(-2.0 * log(1.0 - p));
+        x = -(((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+            ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0);
+    }
+    const double e = 0.5 * erfc(-x / sqrt(2.0)) - p;
+    const double u = e * sqrt(2.0 * 3.14159265358979323846) * exp(x * x / 2.0);
+    return x - u / (1.0 + x * u / 2.0);
+}
+
+/* ThreadLocalNormalRNG::init_lut (lib/loki/math.hpp:304-312). */
+void lko_dts_normal_lut(float* out) {
+    const double n = (double)(LKO_DTS_LUT - 1);
+    for (uint32_t i = 0; i < LKO_DTS_LUT; ++i) {
+        double p = (double)i / n;
+        p = p < 1e-9 ? 1e-9 : (p > 1.0 - 1e-9 ? 1.0 - 1e-9 : p);
+        out[i] = (float)lko_normal_quantile(p);
+    }
+}
+
+/* detail::compute_thresholds (lib/scheme.cpp:16-25). */
+void lko_dts_thresholds(float snr_start, float snr_final, uint32_t n, float* out) {
+    const float step = (snr_final - snr_start) / (float)(n - 1);
+    for (uint32_t i = 0; i < n; ++i) {
+        out[i] = ((float)i * step) + snr_start;
+    }
+}
+
+/* detail::compute_probs (lib/scheme.cpp:27-40). */
+void lko_dts_probs(uint32_t n, float prob_min, float* out) {
+    const float lpm = log10f(prob_min);
+    const float step = (0.0F - lpm) / (float)(n - 1);
+    for (uint32_t i = 0; i < n; ++i) {
+        out[i] = powf(10.0F, lpm + (step * (float)i));
+    }
+}
+
+/* simulation::generate_folded_profile (lib/simulation.cpp:12-50). */
+void lko_dts_profile(uint32_t nbins, float ducy, float center, float* out) {
+    const float step = 1.0F / (float)nbins;
+    const float ln10 = 2.302585092994045684017991454684364208F;
+    const float sigma = ducy / (2.0F * sqrtf(2.0F * ln10));
+    float mx = -FLT_MAX;
+    for (uint32_t i = 0; i < nbins; ++i) {
+        const float p = (float)i * step;
+        const float w = fmodf(p - center + 0.5F, 1.0F) - 0.5F;
+        out[i] = expf(-(w * w) / (2.0F * sigma * sigma));
+        mx = out[i] > mx ? out[i] : mx;
+    }
+    float ss = 0.0F;
+    for (uint32_t i = 0; i < nbins; ++i) {
+        out[i] = out[i] / mx;
+    }
+    for (uint32_t i = 0; i < nbins; ++i) {
+        ss = ss + out[i] * out[i];
+    }
+    const float norm = sqrtf(ss);
+    for (uint32_t i = 0; i < nbins; ++i) {
+        out[i] = out[i] / norm;
+    }
+}
+
+/* detail::guess_scheme = min(bound_scheme, trials_scheme) (lib/scheme.cpp:56-96),
+ * norm_isf(p) = -quantile(p). */
+void lko_dts_guess(uint32_t nstages, float snr_bound, const float* branching, uint32_t trials_start,
+                   float min_trials, float* out) {
+    const uint32_t nseg = nstages + 1;
+    float l2 = log2f((float)trials_start);
+    for (uint32_t i = 0; i < nstages; ++i) {
+        const float bound = sqrtf((float)(i + 2) * snr_bound * snr_bound / (float)nseg);
+        l2 += log2f(branching[i]);
+        const float trials = exp2f(l2);
+        const float eff = trials > min_trials ? trials : min_trials;
+        const float thr = (float)(-lko_normal_quantile((double)(1 / eff)));
+        out[i] = bound < thr ? bound : thr;
+    }
+}
+
+/* utils::find_neighbouring_indices (lib/utils.cpp:138-163). */
+uint32_t lko_dts_neighbours(const uint32_t* idx, uint32_t n, uint32_t target, uint32_t num,
+                            uint32_t* out) {
+    uint32_t pos = 0;
+    while (pos < n && idx[pos] < target) {
+        ++pos;
+    }
+    const uint32_t half = num / 2;
+    uint32_t left = pos > half ? pos - half : 0;
+    const uint32_t right = (left + num < n) ? left + num : n;
+    if (right - left < num && right == n) {
+        left = right > num ? right - num : 0;
+    }
+    for (uint32_t k = left; k < right; ++k) {
+        out[k - left] = idx[k];
+    }
+    return right - left;
+}
+
+/* utils::find_lower_bin_index (lib/utils.cpp:181-185). */
+int64_t lko_dts_lower_bin(const float* range, uint32_t n, float v) {
+    uint32_t k = 0;
+    while (k < n && !(v < range[k])) {
+        ++k;
+    }
+    return (int64_t)k - 1;
+}
+
+static lko_dts_state dts_empty(void) {
+    lko_dts_state s;
+    memset(&s, 0, sizeof(s));
+    s.complexity_cumul = FLT_MAX;
+    s.threshold = -1.0F;
+    s.cost = FLT_MAX;
+    s.threshold_prev = -1.0F;
+    s.is_empty = 1;
+    return s;
+}
+
+/* State::gen_next (include/loki/detection/thresholds.hpp:32-58). */
+lko_dts_state lko_dts_gen_next(const lko_dts_state* s, float threshold, float s0, float s1,
+                               float nbranches) {
+    const float nleaves_next = s->complexity * nbranches;
+    const float nleaves_surv = nleaves_next * s0;
+    const float cc = s->complexity_cumul + nleaves_next;
+    const float h1 = s->success_h1_cumul * s1;
+    lko_dts_state n = dts_empty();
+    n.success_h0 = s0;
+    n.success_h1 = s1;
+    n.complexity = nleaves_surv;
+    n.complexity_cumul = cc;
+    n.success_h1_cumul = h1;
+    n.nbranches = nbranches;
+    n.threshold = threshold;
+    n.cost = cc / h1;
+    n.is_empty = 0;
+    n.threshold_prev = s->threshold;
+    n.success_h1_cumul_prev = s->success_h1_cumul;
+    return n;
+}
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011). */
+void lko_philox4x32_10(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+/* ThreadLocalNormalRNG::generate_impl for one uniform word, mean 0, stddev 1. */
+float lko_dts_normal(uint32_t r, const float* lut) {
+    const float inv_u32 = 1.0F / 4294967296.0F;
+    const float max_idx = (float)(LKO_DTS_LUT - 2);
+    const float u = ((float)r * inv_u32) * max_idx;
+    const uint32_t idx = (uint32_t)u;
+    const float frac = u - (float)idx;
+    const float z = fmaf(frac, lut[idx + 1] - lut[idx], lut[idx]);
+    return fmaf(z, 1.0F, 0.0F);
+}
+
+/* uniform_index(range - 1): Lemire's bounded draw with rejection on the words
+ * of counters (i, 0xffffffff - call, tid2, stage_code). */
+uint32_t lko_dts_resample(uint32_t range, uint32_t i, uint32_t tid2, uint32_t stage_code, uint32_t k0,
+                          uint32_t k1) {
+    const uint64_t t = (1ull << 32) % range;
+    uint64_t m = 0;
+    for (uint32_t call = 0; call < 2; ++call) {
+        const uint32_t ctr[4] = {i, 0xFFFFFFFFu - call, tid2, stage_code};
+        uint32_t w[4];
+        lko_philox4x32_10(ctr, k0, k1, w);
+        for (int q = 0; q < 4; ++q) {
+            m = (uint64_t)w[q] * range;
+            if ((uint32_t)m >= range || (uint32_t)m >= t) {
+                return (uint32_t)(m >> 32);
+            }
+        }
+    }
+    return (uint32_t)(m >> 32);
+}
+
+/* Trial fold i of one (transition, hypothesis): (in[src] + noise) + prof. */
+static void dts_fold(const float* in, uint32_t n_in, const float* prof, uint32_t nbins, uint32_t i,
+                     uint32_t tid2, uint32_t stage_code, uint32_t k0, uint32_t k1, const float* lut,
+                     float* out) {
+    const uint32_t src = i < n_in ? i : lko_dts_resample(n_in, i, tid2, stage_code, k0, k1);
+    const float* ir = in + (uint64_t)src * nbins;
+    for (uint32_t q = 0; q * 4 < nbins; ++q) {
+        const uint32_t ctr[4] = {i, q, tid2, stage_code};
+        uint32_t w[4];
+        lko_philox4x32_10(ctr, k0, k1, w);
+        for (uint32_t k = 0; k < 4 && 4 * q + k < nbins; ++k) {
+            const uint32_t j = 4 * q + k;
+            out[j] = (ir[j] + lko_dts_normal(w[k], lut)) + prof[j];
+        }
+    }
+}
+
+/* simulate_score_prune_fused on one hypothesis: survivors in trial order. */
+static uint32_t dts_sim(const float* in, uint32_t n_in, const float* prof, const lko_dts_config* c,
+                        uint32_t tid2, uint32_t stage_code, float thr, float stdnoise, const uint64_t* w,
+                        uint64_t nw, const float* lut, float* out) {
+    uint32_t n = 0;
+    const uint32_t k0 = (uint32_t)c->seed, k1 = (uint32_t)(c->seed >> 32);
+    for (uint32_t i = 0; i < c->ntrials; ++i) {
+        float* row = out + (uint64_t)n * c->nbins;
+        dts_fold(in, n_in, prof, c->nbins, i, tid2, stage_code, k0, k1, lut, row);
+        if (lko_snr_max_div(row, c->nbins, w, nw, stdnoise) > thr) {
+            ++n;
+        }
+    }
+    return n;
+}
+
+int lko_dts_run(const lko_dts_config* c, uint32_t thres_neigh, uint32_t stages_run, lko_dts_state* states) {
+    const uint32_t S = c->nstages, NT = c->nthresholds, NP = c->nprobs, NB = c->nbins, NTR = c->ntrials;
+    const uint64_t ncell = (uint64_t)NT * NP;
+    const uint64_t fold_f = (uint64_t)NTR * NB;
+    float* lut = (float*)malloc(sizeof(float) * LKO_DTS_LUT);
+    float* prof = (float*)malloc(sizeof(float) * 2 * NB);
+    float* thr = (float*)malloc(sizeof(float) * NT);
+    float* probs = (float*)malloc(sizeof(float) * NP);
+    float* guess = (float*)malloc(sizeof(float) * S);
+    float* pool[2] = {(float*)malloc(sizeof(float) * ncell * 2 * fold_f),
+                      (float*)malloc(sizeof(float) * ncell * 2 * fold_f)};
+    uint32_t* cnt[2] = {(uint32_t*)calloc(ncell * 2, sizeof(uint32_t)),
+                        (uint32_t*)calloc(ncell * 2, sizeof(uint32_t))};
+    float* init = (float*)malloc(sizeof(float) * 2 * fold_f);
+    float* tmp[2] = {(float*)malloc(sizeof(float) * fold_f), (float*)malloc(sizeof(float) * fold_f)};
+    uint32_t* beam_prev = (uint32_t*)malloc(sizeof(uint32_t) * NT);
+    uint32_t* beam_cur = (uint32_t*)malloc(sizeof(uint32_t) * NT);
+    uint32_t* neigh = (uint32_t*)malloc(sizeof(uint32_t) * (thres_neigh + 1));
+    uint64_t w[LKO_MAX_WIDTHS];
+    int rc = 0;
+    if (!lut || !prof || !thr || !probs || !guess || !pool[0] || !pool[1] || !cnt[0] || !cnt[1] ||
+        !init || !tmp[0] || !tmp[1] || !beam_prev || !beam_cur || !neigh) {
+        rc = fail("out of memory");
+        goto done;
+    }
+    {
+        const uint32_t k0 = (uint32_t)c->seed, k1 = (uint32_t)(c->seed >> 32);
+        const uint64_t nw = lko_box_widths(NB, c->ducy_max, c->wtsp, w, LKO_MAX_WIDTHS);
+        float* p1 = (float*)malloc(sizeof(float) * NB);
+        lko_dts_normal_lut(lut);
+        lko_dts_profile(NB, c->ref_ducy, 0.5F, p1);
+        const float bias = c->snr_final / (float)sqrt((double)(S + 1));
+        for (uint32_t j = 0; j < NB; ++j) {
+            prof[j] = p1[j] * 0.0F;
+            prof[NB + j] = p1[j] * bias;
+        }
+        free(p1);
+        lko_dts_thresholds(0.1F, c->snr_final, NT, thr);
+        lko_dts_probs(NP, c->prob_min, probs);
+        lko_dts_guess(S, c->snr_final, c->branching_pattern, c->trials_start, 1E10F, guess);
+        for (uint64_t k = 0; k < (uint64_t)S * ncell; ++k) {
+            states[k] = dts_empty();
+        }
+        /* initial folds: simulate_folds from zero folds (no scoring) */
+        float* zeros = (float*)calloc(fold_f, sizeof(float));
+        for (uint32_t h = 0; h < 2; ++h) {
+            for (uint32_t i = 0; i < NTR; ++i) {
+                dts_fold(zeros, NTR, prof + h * NB, NB, i, h, 0u, k0, k1, lut,
+                         init + (uint64_t)h * fold_f + (uint64_t)i * NB);
+            }
+        }
+        free(zeros);
+        const lko_dts_state initial = {0.0F, 0.0F, 1.0F, 1.0F, 1.0F, 0.0F, -1.0F, FLT_MAX, -1.0F, 0.0F, 0, {0, 0, 0}};
+        float var_in = 1.0F;
+        uint32_t nprev = 0;
+        const uint32_t S_run = (stages_run == 0 || stages_run > S) ? S : stages_run;
+        for (uint32_t st = 0; st < S_run; ++st) {
+            const int cur = (int)(st % 2);
+            const float var_new = var_in + 1.0F;
+            const float stdnoise = sqrtf(var_new);
+            /* beam of this stage (get_current_thresholds_idx) */
+            uint32_t ncur = 0;
+            {
+                const float lo = guess[st] - c->beam_width > 0.0F ? guess[st] - c->beam_width : 0.0F;
+                const float hi = guess[st] + c->beam_width < thr[NT - 1] ? guess[st] + c->beam_width : thr[NT - 1];
+                for (uint32_t i = 0; i < NT; ++i) {
+                    if (thr[i] >= lo && thr[i] <= hi) {
+                        beam_cur[ncur++] = i;
+                    }
+                }
+            }
+            memset(cnt[cur], 0, sizeof(uint32_t) * ncell * 2);
+            lko_dts_state* sc = states + (uint64_t)st * ncell;
+            for (uint32_t b = 0; b < ncur; ++b) {
+                const uint32_t ithres = beam_cur[b];
+                const uint32_t nn = st == 0 ? 1 : lko_dts_neighbours(beam_prev, nprev, ithres, thres_neigh, neigh);
+                for (uint32_t jn = 0; jn < nn; ++jn) {
+                    for (uint32_t k = 0; k < (st == 0 ? 1u : NP); ++k) {
+                        const lko_dts_state* ps;
+                        const float* in0;
+                        const float* in1;
+                        uint32_t n0, n1, tid;
+                        if (st == 0) {
+                            ps = &initial;
+                            in0 = init;
+                            in1 = init + fold_f;
+                            n0 = n1 = NTR;
+                            tid = ithres;
+                        } else {
+                            const uint32_t pc = neigh[jn] * NP + k;
+                            ps = states + (uint64_t)(st - 1) * ncell + pc;
+                            in0 = pool[1 - cur] + (uint64_t)pc * 2 * fold_f;
+                            in1 = in0 + fold_f;
+                            n0 = cnt[1 - cur][2 * pc];
+                            n1 = cnt[1 - cur][2 * pc + 1];
+                            tid = (ithres * NT + neigh[jn]) * NP + k;
+                        }
+                        if (ps->is_empty || n0 == 0 || n1 == 0) {
+                            continue;
+                        }
+                        const uint32_t m0 = dts_sim(in0, n0, prof, c, 2 * tid, st + 1, thr[ithres], stdnoise, w,
+                                                    nw, lut, tmp[0]);
+                        const uint32_t m1 = dts_sim(in1, n1, prof + NB, c, 2 * tid + 1, st + 1, thr[ithres],
+                                                    stdnoise, w, nw, lut, tmp[1]);
+                        const lko_dts_state ns = lko_dts_gen_next(ps, thr[ithres], (float)m0 / (float)NTR,
+                                                                  (float)m1 / (float)NTR, c->branching_pattern[st]);
+                        const int64_t ip = lko_dts_lower_bin(probs, NP, ns.success_h1_cumul);
+                        if (ip < 0) {
+                            continue;
+                        }
+                        const uint64_t cell = (uint64_t)ithres * NP + (uint64_t)ip;
+                        if (sc[cell].is_empty || ns.complexity_cumul < sc[cell].complexity_cumul) {
+                            sc[cell] = ns;
+                            float* dst = pool[cur] + cell * 2 * fold_f;
+                            memcpy(dst, tmp[0], sizeof(float) * (uint64_t)m0 * NB);
+                            memcpy(dst + fold_f, tmp[1], sizeof(float) * (uint64_t)m1 * NB);
+                            cnt[cur][2 * cell] = m0;
+                            cnt[cur][2 * cell + 1] = m1;
+                        }
+                    }
+                }
+            }
+            memcpy(beam_prev, beam_cur, sizeof(uint32_t) * ncur);
+            nprev = ncur;
+            var_in = var_new;
+        }
+    }
+done:
+    free(lut);
+    free(prof);
+    free(thr);
+    free(probs);
+    free(guess);
+    free(pool[0]);
+    free(pool[1]);
+    free(cnt[0]);
+    free(cnt[1]);
+    free(init);
+    free(tmp[0]);
+    free(tmp[1]);
+    free(beam_prev);
+    free(beam_cur);
+    free(neigh);
+    return rc;
+}

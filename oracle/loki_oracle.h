@@ -256,6 +256,45 @@ uint64_t lko_mc_stage(const float* folds_in, const uint32_t* src, uint64_t ntria
                       float threshold, const float* thr, uint64_t n_thr, const uint8_t* cls,
                       float* folds_out, uint32_t* ids_out, uint64_t* counts, float* max_snr);
 
+/* ---- DynamicThresholdScheme beam search (lib/thresholds.cpp:560-907) ---- */
+typedef struct lko_dts_state {
+    float success_h0, success_h1, complexity, complexity_cumul, success_h1_cumul, nbranches,
+        threshold, cost, threshold_prev, success_h1_cumul_prev;
+    uint8_t is_empty;
+    uint8_t pad[3];
+} lko_dts_state;
+typedef struct lko_dts_config {
+    const float* branching_pattern;
+    uint32_t nstages;
+    float ref_ducy;
+    uint32_t nbins, ntrials, nprobs;
+    float prob_min, snr_final;
+    uint32_t nthresholds;
+    float ducy_max, wtsp, beam_width;
+    uint32_t trials_start;
+    uint64_t seed;
+} lko_dts_config;
+double lko_normal_quantile(double p);
+void lko_dts_normal_lut(float* out);
+void lko_dts_thresholds(float snr_start, float snr_final, uint32_t n, float* out);
+void lko_dts_probs(uint32_t n, float prob_min, float* out);
+void lko_dts_profile(uint32_t nbins, float ducy, float center, float* out);
+void lko_dts_guess(uint32_t nstages, float snr_bound, const float* branching, uint32_t trials_start,
+                   float min_trials, float* out);
+uint32_t lko_dts_neighbours(const uint32_t* idx, uint32_t n, uint32_t target, uint32_t num,
+                            uint32_t* out);
+int64_t lko_dts_lower_bin(const float* range, uint32_t n, float v);
+lko_dts_state lko_dts_gen_next(const lko_dts_state* s, float threshold, float s0, float s1,
+                               float nbranches);
+void lko_philox4x32_10(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t out[4]);
+float lko_dts_normal(uint32_t r, const float* lut);
+uint32_t lko_dts_resample(uint32_t range, uint32_t i, uint32_t tid2, uint32_t stage_code,
+                          uint32_t k0, uint32_t k1);
+/* The scheme's first stages_run stages (0: all); states [nstages][nthresholds][nprobs]
+ * (stages not run stay empty). */
+int lko_dts_run(const lko_dts_config* cfg, uint32_t thres_neigh, uint32_t stages_run,
+                lko_dts_state* states);
+
 #ifdef __cplusplus
 }
 #endif

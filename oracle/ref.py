@@ -110,6 +110,17 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
         L.lkref_prune_run_full.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64,
                                            u64, vp, vp, vp, vp, vp, vp, u64, vp]
         L.lkref_region_plan.argtypes = [vp, f64, f64, u64, u64, ctypes.c_int, vp, u64, vp, vp]
+        L.lkref_dts_thresholds.argtypes = [f32, f32, u64, vp]
+        L.lkref_dts_probs.argtypes = [u64, f32, vp]
+        L.lkref_dts_profile.argtypes = [u64, f32, f32, vp]
+        L.lkref_dts_bound.argtypes = [u64, f32, vp]
+        L.lkref_dts_neighbours.argtypes = [vp, u64, u64, u64, vp, vp]
+        L.lkref_dts_lower_bin.restype = ctypes.c_int64
+        L.lkref_dts_lower_bin.argtypes = [vp, u64, f32]
+        L.lkref_dts_gen_next.argtypes = [vp, f32, f32, f32, f32, vp]
+        L.lkref_dts_best_path.argtypes = [vp, u64, vp, u64, vp, u64, f32, vp, vp]
+        L.lkref_dts_run.argtypes = [vp, u64, f32, u64, u64, u64, f32, f32, u64, f32, f32, f32, u64, u64, vp, vp,
+                                    u64, vp]
         _libs[path] = L
     return _libs[path]
 
@@ -493,3 +504,86 @@ def prune_run_full(cfg: RefCfg, ffa_fold, thresholds, ref_seg, max_sugg, batch_s
     k = n.value
     return (stats[: nstats.value], leaves[: k * stride].reshape(k, cfg.nparams + 2, 2),
             folds[: k * 2 * nbins].reshape(k, 2, nbins), scores[:k], scores_ep[:k])
+
+
+# ---- DynamicThresholdScheme pieces (lib/scheme.cpp, lib/simulation.cpp,
+# lib/utils.cpp, thresholds.hpp) and the restated stage loop -----------------
+
+def _chk(L, rc):
+    if rc != 0:
+        raise RuntimeError(L.lkref_last_error().decode())
+
+
+def dts_thresholds(snr_start, snr_final, n, kind="parity"):
+    L = lib(kind)
+    out = np.zeros(n, np.float32)
+    _chk(L, L.lkref_dts_thresholds(snr_start, snr_final, n, _p(out)))
+    return out
+
+
+def dts_probs(n, prob_min, kind="parity"):
+    L = lib(kind)
+    out = np.zeros(n, np.float32)
+    _chk(L, L.lkref_dts_probs(n, prob_min, _p(out)))
+    return out
+
+
+def dts_profile(nbins, ducy, center=0.5, kind="parity"):
+    L = lib(kind)
+    out = np.zeros(nbins, np.float32)
+    _chk(L, L.lkref_dts_profile(nbins, ducy, center, _p(out)))
+    return out
+
+
+def dts_bound(nstages, snr_bound, kind="parity"):
+    L = lib(kind)
+    out = np.zeros(nstages, np.float32)
+    _chk(L, L.lkref_dts_bound(nstages, snr_bound, _p(out)))
+    return out
+
+
+def dts_neighbours(indices, target, num, kind="parity"):
+    L = lib(kind)
+    idx = np.ascontiguousarray(indices, np.uint64)
+    out = np.zeros(max(1, idx.size), np.uint64)
+    n = u64()
+    _chk(L, L.lkref_dts_neighbours(_p(idx), idx.size, target, num, _p(out), ctypes.byref(n)))
+    return out[: n.value].copy()
+
+
+def dts_lower_bin(range_, value, kind="parity"):
+    r = np.ascontiguousarray(range_, np.float32)
+    return int(lib(kind).lkref_dts_lower_bin(_p(r), r.size, value))
+
+
+def dts_gen_next(state, threshold, s0, s1, nbranches, dtype, kind="parity"):
+    L = lib(kind)
+    st = np.ascontiguousarray(np.asarray([state], dtype=dtype))
+    out = np.zeros(1, dtype)
+    _chk(L, L.lkref_dts_gen_next(_p(st), threshold, s0, s1, nbranches, _p(out)))
+    return out[0]
+
+
+def dts_best_path(states, nstages, thresholds, probs, min_pd=0.1, kind="parity"):
+    L = lib(kind)
+    st = np.ascontiguousarray(states)
+    th = np.ascontiguousarray(thresholds, np.float32)
+    pr = np.ascontiguousarray(probs, np.float32)
+    out = np.zeros(nstages, np.float32)
+    n = u64()
+    _chk(L, L.lkref_dts_best_path(_p(st), nstages, _p(th), th.size, _p(pr), pr.size, min_pd, _p(out),
+                                  ctypes.byref(n)))
+    return out[: n.value].copy()
+
+
+def dts_run(branching, ref_ducy, guess, lut, dtype, nbins=64, ntrials=1024, nprobs=10, prob_min=0.05, snr_final=8.0,
+            nthresholds=100, ducy_max=0.3, wtsp=1.0, beam_width=0.7, seed=0x10C1B200, thres_neigh=10,
+            stages_run=0, kind="parity"):
+    L = lib(kind)
+    b = np.ascontiguousarray(branching, np.float32)
+    g = np.ascontiguousarray(guess, np.float32)
+    lt = np.ascontiguousarray(lut, np.float32)
+    out = np.zeros(b.size * nthresholds * nprobs, dtype)
+    _chk(L, L.lkref_dts_run(_p(b), b.size, ref_ducy, nbins, ntrials, nprobs, prob_min, snr_final, nthresholds,
+                            ducy_max, wtsp, beam_width, seed, thres_neigh, _p(g), _p(lt), stages_run, _p(out)))
+    return out

@@ -28,6 +28,19 @@
 //   lkref_branch_max      -> EPMultiPass's branch_max rule (lib/prune.cpp:648-651)
 //   lkref_snr_threshold   -> detection::snr_boxcar_threshold_with_cache
 //                            (lib/score.cpp:434-462)
+//   lkref_dts_*           -> the DynamicThresholdScheme set-up and pieces
+//                            (detail::compute_thresholds / compute_probs /
+//                            bound_scheme / get_best_path_thresholds,
+//                            lib/scheme.cpp; generate_folded_profile,
+//                            lib/simulation.cpp:12-50; find_neighbouring_indices
+//                            / find_lower_bin_index, lib/utils.cpp:138-185;
+//                            State::gen_next, thresholds.hpp:32-58) and
+//                            lkref_dts_run, the scheme's stage loop
+//                            (lib/thresholds.cpp:748-907) restated over those
+//                            pieces and snr_boxcar_threshold_with_cache,
+//                            because thresholds.cpp itself needs HDF5; its
+//                            noise is the counter-based stream of the oracle
+//                            (Philox words through the normal quantile table)
 //   lkref_prune_run       -> PruneImpl::initialize + execute_iteration[_batched]
 //                            (lib/prune.cpp:181-226,429-620), restated here
 //                            because prune.cpp itself needs HDF5 and a
@@ -57,6 +70,10 @@
 #include "loki/core/chebyshev.hpp"
 #include "loki/core/taylor.hpp"
 #include "loki/detection/score.hpp"
+#include "loki/detection/thresholds.hpp"
+#include "loki/scheme.hpp"
+#include "loki/simulation/simulation.hpp"
+#include "loki/utils.hpp"
 #include "loki/kernels.hpp"
 #include "loki/psr_utils.hpp"
 #include "loki/search/configs.hpp"
@@ -861,6 +878,261 @@ static int prune_run_basis(const char* basis, const lkref_cfg* c, int conservati
         }
         (void)ls;
         (void)fs;
+    });
+}
+
+// ---- DynamicThresholdScheme ---------------------------------------------------
+
+int lkref_dts_thresholds(float snr_start, float snr_final, uint64_t n, float* out) {
+    return guarded([&] {
+        const auto t = loki::detection::detail::compute_thresholds(snr_start, snr_final, n);
+        std::copy(t.begin(), t.end(), out);
+    });
+}
+
+int lkref_dts_probs(uint64_t n, float prob_min, float* out) {
+    return guarded([&] {
+        const auto p = loki::detection::detail::compute_probs(n, prob_min);
+        std::copy(p.begin(), p.end(), out);
+    });
+}
+
+int lkref_dts_profile(uint64_t nbins, float ducy, float center, float* out) {
+    return guarded([&] {
+        const auto p = loki::simulation::generate_folded_profile(nbins, ducy, center);
+        std::copy(p.begin(), p.end(), out);
+    });
+}
+
+int lkref_dts_bound(uint64_t nstages, float snr_bound, float* out) {
+    return guarded([&] {
+        const auto b = loki::detection::detail::bound_scheme(nstages, snr_bound);
+        std::copy(b.begin(), b.end(), out);
+    });
+}
+
+int lkref_dts_neighbours(const uint64_t* idx, uint64_t n, uint64_t target, uint64_t num, uint64_t* out,
+                         uint64_t* n_out) {
+    return guarded([&] {
+        const auto r = loki::utils::find_neighbouring_indices(std::span<const loki::SizeType>(idx, n), target, num);
+        std::copy(r.begin(), r.end(), out);
+        *n_out = r.size();
+    });
+}
+
+int64_t lkref_dts_lower_bin(const float* range, uint64_t n, float v) {
+    return loki::utils::find_lower_bin_index(std::span<const float>(range, n), v);
+}
+
+using loki::detection::State;
+static_assert(sizeof(State) == 44, "State layout");
+
+int lkref_dts_gen_next(const void* state, float threshold, float s0, float s1, float nbranches, void* out) {
+    return guarded([&] {
+        State st;
+        std::memcpy(&st, state, sizeof(State));
+        const State n = st.gen_next(threshold, s0, s1, nbranches);
+        std::memcpy(out, &n, sizeof(State));
+    });
+}
+
+int lkref_dts_best_path(const void* states, uint64_t nstages, const float* thresholds, uint64_t nthresholds,
+                        const float* probs, uint64_t nprobs, float min_pd, float* out, uint64_t* n_out) {
+    return guarded([&] {
+        std::vector<State> st(nstages * nthresholds * nprobs);
+        std::memcpy(st.data(), states, st.size() * sizeof(State));
+        const auto r = loki::detection::detail::get_best_path_thresholds(
+            st, std::span<const float>(thresholds, nthresholds), std::span<const float>(probs, nprobs), nstages,
+            nthresholds, nprobs, min_pd);
+        std::copy(r.begin(), r.end(), out);
+        *n_out = r.size();
+    });
+}
+
+namespace {
+
+uint32_t dts_philox_word(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, int q) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+        const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+        const uint32_t hi0 = static_cast<uint32_t>(p0 >> 32), lo0 = static_cast<uint32_t>(p0);
+        const uint32_t hi1 = static_cast<uint32_t>(p1 >> 32), lo1 = static_cast<uint32_t>(p1);
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    const uint32_t w[4] = {c0, c1, c2, c3};
+    return w[q];
+}
+
+// The stream of one (transition, hypothesis): generate_impl / uniform_index
+// of ThreadLocalNormalRNG (lib/loki/math.hpp:267-285,363-390) on counter
+// words instead of a thread-local PCG32.
+struct CounterNormal {
+    const std::vector<float>* lut;
+    uint32_t k0, k1, tid2, stage;
+    float normal(uint32_t i, uint32_t j) const {
+        const uint32_t r = dts_philox_word(i, j / 4, tid2, stage, k0, k1, static_cast<int>(j % 4));
+        constexpr float kInvU32 = 1.0F / static_cast<float>(std::numeric_limits<uint32_t>::max());
+        const auto max_idx = static_cast<float>(lut->size() - 2);
+        const float u_scaled = static_cast<float>(r) * kInvU32 * max_idx;
+        const auto idx = static_cast<loki::SizeType>(u_scaled);
+        const float frac = u_scaled - static_cast<float>(idx);
+        const float z = std::fma(frac, (*lut)[idx + 1] - (*lut)[idx], (*lut)[idx]);
+        return std::fma(z, 1.0F, 0.0F);
+    }
+    uint32_t uniform_index(uint32_t i, uint32_t max_value) const {
+        const uint64_t range = static_cast<uint64_t>(max_value) + 1ULL;
+        const uint64_t t = (1ULL << 32U) % range;
+        uint64_t m = 0;
+        for (uint32_t call = 0; call < 2; ++call) {
+            for (int q = 0; q < 4; ++q) {
+                m = static_cast<uint64_t>(dts_philox_word(i, 0xFFFFFFFFu - call, tid2, stage, k0, k1, q)) * range;
+                const auto l = static_cast<uint32_t>(m);
+                if (l >= range || l >= t) {
+                    return static_cast<uint32_t>(m >> 32U);
+                }
+            }
+        }
+        return static_cast<uint32_t>(m >> 32U);
+    }
+};
+
+// simulate_score_prune_fused (lib/thresholds.cpp:358-431) with the stream above.
+uint32_t dts_sim(const std::vector<float>& in, uint32_t n_in, std::span<const float> profile, float bias,
+                 const CounterNormal& rng, uint32_t ntrials, uint32_t nbins,
+                 loki::detection::BoxcarWidthsCache& cache, float threshold, float var_in,
+                 std::vector<float>& out) {
+    std::vector<float> prof(nbins);
+    for (uint32_t j = 0; j < nbins; ++j) {
+        prof[j] = profile[j] * bias;
+    }
+    const float stdnoise = std::sqrt(var_in + 1.0F);
+    uint32_t n = 0;
+    for (uint32_t i = 0; i < ntrials; ++i) {
+        const uint32_t src = (i < n_in) ? i : rng.uniform_index(i, n_in - 1);
+        float* o = out.data() + static_cast<uint64_t>(n) * nbins;
+        for (uint32_t j = 0; j < nbins; ++j) {
+            o[j] = in[static_cast<uint64_t>(src) * nbins + j] + rng.normal(i, j) + prof[j];
+        }
+        if (loki::detection::snr_boxcar_threshold_with_cache(std::span<const float>(o, nbins), nbins, cache,
+                                                             threshold, stdnoise)) {
+            ++n;
+        }
+    }
+    return n;
+}
+
+} // namespace
+
+// init_states + run / run_segment (lib/thresholds.cpp:748-907), sequential,
+// over the reference's own pieces; guess: the guess path (norm_isf needs
+// Boost.Math, absent here), lut: the normal quantile table; the first
+// stages_run stages (0: all).
+int lkref_dts_run(const float* branching, uint64_t nstages, float ref_ducy, uint64_t nbins, uint64_t ntrials,
+                  uint64_t nprobs, float prob_min, float snr_final, uint64_t nthresholds, float ducy_max, float wtsp,
+                  float beam_width, uint64_t seed, uint64_t thres_neigh, const float* guess, const float* lut_in,
+                  uint64_t stages_run, void* states_out) {
+    return guarded([&] {
+        const std::vector<float> bp(branching, branching + nstages);
+        const auto profile = loki::simulation::generate_folded_profile(nbins, ref_ducy);
+        const auto thresholds = loki::detection::detail::compute_thresholds(0.1F, snr_final, nthresholds);
+        const auto probs = loki::detection::detail::compute_probs(nprobs, prob_min);
+        const auto widths = loki::detection::generate_box_width_trials(nbins, ducy_max, wtsp);
+        loki::detection::BoxcarWidthsCache cache(widths, nbins);
+        const float bias_snr = snr_final / static_cast<float>(std::sqrt(nstages + 1));
+        const std::vector<float> lut(lut_in, lut_in + (1U << 17U) + 1U);
+        const auto k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32U);
+        auto beam = [&](uint64_t istage) {
+            const float lower = std::max(0.0F, guess[istage] - beam_width);
+            const float upper = std::min(thresholds.back(), guess[istage] + beam_width);
+            std::vector<loki::SizeType> r;
+            for (loki::SizeType i = 0; i < thresholds.size(); ++i) {
+                if (thresholds[i] >= lower && thresholds[i] <= upper) {
+                    r.push_back(i);
+                }
+            }
+            return r;
+        };
+        const uint64_t ncell = nthresholds * nprobs;
+        std::vector<State> states(nstages * ncell, State{});
+        struct Folds {
+            std::vector<float> f[2];
+            uint32_t n[2] = {0, 0};
+        };
+        std::vector<Folds> cur(ncell), next(ncell);
+        // initial folds: simulate_folds from zero folds, variance 0 + 1
+        Folds init;
+        for (int h = 0; h < 2; ++h) {
+            init.f[h].resize(ntrials * nbins);
+            init.n[h] = static_cast<uint32_t>(ntrials);
+            const CounterNormal rng{&lut, k0, k1, static_cast<uint32_t>(h), 0U};
+            const float bias = h == 0 ? 0.0F : bias_snr;
+            for (uint32_t i = 0; i < ntrials; ++i) {
+                for (uint32_t j = 0; j < nbins; ++j) {
+                    init.f[h][i * nbins + j] = 0.0F + rng.normal(i, j) + profile[j] * bias;
+                }
+            }
+        }
+        const State initial = State::initial();
+        float var_in = 1.0F;
+        std::vector<loki::SizeType> beam_prev;
+        std::vector<float> tmp[2] = {std::vector<float>(ntrials * nbins), std::vector<float>(ntrials * nbins)};
+        const uint64_t s_run = (stages_run == 0 || stages_run > nstages) ? nstages : stages_run;
+        for (uint64_t st = 0; st < s_run; ++st) {
+            const auto beam_cur = beam(st);
+            for (auto& f : next) {
+                f.n[0] = f.n[1] = 0;
+            }
+            for (loki::SizeType ithres : beam_cur) {
+                std::vector<loki::SizeType> neigh{0};
+                if (st > 0) {
+                    neigh = loki::utils::find_neighbouring_indices(beam_prev, ithres, thres_neigh);
+                }
+                for (loki::SizeType jthresh : neigh) {
+                    for (uint64_t k = 0; k < (st == 0 ? 1 : nprobs); ++k) {
+                        const uint64_t pc = jthresh * nprobs + k;
+                        const State& ps = st == 0 ? initial : states[(st - 1) * ncell + pc];
+                        const Folds& pf = st == 0 ? init : cur[pc];
+                        if (ps.is_empty || pf.n[0] == 0 || pf.n[1] == 0) {
+                            continue;
+                        }
+                        const auto tid = static_cast<uint32_t>(st == 0 ? ithres : (ithres * nthresholds + jthresh) * nprobs + k);
+                        uint32_t m[2];
+                        for (int h = 0; h < 2; ++h) {
+                            const CounterNormal rng{&lut, k0, k1, 2 * tid + static_cast<uint32_t>(h),
+                                                    static_cast<uint32_t>(st + 1)};
+                            m[h] = dts_sim(pf.f[h], pf.n[h], profile, h == 0 ? 0.0F : bias_snr, rng,
+                                           static_cast<uint32_t>(ntrials), static_cast<uint32_t>(nbins), cache,
+                                           thresholds[ithres], var_in, tmp[h]);
+                        }
+                        const State ns = ps.gen_next(thresholds[ithres],
+                                                     static_cast<float>(m[0]) / static_cast<float>(ntrials),
+                                                     static_cast<float>(m[1]) / static_cast<float>(ntrials), bp[st]);
+                        const auto ip = loki::utils::find_lower_bin_index(probs, ns.success_h1_cumul);
+                        if (ip < 0 || ip >= static_cast<loki::IndexType>(nprobs)) {
+                            continue;
+                        }
+                        const uint64_t cell = ithres * nprobs + static_cast<uint64_t>(ip);
+                        State& ex = states[st * ncell + cell];
+                        if (ex.is_empty || ns.complexity_cumul < ex.complexity_cumul) {
+                            ex = ns;
+                            for (int h = 0; h < 2; ++h) {
+                                next[cell].f[h].assign(tmp[h].begin(), tmp[h].begin() + static_cast<int64_t>(m[h]) * nbins);
+                                next[cell].n[h] = m[h];
+                            }
+                        }
+                    }
+                }
+            }
+            std::swap(cur, next);
+            beam_prev = beam_cur;
+            var_in = var_in + 1.0F;
+        }
+        std::memcpy(states_out, states.data(), states.size() * sizeof(State));
     });
 }
 

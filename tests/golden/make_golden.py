@@ -5,6 +5,7 @@ Run from the repository root after ``make -C oracle ref``:
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py prune    # the pruning fixtures only
     python tests/golden/make_golden.py sweep    # the frequency-sweep fixtures only
+    python tests/golden/make_golden.py dts      # the threshold-scheme fixtures only
 
 Every output comes from ``oracle/_ref/libloki_ref_parity.so`` -- the
 reference's CPU sources compiled unmodified with IEEE flags -- so the fixtures
@@ -240,6 +241,38 @@ def sweep_fixtures() -> None:
               out["region_counts"].tolist())
 
 
+# name -> (nstages, branching (lo, hi), ref_ducy, keyword arguments of the scheme)
+DTS_CASES = {
+    "dts_nb32": (8, (1.5, 4.0), 0.1, dict(nbins=32, ntrials=256, nprobs=6, nthresholds=50, thres_neigh=6)),
+    "dts_nb48": (10, (1.5, 4.0), 0.1, dict(nbins=48, ntrials=128, nprobs=8, nthresholds=60, thres_neigh=10,
+                                           ducy_max=0.2, wtsp=1.5, snr_final=7.0)),
+}
+
+
+def dts_fixtures() -> None:
+    """DynamicThresholdScheme: the reference's set-up pieces and the stage
+    loop restated over them (ref_capi.cpp), with the oracle's guess path (the
+    reference's norm_isf needs Boost.Math) and normal quantile table."""
+    from oracle import lko
+
+    lut = lko.dts_normal_lut()
+    for name, (ns, (lo, hi), ducy, kw) in DTS_CASES.items():
+        bp = np.linspace(lo, hi, ns).astype(np.float32)
+        snr_final = kw.get("snr_final", 8.0)
+        guess = lko.dts_guess(ns, snr_final, bp)
+        states = ref.dts_run(bp, ducy, guess, lut, lko.DTS_STATE_DTYPE, **kw)
+        nthr, nprobs = kw["nthresholds"], kw["nprobs"]
+        thr = ref.dts_thresholds(0.1, snr_final, nthr)
+        probs = ref.dts_probs(nprobs, kw.get("prob_min", 0.05))
+        best = ref.dts_best_path(states, ns, thr, probs, 0.1)
+        fields = {f"state_{f}": states[f] for f in lko.DTS_STATE_DTYPE.names if f != "_pad"}
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), branching=bp, ref_ducy=ducy, guess=guess,
+                            lut_sha256=sha(lut), thresholds=thr, probs=probs,
+                            profile=ref.dts_profile(kw["nbins"], ducy), bound=ref.dts_bound(ns, snr_final),
+                            best_path=best, config=np.array([repr(kw)]), **fields)
+        print(name, "non-empty states", int((~states["is_empty"]).sum()), "best path", best.tolist())
+
+
 if __name__ == "__main__":
     if not ref.available():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` first")
@@ -247,7 +280,10 @@ if __name__ == "__main__":
         prune_fixtures()
     elif len(sys.argv) > 1 and sys.argv[1] == "sweep":
         sweep_fixtures()
+    elif len(sys.argv) > 1 and sys.argv[1] == "dts":
+        dts_fixtures()
     else:
         main()
         prune_fixtures()
         sweep_fixtures()
+        dts_fixtures()
