@@ -1,0 +1,105 @@
+// Check program for the C++20 drop-in classes of include/loki_b200.hpp: the
+// reference's FFACUDA<float> / PulsarSearchConfig / compute_ffa_scores_cuda
+// interface, implemented over the C ABI.
+//
+//   ffacuda_check <input.bin> <fold.bin> <scores.bin>
+//
+// input.bin: uint64 nsamps, double tsamp, uint64 nbins, double eta, uint32
+// nparams, double limits[2 * nparams], uint32 nwidths, uint32 widths[nwidths],
+// float ts_e[nsamps], float ts_v[nsamps]. Writes the final fold of
+// FFACUDA<float>::execute (host spans) and the scores of
+// compute_ffa_scores_cuda. Exit status 0 when every check passed.
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+#include <stdexcept>
+#include <vector>
+
+#include "loki_b200.hpp"
+
+namespace {
+
+template <class T> T read_one(std::ifstream& in) {
+    T v{};
+    in.read(reinterpret_cast<char*>(&v), sizeof(T));
+    return v;
+}
+
+template <class T> std::vector<T> read_n(std::ifstream& in, std::size_t n) {
+    std::vector<T> v(n);
+    in.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(n * sizeof(T)));
+    return v;
+}
+
+void write_all(const char* path, const std::vector<float>& v) {
+    std::ofstream out(path, std::ios::binary);
+    out.write(reinterpret_cast<const char*>(v.data()), static_cast<std::streamsize>(v.size() * sizeof(float)));
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    using namespace loki_b200;
+    if (argc != 4) {
+        std::cerr << "usage: ffacuda_check <input.bin> <fold.bin> <scores.bin>\n";
+        return 2;
+    }
+    std::ifstream in(argv[1], std::ios::binary);
+    const auto nsamps = read_one<uint64_t>(in);
+    const auto tsamp = read_one<double>(in);
+    const auto nbins = read_one<uint64_t>(in);
+    const auto eta = read_one<double>(in);
+    const auto np = read_one<uint32_t>(in);
+    const auto lim = read_n<double>(in, 2 * np);
+    const auto nw = read_one<uint32_t>(in);
+    const auto w32 = read_n<uint32_t>(in, nw);
+    const auto ts_e = read_n<float>(in, nsamps);
+    const auto ts_v = read_n<float>(in, nsamps);
+    if (!in) {
+        std::cerr << "short input\n";
+        return 2;
+    }
+    std::vector<ParamLimit> limits(np);
+    for (uint32_t i = 0; i < np; ++i) {
+        limits[i] = {lim[2 * i], lim[2 * i + 1]};
+    }
+    const std::vector<SizeType> widths(w32.begin(), w32.end());
+    try {
+        const search::PulsarSearchConfig cfg(nsamps, tsamp, nbins, eta, limits, 0.2, 1.5,
+                                             /*use_fourier=*/false, 1, std::nullopt, std::nullopt, 5.0,
+                                             widths);
+        const search::PulsarSearchConfig copy = cfg;  // copyable, like the reference's
+        algorithms::FFACUDA<float> ffa(copy);
+        algorithms::FFACUDA<float> moved = std::move(ffa);  // move-only PIMPL
+        std::vector<float> fold(moved.get_plan().get_fold_size());
+        moved.execute(ts_e, ts_v, fold);
+        write_all(argv[2], fold);
+        auto [scores, plan] = algorithms::compute_ffa_scores_cuda(ts_e, ts_v, cfg);
+        if (scores.size() != plan.get_ncoords_final() * widths.size()) {
+            std::cerr << "scores size mismatch\n";
+            return 1;
+        }
+        write_all(argv[3], scores);
+    } catch (const std::exception& e) {
+        std::cerr << "unexpected exception: " << e.what() << "\n";
+        return 1;
+    }
+    // the reference's error behaviour: rejected arguments throw invalid_argument
+    try {
+        const std::vector<ParamLimit> bad{{5.0, 1.0}};
+        const search::PulsarSearchConfig cfg(1000, tsamp, nbins, eta, bad);  // nsamps not a power of two
+        std::cerr << "expected std::invalid_argument\n";
+        return 1;
+    } catch (const std::invalid_argument&) {
+    }
+    try {
+        const search::PulsarSearchConfig cfg(nsamps, tsamp, nbins, eta, limits);  // use_fourier defaults to true
+        algorithms::FFACUDA<float> f(cfg);
+        std::cerr << "expected std::invalid_argument for the Fourier path\n";
+        return 1;
+    } catch (const std::invalid_argument&) {
+    }
+    std::cout << "ffacuda_check: ok\n";
+    return 0;
+}
