@@ -285,6 +285,7 @@ typedef struct lk_tuning {
     float bf_ms;         /* best median stage times (ms): brute fold (+ interleave), */
     float merge_ms;      /* all merge levels, */
     float score_ms;      /* fused final level */
+    uint32_t bf_tmem_warps; /* brute fold: consumer warps (of bf_warps) whose sums are in tensor memory */
 } lk_tuning;
 /* Times the candidates on the given device series (one search's inputs;
  * reps timed passes each, median) and keeps the fastest shape of each stage.

@@ -91,6 +91,7 @@ struct FoldArgs {
     uint32_t nbins;
     uint32_t nwords;           // ceil(seglen / 32)
     uint32_t warps;            // W consumer warps (frequencies) per block
+    uint32_t smem_warps;       // TMEM kernel: consumers with shared-memory sums (the rest use TMEM)
     uint32_t stages;           // depth of the shared-memory ring (<= kMaxStages)
     float* fold;
     uint32_t* status;
@@ -373,6 +374,11 @@ __global__ void __launch_bounds__(640, 1)
     const int warp = threadIdx.x / kWarp;
     const int lane = threadIdx.x % kWarp;
     const int W = static_cast<int>(a.warps);
+    // A block folds W consecutive frequencies: the warps share the sample
+    // ring and so move at the pace of the slowest, and neighbouring
+    // frequencies have nearly the same number of run starts. (Dealing the
+    // frequencies round-robin over the blocks put a high frequency in every
+    // block and measured 30 % slower.)
     const uint32_t q0 = blockIdx.y * a.warps;
     const int nconsumers = static_cast<int>(min(a.warps, a.nfreq - q0));
     const int seg0 = static_cast<int>(blockIdx.x * kWarp);
@@ -562,6 +568,291 @@ __global__ void __launch_bounds__(640, 1)
                 out[a.nbins + b] = p.y;
             }
         }
+    }
+}
+
+// Packed form with part of the accumulators in tensor memory. The block's
+// first a.smem_warps consumer warps keep their float2 [bin][lane] sums in
+// shared memory as in brute_fold_pk_kernel; the next consumer warps keep
+// them in TMEM (each lane's sums in its TMEM lane: column 2 b holds bin b's
+// E sum, 2 b + 1 its V sum), so a block runs more frequencies than shared
+// memory alone holds. Every add is the same add.rn.f32x2 in the same order.
+// The TMEM ops of a warp are warp-collective: the run masks are shared by
+// all lanes, so control flow is uniform, and a timed-out wait makes the
+// whole warp stop (__all_sync). TMEM order: a run-ahead read is waited for
+// before its sums are used; stores are waited for at every word (a bin is
+// revisited only after nbins runs, >= 64 samples when nbins >= 64) and before
+// every read when nbins < 64 or the bins do not step by one.
+// The producer warp allocates all 512 columns and frees them after the final
+// barrier, which every warp reaches (no early return).
+constexpr uint32_t kTmemCols = 512;
+constexpr int kMaxWarpsTm = 25;  // consumers + producer (<= 72 registers)
+
+template <class BinT>
+__global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
+    brute_fold_pk_tm_kernel(const __grid_constant__ CUtensorMap tmap_ev, FoldArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t S = a.stages;
+    unsigned char* ring = smem_raw;
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * kStageBytes);
+    uint64_t* empty = full + S;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(empty + S);
+    float2* accs = reinterpret_cast<float2*>(tslot + 2);  // 8-byte aligned
+
+    const int warp = threadIdx.x / kWarp;
+    const int lane = threadIdx.x % kWarp;
+    const int W = static_cast<int>(a.warps);
+    const int WS = static_cast<int>(a.smem_warps);
+    // W consecutive frequencies per block, as in brute_fold_pk_kernel; the
+    // TMEM warps take the block's first slots, its lowest frequencies (the
+    // fewest run starts, whose TMEM round trips cost the most).
+    const uint32_t q0 = blockIdx.y * a.warps;
+    const int nconsumers = static_cast<int>(min(a.warps, a.nfreq - q0));
+    const int slot = warp >= WS ? warp - WS : warp + (W - WS);
+    const int seg0 = static_cast<int>(blockIdx.x * kWarp);
+    const bool aligned = (ptx::smem_u32(ring) & 1023u) == 0;
+
+    if (warp == W) {
+        ptx::tmem_alloc(tslot, kTmemCols);
+        __syncwarp();
+        ptx::tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        if (!aligned) {
+            atomicOr(a.status, dev::kStatusBadTable);
+        }
+        ptx::prefetch_tensormap(&tmap_ev);
+        for (uint32_t s = 0; s < S; ++s) {
+            ptx::mbar_init(&full[s], 1);
+            ptx::mbar_init(&empty[s], nconsumers * kWarp);
+        }
+        ptx::fence_barrier_init();
+    }
+    ptx::tmem_fence_before_sync();
+    __syncthreads();
+    ptx::tmem_fence_after_sync();
+    const uint32_t tbase = *tslot;
+
+    if (aligned && warp == W) {
+        if (lane == 0) {
+            uint32_t issued = 0;
+            for (uint32_t k = 0; k < a.nwords; ++k) {
+                const uint32_t s = k % S;
+                if (k >= S &&
+                    !ptx::mbar_wait_bounded(&empty[s], ((k / S) - 1) & 1u, a.status,
+                                            dev::kStatusWaitTimeout | dev::kStatusEmpty)) {
+                    break;
+                }
+                unsigned char* st = ring + static_cast<size_t>(s) * kStageBytes;
+                ptx::mbar_arrive_expect_tx(&full[s], kStageBytes);
+                const int x0 = static_cast<int>(k * 64);
+                ptx::tma_load_2d(st, &tmap_ev, &full[s], x0, seg0);
+                ptx::tma_load_2d(st + kTileBytes, &tmap_ev, &full[s], x0 + 32, seg0);
+                ++issued;
+            }
+            const uint32_t first = issued > S ? issued - S : 0;
+            for (uint32_t k = first; k < issued; ++k) {
+                ptx::mbar_wait_bounded(&full[k % S], (k / S) & 1u, a.status,
+                                       dev::kStatusWaitTimeout | dev::kStatusDrain);
+            }
+        }
+    } else if (aligned && warp < W && slot < nconsumers) {
+        const bool tm = warp >= WS;
+        const uint32_t f = q0 + static_cast<uint32_t>(slot);
+        // shared-memory sums: [nbins + 1][32 lanes]; slot nbins absorbs the
+        // store before the first run. TMEM sums: this warp's quadrant, column
+        // block (warp - WS) / 4.
+        float2* A = accs + static_cast<size_t>(tm ? 0 : warp) * (a.nbins + 1) * kWarp + lane;
+        const uint32_t T = tbase + ((static_cast<uint32_t>(warp & 3) * 32u) << 16) +
+                           static_cast<uint32_t>((warp - WS) / 4) * 2u * a.nbins;
+        if (tm) {
+            for (uint32_t b = 0; b < a.nbins; ++b) {
+                ptx::tmem_st2(T + 2 * b, 0.0f, 0.0f);
+            }
+            ptx::tmem_wait_st();
+        } else {
+            for (uint32_t b = 0; b <= a.nbins; ++b) {
+                A[b * kWarp] = make_float2(0.0f, 0.0f);
+            }
+        }
+        const uint32_t* M = a.masks + static_cast<size_t>(f) * a.nwords;
+        const BinT* B = static_cast<const BinT*>(a.bins) + a.bin_off[f];
+        const uint64_t nr = a.nruns[f];
+        const uint32_t lrow = static_cast<uint32_t>(lane) * 128u;
+        const uint32_t lsw = static_cast<uint32_t>(lane) & 7u;
+
+        auto consume = [&](auto seq_tag, auto tm_tag) -> bool {
+            constexpr bool SEQ = decltype(seq_tag)::value;
+            constexpr bool TM = decltype(tm_tag)::value;
+            uint32_t bin;
+            float2 acc = make_float2(0.0f, 0.0f);
+            float2 nacc = make_float2(0.0f, 0.0f);
+            uint64_t r = 0;
+            uint64_t rbase = 0;
+            uint32_t binbuf = 0;
+            if constexpr (SEQ) {
+                const uint32_t b0 = static_cast<uint32_t>(__ldg(B));
+                bin = b0 == 0 ? a.nbins - 1 : b0 - 1;
+            } else {
+                bin = a.nbins;
+                binbuf = load_bins(B, nr, 0, lane);
+            }
+            uint32_t maskbuf = __ldg(M + min(static_cast<uint32_t>(lane), a.nwords - 1));
+            const bool small = a.nbins < 64;
+
+            auto start_run = [&](uint32_t& rl) {
+                if constexpr (TM) {
+                    if (SEQ || bin != a.nbins) {
+                        ptx::tmem_st2(T + 2 * bin, acc.x, acc.y);
+                    }
+                } else {
+                    A[bin * kWarp] = acc;
+                }
+                if constexpr (SEQ) {
+                    bin = bin + 1 == a.nbins ? 0u : bin + 1;
+                    if constexpr (TM) {
+                        ptx::tmem_wait_ld(nacc.x, nacc.y);
+                    }
+                    acc = nacc;
+                    const uint32_t nb = bin + 1 == a.nbins ? 0u : bin + 1;
+                    if constexpr (TM) {
+                        if (small) {
+                            ptx::tmem_wait_st();
+                        }
+                        ptx::tmem_ld2(T + 2 * nb, nacc.x, nacc.y);
+                    } else {
+                        nacc = A[nb * kWarp];
+                    }
+                    ++rl;
+                } else {
+                    bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
+                    ++rl;
+                    if constexpr (TM) {
+                        ptx::tmem_wait_st();
+                        ptx::tmem_ld2(T + 2 * bin, acc.x, acc.y);
+                        ptx::tmem_wait_ld(acc.x, acc.y);
+                    } else {
+                        acc = A[bin * kWarp];
+                    }
+                }
+            };
+
+            uint32_t phase = 0;
+            uint32_t s = 0;
+            for (uint32_t c = 0; c < a.nwords; ++c) {
+                if ((c & 31u) == 0 && c > 0) {
+                    maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
+                }
+                const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
+                if constexpr (!SEQ) {
+                    if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
+                        rbase = r;
+                        binbuf = load_bins(B, nr, rbase, lane);
+                    }
+                }
+                const bool got = ptx::mbar_wait_bounded(
+                    &full[s], phase, a.status,
+                    dev::kStatusWaitTimeout | (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull));
+                if (!__all_sync(0xffffffffu, got)) {
+                    return false;
+                }
+                if constexpr (TM) {
+                    ptx::tmem_wait_st();
+                }
+                const unsigned char* t0 = ring + static_cast<size_t>(s) * kStageBytes + lrow;
+                uint32_t rl = static_cast<uint32_t>(r - rbase);
+                // the word in two halves of 16 samples (fewer registers, so
+                // more warps fit)
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {
+                    float2 x[16];
+#pragma unroll
+                    for (uint32_t j = 0; j < 8; ++j) {
+                        const uint32_t o = (j ^ lsw) << 4;
+                        const float4 v = *reinterpret_cast<const float4*>(t0 + h * kTileBytes + o);
+                        x[2 * j] = make_float2(v.x, v.y);
+                        x[2 * j + 1] = make_float2(v.z, v.w);
+                    }
+                    if (h == 1) {
+                        ptx::mbar_arrive(&empty[s]);
+                    }
+                    const uint32_t mh = m >> (16 * h);
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) {
+                        if (((mh >> (4 * g)) & 0xfu) == 0) {
+#pragma unroll
+                            for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                                acc = add2_rn(acc, x[i]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int i = 4 * g; i < 4 * g + 4; ++i) {
+                                if (mh & (1u << i)) {
+                                    start_run(rl);
+                                }
+                                acc = add2_rn(acc, x[i]);
+                            }
+                        }
+                    }
+                }
+                s = (s + 1 == S) ? 0 : s + 1;
+                if (s == 0) {
+                    phase ^= 1u;
+                }
+                r = rbase + rl;
+            }
+            if constexpr (TM) {
+                if (SEQ || bin != a.nbins) {
+                    ptx::tmem_st2(T + 2 * bin, acc.x, acc.y);
+                }
+                ptx::tmem_wait_ld(nacc.x, nacc.y);
+                ptx::tmem_wait_st();
+            } else {
+                A[bin * kWarp] = acc;
+            }
+            if (r != nr) {
+                atomicOr(a.status, dev::kStatusBadTable);
+            }
+            return true;
+        };
+        bool ok;
+        if (tm) {
+            ok = a.seq[f] != 0 ? consume(std::true_type{}, std::true_type{})
+                               : consume(std::false_type{}, std::true_type{});
+        } else {
+            ok = a.seq[f] != 0 ? consume(std::true_type{}, std::false_type{})
+                               : consume(std::false_type{}, std::false_type{});
+        }
+        const uint32_t seg = static_cast<uint32_t>(seg0 + lane);
+        float* out = a.fold + (static_cast<size_t>(seg) * a.nfreq + f) * 2 * a.nbins;
+        if (ok && tm) {
+            // every lane reads (warp-collective); lanes past nseg do not store
+            for (uint32_t b = 0; b < a.nbins; b += 4) {
+                float4 e4, v4;
+                ptx::tmem_ld2(T + 2 * b, e4.x, v4.x);
+                ptx::tmem_ld2(T + 2 * b + 2, e4.y, v4.y);
+                ptx::tmem_ld2(T + 2 * b + 4, e4.z, v4.z);
+                ptx::tmem_ld2(T + 2 * b + 6, e4.w, v4.w);
+                ptx::tmem_wait_ld4(e4, v4);
+                if (seg < a.nseg) {
+                    reinterpret_cast<float4*>(out)[b / 4] = e4;
+                    reinterpret_cast<float4*>(out + a.nbins)[b / 4] = v4;
+                }
+            }
+        } else if (ok && seg < a.nseg) {
+            for (uint32_t b = 0; b < a.nbins; b += 4) {
+                const float2 p0 = A[b * kWarp], p1 = A[(b + 1) * kWarp];
+                const float2 p2 = A[(b + 2) * kWarp], p3 = A[(b + 3) * kWarp];
+                reinterpret_cast<float4*>(out)[b / 4] = make_float4(p0.x, p1.x, p2.x, p3.x);
+                reinterpret_cast<float4*>(out + a.nbins)[b / 4] = make_float4(p0.y, p1.y, p2.y, p3.y);
+            }
+        }
+    }
+    ptx::tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == W) {
+        ptx::tmem_fence_after_sync();
+        ptx::tmem_dealloc(tbase, kTmemCols);
     }
 }
 
@@ -765,12 +1056,42 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
 // fit, the larger W on a tie -- the kernel is latency-bound per warp, so
 // block time hardly depends on W) and the depth of the shared-memory ring.
 // Returns false (and changes nothing) when the shape does not fit.
-bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages) {
+uint32_t BruteFoldDevice::max_tmem_warps(uint32_t smem_warps) const {
+    // packed form, nbins a multiple of 4, 2 * nbins columns per warp, four
+    // warps (one per TMEM lane quadrant) per column block, block <= 21 warps
+    if (m_nbins > 64 || m_nbins % 4 != 0 || smem_warps + 1 >= static_cast<uint32_t>(kMaxWarpsTm)) {
+        return 0;
+    }
+    const uint32_t blocks = kTmemCols / static_cast<uint32_t>(2 * m_nbins);
+    return std::min<uint32_t>(4 * blocks, static_cast<uint32_t>(kMaxWarpsTm) - 1 - smem_warps);
+}
+
+bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages, uint32_t tmem) {
     if ((rows != 1 && rows != 2) || stages < 2 || stages > kMaxStages) {
         return false;
     }
     const size_t ring = stages * kStageBytes + 2 * stages * sizeof(uint64_t);
     const size_t per_warp = rows * (m_nbins + 1) * kWarp * sizeof(float);
+    if (tmem > 0) {
+        // shared-memory warps = warps - tmem, each with its accumulators
+        if (rows != 2 || warps <= tmem || tmem > max_tmem_warps(warps - tmem)) {
+            return false;
+        }
+        const size_t smem = ring + 16 + static_cast<size_t>(warps - tmem) * per_warp;
+        if (smem > kSmemLimit || (m_nfreq + warps - 1) / warps > 65535) {
+            return false;
+        }
+        m_rows = rows;
+        m_warps = warps;
+        m_stages = stages;
+        m_tmem = tmem;
+        // at least half the SM's shared memory: one block per SM, so a
+        // second block never waits for the first one's tensor memory
+        m_smem = std::max<size_t>(smem, 116 * 1024);
+        m_map_e_ptr = nullptr;
+        m_map_ev_ptr = nullptr;
+        return true;
+    }
     if (ring + per_warp > kSmemLimit) {
         return false;
     }
@@ -799,6 +1120,7 @@ bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages) 
     m_rows = rows;
     m_warps = w;
     m_stages = stages;
+    m_tmem = 0;
     m_smem = ring + w * per_warp;
     m_map_e_ptr = nullptr;  // the input binding depends on the rows
     m_map_ev_ptr = nullptr;
@@ -888,6 +1210,7 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
     a.nbins = static_cast<uint32_t>(m_nbins);
     a.nwords = static_cast<uint32_t>(m_nwords);
     a.warps = m_warps;
+    a.smem_warps = m_warps - m_tmem;
     a.stages = m_stages;
     a.fold = d_fold;
     a.status = m_status;
@@ -904,7 +1227,12 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
                                      static_cast<int>(m_smem)));
         kern<<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, a);
     };
-    if (m_rows == 2) {
+    if (m_rows == 2 && m_tmem > 0) {
+        LK_CUDA(cudaFuncSetAttribute(brute_fold_pk_tm_kernel<uint8_t>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(m_smem)));
+        brute_fold_pk_tm_kernel<uint8_t><<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, a);
+    } else if (m_rows == 2) {
         m_wide_bins ? launch_pk(brute_fold_pk_kernel<uint16_t>)
                     : launch_pk(brute_fold_pk_kernel<uint8_t>);
     } else {

@@ -337,9 +337,9 @@ void FFAExec::apply_tuning(const lk_tuning& t) {
     DeviceGuard g(device);
     require(t.merge_rows_in_flight >= 0 && t.merge_rows_in_flight <= 16,
             "merge rows in flight must lie in [0, 16]");
-    if (t.bf_rows != 0 || t.bf_warps != 0 || t.bf_stages != 0) {
+    if (t.bf_rows != 0 || t.bf_warps != 0 || t.bf_stages != 0 || t.bf_tmem_warps != 0) {
         require(bf->configure(t.bf_rows != 0 ? t.bf_rows : bf->rows(), t.bf_warps,
-                              t.bf_stages != 0 ? t.bf_stages : bf->stages()),
+                              t.bf_stages != 0 ? t.bf_stages : bf->stages(), t.bf_tmem_warps),
                 "brute-fold launch shape does not fit this plan");
     }
     merge_pb = t.merge_rows_in_flight;
@@ -348,6 +348,7 @@ void FFAExec::apply_tuning(const lk_tuning& t) {
     tuning.bf_rows = bf->rows();
     tuning.bf_warps = bf->warps();
     tuning.bf_stages = bf->stages();
+    tuning.bf_tmem_warps = bf->tmem_warps();
 }
 
 lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
@@ -415,7 +416,28 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
                 }
             }
         }
-        require(bf->configure(br, bw, bs), "autotune: lost the brute-fold shape");
+        // 1b. tensor-memory warps added to the best shared-memory shape
+        // (the warps of a block share the sample ring, so a block's time
+        // follows its slowest warp; a few shared-memory warp counts below the
+        // best are tried with each TMEM warp count, for whole waves of blocks)
+        uint32_t bt = 0;
+        if (br == 2) {
+            const uint32_t ws0 = bw;
+            for (uint32_t t = 4; t <= 16; t += 4) {
+                for (uint32_t ws = ws0 > 4 ? ws0 - 4 : 1; ws <= ws0; ++ws) {
+                    if (t > bf->max_tmem_warps(ws) || !bf->configure(2, ws + t, bs, t)) {
+                        continue;
+                    }
+                    const float ms = time_stages({LK_STAGE_INTERLEAVE, LK_STAGE_BRUTE_FOLD});
+                    if (ms < bf_best) {
+                        bf_best = ms;
+                        bt = t;
+                        bw = ws;
+                    }
+                }
+            }
+        }
+        require(bf->configure(br, bw + bt, bs, bt), "autotune: lost the brute-fold shape");
         // 2. merges
         const uint32_t nb = static_cast<uint32_t>(plan.cfg.nbins);
         std::vector<int> pbs{0};
@@ -469,6 +491,7 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         best.bf_rows = br;
         best.bf_warps = bf->warps();
         best.bf_stages = bs;
+        best.bf_tmem_warps = bt;
         best.merge_rows_in_flight = bpb;
         best.score_cells_per_block = bcells;
         best.candidates = tried;

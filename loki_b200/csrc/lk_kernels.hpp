@@ -65,12 +65,17 @@ public:
                      uint64_t nbatch = 1);
     // True when bind_inputs launches the interleave kernel.
     bool interleaves() const { return m_rows == 2; }
-    // Launch shape (see brute_fold.cu); false when it does not fit.
-    bool configure(uint32_t rows, uint32_t warps, uint32_t stages);
+    // Launch shape (see brute_fold.cu); false when it does not fit. tmem:
+    // consumer warps (of `warps`) whose sums live in tensor memory (packed
+    // form only).
+    bool configure(uint32_t rows, uint32_t warps, uint32_t stages, uint32_t tmem = 0);
     uint32_t max_warps(uint32_t rows, uint32_t stages) const;
+    // Most tensor-memory warps a block of smem_warps shared-memory warps can add.
+    uint32_t max_tmem_warps(uint32_t smem_warps) const;
     uint32_t rows() const { return m_rows; }
     uint32_t warps() const { return m_warps; }
     uint32_t stages() const { return m_stages; }
+    uint32_t tmem_warps() const { return m_tmem; }
     void fold(float* d_fold, cudaStream_t s);
     uint64_t nseg() const { return m_nseg; }
     uint64_t nfreq() const { return m_nfreq; }
@@ -84,6 +89,7 @@ private:
     uint32_t m_rows = 2;       // rows (E, V) per consumer warp
     uint32_t m_warps = 0;      // consumer warps per block
     uint32_t m_stages = 0;     // shared-memory ring depth (32-sample words)
+    uint32_t m_tmem = 0;       // consumer warps with tensor-memory sums
     size_t m_smem = 0;         // dynamic shared memory per block
     uint32_t* m_status;
     DeviceBuffer m_masks;      // uint32 [nfreq][ceil(seglen / 32)] run-start bits

@@ -195,3 +195,41 @@ def test_errors_are_loud(cuda):
                                  bseg_ffa=2**16)
     with pytest.raises(RuntimeError, match="nsegments must be 1"):
         FFACUDA(partial).scores(np.zeros(2**18, np.float32), np.ones(2**18, np.float32))
+
+
+# Brute fold with part of the accumulators in tensor memory (TMEM warps):
+# same sums in the same order, so folds stay bit-exact. Cases cover run bins
+# stepping by one (nbins 16 / 32 / 64) and the bin-table path (frequencies
+# above 1 / (tsamp nbins)).
+TMEM_CASES = {
+    "accel_nb64": (4, 8),
+    "accel_multi_nb32": (6, 12),
+    "freq_nb16": (2, 16),
+    "freq_nb64_nonseq": (8, 4),
+}
+CASES_EXTRA = {"freq_nb64_nonseq": (2**17, 1e-3, 64, 1.0, [[20.0, 30.0]], None)}
+
+
+@pytest.mark.parametrize("name", sorted(TMEM_CASES))
+def test_brute_fold_tmem_warps_bit_exact(cuda, name):
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+
+    nsamps, tsamp, nbins, eta, lims, bseg = {**CASES, **CASES_EXTRA}[name]
+    w = [x for x in WIDTHS if x < nbins]
+    cfg = PulsarSearchConfig(nsamps, tsamp, nbins, eta, np.array(lims), use_fourier=False, bseg_brute=bseg,
+                             score_widths=w)
+    op = lko.plan_create(lko.make_cfg(nsamps, tsamp, nbins, eta, lims, bseg_brute=bseg))
+    ts_e, ts_v = series(nsamps, 23)
+    ffa = FFACUDA(cfg)
+    ws, tw = TMEM_CASES[name]
+    t = ffa.tuning
+    t.update(bf_rows=2, bf_warps=ws + tw, bf_tmem_warps=tw)
+    ffa.set_tuning(t)
+    assert ffa.tuning["bf_tmem_warps"] == tw
+    want = lko.ffa(op, ts_e, ts_v)
+    got = ffa.execute(ts_e, ts_v)
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    want_s = lko.snr_boxcar_3d(want, np.array(w, np.uint64), nbins).ravel()
+    np.testing.assert_array_equal(ffa.scores(ts_e, ts_v).view(np.uint32), want_s.view(np.uint32))
+    assert ffa.status() == 0
