@@ -54,6 +54,8 @@ def parse():
                     help="skip the comparison of the candidates with the reference's CPU code")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes instead of timing the candidates first")
+    ap.add_argument("--tuning", default=None,
+                    help="apply these launch shapes (JSON of FFACUDA.tuning) instead of autotuning")
     ap.add_argument("--pipeline-execs", type=int, default=2,
                     help="executors (own compute streams) the end-to-end search pipeline alternates between")
     ap.add_argument("--workload", default="taylor_accel",
@@ -363,7 +365,10 @@ def run_ours(args, rank, world, local_rank):
                                 cap, cnt.data_ptr(), sp))
 
     tuning = None
-    if not args.no_autotune:
+    if args.tuning:
+        ffa.set_tuning(json.loads(args.tuning))
+        tuning = ffa.tuning
+    elif not args.no_autotune:
         # launch shapes timed on this series before the warm-up (not timed)
         tuning = ffa.autotune(e, v, reps=3)
     for _ in range(max(args.warmup, 3)):
