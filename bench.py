@@ -60,13 +60,14 @@ def parse():
                     help="executors (own compute streams) the end-to-end search pipeline alternates between")
     ap.add_argument("--workload", default="taylor_accel",
                     choices=["taylor_accel", "freq_sweep", "prune_jerk", "mc_cascade", "multi_series",
-                             "octave_sweep", "beam_scheme"],
+                             "octave_sweep", "beam_scheme", "fourier_accel"],
                     help="taylor_accel (default): Taylor (f, fdot) FFA + S/N; freq_sweep: plain period "
                          "sweep; prune_jerk: FFA to 32 segments + one pruning run; mc_cascade: 8-stage "
                          "Monte-Carlo threshold cascade; multi_series: 512 series of uneven length, "
                          "batched with CUDA graphs; octave_sweep: the frequency sweep over octave "
                          "regions (FFAFreqSweep) on the freq_sweep series; beam_scheme: the "
-                         "DynamicThresholdScheme beam search (16 stages, reference default sizes)")
+                         "DynamicThresholdScheme beam search (16 stages, reference default sizes); "
+                         "fourier_accel: the default search through the Fourier-domain FFA")
     return ap.parse_args()
 
 

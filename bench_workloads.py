@@ -15,6 +15,12 @@
                cut into chunks for 8 GB under the device memory model; per
                chunk FFA + scores + `>= 7` compaction + parameter decode.
                Metric: param-trials/s summed over chunks.
+  fourier_accel  the default line's search (2^22 samples,
+               nbins 64, eta 2, accel +-200 m/s^2, f 5-50 Hz) through the
+               Fourier-domain FFA (use_fourier = true, the reference default):
+               direct transform of each level-0 segment, phase-rotation merges,
+               inverse real transform, boxcar S/N, compaction at S/N >= 7.
+               Metric: param-trials/s.
   mc_cascade   2^20 profiles x 64 bins, seed 99, 8 Monte-Carlo stages (variance
                doubling, pruning thresholds 2 -> 6) each counted against 64
                thresholds. Metric: param-trials/s = alive profiles x 64
@@ -849,7 +855,180 @@ def run_dts(args, rank, world, local_rank):
     return 0
 
 
+# ---- fourier_accel ------------------------------------------------------------------
+
+FOURIER_SNR_TOL = 2e-3  # |S/N| agreement with the reference's FP32 Fourier path
+
+
+def _ref_fourier_runner(params, kind="timing"):
+    """The reference's Fourier-domain search step: FFA<ComplexType>::execute
+    returning to time (its FFTW c2r through the DFT-definition stand-in of
+    oracle/ref_stubs.cpp), snr_boxcar_3d, then score >= snr_min in flat order."""
+    from oracle import ref
+
+    nthreads = os.cpu_count() or 1
+    cfg = ref.make_cfg(params["nsamps"], params["tsamp"], params["nbins"], params["eta"], params["param_limits"],
+                       nthreads=nthreads)
+    ffa = ref.RefFourier(cfg, kind=kind)
+    widths = np.array(params["score_widths"], dtype=np.uint64)
+
+    def step(ts_e, ts_v):
+        fold = ffa.execute_time(ts_e, ts_v)
+        scores = ref.snr_boxcar_3d(fold, widths, params["nbins"], nthreads=nthreads, kind=kind).ravel()
+        idx = np.flatnonzero(scores >= B.SNR_MIN)
+        return idx, scores[idx], scores
+
+    return step, nthreads
+
+
+def run_fourier(args, rank, world, local_rank):
+    ts_e, ts_v, params, _ = B.workload()
+    name = "fourier_taylor_ffa_accel_2^22x64us_nbins64_eta2"
+    cfgd = {"nsamps": params["nsamps"], "tsamp": params["tsamp"], "nbins": params["nbins"], "eta": params["eta"],
+            "param_limits": params["param_limits"], "score_widths": params["score_widths"], "snr_min": B.SNR_MIN,
+            "use_fourier": True}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        from oracle import ref
+
+        if not ref.available("timing"):
+            B.emit({"impl": "reference", "unavailable": "oracle/_ref was not built"})
+            return 0
+        step, nthreads = _ref_fourier_runner(params)
+        ntrials = None
+        for _ in range(max(args.warmup, 1)):
+            _, _, sc = step(ts_e, ts_v)
+            ntrials = sc.size
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(ts_e, ts_v)
+        total = time.perf_counter() - t0
+        v = ntrials * args.steps / total
+        B.emit(_line(args, world, name, v, 1e3 * total / args.steps, dict(cfgd, cpu_threads=nthreads),
+                     impl="reference",
+                     cpu_baseline={"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                                   "sample": f"full workload, {args.steps} steps; FFTW's c2r replaced by a "
+                                             "DFT-definition stand-in"},
+                     e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}))
+        return 0
+    torch, dist = _init(local_rank, world)
+    from loki_b200 import _capi as C
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACOMPLEXCUDA
+
+    cfg = PulsarSearchConfig(params["nsamps"], params["tsamp"], params["nbins"], params["eta"],
+                             np.array(params["param_limits"]), use_fourier=True,
+                             score_widths=params["score_widths"], snr_min=B.SNR_MIN)
+    ffa = FFACOMPLEXCUDA(cfg, device_id=local_rank)
+    plan = ffa.plan
+    ntrials = int(plan.ncoords[-1]) * cfg.n_scoring_widths
+    cap = 1 << 20
+    e = torch.from_numpy(ts_e).cuda()
+    v = torch.from_numpy(ts_v).cuda()
+    idx = torch.empty(cap, dtype=torch.int32, device="cuda")
+    snr = torch.empty(cap, dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+    L = C.lib()
+
+    def step():
+        C.check(L.lk_fourier_search(ffa._h, e.data_ptr(), v.data_ptr(), B.SNR_MIN, idx.data_ptr(), snr.data_ptr(),
+                                    cap, cnt.data_ptr(), sp))
+
+    ffa.set_profiling(True)
+    clocks = B.ClockSampler(local_rank)
+    clocks.start()
+    ms, _ = _timed(torch, step, args.steps, args.warmup, flush, dist)
+    clk = clocks.stop()
+    prof = {}
+    launches = 0
+    for st in ffa.profile():
+        key = st["stage"] if st["level"] < 0 else f'{st["stage"]}_l{st["level"]}'
+        prof[key] = (st["ms"], st["bytes"])
+        launches += st["launches"]
+    ffa.set_profiling(False)
+    value = ntrials * world / (ms / 1e3)
+    # roofline of the dominant stage: the level-0 direct transform is bound by
+    # the FP32 pipe. Algorithmic flops: the reference's count for it,
+    # 8 * nsamps * 2 * nfreqs * nbins_f (FFAPlan::compute_flops, lib/plans.cpp:520-560).
+    nfreq0 = int(plan.ncoords[0])
+    nbf = params["nbins"] // 2 + 1
+    flops = 8 * params["nsamps"] * 2 * nfreq0 * nbf
+    bf_ms = prof["brute_fold_l0"][0]
+    props = torch.cuda.get_device_properties(local_rank)
+    mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+    fp32_peak = 2 * 128 * props.multi_processor_count * mhz * 1e6 / 1e12
+    ach = flops / (bf_ms / 1e3) / 1e12
+    peak, peak_kind = B.hbm_peak()
+    merges = {k: (p[1] / (p[0] / 1e3) / 1e9) / peak for k, p in sorted(prof.items()) if k.startswith("merge")}
+    roof = {"bound": "fp32", "kernel": "brute_fold_l0 (fourier_dft_kernel)", "achieved": ach, "peak": fp32_peak,
+            "unit": "TFLOP/s", "frac": ach / fp32_peak,
+            "peak_source": "nominal FP32 FMA rate: 128 lanes x 2 flop x SMs x max SM clock",
+            "algorithmic_flops": flops, "avg_ms": bf_ms, "traffic": B.ncu_traffic("fourier_dft"),
+            "merge_hbm_frac": merges, "hbm_peak": peak, "hbm_peak_source": peak_kind}
+    e2e = None
+    if not args.no_e2e:
+        he, hv = torch.from_numpy(ts_e).pin_memory(), torch.from_numpy(ts_v).pin_memory()
+        hc = torch.zeros(1, dtype=torch.int64).pin_memory()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(args.steps):
+            e.copy_(he, non_blocking=True)
+            v.copy_(hv, non_blocking=True)
+            step()
+            hc.copy_(cnt, non_blocking=True)
+            torch.cuda.synchronize()
+            n = min(int(hc.item()), cap)
+            _ = (idx[:n].cpu(), snr[:n].cpu())
+            d2h += 8 + 8 * n
+        el = time.perf_counter() - t0
+        e2e = {"value": ntrials * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": 8 * params["nsamps"],
+               "d2h_bytes_per_step": d2h // args.steps,
+               "api": "FFACOMPLEXCUDA search (lk_fourier_search), host series"}
+    ncand = int(cnt.item())
+    gi = idx[:ncand].cpu().numpy().astype(np.int64)
+    gs = snr[:ncand].cpu().numpy()
+    cpu = parity = None
+    status = 0
+    if rank == 0 and world == 1 and not (args.no_cpu_baseline and args.no_parity):
+        from oracle import ref
+
+        if ref.available("timing"):
+            rstep, nthreads = _ref_fourier_runner(params)
+            t0 = time.perf_counter()
+            r_idx, r_snr, r_all = rstep(ts_e, ts_v)
+            secs = time.perf_counter() - t0
+            if not args.no_cpu_baseline:
+                cpu = {"value": ntrials / secs, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                       "sample": "full workload, one step (the reference's FFA<ComplexType> + snr_boxcar_3d, "
+                                 "Release flags; FFTW's c2r by a DFT-definition stand-in)"}
+            if not args.no_parity:
+                near = np.abs(r_all - B.SNR_MIN) <= FOURIER_SNR_TOL
+                sure = np.setdiff1d(r_idx, np.flatnonzero(near))
+                extra = np.setdiff1d(gi, r_idx)
+                ok = bool(np.isin(sure, gi).all() and near[extra].all())
+                d = float(np.abs(gs - r_all[gi]).max()) if gi.size else 0.0
+                parity = {"checked": True, "vs": "oracle/_ref timing build (reference FFA<ComplexType>, FP32)",
+                          "candidates_match": ok and d <= FOURIER_SNR_TOL, "snr_max_abs_diff": d,
+                          "snr_tol": FOURIER_SNR_TOL, "n": int(gi.size), "n_ref": int(r_idx.size),
+                          "near_threshold_cells": int(near.sum())}
+                status = 0 if parity["candidates_match"] else 1
+        else:
+            parity = {"checked": False, "why": "oracle/_ref was not built"}
+    if rank == 0:
+        B.emit(_line(args, world, name, value, ms,
+                     dict(cfgd, final_coords=int(plan.ncoords[-1]), candidates=ncand, level0_freqs=nfreq0,
+                          lossy_level0=ffa.lossy),
+                     roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps * launches, clocks=clk,
+                     parity=parity, stages={k: {"ms": p[0], "bytes": p[1]} for k, p in prof.items()}))
+    _finish(dist)
+    return status
+
+
 def run(args, rank, world, local_rank):
     return {"freq_sweep": run_freq, "prune_jerk": run_prune, "mc_cascade": run_mc,
             "multi_series": run_multi, "octave_sweep": run_octaves,
-            "beam_scheme": run_dts}[args.workload](args, rank, world, local_rank)
+            "beam_scheme": run_dts, "fourier_accel": run_fourier}[args.workload](args, rank, world, local_rank)

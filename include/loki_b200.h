@@ -116,6 +116,7 @@ typedef struct lk_plan_info {
 typedef struct lk_plan lk_plan;
 typedef struct lk_ffa lk_ffa;
 typedef struct lk_brute_fold lk_brute_fold;
+typedef struct lk_fourier lk_fourier;
 
 /* ---- library ---------------------------------------------------------- */
 const char* lk_last_error(void);
@@ -194,6 +195,53 @@ int lk_ffa_scores_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, u
 int lk_ffa_search_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
                         float snr_min, uint32_t* d_idx, float* d_snr, uint64_t max_cands,
                         uint64_t* d_count, lk_stream_t stream);
+
+/* ---- Fourier-domain FFA (replaces FFACUDA<ComplexTypeCUDA>) ------------- */
+/* The FFA of the reference's use_fourier = true path (the default of
+ * PulsarSearchConfig, include/loki/search/configs.hpp:32): folds are kept as
+ * nbins_f = nbins / 2 + 1 complex harmonics, merges rotate them by the
+ * coordinates' fractional shifts (lib/kernels.cpp:241-453, 942-1130), and
+ * results return to time by an inverse real transform scaled by 1 / nbins
+ * (lib/fft.cpp:503-552). Level 0 is the direct transform of each segment
+ * (lib/kernels.cpp:1156-1242) for nbins <= nbins_min_lossy_bf, else the
+ * time-domain brute fold followed by a real transform (lib/ffa.cpp:170-240).
+ * nbins_min_lossy_bf 0 selects the reference default 64. Complex arrays are
+ * interleaved (re, im) FP32, as cuda::std::complex<float>. FP32 sums; phases
+ * reduced modulo one cycle in FP64 before the FP32 sine and cosine. */
+/* BruteFoldCUDA<ComplexTypeCUDA> / compute_brute_fold_cuda<ComplexTypeCUDA>
+ * (lib/fold_cuda.cu, lib/kernels_cuda.cu:856-965): the direct transform of
+ * each segment at each frequency, [nsamps / segment_len, nfreqs, 2,
+ * nbins / 2 + 1] complex (fold_len counts complex values). freqs is a host
+ * array. */
+int lk_fourier_brute_fold(const float* d_ts_e, const float* d_ts_v, uint64_t nsamps,
+                          const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                          uint64_t nbins, double tsamp, double t_ref, float* d_fold,
+                          uint64_t fold_len, int device, lk_stream_t stream);
+int lk_fourier_create(const lk_plan* plan, int device, uint64_t nbins_min_lossy_bf,
+                      lk_fourier** out);
+void lk_fourier_destroy(lk_fourier* f);
+/* nbins_f; final fold sizes (complex values, and floats back in time);
+ * lossy = 1 when level 0 is the brute fold + real transform. */
+int lk_fourier_info(const lk_fourier* f, uint64_t* nbins_f, uint64_t* fold_size,
+                    uint64_t* fold_size_time, int* lossy, uint64_t* workspace_bytes);
+/* FFACUDA<ComplexTypeCUDA>::execute(ts_e, ts_v, span<ComplexTypeCUDA>, stream)
+ * (include/loki/algorithms/ffa.hpp:126-134): final complex fold
+ * [nseg, ncoords, 2, nbins_f]; fold_len counts complex values. */
+int lk_fourier_execute(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float* d_fold,
+                       uint64_t fold_len, lk_stream_t stream);
+/* FFACUDA<ComplexTypeCUDA>::execute(ts_e, ts_v, span<float>, stream)
+ * (ffa.hpp:142-147): the final fold back in time, [nseg, ncoords, 2, nbins]
+ * FP32 (fold_size_time floats). */
+int lk_fourier_execute_time(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float* d_fold,
+                            uint64_t fold_len, lk_stream_t stream);
+/* compute_ffa_scores with use_fourier (lib/ffa.cpp:444-466): boxcar S/N of
+ * every final coordinate and width of the fold back in time. */
+int lk_fourier_scores(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float* d_scores,
+                      uint64_t scores_len, lk_stream_t stream);
+/* Scores plus threshold compaction, as lk_ffa_search. */
+int lk_fourier_search(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float snr_min,
+                      uint32_t* d_idx, float* d_snr, uint64_t max_cands, uint64_t* d_count,
+                      lk_stream_t stream);
 
 /* Synchronises the stream and reports the executor's device status word
  * (0 = no bounded wait gave up). */
@@ -308,7 +356,9 @@ enum lk_stage_kind {
     LK_STAGE_MERGE = 2,
     LK_STAGE_MERGE_SCORE = 3,
     LK_STAGE_COMPACT = 4,
-    LK_STAGE_RESCORE = 5  /* LK_BF16 search: exact rescoring of near-threshold cells */
+    LK_STAGE_RESCORE = 5, /* LK_BF16 search: exact rescoring of near-threshold cells */
+    LK_STAGE_TRANSFORM = 6, /* Fourier FFA: batched real / inverse real transforms */
+    LK_STAGE_SCORE = 7      /* standalone boxcar S/N of a fold back in time */
 };
 typedef struct lk_stage_time {
     int32_t kind;       /* lk_stage_kind */
@@ -325,6 +375,10 @@ int lk_ffa_get_profile(lk_ffa* ffa, lk_stream_t stream, lk_stage_time* out, uint
  * summed by stage kind over levels and chunks (level -1). */
 int lk_sweep_set_profiling(lk_sweep* sw, int enable);
 int lk_sweep_get_profile(lk_sweep* sw, lk_stage_time* out, uint32_t max_out, uint32_t* n_out);
+/* Stage timing of the Fourier-domain FFA (as lk_ffa_get_profile). */
+int lk_fourier_set_profiling(lk_fourier* f, int enable);
+int lk_fourier_get_profile(lk_fourier* f, lk_stream_t stream, lk_stage_time* out,
+                           uint32_t max_out, uint32_t* n_out);
 
 /* ---- brute fold (replaces BruteFoldCUDA<float>) ------------------------ */
 int lk_brute_fold_create(const double* freqs, uint64_t nfreqs, uint64_t segment_len,

@@ -94,7 +94,8 @@ class LkPlanInfo(ctypes.Structure):
     ]
 
 
-STAGE_NAMES = {0: "interleave", 1: "brute_fold", 2: "merge", 3: "merge_score", 4: "compact", 5: "rescore"}
+STAGE_NAMES = {0: "interleave", 1: "brute_fold", 2: "merge", 3: "merge_score", 4: "compact", 5: "rescore",
+               6: "transform", 7: "score"}
 
 
 class LkStageTime(ctypes.Structure):
@@ -152,6 +153,16 @@ SIGNATURES = [
     ("lk_ffa_execute", i32, [vp, vp, vp, vp, u64, vp]),
     ("lk_ffa_scores", i32, [vp, vp, vp, vp, u64, vp]),
     ("lk_ffa_search", i32, [vp, vp, vp, f32, vp, vp, u64, vp, vp]),
+    ("lk_fourier_create", i32, [vp, i32, u64, vp]),
+    ("lk_fourier_destroy", None, [vp]),
+    ("lk_fourier_info", i32, [vp, vp, vp, vp, vp, vp]),
+    ("lk_fourier_execute", i32, [vp, vp, vp, vp, u64, vp]),
+    ("lk_fourier_execute_time", i32, [vp, vp, vp, vp, u64, vp]),
+    ("lk_fourier_scores", i32, [vp, vp, vp, vp, u64, vp]),
+    ("lk_fourier_search", i32, [vp, vp, vp, f32, vp, vp, u64, vp, vp]),
+    ("lk_fourier_set_profiling", i32, [vp, i32]),
+    ("lk_fourier_get_profile", i32, [vp, vp, vp, u32, vp]),
+    ("lk_fourier_brute_fold", i32, [vp, vp, u64, vp, u64, u64, u64, f64, f64, vp, u64, i32, vp]),
     ("lk_ffa_create_batched", i32, [vp, i32, i32, u64, vp]),
     ("lk_ffa_execute_batch", i32, [vp, vp, vp, u64, vp, u64, vp]),
     ("lk_ffa_scores_batch", i32, [vp, vp, vp, u64, vp, u64, vp]),

@@ -11,6 +11,7 @@
 #include "lk_device.cuh"
 #include "lk_dts.hpp"
 #include "lk_ffa.hpp"
+#include "lk_fourier.hpp"
 #include "lk_kernels.hpp"
 #include "lk_mc.hpp"
 #include "lk_prune.hpp"
@@ -33,6 +34,9 @@ struct lk_sweep {
 };
 struct lk_dts {
     std::unique_ptr<lk::DtsExec> exec;
+};
+struct lk_fourier {
+    std::unique_ptr<lk::FourierExec> exec;
 };
 struct lk_brute_fold {
     int device = 0;
@@ -505,6 +509,157 @@ int lk_ffa_get_profile(lk_ffa* ffa, lk_stream_t stream, lk_stage_time* out, uint
         need(ffa, "ffa");
         need(n_out, "n_out");
         const auto st = ffa->exec->profile(reinterpret_cast<cudaStream_t>(stream));
+        const auto n = static_cast<uint32_t>(std::min<size_t>(st.size(), max_out));
+        if (n > 0) {
+            need(out, "out");
+            std::copy(st.begin(), st.begin() + n, out);
+        }
+        *n_out = static_cast<uint32_t>(st.size());
+    });
+}
+
+int lk_fourier_brute_fold(const float* d_ts_e, const float* d_ts_v, uint64_t nsamps,
+                          const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                          uint64_t nbins, double tsamp, double t_ref, float* d_fold,
+                          uint64_t fold_len, int device, lk_stream_t stream) {
+    return guarded([&] {
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(freqs, "freqs");
+        need(d_fold, "d_fold");
+        lk::require(nfreqs >= 1 && nfreqs <= 0xffffffffULL, "nfreqs out of range");
+        lk::require(segment_len >= 1 && segment_len <= nsamps, "segment_len must lie in [1, nsamps]");
+        lk::require(nbins >= 2 && nbins <= 2048, "nbins must lie in [2, 2048]");
+        lk::require(reinterpret_cast<uintptr_t>(d_fold) % 8 == 0, "d_fold must be 8-byte aligned");
+        const uint64_t nseg = nsamps / segment_len;
+        lk::require(fold_len >= nseg * nfreqs * 2 * (nbins / 2 + 1),
+                    "fold must hold nseg * nfreqs * 2 * (nbins / 2 + 1) complex values");
+        lk::DeviceGuard g(device);
+        const auto s = reinterpret_cast<cudaStream_t>(stream);
+        lk::DeviceBuffer f(sizeof(double) * nfreqs);
+        LK_CUDA(cudaMemcpyAsync(f.ptr, freqs, sizeof(double) * nfreqs, cudaMemcpyHostToDevice, s));
+        lk::fourier_dft_fold(d_ts_e, d_ts_v, f.as<double>(), static_cast<uint32_t>(nfreqs),
+                             segment_len, nseg, static_cast<uint32_t>(nbins), tsamp, t_ref,
+                             reinterpret_cast<float2*>(d_fold), s);
+        // the frequency table is freed on return: finish the launch first
+        LK_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int lk_fourier_create(const lk_plan* plan, int device, uint64_t nbins_min_lossy_bf,
+                      lk_fourier** out) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(out, "out");
+        auto f = std::make_unique<lk_fourier>();
+        f->exec = std::make_unique<lk::FourierExec>(plan->plan, device, nbins_min_lossy_bf);
+        *out = f.release();
+    });
+}
+
+void lk_fourier_destroy(lk_fourier* f) {
+    if (f != nullptr) {
+        try {
+            lk::DeviceGuard g(f->exec->device);
+            delete f;
+        } catch (...) {
+            delete f;
+        }
+    }
+}
+
+int lk_fourier_info(const lk_fourier* f, uint64_t* nbins_f, uint64_t* fold_size,
+                    uint64_t* fold_size_time, int* lossy, uint64_t* workspace_bytes) {
+    return guarded([&] {
+        need(f, "f");
+        const auto& e = *f->exec;
+        const uint32_t L = e.plan.n_levels;
+        if (nbins_f != nullptr) {
+            *nbins_f = e.nbf;
+        }
+        if (fold_size != nullptr) {
+            *fold_size = e.fold_size(L - 1);
+        }
+        if (fold_size_time != nullptr) {
+            *fold_size_time = e.fold_size_time(L - 1);
+        }
+        if (lossy != nullptr) {
+            *lossy = e.lossy ? 1 : 0;
+        }
+        if (workspace_bytes != nullptr) {
+            *workspace_bytes = e.device_bytes();
+        }
+    });
+}
+
+int lk_fourier_execute(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float* d_fold,
+                       uint64_t fold_len, lk_stream_t stream) {
+    return guarded([&] {
+        need(f, "f");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_fold, "d_fold");
+        lk::require(reinterpret_cast<uintptr_t>(d_fold) % 8 == 0, "d_fold must be 8-byte aligned");
+        f->exec->execute(d_ts_e, d_ts_v, reinterpret_cast<float2*>(d_fold), fold_len,
+                         reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_fourier_execute_time(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float* d_fold,
+                            uint64_t fold_len, lk_stream_t stream) {
+    return guarded([&] {
+        need(f, "f");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_fold, "d_fold");
+        f->exec->execute_time(d_ts_e, d_ts_v, d_fold, fold_len,
+                              reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_fourier_scores(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float* d_scores,
+                      uint64_t scores_len, lk_stream_t stream) {
+    return guarded([&] {
+        need(f, "f");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_scores, "d_scores");
+        f->exec->scores(d_ts_e, d_ts_v, d_scores, scores_len,
+                        reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_fourier_search(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, float snr_min,
+                      uint32_t* d_idx, float* d_snr, uint64_t max_cands, uint64_t* d_count,
+                      lk_stream_t stream) {
+    return guarded([&] {
+        need(f, "f");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        need(d_count, "d_count");
+        if (max_cands > 0) {
+            need(d_idx, "d_idx");
+            need(d_snr, "d_snr");
+        }
+        f->exec->search(d_ts_e, d_ts_v, snr_min, d_idx, d_snr, max_cands, d_count,
+                        reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int lk_fourier_set_profiling(lk_fourier* f, int enable) {
+    return guarded([&] {
+        need(f, "f");
+        f->exec->prof.enabled = enable != 0;
+        f->exec->prof.reset();
+    });
+}
+
+int lk_fourier_get_profile(lk_fourier* f, lk_stream_t stream, lk_stage_time* out,
+                           uint32_t max_out, uint32_t* n_out) {
+    return guarded([&] {
+        need(f, "f");
+        need(n_out, "n_out");
+        const auto st = f->exec->profile(reinterpret_cast<cudaStream_t>(stream));
         const auto n = static_cast<uint32_t>(std::min<size_t>(st.size(), max_out));
         if (n > 0) {
             need(out, "out");

@@ -1,0 +1,77 @@
+// Fourier-domain FFA executor (internal): FFACUDA<ComplexTypeCUDA> of the
+// reference (lib/ffa_cuda.cu, lib/ffa.cpp:75-135,170-310). Kernels in
+// fourier.cu.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "lk_ffa.hpp"
+#include "lk_kernels.hpp"
+
+namespace lk {
+
+// PulsarSearchConfig's nbins_min_lossy_bf default (include/loki/search/
+// configs.hpp:37): above it the level-0 fold is the time-domain brute fold
+// followed by a real transform instead of the direct transform.
+constexpr uint64_t kNbinsMinLossy = 64;
+
+// Level-0 direct transform of segments (kernels::brute_fold_ts_complex,
+// lib/kernels.cpp:1156-1242): out [nseg][nfreq][2][nbf] complex.
+void fourier_dft_fold(const float* d_ts_e, const float* d_ts_v, const double* d_freqs,
+                      uint32_t nfreq, uint64_t seglen, uint64_t nseg, uint32_t nbins, double tsamp,
+                      double t_ref, float2* d_out, cudaStream_t s);
+// One merge level in the Fourier domain (kernels::ffa_complex_iter[_freq],
+// lib/kernels.cpp:942-1130): fractional shifts as phase rotations.
+void fourier_merge_level(const float2* d_in, float2* d_out, const void* d_coords, bool taylor,
+                         uint64_t ncur, uint64_t nprev, uint64_t nseg, uint32_t nbins,
+                         cudaStream_t s);
+// Batched real transforms of size nbins over nprof profiles (FFTW's r2c
+// unscaled; c2r scaled by 1 / nbins, as math::irfft_batch).
+void rfft_profiles(const float* d_in, float2* d_out, uint64_t nprof, uint32_t nbins,
+                   cudaStream_t s);
+void irfft_profiles(const float2* d_in, float* d_out, uint64_t nprof, uint32_t nbins,
+                    cudaStream_t s);
+
+struct FourierExec {
+    Plan plan;
+    int device;
+    uint32_t nbf;        // nbins / 2 + 1
+    bool lossy = false;  // level 0 by time-domain brute fold + real transform
+    StageProfiler prof;
+    DeviceBuffer status;  // brute-fold status word (lossy path)
+    DeviceBuffer coords;  // all levels, reference layout
+    DeviceBuffer freqs0;  // level-0 frequencies (double)
+    DeviceBuffer buf[2];  // complex ping-pong levels
+    DeviceBuffer tfold;   // lossy: level-0 time-domain fold
+    DeviceBuffer tfinal;  // final fold back in time (scores / search)
+    DeviceBuffer scores_tmp, compact_scratch;
+    std::unique_ptr<BruteFoldDevice> bf;  // lossy path only
+    ScoreParams sp{};
+
+    FourierExec(const Plan& p, int device, uint64_t nbins_min_lossy);
+    uint64_t fold_size(uint32_t level) const {
+        return plan.nsegments[level] * plan.ncoords[level] * 2 * nbf;
+    }
+    uint64_t fold_size_time(uint32_t level) const { return plan.fold_size(level); }
+    uint64_t device_bytes() const;
+    const void* level_coords(uint32_t l) const;
+    // Levels 0 .. n_levels - 1; the final level lands in final_out when given
+    // (else in a ping-pong buffer). Returns the final complex fold.
+    const float2* run_levels(const float* ts_e, const float* ts_v, float2* final_out,
+                             cudaStream_t s);
+    void execute(const float* ts_e, const float* ts_v, float2* fold, uint64_t len_complex,
+                 cudaStream_t s);
+    void execute_time(const float* ts_e, const float* ts_v, float* fold, uint64_t len,
+                      cudaStream_t s);
+    void scores(const float* ts_e, const float* ts_v, float* d_scores, uint64_t len,
+                cudaStream_t s);
+    void search(const float* ts_e, const float* ts_v, float snr_min, uint32_t* d_idx, float* d_snr,
+                uint64_t max_cands, uint64_t* d_count, cudaStream_t s);
+    std::vector<lk_stage_time> profile(cudaStream_t s);
+
+private:
+    void scores_into(const float* ts_e, const float* ts_v, float* d_scores, cudaStream_t s);
+};
+
+}  // namespace lk

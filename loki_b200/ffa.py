@@ -1,4 +1,6 @@
-"""FFA on the GPU: ``FFACUDA``, ``compute_ffa_time_cuda``, ``compute_ffa_scores_cuda``,
+"""FFA on the GPU: ``FFACUDA`` (time domain), ``FFACOMPLEXCUDA`` (Fourier
+domain), ``compute_ffa_time_cuda``, ``compute_ffa_fourier_cuda``,
+``compute_ffa_fourier_return_to_time_cuda`` and ``compute_ffa_scores_cuda``,
 mirroring ``libculoki.ffa`` of the reference (src/loki_python_cuda.cpp:148-204,
 lib/ffa_cuda.cu:609-692).
 
@@ -17,16 +19,9 @@ import numpy as np
 from . import _capi as C
 from . import _device as D
 from .configs import PulsarSearchConfig
-from .plans import FFAPlanTime
+from .plans import FFAPlanFourier, FFAPlanTime
 
 _STORAGE = {"fp32": C.LK_FP32, "float32": C.LK_FP32, "bf16": C.LK_BF16, "fp16": C.LK_FP16}
-
-
-def _check_time_domain(cfg: PulsarSearchConfig) -> None:
-    if cfg.use_fourier:
-        raise NotImplementedError(
-            "the Fourier-domain FFA is not implemented; construct the config with use_fourier=False"
-        )
 
 
 class FFACUDA:
@@ -266,12 +261,172 @@ def compute_ffa_time_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int = 
     return ffa.execute(np.asarray(ts_e, dtype=np.float32), np.asarray(ts_v, dtype=np.float32)), ffa.plan
 
 
+def compute_ffa_fourier_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int = 0, quiet: bool = False):
+    """Final-level Fourier-domain fold (complex64, flattened) and its plan
+    (reference compute_ffa_cuda<ComplexTypeCUDA>, lib/ffa_cuda.cu:629-650)."""
+    ffa = FFACOMPLEXCUDA(cfg, device_id)
+    return ffa.execute(np.asarray(ts_e, dtype=np.float32), np.asarray(ts_v, dtype=np.float32)), ffa.plan
+
+
+def compute_ffa_fourier_return_to_time_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int = 0,
+                                            quiet: bool = False):
+    """Final-level fold of the Fourier-domain FFA back in time and the
+    time-domain plan (reference lib/ffa_cuda.cu:651-670)."""
+    ffa = FFACOMPLEXCUDA(cfg, device_id)
+    fold = ffa.execute_time(np.asarray(ts_e, dtype=np.float32), np.asarray(ts_v, dtype=np.float32))
+    return fold, FFAPlanTime(cfg)
+
+
 def compute_ffa_scores_cuda(ts_e, ts_v, cfg: PulsarSearchConfig, device_id: int = 0, quiet: bool = False):
-    """Boxcar S/N of every final coordinate and width, and the plan
-    (reference lib/ffa_cuda.cu:671-692)."""
-    _check_time_domain(cfg)
+    """Boxcar S/N of every final coordinate and width, and the time-domain
+    plan (reference lib/ffa_cuda.cu:671-692): through the Fourier-domain FFA
+    when ``cfg.use_fourier`` (the reference default), else the time domain."""
+    e = np.asarray(ts_e, dtype=np.float32)
+    v = np.asarray(ts_v, dtype=np.float32)
+    if cfg.use_fourier:
+        ffa = FFACOMPLEXCUDA(cfg, device_id)
+        return ffa.scores(e, v), FFAPlanTime(cfg)
     ffa = FFACUDA(cfg, device_id)
-    return ffa.scores(np.asarray(ts_e, dtype=np.float32), np.asarray(ts_v, dtype=np.float32)), ffa.plan
+    return ffa.scores(e, v), ffa.plan
+
+
+class FFACOMPLEXCUDA:
+    """Fourier-domain FFA executor on one device (reference
+    ``FFACUDA<ComplexTypeCUDA>``, bound as ``FFACOMPLEXCUDA``): folds are
+    nbins // 2 + 1 complex harmonics, merges rotate them by the fractional
+    shifts, results return to time by an inverse real transform. Level 0 is
+    the direct transform of each segment for nbins <= cfg.nbins_min_lossy_bf,
+    else the time-domain brute fold and a real transform."""
+
+    def __init__(self, cfg: PulsarSearchConfig, device_id: int = 0):
+        D.require_cuda(device_id)
+        self._cfg = cfg
+        self._plan = FFAPlanFourier(cfg)
+        self._device = device_id
+        h = ctypes.c_void_p()
+        with D.torch().cuda.device(device_id):
+            C.check(C.lib().lk_fourier_create(cfg._plan_handle, device_id, int(cfg.nbins_min_lossy_bf),
+                                              ctypes.byref(h)))
+        self._h = h
+        nbf, fs, fst, ws = (ctypes.c_uint64() for _ in range(4))
+        lossy = ctypes.c_int()
+        C.check(C.lib().lk_fourier_info(h, ctypes.byref(nbf), ctypes.byref(fs), ctypes.byref(fst),
+                                        ctypes.byref(lossy), ctypes.byref(ws)))
+        self._fold_size, self._fold_size_time = int(fs.value), int(fst.value)
+        self.lossy = bool(lossy.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                C.lib().lk_fourier_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def plan(self) -> FFAPlanFourier:
+        return self._plan
+
+    @property
+    def device_id(self) -> int:
+        return self._device
+
+    @property
+    def workspace_bytes(self) -> int:
+        n = ctypes.c_uint64()
+        C.check(C.lib().lk_fourier_info(self._h, None, None, None, None, ctypes.byref(n)))
+        return int(n.value)
+
+    def _inputs(self, ts_e, ts_v):
+        n = self._cfg.nsamps
+        e = D.to_device_f32(ts_e, self._device)
+        v = D.to_device_f32(ts_v, self._device)
+        if e.numel() != n:
+            raise RuntimeError("FFA::execute: ts_e must have size nsamps")
+        if v.numel() != e.numel():
+            raise RuntimeError("FFA::execute: ts_v must have size nsamps")
+        return e, v
+
+    def execute(self, ts_e, ts_v, fold=None):
+        """Final complex fold [nseg, ncoords, 2, nbins_f], flattened. A host
+        ``fold`` of complex64 receives the complex fold; one of float32
+        receives the fold back in time (the reference's two overloads). A CUDA
+        tensor ``fold`` (float32, 2 * fold_size values) receives the complex
+        fold as interleaved (re, im). Without ``fold`` a complex64 array (host
+        inputs) or an interleaved float32 tensor (CUDA inputs) is returned."""
+        if fold is not None and not D.is_device_tensor(fold) and np.asarray(fold).dtype == np.float32:
+            out = self.execute_time(ts_e, ts_v)
+            np.copyto(np.asarray(fold).reshape(-1)[: out.size], out)
+            return fold
+        host = not (D.is_device_tensor(ts_e) and D.is_device_tensor(ts_v))
+        e, v = self._inputs(ts_e, ts_v)
+        n = self._fold_size
+        out = fold if D.is_device_tensor(fold) else D.empty_f32(2 * n, self._device)
+        if out.numel() < 2 * n:
+            raise RuntimeError("FFA::execute: fold must have size >= 2 * fold_size")
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_fourier_execute(self._h, D.ptr(e), D.ptr(v), D.ptr(out), out.numel() // 2,
+                                               D.stream_ptr(self._device)))
+        if fold is not None and not D.is_device_tensor(fold):
+            np.copyto(np.asarray(fold).reshape(-1)[:n], out[: 2 * n].cpu().numpy().view(np.complex64))
+            return fold
+        return out[: 2 * n].cpu().numpy().view(np.complex64) if host else out[: 2 * n]
+
+    def execute_time(self, ts_e, ts_v, fold=None):
+        """Final fold back in time [nseg, ncoords, 2, nbins] float32, flattened."""
+        host = not (D.is_device_tensor(ts_e) and D.is_device_tensor(ts_v))
+        e, v = self._inputs(ts_e, ts_v)
+        n = self._fold_size_time
+        out = fold if D.is_device_tensor(fold) else D.empty_f32(n, self._device)
+        if out.numel() < n:
+            raise RuntimeError("FFA::execute: fold must have size >= fold_size_time")
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_fourier_execute_time(self._h, D.ptr(e), D.ptr(v), D.ptr(out), out.numel(),
+                                                    D.stream_ptr(self._device)))
+        return out[:n].cpu().numpy() if host else out[:n]
+
+    def scores(self, ts_e, ts_v, out=None):
+        """Boxcar S/N [ncoords_final * n_widths] of the fold back in time."""
+        host = not (D.is_device_tensor(ts_e) and D.is_device_tensor(ts_v))
+        e, v = self._inputs(ts_e, ts_v)
+        nc = int(self._plan.ncoords[-1])
+        nw = self._cfg.n_scoring_widths
+        res = out if D.is_device_tensor(out) else D.empty_f32(nc * nw, self._device)
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_fourier_scores(self._h, D.ptr(e), D.ptr(v), D.ptr(res), res.numel(),
+                                              D.stream_ptr(self._device)))
+        return res[: nc * nw].cpu().numpy() if host else res
+
+    def search(self, ts_e, ts_v, snr_min: float | None = None, max_cands: int | None = None):
+        """Scores compacted to ``score >= snr_min`` in flat order. Returns
+        (indices, snrs, n_total_passing)."""
+        e, v = self._inputs(ts_e, ts_v)
+        thr = self._cfg.snr_min if snr_min is None else float(snr_min)
+        cap = self._cfg.max_passing_candidates if max_cands is None else int(max_cands)
+        t = D.torch()
+        idx = t.empty(cap, dtype=t.int32, device=f"cuda:{self._device}")
+        snr = D.empty_f32(cap, self._device)
+        cnt = t.zeros(1, dtype=t.int64, device=f"cuda:{self._device}")
+        with t.cuda.device(self._device):
+            C.check(C.lib().lk_fourier_search(self._h, D.ptr(e), D.ptr(v), thr, idx.data_ptr(), D.ptr(snr), cap,
+                                              cnt.data_ptr(), D.stream_ptr(self._device)))
+        total = int(cnt.item())
+        k = min(total, cap)
+        return idx[:k].cpu().numpy().view(np.uint32), snr[:k].cpu().numpy(), total
+
+    def set_profiling(self, enable: bool = True) -> None:
+        C.check(C.lib().lk_fourier_set_profiling(self._h, 1 if enable else 0))
+
+    def profile(self) -> list[dict]:
+        arr = (C.LkStageTime * 128)()
+        n = ctypes.c_uint32()
+        C.check(C.lib().lk_fourier_get_profile(self._h, D.stream_ptr(self._device), arr, 128, ctypes.byref(n)))
+        return [
+            {"stage": C.STAGE_NAMES.get(arr[i].kind, str(arr[i].kind)), "level": arr[i].level,
+             "launches": arr[i].launches, "ms": float(arr[i].ms), "bytes": int(arr[i].bytes)}
+            for i in range(min(n.value, 128))
+        ]
 
 
 from .sweep import FFAFreqSweepCUDA  # noqa: E402  (the reference binds it in the ffa submodule)

@@ -65,3 +65,27 @@ def compute_brute_fold_time_cuda(ts_e, ts_v, freq_arr, segment_len: int, nbins: 
     ts_e = np.asarray(ts_e, dtype=np.float32)
     bf = BruteFoldCUDA(freq_arr, segment_len, nbins, ts_e.size, tsamp, t_ref, device_id)
     return bf.execute(ts_e, np.asarray(ts_v, dtype=np.float32))
+
+
+def compute_brute_fold_fourier_cuda(ts_e, ts_v, freq_arr, segment_len: int, nbins: int, tsamp: float,
+                                    t_ref: float = 0.0, device_id: int = 0):
+    """Direct transform of each segment at each frequency, [nseg, nfreqs, 2,
+    nbins // 2 + 1] complex64 flattened (reference
+    ``compute_brute_fold_fourier_cuda``, src/loki_python_cuda.cpp:133-146)."""
+    D.require_cuda(device_id)
+    host = not (D.is_device_tensor(ts_e) and D.is_device_tensor(ts_v))
+    f = np.ascontiguousarray(freq_arr, dtype=np.float64).ravel()
+    e = D.to_device_f32(ts_e, device_id)
+    v = D.to_device_f32(ts_v, device_id)
+    if e.numel() != v.numel():
+        raise RuntimeError("BruteFold::execute: ts_e and ts_v must have the same size")
+    nseg = e.numel() // int(segment_len) if segment_len else 0
+    n = nseg * f.size * 2 * (int(nbins) // 2 + 1)
+    out = D.empty_f32(2 * max(n, 1), device_id)
+    with D.torch().cuda.device(device_id):
+        C.check(C.lib().lk_fourier_brute_fold(D.ptr(e), D.ptr(v), e.numel(), f.ctypes.data, f.size,
+                                              int(segment_len), int(nbins), float(tsamp), float(t_ref),
+                                              D.ptr(out), n, device_id, D.stream_ptr(device_id)))
+    if host:
+        return out[: 2 * n].cpu().numpy().view(np.complex64)
+    return out[: 2 * n]

@@ -193,5 +193,50 @@ class FFAPlanTime:
         return self._resolve(device_id)
 
 
+class FFAPlanFourier(FFAPlanTime):
+    """FFAPlan<ComplexType> (reference ``libloki.plans.FFAPlanFourier``): the
+    same levels and coordinates, folds of nbins_f = nbins // 2 + 1 complex
+    harmonics; the *_time sizes are those of the fold back in time."""
+
+    @property
+    def nbins_f(self) -> int:
+        return int(self._info.nbins) // 2 + 1
+
+    def _fourier_size(self, time_size: int) -> int:
+        return time_size // int(self._info.nbins) * self.nbins_f
+
+    @property
+    def fold_shapes(self) -> list[np.ndarray]:
+        return [np.array([*s[:-1], self.nbins_f], dtype=np.uint64) for s in super().fold_shapes]
+
+    @property
+    def fold_shapes_time(self) -> list[np.ndarray]:
+        return super().fold_shapes
+
+    @property
+    def brute_fold_size(self) -> int:
+        return self._fourier_size(int(self._info.brute_fold_size))
+
+    @property
+    def fold_size(self) -> int:
+        return self._fourier_size(int(self._info.fold_size))
+
+    @property
+    def fold_size_time(self) -> int:
+        return int(self._info.fold_size)
+
+    @property
+    def buffer_size(self) -> int:
+        return self._fourier_size(int(self._info.buffer_size))
+
+    @property
+    def buffer_size_time(self) -> int:
+        return 2 * self.buffer_size
+
+    @property
+    def buffer_memory_usage(self) -> float:
+        return float(np.float32(2 * self.buffer_size * 8) / np.float32(1 << 30))
+
+
 # The reference binds the region planner in the plans submodule.
 from .sweep import FFARegionPlannerTime, generate_ffa_regions  # noqa: E402

@@ -129,6 +129,12 @@ def lib() -> ctypes.CDLL:
         L.lko_cheby_transform.argtypes = [vp, vp, u64, u32, f64, f64, f64, f64]
         L.lko_cheby_branch.argtypes = [vp, u64, u32, f64, f64, f64, f64, u64, f64, u64, vp, vp, u64, vp]
         L.lko_cheby_resolve.argtypes = [vp, vp, u64, vp, vp, vp]
+        L.lko_fourier_brute_fold.argtypes = [vp, vp, u64, vp, u64, u64, u64, f64, f64, vp]
+        L.lko_fourier_merge.argtypes = [vp, vp, vp, ctypes.c_int, u64, u64, u64, u64]
+        L.lko_irfft.argtypes = [vp, vp, u64, u64]
+        L.lko_rfft.argtypes = [vp, vp, u64, u64]
+        L.lko_ffa_fourier.argtypes = [vp, vp, vp, u32, u64, vp]
+        L.lko_ffa_fourier_scores64.argtypes = [vp, vp, vp, u64, vp, u64, vp]
         _lib = L
     return _lib
 
@@ -289,6 +295,70 @@ def ffa_scores64(plan: OraclePlan, ts_e, ts_v, widths) -> np.ndarray:
     w = np.ascontiguousarray(widths, dtype=np.uint64)
     out = np.zeros((int(plan.ncoords[-1]), w.size), dtype=np.float64)
     _check(lib().lko_ffa_scores64(ctypes.byref(plan.raw), _p(ts_e), _p(ts_v), _p(w), w.size, _p(out)))
+    return out
+
+
+# Fourier-domain FFA (FFA<ComplexType>), every sum in double. Complex
+# results are complex128 arrays; folds [nseg, ncoords, 2, nbins // 2 + 1].
+NBINS_MIN_LOSSY = 64  # PulsarSearchConfig's nbins_min_lossy_bf default
+
+
+def fourier_brute_fold(ts_e, ts_v, freqs, segment_len, nbins, tsamp, t_ref=0.0) -> np.ndarray:
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+    nseg = ts_e.size // segment_len
+    nbf = nbins // 2 + 1
+    out = np.zeros((nseg, freqs.size, 2, nbf), dtype=np.complex128)
+    _check(lib().lko_fourier_brute_fold(_p(ts_e), _p(ts_v), ts_e.size, _p(freqs), freqs.size, segment_len, nbins,
+                                        tsamp, t_ref, _p(out)))
+    return out
+
+
+def fourier_merge(fold_in, coords, ncur, nprev, nseg, nbins) -> np.ndarray:
+    fold_in = np.ascontiguousarray(fold_in, dtype=np.complex128)
+    coords = np.ascontiguousarray(coords)
+    taylor = 1 if coords.dtype == COORD_DTYPE else 0
+    out = np.zeros((nseg, ncur, 2, nbins // 2 + 1), dtype=np.complex128)
+    lib().lko_fourier_merge(_p(fold_in), _p(out), _p(coords), taylor, ncur, nprev, nseg, nbins)
+    return out
+
+
+def irfft(x, n) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    nprof = x.size // (n // 2 + 1)
+    out = np.zeros(x.shape[:-1] + (n,), dtype=np.float64)
+    lib().lko_irfft(_p(x), _p(out), nprof, n)
+    return out
+
+
+def rfft(x, n) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    nprof = x.size // n
+    out = np.zeros(x.shape[:-1] + (n // 2 + 1,), dtype=np.complex128)
+    lib().lko_rfft(_p(x), _p(out), nprof, n)
+    return out
+
+
+def ffa_fourier(plan: OraclePlan, ts_e, ts_v, level: int | None = None,
+                nbins_min_lossy: int = NBINS_MIN_LOSSY) -> np.ndarray:
+    l = plan.n_levels - 1 if level is None else level
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    nbf = plan.nbins // 2 + 1
+    out = np.zeros((int(plan.nsegments[l]), int(plan.ncoords[l]), 2, nbf), dtype=np.complex128)
+    _check(lib().lko_ffa_fourier(ctypes.byref(plan.raw), _p(ts_e), _p(ts_v), l, nbins_min_lossy, _p(out)))
+    return out
+
+
+def ffa_fourier_scores64(plan: OraclePlan, ts_e, ts_v, widths,
+                         nbins_min_lossy: int = NBINS_MIN_LOSSY) -> np.ndarray:
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    w = np.ascontiguousarray(widths, dtype=np.uint64)
+    out = np.zeros((int(plan.ncoords[-1]), w.size), dtype=np.float64)
+    _check(lib().lko_ffa_fourier_scores64(ctypes.byref(plan.raw), _p(ts_e), _p(ts_v), nbins_min_lossy, _p(w),
+                                          w.size, _p(out)))
     return out
 
 

@@ -707,6 +707,48 @@ static void merge64(const double* in, double* out, const void* coords, int taylo
     }
 }
 
+/* snr_boxcar_impl<Is3D=true> (lib/score.cpp:95-172) in double: per profile
+ * x_j = E_j / sqrt(V_j), circular prefix sums, the largest window sum of
+ * each width and (h + b) * dmax - b * sum(x). folds [nc][2][nbins]. */
+static void score64(const double* a, uint64_t nc, uint64_t nbins, const uint64_t* widths,
+                    uint64_t nw, double* scores) {
+    uint64_t wmax = 0;
+    double hb[LKO_MAX_WIDTHS], bb[LKO_MAX_WIDTHS];
+    for (uint64_t k = 0; k < nw; ++k) {
+        const double w = (double)widths[k];
+        const double h = sqrt(((double)nbins - w) / ((double)nbins * w));
+        bb[k] = w * h / ((double)nbins - w);
+        hb[k] = h + bb[k];
+        wmax = widths[k] > wmax ? widths[k] : wmax;
+    }
+#pragma omp parallel
+    {
+        double* ps = (double*)malloc(sizeof(double) * (nbins + wmax));
+#pragma omp for schedule(static)
+        for (int64_t ci = 0; ci < (int64_t)nc; ++ci) {
+            const double* e = a + (uint64_t)ci * 2 * nbins;
+            const double* v = e + nbins;
+            double acc = 0.0;
+            for (uint64_t j = 0; j < nbins; ++j) {
+                acc += e[j] / sqrt(v[j]);
+                ps[j] = acc;
+            }
+            for (uint64_t k = 0; k < wmax; ++k) {
+                ps[nbins + k] = ps[k] + acc;
+            }
+            for (uint64_t k = 0; k < nw; ++k) {
+                double dm = -DBL_MAX;
+                for (uint64_t j = 0; j < nbins; ++j) {
+                    const double d = ps[j + widths[k]] - ps[j];
+                    dm = d > dm ? d : dm;
+                }
+                scores[(uint64_t)ci * nw + k] = hb[k] * dm - bb[k] * acc;
+            }
+        }
+        free(ps);
+    }
+}
+
 int lko_ffa_scores64(const lko_plan* p, const float* ts_e, const float* ts_v,
                      const uint64_t* widths, uint64_t nw, double* scores) {
     if (p->n_levels < 2 || p->nsegments[p->n_levels - 1] != 1) {
@@ -760,44 +802,7 @@ int lko_ffa_scores64(const lko_plan* p, const float* ts_e, const float* ts_v,
         a = b;
         b = t;
     }
-    {
-        uint64_t wmax = 0;
-        double hb[LKO_MAX_WIDTHS], bb[LKO_MAX_WIDTHS];
-        for (uint64_t k = 0; k < nw; ++k) {
-            const double w = (double)widths[k];
-            const double h = sqrt(((double)nbins - w) / ((double)nbins * w));
-            bb[k] = w * h / ((double)nbins - w);
-            hb[k] = h + bb[k];
-            wmax = widths[k] > wmax ? widths[k] : wmax;
-        }
-        const uint64_t nc = p->ncoords[p->n_levels - 1];
-#pragma omp parallel
-        {
-            double* ps = (double*)malloc(sizeof(double) * (nbins + wmax));
-#pragma omp for schedule(static)
-            for (int64_t ci = 0; ci < (int64_t)nc; ++ci) {
-                const double* e = a + (uint64_t)ci * 2 * nbins;
-                const double* v = e + nbins;
-                double acc = 0.0;
-                for (uint64_t j = 0; j < nbins; ++j) {
-                    acc += e[j] / sqrt(v[j]);
-                    ps[j] = acc;
-                }
-                for (uint64_t k = 0; k < wmax; ++k) {
-                    ps[nbins + k] = ps[k] + acc;
-                }
-                for (uint64_t k = 0; k < nw; ++k) {
-                    double dm = -DBL_MAX;
-                    for (uint64_t j = 0; j < nbins; ++j) {
-                        const double d = ps[j + widths[k]] - ps[j];
-                        dm = d > dm ? d : dm;
-                    }
-                    scores[(uint64_t)ci * nw + k] = hb[k] * dm - bb[k] * acc;
-                }
-            }
-            free(ps);
-        }
-    }
+    score64(a, p->ncoords[p->n_levels - 1], nbins, widths, nw, scores);
 done:
     free(freqs);
     free(map);
@@ -2493,5 +2498,279 @@ done:
     free(beam_prev);
     free(beam_cur);
     free(neigh);
+    return rc;
+}
+
+/* ======================================================================== */
+/* Fourier-domain FFA (FFA<ComplexType>, lib/ffa.cpp:99-135,170-240), every  */
+/* sum and phasor in double. Complex folds are [nseg][ncoords][2][nbins_f]   */
+/* with nbins_f = nbins / 2 + 1, stored as interleaved (re, im) doubles.      */
+/* ======================================================================== */
+
+static const double kTwoPi = 6.283185307179586476925286766559;
+
+/* exp(-2 pi i * cycles), the angle taken modulo one cycle first. */
+static void unit_phasor(double cycles, double* re, double* im) {
+    const double fr = cycles - floor(cycles);
+    *re = cos(kTwoPi * fr);
+    *im = -sin(kTwoPi * fr);
+}
+
+/* kernels::brute_fold_ts_complex (lib/kernels.cpp:1156-1242) with
+ * brute_fold_segment_complex (:582-720): harmonic m of segment s at
+ * frequency f is sum_k x[s * L + k] * exp(-2 pi i m f t_k) with
+ * t_k = k * tsamp - t_ref (the DC term m = 0 is the plain sum). The
+ * reference forms the phasor in float and raises it to the m-th power by a
+ * recurrence; here the phase is reduced modulo one cycle in double and the
+ * powers are taken in double. */
+int lko_fourier_brute_fold(const float* ts_e, const float* ts_v, uint64_t nsamps,
+                           const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                           uint64_t nbins, double tsamp, double t_ref, double* out) {
+    if (segment_len == 0 || nbins < 2 || nfreqs == 0) {
+        return fail("lko_fourier_brute_fold: empty segment, frequency list or nbins < 2");
+    }
+    const uint64_t nbf = nbins / 2 + 1;
+    const uint64_t nseg = nsamps / segment_len;
+#pragma omp parallel
+    {
+        double* acc = (double*)malloc(sizeof(double) * 4 * nbf);
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t sf = 0; sf < (int64_t)(nseg * nfreqs); ++sf) {
+            const uint64_t s = (uint64_t)sf / nfreqs, f = (uint64_t)sf % nfreqs;
+            memset(acc, 0, sizeof(double) * 4 * nbf);
+            const float* e = ts_e + s * segment_len;
+            const float* v = ts_v + s * segment_len;
+            for (uint64_t k = 0; k < segment_len; ++k) {
+                const double t = (double)k * tsamp - t_ref;
+                double zr, zi;
+                unit_phasor(freqs[f] * t, &zr, &zi);
+                const double xe = (double)e[k], xv = (double)v[k];
+                double pr = 1.0, pi = 0.0;
+                for (uint64_t m = 0; m < nbf; ++m) {
+                    acc[4 * m + 0] += xe * pr;
+                    acc[4 * m + 1] += xe * pi;
+                    acc[4 * m + 2] += xv * pr;
+                    acc[4 * m + 3] += xv * pi;
+                    const double nr = pr * zr - pi * zi;
+                    pi = pr * zi + pi * zr;
+                    pr = nr;
+                }
+            }
+            double* oe = out + (s * nfreqs + f) * 4 * nbf;
+            double* ov = oe + 2 * nbf;
+            for (uint64_t m = 0; m < nbf; ++m) {
+                oe[2 * m] = acc[4 * m + 0];
+                oe[2 * m + 1] = acc[4 * m + 1];
+                ov[2 * m] = acc[4 * m + 2];
+                ov[2 * m + 1] = acc[4 * m + 3];
+            }
+        }
+        free(acc);
+    }
+    return 0;
+}
+
+/* kernels::ffa_complex_iter / ffa_complex_iter_freq (lib/kernels.cpp:
+ * 942-1130, 1283-1326) with shift_add_complex_recurrence_binary / _linear
+ * (:241-453): out[k] = tail[k] * exp(-2 pi i k shift_tail / nbins)
+ * + head[k] * exp(-2 pi i k shift_head / nbins) for E and V, the shifts
+ * fractional (the frequency-only table has no tail shift). */
+void lko_fourier_merge(const double* in, double* out, const void* coords, int taylor,
+                       uint64_t ncur, uint64_t nprev, uint64_t nseg, uint64_t nbins) {
+    const uint64_t nbf = nbins / 2 + 1;
+    const uint64_t fs = 4 * nbf; /* doubles per (E, V) row pair */
+#pragma omp parallel for schedule(static)
+    for (int64_t sc = 0; sc < (int64_t)(nseg * ncur); ++sc) {
+        const uint64_t s = (uint64_t)sc / ncur, c = (uint64_t)sc % ncur;
+        uint64_t it, ih;
+        double st, sh;
+        if (taylor) {
+            const lko_coord* cc = (const lko_coord*)coords + c;
+            it = cc->i_tail;
+            ih = cc->i_head;
+            st = (double)cc->shift_tail;
+            sh = (double)cc->shift_head;
+        } else {
+            const lko_coord_freq* cc = (const lko_coord_freq*)coords + c;
+            it = ih = cc->idx;
+            st = 0.0;
+            sh = (double)cc->shift;
+        }
+        const double* tail = in + ((2 * s) * nprev + it) * fs;
+        const double* head = in + ((2 * s + 1) * nprev + ih) * fs;
+        double* o = out + (s * ncur + c) * fs;
+        for (uint64_t k = 0; k < nbf; ++k) {
+            double tr, ti, hr, hi;
+            unit_phasor((double)k * st / (double)nbins, &tr, &ti);
+            unit_phasor((double)k * sh / (double)nbins, &hr, &hi);
+            for (uint64_t r = 0; r < 2; ++r) {
+                const double* a = tail + r * 2 * nbf + 2 * k;
+                const double* b = head + r * 2 * nbf + 2 * k;
+                double* d = o + r * 2 * nbf + 2 * k;
+                d[0] = (a[0] * tr - a[1] * ti) + (b[0] * hr - b[1] * hi);
+                d[1] = (a[0] * ti + a[1] * tr) + (b[0] * hi + b[1] * hr);
+            }
+        }
+    }
+}
+
+/* math::irfft_batch (lib/fft.cpp:503-552): FFTW's c2r transform of size n
+ * (the imaginary parts of the DC and, for even n, the Nyquist term are not
+ * used) scaled by 1 / n. in [nprof][n/2 + 1] complex, out [nprof][n]. */
+void lko_irfft(const double* in, double* out, uint64_t nprof, uint64_t n) {
+    const uint64_t nbf = n / 2 + 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < (int64_t)nprof; ++p) {
+        const double* x = in + (uint64_t)p * 2 * nbf;
+        double* y = out + (uint64_t)p * n;
+        for (uint64_t j = 0; j < n; ++j) {
+            double acc = x[0];
+            for (uint64_t m = 1; m < nbf; ++m) {
+                double c, s;
+                unit_phasor((double)((m * j) % n) / (double)n, &c, &s);
+                /* Re(X_m exp(+2 pi i m j / n)) = Re X c + Im X s  (s = -sin) */
+                const double re = x[2 * m] * c + x[2 * m + 1] * s;
+                acc += (2 * m == n) ? re : 2.0 * re;
+            }
+            y[j] = acc / (double)n;
+        }
+    }
+}
+
+/* math::rfft_batch (lib/fft.cpp:375-415): FFTW's r2c transform of size n,
+ * unscaled. in [nprof][n], out [nprof][n/2 + 1] complex. */
+void lko_rfft(const double* in, double* out, uint64_t nprof, uint64_t n) {
+    const uint64_t nbf = n / 2 + 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < (int64_t)nprof; ++p) {
+        const double* x = in + (uint64_t)p * n;
+        double* y = out + (uint64_t)p * 2 * nbf;
+        for (uint64_t m = 0; m < nbf; ++m) {
+            double re = 0.0, im = 0.0;
+            for (uint64_t j = 0; j < n; ++j) {
+                double c, s;
+                unit_phasor((double)((m * j) % n) / (double)n, &c, &s);
+                re += x[j] * c;
+                im += x[j] * s;
+            }
+            y[2 * m] = re;
+            y[2 * m + 1] = im;
+        }
+    }
+}
+
+/* FFA<ComplexType>::execute (lib/ffa.cpp:75-97, 242-310): level-0 fold by
+ * the direct transform, or for nbins > nbins_min_lossy by the time-domain
+ * brute fold (float sums, as lko_brute_fold) and a real transform
+ * (initialize, :201-240); then every merge level up to level_out. out holds
+ * the level's complex fold. */
+int lko_ffa_fourier(const lko_plan* p, const float* ts_e, const float* ts_v, uint32_t level_out,
+                    uint64_t nbins_min_lossy, double* fold_out) {
+    if (p->n_levels < 2) {
+        return fail("FFA::execute_unified: levels must be greater than or equal to 2");
+    }
+    if (level_out >= p->n_levels) {
+        return fail("level_out out of range");
+    }
+    const uint32_t np = p->nparams;
+    const uint64_t nbins = p->nbins;
+    const uint64_t nbf = nbins / 2 + 1;
+    const uint64_t nfreq0 = p->param_counts[0][np - 1];
+    uint64_t cmax = 0;
+    for (uint32_t l = 0; l < p->n_levels; ++l) {
+        const uint64_t c = p->nsegments[l] * p->ncoords[l] * 4 * nbf;
+        cmax = c > cmax ? c : cmax;
+    }
+    double* freqs = (double*)malloc(sizeof(double) * nfreq0);
+    double* a = (double*)malloc(sizeof(double) * cmax);
+    double* b = (double*)malloc(sizeof(double) * cmax);
+    void* coords = malloc((np == 1 ? sizeof(lko_coord_freq) : sizeof(lko_coord)) * p->coord_size);
+    float* tfold = NULL;
+    double* tfold64 = NULL;
+    int rc = 0;
+    if (freqs == NULL || a == NULL || b == NULL || coords == NULL) {
+        rc = fail("out of memory");
+        goto done;
+    }
+    lko_range_param(p->limits[2 * (np - 1)], p->limits[2 * (np - 1) + 1], p->dparams[0][np - 1], freqs,
+                    nfreq0);
+    const double t_ref = (np == 1) ? 0.0 : p->tsegments[0] / 2.0;
+    rc = (np == 1) ? lko_resolve_freq(p, (lko_coord_freq*)coords)
+                   : lko_resolve_taylor(p, (lko_coord*)coords);
+    if (rc != 0) {
+        goto done;
+    }
+    if (nbins > nbins_min_lossy) {
+        const uint64_t nprof = p->nsegments[0] * nfreq0 * 2;
+        tfold = (float*)malloc(sizeof(float) * nprof * nbins);
+        tfold64 = (double*)malloc(sizeof(double) * nprof * nbins);
+        if (tfold == NULL || tfold64 == NULL) {
+            rc = fail("out of memory");
+            goto done;
+        }
+        rc = lko_brute_fold(ts_e, ts_v, p->nsamps, freqs, nfreq0, p->segment_lens[0], nbins, p->tsamp,
+                            t_ref, tfold);
+        if (rc != 0) {
+            goto done;
+        }
+        for (uint64_t i = 0; i < nprof * nbins; ++i) {
+            tfold64[i] = (double)tfold[i];
+        }
+        lko_rfft(tfold64, a, nprof, nbins);
+    } else {
+        rc = lko_fourier_brute_fold(ts_e, ts_v, p->nsamps, freqs, nfreq0, p->segment_lens[0], nbins,
+                                    p->tsamp, t_ref, a);
+        if (rc != 0) {
+            goto done;
+        }
+    }
+    for (uint32_t l = 1; l <= level_out; ++l) {
+        const void* cl = (np == 1) ? (const void*)((const lko_coord_freq*)coords + p->ncoords_offsets[l])
+                                   : (const void*)((const lko_coord*)coords + p->ncoords_offsets[l]);
+        lko_fourier_merge(a, b, cl, np > 1, p->ncoords[l], p->ncoords[l - 1], p->nsegments[l], nbins);
+        double* t = a;
+        a = b;
+        b = t;
+    }
+    memcpy(fold_out, a, sizeof(double) * p->nsegments[level_out] * p->ncoords[level_out] * 4 * nbf);
+done:
+    free(freqs);
+    free(a);
+    free(b);
+    free(coords);
+    free(tfold);
+    free(tfold64);
+    return rc;
+}
+
+/* compute_ffa_scores with use_fourier (lib/ffa.cpp:425-466): the final
+ * complex fold, back to time by the inverse real transform, and the boxcar
+ * S/N of every final cell and width, all in double. scores [ncoords][nw]. */
+int lko_ffa_fourier_scores64(const lko_plan* p, const float* ts_e, const float* ts_v,
+                             uint64_t nbins_min_lossy, const uint64_t* widths, uint64_t nw,
+                             double* scores) {
+    if (p->n_levels < 2 || p->nsegments[p->n_levels - 1] != 1) {
+        return fail("compute_ffa_scores: nsegments must be 1 for scores");
+    }
+    if (nw == 0 || nw > LKO_MAX_WIDTHS) {
+        return fail("lko_ffa_fourier_scores64: number of widths out of range");
+    }
+    const uint64_t nbins = p->nbins;
+    const uint64_t nbf = nbins / 2 + 1;
+    const uint64_t nc = p->ncoords[p->n_levels - 1];
+    double* cf = (double*)malloc(sizeof(double) * nc * 4 * nbf);
+    double* tf = (double*)malloc(sizeof(double) * nc * 2 * nbins);
+    int rc = 0;
+    if (cf == NULL || tf == NULL) {
+        rc = fail("out of memory");
+    } else {
+        rc = lko_ffa_fourier(p, ts_e, ts_v, p->n_levels - 1, nbins_min_lossy, cf);
+        if (rc == 0) {
+            lko_irfft(cf, tf, nc * 2, nbins);
+            score64(tf, nc, nbins, widths, nw, scores);
+        }
+    }
+    free(cf);
+    free(tf);
     return rc;
 }

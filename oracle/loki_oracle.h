@@ -295,6 +295,21 @@ uint32_t lko_dts_resample(uint32_t range, uint32_t i, uint32_t tid2, uint32_t st
 int lko_dts_run(const lko_dts_config* cfg, uint32_t thres_neigh, uint32_t stages_run,
                 lko_dts_state* states);
 
+/* Fourier-domain FFA in double (FFA<ComplexType>). Complex arrays are
+ * interleaved (re, im) doubles; folds [nseg][ncoords][2][nbins/2 + 1]. */
+int lko_fourier_brute_fold(const float* ts_e, const float* ts_v, uint64_t nsamps,
+                           const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                           uint64_t nbins, double tsamp, double t_ref, double* out);
+void lko_fourier_merge(const double* in, double* out, const void* coords, int taylor,
+                       uint64_t ncur, uint64_t nprev, uint64_t nseg, uint64_t nbins);
+void lko_irfft(const double* in, double* out, uint64_t nprof, uint64_t n);
+void lko_rfft(const double* in, double* out, uint64_t nprof, uint64_t n);
+int lko_ffa_fourier(const lko_plan* p, const float* ts_e, const float* ts_v, uint32_t level_out,
+                    uint64_t nbins_min_lossy, double* fold_out);
+int lko_ffa_fourier_scores64(const lko_plan* p, const float* ts_e, const float* ts_v,
+                             uint64_t nbins_min_lossy, const uint64_t* widths, uint64_t nw,
+                             double* scores);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,6 +80,13 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
         L.lkref_resolve_freq.argtypes = [vp, vp, u64]
         L.lkref_resolve.argtypes = [vp, vp, u64]
         L.lkref_brute_fold.argtypes = [vp, vp, u64, vp, u64, u64, u64, f64, f64, ctypes.c_int, vp, u64]
+        L.lkref_brute_fold_complex.argtypes = [vp, vp, u64, vp, u64, u64, u64, f64, f64, ctypes.c_int, vp, u64]
+        L.lkref_fourier_create.argtypes = [vp, vp]
+        L.lkref_fourier_destroy.argtypes = [vp]
+        L.lkref_fourier_info.argtypes = [vp, vp, vp, vp]
+        L.lkref_fourier_execute.argtypes = [vp, vp, vp, u64, vp, u64]
+        L.lkref_fourier_execute_time.argtypes = [vp, vp, vp, u64, vp, u64]
+        L.lkref_fourier_scores.argtypes = [vp, vp, vp, u64, vp, u64]
         L.lkref_snr_boxcar_3d.argtypes = [vp, u64, u64, vp, u64, ctypes.c_int, vp]
         L.lkref_snr_boxcar_3d_max.argtypes = [vp, u64, u64, vp, u64, ctypes.c_int, vp]
         L.lkref_box_widths.argtypes = [u64, f64, f64, vp, u64, vp]
@@ -194,6 +201,60 @@ class RefFFA:
         if getattr(self, "_h", None):
             self._lib.lkref_ffa_destroy(self._h)
             self._h = None
+
+
+class RefFourier:
+    """algorithms::FFA<ComplexType> of the reference (the Fourier-domain FFA)."""
+
+    def __init__(self, cfg: RefCfg, kind: str = "parity"):
+        self._lib = lib(kind)
+        self.cfg = cfg
+        self._h = vp()
+        _check(self._lib, self._lib.lkref_fourier_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+        buf, fs, fst = u64(), u64(), u64()
+        _check(self._lib, self._lib.lkref_fourier_info(self._h, ctypes.byref(buf), ctypes.byref(fs),
+                                                       ctypes.byref(fst)))
+        self.buffer_size, self.fold_size, self.fold_size_time = buf.value, fs.value, fst.value
+        self._fold = np.zeros(self.buffer_size, dtype=np.complex64)
+        self._tfold = np.zeros(2 * self.buffer_size, dtype=np.float32)
+
+    def execute(self, ts_e, ts_v) -> np.ndarray:
+        """Final complex fold (a view of an internal buffer, valid until the next call)."""
+        _check(self._lib, self._lib.lkref_fourier_execute(self._h, _p(ts_e), _p(ts_v), ts_e.size, _p(self._fold),
+                                                          self._fold.size))
+        return self._fold[: self.fold_size]
+
+    def execute_time(self, ts_e, ts_v) -> np.ndarray:
+        """Final fold back in time (a view of an internal buffer)."""
+        _check(self._lib, self._lib.lkref_fourier_execute_time(self._h, _p(ts_e), _p(ts_v), ts_e.size,
+                                                               _p(self._tfold), self._tfold.size))
+        return self._tfold[: self.fold_size_time]
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.lkref_fourier_destroy(self._h)
+            self._h = None
+
+
+def fourier_scores(cfg: RefCfg, ts_e, ts_v, n_scores: int, kind: str = "parity") -> np.ndarray:
+    """compute_ffa_scores with use_fourier = true: [ncoords * n_widths] float32."""
+    L = lib(kind)
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    out = np.zeros(n_scores, dtype=np.float32)
+    _check(L, L.lkref_fourier_scores(ctypes.byref(cfg), _p(ts_e), _p(ts_v), ts_e.size, _p(out), out.size))
+    return out
+
+
+def brute_fold_complex(ts_e, ts_v, freqs, segment_len, nbins, tsamp, t_ref=0.0, nthreads=1) -> np.ndarray:
+    L = lib()
+    ts_e = np.ascontiguousarray(ts_e, dtype=np.float32)
+    ts_v = np.ascontiguousarray(ts_v, dtype=np.float32)
+    freqs = np.ascontiguousarray(freqs, dtype=np.float64)
+    out = np.zeros((ts_e.size // segment_len, freqs.size, 2, nbins // 2 + 1), dtype=np.complex64)
+    _check(L, L.lkref_brute_fold_complex(_p(ts_e), _p(ts_v), ts_e.size, _p(freqs), freqs.size, segment_len, nbins,
+                                         tsamp, t_ref, nthreads, _p(out), out.size))
+    return out
 
 
 def resolve(cfg: RefCfg, coord_size: int) -> np.ndarray:

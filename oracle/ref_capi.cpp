@@ -131,7 +131,7 @@ const char* lkref_last_error(void) { return g_last_error.c_str(); }
 
 int lkref_max_threads(void) { return omp_get_max_threads(); }
 
-static loki::search::PulsarSearchConfig make_cfg(const lkref_cfg* c) {
+static loki::search::PulsarSearchConfig make_cfg(const lkref_cfg* c, bool use_fourier = false) {
     std::vector<loki::ParamLimit> lims(c->nparams);
     for (uint32_t i = 0; i < c->nparams; ++i) {
         lims[i] = {.min = c->limits[2 * i], .max = c->limits[(2 * i) + 1]};
@@ -145,7 +145,7 @@ static loki::search::PulsarSearchConfig make_cfg(const lkref_cfg* c) {
         bf = c->bseg_ffa;
     }
     return {c->nsamps, c->tsamp, c->nbins, c->eta, lims, c->ducy_max, c->wtsp,
-            /*use_fourier=*/false, c->nthreads,
+            use_fourier, c->nthreads,
             /*max_process_memory_gb=*/8.0, /*octave_scale=*/2.0,
             /*nbins_max=*/1024, /*nbins_min_lossy_bf=*/64, bb, bf};
 }
@@ -217,6 +217,89 @@ int lkref_ffa_execute(lkref_ffa* h,
         h->ffa->execute(std::span<const float>(ts_e, nsamps),
                         std::span<const float>(ts_v, nsamps),
                         std::span<float>(fold, fold_len));
+    });
+}
+
+// ---- Fourier-domain FFA (FFA<ComplexType>, lib/ffa.cpp) ----------------
+struct lkref_fourier {
+    std::unique_ptr<loki::search::PulsarSearchConfig> cfg;
+    std::unique_ptr<loki::algorithms::FFA<loki::ComplexType>> ffa;
+};
+
+int lkref_fourier_create(const lkref_cfg* c, lkref_fourier** out) {
+    return guarded([&] {
+        auto h = std::make_unique<lkref_fourier>();
+        h->cfg = std::make_unique<loki::search::PulsarSearchConfig>(make_cfg(c, true));
+        h->ffa = std::make_unique<loki::algorithms::FFA<loki::ComplexType>>(*h->cfg, false);
+        *out   = h.release();
+    });
+}
+
+void lkref_fourier_destroy(lkref_fourier* h) { delete h; }
+
+// Complex counts: buffer (ping-pong side), final fold; final fold in floats
+// once back in time.
+int lkref_fourier_info(const lkref_fourier* h, uint64_t* buffer_size, uint64_t* fold_size,
+                       uint64_t* fold_size_time) {
+    return guarded([&] {
+        const auto& plan = h->ffa->get_plan();
+        *buffer_size     = plan.get_buffer_size();
+        *fold_size       = plan.get_fold_size();
+        *fold_size_time  = plan.get_fold_size_time();
+    });
+}
+
+// FFA<ComplexType>::execute(span<ComplexType>): fold holds buffer_size
+// complex values as interleaved floats; its first fold_size are the result.
+int lkref_fourier_execute(lkref_fourier* h, const float* ts_e, const float* ts_v, uint64_t nsamps,
+                          float* fold, uint64_t fold_len_complex) {
+    return guarded([&] {
+        h->ffa->execute(std::span<const float>(ts_e, nsamps), std::span<const float>(ts_v, nsamps),
+                        std::span<loki::ComplexType>(reinterpret_cast<loki::ComplexType*>(fold),
+                                                     fold_len_complex));
+    });
+}
+
+// FFA<ComplexType>::execute(span<float>): back to time by the inverse real
+// transform; fold holds 2 * buffer_size floats, its first fold_size_time the
+// result.
+int lkref_fourier_execute_time(lkref_fourier* h, const float* ts_e, const float* ts_v,
+                               uint64_t nsamps, float* fold, uint64_t fold_len) {
+    return guarded([&] {
+        h->ffa->execute(std::span<const float>(ts_e, nsamps), std::span<const float>(ts_v, nsamps),
+                        std::span<float>(fold, fold_len));
+    });
+}
+
+// compute_ffa_scores with use_fourier = true (lib/ffa.cpp:444-466).
+int lkref_fourier_scores(const lkref_cfg* c, const float* ts_e, const float* ts_v, uint64_t nsamps,
+                         float* scores, uint64_t len) {
+    return guarded([&] {
+        const auto cfg = make_cfg(c, true);
+        auto [sc, plan] = loki::algorithms::compute_ffa_scores(
+            std::span<const float>(ts_e, nsamps), std::span<const float>(ts_v, nsamps), cfg, true,
+            false);
+        if (sc.size() != len) {
+            throw std::runtime_error("lkref_fourier_scores: output size mismatch");
+        }
+        std::memcpy(scores, sc.data(), sc.size() * sizeof(float));
+    });
+}
+
+// compute_brute_fold<ComplexType> (lib/fold.cpp): [nseg, nfreqs, 2, nbins/2+1]
+// complex as interleaved floats.
+int lkref_brute_fold_complex(const float* ts_e, const float* ts_v, uint64_t nsamps,
+                             const double* freqs, uint64_t nfreqs, uint64_t segment_len,
+                             uint64_t nbins, double tsamp, double t_ref, int nthreads, float* out,
+                             uint64_t out_len_complex) {
+    return guarded([&] {
+        auto fold = loki::algorithms::compute_brute_fold<loki::ComplexType>(
+            std::span<const float>(ts_e, nsamps), std::span<const float>(ts_v, nsamps),
+            std::span<const double>(freqs, nfreqs), segment_len, nbins, tsamp, t_ref, nthreads);
+        if (fold.size() != out_len_complex) {
+            throw std::runtime_error("lkref_brute_fold_complex: output size mismatch");
+        }
+        std::memcpy(out, fold.data(), fold.size() * sizeof(loki::ComplexType));
     });
 }
 

@@ -5,8 +5,9 @@
 // Fourier-domain FFA and the matched-filter templates, both off the
 // time-domain FP32 path. FFTW is not installed here; this header declares the
 // handful of single-precision entry points that lib/fft.cpp names, and
-// oracle/ref_stubs.cpp defines them: planning and execution throw, clean-up
-// calls (run from a static destructor at exit) do nothing.
+// oracle/ref_stubs.cpp defines them: batched 1-D r2c / c2r plans compute the
+// DFT definition in double (FFTW's unscaled conventions), the 2-D plans and
+// FFTW's allocators throw, clean-up calls do nothing.
 
 #include <cstddef>
 

@@ -2,13 +2,16 @@
 // reference's FFACUDA<float> / PulsarSearchConfig / compute_ffa_scores_cuda
 // interface, implemented over the C ABI.
 //
-//   ffacuda_check <input.bin> <fold.bin> <scores.bin>
+//   ffacuda_check <input.bin> <fold.bin> <scores.bin> <cfold.bin> <cscores.bin>
 //
 // input.bin: uint64 nsamps, double tsamp, uint64 nbins, double eta, uint32
 // nparams, double limits[2 * nparams], uint32 nwidths, uint32 widths[nwidths],
 // float ts_e[nsamps], float ts_v[nsamps]. Writes the final fold of
 // FFACUDA<float>::execute (host spans) and the scores of
-// compute_ffa_scores_cuda. Exit status 0 when every check passed.
+// compute_ffa_scores_cuda with use_fourier = false, then the final complex
+// fold of FFACUDA<ComplexTypeCUDA>::execute and the scores of
+// compute_ffa_scores_cuda with use_fourier = true (the default). Exit status
+// 0 when every check passed.
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -19,6 +22,8 @@
 #include "loki_b200.hpp"
 
 namespace {
+
+using loki_b200::SizeType;
 
 template <class T> T read_one(std::ifstream& in) {
     T v{};
@@ -32,17 +37,19 @@ template <class T> std::vector<T> read_n(std::ifstream& in, std::size_t n) {
     return v;
 }
 
-void write_all(const char* path, const std::vector<float>& v) {
+template <class T> void write_all(const char* path, const std::vector<T>& v) {
     std::ofstream out(path, std::ios::binary);
-    out.write(reinterpret_cast<const char*>(v.data()), static_cast<std::streamsize>(v.size() * sizeof(float)));
+    out.write(reinterpret_cast<const char*>(v.data()), static_cast<std::streamsize>(v.size() * sizeof(T)));
 }
+
+SizeType plan_nbins_f(SizeType nbins) { return nbins / 2 + 1; }
 
 }  // namespace
 
 int main(int argc, char** argv) {
     using namespace loki_b200;
-    if (argc != 4) {
-        std::cerr << "usage: ffacuda_check <input.bin> <fold.bin> <scores.bin>\n";
+    if (argc != 6) {
+        std::cerr << "usage: ffacuda_check <input.bin> <fold.bin> <scores.bin> <cfold.bin> <cscores.bin>\n";
         return 2;
     }
     std::ifstream in(argv[1], std::ios::binary);
@@ -94,11 +101,26 @@ int main(int argc, char** argv) {
     } catch (const std::invalid_argument&) {
     }
     try {
-        const search::PulsarSearchConfig cfg(nsamps, tsamp, nbins, eta, limits);  // use_fourier defaults to true
-        algorithms::FFACUDA<float> f(cfg);
-        std::cerr << "expected std::invalid_argument for the Fourier path\n";
+        // use_fourier defaults to true, as the reference's
+        const search::PulsarSearchConfig cfg(nsamps, tsamp, nbins, eta, limits, 0.2, 1.5, true, 1, std::nullopt,
+                                             std::nullopt, 5.0, widths);
+        algorithms::FFACUDA<ComplexTypeCUDA> ffa(cfg);
+        const auto& plan = ffa.get_plan();
+        std::vector<ComplexType> cfold(plan.get_fold_size());
+        ffa.execute(ts_e, ts_v, cfold);
+        // the overload pair: a float span receives the fold back in time
+        std::vector<float> tfold(plan.get_buffer_size_time());
+        ffa.execute(ts_e, ts_v, tfold);
+        if (plan.get_fold_size_time() != plan.get_fold_size() / plan_nbins_f(nbins) * nbins) {
+            std::cerr << "fold_size_time mismatch\n";
+            return 1;
+        }
+        write_all(argv[4], cfold);
+        auto [scores, tplan] = algorithms::compute_ffa_scores_cuda(ts_e, ts_v, cfg);
+        write_all(argv[5], scores);
+    } catch (const std::exception& e) {
+        std::cerr << "unexpected exception (Fourier path): " << e.what() << "\n";
         return 1;
-    } catch (const std::invalid_argument&) {
     }
     std::cout << "ffacuda_check: ok\n";
     return 0;

@@ -6,6 +6,7 @@ Run from the repository root after ``make -C oracle ref``:
     python tests/golden/make_golden.py prune    # the pruning fixtures only
     python tests/golden/make_golden.py sweep    # the frequency-sweep fixtures only
     python tests/golden/make_golden.py dts      # the threshold-scheme fixtures only
+    python tests/golden/make_golden.py fourier  # the Fourier-domain FFA fixtures only
 
 Every output comes from ``oracle/_ref/libloki_ref_parity.so`` -- the
 reference's CPU sources compiled unmodified with IEEE flags -- so the fixtures
@@ -273,6 +274,51 @@ def dts_fixtures() -> None:
         print(name, "non-empty states", int((~states["is_empty"]).sum()), "best path", best.tolist())
 
 
+# Fourier-domain FFA (FFA<ComplexType>): name -> (nsamps, tsamp, nbins, eta,
+# param_limits, seed). nbins 128 takes the lossy level 0 (time-domain brute
+# fold + real transform); the reference's FFTW calls run through the
+# DFT-definition stand-in of oracle/ref_stubs.cpp.
+FOURIER_CASES = {
+    "fourier_freq_nb32": (16384, 64e-6, 32, 1.0, [[50.0, 60.0]], 21),
+    "fourier_freq_nb64": (8192, 64e-6, 64, 1.0, [[70.0, 90.0]], 22),
+    "fourier_accel_nb16": (16384, 8e-3, 16, 1.0, [[-1000.0, 1000.0], [10.0, 10.3]], 23),
+    "fourier_jerk_nb16": (16384, 8e-3, 16, 1.0, [[-100.0, 100.0], [-900.0, 900.0], [10.0, 10.2]], 24),
+    "fourier_freq_nb128_lossy": (8192, 64e-6, 128, 1.0, [[70.0, 90.0]], 25),
+}
+
+
+def fourier_fixtures() -> None:
+    for name, (nsamps, tsamp, nbins, eta, lims, seed) in FOURIER_CASES.items():
+        ts_e, ts_v = series(nsamps, seed)
+        cfg = ref.make_cfg(nsamps, tsamp, nbins, eta, lims)
+        ffa = ref.RefFourier(cfg)
+        fold = ffa.execute(ts_e, ts_v).copy()
+        fold_time = ffa.execute_time(ts_e, ts_v).copy()
+        plan = ref.RefFFA(cfg)
+        nw = ref.box_widths(nbins).size
+        scores = ref.fourier_scores(cfg, ts_e, ts_v, int(plan.ncoords[-1]) * nw)
+        np.savez_compressed(
+            os.path.join(OUT, f"{name}.npz"),
+            ts_e=ts_e, ts_v=ts_v, nsamps=nsamps, nbins=nbins, eta=eta, tsamp=tsamp,
+            param_limits=np.array(lims, dtype=np.float64), n_levels=plan.n_levels,
+            ncoords=plan.ncoords, fold=fold if fold.size <= FOLD_KEEP else fold[:0],
+            fold_size=fold.size, fold_time=fold_time if fold_time.size <= FOLD_KEEP else fold_time[:0],
+            scores=scores, widths=ref.box_widths(nbins),
+        )
+        print(name, "levels", plan.n_levels, "final coords", int(plan.ncoords[-1]), "fold", fold.size)
+
+    # Direct transform with an explicit frequency list (reference test shape,
+    # tests/python/test_cpu_match.py:20-61, scaled down), odd nbins included.
+    ts_e, ts_v = series(1 << 14, 26)
+    freqs = np.linspace(140.0, 145.0, 7)
+    out = {}
+    for nb in (64, 33):
+        out[f"fold_nb{nb}"] = ref.brute_fold_complex(ts_e, ts_v, freqs, 1 << 11, nb, 64e-6, 0.0123)
+    np.savez_compressed(os.path.join(OUT, "brute_fold_fourier.npz"), ts_e=ts_e, ts_v=ts_v, freqs=freqs,
+                        segment_len=1 << 11, tsamp=64e-6, t_ref=0.0123, **out)
+    print("brute_fold_fourier", {k: v.shape for k, v in out.items()})
+
+
 if __name__ == "__main__":
     if not ref.available():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` first")
@@ -282,8 +328,11 @@ if __name__ == "__main__":
         sweep_fixtures()
     elif len(sys.argv) > 1 and sys.argv[1] == "dts":
         dts_fixtures()
+    elif len(sys.argv) > 1 and sys.argv[1] == "fourier":
+        fourier_fixtures()
     else:
         main()
         prune_fixtures()
         sweep_fixtures()
         dts_fixtures()
+        fourier_fixtures()
