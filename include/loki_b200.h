@@ -220,6 +220,17 @@ int lk_fourier_brute_fold(const float* d_ts_e, const float* d_ts_v, uint64_t nsa
 int lk_fourier_create(const lk_plan* plan, int device, uint64_t nbins_min_lossy_bf,
                       lk_fourier** out);
 void lk_fourier_destroy(lk_fourier* f);
+/* Kernel of the level-0 direct transform (results agree to FP32 accuracy):
+ * AUTO = the tensor cores when the shape allows (nbins / 2 <= 64 harmonics,
+ * segment length a multiple of 8), else the CUDA cores. */
+enum lk_fourier_level0 {
+    LK_FOURIER_L0_AUTO = 0,
+    LK_FOURIER_L0_CUDA_CORES = 1,  /* FP32 phasor recurrence per harmonic */
+    LK_FOURIER_L0_TENSOR_CORES = 2 /* tcgen05.mma, three FP16 hi / lo passes, FP32 sums */
+};
+int lk_fourier_set_level0(lk_fourier* f, int mode);
+/* Synchronises the stream; the device status word (bounded-wait give-ups). */
+int lk_fourier_status(lk_fourier* f, lk_stream_t stream, uint32_t* status);
 /* nbins_f; final fold sizes (complex values, and floats back in time);
  * lossy = 1 when level 0 is the brute fold + real transform. */
 int lk_fourier_info(const lk_fourier* f, uint64_t* nbins_f, uint64_t* fold_size,

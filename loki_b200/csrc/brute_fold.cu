@@ -880,20 +880,6 @@ __global__ void interleave_kernel(const float* __restrict__ e, const float* __re
     }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        LK_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000,
-                                                 cudaEnableDefault, &q));
-        if (q != cudaDriverEntryPointSuccess || p == nullptr) {
-            fail(LK_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-        }
-        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }();
-    return fn;
-}
-
 // 2-D map over one row of the series viewed as [nseg][seglen]; box 32
 // samples x 32 segments, 128-byte swizzle; rows past nseg read as zero.
 void encode_series_map(CUtensorMap* map, const float* base, uint64_t seglen, uint64_t nseg) {
@@ -928,6 +914,21 @@ void encode_ev_map(CUtensorMap* map, const float2* base, uint64_t seglen, uint64
 }
 
 }  // namespace
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        LK_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000,
+                                                 cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || p == nullptr) {
+            fail(LK_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
 
 BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segment_len,
                                  uint64_t nbins, uint64_t nsamps, double tsamp, double t_ref,

@@ -646,6 +646,21 @@ int lk_fourier_search(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, f
     });
 }
 
+int lk_fourier_set_level0(lk_fourier* f, int mode) {
+    return guarded([&] {
+        need(f, "f");
+        f->exec->set_level0(mode);
+    });
+}
+
+int lk_fourier_status(lk_fourier* f, lk_stream_t stream, uint32_t* status) {
+    return guarded([&] {
+        need(f, "f");
+        need(status, "status");
+        *status = f->exec->read_status(reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 int lk_fourier_set_profiling(lk_fourier* f, int enable) {
     return guarded([&] {
         need(f, "f");

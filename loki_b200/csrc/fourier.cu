@@ -22,6 +22,7 @@
 
 #include "lk_fourier.hpp"
 #include "lk_merge.cuh"
+#include "lk_score.cuh"
 
 namespace lk {
 namespace {
@@ -290,6 +291,120 @@ rfft_kernel(const float* __restrict__ in, float2* __restrict__ out, uint64_t npr
     }
 }
 
+// ---- fused final level: merge + inverse real transform + boxcar S/N ----
+//
+// One block of kFinCells final cells (nbins <= 64, one final segment).
+// Phase 1, all threads: the merged harmonics of the block's cells (tail and
+// head rows of the previous level rotated and added, as fourier_merge_kernel)
+// into shared memory as [harmonic][cell] (E re, E im, V re, V im).
+// Phase 2, a thread per cell: the inverse transform by sums over the
+// harmonics with the folding symmetries of the c2r kernel (x_j and x_{n-j}
+// from one cosine and one sine sum; for n divisible by 4 also x_{n/2-j} and
+// x_{n/2+j} from the even and odd harmonics apart), each output normalised
+// E / sqrt(V) into the cell's row. Phase 3: the boxcar scorer on the row.
+// The twiddle table holds (c_m / n) (cos, sin)(2 pi m j / n) for the j a
+// thread evaluates (c_m = 1 for the DC and Nyquist terms, else 2), so the
+// scale of the c2r transform and the unused imaginary parts of the DC and
+// Nyquist terms come out of the table.
+constexpr uint32_t kFinCells = 64;
+
+struct FinalArgs {
+    const float2* in;       // level L-2 complex fold [2 segments][nprev][2][nbf]
+    const void* coords;     // level L-1 coordinates
+    const float2* tw;       // [jcount][nbf] scaled twiddles
+    float* scores;          // [ncur][nwidths]
+    uint64_t ncur, nprev;
+    uint32_t nbins, nbf, jcount, rs;
+    ScoreParams sp;
+};
+
+template <bool TAYLOR, int NW>
+__global__ void __launch_bounds__(kFinCells)
+fourier_final_kernel(FinalArgs a) {
+    extern __shared__ float4 fsm[];
+    float4* coef = fsm;                                               // [nbf][kFinCells]
+    float2* tw = reinterpret_cast<float2*>(coef + a.nbf * kFinCells);  // [jcount][nbf]
+    float* rows = reinterpret_cast<float*>(tw + a.jcount * a.nbf);     // [kFinCells][rs]
+    const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kFinCells;
+    const uint64_t left = a.ncur - c0;
+    const uint32_t ncells = left < kFinCells ? static_cast<uint32_t>(left) : kFinCells;
+    for (uint32_t i = threadIdx.x; i < a.jcount * a.nbf; i += blockDim.x) {
+        tw[i] = a.tw[i];
+    }
+    const double inv_nbins = 1.0 / static_cast<double>(a.nbins);
+    const uint64_t rs2 = 2ull * a.nbf;
+    for (uint32_t i = threadIdx.x; i < ncells * a.nbf; i += blockDim.x) {
+        const uint32_t cl = i / a.nbf;
+        const uint32_t k = i - cl * a.nbf;
+        const uint64_t c = c0 + cl;
+        uint32_t it, ih;
+        float st = 0.0f, sh;
+        if constexpr (TAYLOR) {
+            const CoordTaylor cc = reinterpret_cast<const CoordTaylor*>(a.coords)[c];
+            it = cc.i_tail;
+            ih = cc.i_head;
+            st = cc.shift_tail;
+            sh = cc.shift_head;
+        } else {
+            const CoordFreq cc = reinterpret_cast<const CoordFreq*>(a.coords)[c];
+            it = ih = cc.idx;
+            sh = cc.shift;
+        }
+        const float2* tail = a.in + static_cast<uint64_t>(it) * rs2 + k;
+        const float2* head = a.in + (a.nprev + ih) * rs2 + k;
+        const float2 ph = unit_phasor(static_cast<double>(k) * static_cast<double>(sh) * inv_nbins);
+        float2 te = __ldg(tail), tv = __ldg(tail + a.nbf);
+        if constexpr (TAYLOR) {
+            const float2 pt =
+                unit_phasor(static_cast<double>(k) * static_cast<double>(st) * inv_nbins);
+            te = cmul(te, pt);
+            tv = cmul(tv, pt);
+        }
+        const float2 he = cmul(__ldg(head), ph), hv = cmul(__ldg(head + a.nbf), ph);
+        coef[k * kFinCells + cl] = make_float4(te.x + he.x, te.y + he.y, tv.x + hv.x, tv.y + hv.y);
+    }
+    __syncthreads();
+    const uint32_t t = threadIdx.x;
+    if (t >= ncells) {
+        return;
+    }
+    float* r = rows + t * a.rs;
+    const uint32_t n = a.nbins;
+    const bool quad = (n % 4) == 0;
+    for (uint32_t j = 0; j < a.jcount; ++j) {
+        float ce0 = 0.0f, ce1 = 0.0f, se0 = 0.0f, se1 = 0.0f;  // E: even / odd harmonics
+        float cv0 = 0.0f, cv1 = 0.0f, sv0 = 0.0f, sv1 = 0.0f;  // V
+        const float2* twj = tw + j * a.nbf;
+        for (uint32_t m = 0; m < a.nbf; m += 2) {
+            const float4 x = coef[m * kFinCells + t];
+            const float2 w = twj[m];
+            ce0 = fmaf(x.x, w.x, ce0);
+            se0 = fmaf(x.y, w.y, se0);
+            cv0 = fmaf(x.z, w.x, cv0);
+            sv0 = fmaf(x.w, w.y, sv0);
+            if (m + 1 < a.nbf) {
+                const float4 y = coef[(m + 1) * kFinCells + t];
+                const float2 u = twj[m + 1];
+                ce1 = fmaf(y.x, u.x, ce1);
+                se1 = fmaf(y.y, u.y, se1);
+                cv1 = fmaf(y.z, u.x, cv1);
+                sv1 = fmaf(y.w, u.y, sv1);
+            }
+        }
+        const float ce = ce0 + ce1, se = se0 + se1, cv = cv0 + cv1, sv = sv0 + sv1;
+        r[j] = sc::normalise(ce - se, cv - sv);
+        if (j > 0) {
+            r[n - j] = sc::normalise(ce + se, cv + sv);
+        }
+        if (quad) {
+            const float de = ce0 - ce1, he = se0 - se1, dv = cv0 - cv1, hv = sv0 - sv1;
+            r[n / 2 - j] = sc::normalise(de + he, dv + hv);
+            r[n / 2 + j] = sc::normalise(de - he, dv - hv);
+        }
+    }
+    sc::score_row<NW>(r, n, 1.0f, a.sp, LK_SCORE_PER_WIDTH, a.scores + (c0 + t) * a.sp.nwidths);
+}
+
 uint32_t grid_for(uint64_t work, uint32_t per_block) {
     const uint64_t b = (work + per_block - 1) / per_block;
     return static_cast<uint32_t>(std::clamp<uint64_t>(b, 1, 148ull * 64));
@@ -372,6 +487,75 @@ void irfft_profiles(const float2* d_in, float* d_out, uint64_t nprof, uint32_t n
     LK_CUDA(cudaGetLastError());
 }
 
+bool fourier_final_supported(uint32_t nbins) { return nbins >= 2 && nbins <= 64; }
+
+uint32_t fourier_final_jcount(uint32_t nbins) {
+    // outputs a thread evaluates directly: j in [0, n/4] with the four-fold
+    // symmetry (n divisible by 4), else j in [0, n/2]
+    return (nbins % 4 == 0) ? nbins / 4 + 1 : nbins / 2 + 1;
+}
+
+std::vector<float2> fourier_final_twiddles(uint32_t nbins) {
+    const uint32_t nbf = nbins / 2 + 1;
+    const uint32_t jc = fourier_final_jcount(nbins);
+    std::vector<float2> tw(static_cast<size_t>(jc) * nbf);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (uint32_t j = 0; j < jc; ++j) {
+        for (uint32_t m = 0; m < nbf; ++m) {
+            const bool edge = m == 0 || 2 * m == nbins;
+            const double cm = edge ? 1.0 : 2.0;
+            const double th = two_pi * static_cast<double>((static_cast<uint64_t>(m) * j) % nbins) /
+                              static_cast<double>(nbins);
+            const double sn = edge ? 0.0 : std::sin(th);
+            tw[static_cast<size_t>(j) * nbf + m] = make_float2(static_cast<float>(cm * std::cos(th) / nbins),
+                                                               static_cast<float>(cm * sn / nbins));
+        }
+    }
+    return tw;
+}
+
+void fourier_final_score(const float2* d_in, const void* d_coords, bool taylor, uint64_t ncur,
+                         uint64_t nprev, uint32_t nbins, const ScoreParams& sp, const float2* d_tw,
+                         float* d_scores, cudaStream_t s) {
+    require(fourier_final_supported(nbins), "fused Fourier final level: nbins must lie in [2, 64]");
+    FinalArgs a{};
+    a.in = d_in;
+    a.coords = d_coords;
+    a.tw = d_tw;
+    a.scores = d_scores;
+    a.ncur = ncur;
+    a.nprev = nprev;
+    a.nbins = nbins;
+    a.nbf = nbins / 2 + 1;
+    a.jcount = fourier_final_jcount(nbins);
+    a.rs = sc::row_stride(nbins, sp.wmax);
+    a.sp = sp;
+    const size_t smem = sizeof(float4) * a.nbf * kFinCells + sizeof(float2) * a.jcount * a.nbf +
+                        sizeof(float) * kFinCells * a.rs;
+    const uint64_t blocks = (ncur + kFinCells - 1) / kFinCells;
+    require(blocks <= 0x7fffffffULL, "fused Fourier final level: too many cells");
+    auto launch = [&](auto kern) {
+        sc::set_smem(kern, smem);
+        kern<<<static_cast<uint32_t>(blocks), kFinCells, smem, s>>>(a);
+    };
+    auto by_nw = [&](auto tay) {
+        constexpr bool T = decltype(tay)::value;
+        if (sp.nwidths <= 8) {
+            launch(fourier_final_kernel<T, 8>);
+        } else if (sp.nwidths <= 16) {
+            launch(fourier_final_kernel<T, 16>);
+        } else {
+            launch(fourier_final_kernel<T, 32>);
+        }
+    };
+    if (taylor) {
+        by_nw(std::true_type{});
+    } else {
+        by_nw(std::false_type{});
+    }
+    LK_CUDA(cudaGetLastError());
+}
+
 // ---- executor -------------------------------------------------------------
 
 FourierExec::FourierExec(const Plan& p, int device_, uint64_t nbins_min_lossy)
@@ -404,6 +588,10 @@ FourierExec::FourierExec(const Plan& p, int device_, uint64_t nbins_min_lossy)
                                                status.as<uint32_t>());
         tfold.alloc(sizeof(float) * plan.fold_size(0));
     }
+    if (!lossy && fourier_mma_supported(plan.segment_lens[0], plan.nsegments[0], nbins)) {
+        mma = std::make_unique<FourierMma>(plan.segment_lens[0], plan.nsegments[0], nbins,
+                                           static_cast<uint32_t>(plan.ncoords[0]));
+    }
     uint64_t inter = 0;
     for (uint32_t l = 0; l < plan.n_levels; ++l) {
         inter = std::max(inter, fold_size(l));
@@ -411,12 +599,18 @@ FourierExec::FourierExec(const Plan& p, int device_, uint64_t nbins_min_lossy)
     buf[0].alloc(sizeof(float2) * inter);
     buf[1].alloc(sizeof(float2) * inter);
     sp = make_score_params(plan.widths.data(), static_cast<uint32_t>(plan.widths.size()), nbins);
+    if (fourier_final_supported(nbins) && plan.nsegments[plan.n_levels - 1] == 1) {
+        const std::vector<float2> tw = fourier_final_twiddles(nbins);
+        final_tw.alloc(sizeof(float2) * tw.size());
+        LK_CUDA(cudaMemcpy(final_tw.ptr, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+    }
     LK_CUDA(cudaDeviceSynchronize());
 }
 
 uint64_t FourierExec::device_bytes() const {
     return status.bytes + coords.bytes + freqs0.bytes + buf[0].bytes + buf[1].bytes + tfold.bytes +
-           tfinal.bytes + scores_tmp.bytes + compact_scratch.bytes + (bf ? bf->device_bytes() : 0);
+           tfinal.bytes + scores_tmp.bytes + compact_scratch.bytes + (bf ? bf->device_bytes() : 0) +
+           (mma ? mma->device_bytes() : 0) + final_tw.bytes;
 }
 
 const void* FourierExec::level_coords(uint32_t l) const {
@@ -425,13 +619,13 @@ const void* FourierExec::level_coords(uint32_t l) const {
 }
 
 const float2* FourierExec::run_levels(const float* ts_e, const float* ts_v, float2* final_out,
-                                      cudaStream_t s) {
-    const uint32_t L = plan.n_levels;
+                                      cudaStream_t s, int last_level) {
+    const uint32_t L = last_level < 0 ? plan.n_levels : static_cast<uint32_t>(last_level) + 1;
     const auto nbins = static_cast<uint32_t>(plan.cfg.nbins);
     const bool taylor = plan.nparams > 1;
     // Level l lands in buf[l % 2], the final one in final_out when given.
     auto dst = [&](uint32_t l) -> float2* {
-        return (l == L - 1 && final_out != nullptr) ? final_out : buf[l % 2].as<float2>();
+        return (l == plan.n_levels - 1 && final_out != nullptr) ? final_out : buf[l % 2].as<float2>();
     };
     const uint64_t series_bytes = 8 * plan.cfg.nsamps;
     float2* in = dst(0);
@@ -443,6 +637,13 @@ const float2* FourierExec::run_levels(const float* ts_e, const float* ts_v, floa
         prof.end(s);
         prof.begin(LK_STAGE_TRANSFORM, 0, 1, 4 * plan.fold_size(0) + 8 * fold_size(0), s);
         rfft_profiles(tfold.as<float>(), in, plan.fold_size(0) / nbins, nbins, s);
+        prof.end(s);
+    } else if (uses_mma()) {
+        // series in, FP16 staging out and in again (hi + lo), fold out
+        prof.begin(LK_STAGE_BRUTE_FOLD, 0, 4, 2 * series_bytes + 16 * plan.cfg.nsamps + 8 * fold_size(0),
+                   s);
+        mma->run(ts_e, ts_v, freqs0.as<double>(), plan.cfg.tsamp, plan.t_ref0(), in,
+                 status.as<uint32_t>(), s);
         prof.end(s);
     } else {
         prof.begin(LK_STAGE_BRUTE_FOLD, 0, 1, series_bytes + 8 * fold_size(0), s);
@@ -492,6 +693,19 @@ void FourierExec::scores_into(const float* ts_e, const float* ts_v, float* d_sco
     const uint32_t L = plan.n_levels;
     const uint64_t nc = plan.ncoords[L - 1];
     const auto nbins = static_cast<uint32_t>(plan.cfg.nbins);
+    if (final_tw.ptr != nullptr) {
+        // levels 0 .. L-2, then the final merge fused with the transform and scorer
+        run_levels(ts_e, ts_v, nullptr, s, static_cast<int>(L) - 2);
+        const float2* in = buf[(L - 2) % 2].as<float2>();
+        prof.begin(LK_STAGE_MERGE_SCORE, static_cast<int>(L - 1), 1,
+                   8 * fold_size(L - 2) + 4 * nc * plan.widths.size() +
+                       plan.ncoords[L - 1] * (plan.nparams == 1 ? 8 : 16),
+                   s);
+        fourier_final_score(in, level_coords(L - 1), plan.nparams > 1, nc, plan.ncoords[L - 2], nbins, sp,
+                            final_tw.as<float2>(), d_scores, s);
+        prof.end(s);
+        return;
+    }
     if (tfinal.bytes < sizeof(float) * fold_size_time(L - 1)) {
         tfinal.alloc(sizeof(float) * fold_size_time(L - 1));
     }
@@ -533,6 +747,26 @@ void FourierExec::search(const float* ts_e, const float* ts_v, float snr_min, ui
     compact_ge(scores_tmp.as<float>(), n, snr_min, d_idx, d_snr, max_cands, d_count,
                compact_scratch.ptr, s);
     prof.end(s);
+}
+
+void FourierExec::set_level0(int mode) {
+    require(mode == LK_FOURIER_L0_AUTO || mode == LK_FOURIER_L0_CUDA_CORES ||
+                mode == LK_FOURIER_L0_TENSOR_CORES,
+            "level-0 mode must be LK_FOURIER_L0_AUTO, _CUDA_CORES or _TENSOR_CORES");
+    if (mode == LK_FOURIER_L0_TENSOR_CORES && mma == nullptr) {
+        fail(LK_ERR_UNSUPPORTED, lossy ? "the level-0 fold of nbins > nbins_min_lossy_bf is the lossy one"
+                                       : "tensor-core level 0 needs nbins / 2 <= 64 and segment lengths "
+                                         "that are multiples of 8");
+    }
+    level0 = mode;
+}
+
+uint32_t FourierExec::read_status(cudaStream_t s) {
+    DeviceGuard g(device);
+    LK_CUDA(cudaStreamSynchronize(s));
+    uint32_t st = 0;
+    LK_CUDA(cudaMemcpy(&st, status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return st;
 }
 
 std::vector<lk_stage_time> FourierExec::profile(cudaStream_t s) {

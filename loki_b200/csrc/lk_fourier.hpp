@@ -33,6 +33,32 @@ void rfft_profiles(const float* d_in, float2* d_out, uint64_t nprof, uint32_t nb
 void irfft_profiles(const float2* d_in, float* d_out, uint64_t nprof, uint32_t nbins,
                     cudaStream_t s);
 
+// Final level fused with the inverse transform and the boxcar scorer
+// (nbins <= 64, one final segment): scores [ncur][nwidths].
+bool fourier_final_supported(uint32_t nbins);
+uint32_t fourier_final_jcount(uint32_t nbins);
+std::vector<float2> fourier_final_twiddles(uint32_t nbins);
+void fourier_final_score(const float2* d_in, const void* d_coords, bool taylor, uint64_t ncur,
+                         uint64_t nprev, uint32_t nbins, const ScoreParams& sp, const float2* d_tw,
+                         float* d_scores, cudaStream_t s);
+
+// The same level-0 transform on the tensor cores (fourier_mma.cu): three
+// FP16 tcgen05.mma passes over hi / lo halves, FP32 accumulation. Needs
+// nbins / 2 <= 64 harmonics and segment lengths that are multiples of 8.
+bool fourier_mma_supported(uint64_t seglen, uint64_t nseg, uint32_t nbins);
+struct FourierMma {
+    uint64_t seglen, nseg;
+    uint32_t nbins, nfreq;
+    uint32_t ntile = 0, nsub = 0, ngroups = 0, tmem_cols = 0;
+    size_t smem_bytes = 0;
+    DeviceBuffer hi, lo, dc, aux;  // FP16 staging [2 nseg][seglen], row sums, max / exponents
+    CUtensorMap map_hi{}, map_lo{};
+    FourierMma(uint64_t seglen, uint64_t nseg, uint32_t nbins, uint32_t nfreq);
+    uint64_t device_bytes() const;
+    void run(const float* d_ts_e, const float* d_ts_v, const double* d_freqs, double tsamp,
+             double t_ref, float2* d_out, uint32_t* d_status, cudaStream_t s);
+};
+
 struct FourierExec {
     Plan plan;
     int device;
@@ -46,7 +72,12 @@ struct FourierExec {
     DeviceBuffer tfold;   // lossy: level-0 time-domain fold
     DeviceBuffer tfinal;  // final fold back in time (scores / search)
     DeviceBuffer scores_tmp, compact_scratch;
+    DeviceBuffer final_tw;  // twiddles of the fused final level (nbins <= 64)
     std::unique_ptr<BruteFoldDevice> bf;  // lossy path only
+    std::unique_ptr<FourierMma> mma;      // tensor-core level 0 (when the shape allows)
+    // Level-0 kernel of the direct transform: LK_FOURIER_L0_AUTO (tensor cores
+    // when supported), _CUDA_CORES or _TENSOR_CORES.
+    int level0 = LK_FOURIER_L0_AUTO;
     ScoreParams sp{};
 
     FourierExec(const Plan& p, int device, uint64_t nbins_min_lossy);
@@ -58,8 +89,9 @@ struct FourierExec {
     const void* level_coords(uint32_t l) const;
     // Levels 0 .. n_levels - 1; the final level lands in final_out when given
     // (else in a ping-pong buffer). Returns the final complex fold.
+    // last_level < 0: the final level.
     const float2* run_levels(const float* ts_e, const float* ts_v, float2* final_out,
-                             cudaStream_t s);
+                             cudaStream_t s, int last_level = -1);
     void execute(const float* ts_e, const float* ts_v, float2* fold, uint64_t len_complex,
                  cudaStream_t s);
     void execute_time(const float* ts_e, const float* ts_v, float* fold, uint64_t len,
@@ -69,6 +101,9 @@ struct FourierExec {
     void search(const float* ts_e, const float* ts_v, float snr_min, uint32_t* d_idx, float* d_snr,
                 uint64_t max_cands, uint64_t* d_count, cudaStream_t s);
     std::vector<lk_stage_time> profile(cudaStream_t s);
+    void set_level0(int mode);
+    bool uses_mma() const { return mma != nullptr && level0 != LK_FOURIER_L0_CUDA_CORES; }
+    uint32_t read_status(cudaStream_t s);
 
 private:
     void scores_into(const float* ts_e, const float* ts_v, float* d_scores, cudaStream_t s);

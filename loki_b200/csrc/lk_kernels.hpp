@@ -7,6 +7,7 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include "lk_internal.hpp"
 
@@ -201,6 +202,9 @@ void rescore_cells(const float* d_fold0, const RescoreTree& t, bool taylor, cons
 void score_folds(const float* d_folds, uint64_t nprof, uint32_t nbins, bool is3d,
                  float inv_stdnoise, const ScoreParams& sp, int mode, float* d_scores,
                  cudaStream_t s);
+
+// cuTensorMapEncodeTiled, resolved from the driver once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // Ordered compaction of scores >= thr.
 uint64_t compact_scratch_bytes(uint64_t n);

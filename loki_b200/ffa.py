@@ -415,6 +415,19 @@ class FFACOMPLEXCUDA:
         k = min(total, cap)
         return idx[:k].cpu().numpy().view(np.uint32), snr[:k].cpu().numpy(), total
 
+    _LEVEL0 = {"auto": 0, "cuda_cores": 1, "tensor_cores": 2}
+
+    def set_level0(self, mode: str = "auto") -> None:
+        """Kernel of the level-0 direct transform: "auto" (the tensor cores when
+        the shape allows), "cuda_cores" or "tensor_cores"."""
+        C.check(C.lib().lk_fourier_set_level0(self._h, self._LEVEL0[mode]))
+
+    def status(self) -> int:
+        """Device status word (bits set by bounded waits that gave up)."""
+        st = ctypes.c_uint32()
+        C.check(C.lib().lk_fourier_status(self._h, D.stream_ptr(self._device), ctypes.byref(st)))
+        return st.value
+
     def set_profiling(self, enable: bool = True) -> None:
         C.check(C.lib().lk_fourier_set_profiling(self._h, 1 if enable else 0))
 

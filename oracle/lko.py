@@ -325,19 +325,31 @@ def fourier_merge(fold_in, coords, ncur, nprev, nseg, nbins) -> np.ndarray:
 
 
 def irfft(x, n) -> np.ndarray:
+    """Inverse real transforms of size n over the profiles of x (its last
+    axis the n // 2 + 1 harmonics, or flat): [..., n] float64."""
+    nbf = n // 2 + 1
     x = np.ascontiguousarray(x, dtype=np.complex128)
-    nprof = x.size // (n // 2 + 1)
-    out = np.zeros(x.shape[:-1] + (n,), dtype=np.float64)
+    if x.size % nbf != 0:
+        raise ValueError("irfft: input size is not a multiple of n // 2 + 1")
+    nprof = x.size // nbf
+    shape = x.shape[:-1] + (n,) if x.ndim > 1 and x.shape[-1] == nbf else (nprof * n,)
+    out = np.zeros(nprof * n, dtype=np.float64)
     lib().lko_irfft(_p(x), _p(out), nprof, n)
-    return out
+    return out.reshape(shape)
 
 
 def rfft(x, n) -> np.ndarray:
+    """Real transforms of size n over the profiles of x (its last axis n, or
+    flat): [..., n // 2 + 1] complex128."""
+    nbf = n // 2 + 1
     x = np.ascontiguousarray(x, dtype=np.float64)
+    if x.size % n != 0:
+        raise ValueError("rfft: input size is not a multiple of n")
     nprof = x.size // n
-    out = np.zeros(x.shape[:-1] + (n // 2 + 1,), dtype=np.complex128)
+    shape = x.shape[:-1] + (nbf,) if x.ndim > 1 and x.shape[-1] == n else (nprof * nbf,)
+    out = np.zeros(nprof * nbf, dtype=np.complex128)
     lib().lko_rfft(_p(x), _p(out), nprof, n)
-    return out
+    return out.reshape(shape)
 
 
 def ffa_fourier(plan: OraclePlan, ts_e, ts_v, level: int | None = None,

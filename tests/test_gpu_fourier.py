@@ -159,3 +159,44 @@ def test_profile_stages(cuda):
     stages = [p["stage"] for p in ffa.profile()]
     assert stages[0] == "brute_fold" and stages[1] == "transform" and stages[-1] == "score"
     assert stages.count("merge") == ffa.plan.n_levels - 1
+
+
+# level-0 shapes: (nsamps, tsamp, nbins, eta, limits, bseg_brute) -> tensor-core
+# tiles of one subtile (few segments), two subtiles and several column groups
+L0_CASES = {
+    "nb64_few_segments": (2**14, 64e-6, 64, 1.0, [[20.0, 30.0]], None),
+    "nb64_accel": (2**18, 64e-6, 64, 2.0, [[-200.0, 200.0], [20.0, 50.0]], None),
+    "nb32_many_segments": (2**17, 64e-6, 32, 1.0, [[30.0, 60.0]], 256),
+    "nb33_odd": (2**16, 64e-6, 33, 1.0, [[20.0, 40.0]], 1024),
+    "nb16_1024_segments": (2**18, 1e-3, 16, 1.0, [[5.0, 8.0]], 256),
+}
+
+
+@pytest.mark.parametrize("name", sorted(L0_CASES))
+def test_level0_tensor_cores_vs_cuda_cores(cuda, name):
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACOMPLEXCUDA
+    from loki_b200.fold import compute_brute_fold_fourier_cuda
+
+    nsamps, tsamp, nb, eta, lims, bseg = L0_CASES[name]
+    op = lko.plan_create(lko.make_cfg(nsamps, tsamp, nb, eta, lims, bseg_brute=bseg))
+    cfg = PulsarSearchConfig(nsamps, tsamp, nb, eta, np.array(lims), use_fourier=True, bseg_brute=bseg,
+                             score_widths=[int(w) for w in op.widths])
+    ts_e, ts_v = series(nsamps, 23)
+    ts_e *= np.float32(37.5)  # not unit scale: the FP16 staging exponent is exercised
+    final = lko.ffa_fourier(op, ts_e, ts_v).ravel()
+    s64 = lko.ffa_fourier_scores64(op, ts_e, ts_v, op.widths).ravel()
+    ffa = FFACOMPLEXCUDA(cfg)
+    for mode in ("cuda_cores", "tensor_cores"):
+        ffa.set_level0(mode)
+        fold = ffa.execute(ts_e, ts_v)
+        assert ffa.status() == 0
+        assert _rel(fold, final) < FOLD_RTOL, mode
+        s = ffa.scores(ts_e, ts_v)
+        assert np.abs(s - s64).max() < SNR_ATOL, mode
+    # level 0 alone through the brute-fold entry (the direct transform on the CUDA cores)
+    want0 = lko.ffa_fourier(op, ts_e, ts_v, level=0).ravel()
+    freqs = ffa.plan.compute_param_grid(0)[-1]
+    t_ref = 0.0 if len(lims) == 1 else float(op.raw.tsegments[0]) / 2
+    bf = compute_brute_fold_fourier_cuda(ts_e, ts_v, freqs, int(op.segment_lens[0]), nb, tsamp, t_ref)
+    assert _rel(bf, want0) < FOLD_RTOL

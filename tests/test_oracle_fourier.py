@@ -131,3 +131,23 @@ def test_ffa_matches_reference_live():
         assert _rel(fold.ravel(), R.execute(e, v)) < FOLD_RTOL
         s = ref.fourier_scores(rc, e, v, int(p.ncoords[-1]) * p.widths.size)
         assert np.abs(lko.ffa_fourier_scores64(p, e, v, p.widths).ravel() - s).max() < SNR_ATOL
+
+
+@needs_ref
+@pytest.mark.parametrize("lims,nb", [([[20.0, 40.0]], 64), ([[-500.0, 500.0], [12.0, 12.4]], 32),
+                                      ([[20.0, 40.0]], 128), ([[20.0, 40.0]], 33)])
+def test_fourier_plan_geometry_matches_reference(lims, nb):
+    """FFAPlanFourier (library, host only) against FFAPlan<ComplexType> of the reference."""
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.plans import FFAPlanFourier
+
+    n, tsamp = 1 << 16, 64e-6 if len(lims) == 1 else 4e-3
+    cfg = PulsarSearchConfig(n, tsamp, nb, 1.0, np.array(lims), use_fourier=True)
+    p = FFAPlanFourier(cfg)
+    R = ref.RefFourier(ref.make_cfg(n, tsamp, nb, 1.0, np.array(lims)))
+    assert p.fold_size == R.fold_size
+    assert p.buffer_size == R.buffer_size
+    assert p.fold_size_time == R.fold_size_time
+    assert p.buffer_size_time == 2 * R.buffer_size
+    assert p.nbins_f == nb // 2 + 1
+    assert [int(x) for x in p.fold_shapes[-1]][-1] == nb // 2 + 1
