@@ -158,6 +158,17 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
+def tensor_peak():
+    """Dense BF16/FP16 tensor-core peak (TFLOP/s): the measured burst figure if
+    present, else the fallback measured earlier on these GPUs."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
 def ncu_traffic(stage: str):
     """Per-launch DRAM bytes of a stage from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")

@@ -950,24 +950,41 @@ def run_fourier(args, rank, world, local_rank):
         launches += st["launches"]
     ffa.set_profiling(False)
     value = ntrials * world / (ms / 1e3)
-    # roofline of the dominant stage: the level-0 direct transform is bound by
-    # the FP32 pipe. Algorithmic flops: the reference's count for it,
-    # 8 * nsamps * 2 * nfreqs * nbins_f (FFAPlan::compute_flops, lib/plans.cpp:520-560).
+    # roofline of the dominant stage, the level-0 direct transform. On the
+    # tensor cores: algorithmic flops of its matrix product, 2 (multiply-add)
+    # x 2 (re, im) x 2 (E, V) x nsamps x nfreqs x harmonics (m >= 1), and the
+    # three FP16 passes the kernel issues for them, against the dense tensor
+    # peak; on the CUDA cores: the reference's count for it, 8 * nsamps * 2 *
+    # nfreqs * nbins_f (FFAPlan::compute_flops, lib/plans.cpp:520-560),
+    # against the FP32 FMA rate.
     nfreq0 = int(plan.ncoords[0])
     nbf = params["nbins"] // 2 + 1
-    flops = 8 * params["nsamps"] * 2 * nfreq0 * nbf
     bf_ms = prof["brute_fold_l0"][0]
-    props = torch.cuda.get_device_properties(local_rank)
-    mhz = (clk or {}).get("sm_max_mhz") or 1965.0
-    fp32_peak = 2 * 128 * props.multi_processor_count * mhz * 1e6 / 1e12
-    ach = flops / (bf_ms / 1e3) / 1e12
     peak, peak_kind = B.hbm_peak()
-    merges = {k: (p[1] / (p[0] / 1e3) / 1e9) / peak for k, p in sorted(prof.items()) if k.startswith("merge")}
-    roof = {"bound": "fp32", "kernel": "brute_fold_l0 (fourier_dft_kernel)", "achieved": ach, "peak": fp32_peak,
-            "unit": "TFLOP/s", "frac": ach / fp32_peak,
-            "peak_source": "nominal FP32 FMA rate: 128 lanes x 2 flop x SMs x max SM clock",
-            "algorithmic_flops": flops, "avg_ms": bf_ms, "traffic": B.ncu_traffic("fourier_dft"),
-            "merge_hbm_frac": merges, "hbm_peak": peak, "hbm_peak_source": peak_kind}
+    merges = {k: (p[1] / (p[0] / 1e3) / 1e9) / peak for k, p in sorted(prof.items()) if k.startswith("merge_l")}
+    if ffa.level0 == "tensor_cores":
+        flops = 8 * params["nsamps"] * nfreq0 * (nbf - 1)
+        issued = 3 * flops
+        tpeak, tkind = B.tensor_peak()
+        ach = issued / (bf_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "kernel": "brute_fold_l0 (fourier_dft_mma_kernel + staging)", "achieved": ach,
+                "peak": tpeak, "unit": "TFLOP/s", "frac": ach / tpeak,
+                "peak_source": f"{tkind} dense BF16 tensor peak (FP16 runs at the same rate)",
+                "issued_flops": issued, "algorithmic_flops": flops, "passes": 3,
+                "algorithmic_achieved": flops / (bf_ms / 1e3) / 1e12, "avg_ms": bf_ms,
+                "traffic": B.ncu_traffic("fourier_dft_mma"), "merge_hbm_frac": merges, "hbm_peak": peak,
+                "hbm_peak_source": peak_kind}
+    else:
+        flops = 8 * params["nsamps"] * 2 * nfreq0 * nbf
+        props = torch.cuda.get_device_properties(local_rank)
+        mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+        fp32_peak = 2 * 128 * props.multi_processor_count * mhz * 1e6 / 1e12
+        ach = flops / (bf_ms / 1e3) / 1e12
+        roof = {"bound": "fp32", "kernel": "brute_fold_l0 (fourier_dft_kernel)", "achieved": ach,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                "peak_source": "nominal FP32 FMA rate: 128 lanes x 2 flop x SMs x max SM clock",
+                "algorithmic_flops": flops, "avg_ms": bf_ms, "traffic": B.ncu_traffic("fourier_dft"),
+                "merge_hbm_frac": merges, "hbm_peak": peak, "hbm_peak_source": peak_kind}
     e2e = None
     if not args.no_e2e:
         he, hv = torch.from_numpy(ts_e).pin_memory(), torch.from_numpy(ts_v).pin_memory()
@@ -1021,7 +1038,7 @@ def run_fourier(args, rank, world, local_rank):
     if rank == 0:
         B.emit(_line(args, world, name, value, ms,
                      dict(cfgd, final_coords=int(plan.ncoords[-1]), candidates=ncand, level0_freqs=nfreq0,
-                          lossy_level0=ffa.lossy),
+                          level0_kernel=ffa.level0),
                      roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps * launches, clocks=clk,
                      parity=parity, stages={k: {"ms": p[0], "bytes": p[1]} for k, p in prof.items()}))
     _finish(dist)

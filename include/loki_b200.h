@@ -229,6 +229,10 @@ enum lk_fourier_level0 {
     LK_FOURIER_L0_TENSOR_CORES = 2 /* tcgen05.mma, three FP16 hi / lo passes, FP32 sums */
 };
 int lk_fourier_set_level0(lk_fourier* f, int mode);
+/* Level-0 kernel the executor runs now: LK_FOURIER_L0_CUDA_CORES or
+ * LK_FOURIER_L0_TENSOR_CORES, or LK_FOURIER_L0_AUTO (0) for the lossy level 0
+ * (time-domain brute fold + real transform). */
+int lk_fourier_get_level0(const lk_fourier* f, int* mode);
 /* Synchronises the stream; the device status word (bounded-wait give-ups). */
 int lk_fourier_status(lk_fourier* f, lk_stream_t stream, uint32_t* status);
 /* nbins_f; final fold sizes (complex values, and floats back in time);

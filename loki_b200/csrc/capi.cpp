@@ -653,6 +653,16 @@ int lk_fourier_set_level0(lk_fourier* f, int mode) {
     });
 }
 
+int lk_fourier_get_level0(const lk_fourier* f, int* mode) {
+    return guarded([&] {
+        need(f, "f");
+        need(mode, "mode");
+        const auto& e = *f->exec;
+        *mode = e.lossy ? LK_FOURIER_L0_AUTO
+                        : (e.uses_mma() ? LK_FOURIER_L0_TENSOR_CORES : LK_FOURIER_L0_CUDA_CORES);
+    });
+}
+
 int lk_fourier_status(lk_fourier* f, lk_stream_t stream, uint32_t* status) {
     return guarded([&] {
         need(f, "f");

@@ -295,18 +295,21 @@ rfft_kernel(const float* __restrict__ in, float2* __restrict__ out, uint64_t npr
 //
 // One block of kFinCells final cells (nbins <= 64, one final segment).
 // Phase 1, all threads: the merged harmonics of the block's cells (tail and
-// head rows of the previous level rotated and added, as fourier_merge_kernel)
-// into shared memory as [harmonic][cell] (E re, E im, V re, V im).
-// Phase 2, a thread per cell: the inverse transform by sums over the
-// harmonics with the folding symmetries of the c2r kernel (x_j and x_{n-j}
-// from one cosine and one sine sum; for n divisible by 4 also x_{n/2-j} and
-// x_{n/2+j} from the even and odd harmonics apart), each output normalised
-// E / sqrt(V) into the cell's row. Phase 3: the boxcar scorer on the row.
-// The twiddle table holds (c_m / n) (cos, sin)(2 pi m j / n) for the j a
-// thread evaluates (c_m = 1 for the DC and Nyquist terms, else 2), so the
-// scale of the c2r transform and the unused imaginary parts of the DC and
-// Nyquist terms come out of the table.
+// head rows of the previous level rotated and added, as fourier_merge_kernel;
+// consecutive threads take consecutive harmonics of a row) into shared memory
+// as [harmonic][cell] (E re, E im, V re, V im), rows padded by one entry.
+// Phase 2, a thread per cell: its harmonics into registers, then the inverse
+// transform by sums over the harmonics with the folding symmetries of the c2r
+// kernel (x_j and x_{n-j} from one cosine and one sine sum; for n divisible
+// by 4 also x_{n/2-j} and x_{n/2+j} from the even and odd harmonics apart),
+// each output normalised E / sqrt(V) into the cell's row, which reuses the
+// harmonic tile. Phase 3: the boxcar scorer on the row. The twiddle table
+// holds (c_m / n) (cos, sin)(2 pi m j / n) for the j a thread evaluates
+// (c_m = 1 for the DC and Nyquist terms, else 2), so the scale of the c2r
+// transform and the unused imaginary parts of the DC and Nyquist terms come
+// out of the table.
 constexpr uint32_t kFinCells = 64;
+constexpr uint32_t kFinPitch = kFinCells + 1;  // float4 entries per harmonic row
 
 struct FinalArgs {
     const float2* in;       // level L-2 complex fold [2 segments][nprev][2][nbf]
@@ -318,13 +321,13 @@ struct FinalArgs {
     ScoreParams sp;
 };
 
-template <bool TAYLOR, int NW>
+template <bool TAYLOR, int NW, int NBF>
 __global__ void __launch_bounds__(kFinCells)
 fourier_final_kernel(FinalArgs a) {
     extern __shared__ float4 fsm[];
-    float4* coef = fsm;                                               // [nbf][kFinCells]
-    float2* tw = reinterpret_cast<float2*>(coef + a.nbf * kFinCells);  // [jcount][nbf]
-    float* rows = reinterpret_cast<float*>(tw + a.jcount * a.nbf);     // [kFinCells][rs]
+    float2* tw = reinterpret_cast<float2*>(fsm);                       // [jcount][nbf]
+    float4* coef = fsm + (a.jcount * a.nbf + 1) / 2;                   // [nbf][kFinPitch]
+    float* rows = reinterpret_cast<float*>(coef);                      // [kFinCells][rs], after phase 2 loads
     const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kFinCells;
     const uint64_t left = a.ncur - c0;
     const uint32_t ncells = left < kFinCells ? static_cast<uint32_t>(left) : kFinCells;
@@ -361,10 +364,17 @@ fourier_final_kernel(FinalArgs a) {
             tv = cmul(tv, pt);
         }
         const float2 he = cmul(__ldg(head), ph), hv = cmul(__ldg(head + a.nbf), ph);
-        coef[k * kFinCells + cl] = make_float4(te.x + he.x, te.y + he.y, tv.x + hv.x, tv.y + hv.y);
+        coef[k * kFinPitch + cl] = make_float4(te.x + he.x, te.y + he.y, tv.x + hv.x, tv.y + hv.y);
     }
     __syncthreads();
     const uint32_t t = threadIdx.x;
+    float4 x[NBF];
+#pragma unroll
+    for (int m = 0; m < NBF; ++m) {
+        x[m] = (t < ncells && m < static_cast<int>(a.nbf)) ? coef[m * kFinPitch + t]
+                                                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    __syncthreads();  // the harmonic tile becomes the rows
     if (t >= ncells) {
         return;
     }
@@ -375,31 +385,32 @@ fourier_final_kernel(FinalArgs a) {
         float ce0 = 0.0f, ce1 = 0.0f, se0 = 0.0f, se1 = 0.0f;  // E: even / odd harmonics
         float cv0 = 0.0f, cv1 = 0.0f, sv0 = 0.0f, sv1 = 0.0f;  // V
         const float2* twj = tw + j * a.nbf;
-        for (uint32_t m = 0; m < a.nbf; m += 2) {
-            const float4 x = coef[m * kFinCells + t];
-            const float2 w = twj[m];
-            ce0 = fmaf(x.x, w.x, ce0);
-            se0 = fmaf(x.y, w.y, se0);
-            cv0 = fmaf(x.z, w.x, cv0);
-            sv0 = fmaf(x.w, w.y, sv0);
-            if (m + 1 < a.nbf) {
-                const float4 y = coef[(m + 1) * kFinCells + t];
-                const float2 u = twj[m + 1];
-                ce1 = fmaf(y.x, u.x, ce1);
-                se1 = fmaf(y.y, u.y, se1);
-                cv1 = fmaf(y.z, u.x, cv1);
-                sv1 = fmaf(y.w, u.y, sv1);
+#pragma unroll
+        for (int m = 0; m < NBF; ++m) {
+            if (m < static_cast<int>(a.nbf)) {
+                const float2 w = twj[m];
+                if (m % 2 == 0) {
+                    ce0 = fmaf(x[m].x, w.x, ce0);
+                    se0 = fmaf(x[m].y, w.y, se0);
+                    cv0 = fmaf(x[m].z, w.x, cv0);
+                    sv0 = fmaf(x[m].w, w.y, sv0);
+                } else {
+                    ce1 = fmaf(x[m].x, w.x, ce1);
+                    se1 = fmaf(x[m].y, w.y, se1);
+                    cv1 = fmaf(x[m].z, w.x, cv1);
+                    sv1 = fmaf(x[m].w, w.y, sv1);
+                }
             }
         }
         const float ce = ce0 + ce1, se = se0 + se1, cv = cv0 + cv1, sv = sv0 + sv1;
-        r[j] = sc::normalise(ce - se, cv - sv);
+        r[j] = (ce - se) * rsqrtf(cv - sv);
         if (j > 0) {
-            r[n - j] = sc::normalise(ce + se, cv + sv);
+            r[n - j] = (ce + se) * rsqrtf(cv + sv);
         }
         if (quad) {
             const float de = ce0 - ce1, he = se0 - se1, dv = cv0 - cv1, hv = sv0 - sv1;
-            r[n / 2 - j] = sc::normalise(de + he, dv + hv);
-            r[n / 2 + j] = sc::normalise(de - he, dv - hv);
+            r[n / 2 - j] = (de + he) * rsqrtf(dv + hv);
+            r[n / 2 + j] = (de - he) * rsqrtf(dv - hv);
         }
     }
     sc::score_row<NW>(r, n, 1.0f, a.sp, LK_SCORE_PER_WIDTH, a.scores + (c0 + t) * a.sp.nwidths);
@@ -530,22 +541,32 @@ void fourier_final_score(const float2* d_in, const void* d_coords, bool taylor, 
     a.jcount = fourier_final_jcount(nbins);
     a.rs = sc::row_stride(nbins, sp.wmax);
     a.sp = sp;
-    const size_t smem = sizeof(float4) * a.nbf * kFinCells + sizeof(float2) * a.jcount * a.nbf +
-                        sizeof(float) * kFinCells * a.rs;
+    const size_t tile = std::max(sizeof(float4) * a.nbf * kFinPitch, sizeof(float) * kFinCells * a.rs);
+    const size_t smem = sizeof(float4) * ((a.jcount * a.nbf + 1) / 2) + tile;
     const uint64_t blocks = (ncur + kFinCells - 1) / kFinCells;
     require(blocks <= 0x7fffffffULL, "fused Fourier final level: too many cells");
     auto launch = [&](auto kern) {
         sc::set_smem(kern, smem);
         kern<<<static_cast<uint32_t>(blocks), kFinCells, smem, s>>>(a);
     };
-    auto by_nw = [&](auto tay) {
+    auto by_nbf = [&](auto tay, auto nw) {
         constexpr bool T = decltype(tay)::value;
-        if (sp.nwidths <= 8) {
-            launch(fourier_final_kernel<T, 8>);
-        } else if (sp.nwidths <= 16) {
-            launch(fourier_final_kernel<T, 16>);
+        constexpr int NW = decltype(nw)::value;
+        if (a.nbf <= 9) {
+            launch(fourier_final_kernel<T, NW, 9>);
+        } else if (a.nbf <= 17) {
+            launch(fourier_final_kernel<T, NW, 17>);
         } else {
-            launch(fourier_final_kernel<T, 32>);
+            launch(fourier_final_kernel<T, NW, 33>);
+        }
+    };
+    auto by_nw = [&](auto tay) {
+        if (sp.nwidths <= 8) {
+            by_nbf(tay, std::integral_constant<int, 8>{});
+        } else if (sp.nwidths <= 16) {
+            by_nbf(tay, std::integral_constant<int, 16>{});
+        } else {
+            by_nbf(tay, std::integral_constant<int, 32>{});
         }
     };
     if (taylor) {

@@ -39,6 +39,8 @@ constexpr uint32_t kMaxN = 256;       // MMA N per instruction
 constexpr uint32_t kThreads = 192;    // 6 warps
 constexpr uint32_t kGenThreads = 128; // warps 2-5
 constexpr uint32_t kAnchor = 8;       // stages between exact phasor anchors (256 samples)
+constexpr uint32_t kPartChunks = 64;  // K chunks per part at most (2048 samples), before rounding
+constexpr uint32_t kMaxParts = 8;
 constexpr uint32_t kRowBytes = kKc * 2;               // 64
 constexpr uint32_t kATileBytes = kRows * kRowBytes;   // 8 KB per (hi | lo)
 
@@ -65,7 +67,9 @@ struct MmaArgs {
     uint32_t fpt;         // frequencies per tile
     uint32_t ntile;       // MMA N (columns per subtile)
     uint32_t nsub;        // subtiles per block (1 or 2)
-    uint32_t nk;          // K chunks
+    uint32_t nk;          // K chunks of the segment
+    uint32_t cpp;         // K chunks per part (a multiple of kAnchor); part z = blockIdx.z
+    uint64_t part_stride; // floats between the parts' partial folds (0: one part)
     uint32_t tmem_cols;
 };
 
@@ -200,16 +204,22 @@ fourier_dft_mma_kernel(const __grid_constant__ CUtensorMap map_hi,
 
     const uint32_t mt = blockIdx.x;                      // frequency tile
     const uint32_t col0 = blockIdx.y * a.nsub * a.ntile; // first B row of this block
+    // K part of this block: chunks [it0, it0 + nloc); each part sums into its
+    // own partial fold, so no accumulator sums more than cpp chunks
+    const uint32_t it0 = blockIdx.z * a.cpp;
+    const uint32_t nloc = min(a.cpp, a.nk - it0);
+    float* const out = a.out + blockIdx.z * a.part_stride;
 
     if (warp == 0) {
         // ---- TMA producer ----
         if (lane == 0) {
             const uint32_t tx = 2 * bbytes;
             uint32_t issued = 0;
-            for (uint32_t it = 0; it < a.nk; ++it) {
-                const uint32_t s = it % kStages;
-                if (it >= kStages &&
-                    !ptx::mbar_wait_bounded(&empty[s], ((it / kStages) - 1) & 1, a.status, kStProdWait)) {
+            for (uint32_t li = 0; li < nloc; ++li) {
+                const uint32_t it = it0 + li;
+                const uint32_t s = li % kStages;
+                if (li >= kStages &&
+                    !ptx::mbar_wait_bounded(&empty[s], ((li / kStages) - 1) & 1, a.status, kStProdWait)) {
                     break;
                 }
                 ptx::mbar_arrive_expect_tx(&full_b[s], tx);
@@ -219,20 +229,20 @@ fourier_dft_mma_kernel(const __grid_constant__ CUtensorMap map_hi,
                     ptx::tma_load_2d(b_hi(s) + sub * a.ntile * kRowBytes, &map_hi, &full_b[s], x, y);
                     ptx::tma_load_2d(b_lo(s) + sub * a.ntile * kRowBytes, &map_lo, &full_b[s], x, y);
                 }
-                issued = it + 1;
+                issued = li + 1;
             }
             // the copies of the last stages land before the block can exit
-            for (uint32_t it = (issued > kStages ? issued - kStages : 0); it < issued; ++it) {
-                ptx::mbar_wait_bounded(&full_b[it % kStages], (it / kStages) & 1, a.status, kStProdWait);
+            for (uint32_t li = (issued > kStages ? issued - kStages : 0); li < issued; ++li) {
+                ptx::mbar_wait_bounded(&full_b[li % kStages], (li / kStages) & 1, a.status, kStProdWait);
             }
         }
     } else if (warp == 1) {
         // ---- MMA issuer ----
         if (lane == 0) {
             const uint32_t idesc = idesc_f16(a.ntile);
-            for (uint32_t it = 0; it < a.nk; ++it) {
-                const uint32_t s = it % kStages;
-                const uint32_t par = (it / kStages) & 1;
+            for (uint32_t li = 0; li < nloc; ++li) {
+                const uint32_t s = li % kStages;
+                const uint32_t par = (li / kStages) & 1;
                 if (!ptx::mbar_wait_bounded(&full_a[s], par, a.status, kStMmaWaitA) ||
                     !ptx::mbar_wait_bounded(&full_b[s], par, a.status, kStMmaWaitB)) {
                     break;
@@ -245,7 +255,7 @@ fourier_dft_mma_kernel(const __grid_constant__ CUtensorMap map_hi,
                     const uint32_t boff = sub * a.ntile * kRowBytes;
 #pragma unroll
                     for (uint32_t kk = 0; kk < kKc / 16; ++kk) {
-                        const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+                        const uint32_t acc = (li > 0 || kk > 0) ? 1u : 0u;
                         mma_f16(d, sdesc(ah + 32 * kk), sdesc(bh + boff + 32 * kk), idesc, acc);
                         mma_f16(d, sdesc(ah + 32 * kk), sdesc(bl + boff + 32 * kk), idesc, 1u);
                         mma_f16(d, sdesc(al + 32 * kk), sdesc(bh + boff + 32 * kk), idesc, 1u);
@@ -270,10 +280,11 @@ fourier_dft_mma_kernel(const __grid_constant__ CUtensorMap map_hi,
         const float2 w1 = unit_phasor(static_cast<double>(m) * ustep);
         const float2 w32 = unit_phasor(static_cast<double>(m) * ustep * static_cast<double>(kKc));
         float2 start = make_float2(1.0f, 0.0f);
-        for (uint32_t it = 0; it < a.nk; ++it) {
-            const uint32_t s = it % kStages;
-            if (it >= kStages &&
-                !ptx::mbar_wait_bounded(&empty[s], ((it / kStages) - 1) & 1, a.status, kStGenWait)) {
+        for (uint32_t li = 0; li < nloc; ++li) {
+            const uint32_t it = it0 + li;
+            const uint32_t s = li % kStages;
+            if (li >= kStages &&
+                !ptx::mbar_wait_bounded(&empty[s], ((li / kStages) - 1) & 1, a.status, kStGenWait)) {
                 break;
             }
             const uint64_t k0 = static_cast<uint64_t>(it) * kKc + 16 * h;
@@ -343,10 +354,10 @@ fourier_dft_mma_kernel(const __grid_constant__ CUtensorMap map_hi,
                             const uint32_t ev = n >= a.nseg ? 1u : 0u;
                             const uint64_t sg = n - ev * a.nseg;
                             const uint64_t row = ((sg * a.nfreq + ef) * 2 + ev) * a.nbf;
-                            a.out[(row + em) * 2 + ec] = v[j] * (ev ? scale_v : scale_e);
+                            out[(row + em) * 2 + ec] = v[j] * (ev ? scale_v : scale_e);
                             if (em == 1 && ec == 0) {
-                                a.out[row * 2] = a.dc[n];
-                                a.out[row * 2 + 1] = 0.0f;
+                                out[row * 2] = blockIdx.z == 0 ? a.dc[n] : 0.0f;
+                                out[row * 2 + 1] = 0.0f;
                             }
                         }
                     }
@@ -438,6 +449,23 @@ stage_rows_kernel(const float* __restrict__ e, const float* __restrict__ v, uint
     }
 }
 
+// out[i] = sum over the parts of part[p][i], in part order (FP32).
+__global__ void sum_parts_kernel(const float4* __restrict__ parts, uint64_t n4, uint32_t nparts,
+                                 float4* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n4;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        float4 acc = __ldg(parts + i);
+        for (uint32_t p = 1; p < nparts; ++p) {
+            const float4 x = __ldg(parts + p * n4 + i);
+            acc.x += x.x;
+            acc.y += x.y;
+            acc.z += x.z;
+            acc.w += x.w;
+        }
+        out[i] = acc;
+    }
+}
+
 }  // namespace
 
 bool fourier_mma_supported(uint64_t seglen, uint64_t nseg, uint32_t nbins) {
@@ -467,6 +495,17 @@ FourierMma::FourierMma(uint64_t seglen_, uint64_t nseg_, uint32_t nbins_, uint32
     while (tmem_cols < nsub * ntile) {
         tmem_cols *= 2;
     }
+    // K parts of at most kPartChunks chunks each (anchored starts): shorter
+    // accumulation chains in tensor memory, and more blocks per wave
+    const uint32_t nk = static_cast<uint32_t>((seglen + kKc - 1) / kKc);
+    const uint32_t want = std::min<uint32_t>(kMaxParts, (nk + kPartChunks - 1) / kPartChunks);
+    cpp = (nk + want - 1) / want;
+    cpp = (cpp + kAnchor - 1) / kAnchor * kAnchor;
+    nparts = (nk + cpp - 1) / cpp;
+    if (nparts > 1) {
+        const uint64_t elems = 2 * nseg * nfreq * 2 * static_cast<uint64_t>(nbins / 2 + 1);  // floats
+        parts.alloc(sizeof(float) * elems * nparts);
+    }
     auto encode = [&](CUtensorMap* map, void* ptr) {
         cuuint64_t dims[2] = {seglen, rows};
         cuuint64_t strides[1] = {seglen * sizeof(__half)};
@@ -488,7 +527,9 @@ FourierMma::FourierMma(uint64_t seglen_, uint64_t nseg_, uint32_t nbins_, uint32
                                  static_cast<int>(smem_bytes)));
 }
 
-uint64_t FourierMma::device_bytes() const { return hi.bytes + lo.bytes + dc.bytes + aux.bytes; }
+uint64_t FourierMma::device_bytes() const {
+    return hi.bytes + lo.bytes + dc.bytes + aux.bytes + parts.bytes;
+}
 
 void FourierMma::run(const float* d_ts_e, const float* d_ts_v, const double* d_freqs, double tsamp,
                      double t_ref, float2* d_out, uint32_t* d_status, cudaStream_t s) {
@@ -504,10 +545,12 @@ void FourierMma::run(const float* d_ts_e, const float* d_ts_v, const double* d_f
         dc.as<float>(), qexp);
     LK_CUDA(cudaGetLastError());
     MmaArgs a{};
+    const uint64_t elems = 2 * nseg * static_cast<uint64_t>(nfreq) * 2 * (nbins / 2 + 1);  // floats
     a.freqs = d_freqs;
     a.dc = dc.as<float>();
     a.qexp = qexp;
-    a.out = reinterpret_cast<float*>(d_out);
+    a.out = nparts > 1 ? parts.as<float>() : reinterpret_cast<float*>(d_out);
+    a.part_stride = nparts > 1 ? elems : 0;
     a.status = d_status;
     a.seglen = seglen;
     a.tsamp = tsamp;
@@ -520,10 +563,17 @@ void FourierMma::run(const float* d_ts_e, const float* d_ts_v, const double* d_f
     a.ntile = ntile;
     a.nsub = nsub;
     a.nk = static_cast<uint32_t>((seglen + kKc - 1) / kKc);
+    a.cpp = cpp;
     a.tmem_cols = tmem_cols;
     const uint32_t mtiles = (nfreq + a.fpt - 1) / a.fpt;
-    fourier_dft_mma_kernel<<<dim3(mtiles, ngroups), kThreads, smem_bytes, s>>>(map_hi, map_lo, a);
+    fourier_dft_mma_kernel<<<dim3(mtiles, ngroups, nparts), kThreads, smem_bytes, s>>>(map_hi, map_lo, a);
     LK_CUDA(cudaGetLastError());
+    if (nparts > 1) {
+        const uint64_t n4 = elems / 4;  // elems = 4 * (...) floats
+        sum_parts_kernel<<<static_cast<uint32_t>(std::min<uint64_t>((n4 + 255) / 256, 148 * 16)), 256, 0, s>>>(
+            parts.as<float4>(), n4, nparts, reinterpret_cast<float4*>(d_out));
+        LK_CUDA(cudaGetLastError());
+    }
 }
 
 }  // namespace lk

@@ -50,8 +50,10 @@ struct FourierMma {
     uint64_t seglen, nseg;
     uint32_t nbins, nfreq;
     uint32_t ntile = 0, nsub = 0, ngroups = 0, tmem_cols = 0;
+    uint32_t cpp = 0, nparts = 1;  // K chunks per part, parts (partial folds summed in FP32)
     size_t smem_bytes = 0;
     DeviceBuffer hi, lo, dc, aux;  // FP16 staging [2 nseg][seglen], row sums, max / exponents
+    DeviceBuffer parts;            // [nparts][level-0 fold] partial folds (nparts > 1)
     CUtensorMap map_hi{}, map_lo{};
     FourierMma(uint64_t seglen, uint64_t nseg, uint32_t nbins, uint32_t nfreq);
     uint64_t device_bytes() const;

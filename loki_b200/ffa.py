@@ -422,6 +422,13 @@ class FFACOMPLEXCUDA:
         the shape allows), "cuda_cores" or "tensor_cores"."""
         C.check(C.lib().lk_fourier_set_level0(self._h, self._LEVEL0[mode]))
 
+    @property
+    def level0(self) -> str:
+        """Level-0 kernel in use: "tensor_cores", "cuda_cores" or "lossy"."""
+        m = ctypes.c_int()
+        C.check(C.lib().lk_fourier_get_level0(self._h, ctypes.byref(m)))
+        return {0: "lossy", 1: "cuda_cores", 2: "tensor_cores"}[m.value]
+
     def status(self) -> int:
         """Device status word (bits set by bounded waits that gave up)."""
         st = ctypes.c_uint32()

@@ -5,8 +5,10 @@ fixtures, against the reference's own FFA<ComplexType>.
 The path sums in FP32 with phasors from phases reduced in FP64, so the bar
 is a tolerance written here: complex and back-in-time folds within
 FOLD_RTOL of the fold's largest magnitude of the FP64 oracle, S/N within
-SNR_ATOL of the oracle's FP64 S/N, and candidate sets equal to the oracle's
-except for cells whose FP64 S/N lies within SNR_ATOL of the threshold.
+SNR_ATOL + SNR_RTOL |S/N| of the oracle's FP64 S/N (an FP32 sum's error
+grows with its value; the reference's own FP32 Fourier path sits up to
+7e-5 |S/N| from FP64), and candidate sets equal to the oracle's except for
+cells whose FP64 S/N lies within that tolerance of the threshold.
 """
 
 from __future__ import annotations
@@ -21,6 +23,13 @@ pytestmark = pytest.mark.gpu
 
 FOLD_RTOL = 2e-5
 SNR_ATOL = 1e-3
+SNR_RTOL = 5e-5
+
+
+def _snr_ok(got, want):
+    got = np.asarray(got, dtype=np.float64)
+    want = np.asarray(want, dtype=np.float64)
+    return bool(np.all(np.abs(got - want) <= SNR_ATOL + SNR_RTOL * np.abs(want)))
 FIXTURES = ["fourier_freq_nb32", "fourier_freq_nb64", "fourier_accel_nb16", "fourier_jerk_nb16",
             "fourier_freq_nb128_lossy"]
 # name -> (nsamps, tsamp, nbins, eta, param_limits)
@@ -96,7 +105,7 @@ def test_ffa_vs_reference_fixture(cuda, name):
         assert _rel(tfold, g["fold_time"]) < 2 * FOLD_RTOL
     s = ffa.scores(g["ts_e"], g["ts_v"])
     s64 = lko.ffa_fourier_scores64(op, g["ts_e"], g["ts_v"], op.widths).ravel()
-    assert np.abs(s - s64).max() < SNR_ATOL
+    assert _snr_ok(s, s64)
     assert np.abs(s - g["scores"]).max() < 2 * SNR_ATOL
 
 
@@ -113,15 +122,16 @@ def test_ffa_vs_oracle(cuda, name):
     assert _rel(fold, want) < FOLD_RTOL
     s = ffa.scores(ts_e, ts_v)
     s64 = lko.ffa_fourier_scores64(op, ts_e, ts_v, op.widths).ravel()
-    assert np.abs(s - s64).max() < SNR_ATOL
+    assert _snr_ok(s, s64)
     # candidate set of a threshold inside the S/N distribution
     thr = float(np.quantile(s64, 0.999))
     idx, snr, total = ffa.search(ts_e, ts_v, snr_min=thr, max_cands=1 << 20)
     assert total == idx.size
     assert np.all(np.diff(idx.astype(np.int64)) > 0)
     assert np.array_equal(snr, s[idx])
-    sure = np.flatnonzero(s64 >= thr + SNR_ATOL)
-    maybe = np.flatnonzero(s64 >= thr - SNR_ATOL)
+    tol = SNR_ATOL + SNR_RTOL * abs(thr)
+    sure = np.flatnonzero(s64 >= thr + tol)
+    maybe = np.flatnonzero(s64 >= thr - tol)
     assert np.isin(sure, idx).all() and np.isin(idx, maybe).all()
 
 
@@ -193,7 +203,7 @@ def test_level0_tensor_cores_vs_cuda_cores(cuda, name):
         assert ffa.status() == 0
         assert _rel(fold, final) < FOLD_RTOL, mode
         s = ffa.scores(ts_e, ts_v)
-        assert np.abs(s - s64).max() < SNR_ATOL, mode
+        assert _snr_ok(s, s64), mode
     # level 0 alone through the brute-fold entry (the direct transform on the CUDA cores)
     want0 = lko.ffa_fourier(op, ts_e, ts_v, level=0).ravel()
     freqs = ffa.plan.compute_param_grid(0)[-1]
