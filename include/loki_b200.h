@@ -305,6 +305,20 @@ typedef struct lk_sweep_options {
      * series (lk_ffa_autotune) and keep them, also for executors re-created
      * in mode 2; results do not change. */
     int32_t autotune;
+    /* 1: every chunk through the Fourier-domain FFA (lk_fourier_*), as
+     * FFAFreqSweep does for use_fourier = true (lib/ffa_freq_sweep.cpp:
+     * 273-281); the planner then sizes fold buffers in complex harmonics of
+     * 8 bytes (FFAPlan<ComplexType>, lib/regions.cpp:111-115). */
+    int32_t use_fourier;
+    /* nbins above which a Fourier chunk's level 0 is the lossy one (0: 64). */
+    uint64_t nbins_min_lossy_bf;
+    /* Fold-buffer sizes of the plan: 0 as the executors need them (complex
+     * harmonics with use_fourier, else nbins per row), 1 nbins per row
+     * (FFARegionPlanner<float>), 2 nbins / 2 + 1 harmonics per row
+     * (FFARegionPlanner<ComplexType>). Fold elements count 8 bytes with
+     * use_fourier, else 4, whatever the sizes (lib/regions.cpp:111-115).
+     * 1 and 2 are for planning only. */
+    int32_t plan_sizes;
 } lk_sweep_options;
 /* regions::generate_ffa_regions (lib/regions.cpp:31-78): rows of (f_start,
  * f_end, nbins, eta); *n_out regions, rows written up to cap. */

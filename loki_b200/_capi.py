@@ -113,7 +113,8 @@ class LkSweepOptions(ctypes.Structure):
     _fields_ = [("max_memory_gb", f64), ("octave_scale", f64), ("nbins_max", u64),
                 ("max_passing_candidates", u64), ("decode_chunk_widths", ctypes.c_int32),
                 ("device_memory_model", ctypes.c_int32), ("executor_mode", ctypes.c_int32),
-                ("autotune", ctypes.c_int32)]
+                ("autotune", ctypes.c_int32), ("use_fourier", ctypes.c_int32), ("nbins_min_lossy_bf", u64),
+                ("plan_sizes", ctypes.c_int32)]
 
 
 class LkSweepChunk(ctypes.Structure):

@@ -343,6 +343,10 @@ int lk_sweep_create(const lk_config* base, const lk_sweep_options* opt, int devi
                         "executor_mode must be 0 (auto), 1 (resident) or 2 (one chunk at a time)");
             o.executor_mode = opt->executor_mode;
             o.autotune = opt->autotune != 0;
+            o.use_fourier = opt->use_fourier != 0;
+            o.nbins_min_lossy_bf = opt->nbins_min_lossy_bf == 0 ? 64 : opt->nbins_min_lossy_bf;
+            lk::require(opt->plan_sizes >= 0 && opt->plan_sizes <= 2, "plan_sizes must be 0, 1 or 2");
+            o.plan_sizes = opt->plan_sizes;
         }
         lk::require(o.max_memory_gb > 0, "max_process_memory_gb must be positive");
         auto h = std::make_unique<lk_sweep>();

@@ -4,6 +4,8 @@
 #include <memory>
 #include <vector>
 
+#include "lk_ffa.hpp"
+#include "lk_fourier.hpp"
 #include "lk_internal.hpp"
 #include "lk_kernels.hpp"
 
@@ -28,6 +30,9 @@ struct SweepOptions {
     bool device_memory_model = true;   // FFAFreqSweepCUDA's model; false: FFAFreqSweep's
     int executor_mode = 0;             // 0 auto, 1 resident, 2 one chunk at a time
     bool autotune = false;             // tune each chunk executor's launch shapes once
+    bool use_fourier = false;          // chunks through the Fourier-domain FFA
+    uint64_t nbins_min_lossy_bf = 64;  // Fourier chunks: lossy level 0 above this nbins
+    int plan_sizes = 0;  // 0 as the executors need, 1 FFARegionPlanner<float>, 2 <ComplexType>
 };
 
 // One chunk: its configuration (drift-widened frequency limits, the region's
@@ -44,6 +49,23 @@ std::vector<SweepRegion> generate_ffa_regions(double p_min, double p_max, double
                                               uint64_t nbins_min, double eta_min,
                                               double octave_scale, uint64_t nbins_max);
 std::vector<SweepChunk> plan_freq_sweep(const lk_config& base, const SweepOptions& opt);
+
+// One chunk's executor: the time-domain FFA, or the Fourier-domain FFA.
+struct ChunkExec {
+    std::unique_ptr<FFAExec> t;
+    std::unique_ptr<FourierExec> f;
+    const Plan& plan() const { return t ? t->plan : f->plan; }
+    StageProfiler& prof() { return t ? t->prof : f->prof; }
+    std::vector<lk_stage_time> profile(cudaStream_t s) { return t ? t->profile(s) : f->profile(s); }
+    void search(const float* ts_e, const float* ts_v, float snr_min, uint32_t* d_idx, float* d_snr,
+                uint64_t max_cands, uint64_t* d_count, cudaStream_t s) {
+        if (t) {
+            t->search(ts_e, ts_v, snr_min, d_idx, d_snr, max_cands, d_count, s);
+        } else {
+            f->search(ts_e, ts_v, snr_min, d_idx, d_snr, max_cands, d_count, s);
+        }
+    }
+};
 
 class FreqSweepExec {
 public:
@@ -64,15 +86,16 @@ public:
     std::vector<lk_stage_time> profile(cudaStream_t s);
 
 private:
-    FFAExec& exec(size_t i);
+    ChunkExec& exec(size_t i);
     // exec(i), its launch shapes tuned on (or restored for) these series
-    FFAExec& tuned_exec(size_t i, const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
+    // (time-domain chunks)
+    ChunkExec& tuned_exec(size_t i, const float* d_ts_e, const float* d_ts_v, cudaStream_t s);
     lk_config m_base;
     SweepOptions m_opt;
     int m_device, m_storage;
     std::vector<SweepChunk> m_chunks;
     std::vector<uint32_t> m_base_widths;
-    std::vector<std::unique_ptr<FFAExec>> m_execs;
+    std::vector<std::unique_ptr<ChunkExec>> m_execs;
     DeviceBuffer m_idx, m_snr, m_cnt;
     std::vector<double> m_params;
     std::vector<float> m_scores;

@@ -32,9 +32,9 @@ constexpr uint64_t kWriteBatchSize = 1u << 16;  // kFFAFreqSweepWriteBatchSize
 
 // FFARegionStats::get_cpu_memory_usage (lib/regions.cpp:101-135), in GB.
 float cpu_memory_gb(uint64_t buf, uint64_t coord, uint64_t nc, uint64_t n_widths,
-                    uint32_t n_params, uint64_t max_passing) {
+                    uint32_t n_params, uint64_t max_passing, uint64_t fold_bytes) {
     const float gib = static_cast<float>(1ull << 30);
-    const float buffer = static_cast<float>(2 * buf * sizeof(float)) / gib;
+    const float buffer = static_cast<float>(2 * buf * fold_bytes) / gib;
     const uint64_t coord_bytes = coord * (n_params == 1 ? 8 : 16);
     const float coords = static_cast<float>(coord_bytes) / gib;
     const uint64_t scores = std::max(nc * n_widths, max_passing);
@@ -49,13 +49,13 @@ float cpu_memory_gb(uint64_t buf, uint64_t coord, uint64_t nc, uint64_t n_widths
 // the input series, scores and passing indices on the device, then the fold
 // buffers and coordinates.
 float device_memory_gb(uint64_t buf, uint64_t coord, uint64_t nc, uint64_t n_widths,
-                       uint32_t n_params, uint64_t nsamps, uint64_t max_passing) {
+                       uint32_t n_params, uint64_t nsamps, uint64_t max_passing, uint64_t fold_bytes) {
     const float gib = static_cast<float>(1ull << 30);
     const uint64_t scores = std::max(nc * n_widths, max_passing);
     const float extra = static_cast<float>((((2 * nsamps) + scores) * sizeof(float)) +
                                            (scores * sizeof(uint32_t))) /
                         gib;
-    const float buffer = static_cast<float>(2 * buf * sizeof(float)) / gib;
+    const float buffer = static_cast<float>(2 * buf * fold_bytes) / gib;
     const uint64_t coord_bytes = coord * (n_params == 1 ? 8 : 16);
     const float coords = static_cast<float>(coord_bytes) / gib;
     return extra + buffer + coords;
@@ -139,12 +139,14 @@ std::vector<SweepChunk> plan_freq_sweep(const lk_config& base, const SweepOption
 
     // get_freq_sweep_memory_usage: the device model for FFAFreqSweepCUDA, the
     // process model for FFAFreqSweep.
+    // fold elements are complex harmonics (8 bytes) for the Fourier-domain FFA
+    const uint64_t fold_bytes = opt.use_fourier ? 8 : sizeof(float);
     auto memory_gb = [&](uint64_t buf, uint64_t coord, uint64_t nc) -> double {
         if (opt.device_memory_model) {
             return device_memory_gb(buf, coord, nc, n_widths, np, base.nsamps,
-                                    opt.max_passing_candidates);
+                                    opt.max_passing_candidates, fold_bytes);
         }
-        return cpu_memory_gb(buf, coord, nc, n_widths, np, opt.max_passing_candidates);
+        return cpu_memory_gb(buf, coord, nc, n_widths, np, opt.max_passing_candidates, fold_bytes);
     };
     std::vector<SweepChunk> chunks;
     uint64_t mbuf = 0, mcoord = 0, mnc = 0, mlv = 0;
@@ -176,7 +178,11 @@ std::vector<SweepChunk> plan_freq_sweep(const lk_config& base, const SweepOption
             const Plan pl = make_plan(ch.cfg, /*sizes_only=*/true);
             ch.nominal_f_start = nominal_start;
             ch.nominal_f_end = nominal_end;
-            ch.buffer_size = pl.buffer_size;
+            // FFAPlan<ComplexType>::get_buffer_size counts nbins / 2 + 1 harmonics per row
+            const bool complex_sizes =
+                opt.plan_sizes == 2 || (opt.plan_sizes == 0 && opt.use_fourier);
+            ch.buffer_size = complex_sizes ? pl.buffer_size / rg.nbins * (rg.nbins / 2 + 1)
+                                           : pl.buffer_size;
             ch.coord_size = pl.coord_size;
             ch.ncoords = pl.ncoords.back();
             ch.n_levels = pl.n_levels;
@@ -251,21 +257,29 @@ FreqSweepExec::FreqSweepExec(const lk_config& base, const SweepOptions& opt, int
     m_execs.resize(m_chunks.size());
 }
 
-FFAExec& FreqSweepExec::exec(size_t i) {
+ChunkExec& FreqSweepExec::exec(size_t i) {
     if (!m_execs[i]) {
-        m_execs[i] = std::make_unique<FFAExec>(make_plan(m_chunks[i].cfg), m_device, m_storage);
-        m_execs[i]->prof.enabled = m_profiling;
+        auto c = std::make_unique<ChunkExec>();
+        if (m_opt.use_fourier) {
+            c->f = std::make_unique<FourierExec>(make_plan(m_chunks[i].cfg), m_device,
+                                                 m_opt.nbins_min_lossy_bf);
+        } else {
+            c->t = std::make_unique<FFAExec>(make_plan(m_chunks[i].cfg), m_device, m_storage);
+        }
+        c->prof().enabled = m_profiling;
+        m_execs[i] = std::move(c);
     }
     return *m_execs[i];
 }
 
-FFAExec& FreqSweepExec::tuned_exec(size_t i, const float* d_ts_e, const float* d_ts_v,
-                                   cudaStream_t s) {
+ChunkExec& FreqSweepExec::tuned_exec(size_t i, const float* d_ts_e, const float* d_ts_v,
+                                     cudaStream_t s) {
     const bool fresh = !m_execs[i];
-    FFAExec& ex = exec(i);
-    if (!m_opt.autotune) {
-        return ex;
+    ChunkExec& cx = exec(i);
+    if (!m_opt.autotune || !cx.t) {
+        return cx;
     }
+    FFAExec& ex = *cx.t;
     if (m_tuned.size() != m_chunks.size()) {
         m_tuned.assign(m_chunks.size(), false);
         m_tunings.assign(m_chunks.size(), lk_tuning{});
@@ -276,15 +290,15 @@ FFAExec& FreqSweepExec::tuned_exec(size_t i, const float* d_ts_e, const float* d
     } else if (fresh) {
         ex.apply_tuning(m_tunings[i]);
     }
-    return ex;
+    return cx;
 }
 
 void FreqSweepExec::set_profiling(bool enable) {
     m_profiling = enable;
     for (auto& e : m_execs) {
         if (e) {
-            e->prof.enabled = enable;
-            e->prof.reset();
+            e->prof().enabled = enable;
+            e->prof().reset();
         }
     }
     m_prof.clear();
@@ -381,7 +395,7 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
     std::vector<std::vector<uint32_t>> h_idx(nch);
     std::vector<std::vector<float>> h_snr(nch);
     std::vector<Plan> plans(nch);
-    auto add_profile = [&](FFAExec& ex, cudaStream_t st_of) {
+    auto add_profile = [&](ChunkExec& ex, cudaStream_t st_of) {
         for (const lk_stage_time& st : ex.profile(st_of)) {
             auto it = std::find_if(m_prof.begin(), m_prof.end(),
                                    [&](const lk_stage_time& a) { return a.kind == st.kind; });
@@ -414,8 +428,8 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
         }
         LK_CUDA(cudaStreamSynchronize(s));
     };
-    auto check_plan = [](const FFAExec& ex) {
-        require(ex.plan.nsegments[ex.plan.n_levels - 1] == 1,
+    auto check_plan = [](const ChunkExec& ex) {
+        require(ex.plan().nsegments[ex.plan().n_levels - 1] == 1,
                 "FFAFreqSweep::execute_ffa_region: nsegments must be 1 to call scoring function");
     };
     if (resident) {
@@ -445,11 +459,11 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
             if (m_profiling) {
                 add_profile(*m_execs[i], m_streams[i % kSweepStreams]);
             }
-            plans[i] = m_execs[i]->plan;
+            plans[i] = m_execs[i]->plan();
         }
     } else {
         for (size_t i = 0; i < nch; ++i) {
-            FFAExec& ex = tuned_exec(i, d_ts_e, d_ts_v, s);
+            ChunkExec& ex = tuned_exec(i, d_ts_e, d_ts_v, s);
             check_plan(ex);
             ex.search(d_ts_e, d_ts_v, thr, m_idx.as<uint32_t>(), m_snr.as<float>(), cap[i],
                       m_cnt.as<uint64_t>() + i, s);
@@ -457,7 +471,7 @@ void FreqSweepExec::execute(const float* d_ts_e, const float* d_ts_v, cudaStream
             if (m_profiling) {
                 add_profile(ex, s);
             }
-            plans[i] = ex.plan;
+            plans[i] = ex.plan();
             m_execs[i].reset();  // release this chunk's workspace
         }
     }

@@ -239,4 +239,4 @@ class FFAPlanFourier(FFAPlanTime):
 
 
 # The reference binds the region planner in the plans submodule.
-from .sweep import FFARegionPlannerTime, generate_ffa_regions  # noqa: E402
+from .sweep import FFARegionPlannerFourier, FFARegionPlannerTime, generate_ffa_regions  # noqa: E402

@@ -30,13 +30,6 @@ from .configs import PulsarSearchConfig
 _STORAGE = {"fp32": C.LK_FP32, "float32": C.LK_FP32, "bf16": C.LK_BF16, "fp16": C.LK_FP16}
 
 
-def _check_time_domain(cfg: PulsarSearchConfig) -> None:
-    if cfg.use_fourier:
-        raise NotImplementedError(
-            "the Fourier-domain FFA is not implemented; construct the config with use_fourier=False"
-        )
-
-
 FFA_REGION_DTYPE = np.dtype([("f_start", np.float64), ("f_end", np.float64), ("nbins", np.uint64),
                              ("eta", np.float64)])
 
@@ -61,7 +54,7 @@ _EXECUTORS = {None: 0, "auto": 0, "resident": 1, "one_at_a_time": 2}
 
 
 def _options(cfg: PulsarSearchConfig, device_model: bool, decode_chunk_widths: bool,
-             executors=None, autotune: bool = False) -> C.LkSweepOptions:
+             executors=None, autotune: bool = False, plan_sizes: int = 0) -> C.LkSweepOptions:
     o = C.LkSweepOptions()
     o.max_memory_gb = cfg.max_process_memory_gb
     o.octave_scale = cfg.octave_scale
@@ -73,15 +66,17 @@ def _options(cfg: PulsarSearchConfig, device_model: bool, decode_chunk_widths: b
         raise ValueError(f"executors must be one of {sorted(k for k in _EXECUTORS if k)}")
     o.executor_mode = _EXECUTORS[executors]
     o.autotune = int(bool(autotune))
+    o.use_fourier = int(bool(cfg.use_fourier))
+    o.nbins_min_lossy_bf = int(cfg.nbins_min_lossy_bf)
+    o.plan_sizes = int(plan_sizes)
     return o
 
 
 class _SweepHandle:
     def __init__(self, cfg: PulsarSearchConfig, device_id: int, storage: int, device_model: bool,
-                 decode_chunk_widths: bool, executors=None, autotune: bool = False):
-        _check_time_domain(cfg)
+                 decode_chunk_widths: bool, executors=None, autotune: bool = False, plan_sizes: int = 0):
         self._cfg = cfg
-        self._opt = _options(cfg, device_model, decode_chunk_widths, executors, autotune)
+        self._opt = _options(cfg, device_model, decode_chunk_widths, executors, autotune, plan_sizes)
         h = ctypes.c_void_p()
         C.check(C.lib().lk_sweep_create(ctypes.byref(cfg.c_config), ctypes.byref(self._opt), device_id, storage,
                                         ctypes.byref(h)))
@@ -139,18 +134,29 @@ class _SweepHandle:
 
 
 class FFARegionPlannerTime(_SweepHandle):
-    """Chunk plan of a frequency sweep (reference ``FFARegionPlannerTime``).
+    """Chunk plan of a frequency sweep (reference ``FFARegionPlannerTime``,
+    FFARegionPlanner<float>: fold buffers sized in nbins per row; a
+    ``use_fourier`` configuration counts them 8 bytes each, as there).
     ``use_gpu`` selects the device memory model of FFAFreqSweepCUDA (else the
     process model of FFAFreqSweep). Planning touches no device."""
 
     def __init__(self, cfg: PulsarSearchConfig, use_gpu: bool = False):
-        super().__init__(cfg, 0, C.LK_FP32, use_gpu, False)
+        super().__init__(cfg, 0, C.LK_FP32, use_gpu, False, plan_sizes=1)
 
     def get_cfgs(self) -> list[PulsarSearchConfig]:
         return self.cfgs
 
     def get_nregions(self) -> int:
         return self.nregions
+
+
+class FFARegionPlannerFourier(FFARegionPlannerTime):
+    """Chunk plan of the Fourier-domain sweep (reference
+    ``FFARegionPlannerFourier``, FFARegionPlanner<ComplexType>: fold buffers
+    sized in nbins // 2 + 1 complex harmonics per row)."""
+
+    def __init__(self, cfg: PulsarSearchConfig, use_gpu: bool = False):
+        _SweepHandle.__init__(self, cfg, 0, C.LK_FP32, use_gpu, False, plan_sizes=2)
 
 
 class FFAFreqSweepCUDA(_SweepHandle):

@@ -117,6 +117,8 @@ def lib(kind: str = "parity") -> ctypes.CDLL:
         L.lkref_prune_run_full.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, u64, vp, u64, u64, u64, u64, u64,
                                            u64, vp, vp, vp, vp, vp, vp, u64, vp]
         L.lkref_region_plan.argtypes = [vp, f64, f64, u64, u64, ctypes.c_int, vp, u64, vp, vp]
+        L.lkref_region_plan_typed.argtypes = [vp, f64, f64, u64, u64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                              u64, vp, vp]
         L.lkref_dts_thresholds.argtypes = [f32, f32, u64, vp]
         L.lkref_dts_probs.argtypes = [u64, f32, vp]
         L.lkref_dts_profile.argtypes = [u64, f32, f32, vp]
@@ -527,7 +529,7 @@ def snr_threshold(profiles, nbins, widths, thresholds, stdnoise) -> np.ndarray:
 
 
 def region_plan(cfg: RefCfg, max_memory_gb=8.0, octave_scale=2.0, nbins_max=1024, max_passing=1 << 22,
-                use_gpu=False):
+                use_gpu=False, complex_fold=None, use_fourier=False):
     """FFARegionPlanner<float> of the reference: (chunks [n, 6] = f_min, f_max,
     nbins, eta, bseg_brute, bseg_ffa; stats [5] = max buffer size, max coord
     size, max ncoords, max levels, sweep memory usage in GB -- the device
@@ -537,8 +539,14 @@ def region_plan(cfg: RefCfg, max_memory_gb=8.0, octave_scale=2.0, nbins_max=1024
     rows = np.zeros(cap * 6, np.float64)
     stats = np.zeros(5, np.float64)
     n = u64()
-    _check(L, L.lkref_region_plan(ctypes.byref(cfg), max_memory_gb, octave_scale, nbins_max, max_passing,
-                                  int(use_gpu), _p(rows), cap, ctypes.byref(n), _p(stats)))
+    if complex_fold is None and not use_fourier:
+        _check(L, L.lkref_region_plan(ctypes.byref(cfg), max_memory_gb, octave_scale, nbins_max, max_passing,
+                                      int(use_gpu), _p(rows), cap, ctypes.byref(n), _p(stats)))
+    else:
+        cf = bool(use_fourier) if complex_fold is None else bool(complex_fold)
+        _check(L, L.lkref_region_plan_typed(ctypes.byref(cfg), max_memory_gb, octave_scale, nbins_max, max_passing,
+                                            int(use_gpu), int(cf), int(bool(use_fourier)), _p(rows), cap,
+                                            ctypes.byref(n), _p(stats)))
     k = min(n.value, cap)
     return rows[: k * 6].reshape(k, 6), stats
 

@@ -700,9 +700,12 @@ int lkref_prune_run(const lkref_cfg* c, int conservative, const float* ffa_fold,
 // drift-widened frequency limits), nbins, eta, bseg_brute, bseg_ffa. stats_out
 // (5 doubles): max buffer size, max coord size, max ncoords, max FFA levels,
 // get_freq_sweep_memory_usage() in GB (the device model when use_gpu).
-int lkref_region_plan(const lkref_cfg* c, double max_memory_gb, double octave_scale,
-                      uint64_t nbins_max, uint64_t max_passing, int use_gpu, double* chunks_out,
-                      uint64_t cap, uint64_t* n_out, double* stats_out) {
+}  // extern "C"
+
+template <class FoldType>
+static int region_plan(const lkref_cfg* c, double max_memory_gb, double octave_scale,
+                       uint64_t nbins_max, uint64_t max_passing, int use_gpu, bool use_fourier,
+                       double* chunks_out, uint64_t cap, uint64_t* n_out, double* stats_out) {
     return guarded([&] {
         std::vector<loki::ParamLimit> lims(c->nparams);
         for (uint32_t i = 0; i < c->nparams; ++i) {
@@ -718,9 +721,9 @@ int lkref_region_plan(const lkref_cfg* c, double max_memory_gb, double octave_sc
         }
         const loki::search::PulsarSearchConfig cfg(
             c->nsamps, c->tsamp, c->nbins, c->eta, lims, c->ducy_max, c->wtsp,
-            /*use_fourier=*/false, c->nthreads, max_memory_gb, octave_scale, nbins_max,
+            use_fourier, c->nthreads, max_memory_gb, octave_scale, nbins_max,
             /*nbins_min_lossy_bf=*/64, bb, bf, /*snr_min=*/5.0, max_passing);
-        const loki::regions::FFARegionPlanner<float> planner(cfg, use_gpu != 0);
+        const loki::regions::FFARegionPlanner<FoldType> planner(cfg, use_gpu != 0);
         const auto& cfgs = planner.get_cfgs();
         *n_out = cfgs.size();
         for (std::size_t i = 0; i < cfgs.size() && i < cap; ++i) {
@@ -740,6 +743,29 @@ int lkref_region_plan(const lkref_cfg* c, double max_memory_gb, double octave_sc
         stats_out[3] = static_cast<double>(st.get_max_ffa_levels());
         stats_out[4] = static_cast<double>(st.get_freq_sweep_memory_usage());
     });
+}
+
+extern "C" {
+
+int lkref_region_plan(const lkref_cfg* c, double max_memory_gb, double octave_scale,
+                      uint64_t nbins_max, uint64_t max_passing, int use_gpu, double* chunks_out,
+                      uint64_t cap, uint64_t* n_out, double* stats_out) {
+    return region_plan<float>(c, max_memory_gb, octave_scale, nbins_max, max_passing, use_gpu, false,
+                              chunks_out, cap, n_out, stats_out);
+}
+
+// The planner of a given fold type (0 float, 1 ComplexType) on a configuration
+// with the given use_fourier.
+int lkref_region_plan_typed(const lkref_cfg* c, double max_memory_gb, double octave_scale,
+                            uint64_t nbins_max, uint64_t max_passing, int use_gpu, int complex_fold,
+                            int use_fourier, double* chunks_out, uint64_t cap, uint64_t* n_out,
+                            double* stats_out) {
+    return complex_fold != 0
+               ? region_plan<loki::ComplexType>(c, max_memory_gb, octave_scale, nbins_max, max_passing,
+                                                use_gpu, use_fourier != 0, chunks_out, cap, n_out,
+                                                stats_out)
+               : region_plan<float>(c, max_memory_gb, octave_scale, nbins_max, max_passing, use_gpu,
+                                    use_fourier != 0, chunks_out, cap, n_out, stats_out);
 }
 
 // The same run with poly_basis "taylor" (basis 0) or "chebyshev" (basis 1).

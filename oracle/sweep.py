@@ -30,6 +30,15 @@ def lko_backend(nsamps, tsamp, nbins, eta, lims, ts_e, ts_v, widths=None):
     return scores.ravel(), np.asarray(plan.param_counts[-1], np.uint64), w
 
 
+def lko_fourier_backend(nsamps, tsamp, nbins, eta, lims, ts_e, ts_v, widths=None):
+    """The same from the oracle's FP64 Fourier-domain FFA (FFA<ComplexType>
+    back to time, boxcar S/N), scores in float64."""
+    plan = lko.plan_create(lko.make_cfg(nsamps, tsamp, nbins, eta, lims))
+    w = plan.widths if widths is None else np.asarray(widths, np.uint64)
+    scores = lko.ffa_fourier_scores64(plan, ts_e, ts_v, w)
+    return scores.ravel(), np.asarray(plan.param_counts[-1], np.uint64), w
+
+
 def param_val_at_idx(vmin: float, vmax: float, count: int, idx: np.ndarray) -> np.ndarray:
     """psr_utils::get_param_val_at_idx on an index array (IEEE double)."""
     if count <= 1:

@@ -188,9 +188,9 @@ def test_errors_are_loud(cuda):
     ffa = FFACUDA(cfg)
     with pytest.raises(RuntimeError, match="nsamps"):
         ffa.execute(np.zeros(100, np.float32), np.zeros(100, np.float32))
-    fourier = PulsarSearchConfig(2**18, 64e-6, 64, 1.0, np.array([[5.0, 50.0]]))
-    with pytest.raises(NotImplementedError):
-        compute_ffa_scores_cuda(np.zeros(2**18, np.float32), np.ones(2**18, np.float32), fourier)
+    fourier = PulsarSearchConfig(2**18, 64e-6, 64, 1.0, np.array([[5.0, 50.0]]))  # use_fourier default
+    with pytest.raises(RuntimeError, match="nsamps"):
+        compute_ffa_scores_cuda(np.zeros(100, np.float32), np.ones(100, np.float32), fourier)
     partial = PulsarSearchConfig(2**18, 64e-6, 64, 1.0, np.array([[5.0, 50.0]]), use_fourier=False,
                                  bseg_ffa=2**16)
     with pytest.raises(RuntimeError, match="nsegments must be 1"):

@@ -159,3 +159,53 @@ def test_sweep_octaves_to_nbins_max_vs_oracle(cuda):
         np.testing.assert_array_equal(params, o_params)
         np.testing.assert_array_equal(snr.view(np.uint32), o_snr.view(np.uint32))
         assert snr.size > 0
+
+
+def test_fourier_sweep_vs_oracle(cuda):
+    """The sweep with use_fourier = true (the reference default): chunks of the
+    Fourier-domain planner, each through the Fourier-domain FFA (direct
+    transform at 32 and 64 bins, the lossy level 0 at 128), against the FP64
+    oracle chunk by chunk: every candidate whose FP64 S/N clears snr_min by the
+    Fourier tolerance is found, nothing below it by that tolerance is, and
+    every S/N agrees within it."""
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.sweep import FFAFreqSweepCUDA, FFARegionPlannerFourier
+
+    nsamps, tsamp, snr_min = 1 << 17, 64e-6, 6.0
+    lims = [[4.0, 70.0]]
+    ts_e, ts_v = series(nsamps, 91)
+    tt = np.arange(nsamps) * tsamp
+    for f0 in (5.7, 21.3, 55.5):
+        ts_e += (0.3 * (np.mod(tt * f0, 1.0) < 0.03)).astype(np.float32)
+    cfg = PulsarSearchConfig(nsamps, tsamp, 32, 1.0, np.array(lims), max_passing_candidates=1 << 16,
+                             snr_min=snr_min)  # use_fourier defaults to true
+    sw = FFAFreqSweepCUDA(cfg, decode_chunk_widths=True)
+    plan = FFARegionPlannerFourier(cfg, use_gpu=True)
+    rows = np.array([[c["f_min"], c["f_max"], c["nbins"], c["eta"]] for c in sw.chunks])
+    np.testing.assert_array_equal(rows, np.array([[c["f_min"], c["f_max"], c["nbins"], c["eta"]]
+                                                  for c in plan.chunks]))
+    assert {32, 64, 128} <= {int(r[2]) for r in rows}
+    params, snr = sw.run(ts_e, ts_v)
+    counts = np.asarray(sw.region_counts, np.int64)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    lims0 = np.asarray(lims, np.float64)
+    for i, (f_min, f_max, nb, eta) in enumerate(rows):
+        lo = lims0.copy()
+        lo[-1] = (f_min, f_max)
+        s64, pc, w = osweep.lko_fourier_backend(nsamps, tsamp, int(nb), float(eta), lo, ts_e, ts_v)
+        tol = 1e-3 + 5e-5 * np.abs(s64)
+        sure = np.flatnonzero(s64 >= snr_min + tol)
+        maybe = np.flatnonzero(s64 >= snr_min - tol)
+        got = params[off[i]:off[i + 1]]
+        got_snr = snr[off[i]:off[i + 1]].astype(np.float64)
+        want_sure = osweep.decode(sure, pc, lo, w)
+        want_maybe = osweep.decode(maybe, pc, lo, w)
+        as_set = lambda a: {tuple(r) for r in a.tolist()}
+        assert as_set(want_sure) <= as_set(got) <= as_set(want_maybe)
+        # S/N of each candidate against the FP64 value of the same cell
+        lookup = {tuple(r): s64[k] for r, k in zip(want_maybe.tolist(), maybe)}
+        ref = np.array([lookup[tuple(r)] for r in got.tolist()])
+        assert np.all(np.abs(got_snr - ref) <= 1e-3 + 5e-5 * np.abs(ref))
+    assert snr.size > 0
+    for f0 in (5.7, 21.3, 55.5):
+        assert np.any(np.abs(params[:, 0] - f0) < 0.05 * f0)

@@ -142,3 +142,33 @@ def test_oracle_sweep_matches_reference_fixture(name):
         np.testing.assert_array_equal(params, g[f"params_{tag}"])
         np.testing.assert_array_equal(snr.view(np.uint32), g[f"snr_{tag}"].view(np.uint32))
     assert g["snr_base_widths"].size > 0
+
+
+def _planner_typed(nsamps, tsamp, nbins, eta, lims, mem, mp, gpu, fourier_plan, use_fourier):
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.sweep import FFARegionPlannerFourier, FFARegionPlannerTime
+
+    cfg = PulsarSearchConfig(int(nsamps), float(tsamp), int(nbins), float(eta), np.asarray(lims, np.float64),
+                             use_fourier=use_fourier, max_process_memory_gb=float(mem),
+                             max_passing_candidates=int(mp))
+    cls = FFARegionPlannerFourier if fourier_plan else FFARegionPlannerTime
+    return cls(cfg, use_gpu=bool(gpu))
+
+
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("fourier_plan,use_fourier", [(True, True), (False, True), (True, False)])
+@pytest.mark.parametrize("case", _random_cases(10, seed=9), ids=lambda c: f"np{len(c[4])}_n{c[0]}_m{c[5]}")
+def test_planner_fold_types_match_live_reference(case, fourier_plan, use_fourier):
+    """FFARegionPlanner<ComplexType> / <float> on use_fourier configurations
+    (fold buffers in harmonics or bins per row; 8-byte elements with
+    use_fourier) against the reference's planner of the same fold type."""
+    nsamps, tsamp, nbins, eta, lims, mem, mp, gpu = case
+    try:
+        rows, stats = R.region_plan(R.make_cfg(nsamps, tsamp, nbins, eta, lims), mem, 2.0, 1024, mp, gpu,
+                                    complex_fold=fourier_plan, use_fourier=use_fourier)
+    except RuntimeError:
+        with pytest.raises(Exception):
+            _planner_typed(nsamps, tsamp, nbins, eta, lims, mem, mp, gpu, fourier_plan, use_fourier)
+        return
+    _check_plan(_planner_typed(nsamps, tsamp, nbins, eta, lims, mem, mp, gpu, fourier_plan, use_fourier), rows,
+                stats)
