@@ -933,6 +933,8 @@ def run_fourier(args, rank, world, local_rank):
     sp = torch.cuda.current_stream().cuda_stream
     L = C.lib()
 
+    level0_tuned_ms = None if args.no_autotune else ffa.autotune(e, v, reps=3)
+
     def step():
         C.check(L.lk_fourier_search(ffa._h, e.data_ptr(), v.data_ptr(), B.SNR_MIN, idx.data_ptr(), snr.data_ptr(),
                                     cap, cnt.data_ptr(), sp))
@@ -1038,7 +1040,7 @@ def run_fourier(args, rank, world, local_rank):
     if rank == 0:
         B.emit(_line(args, world, name, value, ms,
                      dict(cfgd, final_coords=int(plan.ncoords[-1]), candidates=ncand, level0_freqs=nfreq0,
-                          level0_kernel=ffa.level0),
+                          level0_kernel=ffa.level0, level0_tuned_ms=level0_tuned_ms),
                      roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps * launches, clocks=clk,
                      parity=parity, stages={k: {"ms": p[0], "bytes": p[1]} for k, p in prof.items()}))
     _finish(dist)

@@ -233,6 +233,13 @@ int lk_fourier_set_level0(lk_fourier* f, int mode);
  * LK_FOURIER_L0_TENSOR_CORES, or LK_FOURIER_L0_AUTO (0) for the lossy level 0
  * (time-domain brute fold + real transform). */
 int lk_fourier_get_level0(const lk_fourier* f, int* mode);
+/* Times the tensor-core level 0's tilings (column subtiles per block, K
+ * part length) on these device series and keeps the fastest (synchronises the
+ * stream; results agree to FP32 accuracy whichever is kept); *level0_ms the
+ * kept time, 0 when level 0 is not on the tensor cores. No reference
+ * counterpart (launch shapes). */
+int lk_fourier_autotune(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, uint32_t reps,
+                        float* level0_ms, lk_stream_t stream);
 /* Synchronises the stream; the device status word (bounded-wait give-ups). */
 int lk_fourier_status(lk_fourier* f, lk_stream_t stream, uint32_t* status);
 /* nbins_f; final fold sizes (complex values, and floats back in time);

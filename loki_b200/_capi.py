@@ -164,6 +164,7 @@ SIGNATURES = [
     ("lk_fourier_set_profiling", i32, [vp, i32]),
     ("lk_fourier_set_level0", i32, [vp, i32]),
     ("lk_fourier_get_level0", i32, [vp, vp]),
+    ("lk_fourier_autotune", i32, [vp, vp, vp, u32, vp, vp]),
     ("lk_fourier_status", i32, [vp, vp, vp]),
     ("lk_fourier_get_profile", i32, [vp, vp, vp, u32, vp]),
     ("lk_fourier_brute_fold", i32, [vp, vp, u64, vp, u64, u64, u64, f64, f64, vp, u64, i32, vp]),

@@ -667,6 +667,19 @@ int lk_fourier_get_level0(const lk_fourier* f, int* mode) {
     });
 }
 
+int lk_fourier_autotune(lk_fourier* f, const float* d_ts_e, const float* d_ts_v, uint32_t reps,
+                        float* level0_ms, lk_stream_t stream) {
+    return guarded([&] {
+        need(f, "f");
+        need(d_ts_e, "d_ts_e");
+        need(d_ts_v, "d_ts_v");
+        const float ms = f->exec->tune_level0(d_ts_e, d_ts_v, reps, reinterpret_cast<cudaStream_t>(stream));
+        if (level0_ms != nullptr) {
+            *level0_ms = ms;
+        }
+    });
+}
+
 int lk_fourier_status(lk_fourier* f, lk_stream_t stream, uint32_t* status) {
     return guarded([&] {
         need(f, "f");

@@ -336,35 +336,61 @@ fourier_final_kernel(FinalArgs a) {
     }
     const double inv_nbins = 1.0 / static_cast<double>(a.nbins);
     const uint64_t rs2 = 2ull * a.nbf;
-    for (uint32_t i = threadIdx.x; i < ncells * a.nbf; i += blockDim.x) {
-        const uint32_t cl = i / a.nbf;
-        const uint32_t k = i - cl * a.nbf;
-        const uint64_t c = c0 + cl;
-        uint32_t it, ih;
-        float st = 0.0f, sh;
+    // the block's coordinates, staged once: the row loads below then depend
+    // on shared memory only
+    __shared__ uint32_t c_it[kFinCells], c_ih[kFinCells];
+    __shared__ float c_st[kFinCells], c_sh[kFinCells];
+    if (threadIdx.x < ncells) {
+        const uint64_t c = c0 + threadIdx.x;
         if constexpr (TAYLOR) {
             const CoordTaylor cc = reinterpret_cast<const CoordTaylor*>(a.coords)[c];
-            it = cc.i_tail;
-            ih = cc.i_head;
-            st = cc.shift_tail;
-            sh = cc.shift_head;
+            c_it[threadIdx.x] = cc.i_tail;
+            c_ih[threadIdx.x] = cc.i_head;
+            c_st[threadIdx.x] = cc.shift_tail;
+            c_sh[threadIdx.x] = cc.shift_head;
         } else {
             const CoordFreq cc = reinterpret_cast<const CoordFreq*>(a.coords)[c];
-            it = ih = cc.idx;
-            sh = cc.shift;
+            c_it[threadIdx.x] = c_ih[threadIdx.x] = cc.idx;
+            c_st[threadIdx.x] = 0.0f;
+            c_sh[threadIdx.x] = cc.shift;
         }
-        const float2* tail = a.in + static_cast<uint64_t>(it) * rs2 + k;
-        const float2* head = a.in + (a.nprev + ih) * rs2 + k;
-        const float2 ph = unit_phasor(static_cast<double>(k) * static_cast<double>(sh) * inv_nbins);
-        float2 te = __ldg(tail), tv = __ldg(tail + a.nbf);
-        if constexpr (TAYLOR) {
-            const float2 pt =
-                unit_phasor(static_cast<double>(k) * static_cast<double>(st) * inv_nbins);
-            te = cmul(te, pt);
-            tv = cmul(tv, pt);
+    }
+    __syncthreads();
+    // four items per thread in flight: all their row loads first
+    constexpr uint32_t kU = 4;
+    const uint32_t total = ncells * a.nbf;
+    for (uint32_t base = threadIdx.x; base < total; base += kU * blockDim.x) {
+        float2 te[kU], tv[kU], he[kU], hv[kU];
+        uint32_t kk[kU], cls[kU];
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) {
+            const uint32_t i = base + u * blockDim.x;
+            const uint32_t ii = i < total ? i : base;
+            cls[u] = ii / a.nbf;
+            kk[u] = ii - cls[u] * a.nbf;
+            const float2* tail = a.in + static_cast<uint64_t>(c_it[cls[u]]) * rs2 + kk[u];
+            const float2* head = a.in + (a.nprev + c_ih[cls[u]]) * rs2 + kk[u];
+            te[u] = __ldg(tail);
+            tv[u] = __ldg(tail + a.nbf);
+            he[u] = __ldg(head);
+            hv[u] = __ldg(head + a.nbf);
         }
-        const float2 he = cmul(__ldg(head), ph), hv = cmul(__ldg(head + a.nbf), ph);
-        coef[k * kFinPitch + cl] = make_float4(te.x + he.x, te.y + he.y, tv.x + hv.x, tv.y + hv.y);
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) {
+            if (base + u * blockDim.x >= total) {
+                break;
+            }
+            const double k = static_cast<double>(kk[u]);
+            const float2 ph = unit_phasor(k * static_cast<double>(c_sh[cls[u]]) * inv_nbins);
+            float2 e0 = te[u], v0 = tv[u];
+            if constexpr (TAYLOR) {
+                const float2 pt = unit_phasor(k * static_cast<double>(c_st[cls[u]]) * inv_nbins);
+                e0 = cmul(e0, pt);
+                v0 = cmul(v0, pt);
+            }
+            const float2 e1 = cmul(he[u], ph), v1 = cmul(hv[u], ph);
+            coef[kk[u] * kFinPitch + cls[u]] = make_float4(e0.x + e1.x, e0.y + e1.y, v0.x + v1.x, v0.y + v1.y);
+        }
     }
     __syncthreads();
     const uint32_t t = threadIdx.x;
@@ -780,6 +806,49 @@ void FourierExec::set_level0(int mode) {
                                          "that are multiples of 8");
     }
     level0 = mode;
+}
+
+float FourierExec::tune_level0(const float* ts_e, const float* ts_v, uint32_t reps, cudaStream_t s) {
+    require(reps >= 1 && reps <= 100, "reps must lie in [1, 100]");
+    DeviceGuard g(device);
+    if (!mma) {
+        return 0.0f;
+    }
+    const auto nbins = static_cast<uint32_t>(plan.cfg.nbins);
+    const uint32_t nfreq = static_cast<uint32_t>(plan.ncoords[0]);
+    cudaEvent_t e0, e1;
+    LK_CUDA(cudaEventCreate(&e0));
+    LK_CUDA(cudaEventCreate(&e1));
+    float best = 0.0f;
+    std::unique_ptr<FourierMma> keep;
+    for (uint32_t sub : {2u, 1u}) {
+        for (uint32_t pc : {64u, 128u, 256u}) {
+            auto cand = std::make_unique<FourierMma>(plan.segment_lens[0], plan.nsegments[0], nbins, nfreq,
+                                                     sub, pc);
+            auto run = [&] {
+                cand->run(ts_e, ts_v, freqs0.as<double>(), plan.cfg.tsamp, plan.t_ref0(),
+                          buf[0].as<float2>(), status.as<uint32_t>(), s);
+            };
+            run();  // warm-up
+            LK_CUDA(cudaEventRecord(e0, s));
+            for (uint32_t r = 0; r < reps; ++r) {
+                run();
+            }
+            LK_CUDA(cudaEventRecord(e1, s));
+            LK_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            LK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            ms /= static_cast<float>(reps);
+            if (!keep || ms < best) {
+                best = ms;
+                keep = std::move(cand);
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    mma = std::move(keep);
+    return best;
 }
 
 uint32_t FourierExec::read_status(cudaStream_t s) {

@@ -39,8 +39,7 @@ constexpr uint32_t kMaxN = 256;       // MMA N per instruction
 constexpr uint32_t kThreads = 192;    // 6 warps
 constexpr uint32_t kGenThreads = 128; // warps 2-5
 constexpr uint32_t kAnchor = 8;       // stages between exact phasor anchors (256 samples)
-constexpr uint32_t kPartChunks = 64;  // K chunks per part at most (2048 samples), before rounding
-constexpr uint32_t kMaxParts = 8;
+constexpr uint32_t kMaxParts = 8;     // K parts at most
 constexpr uint32_t kRowBytes = kKc * 2;               // 64
 constexpr uint32_t kATileBytes = kRows * kRowBytes;   // 8 KB per (hi | lo)
 
@@ -474,9 +473,13 @@ bool fourier_mma_supported(uint64_t seglen, uint64_t nseg, uint32_t nbins) {
            2 * nseg < (1ull << 31) && seglen < (1ull << 31);
 }
 
-FourierMma::FourierMma(uint64_t seglen_, uint64_t nseg_, uint32_t nbins_, uint32_t nfreq_)
+FourierMma::FourierMma(uint64_t seglen_, uint64_t nseg_, uint32_t nbins_, uint32_t nfreq_,
+                       uint32_t max_sub, uint32_t part_chunks)
     : seglen(seglen_), nseg(nseg_), nbins(nbins_), nfreq(nfreq_) {
     require(fourier_mma_supported(seglen, nseg, nbins), "tensor-core transform: unsupported shape");
+    require(max_sub == 1 || max_sub == 2, "tensor-core transform: subtiles per block must be 1 or 2");
+    require(part_chunks >= kAnchor && part_chunks % kAnchor == 0,
+            "tensor-core transform: K part length must be a multiple of 256 samples");
     const uint64_t rows = 2 * nseg;
     hi.alloc(sizeof(__half) * rows * seglen);
     lo.alloc(sizeof(__half) * rows * seglen);
@@ -486,7 +489,7 @@ FourierMma::FourierMma(uint64_t seglen_, uint64_t nseg_, uint32_t nbins_, uint32
         nsub = 1;
         ntile = static_cast<uint32_t>((rows + 15) / 16 * 16);
     } else {
-        nsub = 2;
+        nsub = max_sub;
         ntile = kMaxN;
     }
     ngroups = static_cast<uint32_t>((rows + nsub * ntile - 1) / (nsub * ntile));
@@ -498,7 +501,7 @@ FourierMma::FourierMma(uint64_t seglen_, uint64_t nseg_, uint32_t nbins_, uint32
     // K parts of at most kPartChunks chunks each (anchored starts): shorter
     // accumulation chains in tensor memory, and more blocks per wave
     const uint32_t nk = static_cast<uint32_t>((seglen + kKc - 1) / kKc);
-    const uint32_t want = std::min<uint32_t>(kMaxParts, (nk + kPartChunks - 1) / kPartChunks);
+    const uint32_t want = std::min<uint32_t>(kMaxParts, (nk + part_chunks - 1) / part_chunks);
     cpp = (nk + want - 1) / want;
     cpp = (cpp + kAnchor - 1) / kAnchor * kAnchor;
     nparts = (nk + cpp - 1) / cpp;
@@ -523,8 +526,6 @@ FourierMma::FourierMma(uint64_t seglen_, uint64_t nseg_, uint32_t nbins_, uint32
     encode(&map_lo, lo.ptr);
     smem_bytes = kStages * (2 * kATileBytes + 2 * nsub * ntile * kRowBytes) + 1024 + 128;
     require(smem_bytes <= 227 * 1024, "tensor-core transform: shared memory");
-    LK_CUDA(cudaFuncSetAttribute(fourier_dft_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem_bytes)));
 }
 
 uint64_t FourierMma::device_bytes() const {
@@ -566,6 +567,10 @@ void FourierMma::run(const float* d_ts_e, const float* d_ts_v, const double* d_f
     a.cpp = cpp;
     a.tmem_cols = tmem_cols;
     const uint32_t mtiles = (nfreq + a.fpt - 1) / a.fpt;
+    // the kernel's shared-memory limit is per function, and executors of
+    // other shapes set it too: set it for this launch
+    LK_CUDA(cudaFuncSetAttribute(fourier_dft_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem_bytes)));
     fourier_dft_mma_kernel<<<dim3(mtiles, ngroups, nparts), kThreads, smem_bytes, s>>>(map_hi, map_lo, a);
     LK_CUDA(cudaGetLastError());
     if (nparts > 1) {

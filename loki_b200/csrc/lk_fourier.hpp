@@ -55,7 +55,11 @@ struct FourierMma {
     DeviceBuffer hi, lo, dc, aux;  // FP16 staging [2 nseg][seglen], row sums, max / exponents
     DeviceBuffer parts;            // [nparts][level-0 fold] partial folds (nparts > 1)
     CUtensorMap map_hi{}, map_lo{};
-    FourierMma(uint64_t seglen, uint64_t nseg, uint32_t nbins, uint32_t nfreq);
+    // max_sub: MMA column subtiles of 256 per block (2: both rows E and V of
+    // 256 segments in one block, one block per SM; 1: two blocks per SM);
+    // part_chunks: K chunks of 32 samples per part at most (a multiple of 8)
+    FourierMma(uint64_t seglen, uint64_t nseg, uint32_t nbins, uint32_t nfreq, uint32_t max_sub = 2,
+               uint32_t part_chunks = 64);
     uint64_t device_bytes() const;
     void run(const float* d_ts_e, const float* d_ts_v, const double* d_freqs, double tsamp,
              double t_ref, float2* d_out, uint32_t* d_status, cudaStream_t s);
@@ -104,6 +108,10 @@ struct FourierExec {
                 uint64_t max_cands, uint64_t* d_count, cudaStream_t s);
     std::vector<lk_stage_time> profile(cudaStream_t s);
     void set_level0(int mode);
+    // Times the tensor-core level 0's tilings (subtiles per block, K part
+    // length) on these series and keeps the fastest; results agree to FP32
+    // accuracy whichever is kept. Returns the kept level-0 time (ms).
+    float tune_level0(const float* ts_e, const float* ts_v, uint32_t reps, cudaStream_t s);
     bool uses_mma() const { return mma != nullptr && level0 != LK_FOURIER_L0_CUDA_CORES; }
     uint32_t read_status(cudaStream_t s);
 

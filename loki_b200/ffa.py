@@ -422,6 +422,17 @@ class FFACOMPLEXCUDA:
         the shape allows), "cuda_cores" or "tensor_cores"."""
         C.check(C.lib().lk_fourier_set_level0(self._h, self._LEVEL0[mode]))
 
+    def autotune(self, ts_e, ts_v, reps: int = 3) -> float:
+        """Time the tensor-core level 0's tilings on this series and keep the
+        fastest; returns its time (ms), 0 when level 0 is not on the tensor
+        cores. Results agree to FP32 accuracy whichever is kept."""
+        e, v = self._inputs(ts_e, ts_v)
+        ms = ctypes.c_float()
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_fourier_autotune(self._h, D.ptr(e), D.ptr(v), int(reps), ctypes.byref(ms),
+                                                D.stream_ptr(self._device)))
+        return float(ms.value)
+
     @property
     def level0(self) -> str:
         """Level-0 kernel in use: "tensor_cores", "cuda_cores" or "lossy"."""

@@ -210,3 +210,20 @@ def test_level0_tensor_cores_vs_cuda_cores(cuda, name):
     t_ref = 0.0 if len(lims) == 1 else float(op.raw.tsegments[0]) / 2
     bf = compute_brute_fold_fourier_cuda(ts_e, ts_v, freqs, int(op.segment_lens[0]), nb, tsamp, t_ref)
     assert _rel(bf, want0) < FOLD_RTOL
+
+
+def test_autotune_keeps_results(cuda):
+    from loki_b200.ffa import FFACOMPLEXCUDA
+
+    nsamps, tsamp, nb, eta, lims = CASES["accel_nb64_2p18"]
+    cfg, op = _make(nsamps, tsamp, nb, eta, lims)
+    ts_e, ts_v = series(nsamps, 31)
+    ffa = FFACOMPLEXCUDA(cfg)
+    assert ffa.level0 == "tensor_cores"
+    before = ffa.scores(ts_e, ts_v)
+    ms = ffa.autotune(ts_e, ts_v, reps=2)
+    assert ms > 0
+    after = ffa.scores(ts_e, ts_v)
+    assert ffa.status() == 0
+    s64 = lko.ffa_fourier_scores64(op, ts_e, ts_v, op.widths).ravel()
+    assert _snr_ok(before, s64) and _snr_ok(after, s64)
