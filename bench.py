@@ -56,6 +56,9 @@ def parse():
                     help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--tuning", default=None,
                     help="apply these launch shapes (JSON of FFACUDA.tuning) instead of autotuning")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU path (oracle/_ref/libloki_ref_cuda.so)")
+    ap.add_argument("--reference-gpu-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--pipeline-execs", type=int, default=2,
                     help="executors (own compute streams) the end-to-end search pipeline alternates between")
     ap.add_argument("--workload", default="taylor_accel",
@@ -284,6 +287,102 @@ def candidate_parity(params, ts_e, ts_v, idx, snr):
             "ref_threads": nthreads, "ref_seconds": secs}
 
 
+# ---- the reference's own GPU path ---------------------------------------------
+
+def _reference_gpu_child(args):
+    """Child process: time the reference's GPU FFA + scorer (FFACUDA::execute on
+    device spans, snr_boxcar_3d_cuda_d; lib/*_cuda.cu with its Release flags) on
+    the workload's series, as this library's line times its own (CUDA events,
+    L2 flushed between steps); write the timing as JSON to OUT.json and the
+    last step's scores to OUT.npy."""
+    import torch
+
+    from oracle import ref
+
+    if args.workload != "taylor_accel":
+        raise SystemExit(f"the reference's GPU path is timed on taylor_accel only, not {args.workload}")
+    ts_e, ts_v, params, _ = workload()
+    torch.cuda.set_device(0)
+    cfg = ref.make_cfg(params["nsamps"], params["tsamp"], params["nbins"], params["eta"], params["param_limits"])
+    R = ref.RefGPU(cfg, device=0, use_fourier=False)
+    widths = np.asarray(params["score_widths"], np.uint32)
+    e = torch.from_numpy(ts_e).cuda()
+    v = torch.from_numpy(ts_v).cuda()
+    fold = torch.empty(R.fold_len, dtype=torch.float32, device="cuda")
+    w = torch.from_numpy(widths.view(np.int32)).cuda()
+    scores = torch.empty(R.ncoords_final * widths.size, dtype=torch.float32, device="cuda")
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        R.scores(e.data_ptr(), v.data_ptr(), params["nsamps"], fold.data_ptr(), w.data_ptr(), widths.size,
+                 scores.data_ptr(), sp)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record()
+        step()
+        stops[k].record()
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / args.steps
+    np.save(args.reference_gpu_child + ".npy", scores.cpu().numpy())
+    with open(args.reference_gpu_child + ".json", "w") as fh:
+        json.dump({"ms_per_step": ms, "ntrials": int(R.ncoords_final * widths.size)}, fh)
+    return 0
+
+
+# At this workload's sizes (segments of 16384 samples) the reference's GPU
+# Fourier brute fold launches kernel_fold_complex_unified<false> (lib/kernels_cuda.cu)
+# with 256 threads for 33 harmonics: threads 33..255 return before the block's
+# DC reduction, whose warp shuffles then name lanes that have exited and whose
+# second stage reads per-warp sums that were never written. Its scores come out
+# wrong by up to 4e6 in S/N; the code has undefined behaviour, so it is not run.
+REF_GPU_FOURIER_WHY = ("not run: the reference's GPU Fourier brute fold takes kernel_fold_complex_unified<false> "
+                       "here (2 x 16384 x 4 B > 48 KB shared), whose block reduction follows an early return of "
+                       "threads >= nbins_f (undefined behaviour, wrong DC terms)")
+
+
+def reference_gpu(args, ours_ms, ours_scores):
+    """The reference's GPU path timed in a child process (so that a failure
+    there cannot take this run with it), compared with this library's scores
+    of the same series."""
+    import subprocess
+    import tempfile
+
+    from oracle import ref
+
+    if args.workload == "fourier_accel":
+        return {"checked": False, "why": REF_GPU_FOURIER_WHY}
+    if not ref.gpu_available():
+        return {"checked": False, "why": "oracle/_ref/libloki_ref_cuda.so was not built"}
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "refgpu")
+        cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--workload", args.workload, "--steps",
+               str(args.steps), "--warmup", str(args.warmup), "--reference-gpu-child", out]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        except subprocess.TimeoutExpired:
+            return {"checked": False, "why": "the reference's GPU path did not finish within 900 s"}
+        if r.returncode != 0 or not os.path.exists(out + ".json"):
+            return {"checked": False, "why": f"the reference's GPU path failed (exit {r.returncode}): "
+                                             f"{(r.stderr or '').strip().splitlines()[-1:]}"}
+        with open(out + ".json") as fh:
+            t = json.load(fh)
+        rs = np.load(out + ".npy")
+    d = np.abs(rs.astype(np.float64) - np.asarray(ours_scores, np.float64))
+    return {"checked": True, "what": "FFACUDA::execute (device spans) + snr_boxcar_3d_cuda_d, the reference's "
+                                     "lib/*_cuda.cu built with its Release flags (-O3 -use_fast_math), same "
+                                     "series on the same GPU, L2 flushed between steps",
+            "ms_per_step": t["ms_per_step"], "value": t["ntrials"] / (t["ms_per_step"] / 1e3), "unit": UNIT,
+            "ours_ms_per_step": ours_ms, "speedup": t["ms_per_step"] / ours_ms,
+            "scores_max_abs_diff": float(d.max()), "scores_mean_abs_diff": float(d.mean())}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return 0
@@ -468,6 +567,9 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_parity:
         # the last timed step's candidates against the reference's, full size
         parity = candidate_parity(params, ts_e, ts_v, idx[:ncand].cpu().numpy(), snr[:ncand].cpu().numpy())
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu(args, step_ms_max, ffa.scores(e, v).cpu().numpy())
 
     if rank == 0:
         line = {
@@ -479,7 +581,7 @@ def run_ours(args, rank, world, local_rank):
                                            "rescore_margin": list(ffa.rescore_margin),
                                            "tuning": tuning}),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "stages": stages, "wall_s": wall, "parity": parity,
+            "clocks": clk, "stages": stages, "wall_s": wall, "parity": parity, "reference_gpu": ref_gpu,
         }
         emit(line)
         if parity is not None and parity.get("checked") and not parity["candidates_match"]:
@@ -517,6 +619,8 @@ def main():
     sys.modules.setdefault("bench", sys.modules[__name__])
     _reserve_stdout()
     args = parse()
+    if args.reference_gpu_child is not None:
+        return _reference_gpu_child(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -1037,12 +1037,16 @@ def run_fourier(args, rank, world, local_rank):
                 status = 0 if parity["candidates_match"] else 1
         else:
             parity = {"checked": False, "why": "oracle/_ref was not built"}
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = B.reference_gpu(args, ms, ffa.scores(e, v).cpu().numpy())
     if rank == 0:
         B.emit(_line(args, world, name, value, ms,
                      dict(cfgd, final_coords=int(plan.ncoords[-1]), candidates=ncand, level0_freqs=nfreq0,
                           level0_kernel=ffa.level0, level0_tuned_ms=level0_tuned_ms),
                      roofline=roof, cpu_baseline=cpu, e2e=e2e, gpu_launches=args.steps * launches, clocks=clk,
-                     parity=parity, stages={k: {"ms": p[0], "bytes": p[1]} for k, p in prof.items()}))
+                     parity=parity, reference_gpu=ref_gpu,
+                     stages={k: {"ms": p[0], "bytes": p[1]} for k, p in prof.items()}))
     _finish(dist)
     return status
 

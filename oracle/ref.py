@@ -62,6 +62,55 @@ def available(kind: str = "parity") -> bool:
     return os.path.exists(lib_path(kind))
 
 
+_GPU_LIB = os.path.join(REF_DIR, "libloki_ref_cuda.so")
+_gpu_lib = None
+
+
+def gpu_available() -> bool:
+    """The reference's GPU FFA library (make -C oracle refgpu) is built."""
+    return os.path.exists(_GPU_LIB)
+
+
+def gpu_lib() -> ctypes.CDLL:
+    global _gpu_lib
+    if _gpu_lib is None:
+        if not gpu_available():
+            raise RuntimeError(f"reference GPU library missing: {_GPU_LIB} (run `make -C oracle refgpu`)")
+        L = ctypes.CDLL(_GPU_LIB)
+        L.lkrefg_last_error.restype = ctypes.c_char_p
+        L.lkrefg_create.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+        L.lkrefg_destroy.argtypes = [vp]
+        L.lkrefg_info.argtypes = [vp, vp, vp, vp]
+        L.lkrefg_scores.argtypes = [vp, vp, vp, u64, vp, vp, u64, vp, vp]
+        _gpu_lib = L
+    return _gpu_lib
+
+
+class RefGPU:
+    """The reference's own GPU path: FFACUDA<float> (or <ComplexTypeCUDA>)
+    ::execute on device spans, then snr_boxcar_3d_cuda_d, enqueued on a
+    stream. Device pointers are plain integers (e.g. torch data_ptr())."""
+
+    def __init__(self, cfg: "RefCfg", device: int = 0, use_fourier: bool = False):
+        self._lib = gpu_lib()
+        self._h = vp()
+        if self._lib.lkrefg_create(ctypes.byref(cfg), device, int(bool(use_fourier)), ctypes.byref(self._h)) != 0:
+            raise RuntimeError(self._lib.lkrefg_last_error().decode())
+        fl, fst, nc = u64(), u64(), u64()
+        self._lib.lkrefg_info(self._h, ctypes.byref(fl), ctypes.byref(fst), ctypes.byref(nc))
+        self.fold_len, self.fold_size_time, self.ncoords_final = fl.value, fst.value, nc.value
+
+    def scores(self, d_e: int, d_v: int, nsamps: int, d_fold: int, d_widths: int, nw: int, d_scores: int,
+               stream: int) -> None:
+        if self._lib.lkrefg_scores(self._h, d_e, d_v, nsamps, d_fold, d_widths, nw, d_scores, stream) != 0:
+            raise RuntimeError(self._lib.lkrefg_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.lkrefg_destroy(self._h)
+            self._h = None
+
+
 _libs: dict[str, ctypes.CDLL] = {}
 
 
