@@ -1058,9 +1058,10 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
 // block time hardly depends on W) and the depth of the shared-memory ring.
 // Returns false (and changes nothing) when the shape does not fit.
 uint32_t BruteFoldDevice::max_tmem_warps(uint32_t smem_warps) const {
-    // packed form, nbins a multiple of 4, 2 * nbins columns per warp, four
-    // warps (one per TMEM lane quadrant) per column block, block <= 21 warps
-    if (m_nbins > 64 || m_nbins % 4 != 0 || smem_warps + 1 >= static_cast<uint32_t>(kMaxWarpsTm)) {
+    // packed form, nbins a multiple of 4 up to 256, 2 * nbins columns per
+    // warp, four warps (one per TMEM lane quadrant) per column block, block
+    // <= 24 consumer warps
+    if (m_nbins > 256 || m_nbins % 4 != 0 || smem_warps + 1 >= static_cast<uint32_t>(kMaxWarpsTm)) {
         return 0;
     }
     const uint32_t blocks = kTmemCols / static_cast<uint32_t>(2 * m_nbins);

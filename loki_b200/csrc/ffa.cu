@@ -386,6 +386,9 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         const uint32_t rows0 = bf->rows(), warps0 = bf->warps(), stages0 = bf->stages();
         float bf_best = INFINITY;
         uint32_t br = rows0, bw = warps0, bs = stages0;
+        // best packed (two-row) shared-memory shape, the base of step 1b
+        float pk_best = INFINITY;
+        uint32_t pw = 0, ps = stages0;
         for (uint32_t rows = 1; rows <= 2; ++rows) {
             if (rows == 2 && plan.cfg.nbins > 128) {
                 continue;
@@ -413,6 +416,11 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
                         bw = bf->warps();
                         bs = stages;
                     }
+                    if (rows == 2 && ms < pk_best) {
+                        pk_best = ms;
+                        pw = bf->warps();
+                        ps = stages;
+                    }
                 }
             }
         }
@@ -420,19 +428,24 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         // (the warps of a block share the sample ring, so a block's time
         // follows its slowest warp; a few shared-memory warp counts below the
         // best are tried with each TMEM warp count, for whole waves of blocks)
+        // The base is the best two-row shape even when one row per warp was
+        // faster: with nbins above 64 few two-row warps fit shared memory
+        // alone, and the TMEM warps are what make the packed form pay.
         uint32_t bt = 0;
-        if (br == 2) {
-            const uint32_t ws0 = bw;
+        if (pw > 0) {
+            const uint32_t ws0 = pw;
             for (uint32_t t = 4; t <= 16; t += 4) {
                 for (uint32_t ws = ws0 > 4 ? ws0 - 4 : 1; ws <= ws0; ++ws) {
-                    if (t > bf->max_tmem_warps(ws) || !bf->configure(2, ws + t, bs, t)) {
+                    if (t > bf->max_tmem_warps(ws) || !bf->configure(2, ws + t, ps, t)) {
                         continue;
                     }
                     const float ms = time_stages({LK_STAGE_INTERLEAVE, LK_STAGE_BRUTE_FOLD});
                     if (ms < bf_best) {
                         bf_best = ms;
                         bt = t;
+                        br = 2;
                         bw = ws;
+                        bs = ps;
                     }
                 }
             }
