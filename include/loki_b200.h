@@ -195,6 +195,16 @@ int lk_ffa_scores_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, u
 int lk_ffa_search_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint64_t nbatch,
                         float snr_min, uint32_t* d_idx, float* d_snr, uint64_t max_cands,
                         uint64_t* d_count, lk_stream_t stream);
+/* Valid samples of each series of a batch, as a DEVICE array of uint64 (one
+ * per series of the next batched calls; NULL turns it off). Every sample of
+ * series i at or past d_lengths[i] must be zero: the brute fold then skips
+ * the segments that hold none of the first d_lengths[i] samples (in groups
+ * of 8) and sets their folds to +0.0, the result folding the zeros gives, so
+ * outputs do not change. The array is read by every launch (a captured graph
+ * sees lengths written into it later) and must outlive the calls. The
+ * reference pads uneven series to a power of two (lib/configs.cpp:264); this
+ * lets the padding cost nothing. */
+int lk_ffa_set_batch_lengths(lk_ffa* ffa, const uint64_t* d_lengths);
 
 /* ---- Fourier-domain FFA (replaces FFACUDA<ComplexTypeCUDA>) ------------- */
 /* The FFA of the reference's use_fourier = true path (the default of

@@ -172,6 +172,7 @@ SIGNATURES = [
     ("lk_ffa_execute_batch", i32, [vp, vp, vp, u64, vp, u64, vp]),
     ("lk_ffa_scores_batch", i32, [vp, vp, vp, u64, vp, u64, vp]),
     ("lk_ffa_search_batch", i32, [vp, vp, vp, u64, f32, vp, vp, u64, vp, vp]),
+    ("lk_ffa_set_batch_lengths", i32, [vp, vp]),
     ("lk_ffa_status", i32, [vp, vp, vp]),
     ("lk_ffa_set_rescore_margin", i32, [vp, ctypes.c_float, ctypes.c_float]),
     ("lk_ffa_get_rescore_margin", i32, [vp, vp, vp]),

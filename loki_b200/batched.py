@@ -2,7 +2,8 @@
 
 Each series is padded to the next power of two with ``ts_e = ts_v = 0`` (the
 reference requires power-of-two ``nsamps``, lib/configs.cpp:264; padded
-samples add nothing to any fold), series of one padded length share one
+samples add nothing to any fold, and the brute fold skips the segments that
+hold only padding, in groups of 8), series of one padded length share one
 executor (one plan), and are folded, scored and compacted ``max_batch`` at a
 time: one launch per level for the whole batch (a batch of series is, level by
 level, one series with ``max_batch`` times the segments). Each full batch step
@@ -52,6 +53,11 @@ class _Group:
         self.idx = t.empty(cap, dtype=t.int32, device=dev)
         self.snr = t.empty(cap, dtype=t.float32, device=dev)
         self.cnt = t.zeros(1, dtype=t.int64, device=dev)
+        # valid samples of each series of the batch: the brute fold skips the
+        # segments that hold only padding (read by the captured graph too)
+        self.lens = t.zeros(nbatch, dtype=t.int64, device=dev)
+        self.hlens = t.zeros(nbatch, dtype=t.int64).pin_memory()
+        self.ffa.set_batch_lengths(self.lens)
         self.use_graph = use_graph
         self.graph = None
         self.stream = t.cuda.Stream(device=dev)
@@ -177,6 +183,12 @@ class MultiSeriesSearch:
                 self._collect(g, out)  # the slot's previous batch
                 chunk = ks[b0 : b0 + nbatch]
                 with t.cuda.stream(g.stream):
+                    # the slot's previous batch has finished (collected above),
+                    # so its copy of the lengths has been read
+                    g.hlens.zero_()
+                    for j, k in enumerate(chunk):
+                        g.hlens[j] = int(data[k][0].shape[-1])
+                    g.lens.copy_(g.hlens, non_blocking=True)
                     for j, k in enumerate(chunk):
                         e, v = data[k]
                         n = int(e.shape[-1])

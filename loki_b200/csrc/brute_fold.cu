@@ -95,7 +95,62 @@ struct FoldArgs {
     uint32_t stages;           // depth of the shared-memory ring (<= kMaxStages)
     float* fold;
     uint32_t* status;
+    // Segment-group mode (packed kernels, batches of zero-padded series):
+    // block b folds the 32 segments of groups 4 b .. 4 b + 3, each group 8
+    // consecutive segments starting at row groups[g]; blocks with 4 b >=
+    // *ngroups have no work. nullptr: block b folds segments 32 b .. 32 b + 31.
+    const uint32_t* groups;
+    const uint32_t* ngroups;
 };
+
+// Group mode: true when the block has at least one segment group.
+__device__ __forceinline__ bool block_has_groups(const FoldArgs& a) {
+    return blockIdx.x * 4u < *a.ngroups;
+}
+
+// Group mode: the first rows of the block's four groups (a missing group
+// re-reads the block's first group; its lanes do not store).
+__device__ __forceinline__ void block_group_rows(const FoldArgs& a, uint32_t (&grow)[4]) {
+    const uint32_t ng = *a.ngroups;
+    const uint32_t g0 = blockIdx.x * 4u;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        grow[q] = a.groups[g0 + q < ng ? g0 + q : g0];
+    }
+}
+
+// The segment whose fold lane `lane` holds, and whether it is stored.
+__device__ __forceinline__ uint32_t lane_segment(const FoldArgs& a, int seg0, int lane, bool* store) {
+    if (a.groups == nullptr) {
+        const auto seg = static_cast<uint32_t>(seg0 + lane);
+        *store = seg < a.nseg;
+        return seg;
+    }
+    const uint32_t g = blockIdx.x * 4u + static_cast<uint32_t>(lane / 8);
+    *store = g < *a.ngroups;
+    return a.groups[*store ? g : blockIdx.x * 4u] + static_cast<uint32_t>(lane % 8);
+}
+
+// One word's two 32-float boxes of (e, v) pairs into a stage: 32 rows from
+// seg0, or (group mode) four 8-row boxes, each into its 1024-byte quarter of
+// the tile, where the 128-byte swizzle of rows 8 q .. 8 q + 7 is the same.
+__device__ __forceinline__ void load_word(unsigned char* st, const CUtensorMap* tmap_ev,
+                                          const CUtensorMap* tmap_ev8, uint64_t* bar, int x0,
+                                          int seg0, bool grouped, const uint32_t (&grow)[4]) {
+    if (!grouped) {
+        ptx::tma_load_2d(st, tmap_ev, bar, x0, seg0);
+        ptx::tma_load_2d(st + kTileBytes, tmap_ev, bar, x0 + 32, seg0);
+        return;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ptx::tma_load_2d(st + h * kTileBytes + q * 1024, tmap_ev8, bar, x0 + 32 * h,
+                             static_cast<int>(grow[q]));
+        }
+    }
+}
 
 template <class BinT>
 __device__ __forceinline__ uint32_t load_bins(const BinT* b, uint64_t n, uint64_t first,
@@ -363,8 +418,13 @@ __device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
 // (e, v) pairs. Same pipeline, tables and order of adds as the mask kernel.
 template <class BinT>
 __global__ void __launch_bounds__(640, 1)
-    brute_fold_pk_kernel(const __grid_constant__ CUtensorMap tmap_ev, FoldArgs a) {
+    brute_fold_pk_kernel(const __grid_constant__ CUtensorMap tmap_ev,
+                         const __grid_constant__ CUtensorMap tmap_ev8, FoldArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const bool grouped = a.groups != nullptr;
+    if (grouped && !block_has_groups(a)) {
+        return;  // uniform: no group for this block
+    }
     const uint32_t S = a.stages;
     unsigned char* ring = smem_raw;
     uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * kStageBytes);
@@ -390,7 +450,7 @@ __global__ void __launch_bounds__(640, 1)
         return;
     }
     if (threadIdx.x == 0) {
-        ptx::prefetch_tensormap(&tmap_ev);
+        ptx::prefetch_tensormap(grouped ? &tmap_ev8 : &tmap_ev);
         for (uint32_t s = 0; s < S; ++s) {
             ptx::mbar_init(&full[s], 1);
             ptx::mbar_init(&empty[s], nconsumers * kWarp);
@@ -401,8 +461,13 @@ __global__ void __launch_bounds__(640, 1)
 
     if (warp == W) {
         // Producer: word k is samples 32k .. 32k+31, i.e. floats 64k ..
-        // 64k+63 of each segment's interleaved row, as two 32-float boxes.
+        // 64k+63 of each segment's interleaved row, as two 32-float boxes
+        // (eight 8-row boxes in group mode).
         if (lane == 0) {
+            uint32_t grow[4] = {0, 0, 0, 0};
+            if (grouped) {
+                block_group_rows(a, grow);
+            }
             uint32_t issued = 0;
             for (uint32_t k = 0; k < a.nwords; ++k) {
                 const uint32_t s = k % S;
@@ -413,9 +478,8 @@ __global__ void __launch_bounds__(640, 1)
                 }
                 unsigned char* st = ring + static_cast<size_t>(s) * kStageBytes;
                 ptx::mbar_arrive_expect_tx(&full[s], kStageBytes);
-                const int x0 = static_cast<int>(k * 64);
-                ptx::tma_load_2d(st, &tmap_ev, &full[s], x0, seg0);
-                ptx::tma_load_2d(st + kTileBytes, &tmap_ev, &full[s], x0 + 32, seg0);
+                load_word(st, &tmap_ev, &tmap_ev8, &full[s], static_cast<int>(k * 64), seg0, grouped,
+                          grow);
                 ++issued;
             }
             const uint32_t first = issued > S ? issued - S : 0;
@@ -550,8 +614,9 @@ __global__ void __launch_bounds__(640, 1)
         return;
     }
 
-    const uint32_t seg = static_cast<uint32_t>(seg0 + lane);
-    if (seg < a.nseg) {
+    bool store;
+    const uint32_t seg = lane_segment(a, seg0, lane, &store);
+    if (store) {
         float* out = a.fold + (static_cast<size_t>(seg) * a.nfreq + f) * 2 * a.nbins;
         if ((a.nbins & 3u) == 0) {
             for (uint32_t b = 0; b < a.nbins; b += 4) {
@@ -590,8 +655,13 @@ constexpr int kMaxWarpsTm = 25;  // consumers + producer (<= 72 registers)
 
 template <class BinT>
 __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
-    brute_fold_pk_tm_kernel(const __grid_constant__ CUtensorMap tmap_ev, FoldArgs a) {
+    brute_fold_pk_tm_kernel(const __grid_constant__ CUtensorMap tmap_ev,
+                            const __grid_constant__ CUtensorMap tmap_ev8, FoldArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const bool grouped = a.groups != nullptr;
+    if (grouped && !block_has_groups(a)) {
+        return;  // uniform, before any tensor memory is allocated
+    }
     const uint32_t S = a.stages;
     unsigned char* ring = smem_raw;
     uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * kStageBytes);
@@ -621,7 +691,7 @@ __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
         if (!aligned) {
             atomicOr(a.status, dev::kStatusBadTable);
         }
-        ptx::prefetch_tensormap(&tmap_ev);
+        ptx::prefetch_tensormap(grouped ? &tmap_ev8 : &tmap_ev);
         for (uint32_t s = 0; s < S; ++s) {
             ptx::mbar_init(&full[s], 1);
             ptx::mbar_init(&empty[s], nconsumers * kWarp);
@@ -635,6 +705,10 @@ __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
 
     if (aligned && warp == W) {
         if (lane == 0) {
+            uint32_t grow[4] = {0, 0, 0, 0};
+            if (grouped) {
+                block_group_rows(a, grow);
+            }
             uint32_t issued = 0;
             for (uint32_t k = 0; k < a.nwords; ++k) {
                 const uint32_t s = k % S;
@@ -645,9 +719,8 @@ __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
                 }
                 unsigned char* st = ring + static_cast<size_t>(s) * kStageBytes;
                 ptx::mbar_arrive_expect_tx(&full[s], kStageBytes);
-                const int x0 = static_cast<int>(k * 64);
-                ptx::tma_load_2d(st, &tmap_ev, &full[s], x0, seg0);
-                ptx::tma_load_2d(st + kTileBytes, &tmap_ev, &full[s], x0 + 32, seg0);
+                load_word(st, &tmap_ev, &tmap_ev8, &full[s], static_cast<int>(k * 64), seg0, grouped,
+                          grow);
                 ++issued;
             }
             const uint32_t first = issued > S ? issued - S : 0;
@@ -823,7 +896,8 @@ __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
             ok = a.seq[f] != 0 ? consume(std::true_type{}, std::false_type{})
                                : consume(std::false_type{}, std::false_type{});
         }
-        const uint32_t seg = static_cast<uint32_t>(seg0 + lane);
+        bool store;
+        const uint32_t seg = lane_segment(a, seg0, lane, &store);
         float* out = a.fold + (static_cast<size_t>(seg) * a.nfreq + f) * 2 * a.nbins;
         if (ok && tm) {
             // every lane reads (warp-collective); lanes past nseg do not store
@@ -834,12 +908,12 @@ __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
                 ptx::tmem_ld2(T + 2 * b + 4, e4.z, v4.z);
                 ptx::tmem_ld2(T + 2 * b + 6, e4.w, v4.w);
                 ptx::tmem_wait_ld4(e4, v4);
-                if (seg < a.nseg) {
+                if (store) {
                     reinterpret_cast<float4*>(out)[b / 4] = e4;
                     reinterpret_cast<float4*>(out + a.nbins)[b / 4] = v4;
                 }
             }
-        } else if (ok && seg < a.nseg) {
+        } else if (ok && store) {
             for (uint32_t b = 0; b < a.nbins; b += 4) {
                 const float2 p0 = A[b * kWarp], p1 = A[(b + 1) * kWarp];
                 const float2 p2 = A[(b + 2) * kWarp], p3 = A[(b + 3) * kWarp];
@@ -853,6 +927,61 @@ __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
     if (warp == W) {
         ptx::tmem_fence_after_sync();
         ptx::tmem_dealloc(tbase, kTmemCols);
+    }
+}
+
+// Valid segments of series i, in whole groups of 8: the segments that hold
+// any of its lens[i] samples, rounded up to 8 (at most nseg).
+__device__ __forceinline__ uint32_t valid_segments8(uint64_t len, uint32_t nseg, uint64_t seglen) {
+    const uint64_t used = (len + seglen - 1) / seglen;
+    const uint64_t r8 = (used + 7) / 8 * 8;
+    return static_cast<uint32_t>(r8 < nseg ? r8 : nseg);
+}
+
+// Group table of a batch (one block): tab[0] = number of groups, tab[1 ..
+// nbatch] = each series' first group, tab[1 + nbatch ..] = each group's first
+// row (series i's groups follow those of series < i).
+__global__ void seg_groups_kernel(const uint64_t* __restrict__ lens, uint32_t nbatch, uint32_t nseg,
+                                  uint64_t seglen, uint32_t* __restrict__ tab) {
+    uint32_t* first = tab + 1;
+    uint32_t* rows = tab + 1 + nbatch;
+    if (threadIdx.x == 0) {
+        uint32_t total = 0;
+        for (uint32_t i = 0; i < nbatch; ++i) {
+            first[i] = total;
+            total += valid_segments8(lens[i], nseg, seglen) / 8;
+        }
+        tab[0] = total;
+    }
+    __syncthreads();
+    for (uint32_t i = 0; i < nbatch; ++i) {
+        const uint32_t n = valid_segments8(lens[i], nseg, seglen) / 8;
+        for (uint32_t g = threadIdx.x; g < n; g += blockDim.x) {
+            rows[first[i] + g] = i * nseg + 8 * g;
+        }
+    }
+}
+
+// Zeroes the fold of every segment that group mode skipped (all samples
+// zero, so the fold is +0.0 in every bin, as folding them would give: a sum
+// that starts at +0.0 stays +0.0 when +0.0 is added). Block = one segment.
+__global__ void zero_skipped_kernel(const uint64_t* __restrict__ lens, uint32_t nseg, uint64_t seglen,
+                                    uint64_t seg_floats, float* __restrict__ fold) {
+    const uint32_t series = blockIdx.x / nseg;
+    const uint32_t seg = blockIdx.x - series * nseg;
+    if (seg < valid_segments8(lens[series], nseg, seglen)) {
+        return;
+    }
+    float* out = fold + static_cast<uint64_t>(blockIdx.x) * seg_floats;
+    if (seg_floats % 4 == 0) {
+        float4* o4 = reinterpret_cast<float4*>(out);
+        for (uint64_t i = threadIdx.x; i < seg_floats / 4; i += blockDim.x) {
+            o4[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    } else {
+        for (uint64_t i = threadIdx.x; i < seg_floats; i += blockDim.x) {
+            out[i] = 0.0f;
+        }
     }
 }
 
@@ -899,10 +1028,11 @@ void encode_series_map(CUtensorMap* map, const float* base, uint64_t seglen, uin
 // Interleaved series viewed as [nseg][2 * seglen] floats; box 32 floats
 // (16 samples' pairs) x 32 segments, 128-byte swizzle; reads past a row's end
 // or past nseg are zero.
-void encode_ev_map(CUtensorMap* map, const float2* base, uint64_t seglen, uint64_t nseg) {
+void encode_ev_map(CUtensorMap* map, const float2* base, uint64_t seglen, uint64_t nseg,
+                   uint32_t box_rows = 32) {
     cuuint64_t dims[2] = {2 * seglen, nseg};
     cuuint64_t strides[1] = {2 * seglen * sizeof(float)};
-    cuuint32_t box[2] = {32, 32};
+    cuuint32_t box[2] = {32, box_rows};
     cuuint32_t estr[2] = {1, 1};
     const CUresult r = tensor_map_encoder()(
         map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float2*>(base), dims, strides, box,
@@ -1140,7 +1270,7 @@ uint32_t BruteFoldDevice::max_warps(uint32_t rows, uint32_t stages) const {
 
 uint64_t BruteFoldDevice::device_bytes() const {
     return m_masks.bytes + m_bins.bytes + m_bin_off.bytes + m_nruns.bytes + m_stage.bytes +
-           m_ev.bytes + m_seq.bytes;
+           m_ev.bytes + m_seq.bytes + m_groups.bytes;
 }
 
 // The TMA maps read the series in place; a base address that is not 16-byte
@@ -1167,6 +1297,7 @@ void BruteFoldDevice::bind_inputs(const float* d_ts_e, const float* d_ts_v, cuda
         LK_CUDA(cudaGetLastError());
         if (m_ev.ptr != m_map_ev_ptr || nbatch != m_map_batch) {
             encode_ev_map(&m_tmap_ev, m_ev.as<float2>(), m_seglen, nbatch * m_nseg);
+            encode_ev_map(&m_tmap_ev8, m_ev.as<float2>(), m_seglen, nbatch * m_nseg, 8);
             m_map_ev_ptr = m_ev.ptr;
             m_map_batch = nbatch;
         }
@@ -1197,7 +1328,7 @@ void BruteFoldDevice::bind_inputs(const float* d_ts_e, const float* d_ts_v, cuda
     }
 }
 
-void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
+void BruteFoldDevice::fold(float* d_fold, cudaStream_t s, const uint64_t* d_lens) {
     require(m_map_e_ptr != nullptr, "BruteFold: inputs not bound");
     FoldArgs a{};
     a.masks = m_masks.as<uint32_t>();
@@ -1219,6 +1350,24 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
     const uint64_t nitems = (m_rows == 2 ? 1 : 2) * m_nfreq;
     dim3 grid(static_cast<unsigned>((nseg + kWarp - 1) / kWarp),
               static_cast<unsigned>((nitems + m_warps - 1) / m_warps));
+    // Group mode: only the segments that hold samples are folded (in groups
+    // of 8); the grid keeps its full size so that a captured graph stays
+    // valid for any lengths, and blocks past the groups return at once.
+    const bool grouped = d_lens != nullptr && m_rows == 2 && m_nseg % 8 == 0;
+    if (grouped) {
+        const uint64_t ngmax = nseg / 8;
+        const uint64_t words = 1 + m_map_batch + ngmax;
+        if (m_groups.bytes < words * sizeof(uint32_t)) {
+            m_groups.alloc(words * sizeof(uint32_t));
+        }
+        uint32_t* tab = m_groups.as<uint32_t>();
+        seg_groups_kernel<<<1, 256, 0, s>>>(d_lens, static_cast<uint32_t>(m_map_batch),
+                                            static_cast<uint32_t>(m_nseg), m_seglen, tab);
+        LK_CUDA(cudaGetLastError());
+        a.ngroups = tab;
+        a.groups = tab + 1 + m_map_batch;
+        grid.x = static_cast<unsigned>((ngmax + 3) / 4);
+    }
     auto launch = [&](auto kern) {
         LK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(m_smem)));
@@ -1227,13 +1376,14 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
     auto launch_pk = [&](auto kern) {
         LK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(m_smem)));
-        kern<<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, a);
+        kern<<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, m_tmap_ev8, a);
     };
     if (m_rows == 2 && m_tmem > 0) {
         LK_CUDA(cudaFuncSetAttribute(brute_fold_pk_tm_kernel<uint8_t>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(m_smem)));
-        brute_fold_pk_tm_kernel<uint8_t><<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, a);
+        brute_fold_pk_tm_kernel<uint8_t>
+            <<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, m_tmap_ev8, a);
     } else if (m_rows == 2) {
         m_wide_bins ? launch_pk(brute_fold_pk_kernel<uint16_t>)
                     : launch_pk(brute_fold_pk_kernel<uint8_t>);
@@ -1242,6 +1392,11 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s) {
                     : launch(brute_fold_mask_kernel<uint8_t, 1>);
     }
     LK_CUDA(cudaGetLastError());
+    if (grouped) {
+        zero_skipped_kernel<<<static_cast<unsigned>(nseg), 256, 0, s>>>(
+            d_lens, static_cast<uint32_t>(m_nseg), m_seglen, m_nfreq * 2 * m_nbins, d_fold);
+        LK_CUDA(cudaGetLastError());
+    }
 }
 
 }  // namespace lk

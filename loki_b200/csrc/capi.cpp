@@ -287,6 +287,13 @@ int lk_ffa_search_batch(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, u
     });
 }
 
+int lk_ffa_set_batch_lengths(lk_ffa* ffa, const uint64_t* d_lengths) {
+    return guarded([&] {
+        need(ffa, "ffa");
+        ffa->exec->batch_lens = d_lengths;
+    });
+}
+
 int lk_ffa_status(lk_ffa* ffa, lk_stream_t stream, uint32_t* status) {
     return guarded([&] {
         need(ffa, "ffa");

@@ -176,7 +176,7 @@ const void* FFAExec::run_levels(const float* ts_e, const float* ts_v, uint32_t l
         bf->bind_inputs(ts_e, ts_v, s, nbatch);
     }
     prof.begin(LK_STAGE_BRUTE_FOLD, 0, 1, series_bytes + 4 * plan.fold_size(0) * nbatch, s);
-    bf->fold(static_cast<float*>(in), s);
+    bf->fold(static_cast<float*>(in), s, batch_lens);
     prof.end(s);
     for (uint32_t l = 1; l <= last; ++l) {
         void* out = (l == last && final_out != nullptr) ? final_out : buf[l % 2].ptr;
@@ -364,6 +364,9 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
     }
     const bool was_enabled = prof.enabled;
     prof.enabled = true;
+    // the candidates are timed on the caller's single series, in full
+    const uint64_t* saved_lens = batch_lens;
+    batch_lens = nullptr;
     lk_tuning best{};
     uint32_t tried = 0;
     // Median of reps timed passes (after one untimed pass) of the stages.
@@ -514,10 +517,12 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
     } catch (...) {
         prof.enabled = was_enabled;
         prof.reset();
+        batch_lens = saved_lens;
         throw;
     }
     prof.enabled = was_enabled;
     prof.reset();
+    batch_lens = saved_lens;
     tuning = best;
     return best;
 }

@@ -81,6 +81,11 @@ struct FFAExec {
     RescoreTree rtree{};
 
     uint64_t max_batch = 1;  // series per call (buffers are sized for it)
+    // Device array of the valid samples of each series of a batch (or
+    // nullptr): the brute fold skips the segments past them (see
+    // BruteFoldDevice::fold). Read by every launch, so a captured graph picks
+    // up new lengths written into the same array.
+    const uint64_t* batch_lens = nullptr;
     // Tuned launch shapes (0: defaults); see autotune.
     int merge_pb = 0;            // merge: output rows per warp in flight
     uint32_t score_cells = 0;    // final level + score: cells per block

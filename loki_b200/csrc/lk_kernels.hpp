@@ -77,7 +77,12 @@ public:
     uint32_t warps() const { return m_warps; }
     uint32_t stages() const { return m_stages; }
     uint32_t tmem_warps() const { return m_tmem; }
-    void fold(float* d_fold, cudaStream_t s);
+    // d_lens (device, one uint64 per bound series, or nullptr): samples of
+    // each series that may be nonzero (the rest must be zero). With both rows
+    // per warp and nseg a multiple of 8, only the segments holding them are
+    // folded (in groups of 8) and the others' folds are set to +0.0, the
+    // result folding the zeros gives; otherwise every segment is folded.
+    void fold(float* d_fold, cudaStream_t s, const uint64_t* d_lens = nullptr);
     uint64_t nseg() const { return m_nseg; }
     uint64_t nfreq() const { return m_nfreq; }
     uint64_t fold_size() const { return m_nseg * m_nfreq * 2 * m_nbins; }
@@ -103,6 +108,8 @@ private:
     DeviceBuffer m_ev;         // (e, v) interleaved series (both rows per warp)
     CUtensorMap m_tmap_e{}, m_tmap_v{};
     CUtensorMap m_tmap_ev{};
+    CUtensorMap m_tmap_ev8{};  // same rows, 8-row boxes (group mode)
+    DeviceBuffer m_groups;     // uint32 group table of the bound batch (group mode)
     const void* m_map_ev_ptr = nullptr;
     const float* m_map_e_ptr = nullptr;
     const float* m_map_v_ptr = nullptr;

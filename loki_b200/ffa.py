@@ -154,6 +154,17 @@ class FFACUDA:
             raise RuntimeError(f"nbatch must lie in [1, max_batch={self._max_batch}]")
         return e, v, nb
 
+    def execute_batch(self, ts_e, ts_v, out=None):
+        """Final-level fold of each series of the batch: a [nbatch, fold_size]
+        CUDA tensor (one launch per level for the whole batch)."""
+        e, v, nb = self._batch_inputs(ts_e, ts_v)
+        per = int(self._plan.fold_size)
+        res = out if out is not None else D.empty_f32(nb * per, self._device)
+        with D.torch().cuda.device(self._device):
+            C.check(C.lib().lk_ffa_execute_batch(self._h, D.ptr(e), D.ptr(v), nb, D.ptr(res), res.numel(),
+                                                 D.stream_ptr(self._device)))
+        return res.reshape(nb, per) if out is None else res
+
     def scores_batch(self, ts_e, ts_v, out=None):
         """Boxcar S/N of each series of the batch: a [nbatch, ncoords_final *
         n_widths] CUDA tensor (one launch per level for the whole batch)."""
@@ -188,6 +199,22 @@ class FFACUDA:
         total = int(count.item())
         k = min(total, idx.numel())
         return idx[:k].cpu().numpy().view(np.uint32), snr[:k].cpu().numpy(), total
+
+    def set_batch_lengths(self, lengths) -> None:
+        """Valid samples of each series of the next batched calls: a CUDA
+        int64 tensor (one entry per series, read by every launch, so a
+        captured graph sees values written into it later) or None (off).
+        Samples at or past a series' length must be zero; the brute fold
+        then skips the segments holding none of its samples and sets their
+        folds to +0.0 (the folds of zeros), so outputs do not change."""
+        if lengths is None:
+            self._batch_lengths = None
+            C.check(C.lib().lk_ffa_set_batch_lengths(self._h, None))
+            return
+        if not D.is_device_tensor(lengths) or lengths.dtype != D.torch().int64 or not lengths.is_contiguous():
+            raise ValueError("lengths must be a contiguous int64 CUDA tensor")
+        self._batch_lengths = lengths  # kept alive while the executor reads it
+        C.check(C.lib().lk_ffa_set_batch_lengths(self._h, D.ptr(lengths)))
 
     def set_profiling(self, enable: bool = True) -> None:
         """Record CUDA events around every kernel stage of subsequent calls."""

@@ -187,3 +187,82 @@ def test_multi_series_slots_identical(cuda):
             np.testing.assert_array_equal(r["idx"], a["idx"])
             np.testing.assert_array_equal(r["snr"].view(np.uint32), a["snr"].view(np.uint32))
     assert sum(r["total"] for r in one) > 0
+
+
+# Valid-length batches: segments holding only padding are skipped by the
+# brute fold (groups of 8 segments) and their folds set to +0.0, so folds and
+# scores are bit-identical to folding the zeros. Lengths cover a full series,
+# a partial last segment, fewer valid segments than one group, one sample and
+# none. Shapes: two rows per warp in shared memory, with TMEM warps, and one
+# row per warp (which folds everything).
+LEN_CASES = {
+    "accel_nb32_pk": (1 << 17, 1e-3, 32, ((-300.0, 300.0), (5.0, 8.0)), None),
+    "accel_nb32_tmem": (1 << 17, 1e-3, 32, ((-300.0, 300.0), (5.0, 8.0)), (2, 6, 8)),
+    "freq_nb128_tmem": (1 << 18, 64e-6, 128, ((20.0, 40.0),), (2, 4, 8)),
+    "freq_nb128_rows1": (1 << 18, 64e-6, 128, ((20.0, 40.0),), (1, 8, 0)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(LEN_CASES))
+def test_batch_lengths_skip_padding(cuda, name):
+    from loki_b200.ffa import FFACUDA
+
+    t = cuda
+    n, tsamp, nbins, lims, shape = LEN_CASES[name]
+    cfg = _cfg(n, nbins, lims, tsamp=tsamp)
+    lengths = [n, int(0.6 * n) + 37, int(0.13 * n), 1, 0]
+    nb = len(lengths)
+    plain = FFACUDA(cfg, max_batch=nb)
+    skip = FFACUDA(cfg, max_batch=nb)
+    if shape is not None:
+        rows, ws, tw = shape
+        tu = skip.tuning
+        tu.update(bf_rows=rows, bf_warps=ws + tw, bf_tmem_warps=tw)
+        skip.set_tuning(tu)
+        plain.set_tuning(tu)
+    es = np.zeros((nb, n), np.float32)
+    vs = np.zeros((nb, n), np.float32)
+    for k, L in enumerate(lengths):
+        e, v = series(n, 60 + k)
+        es[k, :L], vs[k, :L] = e[:L], v[:L]
+    e = t.from_numpy(es).cuda()
+    v = t.from_numpy(vs).cuda()
+    lens = t.tensor(lengths, dtype=t.int64, device="cuda")
+    skip.set_batch_lengths(lens)
+    want_f = plain.execute_batch(e, v).cpu().numpy()
+    want = plain.scores_batch(e, v).cpu().numpy()
+    got = skip.scores_batch(e, v).cpu().numpy()
+    nan = np.isnan(want)
+    np.testing.assert_array_equal(np.isnan(got), nan)
+    np.testing.assert_array_equal(got[~nan].view(np.uint32), want[~nan].view(np.uint32))
+    got_f = skip.execute_batch(e, v).cpu().numpy()
+    np.testing.assert_array_equal(got_f.view(np.uint32), want_f.view(np.uint32))
+    # a captured step sees lengths (and data) written after the capture
+    idx = t.empty(1 << 16, dtype=t.int32, device="cuda")
+    snr = t.empty(1 << 16, dtype=t.float32, device="cuda")
+    cnt = t.zeros(1, dtype=t.int64, device="cuda")
+    thr = float(np.nanquantile(want, 0.999))
+    skip.search_batch(e, v, thr, idx, snr, cnt)
+    t.cuda.synchronize()
+    g = t.cuda.CUDAGraph()
+    with t.cuda.graph(g):
+        skip.search_batch(e, v, thr, idx, snr, cnt)
+    lengths2 = [0, n, 3, int(0.3 * n), n // 2]
+    es2 = np.zeros((nb, n), np.float32)
+    vs2 = np.zeros((nb, n), np.float32)
+    for k, L in enumerate(lengths2):
+        e2, v2 = series(n, 80 + k)
+        es2[k, :L], vs2[k, :L] = e2[:L], v2[:L]
+    e.copy_(t.from_numpy(es2))
+    v.copy_(t.from_numpy(vs2))
+    lens.copy_(t.tensor(lengths2, dtype=t.int64))
+    g.replay()
+    t.cuda.synchronize()
+    k_n = int(cnt.item())
+    flat = plain.scores_batch(e, v).cpu().numpy().ravel()
+    want_idx = np.flatnonzero(flat >= thr)
+    assert k_n == want_idx.size
+    np.testing.assert_array_equal(idx[:k_n].cpu().numpy().view(np.uint32), want_idx.astype(np.uint32))
+    np.testing.assert_array_equal(snr[:k_n].cpu().numpy().view(np.uint32), flat[want_idx].view(np.uint32))
+    del g
+    assert skip.status() == 0
