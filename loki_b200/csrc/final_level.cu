@@ -19,10 +19,12 @@
 //    into registers 16 positions (plus the widest width) at a time and every
 //    width w up to the bucket WM (8, 16 or 32) is a compile-time register
 //    offset, taken when bit w of the width mask is set; window differences
-//    are the same IEEE subtracts, reduced by a pairwise fmaxf tree. fmaxf
-//    returns the same value as the reference's `(m < d) ? d : m` scan (NaN
-//    differences are skipped by both) except possibly for the sign of a zero
-//    maximum, so a zero maximum is recomputed with the reference's rule;
+//    are the same IEEE subtracts, reduced by a tree of three-input maxima
+//    (max.f32 a, b, c), which return the same value as the reference's
+//    `(m < d) ? d : m` scan (NaN differences are skipped by both) except
+//    possibly for the sign of a zero maximum, so a zero maximum is
+//    recomputed with the reference's rule; rows are read and the prefix
+//    sums written two bins per 64-bit shared-memory access;
 //  * with a count target, each block counts its scores >= thr; a block's
 //    cells are contiguous in flat score order, so the candidate list is an
 //    exclusive scan of the block counts plus an ordered scatter of the blocks
@@ -50,6 +52,14 @@ __global__ void norm_table_kernel(float* __restrict__ tab, uint32_t n) {
     }
 }
 
+// max of three (sm_100 three-input max.f32: the largest non-NaN input, as
+// two nested fmaxf).
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Exact reference maximum (first maximum kept) of p[i + w] - p[i].
 __device__ __noinline__ float dmax_exact(const float* r, uint32_t w, uint32_t nbins) {
     float m = -FLT_MAX;
@@ -70,7 +80,10 @@ __global__ void __launch_bounds__(128, 5)
                           int mode, float* __restrict__ scores, float* __restrict__ cmax,
                           const float* __restrict__ tab, float thr, uint32_t* __restrict__ counts) {
     constexpr int NJ = NB / kWarp;      // bins per lane in phase 1
-    constexpr int RS = NB + WM + 1;  // odd row stride, room for every window read
+    // Row stride, room for every window read: NB + WM + 2 floats, so that
+    // rows start on 8 bytes and half the stride is odd -- the 64-bit loads
+    // of 16 threads (one row each) then fall on distinct bank pairs.
+    constexpr int RS = NB + WM + 2;
     constexpr int CH = 16;
     static_assert(NB % CH == 0 && WM <= kMaxW, "chunking");
     extern __shared__ float rows[];
@@ -180,11 +193,15 @@ __global__ void __launch_bounds__(128, 5)
     uint32_t passed = 0;
     if (threadIdx.x < nhere) {
         float* r = rows + static_cast<size_t>(threadIdx.x) * RS;
-        float acc = r[0];
+        float2* r2 = reinterpret_cast<float2*>(r);
+        // sequential inclusive prefix sum, two bins per 64-bit access
+        float acc = 0.0f;
 #pragma unroll
-        for (int j = 1; j < NB; ++j) {
-            acc = __fadd_rn(acc, r[j]);
-            r[j] = acc;
+        for (int j = 0; j < NB / 2; ++j) {
+            const float2 x = r2[j];
+            const float a0 = j == 0 ? x.x : __fadd_rn(acc, x.x);
+            acc = __fadd_rn(a0, x.y);
+            r2[j] = make_float2(a0, acc);
         }
         const float sum = acc;
         for (uint32_t k = 0; k < mp.wmax; ++k) {
@@ -201,27 +218,30 @@ __global__ void __launch_bounds__(128, 5)
             // NB + wmax - 1 are only used by widths above wmax (not taken)
             float win[CH + WM];
 #pragma unroll
-            for (int k = 0; k < CH + WM; ++k) {
-                win[k] = r[c + k];
+            for (int k = 0; k < (CH + WM) / 2; ++k) {
+                const float2 x = r2[c / 2 + k];
+                win[2 * k] = x.x;
+                win[2 * k + 1] = x.y;
             }
 #pragma unroll
             for (int w = 1; w <= WM; ++w) {
                 if ((mp.wmask >> w) & 1ull) {
-                    // pairwise tree of the chunk's differences (short
-                    // dependency chains), then the running maximum
+                    // the chunk's 16 differences and the running maximum
+                    // in a tree of three-input maxima (depth 3)
                     float d[CH];
 #pragma unroll
                     for (int k = 0; k < CH; ++k) {
                         d[k] = __fsub_rn(win[k + w], win[k]);
                     }
-#pragma unroll
-                    for (int h = CH / 2; h >= 1; h /= 2) {
-#pragma unroll
-                        for (int k = 0; k < h; ++k) {
-                            d[k] = fmaxf(d[k], d[k + h]);
-                        }
-                    }
-                    dm[w] = fmaxf(dm[w], d[0]);
+                    static_assert(CH == 16, "tree below is for 16 differences");
+                    const float m0 = fmax3(d[0], d[1], d[2]);
+                    const float m1 = fmax3(d[3], d[4], d[5]);
+                    const float m2 = fmax3(d[6], d[7], d[8]);
+                    const float m3 = fmax3(d[9], d[10], d[11]);
+                    const float m4 = fmax3(d[12], d[13], d[14]);
+                    const float n0 = fmax3(m0, m1, m2);
+                    const float n1 = fmax3(m3, m4, d[15]);
+                    dm[w] = fmax3(dm[w], n0, n1);
                 }
             }
         }
@@ -364,7 +384,7 @@ void merge_score_level_wm(const void* d_in, const void* d_coords, bool taylor, u
         constexpr bool TB = decltype(tabc)::value;
         constexpr int PB = NB == 128 ? 4 : 8;
         auto kern = merge_score_wm_kernel<TG, NB, PB, TI, WM, TB>;
-        const size_t smem = static_cast<size_t>(T) * (NB + WM + 1) * sizeof(float);
+        const size_t smem = static_cast<size_t>(T) * (NB + WM + 2) * sizeof(float);
         sc::set_smem(kern, smem);
         kern<<<dim3(blocks, static_cast<unsigned>(nbatch)), T, smem, s>>>(
             static_cast<const TI*>(d_in), d_coords, static_cast<uint32_t>(n_inner),
