@@ -453,6 +453,10 @@ def run_prune(args, rank, world, local_rank):
     widths = cfg.score_widths
     e = torch.from_numpy(ts_e).cuda()
     v = torch.from_numpy(ts_v).cuda()
+    tuning = None
+    if not args.no_autotune:
+        ffa.autotune(e, v, reps=3)  # brute fold and merges of the 32-segment FFA
+        tuning = ffa.tuning
     fold = torch.empty(ffa.plan.fold_size, dtype=torch.float32, device="cuda")
     flush = torch.empty(B.FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -507,7 +511,7 @@ def run_prune(args, rank, world, local_rank):
         B.emit(_line(
             args, world, "prune_jerk_2^23x64us_nbins32", value, ms,
             dict(_prune_cfgd(p, nseg, ref_seg, widths), poly_basis=args.basis, leaves_scored=leaves,
-                 survivors=int(stats["n_leaves_surv"][-1]), levels_run=int(len(stats) - 1)),
+                 survivors=int(stats["n_leaves_surv"][-1]), levels_run=int(len(stats) - 1), ffa_tuning=tuning),
             roofline=_roofline("prune_run", algo, prune_ms), cpu_baseline=cpu, e2e=e2e,
             clocks=clk, stages={"ffa_ms": ms - prune_ms, "prune_ms": prune_ms},
             level_stats=[{k: (float(r[k]) if k in ("threshold", "score_min", "score_max") else int(r[k]))

@@ -384,7 +384,9 @@ typedef struct lk_tuning {
 /* Times the candidates on the given device series (one search's inputs;
  * reps timed passes each, median) and keeps the fastest shape of each stage.
  * Results of every later call are unchanged (same sums, same order).
- * Synchronises the stream; needs a plan with one final segment. */
+ * Synchronises the stream. A plan that stops at several segments (the
+ * pruning input, bseg_ffa) has no fused final level: its brute fold and
+ * merges are tuned and score_ms is 0. */
 int lk_ffa_autotune(lk_ffa* ffa, const float* d_ts_e, const float* d_ts_v, uint32_t reps,
                     lk_tuning* out, lk_stream_t stream);
 int lk_ffa_get_tuning(const lk_ffa* ffa, lk_tuning* out);

@@ -353,12 +353,14 @@ void FFAExec::apply_tuning(const lk_tuning& t) {
 
 lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
                             cudaStream_t s) {
-    require(plan.nsegments[plan.n_levels - 1] == 1,
-            "autotune needs a plan whose final level has one segment (a scoring plan)");
+    // A scoring plan (one final segment) is timed through the fused final
+    // level; a plan that stops at several segments (the pruning input) through
+    // its levels alone, and has no final-level step.
+    const bool scoring = plan.nsegments[plan.n_levels - 1] == 1;
     DeviceGuard g(device);
     reps = std::max<uint32_t>(1, std::min<uint32_t>(reps, 20));
     const uint64_t n = plan.ncoords[plan.n_levels - 1] * plan.widths.size();
-    if (scores_tmp.bytes < n * sizeof(float)) {
+    if (scoring && scores_tmp.bytes < n * sizeof(float)) {
         scores_tmp.alloc(n * sizeof(float));
         compact_scratch.alloc(compact_scratch_bytes(n));
     }
@@ -374,7 +376,12 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         std::vector<float> t;
         for (uint32_t r = 0; r <= reps; ++r) {
             prof.reset();
-            scores_impl(ts_e, ts_v, scores_tmp.as<float>(), nullptr, s, 1);
+            if (scoring) {
+                scores_impl(ts_e, ts_v, scores_tmp.as<float>(), nullptr, s, 1);
+            } else {
+                bool last_bf16 = false;
+                run_levels(ts_e, ts_v, plan.n_levels - 1, nullptr, s, 1, &last_bf16);
+            }
             LK_CUDA(cudaStreamSynchronize(s));
             if (r > 0) {
                 t.push_back(stage_ms(prof, kinds));
@@ -466,7 +473,8 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         }
         float merge_best = INFINITY;
         int bpb = 0;
-        if (plan.n_levels > 2) {
+        // levels 1 .. L-2 are plain merges when scoring, 1 .. L-1 otherwise
+        if (plan.n_levels > (scoring ? 2u : 1u)) {
             for (int pb : pbs) {
                 merge_pb = pb;
                 const float ms = time_stages({LK_STAGE_MERGE});
@@ -482,9 +490,9 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         // 3. fused final level: cells per block
         const uint32_t rs = sc::row_stride(nb, sp.wmax);
         const uint32_t tmax = sc::profiles_per_block(rs);
-        float score_best = INFINITY;
+        float score_best = scoring ? INFINITY : 0.0f;
         uint32_t bcells = 0;
-        if (wm) {
+        if (scoring && wm) {
             // masked final level (final_level.cu), with and without the table
             for (uint32_t v : {0u, 1u}) {
                 score_cells = v;
@@ -495,7 +503,7 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
                 }
             }
         }
-        for (uint32_t cells = 32; cells <= tmax; cells += 32) {
+        for (uint32_t cells = 32; scoring && cells <= tmax; cells += 32) {
             score_cells = cells;
             const float ms = time_stages({LK_STAGE_MERGE_SCORE});
             if (ms < score_best) {

@@ -241,9 +241,9 @@ class FFACUDA:
 
     def autotune(self, ts_e, ts_v, reps: int = 3) -> dict:
         """Time launch-shape candidates of the brute fold, the merges and the
-        fused final level on this series (CUDA tensors or host arrays) and keep
-        the fastest of each; results are unchanged. Returns the tuning with
-        the best stage times (ms)."""
+        fused final level (plans with one final segment) on this series (CUDA
+        tensors or host arrays) and keep the fastest of each; results are
+        unchanged. Returns the tuning with the best stage times (ms)."""
         e, v = self._inputs(ts_e, ts_v)
         t = C.LkTuning()
         with D.torch().cuda.device(self._device):

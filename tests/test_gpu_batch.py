@@ -163,6 +163,26 @@ def test_autotune_keeps_results(cuda, nbins, lims, storage):
         assert other.tuning[k] == t[k]
 
 
+def test_autotune_multi_segment_plan(cuda):
+    """A plan that stops at several segments (the pruning input) is tuned
+    through its brute fold and merges; the fold stays bit-exact."""
+    from loki_b200.configs import PulsarSearchConfig
+    from loki_b200.ffa import FFACUDA
+
+    ns, bseg = 2**18, 2**13
+    lims = [[-20.0, 20.0], [5.0, 6.0]]
+    cfg = PulsarSearchConfig(ns, 1e-3, 32, 1.0, np.array(lims), use_fourier=False, bseg_ffa=bseg)
+    op = lko.plan_create(lko.make_cfg(ns, 1e-3, 32, 1.0, lims, bseg_ffa=bseg))
+    assert op.nsegments[-1] > 1
+    e, v = series(ns, 93)
+    ffa = FFACUDA(cfg)
+    t = ffa.autotune(e, v, reps=1)
+    assert t["candidates"] > 3 and t["score_ms"] == 0.0 and t["bf_ms"] > 0.0
+    got = ffa.execute(e, v)
+    np.testing.assert_array_equal(got.view(np.uint32), lko.ffa(op, e, v).view(np.uint32))
+    assert ffa.status() == 0
+
+
 def test_multi_series_slots_identical(cuda):
     """Batches alternating over two executor slots (own streams, own graphs)
     give exactly the one-slot results; device inputs, several batches per
