@@ -527,6 +527,12 @@ int lk_prune_run(lk_prune* pr, const float* d_ffa_fold, uint64_t ref_seg,
                  const float* thresholds, uint64_t n_thresholds, uint64_t n_iters,
                  lk_prune_stats* stats, uint64_t max_stats, uint64_t* n_stats,
                  lk_stream_t stream);
+/* Whether lk_prune_run runs the levels of a small tree (at most 16384
+ * parents and a bounded number of children per level) in one persistent
+ * cooperative launch, the batch replay done on the device (1, the default;
+ * LOKI_B200_PRUNE_TAIL=0 in the environment makes 0 the default) or level by
+ * level with host round trips (0). Results are identical. */
+int lk_prune_set_tail(lk_prune* pr, int enable);
 /* core::generate_bp_poly_taylor (lib/taylor.cpp:1643-1741), the
  * FFAPlan::get_branching_pattern("taylor", ref_seg) of the reference: the
  * average branching factor of each of the nsegments - 1 pruning levels. */

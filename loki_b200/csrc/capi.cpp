@@ -1058,6 +1058,13 @@ int lk_plan_branching_pattern(const lk_plan* plan, uint64_t ref_seg, int conserv
     });
 }
 
+int lk_prune_set_tail(lk_prune* pr, int enable) {
+    return guarded([&] {
+        need(pr, "pr");
+        pr->exec->tail_enabled = enable != 0;
+    });
+}
+
 int lk_prune_run(lk_prune* pr, const float* d_ffa_fold, uint64_t ref_seg,
                  const float* thresholds, uint64_t n_thresholds, uint64_t n_iters,
                  lk_prune_stats* stats, uint64_t max_stats, uint64_t* n_stats,

@@ -69,6 +69,12 @@ public:
 
 private:
     void ensure_level_buffers(uint64_t n_parents, uint64_t n_children);
+    // Runs levels first .. last in one cooperative launch while the tree is
+    // small (see prune.cu); appends their stats rows and returns the next
+    // level to run (the host's, when the tail handed a large level back).
+    uint64_t run_tail(const float* d_ffa_fold, const std::vector<uint64_t>& order, uint64_t first,
+                      uint64_t last, const float* thresholds, std::vector<lk_prune_stats>* stats,
+                      cudaStream_t s);
     void level(const float* d_seg, const std::vector<uint64_t>& order, uint64_t level,
                float threshold, lk_prune_stats* st, cudaStream_t s);
     void compact_children(uint64_t c_begin, uint64_t c_end, uint32_t* out_ids, float* out_sc,
@@ -103,6 +109,11 @@ private:
     bool m_ran = false, m_finalized = false;
     DeviceBuffer m_segs, m_tscores_ep;
     DeviceBuffer m_level_mm;  // per level: orderable min / max score keys
+public:
+    // The persistent tail (on by default; LOKI_B200_PRUNE_TAIL=0 turns it off).
+    bool tail_enabled = true;
+private:
+    DeviceBuffer m_tail_ctl, m_tail_levels, m_tail_stats, m_tail_tp;
 };
 
 // Single steps (the Taylor PruneDPFuncts interface, include/loki/core/

@@ -35,12 +35,14 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "lk_block.cuh"
 #include "lk_device.cuh"
 #include "lk_prune.hpp"
+#include "lk_ptx.cuh"
 #include "lk_score.cuh"
 
 namespace lk {
@@ -502,21 +504,25 @@ __device__ __forceinline__ float fkey_inv(uint32_t k) {
 // Phase 2 (thread per child): the reference's sequential prefix sum and
 // width maxima. Phase 3 (warp per child): children scoring at or above
 // thr_keep get their fold written for the world tree.
+// One tile of blockDim.x children starting at c0 (< n); rows: the block's
+// dynamic shared memory (blockDim.x rows of rs floats + 4 blockDim.x words).
+// Ends with warps still writing kept folds: a caller that runs another tile
+// synchronises the block first.
 template <int NW, int NB>
-__global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* __restrict__ parent,
-                            uint64_t n, const float* __restrict__ tree_folds, uint64_t head,
-                            uint64_t cap, const float* __restrict__ ffa_seg, LeafGeom g,
-                            ResolveConsts rc, uint32_t rs, ScoreParams sp, float thr_keep,
-                            float* __restrict__ scores, float* __restrict__ folds_out,
-                            uint32_t* __restrict__ minmax) {
-    extern __shared__ float rows[];
+__device__ __forceinline__ void leaf_tile(float* rows, uint64_t c0, const double* __restrict__ leaves,
+                                          const uint32_t* __restrict__ parent, uint64_t n,
+                                          const float* __restrict__ tree_folds, uint64_t head,
+                                          uint64_t cap, const float* __restrict__ ffa_seg,
+                                          const LeafGeom& g, const ResolveConsts& rc, uint32_t rs,
+                                          const ScoreParams& sp, float thr_keep,
+                                          float* __restrict__ scores, float* __restrict__ folds_out,
+                                          uint32_t* __restrict__ minmax) {
     const uint32_t T = blockDim.x;
     uint32_t* s_pidx = reinterpret_cast<uint32_t*>(rows + static_cast<size_t>(T) * rs);
     uint32_t* s_shift = s_pidx + T;
     uint32_t* s_tree = s_shift + T;
     uint32_t* s_keep = s_tree + T;
     __shared__ uint32_t s_min, s_max;
-    const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * T;
     const uint32_t nhere = static_cast<uint32_t>((n - c0) < T ? (n - c0) : T);
     const uint32_t nb = g.nbins;
     if (threadIdx.x == 0) {
@@ -588,6 +594,19 @@ __global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* _
             o[nb + j] = __fadd_rn(__ldg(tail + nb + j), __ldg(hd + nb + jh));
         }
     }
+}
+
+template <int NW, int NB>
+__global__ void leaf_kernel(const double* __restrict__ leaves, const uint32_t* __restrict__ parent,
+                            uint64_t n, const float* __restrict__ tree_folds, uint64_t head,
+                            uint64_t cap, const float* __restrict__ ffa_seg, LeafGeom g,
+                            ResolveConsts rc, uint32_t rs, ScoreParams sp, float thr_keep,
+                            float* __restrict__ scores, float* __restrict__ folds_out,
+                            uint32_t* __restrict__ minmax) {
+    extern __shared__ float rows[];
+    leaf_tile<NW, NB>(rows, static_cast<uint64_t>(blockIdx.x) * blockDim.x, leaves, parent, n,
+                      tree_folds, head, cap, ffa_seg, g, rc, rs, sp, thr_keep, scores, folds_out,
+                      minmax);
 }
 
 // ---- end of a run: ascend and report --------------------------------------
@@ -867,14 +886,16 @@ __global__ void pc_finish_kernel(const uint64_t* d_base, const uint64_t* d_total
 // D[N-1-N/2+K]. Both are found exactly by an 8-bit MSD radix select over
 // orderable keys (one block, four passes). The new threshold
 // max(current, nextafter(topk), nextafter(median)) replaces *d_thr.
-__global__ void select_threshold_kernel(const float* __restrict__ list_sc, uint64_t size,
+// The body, for one block of any size: returns the new threshold (to every
+// thread) for the current threshold thr.
+__device__ float select_threshold_block(const float* __restrict__ list_sc, uint64_t size,
                                         const float* __restrict__ scores, uint64_t cb0,
                                         uint64_t cb1, uint64_t N, uint64_t r_topk,
-                                        uint64_t r_med, float* d_thr, float* d_debug) {
+                                        uint64_t r_med, float thr, float* d_debug) {
     __shared__ uint32_t hist[2][256];
     __shared__ uint32_t prefix[2];
     __shared__ uint64_t q[2];
-    const float thr = *d_thr;
+    __shared__ float s_eff;
     if (threadIdx.x < 2) {
         prefix[threadIdx.x] = 0;
         // ascending rank of the wanted descending rank
@@ -925,13 +946,28 @@ __global__ void select_threshold_kernel(const float* __restrict__ list_sc, uint6
         float eff = thr;
         eff = (eff < topk) ? topk : eff;
         eff = (eff < med) ? med : eff;
-        *d_thr = eff;
+        s_eff = eff;
         if (d_debug != nullptr) {
             d_debug[0] = fkey_inv(prefix[0]);
             d_debug[1] = fkey_inv(prefix[1]);
         }
     }
+    __syncthreads();
+    const float eff = s_eff;
+    __syncthreads();  // s_eff, hist and prefix are free for the next call
     (void)N;
+    return eff;
+}
+
+__global__ void select_threshold_kernel(const float* __restrict__ list_sc, uint64_t size,
+                                        const float* __restrict__ scores, uint64_t cb0,
+                                        uint64_t cb1, uint64_t N, uint64_t r_topk,
+                                        uint64_t r_med, float* d_thr, float* d_debug) {
+    const float eff = select_threshold_block(list_sc, size, scores, cb0, cb1, N, r_topk, r_med,
+                                             *d_thr, d_debug);
+    if (threadIdx.x == 0) {
+        *d_thr = eff;
+    }
 }
 
 // Level end: transform (poly_taylor_transform_{accel,jerk}_batch,
@@ -1022,17 +1058,15 @@ __device__ __forceinline__ void transform_leaf(const double* in, double* o, uint
     }
 }
 
-__global__ void gather_kernel(const uint32_t* __restrict__ list_ids,
-                              const float* __restrict__ list_sc, uint64_t size,
-                              const double* __restrict__ leaves, const float* __restrict__ folds,
-                              uint64_t write_start, uint64_t cap, uint32_t np, uint32_t nbins,
-                              TransformConsts tc, double* __restrict__ t_leaves,
-                              float* __restrict__ t_folds, float* __restrict__ t_scores) {
-    const uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
-    const uint32_t lane = threadIdx.x % kWarp;
-    if (w >= size) {
-        return;
-    }
+// Survivor w of the write list (one warp): transformed leaf, fold and score
+// into physical slot (write_start + w) mod cap of the other tree buffer.
+__device__ __forceinline__ void gather_one(uint64_t w, uint32_t lane, const uint32_t* __restrict__ list_ids,
+                                           const float* __restrict__ list_sc,
+                                           const double* __restrict__ leaves,
+                                           const float* __restrict__ folds, uint64_t write_start,
+                                           uint64_t cap, uint32_t np, uint32_t nbins,
+                                           const TransformConsts& tc, double* __restrict__ t_leaves,
+                                           float* __restrict__ t_folds, float* __restrict__ t_scores) {
     const uint64_t c = list_ids[w];
     const uint64_t ph = (write_start + w) % cap;
     const uint32_t ls = (np + 2) * 2;
@@ -1045,6 +1079,20 @@ __global__ void gather_kernel(const uint32_t* __restrict__ list_ids,
     for (uint32_t j = lane; j < 2 * nbins; j += kWarp) {
         dst[j] = src[j];
     }
+}
+
+__global__ void gather_kernel(const uint32_t* __restrict__ list_ids,
+                              const float* __restrict__ list_sc, uint64_t size,
+                              const double* __restrict__ leaves, const float* __restrict__ folds,
+                              uint64_t write_start, uint64_t cap, uint32_t np, uint32_t nbins,
+                              TransformConsts tc, double* __restrict__ t_leaves,
+                              float* __restrict__ t_folds, float* __restrict__ t_scores) {
+    const uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
+    if (w >= size) {
+        return;
+    }
+    gather_one(w, threadIdx.x % kWarp, list_ids, list_sc, leaves, folds, write_start, cap, np, nbins,
+               tc, t_leaves, t_folds, t_scores);
 }
 
 // In-place transform of leaves named by indices (the standalone entry
@@ -1083,6 +1131,406 @@ __global__ void parent_transform_kernel(double* __restrict__ tree_leaves, uint64
     transform_leaf(lf, tmp, np, tc);
     for (uint32_t q = 0; q < (np + 2) * 2; ++q) {
         lf[q] = tmp[q];
+    }
+}
+
+// ---- persistent tail of a run -----------------------------------------------
+//
+// Once the tree is small, a level's kernels are short and the level is bound
+// by launches and by the two host round trips of its batch replay. The tail
+// kernel runs the remaining levels in ONE cooperative launch (one block per
+// SM): the same steps and the same device functions as the level-by-level
+// path, separated by grid barriers, with the batch replay (sizes, space left,
+// batch boundaries at the buffer's wrap, overload steps) done by block 0 on
+// the device. It hands the run back to the host, before changing anything,
+// when a level has more parents or children than its buffers hold.
+
+constexpr uint32_t kTailBatches = 64;    // batches of one level (wrap splits included)
+constexpr uint64_t kTailParents = 16384;  // largest level (parents) the tail runs
+constexpr uint64_t kTailChildren = 1 << 17;  // most children of one tail level
+constexpr uint32_t kTailExitNone = 0;
+constexpr uint32_t kTailExitDone = 1;    // every level run, or the tree emptied
+constexpr uint32_t kTailExitHandBack = 2;  // level `level` too large: host continues
+constexpr uint32_t kTailExitError = 3;   // status bits / reason set; the host fails
+constexpr uint32_t kTailReasonBatch = 1; // a batch's children exceed batch_size * branch_max
+constexpr uint32_t kTailReasonBig = 2;   // a level's children exceed 2^32 - 1
+
+// One level's constants (host-computed, as the level-by-level path does).
+struct TailLevel {
+    const float* seg;      // FFA segment of the level
+    float threshold;
+    double dt;             // current coordinate's scale (branching)
+    ResolveConsts rc;
+    TransformConsts tc;    // survivors to the next coordinate
+    TransformConsts pt;    // Chebyshev: parents re-centred first
+};
+
+// Device-resident state of the tail (zeroed barrier words, the tree entering
+// the first level; the rest is scratch written by block 0).
+struct TailCtl {
+    uint64_t head, size;
+    uint32_t cur, level, exit, reason;
+    uint32_t status;
+    uint32_t bar_count, bar_gen;
+    uint32_t li, nbat;
+    float thr;
+    uint64_t n_par, n_child, write_start;
+    uint64_t bstart[kTailBatches + 1], bsize[kTailBatches], cstart[kTailBatches + 1];
+};
+
+struct TailArgs {
+    double* tleaves[2];
+    float* tfolds[2];
+    float* tscores[2];
+    uint32_t* lids[2];
+    float* lsc[2];
+    double* cleaves;
+    uint32_t* cparent;
+    float* cscores;
+    float* cfolds;
+    double* tp;            // re-centred parents (Chebyshev)
+    uint32_t* counts;
+    uint64_t* offsets;
+    const TailLevel* lconst;  // indexed by level
+    TailCtl* ctl;
+    uint64_t* stats;       // per level: parents, children, survivors
+    uint32_t* level_mm;    // per level: orderable min / max score keys
+    uint64_t cap, batch, branch_max, max_parents, max_children;
+    uint32_t last_level, rs;
+    LeafGeom geom;
+    ScoreParams sp;
+};
+
+// Grid barrier of a cooperative launch (all blocks resident), bounded like
+// every device wait here: false (and the status bit set) when it gave up.
+__device__ bool tail_barrier(TailCtl* ctl) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile uint32_t* gen = &ctl->bar_gen;
+        const uint32_t g0 = *gen;
+        __threadfence();
+        if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
+            atomicExch(&ctl->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&ctl->bar_gen, 1u);
+        } else {
+            const uint64_t t0 = ptx::globaltimer_ns();
+            uint32_t it = 0;
+            while (*gen == g0) {
+                ++it;
+                if (((it & 255u) == 0 && ptx::globaltimer_ns() - t0 > ptx::kWaitLimitNs) ||
+                    it >= (1u << 26)) {
+                    atomicOr(&ctl->status, dev::kStatusWaitTimeout);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Ordered compaction by one block: items [0, n) kept by keep(i) are written
+// as (id(i), score(i)) at out[pos + rank] while pos + rank < limit; returns
+// the number kept. Thread t takes a contiguous run of the items.
+template <class Keep, class Id, class Score>
+__device__ uint64_t block_append(uint64_t n, Keep keep, Id id, Score score, uint32_t* out_ids,
+                                 float* out_sc, uint64_t pos, uint64_t limit) {
+    __shared__ uint32_t ws[32];
+    const uint64_t per = (n + blockDim.x - 1) / blockDim.x;
+    const uint64_t i0 = threadIdx.x * per;
+    const uint64_t i1 = min(n, i0 + per);
+    uint32_t c = 0;
+    for (uint64_t i = i0; i < i1; ++i) {
+        c += keep(i) ? 1u : 0u;
+    }
+    uint32_t total;
+    uint64_t o = pos + blk::block_exclusive_scan(c, ws, &total);
+    for (uint64_t i = i0; i < i1; ++i) {
+        if (keep(i)) {
+            if (o < limit) {
+                out_ids[o] = id(i);
+                out_sc[o] = score(i);
+            }
+            ++o;
+        }
+    }
+    __syncthreads();  // ws is reused by the next scan
+    return total;
+}
+
+template <int NW, int NB>
+__global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
+    extern __shared__ float rows[];
+    TailCtl* ctl = a.ctl;
+    // values other blocks wrote before a barrier are read through vc
+    volatile TailCtl* vc = a.ctl;
+    const LeafGeom& g = a.geom;
+    const uint32_t np = g.np, ls = g.ls, nb = g.nbins;
+    const uint64_t cap = a.cap;
+    for (;;) {
+        // 0. the level's set-up (block 0, thread 0): batches as get_leaves_span
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const uint32_t lv = ctl->level;
+            const uint64_t n_par = ctl->size;
+            if (lv > a.last_level || n_par == 0) {
+                ctl->exit = kTailExitDone;
+            } else if (n_par > a.max_parents) {
+                ctl->exit = kTailExitHandBack;
+            } else {
+                const uint64_t bmin = a.batch < n_par ? a.batch : n_par;
+                const uint64_t bs = bmin > 0 ? bmin : 1;
+                uint32_t nbat = 0;
+                uint64_t done = 0;
+                while (done < n_par && nbat < kTailBatches) {
+                    const uint64_t want = min(bs, n_par - done);
+                    const uint64_t phys = (ctl->head + done) % cap;
+                    const uint64_t take = min(want, cap - phys);
+                    ctl->bstart[nbat] = done;
+                    ctl->bsize[nbat] = take;
+                    done += take;
+                    ++nbat;
+                }
+                if (done < n_par) {
+                    ctl->exit = kTailExitHandBack;
+                } else {
+                    ctl->bstart[nbat] = n_par;
+                    ctl->nbat = nbat;
+                    ctl->n_par = n_par;
+                    ctl->write_start = (ctl->head + n_par) % cap;
+                    ctl->thr = a.lconst[lv].threshold;
+                    a.level_mm[2 * lv] = 0xffffffffu;
+                    a.level_mm[2 * lv + 1] = 0u;
+                }
+            }
+        }
+        if (!tail_barrier(ctl) || vc->exit != kTailExitNone) {
+            return;
+        }
+        const uint32_t lv = vc->level;
+        const TailLevel& L = a.lconst[lv];
+        const uint64_t n_par = vc->n_par, head = vc->head;
+        const int cur = static_cast<int>(vc->cur);
+        const double* tree = a.tleaves[cur];
+        const uint64_t gtid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+        const uint64_t gthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+
+        // 1. branch counts (Chebyshev: parents re-centred into tp, the tree
+        //    is not written, so a hand-back leaves it as it was)
+        for (uint64_t i = gtid; i < n_par; i += gthreads) {
+            const double* lf = tree + ((head + i) % cap) * ls;
+            if (g.basis == 1) {
+                double* t = a.tp + i * ls;
+                double tmp[10];
+                transform_leaf(lf, tmp, np, L.pt);
+                for (uint32_t q = 0; q < ls; ++q) {
+                    t[q] = tmp[q];
+                }
+                lf = t;
+            }
+            ParamBranch pb[3];
+            branch_params(lf, L.dt, g, pb, &ctl->status);
+            uint64_t prod = 1;
+            for (uint32_t k = 0; k < np; ++k) {
+                prod *= pb[k].count;
+            }
+            if (prod > 0xffffffffull) {
+                atomicOr(&ctl->status, kStatusBranchCount);
+                prod = 1;
+            }
+            a.counts[i] = static_cast<uint32_t>(prod);
+        }
+        if (!tail_barrier(ctl)) {
+            return;
+        }
+        // 2. offsets, batch child ranges, checks (block 0)
+        if (blockIdx.x == 0) {
+            __shared__ uint32_t ws[32];
+            const uint64_t per = (n_par + blockDim.x - 1) / blockDim.x;
+            const uint64_t i0 = threadIdx.x * per, i1 = min(n_par, i0 + per);
+            uint64_t c = 0;
+            for (uint64_t i = i0; i < i1; ++i) {
+                c += a.counts[i];
+            }
+            // the exact total first: below 2^32 the 32-bit scan is exact too
+            // (a larger total ends the tail with an error before any use)
+            __shared__ unsigned long long s_total;
+            if (threadIdx.x == 0) {
+                s_total = 0;
+            }
+            __syncthreads();
+            atomicAdd(&s_total, static_cast<unsigned long long>(c));
+            uint32_t tot32;
+            uint64_t o = blk::block_exclusive_scan(static_cast<uint32_t>(c), ws, &tot32);
+            __syncthreads();
+            for (uint64_t i = i0; i < i1; ++i) {
+                a.offsets[i] = o;
+                o += a.counts[i];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const uint64_t n_child = s_total;
+                const uint32_t nbat = ctl->nbat;
+                ctl->n_child = n_child;
+                for (uint32_t b = 0; b <= nbat; ++b) {
+                    ctl->cstart[b] = ctl->bstart[b] < n_par ? a.offsets[ctl->bstart[b]] : n_child;
+                }
+                const uint32_t st = ctl->status;
+                if (st & (kStatusBranchMax | kStatusZeroStep | kStatusBranchCount)) {
+                    ctl->exit = kTailExitError;
+                } else if (n_child >= (1ull << 32)) {
+                    ctl->exit = kTailExitError;
+                    ctl->reason = kTailReasonBig;
+                } else {
+                    for (uint32_t b = 0; b < nbat; ++b) {
+                        if (ctl->cstart[b + 1] - ctl->cstart[b] > a.batch * a.branch_max) {
+                            ctl->exit = kTailExitError;
+                            ctl->reason = kTailReasonBatch;
+                        }
+                    }
+                    if (ctl->exit == kTailExitNone && n_child > a.max_children) {
+                        ctl->exit = kTailExitHandBack;
+                    }
+                }
+            }
+        }
+        if (!tail_barrier(ctl) || vc->exit != kTailExitNone) {
+            return;
+        }
+        const uint64_t n_child = vc->n_child;
+        // 3. children's leaves (branch_emit_kernel's order)
+        for (uint64_t i = gtid; i < n_par; i += gthreads) {
+            const double* lf = g.basis == 1 ? a.tp + i * ls : tree + ((head + i) % cap) * ls;
+            ParamBranch pb[3];
+            branch_params(lf, L.dt, g, pb, &ctl->status);
+            uint64_t o = a.offsets[i];
+            const uint32_t c2 = np == 3 ? pb[2].count : 1;
+            for (uint32_t x = 0; x < pb[0].count; ++x) {
+                const double va = branch_value(pb[0], x);
+                for (uint32_t y = 0; y < pb[1].count; ++y) {
+                    const double vb = branch_value(pb[1], y);
+                    for (uint32_t z = 0; z < c2; ++z) {
+                        double* d = a.cleaves + o * ls;
+                        d[0] = va;
+                        d[1] = pb[0].dparam;
+                        d[2] = vb;
+                        d[3] = pb[1].dparam;
+                        if (np == 3) {
+                            d[4] = branch_value(pb[2], z);
+                            d[5] = pb[2].dparam;
+                        }
+                        for (uint32_t q = 2 * np; q < ls; ++q) {
+                            d[q] = lf[q];
+                        }
+                        a.cparent[o] = static_cast<uint32_t>(i);
+                        ++o;
+                    }
+                }
+            }
+        }
+        if (!tail_barrier(ctl)) {
+            return;
+        }
+        // 4. resolve, shift-add, score, kept folds (tiles of blockDim children)
+        for (uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x; c0 < n_child;
+             c0 += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+            leaf_tile<NW, NB>(rows, c0, a.cleaves, a.cparent, n_child, a.tfolds[cur], head, cap, L.seg,
+                              g, L.rc, a.rs, a.sp, L.threshold, a.cscores, a.cfolds,
+                              a.level_mm + 2 * lv);
+            __syncthreads();
+        }
+        if (!tail_barrier(ctl)) {
+            return;
+        }
+        // 5. filter + add in the reference's batch order (block 0)
+        if (blockIdx.x == 0) {
+            const uint32_t nbat = vc->nbat;
+            uint64_t size = 0, read_consumed = 0;
+            int li = 0;
+            float thr = L.threshold;
+            const float* sc = a.cscores;
+            for (uint32_t b = 0; b < nbat; ++b) {
+                const uint64_t cb0 = vc->cstart[b], cb1 = vc->cstart[b + 1];
+                __shared__ uint32_t ws[32];
+                uint32_t cnt_local = 0;
+                for (uint64_t i = cb0 + threadIdx.x; i < cb1; i += blockDim.x) {
+                    cnt_local += sc[i] >= thr ? 1u : 0u;
+                }
+                uint32_t cnt;
+                blk::block_exclusive_scan(cnt_local, ws, &cnt);
+                __syncthreads();
+                const uint64_t space = cap - ((n_par - read_consumed) + size);
+                const uint64_t nb_c = cb1 - cb0;
+                auto child_id = [&](uint64_t i) { return static_cast<uint32_t>(cb0 + i); };
+                auto child_sc = [&](uint64_t i) { return sc[cb0 + i]; };
+                if (cnt <= space) {
+                    const float t = thr;
+                    size += block_append(nb_c, [&](uint64_t i) { return sc[cb0 + i] >= t; }, child_id, child_sc,
+                                         a.lids[li], a.lsc[li], size, cap);
+                } else {
+                    // overload (lib/world_tree.cpp:386-421)
+                    const uint64_t K = size + space;
+                    const uint64_t N = size + cnt;
+                    const uint64_t m = N / 2;
+                    const uint64_t r_med = (m <= K - 1) ? (K - 1 - m) : (N - 1 - m + K);
+                    thr = select_threshold_block(a.lsc[li], size, sc, cb0, cb1, N, K - 1, r_med, thr,
+                                                 nullptr);
+                    const float t = thr;
+                    const uint32_t* lid = a.lids[li];
+                    const float* lsc = a.lsc[li];
+                    const uint64_t kept = block_append(
+                        size, [&](uint64_t i) { return lsc[i] > t; }, [&](uint64_t i) { return lid[i]; },
+                        [&](uint64_t i) { return lsc[i]; }, a.lids[1 - li], a.lsc[1 - li], 0, cap);
+                    const uint64_t added = block_append(
+                        nb_c, [&](uint64_t i) { return sc[cb0 + i] >= t; }, child_id, child_sc,
+                        a.lids[1 - li], a.lsc[1 - li], kept, K);
+                    size = min(kept + added, K);
+                    li = 1 - li;
+                }
+                read_consumed += vc->bsize[b];
+            }
+            if (threadIdx.x == 0) {
+                ctl->li = static_cast<uint32_t>(li);
+                ctl->size = size;  // survivors (the next level's parents)
+                ctl->thr = thr;
+            }
+        }
+        if (!tail_barrier(ctl)) {
+            return;
+        }
+        // 6. survivors transformed and gathered into the other tree buffer
+        {
+            const uint64_t size = vc->size;
+            const int li = static_cast<int>(vc->li);
+            const uint64_t ws0 = vc->write_start;
+            const int nxt = 1 - cur;
+            const uint64_t gw = gtid / kWarp, nwarps = gthreads / kWarp;
+            for (uint64_t w = gw; w < size; w += nwarps) {
+                gather_one(w, threadIdx.x % kWarp, a.lids[li], a.lsc[li], a.cleaves, a.cfolds, ws0, cap, np,
+                           nb, L.tc, a.tleaves[nxt], a.tfolds[nxt], a.tscores[nxt]);
+            }
+        }
+        if (!tail_barrier(ctl)) {
+            return;
+        }
+        // 7. the level's end (finalize_in_place_update) and its statistics
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const uint64_t size = ctl->size;
+            a.stats[3 * lv] = n_par;
+            a.stats[3 * lv + 1] = n_child;
+            a.stats[3 * lv + 2] = size;
+            ctl->head = ctl->write_start;
+            if (size > 0) {
+                ctl->cur = 1u - ctl->cur;
+            }
+            ctl->level = lv + 1;
+        }
+        // the next level's set-up waits at its first barrier
     }
 }
 
@@ -1279,6 +1727,9 @@ PruneExec::PruneExec(const Plan& plan, uint64_t max_sugg, uint64_t batch_size,
       m_branch_max(branch_max),
       m_conservative(conservative),
       m_basis(basis) {
+    if (const char* e = std::getenv("LOKI_B200_PRUNE_TAIL")) {
+        tail_enabled = std::atoi(e) != 0;
+    }
     m_np = plan.nparams;
     require(!plan.offsets_overflow, "coordinate offsets exceed 32 bits");
     require(m_np == 2 || m_np == 3,
@@ -1485,8 +1936,23 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
     if (m_level_mm.bytes < 2 * (levels + 1) * sizeof(uint32_t)) {
         m_level_mm.alloc(2 * (levels + 1) * sizeof(uint32_t));
     }
-    for (uint64_t lv = 1; lv <= levels; ++lv) {
+    // Small trees run in the persistent tail; a level it hands back (too many
+    // parents or children) runs here, then the tail is tried again.
+    bool handed_back = false;
+    for (uint64_t lv = 1; lv <= levels;) {
         require(lv <= n_thresholds, "Pruning complete - exceeded threshold scheme length");
+        if (tail_enabled && !handed_back && m_tree.size <= kTailParents) {
+            const uint64_t last = std::min(levels, n_thresholds);
+            const uint64_t next = run_tail(d_ffa_fold, order, lv, last, thresholds, &stats, s);
+            if (m_tree.size == 0) {
+                break;
+            }
+            // stopped before the last level with leaves left: handed back
+            handed_back = next <= last;
+            lv = next;
+            continue;
+        }
+        handed_back = false;
         const float* d_seg = d_ffa_fold + order[lv] * seg_floats;
         lk_prune_stats st{};
         level(d_seg, order, lv, thresholds[lv - 1], &st, s);
@@ -1495,6 +1961,7 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
         if (m_tree.size == 0) {
             break;
         }
+        ++lv;
     }
     if (stats.size() > 1) {
         std::vector<uint32_t> mm(2 * stats.size());
@@ -1508,6 +1975,145 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
         }
     }
     return stats;
+}
+
+uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t>& order,
+                            uint64_t first, uint64_t last, const float* thresholds,
+                            std::vector<lk_prune_stats>* stats, cudaStream_t s) {
+    const uint64_t seg_floats = m_ncoords * 2 * m_nbins;
+    // children buffers: up to kTailChildren, at most 256 MiB of child data
+    const uint64_t per_child = m_ls * sizeof(double) + 8 + 2 * m_nbins * sizeof(float);
+    const uint64_t max_children = std::min<uint64_t>(kTailChildren, (256ull << 20) / per_child);
+    ensure_level_buffers(kTailParents, max_children);
+    if (m_tail_tp.bytes < kTailParents * m_ls * sizeof(double)) {
+        m_tail_tp.alloc(kTailParents * m_ls * sizeof(double));
+    }
+    if (m_tail_ctl.bytes < sizeof(TailCtl)) {
+        m_tail_ctl.alloc(sizeof(TailCtl));
+    }
+    if (m_tail_levels.bytes < (last + 1) * sizeof(TailLevel)) {
+        m_tail_levels.alloc((last + 1) * sizeof(TailLevel));
+    }
+    if (m_tail_stats.bytes < 3 * (last + 1) * sizeof(uint64_t)) {
+        m_tail_stats.alloc(3 * (last + 1) * sizeof(uint64_t));
+    }
+    // the level constants, as level() derives them
+    std::vector<TailLevel> lc(last + 1);
+    const Coord ci = mo_coord(order, 0, m_tseg);
+    for (uint64_t lv = first; lv <= last; ++lv) {
+        const Coord cp = mo_coord(order, lv - 1, m_tseg);
+        const Coord cn = mo_coord(order, lv, m_tseg);
+        const Coord cc = mo_current_coord(order, lv, m_tseg);
+        const Coord ca = mo_segment_coord(order, lv, m_tseg);
+        TailLevel& L = lc[lv];
+        L.seg = d_ffa_fold + order[lv] * seg_floats;
+        L.threshold = thresholds[lv - 1];
+        L.dt = cc.scale;
+        L.rc = m_basis == 1 ? make_resolve_cheby(m_np, ca, cc, ci) : make_resolve(m_np, ca.ref, cc.ref, ci.ref);
+        L.tc = m_basis == 1 ? make_transform_cheby(cn, cc)
+                            : make_transform(m_np, cn.ref, cc.ref, m_conservative);
+        L.pt = m_basis == 1 ? make_transform_cheby(cc, cp) : TransformConsts{};
+    }
+    LK_CUDA(cudaMemcpyAsync(m_tail_levels.ptr, lc.data(), lc.size() * sizeof(TailLevel),
+                            cudaMemcpyHostToDevice, s));
+    TailCtl c{};
+    c.head = m_tree.head;
+    c.size = m_tree.size;
+    c.cur = static_cast<uint32_t>(m_cur);
+    c.level = static_cast<uint32_t>(first);
+    LK_CUDA(cudaMemcpyAsync(m_tail_ctl.ptr, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+
+    TailArgs a{};
+    for (int i = 0; i < 2; ++i) {
+        a.tleaves[i] = m_tleaves[i].as<double>();
+        a.tfolds[i] = m_tfolds[i].as<float>();
+        a.tscores[i] = m_tscores[i].as<float>();
+        a.lids[i] = m_lids[i].as<uint32_t>();
+        a.lsc[i] = m_lsc[i].as<float>();
+    }
+    a.cleaves = m_cleaves.as<double>();
+    a.cparent = m_cparent.as<uint32_t>();
+    a.cscores = m_cscores.as<float>();
+    a.cfolds = m_cfolds.as<float>();
+    a.tp = m_tail_tp.as<double>();
+    a.counts = m_counts.as<uint32_t>();
+    a.offsets = m_offsets.as<uint64_t>();
+    a.lconst = m_tail_levels.as<TailLevel>();
+    a.ctl = m_tail_ctl.as<TailCtl>();
+    a.stats = m_tail_stats.as<uint64_t>();
+    a.level_mm = m_level_mm.as<uint32_t>();
+    a.cap = m_cap;
+    a.batch = m_batch;
+    a.branch_max = m_branch_max;
+    a.max_parents = kTailParents;
+    a.max_children = max_children;
+    a.last_level = static_cast<uint32_t>(last);
+    a.rs = sc::row_stride(m_nbins, m_sp.wmax);
+    a.geom = make_geom(m_plan, m_branch_max, m_basis);
+    a.sp = m_sp;
+    const uint32_t T = sc::profiles_per_block(a.rs + 4);
+    const size_t smem = static_cast<size_t>(T) * a.rs * sizeof(float) + 4 * T * sizeof(uint32_t);
+    int dev = 0, nsm = 148;
+    LK_CUDA(cudaGetDevice(&dev));
+    LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
+        auto kern = prune_tail_kernel<decltype(nw)::value, decltype(nbc)::value>;
+        sc::set_smem(kern, smem);
+        int per_sm = 0;
+        LK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, static_cast<int>(T), smem));
+        require(per_sm >= 1, "pruning tail: one block per SM does not fit");
+        void* args[] = {&a};
+        // one block per SM, all resident (cooperative launch): the grid
+        // barriers between the steps of a level need every block running
+        LK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(nsm), dim3(T), args,
+                                            smem, s));
+    });
+    LK_CUDA(cudaGetLastError());
+    LK_CUDA(cudaMemcpyAsync(&c, m_tail_ctl.ptr, sizeof(c), cudaMemcpyDeviceToHost, s));
+    std::vector<uint64_t> st(3 * (last + 1));
+    LK_CUDA(cudaMemcpyAsync(st.data(), m_tail_stats.ptr, st.size() * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, s));
+    LK_CUDA(cudaStreamSynchronize(s));
+    if (c.status & dev::kStatusWaitTimeout) {
+        fail(LK_ERR_DEVICE_TIMEOUT, "pruning tail: a grid barrier gave up waiting");
+    }
+    if (c.exit == kTailExitError) {
+        if (c.status & kStatusBranchMax) {
+            fail(LK_ERR_INVALID_ARG, "num_points must be less than or equal to branch_max");
+        }
+        if (c.status & kStatusZeroStep) {
+            fail(LK_ERR_INVALID_ARG, "Both dparam_cur and dparam_new must be positive");
+        }
+        if (c.status & kStatusBranchCount) {
+            fail(LK_ERR_UNSUPPORTED, "a parent has more than 2^32-1 children");
+        }
+        if (c.reason == kTailReasonBatch) {
+            fail(LK_ERR_INVALID_ARG,
+                 "Branch factor exceeded workspace size:n_leaves_batch <= max_branched_leaves");
+        }
+        fail(LK_ERR_UNSUPPORTED, "more than 2^32 children in one level");
+    }
+    for (uint64_t lv = first; lv < c.level; ++lv) {
+        lk_prune_stats r{};
+        r.level = lv;
+        r.seg_idx = order[lv];
+        r.n_branches = st[3 * lv];
+        r.n_leaves = st[3 * lv + 1];
+        r.n_leaves_phy = st[3 * lv + 1];
+        r.n_leaves_surv = st[3 * lv + 2];
+        r.threshold = thresholds[lv - 1];
+        r.score_min = FLT_MAX;   // filled by run() from the level's device slot
+        r.score_max = -FLT_MAX;
+        stats->push_back(r);
+        m_level = lv;
+    }
+    m_tree.head = c.head;
+    m_tree.size = c.size;
+    m_tree.size_old = 0;
+    m_tree.read_consumed = 0;
+    m_tree.write_start = (c.head + c.size) % m_tree.cap;
+    m_cur = static_cast<int>(c.cur);
+    return c.level;
 }
 
 void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, uint64_t lv,

@@ -119,6 +119,12 @@ class PruneCUDA:
                 pass
             self._h = None
 
+    def set_persistent_tail(self, enable: bool = True) -> None:
+        """Run the levels of a small tree in one persistent cooperative launch
+        (the default) or level by level with host round trips; results are
+        identical."""
+        C.check(C.lib().lk_prune_set_tail(self._h, int(bool(enable))))
+
     def run(self, ffa_fold, ref_seg: int, thresholds, n_iters: int | None = None) -> np.ndarray:
         """Seed from segment ``ref_seg`` of the final FFA fold (CUDA tensor or host
         array, [nsegments, ncoords, 2, nbins]) and prune; returns the per-level

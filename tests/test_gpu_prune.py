@@ -88,6 +88,27 @@ def test_prune_run_bit_exact(cuda, name):
     np.testing.assert_array_equal(_stats_matrix(stats2), _stats_matrix(want[0]))
 
 
+@pytest.mark.parametrize("name", ["accel_nb32_overload", "accel_nb32_wrap", "accel_nb32_many_batches",
+                                  "jerk_nb32_big"])
+def test_prune_tail_matches_level_by_level(cuda, name):
+    """The persistent tail (small trees in one cooperative launch, batch
+    replay on the device; hands large levels back) gives exactly the
+    level-by-level run: statistics, leaves, folds, scores."""
+    from loki_b200.prune import PruneCUDA
+
+    plan, cfg, _, fold, nseg, ref_seg, thr, ms, bs, cons = _setup(name)
+    runs = []
+    for tail in (False, True):
+        pr = PruneCUDA(cfg, max_sugg=ms, batch_size=bs, branch_max=None, use_conservative_tile=cons)
+        pr.set_persistent_tail(tail)
+        stats = pr.run(fold, ref_seg, thr)
+        runs.append((_stats_matrix(stats), pr.tree()))
+    (s0, t0), (s1, t1) = runs
+    np.testing.assert_array_equal(s1, s0)
+    for a, b in zip(t0, t1):
+        np.testing.assert_array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
 @pytest.mark.parametrize("name", ["prune_accel_nb16.npz", "prune_jerk_nb16.npz"])
 def test_prune_reference_golden_fixtures(cuda, name):
     from loki_b200.configs import PulsarSearchConfig
