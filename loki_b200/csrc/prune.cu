@@ -2056,6 +2056,10 @@ uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t
     int dev = 0, nsm = 148;
     LK_CUDA(cudaGetDevice(&dev));
     LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    // blocks: one per SM by default (LOKI_B200_PRUNE_TAIL_BLOCKS: fewer)
+    if (const char* e = std::getenv("LOKI_B200_PRUNE_TAIL_BLOCKS")) {
+        nsm = std::max(1, std::min(nsm, std::atoi(e)));
+    }
     sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
         auto kern = prune_tail_kernel<decltype(nw)::value, decltype(nbc)::value>;
         sc::set_smem(kern, smem);
