@@ -110,8 +110,19 @@ class FFACUDA:
             return fold
         return out[:n].cpu().numpy() if host else out
 
+    @property
+    def scores_exact(self) -> bool:
+        """Whether scores() equals the FP32 (reference) S/N bit for bit: True
+        for FP32 storage. With BF16 storage the S/N values carry the storage
+        error (RMS ~0.008, at most ~0.06 on the 2^22-sample accelerated
+        search against FP64); search() still returns the FP32 candidates and
+        S/N, rescoring every cell near the threshold exactly."""
+        return self._storage == "fp32"
+
     def scores(self, ts_e, ts_v, out=None):
-        """Boxcar S/N [ncoords_final, n_widths] (final level fused with scoring)."""
+        """Boxcar S/N [ncoords_final, n_widths] (final level fused with scoring).
+        With fold_storage="bf16" these are approximations (see scores_exact);
+        candidates come exact from search()."""
         host = not (D.is_device_tensor(ts_e) and D.is_device_tensor(ts_v))
         e, v = self._inputs(ts_e, ts_v)
         nc = int(self._plan.ncoords[-1])

@@ -51,6 +51,7 @@ def test_bf16_search_candidates_identical(cuda, name):
     cfg, op, w, ts_e, ts_v = make(name)
     plain = FFACUDA(cfg, fold_storage="fp32")
     mixed = FFACUDA(cfg, fold_storage="bf16")
+    assert plain.scores_exact and not mixed.scores_exact  # BF16 scores() are approximate
     s32 = plain.scores(ts_e, ts_v)
     for q in (0.99, 0.999, 0.99999):
         thr = float(np.quantile(s32, q))
