@@ -380,7 +380,6 @@ typedef struct lk_tuning {
     float merge_ms;      /* all merge levels, */
     float score_ms;      /* fused final level */
     uint32_t bf_tmem_warps; /* brute fold: consumer warps (of bf_warps) whose sums are in tensor memory */
-    uint32_t bf_seg_groups; /* brute fold: 32-segment groups per consumer warp (0 or 1: one, 2: two) */
 } lk_tuning;
 /* Times the candidates on the given device series (one search's inputs;
  * reps timed passes each, median) and keeps the fastest shape of each stage.

@@ -106,7 +106,7 @@ class LkStageTime(ctypes.Structure):
 class LkTuning(ctypes.Structure):
     _fields_ = [("bf_rows", u32), ("bf_warps", u32), ("bf_stages", u32), ("merge_rows_in_flight", ctypes.c_int32),
                 ("score_cells_per_block", u32), ("candidates", u32), ("bf_ms", f32), ("merge_ms", f32),
-                ("score_ms", f32), ("bf_tmem_warps", u32), ("bf_seg_groups", u32)]
+                ("score_ms", f32), ("bf_tmem_warps", u32)]
 
 
 class LkSweepOptions(ctypes.Structure):

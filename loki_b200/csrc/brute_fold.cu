@@ -930,331 +930,6 @@ __global__ void __launch_bounds__(kMaxWarpsTm * 32, 1)
     }
 }
 
-// Two segment groups per warp: the packed TMEM kernel with each consumer
-// warp folding its frequency over 64 segments, lane l holding segments l and
-// 32 + l. Both groups share the frequency's run masks, run bins, branches and
-// bookkeeping, so every sample costs two independent add.rn.f32x2 (one per
-// group: two add chains in flight) against one set of run-start tests. A
-// bin's sums are one float4 (group 0's E, V, group 1's E, V): four TMEM
-// columns 4 b .. 4 b + 3 (one 32x32b.x4 store / read per run start) or one
-// 16-byte shared-memory word per lane. Every add is the same IEEE add in the
-// same order as in the one-group kernels.
-constexpr int kMaxWarpsTm2 = 16;  // consumers + producer (<= 128 registers)
-
-__device__ __forceinline__ float4 add4_rn(float4 acc, float2 x0, float2 x1) {
-    const float2 a = add2_rn(make_float2(acc.x, acc.y), x0);
-    const float2 b = add2_rn(make_float2(acc.z, acc.w), x1);
-    return make_float4(a.x, a.y, b.x, b.y);
-}
-
-template <class BinT>
-__global__ void __launch_bounds__(kMaxWarpsTm2 * 32, 1)
-    brute_fold_pk_tm2_kernel(const __grid_constant__ CUtensorMap tmap_ev,
-                             const __grid_constant__ CUtensorMap tmap_ev8, FoldArgs a) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    constexpr uint32_t kStage2 = 2 * kStageBytes;  // [group][half] tiles
-    const bool grouped = a.groups != nullptr;
-    if (grouped && blockIdx.x * 8u >= *a.ngroups) {
-        return;  // uniform, before any tensor memory is allocated
-    }
-    const uint32_t S = a.stages;
-    unsigned char* ring = smem_raw;
-    uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * kStage2);
-    uint64_t* empty = full + S;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(empty + S);
-    float4* accs = reinterpret_cast<float4*>(smem_raw + S * kStage2 + 1024);  // 16-byte aligned
-
-    const int warp = threadIdx.x / kWarp;
-    const int lane = threadIdx.x % kWarp;
-    const int W = static_cast<int>(a.warps);
-    const int WS = static_cast<int>(a.smem_warps);
-    const uint32_t q0 = blockIdx.y * a.warps;
-    const int nconsumers = static_cast<int>(min(a.warps, a.nfreq - q0));
-    const int slot = warp >= WS ? warp - WS : warp + (W - WS);
-    const int seg0 = static_cast<int>(blockIdx.x * 2 * kWarp);
-    const bool aligned = (ptx::smem_u32(ring) & 1023u) == 0;
-
-    if (warp == W) {
-        ptx::tmem_alloc(tslot, kTmemCols);
-        __syncwarp();
-        ptx::tmem_relinquish();
-    }
-    if (threadIdx.x == 0) {
-        if (!aligned) {
-            atomicOr(a.status, dev::kStatusBadTable);
-        }
-        ptx::prefetch_tensormap(grouped ? &tmap_ev8 : &tmap_ev);
-        for (uint32_t s = 0; s < S; ++s) {
-            ptx::mbar_init(&full[s], 1);
-            ptx::mbar_init(&empty[s], nconsumers * kWarp);
-        }
-        ptx::fence_barrier_init();
-    }
-    ptx::tmem_fence_before_sync();
-    __syncthreads();
-    ptx::tmem_fence_after_sync();
-    const uint32_t tbase = *tslot;
-
-    if (aligned && warp == W) {
-        if (lane == 0) {
-            // group mode: the block's eight 8-segment groups, four per half
-            uint32_t grow[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-            if (grouped) {
-                const uint32_t ng = *a.ngroups, g0 = blockIdx.x * 8u;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    grow[q / 4][q % 4] = a.groups[g0 + q < ng ? g0 + q : g0];
-                }
-            }
-            uint32_t issued = 0;
-            for (uint32_t k = 0; k < a.nwords; ++k) {
-                const uint32_t s = k % S;
-                if (k >= S &&
-                    !ptx::mbar_wait_bounded(&empty[s], ((k / S) - 1) & 1u, a.status,
-                                            dev::kStatusWaitTimeout | dev::kStatusEmpty)) {
-                    break;
-                }
-                unsigned char* st = ring + static_cast<size_t>(s) * kStage2;
-                ptx::mbar_arrive_expect_tx(&full[s], kStage2);
-#pragma unroll
-                for (int g = 0; g < 2; ++g) {
-                    load_word(st + g * kStageBytes, &tmap_ev, &tmap_ev8, &full[s], static_cast<int>(k * 64),
-                              seg0 + 32 * g, grouped, grow[g]);
-                }
-                ++issued;
-            }
-            const uint32_t first = issued > S ? issued - S : 0;
-            for (uint32_t k = first; k < issued; ++k) {
-                ptx::mbar_wait_bounded(&full[k % S], (k / S) & 1u, a.status,
-                                       dev::kStatusWaitTimeout | dev::kStatusDrain);
-            }
-        }
-    } else if (aligned && warp < W && slot < nconsumers) {
-        const bool tm = warp >= WS;
-        const uint32_t f = q0 + static_cast<uint32_t>(slot);
-        // shared-memory sums: float4 [nbins + 1][32 lanes] (slot nbins absorbs
-        // the store before the first run); TMEM sums: this warp's quadrant,
-        // column block (warp - WS) / 4 of 4 nbins columns.
-        float4* A = accs + static_cast<size_t>(tm ? 0 : warp) * (a.nbins + 1) * kWarp + lane;
-        const uint32_t T = tbase + ((static_cast<uint32_t>(warp & 3) * 32u) << 16) +
-                           static_cast<uint32_t>((warp - WS) / 4) * 4u * a.nbins;
-        if (tm) {
-            for (uint32_t b = 0; b < a.nbins; ++b) {
-                ptx::tmem_st4(T + 4 * b, 0.0f, 0.0f, 0.0f, 0.0f);
-            }
-            ptx::tmem_wait_st();
-        } else {
-            for (uint32_t b = 0; b <= a.nbins; ++b) {
-                A[b * kWarp] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            }
-        }
-        const uint32_t* M = a.masks + static_cast<size_t>(f) * a.nwords;
-        const BinT* B = static_cast<const BinT*>(a.bins) + a.bin_off[f];
-        const uint64_t nr = a.nruns[f];
-        const uint32_t lrow = static_cast<uint32_t>(lane) * 128u;
-        const uint32_t lsw = static_cast<uint32_t>(lane) & 7u;
-
-        auto consume = [&](auto seq_tag, auto tm_tag) -> bool {
-            constexpr bool SEQ = decltype(seq_tag)::value;
-            constexpr bool TM = decltype(tm_tag)::value;
-            uint32_t bin;
-            float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            float4 nacc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            uint64_t r = 0;
-            uint64_t rbase = 0;
-            uint32_t binbuf = 0;
-            if constexpr (SEQ) {
-                const uint32_t b0 = static_cast<uint32_t>(__ldg(B));
-                bin = b0 == 0 ? a.nbins - 1 : b0 - 1;
-            } else {
-                bin = a.nbins;
-                binbuf = load_bins(B, nr, 0, lane);
-            }
-            uint32_t maskbuf = __ldg(M + min(static_cast<uint32_t>(lane), a.nwords - 1));
-            const bool small = a.nbins < 64;
-
-            auto start_run = [&](uint32_t& rl) {
-                if constexpr (TM) {
-                    if (SEQ || bin != a.nbins) {
-                        ptx::tmem_st4(T + 4 * bin, acc.x, acc.y, acc.z, acc.w);
-                    }
-                } else {
-                    A[bin * kWarp] = acc;
-                }
-                if constexpr (SEQ) {
-                    bin = bin + 1 == a.nbins ? 0u : bin + 1;
-                    if constexpr (TM) {
-                        ptx::tmem_wait_ld_f4(nacc);
-                    }
-                    acc = nacc;
-                    const uint32_t nb = bin + 1 == a.nbins ? 0u : bin + 1;
-                    if constexpr (TM) {
-                        if (small) {
-                            ptx::tmem_wait_st();
-                        }
-                        ptx::tmem_ld4(T + 4 * nb, nacc.x, nacc.y, nacc.z, nacc.w);
-                    } else {
-                        nacc = A[nb * kWarp];
-                    }
-                    ++rl;
-                } else {
-                    bin = __shfl_sync(0xffffffffu, binbuf, static_cast<int>(rl));
-                    ++rl;
-                    if constexpr (TM) {
-                        ptx::tmem_wait_st();
-                        ptx::tmem_ld4(T + 4 * bin, acc.x, acc.y, acc.z, acc.w);
-                        ptx::tmem_wait_ld_f4(acc);
-                    } else {
-                        acc = A[bin * kWarp];
-                    }
-                }
-            };
-
-            uint32_t phase = 0;
-            uint32_t s = 0;
-            for (uint32_t c = 0; c < a.nwords; ++c) {
-                if ((c & 31u) == 0 && c > 0) {
-                    maskbuf = __ldg(M + min(c + static_cast<uint32_t>(lane), a.nwords - 1));
-                }
-                const uint32_t m = __shfl_sync(0xffffffffu, maskbuf, static_cast<int>(c & 31u));
-                if constexpr (!SEQ) {
-                    if (r + static_cast<uint64_t>(__popc(m)) > rbase + 32) {
-                        rbase = r;
-                        binbuf = load_bins(B, nr, rbase, lane);
-                    }
-                }
-                const bool got = ptx::mbar_wait_bounded(
-                    &full[s], phase, a.status,
-                    dev::kStatusWaitTimeout | (c == 0 ? dev::kStatusFirstFull : dev::kStatusFull));
-                if (!__all_sync(0xffffffffu, got)) {
-                    return false;
-                }
-                if constexpr (TM) {
-                    ptx::tmem_wait_st();
-                }
-                const unsigned char* t0 = ring + static_cast<size_t>(s) * kStage2 + lrow;
-                uint32_t rl = static_cast<uint32_t>(r - rbase);
-#pragma unroll
-                for (uint32_t h = 0; h < 2; ++h) {
-                    float2 x0[16], x1[16];
-#pragma unroll
-                    for (uint32_t j = 0; j < 8; ++j) {
-                        const uint32_t o = (j ^ lsw) << 4;
-                        const float4 v0 = *reinterpret_cast<const float4*>(t0 + h * kTileBytes + o);
-                        const float4 v1 =
-                            *reinterpret_cast<const float4*>(t0 + kStageBytes + h * kTileBytes + o);
-                        x0[2 * j] = make_float2(v0.x, v0.y);
-                        x0[2 * j + 1] = make_float2(v0.z, v0.w);
-                        x1[2 * j] = make_float2(v1.x, v1.y);
-                        x1[2 * j + 1] = make_float2(v1.z, v1.w);
-                    }
-                    if (h == 1) {
-                        ptx::mbar_arrive(&empty[s]);
-                    }
-                    const uint32_t mh = m >> (16 * h);
-#pragma unroll
-                    for (int g = 0; g < 4; ++g) {
-                        if (((mh >> (4 * g)) & 0xfu) == 0) {
-#pragma unroll
-                            for (int i = 4 * g; i < 4 * g + 4; ++i) {
-                                acc = add4_rn(acc, x0[i], x1[i]);
-                            }
-                        } else {
-#pragma unroll
-                            for (int i = 4 * g; i < 4 * g + 4; ++i) {
-                                if (mh & (1u << i)) {
-                                    start_run(rl);
-                                }
-                                acc = add4_rn(acc, x0[i], x1[i]);
-                            }
-                        }
-                    }
-                }
-                s = (s + 1 == S) ? 0 : s + 1;
-                if (s == 0) {
-                    phase ^= 1u;
-                }
-                r = rbase + rl;
-            }
-            if constexpr (TM) {
-                if (SEQ || bin != a.nbins) {
-                    ptx::tmem_st4(T + 4 * bin, acc.x, acc.y, acc.z, acc.w);
-                }
-                ptx::tmem_wait_ld_f4(nacc);
-                ptx::tmem_wait_st();
-            } else {
-                A[bin * kWarp] = acc;
-            }
-            if (r != nr) {
-                atomicOr(a.status, dev::kStatusBadTable);
-            }
-            return true;
-        };
-        bool ok;
-        if (tm) {
-            ok = a.seq[f] != 0 ? consume(std::true_type{}, std::true_type{})
-                               : consume(std::false_type{}, std::true_type{});
-        } else {
-            ok = a.seq[f] != 0 ? consume(std::true_type{}, std::false_type{})
-                               : consume(std::false_type{}, std::false_type{});
-        }
-        // lane l holds segments l (group 0) and 32 + l (group 1)
-        bool store0, store1;
-        uint32_t sg0, sg1;
-        if (grouped) {
-            const uint32_t ng = *a.ngroups;
-            const uint32_t ga = blockIdx.x * 8u + static_cast<uint32_t>(lane / 8);
-            const uint32_t gb = ga + 4;
-            store0 = ga < ng;
-            store1 = gb < ng;
-            sg0 = a.groups[store0 ? ga : blockIdx.x * 8u] + static_cast<uint32_t>(lane % 8);
-            sg1 = a.groups[store1 ? gb : blockIdx.x * 8u] + static_cast<uint32_t>(lane % 8);
-        } else {
-            sg0 = static_cast<uint32_t>(seg0 + lane);
-            sg1 = sg0 + 32;
-            store0 = sg0 < a.nseg;
-            store1 = sg1 < a.nseg;
-        }
-        float* out0 = a.fold + (static_cast<size_t>(sg0) * a.nfreq + f) * 2 * a.nbins;
-        float* out1 = a.fold + (static_cast<size_t>(sg1) * a.nfreq + f) * 2 * a.nbins;
-        if (ok) {
-            for (uint32_t b = 0; b < a.nbins; b += 4) {
-                float4 p[4];
-                if (tm) {
-                    // every lane reads (warp-collective); lanes past nseg do not store
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        ptx::tmem_ld4(T + 4 * (b + k), p[k].x, p[k].y, p[k].z, p[k].w);
-                    }
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        ptx::tmem_wait_ld_f4(p[k]);
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        p[k] = A[(b + k) * kWarp];
-                    }
-                }
-                if (store0) {
-                    reinterpret_cast<float4*>(out0)[b / 4] = make_float4(p[0].x, p[1].x, p[2].x, p[3].x);
-                    reinterpret_cast<float4*>(out0 + a.nbins)[b / 4] = make_float4(p[0].y, p[1].y, p[2].y, p[3].y);
-                }
-                if (store1) {
-                    reinterpret_cast<float4*>(out1)[b / 4] = make_float4(p[0].z, p[1].z, p[2].z, p[3].z);
-                    reinterpret_cast<float4*>(out1 + a.nbins)[b / 4] = make_float4(p[0].w, p[1].w, p[2].w, p[3].w);
-                }
-            }
-        }
-    }
-    ptx::tmem_fence_before_sync();
-    __syncthreads();
-    if (warp == W) {
-        ptx::tmem_fence_after_sync();
-        ptx::tmem_dealloc(tbase, kTmemCols);
-    }
-}
-
 // Valid segments of series i, in whole groups of 8: the segments that hold
 // any of its lens[i] samples, rounded up to 8 (at most nseg).
 __device__ __forceinline__ uint32_t valid_segments8(uint64_t len, uint32_t nseg, uint64_t seglen) {
@@ -1512,55 +1187,20 @@ BruteFoldDevice::BruteFoldDevice(const std::vector<double>& freqs, uint64_t segm
 // fit, the larger W on a tie -- the kernel is latency-bound per warp, so
 // block time hardly depends on W) and the depth of the shared-memory ring.
 // Returns false (and changes nothing) when the shape does not fit.
-uint32_t BruteFoldDevice::max_tmem_warps(uint32_t smem_warps, uint32_t groups) const {
-    // packed form, nbins a multiple of 4 up to 256 / groups, 2 * groups *
-    // nbins columns per warp, four warps (one per TMEM lane quadrant) per
-    // column block, block <= 24 (two groups: 15) consumer warps
-    const uint32_t wcap = static_cast<uint32_t>(groups == 2 ? kMaxWarpsTm2 : kMaxWarpsTm);
-    if (m_nbins * groups > 256 || m_nbins % 4 != 0 || smem_warps + 1 >= wcap) {
+uint32_t BruteFoldDevice::max_tmem_warps(uint32_t smem_warps) const {
+    // packed form, nbins a multiple of 4 up to 256, 2 * nbins columns per
+    // warp, four warps (one per TMEM lane quadrant) per column block, block
+    // <= 24 consumer warps
+    if (m_nbins > 256 || m_nbins % 4 != 0 || smem_warps + 1 >= static_cast<uint32_t>(kMaxWarpsTm)) {
         return 0;
     }
-    const uint32_t blocks = kTmemCols / static_cast<uint32_t>(2 * groups * m_nbins);
-    return std::min<uint32_t>(4 * blocks, wcap - 1 - smem_warps);
+    const uint32_t blocks = kTmemCols / static_cast<uint32_t>(2 * m_nbins);
+    return std::min<uint32_t>(4 * blocks, static_cast<uint32_t>(kMaxWarpsTm) - 1 - smem_warps);
 }
 
-uint32_t BruteFoldDevice::max_warps2(uint32_t stages) const {
-    // ring of 16 KiB stages, barriers in 1 KiB, float4 [nbins + 1][32] per warp
-    const size_t ring = stages * 2 * kStageBytes + 1024;
-    const size_t per_warp = (m_nbins + 1) * kWarp * sizeof(float4);
-    if (m_nbins % 4 != 0 || m_nbins > 128 || ring + per_warp > kSmemLimit) {
-        return 0;
-    }
-    return static_cast<uint32_t>(
-        std::min<size_t>((kSmemLimit - ring) / per_warp, static_cast<size_t>(kMaxWarpsTm2) - 1));
-}
-
-bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages, uint32_t tmem,
-                                uint32_t groups) {
-    if ((rows != 1 && rows != 2) || stages < 2 || stages > kMaxStages || (groups != 1 && groups != 2)) {
+bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages, uint32_t tmem) {
+    if ((rows != 1 && rows != 2) || stages < 2 || stages > kMaxStages) {
         return false;
-    }
-    if (groups == 2) {
-        // two 32-segment groups per warp: packed TMEM kernel (tmem may be 0)
-        if (rows != 2 || warps <= tmem || warps - tmem > max_warps2(stages) ||
-            tmem > max_tmem_warps(warps - tmem, 2) || warps + 1 > static_cast<uint32_t>(kMaxWarpsTm2)) {
-            return false;
-        }
-        const size_t smem = stages * 2 * kStageBytes + 1024 +
-                            static_cast<size_t>(warps - tmem) * (m_nbins + 1) * kWarp * sizeof(float4);
-        if (smem > kSmemLimit || (m_nfreq + warps - 1) / warps > 65535) {
-            return false;
-        }
-        m_rows = 2;
-        m_warps = warps;
-        m_stages = stages;
-        m_tmem = tmem;
-        m_groups_per_warp = 2;
-        // one block per SM (each block allocates all 512 TMEM columns)
-        m_smem = std::max<size_t>(smem, 116 * 1024);
-        m_map_e_ptr = nullptr;
-        m_map_ev_ptr = nullptr;
-        return true;
     }
     const size_t ring = stages * kStageBytes + 2 * stages * sizeof(uint64_t);
     const size_t per_warp = rows * (m_nbins + 1) * kWarp * sizeof(float);
@@ -1577,7 +1217,6 @@ bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages, 
         m_warps = warps;
         m_stages = stages;
         m_tmem = tmem;
-        m_groups_per_warp = 1;
         // at least half the SM's shared memory: one block per SM, so a
         // second block never waits for the first one's tensor memory
         m_smem = std::max<size_t>(smem, 116 * 1024);
@@ -1614,7 +1253,6 @@ bool BruteFoldDevice::configure(uint32_t rows, uint32_t warps, uint32_t stages, 
     m_warps = w;
     m_stages = stages;
     m_tmem = 0;
-    m_groups_per_warp = 1;
     m_smem = ring + w * per_warp;
     m_map_e_ptr = nullptr;  // the input binding depends on the rows
     m_map_ev_ptr = nullptr;
@@ -1715,8 +1353,6 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s, const uint64_t* d_lens
     // Group mode: only the segments that hold samples are folded (in groups
     // of 8); the grid keeps its full size so that a captured graph stays
     // valid for any lengths, and blocks past the groups return at once.
-    const uint32_t G = m_groups_per_warp;  // 32-segment groups per consumer warp
-    grid.x = static_cast<unsigned>((nseg + G * kWarp - 1) / (G * kWarp));
     const bool grouped = d_lens != nullptr && m_rows == 2 && m_nseg % 8 == 0;
     if (grouped) {
         const uint64_t ngmax = nseg / 8;
@@ -1730,7 +1366,7 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s, const uint64_t* d_lens
         LK_CUDA(cudaGetLastError());
         a.ngroups = tab;
         a.groups = tab + 1 + m_map_batch;
-        grid.x = static_cast<unsigned>((ngmax + 4 * G - 1) / (4 * G));
+        grid.x = static_cast<unsigned>((ngmax + 3) / 4);
     }
     auto launch = [&](auto kern) {
         LK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1742,13 +1378,7 @@ void BruteFoldDevice::fold(float* d_fold, cudaStream_t s, const uint64_t* d_lens
                                      static_cast<int>(m_smem)));
         kern<<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, m_tmap_ev8, a);
     };
-    if (G == 2) {
-        LK_CUDA(cudaFuncSetAttribute(brute_fold_pk_tm2_kernel<uint8_t>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(m_smem)));
-        brute_fold_pk_tm2_kernel<uint8_t>
-            <<<grid, (m_warps + 1) * kWarp, m_smem, s>>>(m_tmap_ev, m_tmap_ev8, a);
-    } else if (m_rows == 2 && m_tmem > 0) {
+    if (m_rows == 2 && m_tmem > 0) {
         LK_CUDA(cudaFuncSetAttribute(brute_fold_pk_tm_kernel<uint8_t>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(m_smem)));

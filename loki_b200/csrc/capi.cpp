@@ -492,7 +492,6 @@ int lk_ffa_get_tuning(const lk_ffa* ffa, lk_tuning* out) {
         t.bf_warps = ffa->exec->bf->warps();
         t.bf_stages = ffa->exec->bf->stages();
         t.bf_tmem_warps = ffa->exec->bf->tmem_warps();
-        t.bf_seg_groups = ffa->exec->bf->seg_groups();
         t.merge_rows_in_flight = ffa->exec->merge_pb;
         t.score_cells_per_block = ffa->exec->score_cells;
         *out = t;

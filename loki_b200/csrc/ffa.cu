@@ -337,11 +337,9 @@ void FFAExec::apply_tuning(const lk_tuning& t) {
     DeviceGuard g(device);
     require(t.merge_rows_in_flight >= 0 && t.merge_rows_in_flight <= 16,
             "merge rows in flight must lie in [0, 16]");
-    if (t.bf_rows != 0 || t.bf_warps != 0 || t.bf_stages != 0 || t.bf_tmem_warps != 0 ||
-        t.bf_seg_groups > 1) {
+    if (t.bf_rows != 0 || t.bf_warps != 0 || t.bf_stages != 0 || t.bf_tmem_warps != 0) {
         require(bf->configure(t.bf_rows != 0 ? t.bf_rows : bf->rows(), t.bf_warps,
-                              t.bf_stages != 0 ? t.bf_stages : bf->stages(), t.bf_tmem_warps,
-                              t.bf_seg_groups > 1 ? 2u : 1u),
+                              t.bf_stages != 0 ? t.bf_stages : bf->stages(), t.bf_tmem_warps),
                 "brute-fold launch shape does not fit this plan");
     }
     merge_pb = t.merge_rows_in_flight;
@@ -351,7 +349,6 @@ void FFAExec::apply_tuning(const lk_tuning& t) {
     tuning.bf_warps = bf->warps();
     tuning.bf_stages = bf->stages();
     tuning.bf_tmem_warps = bf->tmem_warps();
-    tuning.bf_seg_groups = bf->seg_groups();
 }
 
 lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
@@ -463,34 +460,7 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
                 }
             }
         }
-        // 1c. two 32-segment groups per consumer warp (packed, TMEM kernel):
-        // the frequency's run handling shared by two add chains
-        uint32_t bg = 1;
-        if (pw > 0) {
-            for (uint32_t stages = 2; stages <= 3; ++stages) {
-                const uint32_t wmax2 = bf->max_warps2(stages);
-                for (uint32_t ws = wmax2; ws + 3 >= wmax2 && ws >= 1; --ws) {
-                    for (uint32_t t = 0; t <= 16; t += 4) {
-                        if (t > bf->max_tmem_warps(ws, 2) || !bf->configure(2, ws + t, stages, t, 2)) {
-                            continue;
-                        }
-                        const float ms = time_stages({LK_STAGE_INTERLEAVE, LK_STAGE_BRUTE_FOLD});
-                        if (ms < bf_best) {
-                            bf_best = ms;
-                            bt = t;
-                            br = 2;
-                            bw = ws;
-                            bs = stages;
-                            bg = 2;
-                        }
-                    }
-                    if (ws == 1) {
-                        break;
-                    }
-                }
-            }
-        }
-        require(bf->configure(br, bw + bt, bs, bt, bg), "autotune: lost the brute-fold shape");
+        require(bf->configure(br, bw + bt, bs, bt), "autotune: lost the brute-fold shape");
         // 2. merges
         const uint32_t nb = static_cast<uint32_t>(plan.cfg.nbins);
         std::vector<int> pbs{0};
@@ -546,7 +516,6 @@ lk_tuning FFAExec::autotune(const float* ts_e, const float* ts_v, uint32_t reps,
         best.bf_warps = bf->warps();
         best.bf_stages = bs;
         best.bf_tmem_warps = bt;
-        best.bf_seg_groups = bg;
         best.merge_rows_in_flight = bpb;
         best.score_cells_per_block = bcells;
         best.candidates = tried;

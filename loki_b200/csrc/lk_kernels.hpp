@@ -69,16 +69,10 @@ public:
     // Launch shape (see brute_fold.cu); false when it does not fit. tmem:
     // consumer warps (of `warps`) whose sums live in tensor memory (packed
     // form only).
-    // groups: 32-segment groups per consumer warp (2: packed TMEM kernel with
-    // two add chains per warp; rows must be 2).
-    bool configure(uint32_t rows, uint32_t warps, uint32_t stages, uint32_t tmem = 0,
-                   uint32_t groups = 1);
+    bool configure(uint32_t rows, uint32_t warps, uint32_t stages, uint32_t tmem = 0);
     uint32_t max_warps(uint32_t rows, uint32_t stages) const;
-    // Most shared-memory consumer warps of the two-group kernel.
-    uint32_t max_warps2(uint32_t stages) const;
     // Most tensor-memory warps a block of smem_warps shared-memory warps can add.
-    uint32_t max_tmem_warps(uint32_t smem_warps, uint32_t groups = 1) const;
-    uint32_t seg_groups() const { return m_groups_per_warp; }
+    uint32_t max_tmem_warps(uint32_t smem_warps) const;
     uint32_t rows() const { return m_rows; }
     uint32_t warps() const { return m_warps; }
     uint32_t stages() const { return m_stages; }
@@ -102,7 +96,6 @@ private:
     uint32_t m_warps = 0;      // consumer warps per block
     uint32_t m_stages = 0;     // shared-memory ring depth (32-sample words)
     uint32_t m_tmem = 0;       // consumer warps with tensor-memory sums
-    uint32_t m_groups_per_warp = 1;  // 32-segment groups per consumer warp
     size_t m_smem = 0;         // dynamic shared memory per block
     uint32_t* m_status;
     DeviceBuffer m_masks;      // uint32 [nfreq][ceil(seglen / 32)] run-start bits

@@ -133,22 +133,6 @@ __device__ __forceinline__ void tmem_wait_ld4(float4& a, float4& b) {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
                  : "+f"(a.x), "+f"(a.y), "+f"(a.z), "+f"(a.w), "+f"(b.x), "+f"(b.y), "+f"(b.z), "+f"(b.w)::"memory");
 }
-// Four columns (32x32b.x4): a store, an asynchronous read, and the wait that
-// ties the four read registers.
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, float a, float b, float c, float d) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "f"(a),
-                 "f"(b), "f"(c), "f"(d)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float& a, float& b, float& c, float& d) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                 : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
-                 : "r"(taddr)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_wait_ld_f4(float4& a) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+f"(a.x), "+f"(a.y), "+f"(a.z), "+f"(a.w)::"memory");
-}
 __device__ __forceinline__ void tmem_wait_st() {
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }

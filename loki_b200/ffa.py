@@ -248,7 +248,7 @@ class FFACUDA:
         return st.value
 
     _TUNING_FIELDS = ("bf_rows", "bf_warps", "bf_stages", "merge_rows_in_flight", "score_cells_per_block",
-                      "bf_tmem_warps", "bf_seg_groups")
+                      "bf_tmem_warps")
 
     def autotune(self, ts_e, ts_v, reps: int = 3) -> dict:
         """Time launch-shape candidates of the brute fold, the merges and the

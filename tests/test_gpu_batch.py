@@ -220,8 +220,6 @@ LEN_CASES = {
     "accel_nb32_tmem": (1 << 17, 1e-3, 32, ((-300.0, 300.0), (5.0, 8.0)), (2, 6, 8)),
     "freq_nb128_tmem": (1 << 18, 64e-6, 128, ((20.0, 40.0),), (2, 4, 8)),
     "freq_nb128_rows1": (1 << 18, 64e-6, 128, ((20.0, 40.0),), (1, 8, 0)),
-    "accel_nb32_two_groups": (1 << 17, 1e-3, 32, ((-300.0, 300.0), (5.0, 8.0)), (2, 6, 8, 2)),
-    "freq_nb128_two_groups": (1 << 18, 64e-6, 128, ((20.0, 40.0),), (2, 2, 4, 2)),
 }
 
 
@@ -237,10 +235,9 @@ def test_batch_lengths_skip_padding(cuda, name):
     plain = FFACUDA(cfg, max_batch=nb)
     skip = FFACUDA(cfg, max_batch=nb)
     if shape is not None:
-        rows, ws, tw = shape[:3]
+        rows, ws, tw = shape
         tu = skip.tuning
-        tu.update(bf_rows=rows, bf_warps=ws + tw, bf_tmem_warps=tw,
-                  bf_seg_groups=shape[3] if len(shape) > 3 else 1, bf_stages=3)
+        tu.update(bf_rows=rows, bf_warps=ws + tw, bf_tmem_warps=tw)
         skip.set_tuning(tu)
         plain.set_tuning(tu)
     es = np.zeros((nb, n), np.float32)

@@ -218,43 +218,6 @@ CASES_EXTRA = {
 }
 
 
-# Two 32-segment groups per consumer warp (bf_seg_groups = 2): two add chains
-# per warp sharing the run handling; (shared-memory warps, TMEM warps).
-TMEM2_CASES = {
-    "accel_nb64": (4, 8),
-    "accel_multi_nb32": (6, 8),
-    "freq_nb16": (2, 8),
-    "freq_nb64_nonseq": (3, 4),
-    "freq_nb128": (2, 4),
-    "freq_nb128_nonseq": (1, 4),
-    "accel_nb64_smem_only": (5, 0),
-}
-CASES_EXTRA["accel_nb64_smem_only"] = (2**20, 64e-6, 64, 2.0, [[-200.0, 200.0], [5.0, 50.0]], None)
-
-
-@pytest.mark.parametrize("name", sorted(TMEM2_CASES))
-def test_brute_fold_two_segment_groups_bit_exact(cuda, name):
-    from loki_b200.configs import PulsarSearchConfig
-    from loki_b200.ffa import FFACUDA
-
-    nsamps, tsamp, nbins, eta, lims, bseg = {**CASES, **CASES_EXTRA}[name]
-    w = [x for x in WIDTHS if x < nbins]
-    cfg = PulsarSearchConfig(nsamps, tsamp, nbins, eta, np.array(lims), use_fourier=False, bseg_brute=bseg,
-                             score_widths=w)
-    op = lko.plan_create(lko.make_cfg(nsamps, tsamp, nbins, eta, lims, bseg_brute=bseg))
-    ts_e, ts_v = series(nsamps, 29)
-    ffa = FFACUDA(cfg)
-    ws, tw = TMEM2_CASES[name]
-    t = ffa.tuning
-    t.update(bf_rows=2, bf_warps=ws + tw, bf_tmem_warps=tw, bf_seg_groups=2, bf_stages=3)
-    ffa.set_tuning(t)
-    assert ffa.tuning["bf_seg_groups"] == 2 and ffa.tuning["bf_tmem_warps"] == tw
-    want = lko.ffa(op, ts_e, ts_v)
-    got = ffa.execute(ts_e, ts_v)
-    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
-    assert ffa.status() == 0
-
-
 @pytest.mark.parametrize("name", sorted(TMEM_CASES))
 def test_brute_fold_tmem_warps_bit_exact(cuda, name):
     from loki_b200.configs import PulsarSearchConfig
