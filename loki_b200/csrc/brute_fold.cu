@@ -40,7 +40,10 @@
 // by one at every run (every frequency below 1 / (tsamp nbins)) take a path
 // without the bin table, with the next run's sums loaded a run ahead (1.82
 // ms); dispatching each four-sample group through a 16-way switch instead of
-// per-sample run-start tests measured slower (2.46 ms).
+// per-sample run-start tests measured slower (2.46 ms). With tensor-memory
+// sums (below; 1.58 ms), two 32-segment groups per warp sharing one
+// frequency's run handling (two add chains per warp, float4 sums, at most 13
+// warps) measured slower as well: 2.41 ms at best.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
