@@ -201,8 +201,8 @@ class EPMultiPassCUDA:
     growing after the first execute). No more workers run than there are
     reference segments to prune, and each worker's executor (device buffers
     sized for ``max_sugg`` leaves) is created when the worker first runs.
-    Eight segments of the jerk search: one worker 29.2 ms, four 15.6 ms,
-    eight 11.4 ms."""
+    Eight segments of the jerk search (FFA included): one worker 19.1 ms,
+    eight 10.0 ms."""
 
     def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
                  max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
