@@ -533,6 +533,17 @@ int lk_prune_run(lk_prune* pr, const float* d_ffa_fold, uint64_t ref_seg,
  * LOKI_B200_PRUNE_TAIL=0 in the environment makes 0 the default) or level by
  * level with host round trips (0). Results are identical. */
 int lk_prune_set_tail(lk_prune* pr, int enable);
+/* n pruning runs at once on one stream, one executor each (created from one
+ * plan with the same sizes; distinct handles): run k seeds from ref_segs[k]
+ * and its results are those lk_prune_run gives it. Each run's large levels
+ * run level by level; then the small trees' tails of all runs share ONE
+ * cooperative launch (its blocks split between the runs); then whatever a
+ * tail handed back. stats: [n][max_stats] rows, n_stats[k] rows of run k. The
+ * reference runs its segments on a thread pool (lib/prune.cpp:839-926). */
+int lk_prune_run_many(lk_prune* const* prs, uint64_t n, const float* d_ffa_fold,
+                      const uint64_t* ref_segs, const float* thresholds, uint64_t n_thresholds,
+                      uint64_t n_iters, lk_prune_stats* stats, uint64_t max_stats, uint64_t* n_stats,
+                      lk_stream_t stream);
 /* core::generate_bp_poly_taylor (lib/taylor.cpp:1643-1741), the
  * FFAPlan::get_branching_pattern("taylor", ref_seg) of the reference: the
  * average branching factor of each of the nsegments - 1 pruning levels. */

@@ -209,6 +209,7 @@ SIGNATURES = [
     ("lk_prune_destroy", None, [vp]),
     ("lk_plan_branching_pattern", i32, [vp, u64, i32, vp, u64, vp]),
     ("lk_prune_set_tail", i32, [vp, i32]),
+    ("lk_prune_run_many", i32, [vp, u64, vp, vp, vp, u64, u64, vp, u64, vp, vp]),
     ("lk_prune_run", i32, [vp, vp, u64, vp, u64, u64, vp, u64, vp, vp]),
     ("lk_prune_finalize", i32, [vp, vp, vp]),
     ("lk_prune_get_scores_ep", i32, [vp, vp, u64, vp]),

@@ -1058,6 +1058,37 @@ int lk_plan_branching_pattern(const lk_plan* plan, uint64_t ref_seg, int conserv
     });
 }
 
+int lk_prune_run_many(lk_prune* const* prs, uint64_t n, const float* d_ffa_fold,
+                      const uint64_t* ref_segs, const float* thresholds, uint64_t n_thresholds,
+                      uint64_t n_iters, lk_prune_stats* stats, uint64_t max_stats, uint64_t* n_stats,
+                      lk_stream_t stream) {
+    return guarded([&] {
+        need(prs, "prs");
+        need(ref_segs, "ref_segs");
+        need(d_ffa_fold, "d_ffa_fold");
+        need(n_stats, "n_stats");
+        lk::require(n >= 1, "n must be positive");
+        if (n_thresholds > 0) {
+            need(thresholds, "thresholds");
+        }
+        if (max_stats > 0) {
+            need(stats, "stats");
+        }
+        std::vector<lk::PruneExec*> ex(n);
+        for (uint64_t k = 0; k < n; ++k) {
+            need(prs[k], "prs[k]");
+            ex[k] = prs[k]->exec.get();
+        }
+        const auto out = lk::PruneExec::run_many(ex, d_ffa_fold, std::vector<uint64_t>(ref_segs, ref_segs + n),
+                                                 thresholds, n_thresholds, n_iters,
+                                                 reinterpret_cast<cudaStream_t>(stream));
+        for (uint64_t k = 0; k < n; ++k) {
+            n_stats[k] = out[k].size();
+            std::copy_n(out[k].begin(), std::min<uint64_t>(out[k].size(), max_stats), stats + k * max_stats);
+        }
+    });
+}
+
 int lk_prune_set_tail(lk_prune* pr, int enable) {
     return guarded([&] {
         need(pr, "pr");

@@ -40,6 +40,20 @@ struct TreeState {
     uint64_t space_left() const { return cap - ((size_old - read_consumed) + size); }
 };
 
+// Where a pruning run stands between its steps (see PruneExec::run).
+struct PruneRunState {
+    std::vector<uint64_t> order;   // middle-out segment order
+    const float* fold = nullptr;   // device FFA fold of the last level
+    const float* thresholds = nullptr;
+    uint64_t n_thresholds = 0;
+    uint64_t levels = 0;           // last level to run
+    uint64_t lv = 1;               // next level to run
+    bool handed_back = false;      // the tail gave level lv back
+    bool at_tail = false;          // stopped where the tail would start
+    bool done = false;
+    std::vector<lk_prune_stats> stats;
+};
+
 // One pruning run over the final FFA level of a plan (EPMultiPass's per
 // ref_seg PruneImpl, lib/prune.cpp:40-226,429-620).
 class PruneExec {
@@ -54,6 +68,14 @@ public:
     std::vector<lk_prune_stats> run(const float* d_ffa_fold, uint64_t ref_seg,
                                     const float* thresholds, uint64_t n_thresholds,
                                     uint64_t n_iters, cudaStream_t s);
+    // Several runs (one executor each, same plan and sizes) on one stream:
+    // each run's large levels level by level, then the small trees' tails of
+    // all runs in ONE cooperative launch (its blocks split between the
+    // trees), then whatever a tail handed back. Results are each run's.
+    static std::vector<std::vector<lk_prune_stats>> run_many(
+        const std::vector<PruneExec*>& ex, const float* d_ffa_fold,
+        const std::vector<uint64_t>& ref_segs, const float* thresholds, uint64_t n_thresholds,
+        uint64_t n_iters, cudaStream_t s);
     // The end of PruneImpl::run (lib/prune.cpp:136-139): the survivors
     // ascended to the middle of the data (folds over every segment searched,
     // scores of those folds; the run's scores kept as scores_ep) and their
@@ -69,12 +91,17 @@ public:
 
 private:
     void ensure_level_buffers(uint64_t n_parents, uint64_t n_children);
-    // Runs levels first .. last in one cooperative launch while the tree is
-    // small (see prune.cu); appends their stats rows and returns the next
-    // level to run (the host's, when the tail handed a large level back).
-    uint64_t run_tail(const float* d_ffa_fold, const std::vector<uint64_t>& order, uint64_t first,
-                      uint64_t last, const float* thresholds, std::vector<lk_prune_stats>* stats,
-                      cudaStream_t s);
+    void run_begin(PruneRunState& rs, const float* d_ffa_fold, uint64_t ref_seg,
+                   const float* thresholds, uint64_t n_thresholds, uint64_t n_iters, cudaStream_t s);
+    // Levels from rs.lv on; with stop_at_tail, returns where the tail would
+    // start (rs.at_tail) instead of launching it.
+    void run_levels(PruneRunState& rs, bool stop_at_tail, cudaStream_t s);
+    std::vector<lk_prune_stats> run_end(PruneRunState& rs, cudaStream_t s);
+    // The tail (see prune.cu): prepare uploads this run's level constants and
+    // state and fills the host TailArgs at args; finish reads the state back
+    // (after the launch has been synchronised) and continues rs.
+    void tail_prepare(PruneRunState& rs, void* args, cudaStream_t s);
+    void tail_finish(PruneRunState& rs, cudaStream_t s);
     void level(const float* d_seg, const std::vector<uint64_t>& order, uint64_t level,
                float threshold, lk_prune_stats* st, cudaStream_t s);
     void compact_children(uint64_t c_begin, uint64_t c_end, uint32_t* out_ids, float* out_sc,
@@ -113,7 +140,7 @@ public:
     // The persistent tail (on by default; LOKI_B200_PRUNE_TAIL=0 turns it off).
     bool tail_enabled = true;
 private:
-    DeviceBuffer m_tail_ctl, m_tail_levels, m_tail_stats, m_tail_tp;
+    DeviceBuffer m_tail_ctl, m_tail_levels, m_tail_stats, m_tail_tp, m_tail_args;
 };
 
 // Single steps (the Taylor PruneDPFuncts interface, include/loki/core/

@@ -1201,9 +1201,10 @@ struct TailArgs {
     ScoreParams sp;
 };
 
-// Grid barrier of a cooperative launch (all blocks resident), bounded like
-// every device wait here: false (and the status bit set) when it gave up.
-__device__ bool tail_barrier(TailCtl* ctl) {
+// Barrier of one tree's nblocks blocks in a cooperative launch (all blocks
+// resident), bounded like every device wait here: false (and the status bit
+// set) when it gave up.
+__device__ bool tail_barrier(TailCtl* ctl, uint32_t nblocks) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1211,7 +1212,7 @@ __device__ bool tail_barrier(TailCtl* ctl) {
         volatile uint32_t* gen = &ctl->bar_gen;
         const uint32_t g0 = *gen;
         __threadfence();
-        if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
+        if (atomicAdd(&ctl->bar_count, 1u) == nblocks - 1) {
             atomicExch(&ctl->bar_count, 0u);
             __threadfence();
             atomicAdd(&ctl->bar_gen, 1u);
@@ -1265,8 +1266,11 @@ __device__ uint64_t block_append(uint64_t n, Keep keep, Id id, Score score, uint
 }
 
 template <int NW, int NB>
-__global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
+__global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restrict__ trees, uint32_t bpt) {
     extern __shared__ float rows[];
+    // blocks [t * bpt, (t + 1) * bpt) run tree t; lb is the block's index there
+    const uint32_t lb = blockIdx.x % bpt;
+    const TailArgs& a = trees[blockIdx.x / bpt];
     TailCtl* ctl = a.ctl;
     // values other blocks wrote before a barrier are read through vc
     volatile TailCtl* vc = a.ctl;
@@ -1275,7 +1279,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
     const uint64_t cap = a.cap;
     for (;;) {
         // 0. the level's set-up (block 0, thread 0): batches as get_leaves_span
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (lb == 0 && threadIdx.x == 0) {
             const uint32_t lv = ctl->level;
             const uint64_t n_par = ctl->size;
             if (lv > a.last_level || n_par == 0) {
@@ -1309,7 +1313,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
                 }
             }
         }
-        if (!tail_barrier(ctl) || vc->exit != kTailExitNone) {
+        if (!tail_barrier(ctl, bpt) || vc->exit != kTailExitNone) {
             return;
         }
         const uint32_t lv = vc->level;
@@ -1317,8 +1321,8 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
         const uint64_t n_par = vc->n_par, head = vc->head;
         const int cur = static_cast<int>(vc->cur);
         const double* tree = a.tleaves[cur];
-        const uint64_t gtid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-        const uint64_t gthreads = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+        const uint64_t gtid = static_cast<uint64_t>(lb) * blockDim.x + threadIdx.x;
+        const uint64_t gthreads = static_cast<uint64_t>(bpt) * blockDim.x;
 
         // 1. branch counts (Chebyshev: parents re-centred into tp, the tree
         //    is not written, so a hand-back leaves it as it was)
@@ -1345,11 +1349,11 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
             }
             a.counts[i] = static_cast<uint32_t>(prod);
         }
-        if (!tail_barrier(ctl)) {
+        if (!tail_barrier(ctl, bpt)) {
             return;
         }
         // 2. offsets, batch child ranges, checks (block 0)
-        if (blockIdx.x == 0) {
+        if (lb == 0) {
             __shared__ uint32_t ws[32];
             const uint64_t per = (n_par + blockDim.x - 1) / blockDim.x;
             const uint64_t i0 = threadIdx.x * per, i1 = min(n_par, i0 + per);
@@ -1399,7 +1403,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
                 }
             }
         }
-        if (!tail_barrier(ctl) || vc->exit != kTailExitNone) {
+        if (!tail_barrier(ctl, bpt) || vc->exit != kTailExitNone) {
             return;
         }
         const uint64_t n_child = vc->n_child;
@@ -1433,22 +1437,22 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
                 }
             }
         }
-        if (!tail_barrier(ctl)) {
+        if (!tail_barrier(ctl, bpt)) {
             return;
         }
         // 4. resolve, shift-add, score, kept folds (tiles of blockDim children)
-        for (uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x; c0 < n_child;
-             c0 += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        for (uint64_t c0 = static_cast<uint64_t>(lb) * blockDim.x; c0 < n_child;
+             c0 += static_cast<uint64_t>(bpt) * blockDim.x) {
             leaf_tile<NW, NB>(rows, c0, a.cleaves, a.cparent, n_child, a.tfolds[cur], head, cap, L.seg,
                               g, L.rc, a.rs, a.sp, L.threshold, a.cscores, a.cfolds,
                               a.level_mm + 2 * lv);
             __syncthreads();
         }
-        if (!tail_barrier(ctl)) {
+        if (!tail_barrier(ctl, bpt)) {
             return;
         }
         // 5. filter + add in the reference's batch order (block 0)
-        if (blockIdx.x == 0) {
+        if (lb == 0) {
             const uint32_t nbat = vc->nbat;
             uint64_t size = 0, read_consumed = 0;
             int li = 0;
@@ -1500,7 +1504,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
                 ctl->thr = thr;
             }
         }
-        if (!tail_barrier(ctl)) {
+        if (!tail_barrier(ctl, bpt)) {
             return;
         }
         // 6. survivors transformed and gathered into the other tree buffer
@@ -1515,11 +1519,11 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
                            nb, L.tc, a.tleaves[nxt], a.tfolds[nxt], a.tscores[nxt]);
             }
         }
-        if (!tail_barrier(ctl)) {
+        if (!tail_barrier(ctl, bpt)) {
             return;
         }
         // 7. the level's end (finalize_in_place_update) and its statistics
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (lb == 0 && threadIdx.x == 0) {
             const uint64_t size = ctl->size;
             a.stats[3 * lv] = n_par;
             a.stats[3 * lv + 1] = n_child;
@@ -1532,6 +1536,53 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(TailArgs a) {
         }
         // the next level's set-up waits at its first barrier
     }
+}
+
+// Launch shape of the tail kernel: blockDim = the leaf kernel's tile, its
+// rows and per-child words in dynamic shared memory.
+uint32_t tail_threads(uint32_t rs) { return sc::profiles_per_block(rs + 4); }
+size_t tail_smem(uint32_t rs) {
+    const uint32_t T = tail_threads(rs);
+    return static_cast<size_t>(T) * rs * sizeof(float) + 4 * T * sizeof(uint32_t);
+}
+
+template <class F>
+void with_tail_kernel(const ScoreParams& sp, uint32_t nbins, F&& f) {
+    sc::dispatch_nw_nb(sp.nwidths, nbins, [&](auto nw, auto nbc) {
+        f(prune_tail_kernel<decltype(nw)::value, decltype(nbc)::value>);
+    });
+}
+
+// Tail blocks that fit one SM together.
+uint32_t tail_blocks_per_sm(const ScoreParams& sp, uint32_t nbins, uint32_t rs) {
+    int per_sm = 0;
+    with_tail_kernel(sp, nbins, [&](auto kern) {
+        sc::set_smem(kern, tail_smem(rs));
+        LK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, static_cast<int>(tail_threads(rs)),
+                                                              tail_smem(rs)));
+    });
+    require(per_sm >= 1, "pruning tail: one block per SM does not fit");
+    return static_cast<uint32_t>(per_sm);
+}
+
+// ntrees trees (TailArgs on the device), bpt blocks each, all resident: a
+// cooperative launch, since each tree's blocks wait on one another at its
+// barriers.
+void launch_tails(const TailArgs* d_args, uint32_t ntrees, uint32_t bpt, const ScoreParams& sp,
+                  uint32_t nbins, uint32_t rs, cudaStream_t s) {
+    int dev = 0, nsm = 148;
+    LK_CUDA(cudaGetDevice(&dev));
+    LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const uint32_t per_sm = tail_blocks_per_sm(sp, nbins, rs);
+    require(static_cast<uint64_t>(ntrees) * bpt <= static_cast<uint64_t>(per_sm) * static_cast<uint32_t>(nsm),
+            "pruning tail: more blocks than the device holds at once");
+    with_tail_kernel(sp, nbins, [&](auto kern) {
+        const TailArgs* trees = d_args;
+        void* args[] = {&trees, &bpt};
+        LK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(ntrees * bpt),
+                                            dim3(tail_threads(rs)), args, tail_smem(rs), s));
+    });
+    LK_CUDA(cudaGetLastError());
 }
 
 __global__ void set_u64_kernel(uint64_t* p, uint64_t v) { *p = v; }
@@ -1878,6 +1929,15 @@ __global__ void minmax_kernel(const float* __restrict__ x, uint64_t n, uint32_t*
 std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref_seg,
                                            const float* thresholds, uint64_t n_thresholds,
                                            uint64_t n_iters, cudaStream_t s) {
+    PruneRunState rs;
+    run_begin(rs, d_ffa_fold, ref_seg, thresholds, n_thresholds, n_iters, s);
+    run_levels(rs, false, s);
+    return run_end(rs, s);
+}
+
+void PruneExec::run_begin(PruneRunState& rs, const float* d_ffa_fold, uint64_t ref_seg,
+                          const float* thresholds, uint64_t n_thresholds, uint64_t n_iters,
+                          cudaStream_t s) {
     require(d_ffa_fold != nullptr, "ffa_fold is null");
     require(ref_seg < m_nseg, "ref_idx must be less than nsegments.");
     DeviceGuard g(m_device);
@@ -1915,7 +1975,7 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
     LK_CUDA(cudaMemcpyAsync(m_host.ptr, d_mm, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     LK_CUDA(cudaStreamSynchronize(s));
     m_tree.size = m_ncoords;
-    std::vector<lk_prune_stats> stats;
+    rs.stats.clear();
     {
         lk_prune_stats s0{};
         s0.level = 0;
@@ -1924,45 +1984,75 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
         s0.threshold = 0.0f;
         s0.score_min = m_ncoords ? key_to_float(m_host.as<uint32_t>()[0]) : 0.0f;
         s0.score_max = m_ncoords ? key_to_float(m_host.as<uint32_t>()[1]) : 0.0f;
-        stats.push_back(s0);
+        rs.stats.push_back(s0);
     }
     m_order = order;
     m_level = 0;
     m_ran = true;
     m_finalized = false;
-    const uint64_t levels = std::min<uint64_t>(m_nseg - 1, n_iters);
+    rs.order = order;
+    rs.fold = d_ffa_fold;
+    rs.thresholds = thresholds;
+    rs.n_thresholds = n_thresholds;
+    rs.levels = std::min<uint64_t>(m_nseg - 1, n_iters);
+    rs.lv = 1;
+    rs.handed_back = rs.at_tail = rs.done = false;
     // Each level's score minimum / maximum stays in its own device slot and
     // is read back once, after the last level.
-    if (m_level_mm.bytes < 2 * (levels + 1) * sizeof(uint32_t)) {
-        m_level_mm.alloc(2 * (levels + 1) * sizeof(uint32_t));
+    if (m_level_mm.bytes < 2 * (rs.levels + 1) * sizeof(uint32_t)) {
+        m_level_mm.alloc(2 * (rs.levels + 1) * sizeof(uint32_t));
     }
+}
+
+void PruneExec::run_levels(PruneRunState& rs, bool stop_at_tail, cudaStream_t s) {
+    DeviceGuard g(m_device);
+    const uint64_t seg_floats = m_ncoords * 2 * m_nbins;
+    rs.at_tail = false;
     // Small trees run in the persistent tail; a level it hands back (too many
     // parents or children) runs here, then the tail is tried again.
-    bool handed_back = false;
-    for (uint64_t lv = 1; lv <= levels;) {
-        require(lv <= n_thresholds, "Pruning complete - exceeded threshold scheme length");
-        if (tail_enabled && !handed_back && m_tree.size <= kTailParents) {
-            const uint64_t last = std::min(levels, n_thresholds);
-            const uint64_t next = run_tail(d_ffa_fold, order, lv, last, thresholds, &stats, s);
-            if (m_tree.size == 0) {
-                break;
+    while (!rs.done && rs.lv <= rs.levels) {
+        require(rs.lv <= rs.n_thresholds, "Pruning complete - exceeded threshold scheme length");
+        if (tail_enabled && !rs.handed_back && m_tree.size <= kTailParents) {
+            if (stop_at_tail) {
+                rs.at_tail = true;
+                return;
             }
-            // stopped before the last level with leaves left: handed back
-            handed_back = next <= last;
-            lv = next;
+            TailArgs a{};
+            tail_prepare(rs, &a, s);
+            if (m_tail_args.bytes < sizeof(TailArgs)) {
+                m_tail_args.alloc(sizeof(TailArgs));
+            }
+            LK_CUDA(cudaMemcpyAsync(m_tail_args.ptr, &a, sizeof(a), cudaMemcpyHostToDevice, s));
+            int dev = 0, nsm = 148;
+            LK_CUDA(cudaGetDevice(&dev));
+            LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            // blocks: one per SM by default (LOKI_B200_PRUNE_TAIL_BLOCKS: fewer)
+            if (const char* e = std::getenv("LOKI_B200_PRUNE_TAIL_BLOCKS")) {
+                nsm = std::max(1, std::min(nsm, std::atoi(e)));
+            }
+            launch_tails(m_tail_args.as<TailArgs>(), 1, static_cast<uint32_t>(nsm), m_sp, m_nbins,
+                         a.rs, s);
+            LK_CUDA(cudaStreamSynchronize(s));
+            tail_finish(rs, s);
             continue;
         }
-        handed_back = false;
-        const float* d_seg = d_ffa_fold + order[lv] * seg_floats;
+        rs.handed_back = false;
+        const float* d_seg = rs.fold + rs.order[rs.lv] * seg_floats;
         lk_prune_stats st{};
-        level(d_seg, order, lv, thresholds[lv - 1], &st, s);
-        stats.push_back(st);
-        m_level = lv;
+        level(d_seg, rs.order, rs.lv, rs.thresholds[rs.lv - 1], &st, s);
+        rs.stats.push_back(st);
+        m_level = rs.lv;
+        ++rs.lv;
         if (m_tree.size == 0) {
-            break;
+            rs.done = true;
         }
-        ++lv;
     }
+    rs.done = true;
+}
+
+std::vector<lk_prune_stats> PruneExec::run_end(PruneRunState& rs, cudaStream_t s) {
+    DeviceGuard g(m_device);
+    std::vector<lk_prune_stats>& stats = rs.stats;
     if (stats.size() > 1) {
         std::vector<uint32_t> mm(2 * stats.size());
         LK_CUDA(cudaMemcpyAsync(mm.data(), m_level_mm.ptr, mm.size() * sizeof(uint32_t),
@@ -1974,12 +2064,74 @@ std::vector<lk_prune_stats> PruneExec::run(const float* d_ffa_fold, uint64_t ref
             stats[k].score_max = any ? key_to_float(mm[2 * k + 1]) : -FLT_MAX;
         }
     }
-    return stats;
+    return std::move(stats);
 }
 
-uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t>& order,
-                            uint64_t first, uint64_t last, const float* thresholds,
-                            std::vector<lk_prune_stats>* stats, cudaStream_t s) {
+std::vector<std::vector<lk_prune_stats>> PruneExec::run_many(
+    const std::vector<PruneExec*>& ex, const float* d_ffa_fold, const std::vector<uint64_t>& ref_segs,
+    const float* thresholds, uint64_t n_thresholds, uint64_t n_iters, cudaStream_t s) {
+    require(ex.size() == ref_segs.size() && !ex.empty(), "run_many: one executor per reference segment");
+    for (size_t k = 1; k < ex.size(); ++k) {
+        require(ex[k] != ex[0] && ex[k]->m_device == ex[0]->m_device && ex[k]->m_nbins == ex[0]->m_nbins &&
+                    ex[k]->m_sp.nwidths == ex[0]->m_sp.nwidths && ex[k]->m_sp.wmax == ex[0]->m_sp.wmax,
+                "run_many: executors of one plan on one device, one per run");
+    }
+    DeviceGuard g(ex[0]->m_device);
+    std::vector<PruneRunState> rs(ex.size());
+    // 1. each run up to where its tail would start
+    for (size_t k = 0; k < ex.size(); ++k) {
+        ex[k]->run_begin(rs[k], d_ffa_fold, ref_segs[k], thresholds, n_thresholds, n_iters, s);
+        ex[k]->run_levels(rs[k], true, s);
+    }
+    // 2. the tails of all runs in one cooperative launch
+    std::vector<size_t> at;
+    for (size_t k = 0; k < ex.size(); ++k) {
+        if (rs[k].at_tail) {
+            at.push_back(k);
+        }
+    }
+    if (!at.empty()) {
+        std::vector<TailArgs> args(at.size());
+        for (size_t i = 0; i < at.size(); ++i) {
+            ex[at[i]]->tail_prepare(rs[at[i]], &args[i], s);
+        }
+        PruneExec* e0 = ex[at[0]];
+        if (e0->m_tail_args.bytes < args.size() * sizeof(TailArgs)) {
+            e0->m_tail_args.alloc(args.size() * sizeof(TailArgs));
+        }
+        LK_CUDA(cudaMemcpyAsync(e0->m_tail_args.ptr, args.data(), args.size() * sizeof(TailArgs),
+                                cudaMemcpyHostToDevice, s));
+        int dev = 0, nsm = 148;
+        LK_CUDA(cudaGetDevice(&dev));
+        LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const uint32_t per_sm = tail_blocks_per_sm(e0->m_sp, e0->m_nbins, args[0].rs);
+        const uint32_t total = per_sm * static_cast<uint32_t>(nsm);
+        const uint32_t bpt = std::max<uint32_t>(
+            1, std::min<uint32_t>(static_cast<uint32_t>(nsm), total / static_cast<uint32_t>(at.size())));
+        require(static_cast<uint64_t>(bpt) * at.size() <= total,
+                "run_many: more runs than the device holds tail blocks");
+        launch_tails(e0->m_tail_args.as<TailArgs>(), static_cast<uint32_t>(at.size()), bpt, e0->m_sp,
+                     e0->m_nbins, args[0].rs, s);
+        LK_CUDA(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < at.size(); ++i) {
+            ex[at[i]]->tail_finish(rs[at[i]], s);
+        }
+    }
+    // 3. whatever a tail handed back, and the runs' ends
+    std::vector<std::vector<lk_prune_stats>> out(ex.size());
+    for (size_t k = 0; k < ex.size(); ++k) {
+        ex[k]->run_levels(rs[k], false, s);
+        out[k] = ex[k]->run_end(rs[k], s);
+    }
+    return out;
+}
+
+void PruneExec::tail_prepare(PruneRunState& rs, void* args, cudaStream_t s) {
+    const uint64_t first = rs.lv;
+    const uint64_t last = std::min(rs.levels, rs.n_thresholds);
+    const std::vector<uint64_t>& order = rs.order;
+    const float* d_ffa_fold = rs.fold;
+    const float* thresholds = rs.thresholds;
     const uint64_t seg_floats = m_ncoords * 2 * m_nbins;
     // children buffers: up to kTailChildren, at most 256 MiB of child data
     const uint64_t per_child = m_ls * sizeof(double) + 8 + 2 * m_nbins * sizeof(float);
@@ -2014,6 +2166,7 @@ uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t
                             : make_transform(m_np, cn.ref, cc.ref, m_conservative);
         L.pt = m_basis == 1 ? make_transform_cheby(cc, cp) : TransformConsts{};
     }
+    // pageable sources: the copies are staged before these calls return
     LK_CUDA(cudaMemcpyAsync(m_tail_levels.ptr, lc.data(), lc.size() * sizeof(TailLevel),
                             cudaMemcpyHostToDevice, s));
     TailCtl c{};
@@ -2023,7 +2176,8 @@ uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t
     c.level = static_cast<uint32_t>(first);
     LK_CUDA(cudaMemcpyAsync(m_tail_ctl.ptr, &c, sizeof(c), cudaMemcpyHostToDevice, s));
 
-    TailArgs a{};
+    TailArgs& a = *static_cast<TailArgs*>(args);
+    a = TailArgs{};
     for (int i = 0; i < 2; ++i) {
         a.tleaves[i] = m_tleaves[i].as<double>();
         a.tfolds[i] = m_tfolds[i].as<float>();
@@ -2051,30 +2205,14 @@ uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t
     a.rs = sc::row_stride(m_nbins, m_sp.wmax);
     a.geom = make_geom(m_plan, m_branch_max, m_basis);
     a.sp = m_sp;
-    const uint32_t T = sc::profiles_per_block(a.rs + 4);
-    const size_t smem = static_cast<size_t>(T) * a.rs * sizeof(float) + 4 * T * sizeof(uint32_t);
-    int dev = 0, nsm = 148;
-    LK_CUDA(cudaGetDevice(&dev));
-    LK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    // blocks: one per SM by default (LOKI_B200_PRUNE_TAIL_BLOCKS: fewer)
-    if (const char* e = std::getenv("LOKI_B200_PRUNE_TAIL_BLOCKS")) {
-        nsm = std::max(1, std::min(nsm, std::atoi(e)));
-    }
-    sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
-        auto kern = prune_tail_kernel<decltype(nw)::value, decltype(nbc)::value>;
-        sc::set_smem(kern, smem);
-        int per_sm = 0;
-        LK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, static_cast<int>(T), smem));
-        require(per_sm >= 1, "pruning tail: one block per SM does not fit");
-        void* args[] = {&a};
-        // one block per SM, all resident (cooperative launch): the grid
-        // barriers between the steps of a level need every block running
-        LK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), dim3(nsm), dim3(T), args,
-                                            smem, s));
-    });
-    LK_CUDA(cudaGetLastError());
-    LK_CUDA(cudaMemcpyAsync(&c, m_tail_ctl.ptr, sizeof(c), cudaMemcpyDeviceToHost, s));
+}
+
+void PruneExec::tail_finish(PruneRunState& rs, cudaStream_t s) {
+    const uint64_t first = rs.lv;
+    const uint64_t last = std::min(rs.levels, rs.n_thresholds);
+    TailCtl c{};
     std::vector<uint64_t> st(3 * (last + 1));
+    LK_CUDA(cudaMemcpyAsync(&c, m_tail_ctl.ptr, sizeof(c), cudaMemcpyDeviceToHost, s));
     LK_CUDA(cudaMemcpyAsync(st.data(), m_tail_stats.ptr, st.size() * sizeof(uint64_t),
                             cudaMemcpyDeviceToHost, s));
     LK_CUDA(cudaStreamSynchronize(s));
@@ -2100,15 +2238,15 @@ uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t
     for (uint64_t lv = first; lv < c.level; ++lv) {
         lk_prune_stats r{};
         r.level = lv;
-        r.seg_idx = order[lv];
+        r.seg_idx = rs.order[lv];
         r.n_branches = st[3 * lv];
         r.n_leaves = st[3 * lv + 1];
         r.n_leaves_phy = st[3 * lv + 1];
         r.n_leaves_surv = st[3 * lv + 2];
-        r.threshold = thresholds[lv - 1];
-        r.score_min = FLT_MAX;   // filled by run() from the level's device slot
+        r.threshold = rs.thresholds[lv - 1];
+        r.score_min = FLT_MAX;   // filled by run_end from the level's device slot
         r.score_max = -FLT_MAX;
-        stats->push_back(r);
+        rs.stats.push_back(r);
         m_level = lv;
     }
     m_tree.head = c.head;
@@ -2117,7 +2255,13 @@ uint64_t PruneExec::run_tail(const float* d_ffa_fold, const std::vector<uint64_t
     m_tree.read_consumed = 0;
     m_tree.write_start = (c.head + c.size) % m_tree.cap;
     m_cur = static_cast<int>(c.cur);
-    return c.level;
+    rs.lv = c.level;
+    rs.at_tail = false;
+    // stopped before the last level with leaves left: handed back
+    rs.handed_back = m_tree.size > 0 && rs.lv <= last;
+    if (m_tree.size == 0) {
+        rs.done = true;
+    }
 }
 
 void PruneExec::level(const float* d_seg, const std::vector<uint64_t>& order, uint64_t lv,

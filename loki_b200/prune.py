@@ -143,6 +143,38 @@ class PruneCUDA:
                 out[name][i] = getattr(stats[i], name)
         return out
 
+    @staticmethod
+    def run_many(prunes, ffa_fold, ref_segs, thresholds, n_iters: int | None = None) -> list:
+        """One run per executor (``prunes[k]`` seeds from ``ref_segs[k]``; same
+        configuration, distinct executors, one device) on the current stream:
+        each run's large levels level by level, then the small trees' tails of
+        all runs in ONE cooperative launch. Returns each run's statistics, as
+        ``run`` gives them; each executor then holds its run's tree."""
+        prunes = list(prunes)
+        if len(prunes) != len(ref_segs) or not prunes:
+            raise ValueError("one executor per reference segment")
+        dev = prunes[0]._device
+        fold = D.to_device_f32(ffa_fold, dev).reshape(-1)
+        thr = np.ascontiguousarray(thresholds, dtype=np.float32)
+        n_iters = thr.size if n_iters is None else int(n_iters)
+        k = len(prunes)
+        per = n_iters + 1
+        stats = (C.LkPruneStats * (k * per))()
+        counts = (ctypes.c_uint64 * k)()
+        handles = (ctypes.c_void_p * k)(*[p._h.value for p in prunes])
+        segs = np.ascontiguousarray(ref_segs, dtype=np.uint64)
+        with D.torch().cuda.device(dev):
+            C.check(C.lib().lk_prune_run_many(handles, k, D.ptr(fold), segs.ctypes.data, thr.ctypes.data, thr.size,
+                                              n_iters, stats, per, counts, D.stream_ptr(dev)))
+        out = []
+        for j in range(k):
+            rows = np.zeros(counts[j], PRUNE_STATS_DTYPE)
+            for i in range(counts[j]):
+                for name in PRUNE_STATS_DTYPE.names:
+                    rows[name][i] = getattr(stats[j * per + i], name)
+            out.append(rows)
+        return out
+
     def finalize(self, ffa_fold) -> None:
         """Ascend the run's survivors to the middle of the data and report them
         there (the end of the reference's PruneImpl::run): folds over every
@@ -192,11 +224,13 @@ class EPMultiPassCUDA:
     (reference ``EPMultiPass``: same arguments; ``device_id`` added).
 
     ``n_workers`` (default ``cfg.nthreads``, the reference's number of pruning
-    workspaces) runs that many reference segments at once on the device, each
-    on its own executor, CUDA stream and host thread (the reference runs its
-    segments on a thread pool of ``nthreads`` workspaces); a pruning level is a
-    few small launches between host synchronisations, so concurrent runs fill
-    the GPU that one run leaves idle. Results do not depend on it. Each worker
+    workspaces) runs that many reference segments at once on the device (the
+    reference runs its segments on a thread pool of ``nthreads``
+    workspaces). ``batched=True`` (default): each group of ``n_workers`` runs
+    goes through ``PruneCUDA.run_many`` on one stream, the small trees' tails
+    of the group in one cooperative launch; ``batched=False``: each worker on
+    its own executor, CUDA stream and host thread. Results do not depend on
+    either. Each worker
     takes a fixed share of the segments (its executor's buffers then stop
     growing after the first execute). No more workers run than there are
     reference segments to prune, and each worker's executor (device buffers
@@ -207,7 +241,7 @@ class EPMultiPassCUDA:
     def __init__(self, cfg: PulsarSearchConfig, threshold_scheme, n_runs: int | None = None, ref_segs=None,
                  max_sugg: int = 1 << 18, batch_size: int = 1024, poly_basis: str = "taylor",
                  show_progress: bool = False, use_conservative_tile: bool = False, device_id: int = 0,
-                 n_workers: int | None = None):
+                 n_workers: int | None = None, batched: bool = True):
         _basis(poly_basis)
         self._cfg = cfg
         self._thr = np.ascontiguousarray(threshold_scheme, dtype=np.float32)
@@ -220,6 +254,7 @@ class EPMultiPassCUDA:
         self._poly_basis = poly_basis
         self._prunes: list[PruneCUDA] = []
         self._device = device_id
+        self._batched = bool(batched)
 
     def _executor(self, k: int) -> "PruneCUDA":
         """Worker k's pruning executor, created on first use."""
@@ -227,15 +262,18 @@ class EPMultiPassCUDA:
             self._prunes.append(PruneCUDA(*self._prune_args, poly_basis=self._poly_basis))
         return self._prunes[k]
 
+    def _result(self, pr: "PruneCUDA", fold, ref_seg: int, nseg: int, stats) -> dict:
+        pr.finalize(fold)
+        leaves, folds, scores = pr.tree()
+        return {"stats": stats, "leaves": leaves, "folds": folds, "scores": scores,
+                "scores_ep": pr.scores_ep(),
+                "snail_scheme": np.array(middle_out_order(nseg, ref_seg), np.uint64)}
+
     def _run_one(self, pr: "PruneCUDA", fold, ref_seg: int, nseg: int, stream) -> dict:
         t = D.torch()
         with t.cuda.device(self._device), t.cuda.stream(stream):
             stats = pr.run(fold, ref_seg, self._thr, n_iters=nseg - 1)
-            pr.finalize(fold)
-            leaves, folds, scores = pr.tree()
-            return {"stats": stats, "leaves": leaves, "folds": folds, "scores": scores,
-                    "scores_ep": pr.scores_ep(),
-                    "snail_scheme": np.array(middle_out_order(nseg, ref_seg), np.uint64)}
+            return self._result(pr, fold, ref_seg, nseg, stats)
 
     @property
     def ffa(self) -> FFACUDA:
@@ -255,7 +293,16 @@ class EPMultiPassCUDA:
         segs = determine_ref_segs(nseg, self._n_runs, self._ref_segs)
         t.cuda.synchronize(self._device)  # the fold is complete before other streams read it
         workers = max(1, min(self._workers, len(segs)))
-        if workers == 1:
+        if self._batched and workers > 1:
+            # groups of `workers` runs, each group's tails in one launch
+            prunes = [self._executor(k) for k in range(workers)]
+            runs = []
+            with t.cuda.device(self._device):
+                for g0 in range(0, len(segs), workers):
+                    group = segs[g0 : g0 + workers]
+                    stats = PruneCUDA.run_many(prunes[: len(group)], fold, group, self._thr, n_iters=nseg - 1)
+                    runs += [self._result(pr, fold, rs, nseg, st) for pr, rs, st in zip(prunes, group, stats)]
+        elif workers == 1:
             stream = t.cuda.current_stream(self._device)
             pr = self._executor(0)
             runs = [self._run_one(pr, fold, rs, nseg, stream) for rs in segs]

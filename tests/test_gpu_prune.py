@@ -109,6 +109,26 @@ def test_prune_tail_matches_level_by_level(cuda, name):
         np.testing.assert_array_equal(a.view(np.uint8), b.view(np.uint8))
 
 
+@pytest.mark.parametrize("name", ["accel_nb32_overload", "accel_nb32_many_batches", "jerk_nb32_big",
+                                  "accel_nb32_wrap"])
+def test_prune_run_many_matches_single_runs(cuda, name):
+    """Several runs with their tails in one cooperative launch (run_many) give
+    each run's own result; the many-batches case hands levels back."""
+    from loki_b200.prune import PruneCUDA
+
+    plan, cfg, _, fold, nseg, _, thr, ms, bs, cons = _setup(name)
+    segs = sorted({0, nseg // 3, nseg // 2, nseg - 1})
+    kw = dict(max_sugg=ms, batch_size=bs, branch_max=None, use_conservative_tile=cons)
+    many = [PruneCUDA(cfg, **kw) for _ in segs]
+    got = PruneCUDA.run_many(many, fold, segs, thr)
+    for pr, rs, st in zip(many, segs, got):
+        one = PruneCUDA(cfg, **kw)
+        want = one.run(fold, rs, thr)
+        np.testing.assert_array_equal(_stats_matrix(st), _stats_matrix(want))
+        for a, b in zip(pr.tree(), one.tree()):
+            np.testing.assert_array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
 @pytest.mark.parametrize("name", ["prune_accel_nb16.npz", "prune_jerk_nb16.npz"])
 def test_prune_reference_golden_fixtures(cuda, name):
     from loki_b200.configs import PulsarSearchConfig
@@ -155,14 +175,17 @@ def test_ep_multipass_concurrent_runs_identical(cuda, tmp_path):
     from loki_b200.prune import EPMultiPassCUDA
 
     plan, cfg, (e, v), fold, nseg, _, thr, ms, bs, cons = _setup("accel_nb32_many_batches")
-    seq = EPMultiPassCUDA(cfg, thr, n_runs=5, max_sugg=ms, batch_size=bs).execute(e, v)
+    seq = EPMultiPassCUDA(cfg, thr, n_runs=5, max_sugg=ms, batch_size=bs, n_workers=1).execute(e, v)
     par = EPMultiPassCUDA(cfg, thr, n_runs=5, max_sugg=ms, batch_size=bs, n_workers=3).execute(
         e, v, outdir=str(tmp_path), file_prefix="t")
-    assert sorted(seq) == sorted(par) and len(seq) == 5
-    for rs in seq:
-        for k in ("leaves", "folds", "scores", "scores_ep"):
-            np.testing.assert_array_equal(par[rs][k].view(np.uint8), seq[rs][k].view(np.uint8))
-        np.testing.assert_array_equal(_stats_matrix(par[rs]["stats"]), _stats_matrix(seq[rs]["stats"]))
+    thr_par = EPMultiPassCUDA(cfg, thr, n_runs=5, max_sugg=ms, batch_size=bs, n_workers=3,
+                              batched=False).execute(e, v)
+    assert sorted(seq) == sorted(par) == sorted(thr_par) and len(seq) == 5
+    for other in (par, thr_par):
+        for rs in seq:
+            for k in ("leaves", "folds", "scores", "scores_ep"):
+                np.testing.assert_array_equal(other[rs][k].view(np.uint8), seq[rs][k].view(np.uint8))
+            np.testing.assert_array_equal(_stats_matrix(other[rs]["stats"]), _stats_matrix(seq[rs]["stats"]))
     z = np.load(tmp_path / f"t_pruning_nstages_{nseg}_results.npz")
     for rs in seq:
         np.testing.assert_array_equal(z[f"{rs:03d}_00/param_sets"], seq[rs]["leaves"])
