@@ -56,6 +56,8 @@ def parse():
                     help="keep the default launch shapes instead of timing the candidates first")
     ap.add_argument("--tuning", default=None,
                     help="apply these launch shapes (JSON of FFACUDA.tuning) instead of autotuning")
+    ap.add_argument("--no-mixed-batched", action="store_true",
+                    help="skip the BF16-storage + batched measurement beside the plain FP32 line")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own GPU path (oracle/_ref/libloki_ref_cuda.so)")
     ap.add_argument("--reference-gpu-child", default=None, help=argparse.SUPPRESS)
@@ -383,6 +385,51 @@ def reference_gpu(args, ours_ms, ours_scores):
             "scores_max_abs_diff": float(d.max()), "scores_mean_abs_diff": float(d.mean())}
 
 
+def mixed_batched(args, cfg, ffa, e, v, plain_ms, want_idx, want_snr, nbatch=4):
+    """The two systems patterns together on the same series: BF16 fold storage
+    and nbatch series per launch (one executor, max_batch = nbatch), ms per
+    series against the plain FP32 single-series step, and the first series'
+    candidates against the plain ones. FP32 batched is timed beside it."""
+    import torch
+
+    from loki_b200.ffa import FFACUDA
+
+    eb = e.reshape(1, -1).repeat(nbatch, 1).contiguous()
+    vb = v.reshape(1, -1).repeat(nbatch, 1).contiguous()
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=e.device)
+    cap = 1 << 22
+    out = {"nbatch": nbatch, "plain_fp32_ms_per_series": plain_ms}
+    for storage in ("bf16", "fp32"):
+        fb = FFACUDA(cfg, device_id=e.device.index or 0, fold_storage=storage, max_batch=nbatch)
+        fb.set_tuning(ffa.tuning)
+        idx = torch.empty(cap, dtype=torch.int32, device=e.device)
+        snr = torch.empty(cap, dtype=torch.float32, device=e.device)
+        cnt = torch.zeros(1, dtype=torch.int64, device=e.device)
+        for _ in range(max(args.warmup, 3)):
+            fb.search_batch(eb, vb, SNR_MIN, idx, snr, cnt)
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record()
+            fb.search_batch(eb, vb, SNR_MIN, idx, snr, cnt)
+            stops[k].record()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / args.steps / nbatch
+        n = int(cnt.item())
+        got = idx[:n].cpu().numpy().view(np.uint32)
+        per = int(fb.plan.ncoords[-1]) * cfg.n_scoring_widths
+        first = got < per
+        same = bool(np.array_equal(got[first], want_idx) and
+                    np.array_equal(snr[:n].cpu().numpy()[first].view(np.uint32), want_snr.view(np.uint32)))
+        out[f"{storage}_batched_ms_per_series"] = ms
+        out[f"{storage}_batched_candidates_equal_plain"] = same
+        del fb
+    out["ratio_mixed_batched_vs_plain"] = plain_ms / out["bf16_batched_ms_per_series"]
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return 0
@@ -567,6 +614,10 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_parity:
         # the last timed step's candidates against the reference's, full size
         parity = candidate_parity(params, ts_e, ts_v, idx[:ncand].cpu().numpy(), snr[:ncand].cpu().numpy())
+    mb = None
+    if rank == 0 and world == 1 and not args.no_mixed_batched:
+        mb = mixed_batched(args, cfg, ffa, e, v, step_ms_max, idx[:ncand].cpu().numpy().view(np.uint32),
+                           snr[:ncand].cpu().numpy())
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu(args, step_ms_max, ffa.scores(e, v).cpu().numpy())
@@ -582,6 +633,7 @@ def run_ours(args, rank, world, local_rank):
                                            "tuning": tuning}),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "stages": stages, "wall_s": wall, "parity": parity, "reference_gpu": ref_gpu,
+            "mixed_batched": mb,
         }
         emit(line)
         if parity is not None and parity.get("checked") and not parity["candidates_match"]:
