@@ -46,6 +46,7 @@ struct McArgs {
     const uint8_t* cls;       // optional: class flag of each noise row
     float* max_snr;
     unsigned long long* counts;
+    int thr_sorted;           // grid non-decreasing: counted by rank (below)
 };
 
 // Input row and noise row of trial i; an index outside its buffer is
@@ -78,12 +79,15 @@ __device__ __forceinline__ float stage_value(const McArgs& a, TrialRows t, uint3
 template <int NW, int NB>
 __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
     extern __shared__ float rows[];
-    __shared__ unsigned int s_cnt[2 * LK_MC_MAX_THRESHOLDS];
+    // counts per grid value (or, sorted grid, per rank 0 .. n_thr), all
+    // trials then the class-flagged ones
+    __shared__ unsigned int s_cnt[2 * LK_MC_MAX_THRESHOLDS + 2];
+    unsigned int* s_hist2 = s_cnt + LK_MC_MAX_THRESHOLDS + 1;
     const uint32_t T = blockDim.x;
     const uint64_t p0 = static_cast<uint64_t>(blockIdx.x) * T;
     const uint32_t nhere = static_cast<uint32_t>((a.n - p0) < T ? (a.n - p0) : T);
     const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    for (uint32_t k = threadIdx.x; k < 2 * a.n_thr; k += T) {
+    for (uint32_t k = threadIdx.x; k < 2 * LK_MC_MAX_THRESHOLDS + 2; k += T) {
         s_cnt[k] = 0;
     }
 #pragma unroll 2
@@ -101,16 +105,47 @@ __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
         const uint64_t i = p0 + threadIdx.x;
         a.max_snr[i] = m;
         const bool flagged = a.cls != nullptr && a.cls[trial_rows(a, i, false).noise] != 0;
-        for (uint32_t k = 0; k < a.n_thr; ++k) {
-            if (m > a.thr[k]) {
-                atomicAdd(&s_cnt[k], 1u);
-                if (flagged) {
-                    atomicAdd(&s_cnt[a.n_thr + k], 1u);
+        if (a.thr_sorted) {
+            // non-decreasing grid: m > thr[k] exactly for k < r, r the number
+            // of grid values below m, so one histogram entry per trial
+            // replaces up to n_thr counter increments
+            uint32_t r = 0;
+            for (uint32_t k = 0; k < a.n_thr; ++k) {
+                r += m > a.thr[k] ? 1u : 0u;
+            }
+            atomicAdd(&s_cnt[r], 1u);
+            if (flagged) {
+                atomicAdd(&s_hist2[r], 1u);
+            }
+        } else {
+            for (uint32_t k = 0; k < a.n_thr; ++k) {
+                if (m > a.thr[k]) {
+                    atomicAdd(&s_cnt[k], 1u);
+                    if (flagged) {
+                        atomicAdd(&s_cnt[a.n_thr + k], 1u);
+                    }
                 }
             }
         }
     }
     __syncthreads();
+    if (a.thr_sorted) {
+        // histogram of ranks -> counts: count[k] = trials of rank > k
+        for (uint32_t k = threadIdx.x; k < a.n_thr; k += T) {
+            unsigned int c1 = 0, c2 = 0;
+            for (uint32_t r = k + 1; r <= a.n_thr; ++r) {
+                c1 += s_cnt[r];
+                c2 += s_hist2[r];
+            }
+            if (c1 != 0) {
+                atomicAdd(&a.counts[k], static_cast<unsigned long long>(c1));
+            }
+            if (a.cls != nullptr && c2 != 0) {
+                atomicAdd(&a.counts[a.n_thr + k], static_cast<unsigned long long>(c2));
+            }
+        }
+        return;
+    }
     const uint32_t ncnt = a.cls != nullptr ? 2 * a.n_thr : a.n_thr;
     for (uint32_t k = threadIdx.x; k < ncnt; k += T) {
         if (s_cnt[k] != 0) {
@@ -204,6 +239,13 @@ void McExec::stage(const McStage& st, cudaStream_t s) {
     a.stdnoise = std::sqrt(st.var_in + st.var_add);  // float, as sqrt(var_new) in the reference
     a.thr = m_thr.as<float>();
     a.n_thr = st.n_thr;
+    // the rank count needs {k : m > thr[k]} to be a prefix for every m: a
+    // non-decreasing grid without NaN
+    a.thr_sorted = std::is_sorted(st.thresholds, st.thresholds + st.n_thr) &&
+                           std::none_of(st.thresholds, st.thresholds + st.n_thr,
+                                        [](float x) { return std::isnan(x); })
+                       ? 1
+                       : 0;
     a.cls = st.d_class;
     a.max_snr = st.d_max_snr != nullptr ? st.d_max_snr : m_max_snr.as<float>();
     a.counts = reinterpret_cast<unsigned long long*>(st.d_counts);

@@ -71,6 +71,33 @@ def test_mc_stage_folds_ids_and_max_snr(cuda, per_trial):
     np.testing.assert_array_equal(r["counts"].cpu().numpy().astype(np.uint64), counts_w)
 
 
+@pytest.mark.parametrize("grid_kind", ["sorted_ties", "shuffled", "with_nan"])
+def test_mc_stage_grid_counts(cuda, grid_kind):
+    """Grid counts (all trials and class-flagged ones) for a non-decreasing
+    grid with repeated values (counted by rank), a shuffled grid and one with
+    a NaN entry (counted per grid value), against the oracle."""
+    from loki_b200.thresholds import MCStageCUDA
+
+    rng = np.random.default_rng(23)
+    n, nb = 4099, 64
+    fin = rng.standard_normal((n, nb)).astype(np.float32)
+    nz = rng.standard_normal((n, nb)).astype(np.float32)
+    sig = rng.random(nb).astype(np.float32)
+    cls = (rng.random(n) < 0.3).astype(np.uint8)
+    grid = np.round(np.linspace(0.0, 8.0, 64), 1).astype(np.float32)
+    grid[10:14] = grid[10]
+    if grid_kind == "shuffled":
+        grid = rng.permutation(grid)
+    elif grid_kind == "with_nan":
+        grid[20] = np.nan
+    f_w, ids_w, counts_w, mx_w = lko.mc_stage(fin, nz, sig, 1.0, 1.0, WIDTHS.astype(np.uint64), 3.0, grid,
+                                              signal_scale=2.0, cls=cls)
+    st = MCStageCUDA(n, nb, WIDTHS)
+    r = st.stage(fin, nz, sig, 3.0, 1.0, 1.0, thresholds=grid, signal_scale=2.0, cls=cls)
+    np.testing.assert_array_equal(r["counts"].cpu().numpy().astype(np.uint64), counts_w)
+    assert int(r["count"].item()) == ids_w.size
+
+
 def test_mc_stage_reference_api_and_errors(cuda):
     from loki_b200 import LokiError
     from loki_b200.thresholds import MCStageCUDA, simulate_score_prune_fused
