@@ -583,7 +583,9 @@ def run_mc(args, rank, world, local_rank):
                          folds_out=bufs[cur])
             trials += alive * len(grids[s])
             kept = int(r["count"].item())
-            stage_bytes.append(alive * nbins * 4 * 3 + kept * nbins * 4 * 4)
+            # score: input and noise rows in, the stage fold out; survivors'
+            # copy: the stage fold in, the next stage's fold out
+            stage_bytes.append(alive * nbins * 4 * 3 + kept * nbins * 4 * 2)
             rows, fin, cur, alive, var = r["ids"][:kept].clone(), bufs[cur], 1 - cur, kept, 2 * var
             if alive == 0:
                 break

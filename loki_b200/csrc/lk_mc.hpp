@@ -51,6 +51,7 @@ private:
     int m_device;
     ScoreParams m_sp{};
     DeviceBuffer m_max_snr, m_idx, m_vals, m_scratch, m_thr, m_status;
+    DeviceBuffer m_stage_folds;  // [max_trials][nbins]: every trial's fold of the stage
 };
 
 }  // namespace lk

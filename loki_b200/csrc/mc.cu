@@ -47,6 +47,7 @@ struct McArgs {
     float* max_snr;
     unsigned long long* counts;
     int thr_sorted;           // grid non-decreasing: counted by rank (below)
+    float* stage_folds;       // every trial's fold [n][nbins], for the survivors' copy
 };
 
 // Input row and noise row of trial i; an index outside its buffer is
@@ -93,9 +94,12 @@ __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
 #pragma unroll 2
     for (uint32_t p = warp; p < nhere; p += T / kWarp) {
         float* dst = rows + static_cast<size_t>(p) * rs;
+        float* keep = a.stage_folds + (p0 + p) * a.nbins;
         const TrialRows tr = trial_rows(a, p0 + p, lane == 0);
         for (uint32_t j = lane; j < a.nbins; j += kWarp) {
-            dst[j] = stage_value(a, tr, j);
+            const float x = stage_value(a, tr, j);
+            dst[j] = x;
+            keep[j] = x;
         }
     }
     __syncthreads();
@@ -154,22 +158,34 @@ __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
     }
 }
 
-// Survivor k (trial idx[k], k < *d_count): rebuild its fold into out[k] and
-// record its noise row. One warp per survivor, grid-stride.
+// Survivor k (trial idx[k], k < *d_count): its fold, kept by the score
+// kernel, copied into out[k], and its noise row recorded. A group of G
+// threads per survivor, float4 copies when nbins is a multiple of 4.
 __global__ void mc_gather_kernel(McArgs a, const uint32_t* __restrict__ idx,
                                  const uint64_t* __restrict__ d_count, float* __restrict__ out,
                                  uint32_t* __restrict__ ids_out) {
     const uint64_t n = *d_count;
-    const uint64_t wpb = blockDim.x / kWarp;
-    const uint32_t lane = threadIdx.x % kWarp;
-    for (uint64_t k = blockIdx.x * wpb + threadIdx.x / kWarp; k < n; k += gridDim.x * wpb) {
+    const uint32_t nb = a.nbins;
+    const bool vec = (nb % 4) == 0;
+    const uint32_t per_row = vec ? nb / 4 : nb;                // items of one row
+    const uint32_t G = per_row >= 32 ? 32 : (per_row >= 16 ? 16 : 8);  // threads per row
+    const uint64_t groups = static_cast<uint64_t>(gridDim.x) * (blockDim.x / G);
+    const uint32_t sub = threadIdx.x % G;
+    for (uint64_t k = blockIdx.x * (blockDim.x / G) + threadIdx.x / G; k < n; k += groups) {
         const uint64_t i = idx[k];
-        const TrialRows tr = trial_rows(a, i, false);
-        for (uint32_t j = lane; j < a.nbins; j += kWarp) {
-            out[k * a.nbins + j] = stage_value(a, tr, j);
+        const float* src = a.stage_folds + i * nb;
+        float* dst = out + k * nb;
+        if (vec) {
+            for (uint32_t q = sub; q < per_row; q += G) {
+                reinterpret_cast<float4*>(dst)[q] = __ldg(reinterpret_cast<const float4*>(src) + q);
+            }
+        } else {
+            for (uint32_t q = sub; q < per_row; q += G) {
+                dst[q] = __ldg(src + q);
+            }
         }
-        if (lane == 0 && ids_out != nullptr) {
-            ids_out[k] = static_cast<uint32_t>(tr.noise);
+        if (sub == 0 && ids_out != nullptr) {
+            ids_out[k] = static_cast<uint32_t>(trial_rows(a, i, false).noise);
         }
     }
 }
@@ -186,6 +202,7 @@ McExec::McExec(uint64_t max_trials, uint32_t nbins, const uint32_t* widths, uint
     m_idx.alloc(max_trials * sizeof(uint32_t));
     m_vals.alloc(max_trials * sizeof(float));
     m_scratch.alloc(compact_scratch_bytes(max_trials));
+    m_stage_folds.alloc(max_trials * nbins * sizeof(float));
     m_thr.alloc(LK_MC_MAX_THRESHOLDS * sizeof(float));
     m_status.alloc(sizeof(uint32_t));
     LK_CUDA(cudaMemset(m_status.ptr, 0, sizeof(uint32_t)));
@@ -201,7 +218,7 @@ uint32_t McExec::read_status(cudaStream_t s) {
 }
 
 uint64_t McExec::device_bytes() const {
-    return m_max_snr.bytes + m_idx.bytes + m_vals.bytes + m_scratch.bytes + m_thr.bytes +
+    return m_max_snr.bytes + m_idx.bytes + m_vals.bytes + m_scratch.bytes + m_thr.bytes + m_stage_folds.bytes +
            m_status.bytes;
 }
 
@@ -248,6 +265,7 @@ void McExec::stage(const McStage& st, cudaStream_t s) {
                        : 0;
     a.cls = st.d_class;
     a.max_snr = st.d_max_snr != nullptr ? st.d_max_snr : m_max_snr.as<float>();
+    a.stage_folds = m_stage_folds.as<float>();
     a.counts = reinterpret_cast<unsigned long long*>(st.d_counts);
     const uint32_t rs = sc::row_stride(m_nbins, m_sp.wmax);
     const uint32_t T = sc::profiles_per_block(rs);
