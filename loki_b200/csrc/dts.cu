@@ -385,8 +385,20 @@ __device__ __forceinline__ bool prev_usable(const DtsArgs& a, uint32_t cell) {
 }
 
 // Pass 1: survivors of every (transition, hypothesis), T trials per block.
-template <int NW, int NB>
-__global__ void dts_count_kernel(DtsArgs a, uint32_t rs, ScoreParams sp) {
+// WM > 0: nbins NB with the width mask mp, scored by sc::max_snr_div_wm
+// (rows of at least NB + WM + 2 floats, rs even); else sc::max_snr_div_any.
+template <int NW, int NB, int WM>
+__device__ __forceinline__ float dts_max_snr(float* r, const DtsArgs& a, const ScoreParams& sp,
+                                             const MaskScoreParams& mp) {
+    if constexpr (WM > 0) {
+        return sc::max_snr_div_wm<NB, WM>(r, mp, a.stdnoise);
+    } else {
+        return sc::max_snr_div_any<NB, NW>(r, a.nbins, a.stdnoise, sp);
+    }
+}
+
+template <int NW, int NB, int WM>
+__global__ void dts_count_kernel(DtsArgs a, uint32_t rs, ScoreParams sp, MaskScoreParams mp) {
     extern __shared__ float rows[];
     __shared__ uint32_t s_cnt;
     const DtsTrans tr = a.trans[blockIdx.y];
@@ -413,8 +425,7 @@ __global__ void dts_count_kernel(DtsArgs a, uint32_t rs, ScoreParams sp) {
     }
     __syncthreads();
     if (threadIdx.x < nhere) {
-        const float m = sc::max_snr_div_any<NB, NW>(rows + static_cast<size_t>(threadIdx.x) * rs,
-                                                    a.nbins, a.stdnoise, sp);
+        const float m = dts_max_snr<NW, NB, WM>(rows + static_cast<size_t>(threadIdx.x) * rs, a, sp, mp);
         if (m > a.thresholds[tr.ithres]) {
             atomicAdd(&s_cnt, 1u);
         }
@@ -467,8 +478,8 @@ __global__ void dts_select_kernel(DtsArgs a) {
 
 // Pass 2: the winners' folds rebuilt, scored again and their survivors
 // stored in trial order; one block per (cell, hypothesis).
-template <int NW, int NB>
-__global__ void dts_regen_kernel(DtsArgs a, uint32_t rs, ScoreParams sp) {
+template <int NW, int NB, int WM>
+__global__ void dts_regen_kernel(DtsArgs a, uint32_t rs, ScoreParams sp, MaskScoreParams mp) {
     extern __shared__ float rows[];
     __shared__ uint32_t ws[32];
     const uint32_t cell = blockIdx.x;
@@ -506,7 +517,7 @@ __global__ void dts_regen_kernel(DtsArgs a, uint32_t rs, ScoreParams sp) {
             for (uint32_t j = 0; j < a.nbins; ++j) {
                 cp[j] = r[j];
             }
-            keep = sc::max_snr_div_any<NB, NW>(cp, a.nbins, a.stdnoise, sp) > thr;
+            keep = dts_max_snr<NW, NB, WM>(cp, a, sp, mp) > thr;
         }
         uint32_t total;
         const uint32_t before = blk::block_exclusive_scan(keep ? 1u : 0u, ws, &total);
@@ -701,7 +712,12 @@ void DtsExec::run(uint32_t thres_neigh, cudaStream_t s) {
         dts_init_kernel<<<blocks, 256, 0, s>>>(a, m_init_pool.as<float>());
         LK_CUDA(cudaGetLastError());
     }
-    const uint32_t rs = sc::row_stride(m_nbins, m_sp.wmax);
+    // the masked scorer (nbins 32 / 64 / 128, strictly increasing widths <=
+    // 32) takes even rows of NB + WM + 2 floats; the generic one odd rows
+    MaskScoreParams mp{};
+    const bool masked = make_mask_score_params(m_sp, m_nbins, &mp);
+    const uint32_t wm = mp.wmax <= 8 ? 8u : (mp.wmax <= 16 ? 16u : 32u);
+    const uint32_t rs = masked ? m_nbins + wm + 2 : sc::row_stride(m_nbins, m_sp.wmax);
     const uint32_t T = 128;
     const size_t smem_count = static_cast<size_t>(T) * rs * sizeof(float);
     const uint32_t TR = 128;  // trials per tile in the rebuild (rows hold a fold and its copy)
@@ -738,20 +754,36 @@ void DtsExec::run(uint32_t thres_neigh, cudaStream_t s) {
         LK_CUDA(cudaMemsetAsync(m_winner.ptr, 0xFF, m_winner.bytes, s));
         if (nt > 0) {
             const dim3 grid((m_ntrials + T - 1) / T, static_cast<unsigned>(nt), 2);
-            sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
-                auto kern = dts_count_kernel<decltype(nw)::value, decltype(nbc)::value>;
-                sc::set_smem(kern, smem_count);
-                kern<<<grid, T, smem_count, s>>>(a, rs, m_sp);
-            });
+            if (masked) {
+                sc::dispatch_nb_wm(m_nbins, mp, [&](auto nbc, auto wmc) {
+                    auto kern = dts_count_kernel<8, decltype(nbc)::value, decltype(wmc)::value>;
+                    sc::set_smem(kern, smem_count);
+                    kern<<<grid, T, smem_count, s>>>(a, rs, m_sp, mp);
+                });
+            } else {
+                sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
+                    auto kern = dts_count_kernel<decltype(nw)::value, decltype(nbc)::value, 0>;
+                    sc::set_smem(kern, smem_count);
+                    kern<<<grid, T, smem_count, s>>>(a, rs, m_sp, mp);
+                });
+            }
             LK_CUDA(cudaGetLastError());
             dts_select_kernel<<<(nb + 127) / 128, 128, 0, s>>>(a);
             LK_CUDA(cudaGetLastError());
         }
-        sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
-            auto kern = dts_regen_kernel<decltype(nw)::value, decltype(nbc)::value>;
-            sc::set_smem(kern, smem_regen);
-            kern<<<dim3(static_cast<unsigned>(ncell), 2), TR, smem_regen, s>>>(a, rs2, m_sp);
-        });
+        if (masked) {
+            sc::dispatch_nb_wm(m_nbins, mp, [&](auto nbc, auto wmc) {
+                auto kern = dts_regen_kernel<8, decltype(nbc)::value, decltype(wmc)::value>;
+                sc::set_smem(kern, smem_regen);
+                kern<<<dim3(static_cast<unsigned>(ncell), 2), TR, smem_regen, s>>>(a, rs2, m_sp, mp);
+            });
+        } else {
+            sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
+                auto kern = dts_regen_kernel<decltype(nw)::value, decltype(nbc)::value, 0>;
+                sc::set_smem(kern, smem_regen);
+                kern<<<dim3(static_cast<unsigned>(ncell), 2), TR, smem_regen, s>>>(a, rs2, m_sp, mp);
+            });
+        }
         LK_CUDA(cudaGetLastError());
         var_in = var_new;
     }

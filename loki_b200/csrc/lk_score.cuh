@@ -189,6 +189,120 @@ __device__ __forceinline__ float max_snr_div_nb(float* r, float stdnoise, const 
     return best;
 }
 
+// ---- masked widths (nbins 32 / 64 / 128, strictly increasing widths <= 32) --
+
+// Three-input max.f32 (sm_100): the largest non-NaN input, as two nested fmaxf.
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Exact reference maximum (first maximum kept) of p[i + w] - p[i].
+__device__ __noinline__ inline float dmax_first(const float* r, uint32_t w, uint32_t nbins) {
+    float m = -FLT_MAX;
+    for (uint32_t i = 0; i < nbins; ++i) {
+        const float d = __fsub_rn(r[i + w], r[i]);
+        m = (m < d) ? d : m;
+    }
+    return m;
+}
+
+// max_snr_div for a profile of NB bins at r (8-byte aligned, room for NB +
+// WM + 2 floats; prefix sums written in place) and the width mask mp: the
+// same IEEE operations -- sequential prefix, circular extension, window
+// differences, ((h + b) dmax - b sum) / stdnoise per width, the maximum over
+// widths in width order -- with the row read two bins per 64-bit access,
+// windows of 16 positions in registers, every width a compile-time offset
+// taken when its mask bit is set, and each width's maximum by a tree of
+// three-input maxima (equal in value to the reference's scan; a zero
+// maximum, whose sign the tree may not keep, is recomputed with its rule).
+template <int NB, int WM>
+__device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams& mp, float stdnoise) {
+    constexpr int CH = 16;
+    static_assert(NB % CH == 0 && WM <= 32, "masked scorer shape");
+    float2* r2 = reinterpret_cast<float2*>(r);
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < NB / 2; ++j) {
+        const float2 x = r2[j];
+        const float a0 = j == 0 ? x.x : __fadd_rn(acc, x.x);
+        acc = __fadd_rn(a0, x.y);
+        r2[j] = make_float2(a0, acc);
+    }
+    const float sum = acc;
+    for (uint32_t k = 0; k < mp.wmax; ++k) {
+        r[NB + k] = __fadd_rn(r[k], sum);
+    }
+    float dm[WM + 1];
+#pragma unroll
+    for (int w = 1; w <= WM; ++w) {
+        dm[w] = -FLT_MAX;
+    }
+#pragma unroll 1
+    for (int c = 0; c < NB; c += CH) {
+        float win[CH + WM];
+#pragma unroll
+        for (int k = 0; k < (CH + WM) / 2; ++k) {
+            const float2 x = r2[c / 2 + k];
+            win[2 * k] = x.x;
+            win[2 * k + 1] = x.y;
+        }
+#pragma unroll
+        for (int w = 1; w <= WM; ++w) {
+            if ((mp.wmask >> w) & 1ull) {
+                float d[CH];
+#pragma unroll
+                for (int k = 0; k < CH; ++k) {
+                    d[k] = __fsub_rn(win[k + w], win[k]);
+                }
+                const float m0 = fmax3(d[0], d[1], d[2]);
+                const float m1 = fmax3(d[3], d[4], d[5]);
+                const float m2 = fmax3(d[6], d[7], d[8]);
+                const float m3 = fmax3(d[9], d[10], d[11]);
+                const float m4 = fmax3(d[12], d[13], d[14]);
+                dm[w] = fmax3(dm[w], fmax3(m0, m1, m2), fmax3(m3, m4, d[15]));
+            }
+        }
+    }
+    float best = -FLT_MAX;
+#pragma unroll
+    for (int w = 1; w <= WM; ++w) {
+        if ((mp.wmask >> w) & 1ull) {
+            float d = dm[w];
+            if (d == 0.0f) {
+                d = dmax_first(r, static_cast<uint32_t>(w), NB);
+            }
+            const float base = __fsub_rn(__fmul_rn(mp.hb[w], d), __fmul_rn(mp.b[w], sum));
+            const float snr = __fdiv_rn(base, stdnoise);
+            best = (best < snr) ? snr : best;
+        }
+    }
+    return best;
+}
+
+// Calls f(NB, WM) for the masked scorer's shape of (nbins, mp) -- NB 32 / 64 /
+// 128, WM the width bucket 8 / 16 / 32.
+template <class F>
+void dispatch_nb_wm(uint32_t nbins, const MaskScoreParams& mp, F&& f) {
+    auto by_wm = [&](auto nbc) {
+        if (mp.wmax <= 8) {
+            f(nbc, std::integral_constant<int, 8>{});
+        } else if (mp.wmax <= 16) {
+            f(nbc, std::integral_constant<int, 16>{});
+        } else {
+            f(nbc, std::integral_constant<int, 32>{});
+        }
+    };
+    if (nbins == 32) {
+        by_wm(std::integral_constant<int, 32>{});
+    } else if (nbins == 64) {
+        by_wm(std::integral_constant<int, 64>{});
+    } else {
+        by_wm(std::integral_constant<int, 128>{});
+    }
+}
+
 // score_row with nbins dispatched to a compile-time constant when it is NB.
 template <int NB, int NW>
 __device__ __forceinline__ float score_row_any(float* r, uint32_t nbins, float inv_stdnoise,

@@ -171,33 +171,9 @@ __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
     mc_flush(a, s_cnt, s_hist2);
 }
 
-__device__ __forceinline__ float mc_fmax3(float a, float b, float c) {
-    float r;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-
-// Exact reference maximum (first maximum kept) of p[i + w] - p[i].
-__device__ __noinline__ float mc_dmax_exact(const float* r, uint32_t w, uint32_t nbins) {
-    float m = -FLT_MAX;
-    for (uint32_t i = 0; i < nbins; ++i) {
-        const float d = __fsub_rn(r[i + w], r[i]);
-        m = (m < d) ? d : m;
-    }
-    return m;
-}
-
-// The same stage for nbins NB (32, 64, 128) and strictly increasing widths of
-// at most WM bins (the mask path of the FFA's final level): the prefix row
-// through 64-bit shared-memory accesses (row stride NB + WM + 2), windows of
-// 16 positions in registers, every width a compile-time offset taken when its
-// mask bit is set, maxima by three-input max.f32 trees (a zero maximum, whose
-// sign the tree may not keep, is recomputed with the reference's rule), and
-// per width ((h + b) dmax - b sum) / stdnoise with the reference's rounding.
 template <int NB, int WM>
 __global__ void __launch_bounds__(128) mc_score_wm_kernel(McArgs a, MaskScoreParams mp) {
     constexpr int RS = NB + WM + 2;
-    constexpr int CH = 16;
     extern __shared__ float rows[];
     __shared__ unsigned int s_cnt[2 * LK_MC_MAX_THRESHOLDS + 2];
     unsigned int* s_hist2 = s_cnt + LK_MC_MAX_THRESHOLDS + 1;
@@ -222,64 +198,8 @@ __global__ void __launch_bounds__(128) mc_score_wm_kernel(McArgs a, MaskScorePar
     }
     __syncthreads();
     if (threadIdx.x < nhere) {
-        float* r = rows + static_cast<size_t>(threadIdx.x) * RS;
-        float2* r2 = reinterpret_cast<float2*>(r);
-        float acc = 0.0f;
-#pragma unroll
-        for (int j = 0; j < NB / 2; ++j) {
-            const float2 x = r2[j];
-            const float a0 = j == 0 ? x.x : __fadd_rn(acc, x.x);
-            acc = __fadd_rn(a0, x.y);
-            r2[j] = make_float2(a0, acc);
-        }
-        const float sum = acc;
-        for (uint32_t k = 0; k < mp.wmax; ++k) {
-            r[NB + k] = __fadd_rn(r[k], sum);
-        }
-        float dm[WM + 1];
-#pragma unroll
-        for (int w = 1; w <= WM; ++w) {
-            dm[w] = -FLT_MAX;
-        }
-#pragma unroll 1
-        for (int c = 0; c < NB; c += CH) {
-            float win[CH + WM];
-#pragma unroll
-            for (int k = 0; k < (CH + WM) / 2; ++k) {
-                const float2 x = r2[c / 2 + k];
-                win[2 * k] = x.x;
-                win[2 * k + 1] = x.y;
-            }
-#pragma unroll
-            for (int w = 1; w <= WM; ++w) {
-                if ((mp.wmask >> w) & 1ull) {
-                    float d[CH];
-#pragma unroll
-                    for (int k = 0; k < CH; ++k) {
-                        d[k] = __fsub_rn(win[k + w], win[k]);
-                    }
-                    const float m0 = mc_fmax3(d[0], d[1], d[2]);
-                    const float m1 = mc_fmax3(d[3], d[4], d[5]);
-                    const float m2 = mc_fmax3(d[6], d[7], d[8]);
-                    const float m3 = mc_fmax3(d[9], d[10], d[11]);
-                    const float m4 = mc_fmax3(d[12], d[13], d[14]);
-                    dm[w] = mc_fmax3(dm[w], mc_fmax3(m0, m1, m2), mc_fmax3(m3, m4, d[15]));
-                }
-            }
-        }
-        float best = -FLT_MAX;
-#pragma unroll
-        for (int w = 1; w <= WM; ++w) {
-            if ((mp.wmask >> w) & 1ull) {
-                float d = dm[w];
-                if (d == 0.0f) {
-                    d = mc_dmax_exact(r, static_cast<uint32_t>(w), NB);
-                }
-                const float base = __fsub_rn(__fmul_rn(mp.hb[w], d), __fmul_rn(mp.b[w], sum));
-                const float snr = __fdiv_rn(base, a.stdnoise);
-                best = (best < snr) ? snr : best;
-            }
-        }
+        const float best = sc::max_snr_div_wm<NB, WM>(rows + static_cast<size_t>(threadIdx.x) * RS, mp,
+                                                      a.stdnoise);
         mc_count(a, p0 + threadIdx.x, best, s_cnt, s_hist2);
     }
     __syncthreads();
@@ -407,7 +327,7 @@ void McExec::stage(const McStage& st, cudaStream_t s) {
     MaskScoreParams mp{};
     if (make_mask_score_params(m_sp, m_nbins, &mp)) {
         // the mask path: nbins 32 / 64 / 128, strictly increasing widths <= 32
-        auto go = [&](auto nbc, auto wmc) {
+        sc::dispatch_nb_wm(m_nbins, mp, [&](auto nbc, auto wmc) {
             constexpr int NB = decltype(nbc)::value;
             constexpr int WM = decltype(wmc)::value;
             auto kern = mc_score_wm_kernel<NB, WM>;
@@ -416,23 +336,7 @@ void McExec::stage(const McStage& st, cudaStream_t s) {
             sc::set_smem(kern, smem_w);
             const uint64_t bw = (st.ntrials + Tw - 1) / Tw;
             kern<<<static_cast<unsigned>(bw), Tw, smem_w, s>>>(a, mp);
-        };
-        auto by_wm = [&](auto nbc) {
-            if (mp.wmax <= 8) {
-                go(nbc, std::integral_constant<int, 8>{});
-            } else if (mp.wmax <= 16) {
-                go(nbc, std::integral_constant<int, 16>{});
-            } else {
-                go(nbc, std::integral_constant<int, 32>{});
-            }
-        };
-        if (m_nbins == 32) {
-            by_wm(std::integral_constant<int, 32>{});
-        } else if (m_nbins == 64) {
-            by_wm(std::integral_constant<int, 64>{});
-        } else {
-            by_wm(std::integral_constant<int, 128>{});
-        }
+        });
     } else {
         sc::dispatch_nw_nb(m_sp.nwidths, m_nbins, [&](auto nw, auto nbc) {
             launch(mc_score_kernel<decltype(nw)::value, decltype(nbc)::value>);
