@@ -1148,6 +1148,12 @@ __global__ void parent_transform_kernel(double* __restrict__ tree_leaves, uint64
 constexpr uint32_t kTailBatches = 64;    // batches of one level (wrap splits included)
 constexpr uint64_t kTailParents = 16384;  // largest level (parents) the tail runs
 constexpr uint64_t kTailChildren = 1 << 17;  // most children of one tail level
+// Block 0 alone runs a tree's levels once a level has at most this many
+// parents and the level before at most this many children; a level with more
+// than kTailSoloMaxParents parents then goes back to the host.
+constexpr uint64_t kTailSoloParents = 64;
+constexpr uint64_t kTailSoloChildren = 256;
+constexpr uint64_t kTailSoloMaxParents = 1024;
 constexpr uint32_t kTailExitNone = 0;
 constexpr uint32_t kTailExitDone = 1;    // every level run, or the tree emptied
 constexpr uint32_t kTailExitHandBack = 2;  // level `level` too large: host continues
@@ -1176,6 +1182,7 @@ struct TailCtl {
     float thr;
     uint64_t n_par, n_child, write_start;
     uint64_t bstart[kTailBatches + 1], bsize[kTailBatches], cstart[kTailBatches + 1];
+    uint32_t active;       // 0: all the tree's blocks; 1: block 0 alone (small levels)
 };
 
 struct TailArgs {
@@ -1274,6 +1281,8 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
     TailCtl* ctl = a.ctl;
     // values other blocks wrote before a barrier are read through vc
     volatile TailCtl* vc = a.ctl;
+    // blocks taking part in the tree's barriers (all, until the tree is small)
+    uint32_t nblk = vc->active != 0 ? vc->active : bpt;
     const LeafGeom& g = a.geom;
     const uint32_t np = g.np, ls = g.ls, nb = g.nbins;
     const uint64_t cap = a.cap;
@@ -1300,7 +1309,12 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
                     done += take;
                     ++nbat;
                 }
-                if (done < n_par) {
+                if (ctl->active == 0 && n_par <= kTailSoloParents && ctl->n_child <= kTailSoloChildren) {
+                    // a small tree: the other blocks leave, block 0 runs the
+                    // remaining levels alone (block barriers, no grid waits)
+                    ctl->active = 1;
+                }
+                if (done < n_par || (ctl->active == 1 && n_par > kTailSoloMaxParents)) {
                     ctl->exit = kTailExitHandBack;
                 } else {
                     ctl->bstart[nbat] = n_par;
@@ -1313,8 +1327,12 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
                 }
             }
         }
-        if (!tail_barrier(ctl, bpt) || vc->exit != kTailExitNone) {
+        if (!tail_barrier(ctl, nblk) || vc->exit != kTailExitNone) {
             return;
+        }
+        nblk = vc->active != 0 ? vc->active : bpt;
+        if (lb >= nblk) {
+            return;  // the level runs on fewer blocks from here on
         }
         const uint32_t lv = vc->level;
         const TailLevel& L = a.lconst[lv];
@@ -1322,7 +1340,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
         const int cur = static_cast<int>(vc->cur);
         const double* tree = a.tleaves[cur];
         const uint64_t gtid = static_cast<uint64_t>(lb) * blockDim.x + threadIdx.x;
-        const uint64_t gthreads = static_cast<uint64_t>(bpt) * blockDim.x;
+        const uint64_t gthreads = static_cast<uint64_t>(nblk) * blockDim.x;
 
         // 1. branch counts (Chebyshev: parents re-centred into tp, the tree
         //    is not written, so a hand-back leaves it as it was)
@@ -1349,7 +1367,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
             }
             a.counts[i] = static_cast<uint32_t>(prod);
         }
-        if (!tail_barrier(ctl, bpt)) {
+        if (!tail_barrier(ctl, nblk)) {
             return;
         }
         // 2. offsets, batch child ranges, checks (block 0)
@@ -1403,7 +1421,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
                 }
             }
         }
-        if (!tail_barrier(ctl, bpt) || vc->exit != kTailExitNone) {
+        if (!tail_barrier(ctl, nblk) || vc->exit != kTailExitNone) {
             return;
         }
         const uint64_t n_child = vc->n_child;
@@ -1437,18 +1455,18 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
                 }
             }
         }
-        if (!tail_barrier(ctl, bpt)) {
+        if (!tail_barrier(ctl, nblk)) {
             return;
         }
         // 4. resolve, shift-add, score, kept folds (tiles of blockDim children)
         for (uint64_t c0 = static_cast<uint64_t>(lb) * blockDim.x; c0 < n_child;
-             c0 += static_cast<uint64_t>(bpt) * blockDim.x) {
+             c0 += static_cast<uint64_t>(nblk) * blockDim.x) {
             leaf_tile<NW, NB>(rows, c0, a.cleaves, a.cparent, n_child, a.tfolds[cur], head, cap, L.seg,
                               g, L.rc, a.rs, a.sp, L.threshold, a.cscores, a.cfolds,
                               a.level_mm + 2 * lv);
             __syncthreads();
         }
-        if (!tail_barrier(ctl, bpt)) {
+        if (!tail_barrier(ctl, nblk)) {
             return;
         }
         // 5. filter + add in the reference's batch order (block 0)
@@ -1504,7 +1522,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
                 ctl->thr = thr;
             }
         }
-        if (!tail_barrier(ctl, bpt)) {
+        if (!tail_barrier(ctl, nblk)) {
             return;
         }
         // 6. survivors transformed and gathered into the other tree buffer
@@ -1519,7 +1537,7 @@ __global__ void __launch_bounds__(128) prune_tail_kernel(const TailArgs* __restr
                            nb, L.tc, a.tleaves[nxt], a.tfolds[nxt], a.tscores[nxt]);
             }
         }
-        if (!tail_barrier(ctl, bpt)) {
+        if (!tail_barrier(ctl, nblk)) {
             return;
         }
         // 7. the level's end (finalize_in_place_update) and its statistics
