@@ -507,13 +507,42 @@ def run_prune(args, rank, world, local_rank):
             cpu = {"value": cv, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": f"reference pruning run (ref_seg {ref_seg}) over its first {k} levels "
                              f"({el:.1f} s), single thread, on the same FFA fold"}
+    parity = None
+    if rank == 0 and not args.no_parity:
+        # the last run against the C oracle (pinned to the reference's own
+        # pruning by the golden fixtures): FFA fold, every level's statistics
+        # and the final tree, bit for bit, at full size
+        from oracle import lko
+        from loki_b200.prune import branching_pattern
+
+        t0 = time.perf_counter()
+        op = lko.plan_create(lko.make_cfg(p["nsamps"], p["tsamp"], nbins, p["eta"], p["param_limits"],
+                                          bseg_ffa=p["bseg_ffa"]))
+        want_fold = lko.ffa(op, ts_e, ts_v)
+        got_fold = fold.cpu().numpy()
+        bm = max(int(np.ceil(branching_pattern(cfg, 0, False, args.basis).max() * 2)), 32)
+        want = lko.prune_run(op, want_fold, thr, ref_seg, PRUNE_MAX_SUGG, PRUNE_BATCH, bm, nseg - 1,
+                             basis=args.basis)
+        lv, fo, sc = pr.tree()
+        fields = ("level", "seg_idx", "n_branches", "n_leaves", "n_leaves_phy", "n_leaves_surv", "threshold",
+                  "score_min", "score_max")
+        parity = {
+            "checked": True, "vs": "C oracle (pinned to the reference's pruning by golden fixtures), full size",
+            "ffa_fold_bits_equal": bool(np.array_equal(got_fold.view(np.uint32), want_fold.view(np.uint32))),
+            "level_stats_equal": bool(all(np.array_equal(stats[k], want[0][k]) for k in fields)),
+            "tree_bits_equal": bool(np.array_equal(lv.view(np.uint64), want[1].view(np.uint64)) and
+                                    np.array_equal(fo.view(np.uint32), want[2].view(np.uint32)) and
+                                    np.array_equal(sc.view(np.uint32), want[3].view(np.uint32))),
+            "survivors": int(lv.shape[0]), "oracle_seconds": time.perf_counter() - t0}
+        parity["candidates_match"] = (parity["ffa_fold_bits_equal"] and parity["level_stats_equal"] and
+                                      parity["tree_bits_equal"])
     if rank == 0:
         B.emit(_line(
             args, world, "prune_jerk_2^23x64us_nbins32", value, ms,
             dict(_prune_cfgd(p, nseg, ref_seg, widths), poly_basis=args.basis, leaves_scored=leaves,
                  survivors=int(stats["n_leaves_surv"][-1]), levels_run=int(len(stats) - 1), ffa_tuning=tuning),
             roofline=_roofline("prune_run", algo, prune_ms), cpu_baseline=cpu, e2e=e2e,
-            clocks=clk, stages={"ffa_ms": ms - prune_ms, "prune_ms": prune_ms},
+            clocks=clk, stages={"ffa_ms": ms - prune_ms, "prune_ms": prune_ms}, parity=parity,
             level_stats=[{k: (float(r[k]) if k in ("threshold", "score_min", "score_max") else int(r[k]))
                           for k in ("level", "n_branches", "n_leaves", "n_leaves_surv", "threshold", "score_max")}
                          for r in stats]))
@@ -619,11 +648,33 @@ def run_mc(args, rank, world, local_rank):
         cpu = {"value": cv, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"the first {nsub} profiles through all stages ({el:.1f} s), C oracle restatement "
                          f"(the reference's thresholds.cpp needs HDF5 and cannot be linked here), one thread"}
+    parity = None
+    if rank == 0 and not args.no_parity:
+        # every stage's alive / kept counts and grid counts against the C
+        # oracle at full size (2^20 profiles, 8 stages), through the public
+        # cascade driver
+        from oracle import lko
+        from loki_b200.thresholds import mc_cascade
+
+        t0 = time.perf_counter()
+        got = mc_cascade(folds0, signal, noises, cls, MC_WIDTHS, thresholds, grids)
+        fin, rws, var, ok = folds0, np.arange(n0, dtype=np.uint32), 1.0, len(got) == len(noises)
+        for s_, g in enumerate(got):
+            f, ids, counts, _ = lko.mc_stage(fin, noises[s_], signal, var, var, MC_WIDTHS.astype(np.uint64),
+                                             thresholds[s_], grids[s_], signal_scale=float(2 ** s_), rowmap=rws,
+                                             cls=cls)
+            ng = len(grids[s_])
+            ok = ok and (g["alive"], g["kept"]) == (rws.size, ids.size)
+            ok = ok and np.array_equal(g["counts"].astype(np.uint64), counts[:ng])
+            ok = ok and np.array_equal(g["counts_flagged"].astype(np.uint64), counts[ng:])
+            fin, rws, var = f, ids, 2 * var
+        parity = {"checked": True, "vs": "C oracle (pinned to the reference's per-profile decision), full size",
+                  "candidates_match": bool(ok), "stages": len(got), "oracle_seconds": time.perf_counter() - t0}
     if rank == 0:
         B.emit(_line(args, world, "mc_cascade_2^20x64_8stages", value, ms,
                                dict(cfgd, trials_per_step=trials),
                                roofline=_roofline("mc_stage", sum(stage_bytes), ms), cpu_baseline=cpu, e2e=e2e,
-                               gpu_launches=args.steps * len(stage_bytes) * 5, clocks=clk))
+                               gpu_launches=args.steps * len(stage_bytes) * 5, clocks=clk, parity=parity))
     _finish(dist)
     return 0
 
