@@ -359,11 +359,26 @@ def run_octaves(args, rank, world, local_rank):
             cpu = {"value": ntrials / med, "unit": UNIT, "cores": nthreads, "kind": "reference",
                    "sample": f"full sweep, median of 3 runs ({med:.3f} s each) of the reference's FFA::execute + "
                              "snr_boxcar_3d + compaction per chunk, Release flags"}
+    parity = None
+    if rank == 0 and not args.no_parity:
+        # the decoded candidates (parameter sets and S/N bits) against the C
+        # oracle's sweep over the same chunks, full size
+        from oracle import sweep as osweep
+
+        t0 = time.perf_counter()
+        o_params, o_snr, o_counts = osweep.run(
+            (params["nsamps"], params["tsamp"], params["nbins"], params["eta"], params["param_limits"]), rows,
+            ts_e, ts_v, B.SNR_MIN, score_widths=params["score_widths"])
+        same = bool(np.array_equal(params_out, o_params) and
+                    np.array_equal(np.asarray(snr_out, np.float32).view(np.uint32), o_snr.view(np.uint32)))
+        parity = {"checked": True, "vs": "C oracle sweep (pinned to the reference's FFA and scorer), full size",
+                  "candidates_match": same, "n": int(snr_out.size), "n_ref": int(o_snr.size),
+                  "oracle_seconds": time.perf_counter() - t0}
     if rank == 0:
         B.emit(_line(args, world, name, value, ms,
                      dict(cfgd, final_cells=ntrials // nw, candidates=int(snr_out.size), fold_storage=args.storage),
                      roofline=_roofline(dom, prof[dom][1], prof[dom][0]), cpu_baseline=cpu, e2e=e2e,
-                     gpu_launches=args.steps * launches, clocks=clk,
+                     gpu_launches=args.steps * launches, clocks=clk, parity=parity,
                      stages={k: {"ms": p[0], "bytes": p[1], "launches": p[2]} for k, p in prof.items()}))
     _finish(dist)
     return 0
