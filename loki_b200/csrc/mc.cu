@@ -184,16 +184,44 @@ __global__ void __launch_bounds__(128) mc_score_wm_kernel(McArgs a, MaskScorePar
     for (uint32_t k = threadIdx.x; k < 2 * LK_MC_MAX_THRESHOLDS + 2; k += T) {
         s_cnt[k] = 0;
     }
-#pragma unroll 2
-    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
-        float* dst = rows + static_cast<size_t>(p) * RS;
-        float* keep = a.stage_folds + (p0 + p) * NB;
-        const TrialRows tr = trial_rows(a, p0 + p, lane == 0);
+    // Phase 1: a warp takes PB trials at a time, lanes over bins; lane q
+    // looks up trial q's rows, then every row load of the PB trials is in
+    // flight before the first value is formed.
+    constexpr int NJ = NB / kWarp;  // bins per lane
+    constexpr int PB = NB == 128 ? 4 : 8;
+    for (uint32_t pw = warp * PB; pw < nhere; pw += (T / kWarp) * PB) {
+        TrialRows mine{0, 0};
+        if (lane < static_cast<uint32_t>(PB) && pw + lane < nhere) {
+            mine = trial_rows(a, p0 + pw + lane, true);
+        }
+        float xin[PB][NJ], xnz[PB][NJ], xsg[PB][NJ];
 #pragma unroll
-        for (int j0 = 0; j0 < NB; j0 += kWarp) {
-            const float x = stage_value(a, tr, j0 + lane);
-            dst[j0 + lane] = x;
-            keep[j0 + lane] = x;
+        for (int q = 0; q < PB; ++q) {
+            const uint64_t rin = __shfl_sync(0xffffffffu, mine.in, q);
+            const uint64_t rnz = __shfl_sync(0xffffffffu, mine.noise, q);
+            const float* sg = a.signal + (a.per_trial ? rnz * NB : 0);
+#pragma unroll
+            for (int u = 0; u < NJ; ++u) {
+                const uint32_t j = lane + kWarp * u;
+                // rows of trials past nhere are row 0 of each buffer (in range, unused)
+                xin[q][u] = __ldg(a.in + rin * NB + j);
+                xnz[q][u] = __ldg(a.noise + rnz * NB + j);
+                xsg[q][u] = __ldg(sg + j);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PB; ++q) {
+            if (pw + q < nhere) {
+                float* dst = rows + static_cast<size_t>(pw + q) * RS;
+                float* keep = a.stage_folds + (p0 + pw + q) * NB;
+#pragma unroll
+                for (int u = 0; u < NJ; ++u) {
+                    // (in + noise) + signal * scale, the reference's order
+                    const float x = __fadd_rn(__fadd_rn(xin[q][u], xnz[q][u]), __fmul_rn(xsg[q][u], a.scale));
+                    dst[lane + kWarp * u] = x;
+                    keep[lane + kWarp * u] = x;
+                }
+            }
         }
     }
     __syncthreads();
