@@ -540,21 +540,48 @@ __device__ __forceinline__ void leaf_tile(float* rows, uint64_t c0, const double
     }
     __syncthreads();
     const uint32_t warp = threadIdx.x / kWarp, lane = threadIdx.x % kWarp;
-    for (uint32_t p = warp; p < nhere; p += T / kWarp) {
-        const float* tail = tree_folds + static_cast<uint64_t>(s_tree[p]) * 2 * nb;
-        const float* hd = ffa_seg + static_cast<uint64_t>(s_pidx[p]) * 2 * nb;
-        const uint32_t s = s_shift[p];
-        float* dst = rows + static_cast<size_t>(p) * rs;
-        if constexpr (NB > 0) {
-            // nbins == NB, a multiple of 32: masked rotation, no bounds test
+    if constexpr (NB > 0) {
+        // nbins == NB, a multiple of 32: masked rotation, no bounds test; a
+        // warp takes PB children at a time with all their row loads in flight
+        constexpr int NJ = NB / static_cast<int>(kWarp);
+        constexpr int PB = NB == 128 ? 2 : 4;
+        for (uint32_t p0 = warp * PB; p0 < nhere; p0 += (T / kWarp) * PB) {
+            float te[PB][NJ], tv[PB][NJ], he[PB][NJ], hv[PB][NJ];
 #pragma unroll
-            for (uint32_t j = lane; j < static_cast<uint32_t>(NB); j += kWarp) {
-                const float* ph = hd + ((j - s) & (NB - 1));
-                const float e = __fadd_rn(__ldg(tail + j), __ldg(ph));
-                const float v = __fadd_rn(__ldg(tail + NB + j), __ldg(ph + NB));
-                dst[j] = sc::normalise(e, v);
+            for (int q = 0; q < PB; ++q) {
+                // children past nhere load the block's first child (in range, unused)
+                const uint32_t p = p0 + q < nhere ? p0 + q : p0;
+                const float* tail = tree_folds + static_cast<uint64_t>(s_tree[p]) * 2 * NB;
+                const float* hd = ffa_seg + static_cast<uint64_t>(s_pidx[p]) * 2 * NB;
+                const uint32_t s = s_shift[p];
+#pragma unroll
+                for (int u = 0; u < NJ; ++u) {
+                    const uint32_t j = lane + kWarp * u;
+                    const float* ph = hd + ((j - s) & (NB - 1));
+                    te[q][u] = __ldg(tail + j);
+                    tv[q][u] = __ldg(tail + NB + j);
+                    he[q][u] = __ldg(ph);
+                    hv[q][u] = __ldg(ph + NB);
+                }
             }
-        } else {
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+                if (p0 + q < nhere) {
+                    float* dst = rows + static_cast<size_t>(p0 + q) * rs;
+#pragma unroll
+                    for (int u = 0; u < NJ; ++u) {
+                        dst[lane + kWarp * u] =
+                            sc::normalise(__fadd_rn(te[q][u], he[q][u]), __fadd_rn(tv[q][u], hv[q][u]));
+                    }
+                }
+            }
+        }
+    } else {
+        for (uint32_t p = warp; p < nhere; p += T / kWarp) {
+            const float* tail = tree_folds + static_cast<uint64_t>(s_tree[p]) * 2 * nb;
+            const float* hd = ffa_seg + static_cast<uint64_t>(s_pidx[p]) * 2 * nb;
+            const uint32_t s = s_shift[p];
+            float* dst = rows + static_cast<size_t>(p) * rs;
             for (uint32_t j = lane; j < nb; j += kWarp) {
                 const uint32_t jh = j >= s ? j - s : j + nb - s;
                 const float e = __fadd_rn(__ldg(tail + j), __ldg(hd + jh));
