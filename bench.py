@@ -60,6 +60,8 @@ def parse():
                     help="skip the BF16-storage + batched measurement beside the plain FP32 line")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own GPU path (oracle/_ref/libloki_ref_cuda.so)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the short runs of the other workloads summarised under `configs`")
     ap.add_argument("--reference-gpu-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--pipeline-execs", type=int, default=2,
                     help="executors (own compute streams) the end-to-end search pipeline alternates between")
@@ -622,6 +624,10 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu(args, step_ms_max, ffa.scores(e, v).cpu().numpy())
 
+    others = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        others = other_configs()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -633,7 +639,7 @@ def run_ours(args, rank, world, local_rank):
                                            "tuning": tuning}),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "stages": stages, "wall_s": wall, "parity": parity, "reference_gpu": ref_gpu,
-            "mixed_batched": mb,
+            "mixed_batched": mb, "configs": others,
         }
         emit(line)
         if parity is not None and parity.get("checked") and not parity["candidates_match"]:
@@ -643,6 +649,54 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return status
+
+
+# The other benchmark workloads, each run once in its own process after the
+# headline's timed region (steps, warm-up): the plain period sweep (2^21
+# samples, nbins 128), the jerk pruning run (2^23 samples, 31 levels), 512
+# series of uneven length, the 8-stage Monte-Carlo cascade, the octave sweep,
+# the beam search and the Fourier-domain search.
+OTHER_CONFIGS = (("freq_sweep", 5, 3), ("prune_jerk", 5, 3), ("multi_series", 1, 3), ("mc_cascade", 5, 3),
+                 ("octave_sweep", 3, 3), ("beam_scheme", 3, 3), ("fourier_accel", 5, 3))
+OTHER_TIMEOUT_S = 300
+
+
+def other_configs():
+    """Runs each workload of OTHER_CONFIGS as `bench.py --workload W` (no CPU
+    baseline) and keeps the parts of its line that describe it: value,
+    step time, end-to-end rate, clocks and its full-size parity fields."""
+    out = {}
+    for name, steps, warmup in OTHER_CONFIGS:
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", name, "--steps", str(steps),
+               "--warmup", str(warmup), "--no-cpu-baseline"]
+        t0 = time.perf_counter()
+        try:
+            r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                               timeout=OTHER_TIMEOUT_S, cwd=ROOT)
+        except subprocess.TimeoutExpired:
+            out[name] = {"rc": None, "error": f"timed out after {OTHER_TIMEOUT_S} s"}
+            continue
+        rec = {"rc": r.returncode, "wall_s": round(time.perf_counter() - t0, 1)}
+        line = None
+        for ln in r.stdout.splitlines():
+            if ln.startswith('{"metric"'):
+                line = json.loads(ln)
+        if line is None:
+            tail = r.stderr.strip().splitlines()[-1:] or [""]
+            rec["error"] = tail[0][-300:]
+        else:
+            e2e = line.get("e2e")
+            cfg = line.get("config") or {}
+            rec.update({
+                "workload": cfg.get("workload"), "metric": line.get("metric"), "value": line.get("value"),
+                "unit": line.get("unit"), "ms_per_step": line.get("ms_per_step"), "steps": line.get("steps"),
+                "warmup": line.get("warmup"), "dtype": line.get("dtype"),
+                "e2e": e2e.get("value") if isinstance(e2e, dict) else None,
+                "parity": line.get("parity"),
+                "clocks": line.get("clocks"),
+            })
+        out[name] = rec
+    return out
 
 
 _JSON_OUT = None
