@@ -37,6 +37,7 @@ from __future__ import annotations
 
 import json
 import os
+import sys
 import time
 
 import numpy as np
@@ -789,6 +790,34 @@ def run_multi(args, rank, world, local_rank):
             cpu = {"value": cv, "unit": UNIT, "cores": nthreads, "kind": "reference",
                    "sample": f"{npick} series spread over the lengths, one FFA + scores + compaction each "
                              f"({el:.1f} s), reference CPU code with its Release flags"}
+    parity = None
+    if rank == 0 and not args.no_parity:
+        # eight series spread over the lengths and four of those carrying a
+        # pulsar (every eighth series; the last timed step's candidates)
+        # against the reference's CPU code on the padded series
+        picked = sorted(range(len(data)), key=lambda k: lens[k])[:: max(1, len(data) // 8)][:8]
+        pulsars = sorted(range(0, len(data), 8), key=lambda k: lens[k])
+        picked += [k for k in pulsars[:: max(1, len(pulsars) // 4)][:4] if k not in picked]
+        checks = []
+        for k in picked:
+            e, v = data[k]
+            L = _pow2_ceil(e.size)
+            ep, vp = np.zeros(L, np.float32), np.zeros(L, np.float32)
+            ep[: e.size], vp[: e.size] = e, v
+            params = dict(nsamps=L, tsamp=p["tsamp"], nbins=p["nbins"], eta=p["eta"],
+                          param_limits=[list(p["f_range"])], score_widths=p["widths"])
+            r = outs[-1][k]
+            checks.append(B.candidate_parity(params, ep, vp, r["idx"].astype(np.int64), r["snr"]))
+        if all(c.get("checked") for c in checks):
+            parity = {"checked": True, "vs": checks[0]["vs"], "series": [int(k) for k in picked],
+                      "lengths": [lens[k] for k in picked],
+                      "candidates_equal": all(c["candidates_equal"] for c in checks),
+                      "snr_bits_equal": all(c["snr_bits_equal"] for c in checks),
+                      "candidates_match": all(c["candidates_match"] for c in checks),
+                      "n": sum(c["n"] for c in checks), "n_ref": sum(c["n_ref"] for c in checks),
+                      "ref_seconds": sum(c["ref_seconds"] for c in checks)}
+        else:
+            parity = checks[0] if checks else None
     groups = {str(L): {"series": sum(1 for n in lens if _pow2_ceil(n) == L), "batch": ms.groups[L][0].nbatch,
                        "slots": len(ms.groups[L]), "trials_per_series": ms.groups[L][0].per}
               for L in sorted(ms.groups)}
@@ -797,8 +826,11 @@ def run_multi(args, rank, world, local_rank):
                                dict(cfgd, trials_per_step=trials, candidates=ncand, groups=groups,
                                     graphs="one CUDA graph per length for full batches",
                                     fold_storage=args.storage),
-                               cpu_baseline=cpu, e2e=e2e, clocks=clk))
+                               cpu_baseline=cpu, e2e=e2e, clocks=clk, parity=parity))
     _finish(dist)
+    if parity is not None and parity.get("checked") and not parity["candidates_match"]:
+        print("bench: the batched search's candidates differ from the reference's", file=sys.stderr)
+        return 1
     return 0
 
 
