@@ -938,6 +938,27 @@ def run_dts(args, rank, world, local_rank):
         cpu = {"value": v, "unit": unit, "cores": 1, "kind": "port",
                "sample": f"the first 4 stages through the reference's stage loop restated over its own pieces "
                          f"({how}; thresholds.cpp itself needs HDF5), single thread, {el:.1f} s"}
+    parity = None
+    if rank == 0 and not args.no_parity:
+        # the first stages of the last timed run, every State field bit for
+        # bit, against the C oracle (pinned to the reference's stage loop by
+        # golden fixtures); a stage depends only on the ones before it
+        from oracle import lko
+
+        nst = 4
+        t0 = time.perf_counter()
+        want = lko.dts_run(bp, **kw, thres_neigh=neigh, stages_run=nst)
+        secs = time.perf_counter() - t0
+        got = dts.get_states()
+        ok = True
+        for fld in (f for f in lko.DTS_STATE_DTYPE.names if f != "_pad"):
+            x = np.asarray(got[fld]).reshape(bp.size, -1)[:nst]
+            y = np.asarray(want[fld]).reshape(bp.size, -1)[:nst]
+            if x.dtype == np.float32:
+                x, y = x.view(np.uint32), y.astype(np.float32).view(np.uint32)
+            ok = ok and bool(np.array_equal(x, y))
+        parity = {"checked": True, "vs": "C oracle (pinned to the reference's stage loop by golden fixtures)",
+                  "stages": nst, "states_bits_equal": ok, "candidates_match": ok, "oracle_seconds": secs}
     e2e = None
     if not args.no_e2e:
         t0 = time.perf_counter()
@@ -952,10 +973,13 @@ def run_dts(args, rank, world, local_rank):
     if rank == 0:
         line = _line(args, world, "beam_scheme_16stages_nbins64_1024trials", value, ms,
                      dict(cfgd, transitions=int(outs[-1])), cpu_baseline=cpu, e2e=e2e, clocks=clk,
-                     gpu_launches=1 + 4 * int(bp.size))
+                     gpu_launches=1 + 4 * int(bp.size), parity=parity)
         line["metric"], line["unit"] = metric, unit
         B.emit(line)
     _finish(dist)
+    if parity is not None and not parity["candidates_match"]:
+        print("bench: the beam search's states differ from the oracle's", file=sys.stderr)
+        return 1
     return 0
 
 
