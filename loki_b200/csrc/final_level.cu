@@ -70,10 +70,17 @@ __device__ __noinline__ float dmax_exact(const float* r, uint32_t w, uint32_t nb
     return m;
 }
 
+// Width mask of the widths {1, 2, 3, 4, 6, 8, 12, 16}, compiled in as a
+// constant so that the width bodies not taken are not generated at all.
+constexpr uint64_t kFixedMask16 = (1ull << 1) | (1ull << 2) | (1ull << 3) | (1ull << 4) | (1ull << 6) |
+                                  (1ull << 8) | (1ull << 12) | (1ull << 16);
+
 // WM: largest width the kernel handles (8, 16 or 32; the width mask has no
 // bit above it), so only WM width bodies are generated. CH: window chunk.
 // TAB: 1 / sqrt(V) from the table where V is an exact integer inside it.
-template <bool TAYLOR, int NB, int PB, class TIn, int WM, bool TAB>
+// FM: the width mask as a compile-time constant (mp.wmask == FM), or 0 to
+// test mp.wmask at run time.
+template <bool TAYLOR, int NB, int PB, class TIn, int WM, bool TAB, uint64_t FM>
 __global__ void __launch_bounds__(128, 5)
     merge_score_wm_kernel(const TIn* __restrict__ in, const void* __restrict__ coords,
                           uint32_t n_inner, uint32_t n_outer, uint64_t nprev, MaskScoreParams mp,
@@ -204,8 +211,19 @@ __global__ void __launch_bounds__(128, 5)
             r2[j] = make_float2(a0, acc);
         }
         const float sum = acc;
-        for (uint32_t k = 0; k < mp.wmax; ++k) {
-            r[NB + k] = __fadd_rn(r[k], sum);
+        auto taken = [&](int w) -> bool {
+            return FM != 0 ? ((FM >> w) & 1ull) != 0 : ((mp.wmask >> w) & 1ull) != 0;
+        };
+        if constexpr (FM != 0) {
+            static_assert((FM >> (WM + 1)) == 0 && ((FM >> WM) & 1ull), "fixed mask's widest width is WM");
+#pragma unroll
+            for (int k = 0; k < WM; ++k) {
+                r[NB + k] = __fadd_rn(r[k], sum);
+            }
+        } else {
+            for (uint32_t k = 0; k < mp.wmax; ++k) {
+                r[NB + k] = __fadd_rn(r[k], sum);
+            }
         }
         float dm[WM + 1];
 #pragma unroll
@@ -225,7 +243,7 @@ __global__ void __launch_bounds__(128, 5)
             }
 #pragma unroll
             for (int w = 1; w <= WM; ++w) {
-                if ((mp.wmask >> w) & 1ull) {
+                if (taken(w)) {
                     // the chunk's 16 differences and the running maximum
                     // in a tree of three-input maxima (depth 3)
                     float d[CH];
@@ -249,7 +267,7 @@ __global__ void __launch_bounds__(128, 5)
         float best = -FLT_MAX;
 #pragma unroll
         for (int w = 1; w <= WM; ++w) {
-            if ((mp.wmask >> w) & 1ull) {
+            if (taken(w)) {
                 float d = dm[w];
                 if (d == 0.0f) {
                     d = dmax_exact(r, static_cast<uint32_t>(w), NB);
@@ -376,6 +394,7 @@ void merge_score_level_wm(const void* d_in, const void* d_coords, bool taylor, u
             "final level too large for the launch grid");
     const auto blocks = static_cast<unsigned>(tiles * n_outer);
     require(d_tab != nullptr || !use_table, "internal: no normalisation table");
+    const bool fixed16 = mp.wmask == kFixedMask16 && mp.wmax == 16;
     auto go2 = [&](auto tg, auto tin, auto nbc, auto wmc, auto tabc) {
         constexpr bool TG = decltype(tg)::value;
         using TI = decltype(tin);
@@ -383,7 +402,12 @@ void merge_score_level_wm(const void* d_in, const void* d_coords, bool taylor, u
         constexpr int WM = decltype(wmc)::value;
         constexpr bool TB = decltype(tabc)::value;
         constexpr int PB = NB == 128 ? 4 : 8;
-        auto kern = merge_score_wm_kernel<TG, NB, PB, TI, WM, TB>;
+        auto kern = merge_score_wm_kernel<TG, NB, PB, TI, WM, TB, 0>;
+        if constexpr (WM == 16) {
+            if (fixed16) {
+                kern = merge_score_wm_kernel<TG, NB, PB, TI, WM, TB, kFixedMask16>;
+            }
+        }
         const size_t smem = static_cast<size_t>(T) * (NB + WM + 2) * sizeof(float);
         sc::set_smem(kern, smem);
         kern<<<dim3(blocks, static_cast<unsigned>(nbatch)), T, smem, s>>>(
