@@ -70,10 +70,7 @@ __device__ __noinline__ float dmax_exact(const float* r, uint32_t w, uint32_t nb
     return m;
 }
 
-// Width mask of the widths {1, 2, 3, 4, 6, 8, 12, 16}, compiled in as a
-// constant so that the width bodies not taken are not generated at all.
-constexpr uint64_t kFixedMask16 = (1ull << 1) | (1ull << 2) | (1ull << 3) | (1ull << 4) | (1ull << 6) |
-                                  (1ull << 8) | (1ull << 12) | (1ull << 16);
+using sc::kFixedMask16;
 
 // WM: largest width the kernel handles (8, 16 or 32; the width mask has no
 // bit above it), so only WM width bodies are generated. CH: window chunk.

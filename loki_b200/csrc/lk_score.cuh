@@ -217,7 +217,10 @@ __device__ __noinline__ inline float dmax_first(const float* r, uint32_t w, uint
 // taken when its mask bit is set, and each width's maximum by a tree of
 // three-input maxima (equal in value to the reference's scan; a zero
 // maximum, whose sign the tree may not keep, is recomputed with its rule).
-template <int NB, int WM>
+// FM: the width mask as a compile-time constant (mp.wmask == FM; its widest
+// width WM), so that the width bodies not taken are not generated, or 0 to
+// test mp.wmask at run time.
+template <int NB, int WM, uint64_t FM = 0>
 __device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams& mp, float stdnoise) {
     constexpr int CH = 16;
     static_assert(NB % CH == 0 && WM <= 32, "masked scorer shape");
@@ -231,8 +234,19 @@ __device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams&
         r2[j] = make_float2(a0, acc);
     }
     const float sum = acc;
-    for (uint32_t k = 0; k < mp.wmax; ++k) {
-        r[NB + k] = __fadd_rn(r[k], sum);
+    auto taken = [&](int w) -> bool {
+        return FM != 0 ? ((FM >> w) & 1ull) != 0 : ((mp.wmask >> w) & 1ull) != 0;
+    };
+    if constexpr (FM != 0) {
+        static_assert((FM >> (WM + 1)) == 0 && ((FM >> WM) & 1ull), "fixed mask's widest width is WM");
+#pragma unroll
+        for (int k = 0; k < WM; ++k) {
+            r[NB + k] = __fadd_rn(r[k], sum);
+        }
+    } else {
+        for (uint32_t k = 0; k < mp.wmax; ++k) {
+            r[NB + k] = __fadd_rn(r[k], sum);
+        }
     }
     float dm[WM + 1];
 #pragma unroll
@@ -250,7 +264,7 @@ __device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams&
         }
 #pragma unroll
         for (int w = 1; w <= WM; ++w) {
-            if ((mp.wmask >> w) & 1ull) {
+            if (taken(w)) {
                 float d[CH];
 #pragma unroll
                 for (int k = 0; k < CH; ++k) {
@@ -268,7 +282,7 @@ __device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams&
     float best = -FLT_MAX;
 #pragma unroll
     for (int w = 1; w <= WM; ++w) {
-        if ((mp.wmask >> w) & 1ull) {
+        if (taken(w)) {
             float d = dm[w];
             if (d == 0.0f) {
                 d = dmax_first(r, static_cast<uint32_t>(w), NB);
@@ -280,6 +294,11 @@ __device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams&
     }
     return best;
 }
+
+// Width mask of the widths {1, 2, 3, 4, 6, 8, 12, 16} (the benchmark widths),
+// for the compile-time mask form of the masked scorers.
+constexpr uint64_t kFixedMask16 = (1ull << 1) | (1ull << 2) | (1ull << 3) | (1ull << 4) | (1ull << 6) |
+                                  (1ull << 8) | (1ull << 12) | (1ull << 16);
 
 // Calls f(NB, WM) for the masked scorer's shape of (nbins, mp) -- NB 32 / 64 /
 // 128, WM the width bucket 8 / 16 / 32.

@@ -171,7 +171,7 @@ __global__ void mc_score_kernel(McArgs a, uint32_t rs, ScoreParams sp) {
     mc_flush(a, s_cnt, s_hist2);
 }
 
-template <int NB, int WM>
+template <int NB, int WM, uint64_t FM>
 __global__ void __launch_bounds__(128) mc_score_wm_kernel(McArgs a, MaskScoreParams mp) {
     constexpr int RS = NB + WM + 2;
     extern __shared__ float rows[];
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(128) mc_score_wm_kernel(McArgs a, MaskScorePar
     }
     __syncthreads();
     if (threadIdx.x < nhere) {
-        const float best = sc::max_snr_div_wm<NB, WM>(rows + static_cast<size_t>(threadIdx.x) * RS, mp,
+        const float best = sc::max_snr_div_wm<NB, WM, FM>(rows + static_cast<size_t>(threadIdx.x) * RS, mp,
                                                       a.stdnoise);
         mc_count(a, p0 + threadIdx.x, best, s_cnt, s_hist2);
     }
@@ -358,7 +358,12 @@ void McExec::stage(const McStage& st, cudaStream_t s) {
         sc::dispatch_nb_wm(m_nbins, mp, [&](auto nbc, auto wmc) {
             constexpr int NB = decltype(nbc)::value;
             constexpr int WM = decltype(wmc)::value;
-            auto kern = mc_score_wm_kernel<NB, WM>;
+            auto kern = mc_score_wm_kernel<NB, WM, 0>;
+            if constexpr (WM == 16) {
+                if (mp.wmask == sc::kFixedMask16 && mp.wmax == 16) {
+                    kern = mc_score_wm_kernel<NB, WM, sc::kFixedMask16>;
+                }
+            }
             const uint32_t Tw = 128;
             const size_t smem_w = static_cast<size_t>(Tw) * (NB + WM + 2) * sizeof(float);
             sc::set_smem(kern, smem_w);
