@@ -319,9 +319,13 @@ struct FinalArgs {
     uint64_t ncur, nprev;
     uint32_t nbins, nbf, jcount, rs;
     ScoreParams sp;
+    MaskScoreParams mp;     // the masked scorer's widths (NB > 0)
 };
 
-template <bool TAYLOR, int NW, int NBF>
+// NB > 0: nbins NB (32 or 64) with the widths in mp, scored by the masked
+// scorer (rows of NB + WM + 2 floats; FM its compile-time mask or 0); NB = 0:
+// any nbins, scored by score_row.
+template <bool TAYLOR, int NW, int NBF, int NB, int WM, uint64_t FM>
 __global__ void __launch_bounds__(kFinCells)
 fourier_final_kernel(FinalArgs a) {
     extern __shared__ float4 fsm[];
@@ -439,7 +443,12 @@ fourier_final_kernel(FinalArgs a) {
             r[n / 2 + j] = (de - he) * rsqrtf(dv - hv);
         }
     }
-    sc::score_row<NW>(r, n, 1.0f, a.sp, LK_SCORE_PER_WIDTH, a.scores + (c0 + t) * a.sp.nwidths);
+    float* out = a.scores + (c0 + t) * a.sp.nwidths;
+    if constexpr (NB > 0) {
+        sc::max_snr_div_wm<NB, WM, FM>(r, a.mp, 1.0f, out);
+    } else {
+        sc::score_row<NW>(r, n, 1.0f, a.sp, LK_SCORE_PER_WIDTH, out);
+    }
 }
 
 uint32_t grid_for(uint64_t work, uint32_t per_block) {
@@ -567,6 +576,14 @@ void fourier_final_score(const float2* d_in, const void* d_coords, bool taylor, 
     a.jcount = fourier_final_jcount(nbins);
     a.rs = sc::row_stride(nbins, sp.wmax);
     a.sp = sp;
+    MaskScoreParams mp{};
+    const bool masked = (nbins == 32 || nbins == 64) && make_mask_score_params(sp, nbins, &mp);
+    uint32_t wm = 0;
+    if (masked) {
+        wm = mp.wmax <= 8 ? 8u : (mp.wmax <= 16 ? 16u : 32u);
+        a.rs = nbins + wm + 2;  // even: rows start on 8 bytes
+        a.mp = mp;
+    }
     const size_t tile = std::max(sizeof(float4) * a.nbf * kFinPitch, sizeof(float) * kFinCells * a.rs);
     const size_t smem = sizeof(float4) * ((a.jcount * a.nbf + 1) / 2) + tile;
     const uint64_t blocks = (ncur + kFinCells - 1) / kFinCells;
@@ -578,12 +595,33 @@ void fourier_final_score(const float2* d_in, const void* d_coords, bool taylor, 
     auto by_nbf = [&](auto tay, auto nw) {
         constexpr bool T = decltype(tay)::value;
         constexpr int NW = decltype(nw)::value;
-        if (a.nbf <= 9) {
-            launch(fourier_final_kernel<T, NW, 9>);
+        if (masked) {
+            auto by_wm = [&](auto nbf, auto nbc) {
+                constexpr int NBF = decltype(nbf)::value;
+                constexpr int NB = decltype(nbc)::value;
+                if (wm == 8) {
+                    launch(fourier_final_kernel<T, NW, NBF, NB, 8, 0>);
+                } else if (wm == 16) {
+                    if (mp.wmask == sc::kFixedMask16 && mp.wmax == 16) {
+                        launch(fourier_final_kernel<T, NW, NBF, NB, 16, sc::kFixedMask16>);
+                    } else {
+                        launch(fourier_final_kernel<T, NW, NBF, NB, 16, 0>);
+                    }
+                } else {
+                    launch(fourier_final_kernel<T, NW, NBF, NB, 32, 0>);
+                }
+            };
+            if (nbins == 32) {
+                by_wm(std::integral_constant<int, 17>{}, std::integral_constant<int, 32>{});
+            } else {
+                by_wm(std::integral_constant<int, 33>{}, std::integral_constant<int, 64>{});
+            }
+        } else if (a.nbf <= 9) {
+            launch(fourier_final_kernel<T, NW, 9, 0, 0, 0>);
         } else if (a.nbf <= 17) {
-            launch(fourier_final_kernel<T, NW, 17>);
+            launch(fourier_final_kernel<T, NW, 17, 0, 0, 0>);
         } else {
-            launch(fourier_final_kernel<T, NW, 33>);
+            launch(fourier_final_kernel<T, NW, 33, 0, 0, 0>);
         }
     };
     auto by_nw = [&](auto tay) {

@@ -220,8 +220,10 @@ __device__ __noinline__ inline float dmax_first(const float* r, uint32_t w, uint
 // FM: the width mask as a compile-time constant (mp.wmask == FM; its widest
 // width WM), so that the width bodies not taken are not generated, or 0 to
 // test mp.wmask at run time.
+// out: when given, each width's S/N is also stored at out[slot of the width].
 template <int NB, int WM, uint64_t FM = 0>
-__device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams& mp, float stdnoise) {
+__device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams& mp, float stdnoise,
+                                                float* out = nullptr) {
     constexpr int CH = 16;
     static_assert(NB % CH == 0 && WM <= 32, "masked scorer shape");
     float2* r2 = reinterpret_cast<float2*>(r);
@@ -289,6 +291,9 @@ __device__ __forceinline__ float max_snr_div_wm(float* r, const MaskScoreParams&
             }
             const float base = __fsub_rn(__fmul_rn(mp.hb[w], d), __fmul_rn(mp.b[w], sum));
             const float snr = __fdiv_rn(base, stdnoise);
+            if (out != nullptr) {
+                out[mp.slot[w]] = snr;
+            }
             best = (best < snr) ? snr : best;
         }
     }
